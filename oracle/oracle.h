@@ -1,0 +1,132 @@
+// CPU oracle: a sequential restatement of the reference's serial pixel chain,
+// used only as the checker by tests/, __graft_entry__.smoke() and the
+// cpu_baseline leg of bench.py.  Nothing in the product links or calls it.
+//
+// Each function states the reference file:line it follows (paths relative to
+// the reference's src/serial tree).  Integer outputs and all orderings are
+// those of the serial backend; floating-point expressions keep the reference's
+// evaluation order and types (including where an unqualified call such as
+// fabs(float) resolves to the double overload in the serial build).
+#ifndef PIXORACLE_H
+#define PIXORACLE_H
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "pixfmt.h"
+
+namespace oracle {
+
+struct ES {
+  std::unique_ptr<PfCablingMap> cab;
+  std::vector<uint8_t> modToUnp;
+  PfGainHeader gain;
+  std::vector<uint8_t> gainPayload;
+  PfCommonParams common;
+  std::vector<PfDetParams> det;
+  PfAverageGeometry ag;
+  PfLayerGeometry lg;
+  PfBeamSpot bs;
+  std::vector<uint32_t> fedIds;
+};
+
+// parse the ES file images (pixfmt.h); throws std::runtime_error on malformed input
+void loadES(ES& es, const uint8_t* cabling, size_t ncab, const uint8_t* gain, size_t ngain, const uint8_t* cpe,
+            size_t ncpe, const uint8_t* bs, size_t nbs, const uint8_t* fedids, size_t nfed);
+
+struct Words {
+  std::vector<uint32_t> word;
+  std::vector<uint8_t> fedId;  // one per word pair, fedId - 1200
+  uint32_t nWords = 0;
+};
+
+struct Digis {
+  uint32_t nDigis = 0, nModules = 0;
+  std::vector<uint16_t> xx, yy, adc, moduleInd;
+  std::vector<int32_t> clus;
+  std::vector<uint32_t> pdigi, rawIdArr;
+  std::vector<PfPixelError> errors;
+};
+
+struct Clusters {
+  uint32_t nClusters = 0;
+  std::vector<uint32_t> moduleStart, clusInModule, moduleId, clusModuleStart;
+};
+
+struct Hits {
+  uint32_t nHits = 0;
+  std::vector<float> xl, yl, xerr, yerr, xg, yg, zg, rg;
+  std::vector<int32_t> charge;
+  std::vector<int16_t> iphi, xsize, ysize;
+  std::vector<uint16_t> detInd;
+  uint32_t layerStart[11] = {};
+  std::vector<uint32_t> phiOff;    // 10*128+1
+  std::vector<uint16_t> phiBins;   // nHits
+  PfAverageGeometry agc;           // beam-spot corrected average geometry
+};
+
+constexpr uint32_t kTupleBins = PF_TRACK_STRIDE;  // OneToManyAssoc<uint16, 32768, 163840>
+
+struct CA {
+  uint32_t nCells = 0;
+  std::vector<uint16_t> inner, outer, used;
+  std::vector<int16_t> layerPair;
+  std::vector<int32_t> doubletId;
+  std::vector<float> innerZ, innerR;
+  std::vector<std::vector<uint32_t>> outerHitCells;  // per hit, capped at 128
+  std::vector<std::vector<uint32_t>> nbr;            // per cell, capped at 36
+  std::vector<std::vector<uint16_t>> trk;            // per cell, capped at 48
+  int32_t nbrPool = 1, trkPool = 1;                  // SimpleVector sizes (slot 0 = empty list)
+  // tuples
+  uint32_t apcM = 0, apcN = 0;                       // AtomicPairCounter {m, n}
+  std::vector<uint32_t> tupleOff;                    // kTupleBins + 1
+  std::vector<uint16_t> tupleHits;                   // 5 * kTupleBins
+  std::vector<uint16_t> tupleDet;
+  std::vector<uint8_t> quality;                      // kTupleBins
+  std::vector<uint32_t> tmOff;                       // TupleMultiplicity off[9]
+  std::vector<uint16_t> tmBins;
+  // fit results
+  std::vector<float> state, cov, pt, eta, chi2;      // state[i*5+k], cov[i*15+k]
+  uint32_t size(uint32_t t) const { return tupleOff[t + 1] - tupleOff[t]; }
+};
+
+struct Vertices {
+  uint32_t nvFinal = 0;
+  std::vector<float> zv, wv, chi2, ptv2;
+  std::vector<int32_t> ndof;
+  std::vector<uint16_t> sortInd;
+  std::vector<int16_t> idv;
+};
+
+struct Event {
+  Words words;
+  Digis digis;
+  Clusters clusters;
+  Hits hits;
+  CA ca;
+  Vertices vtx;
+};
+
+// plugin-SiPixelClusterizer/SiPixelRawToClusterCUDA.cc:78-138 (FED loop, ErrorChecker, WordFedAppender)
+void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w);
+// SiPixelRawToClusterGPUKernel::makeClusters (SiPixelRawToClusterGPUKernel.cc:509-600)
+void makeClusters(const ES& es, const Words& w, Digis& d, Clusters& c);
+// PixelRecHitGPUKernel::makeHits (plugin-SiPixelRecHits/PixelRecHits.cc:33-53)
+void makeHits(const ES& es, const Digis& d, const Clusters& c, Hits& h);
+// CAHitNtupletGeneratorOnGPU::makeTuples (plugin-PixelTriplets/CAHitNtupletGeneratorOnGPU.cc:96-126)
+void makeTuples(const ES& es, const Hits& h, CA& ca);
+// gpuVertexFinder::Producer::make (plugin-PixelVertexFinding/gpuVertexFinderImpl.h:84-111)
+void makeVertices(const CA& ca, Vertices& v);
+
+// broken-line fit of one tuple of N (3 or 4) hits; results in the TrackSoA layout
+void brokenLineFit(int N, const double* hits /*3xN col-major*/, const float* hits_ge /*6xN*/, double B,
+                   float* state5, float* cov15, float* pt, float* eta, float* chi2);
+
+// whole chain for one raw.bin event record
+void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev);
+
+}  // namespace oracle
+
+#endif

@@ -1,0 +1,187 @@
+"""Checker-side Python access to the CPU oracle (liboracle.so) and to the
+checker build of the reference's serial sources (oracle/_ref/libpixref.so).
+
+Test infrastructure only: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline leg of bench.py, never by the product path.
+"""
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path.insert(0, os.path.join(ROOT, "pixeltrack-standalone_b200"))
+import build as _build  # noqa: E402
+from pixgpu import ERROR_DTYPE, SCALARS, _TYPES  # noqa: E402
+
+PRODUCTS = ["nDigis", "nModules", "xx", "yy", "adc", "moduleInd", "clus", "pdigi", "rawIdArr", "errors", "nClusters",
+            "moduleStart", "clusInModule", "moduleId", "clusModuleStart", "nHits", "xl", "yl", "xerr", "yerr", "xg",
+            "yg", "zg", "rg", "charge", "iphi", "xsize", "ysize", "detInd", "hitsLayerStart", "phiOff", "phiBins",
+            "nCells", "cellInner", "cellOuter", "cellLayerPair", "cellDoubletId", "cellUsed", "cellNbrOff",
+            "cellNbr", "cellTrkOff", "cellTrk", "outerHitOff", "outerHitCells", "nNbrLists", "nTrkLists", "nTuples",
+            "tupleOff", "tupleHits", "tupleDet", "quality", "state", "cov", "pt", "eta", "chi2", "nVertices", "zv",
+            "wv", "vchi2", "ptv2", "ndof", "sortInd", "idv"]
+
+
+def _decode(buf, name, elem):
+    if name == "errors":
+        return np.frombuffer(buf, dtype=ERROR_DTYPE).copy()
+    if name in SCALARS:
+        return int(np.frombuffer(buf, dtype=np.uint32)[0])
+    dt = _TYPES.get(name)
+    if dt is None or np.dtype(dt).itemsize != elem:
+        dt = {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[elem]
+    return np.frombuffer(buf, dtype=dt).copy()
+
+
+class _Named:
+    _get = None
+
+    def _products(self, names):
+        out = {}
+        for n in names:
+            d = ctypes.c_void_p()
+            c = ctypes.c_size_t()
+            e = ctypes.c_int()
+            if self._get(self._h, n.encode(), ctypes.byref(d), ctypes.byref(c), ctypes.byref(e)) != 0:
+                continue
+            out[n] = _decode(ctypes.string_at(d, c.value * e.value), n, e.value)
+        return out
+
+
+class Oracle(_Named):
+    """Sequential restatement of the serial chain (oracle/*.cc)."""
+
+    def __init__(self, es_images):
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            _build.build_oracle()
+        self.lib = ctypes.CDLL(path)
+        self.lib.or_create.restype = ctypes.c_void_p
+        self.lib.or_create.argtypes = [ctypes.c_char_p, ctypes.c_size_t] * 5
+        self.lib.or_process.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+        self.lib.or_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p),
+                                    ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int)]
+        self.lib.or_last_seconds.argtypes = [ctypes.c_void_p]
+        self.lib.or_last_seconds.restype = ctypes.c_double
+        self.lib.or_time_events.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_char_p),
+                                            ctypes.POINTER(ctypes.c_size_t), ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_void_p]
+        self.lib.or_time_events.restype = ctypes.c_double
+        self.lib.or_fit.argtypes = [ctypes.c_int, ctypes.c_uint32] + [ctypes.c_void_p] * 2 + [ctypes.c_double] + \
+            [ctypes.c_void_p] * 5
+        self.lib.or_destroy.argtypes = [ctypes.c_void_p]
+        self._keep = list(es_images)
+        args = []
+        for b in self._keep:
+            args += [b, len(b)]
+        self._h = ctypes.c_void_p(self.lib.or_create(*args))
+        if not self._h.value:
+            raise RuntimeError("oracle: malformed ES images")
+        self._get = self.lib.or_get
+
+    def process(self, raw, names=None):
+        if self.lib.or_process(self._h, raw, len(raw)) != 0:
+            raise RuntimeError("oracle failed on this event")
+        return self._products(names or PRODUCTS)
+
+    def last_seconds(self):
+        return self.lib.or_last_seconds(self._h)
+
+    def time_events(self, raws, threads=1):
+        """Wall seconds and per-event seconds for the chain over raws on `threads` host threads."""
+        n = len(raws)
+        ptrs = (ctypes.c_char_p * n)(*raws)
+        sizes = (ctypes.c_size_t * n)(*[len(r) for r in raws])
+        lat = np.zeros(n, dtype=np.float64)
+        wall = self.lib.or_time_events(self._h, ptrs, sizes, n, threads, lat.ctypes.data)
+        if wall < 0:
+            raise RuntimeError("oracle failed while timing")
+        return wall, lat
+
+    def fit(self, N, hits, ge, B=0.0114256972711507):
+        n = hits.shape[0]
+        h = np.ascontiguousarray(hits[:, :N, :], dtype=np.float64)
+        g = np.ascontiguousarray(ge[:, :N, :], dtype=np.float32)
+        out = {"state": np.zeros((n, 5), np.float32), "cov": np.zeros((n, 15), np.float32),
+               "pt": np.zeros(n, np.float32), "eta": np.zeros(n, np.float32), "chi2": np.zeros(n, np.float32)}
+        rc = self.lib.or_fit(N, n, h.ctypes.data, g.ctypes.data, B, out["state"].ctypes.data, out["cov"].ctypes.data,
+                             out["pt"].ctypes.data, out["eta"].ctypes.data, out["chi2"].ctypes.data)
+        if rc != 0:
+            raise RuntimeError("oracle fit failed")
+        return out
+
+    def __del__(self):
+        try:
+            self.lib.or_destroy(self._h)
+        except Exception:
+            pass
+
+
+REF_LIB = os.path.join(HERE, "_ref", "libpixref.so")
+
+
+def ref_available():
+    return os.path.exists(REF_LIB)
+
+
+class Reference(_Named):
+    """The reference's own serial chain, compiled from its sources (checker build)."""
+
+    def __init__(self, datadir):
+        self.lib = ctypes.CDLL(REF_LIB)
+        self.lib.pr_create.restype = ctypes.c_void_p
+        self.lib.pr_create.argtypes = [ctypes.c_char_p]
+        self.lib.pr_process.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int]
+        self.lib.pr_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p),
+                                    ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int)]
+        self.lib.pr_last_seconds.argtypes = [ctypes.c_void_p]
+        self.lib.pr_last_seconds.restype = ctypes.c_double
+        self._h = ctypes.c_void_p(self.lib.pr_create(datadir.encode()))
+        self._get = self.lib.pr_get
+
+    def process(self, raw, names=None, internals=True):
+        if self.lib.pr_process(self._h, raw, len(raw), 1 if internals else 0) != 0:
+            raise RuntimeError("reference chain failed")
+        return self._products(names or PRODUCTS)
+
+    def last_seconds(self):
+        return self.lib.pr_last_seconds(self._h)
+
+
+def compare(a, b, names=None, rtol=1e-5):
+    """Differences between two product dicts: integers exactly, floats within rtol."""
+    diffs = []
+    for n in names or PRODUCTS:
+        if n not in a and n not in b:
+            continue
+        if (n in a) != (n in b):
+            diffs.append((n, "missing on one side"))
+            continue
+        x, y = a[n], b[n]
+        if isinstance(x, int) or isinstance(y, int):
+            if int(x) != int(y):
+                diffs.append((n, "value %d != %d" % (x, y)))
+            continue
+        if x.shape != y.shape:
+            diffs.append((n, "shape %s != %s" % (x.shape, y.shape)))
+            continue
+        if n == "errors":
+            for f in ("rawId", "word", "errorType", "fedId"):
+                if not np.array_equal(x[f], y[f]):
+                    diffs.append((n, "error records differ in %s" % f))
+            continue
+        if x.dtype.kind == "f":
+            xd, yd = x.astype(np.float64), y.astype(np.float64)
+            both_nan = np.isnan(xd) & np.isnan(yd)
+            den = np.maximum(np.abs(xd), np.abs(yd))
+            rel = np.where(both_nan, 0.0, np.abs(xd - yd) / np.where(den > 0, den, 1.0))
+            bad = rel > rtol
+            if bad.any():
+                diffs.append((n, "%d values beyond rtol %g (max rel %.3g)" % (int(bad.sum()), rtol, float(rel.max()))))
+        elif not np.array_equal(x, y):
+            i = np.nonzero(x != y)[0]
+            diffs.append((n, "%d entries differ, first at %d: %s vs %s" % (len(i), i[0], x[i[0]], y[i[0]])))
+    return diffs

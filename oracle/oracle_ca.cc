@@ -359,6 +359,8 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca) {
     ca.tmOff[nh]++;
   }
   for (int b = 1; b < 9; ++b) ca.tmOff[b] += ca.tmOff[b - 1];
+  // beyond this capacity the reference writes past TupleMultiplicity::bins
+  if (ca.tmOff[8] > PF_MAX_TUPLES) throw std::runtime_error("undefined in the reference: TupleMultiplicity overflow");
   for (uint32_t it = 0; it < kTupleBins; ++it) {
     uint32_t nh = ca.size(it);
     if (nh < 3) continue;
@@ -452,6 +454,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca) {
     for (uint32_t k = ca.tupleOff[idx]; k < ca.tupleOff[idx + 1]; ++k) h2tOff[ca.tupleHits[k]]++;
   }
   for (uint32_t b = 1; b < h2tOff.size(); ++b) h2tOff[b] += h2tOff[b - 1];
+  if (h2tOff.back() > h2t.size()) throw std::runtime_error("undefined in the reference: HitToTuple overflow");
   for (uint32_t idx = 0; idx < kTupleBins; ++idx) {
     if (ca.size(idx) == 0) break;
     if (ca.quality[idx] != kLoose) continue;

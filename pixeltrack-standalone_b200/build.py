@@ -1,0 +1,106 @@
+"""Build recipe for the native libraries of this repository.
+
+lib/libpixgpu.so    the B200 chain (CUDA, sm_100a) behind include/pixgpu.h
+lib/libpixsynth.so  the seeded synthetic detector/event generator (include/pixsynth.h)
+oracle/liboracle.so the CPU oracle used by the tests (checker only)
+oracle/_ref/        checker build of the reference's serial sources (only where they exist)
+
+Everything is compiled in-tree so the libraries travel with the repository.
+"""
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+LIB = os.path.join(PKG, "lib")
+CSRC = os.path.join(PKG, "csrc")
+INC = os.path.join(ROOT, "include")
+OBJ = os.path.join(PKG, "_build")
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# --fmad=false: the reference's serial arithmetic has no fused multiply-add,
+# and bit-exact cluster/hit/doublet/tuple results depend on it.
+NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-I", INC, "-I", CSRC,
+           "--expt-relaxed-constexpr"] + ARCH
+CU_SOURCES = ["scan.cu", "k_local.cu", "k_ca.cu", "k_fit.cu", "k_vertex.cu", "chain.cu", "capi.cu"]
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build step failed: %s\n%s" % (" ".join(cmd), r.stdout))
+    return r.stdout
+
+
+def _stale(target, sources):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources)
+
+
+def _headers(d):
+    return [os.path.join(d, f) for f in os.listdir(d) if f.endswith((".h", ".cuh"))]
+
+
+def build_gpu(verbose=False):
+    os.makedirs(LIB, exist_ok=True)
+    os.makedirs(OBJ, exist_ok=True)
+    target = os.path.join(LIB, "libpixgpu.so")
+    deps = _headers(CSRC) + _headers(INC)
+    objs, jobs = [], []
+    for src in CU_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJ, src + ".o")
+        objs.append(o)
+        if _stale(o, [s] + deps):
+            jobs.append([NVCC] + NVFLAGS + ["-c", s, "-o", o])
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        for out in ex.map(_run, jobs):
+            if verbose and out.strip():
+                print(out)
+    if jobs or _stale(target, objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", target] + objs + ["-lcudart"])
+    return target
+
+
+def build_synth():
+    os.makedirs(LIB, exist_ok=True)
+    src = os.path.join(CSRC, "synth", "pixsynth.cc")
+    target = os.path.join(LIB, "libpixsynth.so")
+    if _stale(target, [src] + _headers(INC)):
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I", INC, src, "-o", target])
+    return target
+
+
+def build_oracle():
+    d = os.path.join(ROOT, "oracle")
+    srcs = [os.path.join(d, f) for f in ("oracle_local.cc", "oracle_ca.cc", "oracle_fit.cc", "oracle_vertex.cc",
+                                         "oracle_api.cc")]
+    target = os.path.join(d, "liboracle.so")
+    if _stale(target, srcs + [os.path.join(d, "oracle.h")] + _headers(INC)):
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-pthread", "-I", INC] + srcs + ["-o", target])
+    return target
+
+
+def build_ref(reference="/root/reference"):
+    """Checker build of the reference serial sources (skipped where they are absent)."""
+    if not os.path.isdir(os.path.join(reference, "src", "serial")):
+        return None
+    _run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle", "ref"), "REF=" + reference])
+    return os.path.join(ROOT, "oracle", "_ref", "libpixref.so")
+
+
+def build_all(gpu=True):
+    out = {"synth": build_synth(), "oracle": build_oracle(), "ref": build_ref()}
+    if gpu:
+        out["gpu"] = build_gpu()
+    return out
+
+
+if __name__ == "__main__":
+    print(build_all(gpu="--no-gpu" not in sys.argv))

@@ -1,0 +1,493 @@
+// C ABI of the B200 pixel chain (include/pixgpu.h): context, ES upload,
+// host FED scan, batch slots and product access.
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "pixgpu.h"
+#include "pixgpu_internal.cuh"
+
+namespace pixgpu {
+cudaError_t fitDirect(int N, uint32_t n, const double* hits, const float* ge, double B, float* state, float* cov,
+                      float* pt, float* eta, float* chi2, cudaStream_t stream);
+}
+
+using namespace pixgpu;
+
+namespace {
+
+struct HostES {
+  std::vector<uint32_t> fedIds;
+};
+
+struct Slot {
+  void* dmem = nullptr;
+  Workspace ws{};
+  cudaStream_t stream = nullptr;
+  uint32_t* hWords = nullptr;   // pinned staging
+  uint8_t* hFed = nullptr;
+  uint32_t* hOffsets = nullptr;
+  uint32_t nEvents = 0;
+  bool staged = false;
+};
+
+}  // namespace
+
+struct pg_ctx {
+  int device = 0;
+  pg_config cfg{};
+  HostES hes;
+  void* esMem = nullptr;
+  DeviceES des{};
+  std::vector<Slot> slots;
+  std::string err;
+  std::mutex mu;
+};
+
+namespace {
+
+int fail(pg_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+int cudaFail(pg_ctx* c, cudaError_t e, const char* where) {
+  return fail(c, PG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+struct Rd {
+  const uint8_t* p;
+  size_t n, off = 0;
+  bool ok = true;
+  void bytes(void* d, size_t k) {
+    if (off + k > n) {
+      ok = false;
+      return;
+    }
+    std::memcpy(d, p + off, k);
+    off += k;
+  }
+  template <typename T>
+  T get() {
+    T x{};
+    bytes(&x, sizeof(T));
+    return x;
+  }
+};
+
+// FED scan: Source record -> (words, fed index per word pair); follows
+// SiPixelRawToClusterCUDA.cc:78-138 with ErrorChecker.cc:36-91 semantics.
+int unpackRaw(const std::vector<uint32_t>& fedIds, const uint8_t* raw, size_t n, uint32_t* words, uint8_t* fed,
+              uint32_t cap, uint32_t* nWordsOut) {
+  const uint8_t* fedPtr[4096];
+  uint32_t fedSize[4096];
+  std::memset(fedSize, 0, sizeof(fedSize));
+  Rd r{raw, n};
+  uint32_t nfeds = r.get<uint32_t>();
+  if (!r.ok) return PG_ERR_FORMAT;
+  for (uint32_t i = 0; i < nfeds; ++i) {
+    uint32_t id = r.get<uint32_t>(), size = r.get<uint32_t>();
+    if (!r.ok || id >= 4096 || r.off + size > n) return PG_ERR_FORMAT;
+    fedPtr[id] = raw + r.off;
+    fedSize[id] = size;
+    r.off += size;
+  }
+  uint32_t wc = 0;
+  for (uint32_t fedId : fedIds) {
+    if (fedId == 40 || fedId >= 4096) continue;
+    uint32_t size = fedSize[fedId];
+    int n64 = int(size / 8);
+    if (n64 == 0) continue;
+    const uint8_t* d = fedPtr[fedId];
+    auto w64 = [&](int k) {
+      uint64_t v;
+      std::memcpy(&v, d + 8 * size_t(k), 8);
+      return v;
+    };
+    if ((w64(n64 - 1) >> 2) & 1) continue;  // CRC-modified bit
+    int h = -1;
+    bool more = true;
+    while (more && h + 1 < n64) {
+      ++h;
+      uint64_t v = w64(h);
+      more = (((uint32_t(v >> 32)) >> 28) & 0xf) == 0x5 && ((uint32_t(v) >> 3) & 1);
+    }
+    int t = n64;
+    more = true;
+    while (more && t > 0) {
+      --t;
+      uint64_t v = w64(t);
+      more = (((uint32_t(v >> 32)) >> 28) & 0xf) == 0xa && ((uint32_t(v) >> 3) & 1);
+    }
+    if (t < h + 1) continue;
+    uint32_t len = uint32_t(t - (h + 1)) * 2;
+    if (wc + len > cap) return PG_ERR_CAPACITY;
+    std::memcpy(words + wc, d + 8 * size_t(h + 1), 4 * size_t(len));
+    std::memset(fed + wc / 2, int(fedId - 1200), len / 2);
+    wc += len;
+  }
+  *nWordsOut = wc;
+  return PG_OK;
+}
+
+int uploadES(pg_ctx* c, const pg_es_images* es) {
+  Rd cab{es->cabling, es->cabling_size}, gain{es->gain, es->gain_size}, cpe{es->cpe, es->cpe_size},
+      bs{es->beamspot, es->beamspot_size}, fi{es->fedids, es->fedids_size};
+  // sizes
+  if (es->cabling_size < sizeof(PfCablingMap) + 4) return fail(c, PG_ERR_FORMAT, "cabling image too short");
+  uint32_t nUnp;
+  std::memcpy(&nUnp, es->cabling + sizeof(PfCablingMap), 4);
+  if (es->cabling_size < sizeof(PfCablingMap) + 4 + nUnp || nUnp < PF_MAX_SIZE)
+    return fail(c, PG_ERR_FORMAT, "cabling image: modToUnp size");
+  if (es->gain_size < sizeof(PfGainHeader) + 4) return fail(c, PG_ERR_FORMAT, "gain image too short");
+  uint32_t nGain;
+  std::memcpy(&nGain, es->gain + sizeof(PfGainHeader), 4);
+  if (es->gain_size < sizeof(PfGainHeader) + 4 + nGain) return fail(c, PG_ERR_FORMAT, "gain payload truncated");
+  PfGainHeader gh;
+  std::memcpy(&gh, es->gain, sizeof(gh));
+  for (int i = 0; i < PF_MAX_MODULES; ++i) {
+    if (gh.rangeAndCols[i].nCols <= 0 || gh.rangeAndCols[i].second > nGain)
+      return fail(c, PG_ERR_FORMAT, "gain ranges outside the payload");
+  }
+  PfCommonParams common = cpe.get<PfCommonParams>();
+  uint32_t nDet = cpe.get<uint32_t>();
+  if (!cpe.ok || nDet < PF_N_MODULES || nDet > 4096) return fail(c, PG_ERR_FORMAT, "cpe image: detector count");
+  std::vector<PfDetParams> det(nDet);
+  cpe.bytes(det.data(), nDet * sizeof(PfDetParams));
+  PfAverageGeometry ag = cpe.get<PfAverageGeometry>();
+  PfLayerGeometry lg = cpe.get<PfLayerGeometry>();
+  if (!cpe.ok) return fail(c, PG_ERR_FORMAT, "cpe image truncated");
+  PfBeamSpot b = bs.get<PfBeamSpot>();
+  if (!bs.ok) return fail(c, PG_ERR_FORMAT, "beamspot image truncated");
+  uint32_t nf = fi.get<uint32_t>();
+  if (!fi.ok || nf > 4096) return fail(c, PG_ERR_FORMAT, "fedIds image");
+  c->hes.fedIds.resize(nf);
+  fi.bytes(c->hes.fedIds.data(), nf * 4);
+  if (!fi.ok) return fail(c, PG_ERR_FORMAT, "fedIds image truncated");
+  // one device allocation for the resident conditions
+  size_t off = 0;
+  auto place = [&](size_t bytes) {
+    off = (off + 255) & ~size_t(255);
+    size_t o = off;
+    off += bytes;
+    return o;
+  };
+  size_t oCab = place(sizeof(PfCablingMap)), oUnp = place(PF_MAX_SIZE), oGh = place(sizeof(PfGainHeader)),
+         oGp = place(nGain), oCom = place(sizeof(PfCommonParams)), oDet = place(nDet * sizeof(PfDetParams)),
+         oAg = place(sizeof(PfAverageGeometry)), oLg = place(sizeof(PfLayerGeometry)), oBs = place(sizeof(PfBeamSpot));
+  cudaError_t e = cudaMalloc(&c->esMem, off);
+  if (e != cudaSuccess) return cudaFail(c, e, "cudaMalloc(ES)");
+  char* base = static_cast<char*>(c->esMem);
+  struct Cp {
+    size_t o;
+    const void* src;
+    size_t n;
+  } cps[] = {{oCab, es->cabling, sizeof(PfCablingMap)},
+             {oUnp, es->cabling + sizeof(PfCablingMap) + 4, PF_MAX_SIZE},
+             {oGh, es->gain, sizeof(PfGainHeader)},
+             {oGp, es->gain + sizeof(PfGainHeader) + 4, nGain},
+             {oCom, &common, sizeof(common)},
+             {oDet, det.data(), nDet * sizeof(PfDetParams)},
+             {oAg, &ag, sizeof(ag)},
+             {oLg, &lg, sizeof(lg)},
+             {oBs, &b, sizeof(b)}};
+  for (auto& cp : cps) {
+    e = cudaMemcpy(base + cp.o, cp.src, cp.n, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cudaFail(c, e, "cudaMemcpy(ES)");
+  }
+  c->des.cab = reinterpret_cast<const PfCablingMap*>(base + oCab);
+  c->des.modToUnp = reinterpret_cast<const uint8_t*>(base + oUnp);
+  c->des.gainHdr = reinterpret_cast<const PfGainHeader*>(base + oGh);
+  c->des.gainPayload = reinterpret_cast<const uint8_t*>(base + oGp);
+  c->des.common = reinterpret_cast<const PfCommonParams*>(base + oCom);
+  c->des.det = reinterpret_cast<const PfDetParams*>(base + oDet);
+  c->des.ag = reinterpret_cast<const PfAverageGeometry*>(base + oAg);
+  c->des.lg = reinterpret_cast<const PfLayerGeometry*>(base + oLg);
+  c->des.bs = reinterpret_cast<const PfBeamSpot*>(base + oBs);
+  c->des.nDet = nDet;
+  c->des.gainPayloadSize = nGain;
+  return PG_OK;
+}
+
+int stage(pg_ctx* c, Slot& s, uint32_t nEvents, const uint8_t* const* raws, const size_t* sizes) {
+  if (nEvents == 0 || nEvents > c->cfg.max_events) return fail(c, PG_ERR_CAPACITY, "batch size");
+  uint32_t off = 0;
+  for (uint32_t k = 0; k < nEvents; ++k) {
+    s.hOffsets[k] = off;
+    uint32_t nw = 0;
+    uint32_t room = c->cfg.max_words_per_batch - off;
+    room = room > kMaxFedWords ? kMaxFedWords : room;
+    int rc = unpackRaw(c->hes.fedIds, raws[k], sizes[k], s.hWords + off, s.hFed + off / 2, room, &nw);
+    if (rc != PG_OK) return fail(c, rc, rc == PG_ERR_CAPACITY ? "event or batch too large" : "malformed raw record");
+    off += nw;
+  }
+  s.hOffsets[nEvents] = off;
+  cudaError_t e;
+  if (off) {
+    if ((e = cudaMemcpyAsync(s.ws.words, s.hWords, size_t(off) * 4, cudaMemcpyHostToDevice, s.stream)) != cudaSuccess)
+      return cudaFail(c, e, "H2D words");
+    if ((e = cudaMemcpyAsync(s.ws.fedIds, s.hFed, size_t(off) / 2 + 1, cudaMemcpyHostToDevice, s.stream)) !=
+        cudaSuccess)
+      return cudaFail(c, e, "H2D fedIds");
+  }
+  if ((e = cudaMemcpyAsync(s.ws.wordOffsets, s.hOffsets, size_t(nEvents + 1) * 4, cudaMemcpyHostToDevice,
+                           s.stream)) != cudaSuccess)
+    return cudaFail(c, e, "H2D offsets");
+  s.nEvents = nEvents;
+  s.staged = true;
+  return PG_OK;
+}
+
+template <typename T>
+int copyOut(pg_ctx* c, Slot& s, const T* src, size_t n, void* dst, size_t cap, size_t* count, int* elem) {
+  *elem = int(sizeof(T));
+  *count = n;
+  if (!dst) return PG_OK;
+  if (n * sizeof(T) > cap) return fail(c, PG_ERR_CAPACITY, "product larger than the destination");
+  if (n == 0) return PG_OK;
+  cudaError_t e = cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToHost, s.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);
+  if (e != cudaSuccess) return cudaFail(c, e, "D2H product");
+  return PG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void pg_default_config(pg_config* cfg) {
+  cfg->device = 0;
+  cfg->max_events = 64;
+  cfg->max_words_per_batch = 64u * 160000u;
+  cfg->slots = 1;
+}
+
+int pg_create(const pg_es_images* es, const pg_config* cfgIn, pg_ctx** out) {
+  if (!es || !out) return PG_ERR_ARG;
+  *out = nullptr;
+  auto c = std::make_unique<pg_ctx>();
+  if (cfgIn)
+    c->cfg = *cfgIn;
+  else
+    pg_default_config(&c->cfg);
+  if (c->cfg.max_events == 0 || c->cfg.slots == 0 || c->cfg.max_words_per_batch == 0) return PG_ERR_ARG;
+  cudaError_t e = cudaSetDevice(c->cfg.device);
+  if (e != cudaSuccess) return PG_ERR_CUDA;
+  int rc = uploadES(c.get(), es);
+  if (rc != PG_OK) {
+    if (c->esMem) cudaFree(c->esMem);
+    return rc;
+  }
+  size_t bytes = workspaceBytes(c->cfg.max_events, c->cfg.max_words_per_batch);
+  c->slots.resize(c->cfg.slots);
+  for (auto& s : c->slots) {
+    if ((e = cudaMalloc(&s.dmem, bytes)) != cudaSuccess) {
+      pg_destroy(c.release());
+      return PG_ERR_NOMEM;
+    }
+    workspaceCarve(s.ws, s.dmem, c->cfg.max_events, c->cfg.max_words_per_batch);
+    if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost(&s.hWords, size_t(c->cfg.max_words_per_batch) * 4) != cudaSuccess ||
+        cudaMallocHost(&s.hFed, size_t(c->cfg.max_words_per_batch) / 2 + 16) != cudaSuccess ||
+        cudaMallocHost(&s.hOffsets, size_t(c->cfg.max_events + 1) * 4) != cudaSuccess) {
+      pg_destroy(c.release());
+      return PG_ERR_NOMEM;
+    }
+  }
+  *out = c.release();
+  return PG_OK;
+}
+
+void pg_destroy(pg_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->cfg.device);
+  for (auto& s : c->slots) {
+    if (s.stream) cudaStreamSynchronize(s.stream);
+    if (s.dmem) cudaFree(s.dmem);
+    if (s.stream) cudaStreamDestroy(s.stream);
+    if (s.hWords) cudaFreeHost(s.hWords);
+    if (s.hFed) cudaFreeHost(s.hFed);
+    if (s.hOffsets) cudaFreeHost(s.hOffsets);
+  }
+  if (c->esMem) cudaFree(c->esMem);
+  delete c;
+}
+
+const char* pg_last_error(const pg_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+size_t pg_slot_bytes(const pg_ctx* c) {
+  return c ? workspaceBytes(c->cfg.max_events, c->cfg.max_words_per_batch) : 0;
+}
+
+int pg_unpack_raw(const pg_ctx* c, const uint8_t* raw, size_t n, uint32_t* words, uint8_t* fedIds, uint32_t cap,
+                  uint32_t* nWords) {
+  if (!c || !raw || !words || !fedIds || !nWords) return PG_ERR_ARG;
+  return unpackRaw(c->hes.fedIds, raw, n, words, fedIds, cap, nWords);
+}
+
+int pg_stage_batch(pg_ctx* c, uint32_t slot, uint32_t nEvents, const uint8_t* const* raws, const size_t* sizes) {
+  if (!c || slot >= c->slots.size() || !raws || !sizes) return PG_ERR_ARG;
+  cudaSetDevice(c->cfg.device);
+  return stage(c, c->slots[slot], nEvents, raws, sizes);
+}
+
+int pg_run_staged(pg_ctx* c, uint32_t slot) {
+  if (!c || slot >= c->slots.size() || !c->slots[slot].staged) return PG_ERR_ARG;
+  Slot& s = c->slots[slot];
+  cudaError_t e = runChain(c->des, s.ws, s.nEvents, s.stream);
+  if (e != cudaSuccess) return cudaFail(c, e, "chain launch");
+  return PG_OK;
+}
+
+int pg_sync(pg_ctx* c, uint32_t slot) {
+  if (!c || slot >= c->slots.size()) return PG_ERR_ARG;
+  cudaError_t e = cudaStreamSynchronize(c->slots[slot].stream);
+  if (e != cudaSuccess) return cudaFail(c, e, "chain");
+  return PG_OK;
+}
+
+void* pg_slot_stream(pg_ctx* c, uint32_t slot) {
+  if (!c || slot >= c->slots.size()) return nullptr;
+  return c->slots[slot].stream;
+}
+
+int pg_process_batch(pg_ctx* c, uint32_t nEvents, const uint8_t* const* raws, const size_t* sizes) {
+  int rc = pg_stage_batch(c, 0, nEvents, raws, sizes);
+  if (rc != PG_OK) return rc;
+  rc = pg_run_staged(c, 0);
+  if (rc != PG_OK) return rc;
+  return pg_sync(c, 0);
+}
+
+int pg_event_counts_get(pg_ctx* c, uint32_t k, pg_event_counts* out) {
+  if (!c || !out || k >= c->slots[0].nEvents) return PG_ERR_ARG;
+  Slot& s = c->slots[0];
+  EventCounters ec;
+  cudaError_t e = cudaMemcpy(&ec, s.ws.ev + k, sizeof(ec), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cudaFail(c, e, "D2H counters");
+  out->n_words = ec.nWords;
+  out->n_modules = ec.nModules;
+  out->n_digi_errors = ec.nErrors;
+  out->n_hits = ec.nHits;
+  out->n_cells = ec.nCells;
+  out->n_tuples = ec.nTuples;
+  out->n_loose = ec.nLoose;
+  out->n_vertices = ec.nVertices;
+  out->flags = ec.flags;
+  return PG_OK;
+}
+
+int pg_get_product(pg_ctx* c, uint32_t k, const char* name, void* dst, size_t cap, size_t* count, int* elem) {
+  if (!c || !name || !count || !elem || k >= c->slots[0].nEvents) return PG_ERR_ARG;
+  Slot& s = c->slots[0];
+  const Workspace& ws = s.ws;
+  EventCounters ec;
+  cudaError_t e = cudaMemcpy(&ec, ws.ev + k, sizeof(ec), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cudaFail(c, e, "D2H counters");
+  std::string n(name);
+  const size_t w0 = ec.wordStart, nw = ec.nWords;
+  const size_t hb = size_t(k) * kHitCap, mb = size_t(k) * kModStride, cb = size_t(k) * kCellCap,
+               tb = size_t(k) * kTupleBins, vb = size_t(k) * kMaxVtx;
+  const uint32_t nh = ec.nHits, nc = ec.nCells;
+  if (n == "nDigis" || n == "nModules" || n == "nClusters" || n == "nHits" || n == "nCells" || n == "nTuples" ||
+      n == "nVertices" || n == "nNbrLists" || n == "nTrkLists") {
+    uint32_t v = n == "nDigis" ? ec.nWords
+                 : n == "nModules" ? ec.nModules
+                 : (n == "nClusters" || n == "nHits") ? ec.nHits
+                 : n == "nCells" ? ec.nCells
+                 : n == "nTuples" ? 0u
+                 : n == "nVertices" ? ec.nVertices
+                 : n == "nNbrLists" ? ec.nNbrLists
+                                    : ec.nTrkLists;
+    if (n == "nTuples") {
+      // number of tuples before the first empty one (the serial loops' guard)
+      uint32_t g = ec.nTuples;
+      if (ec.apcM >= kTupleBins) g = kTupleBins - 1;
+      v = g;
+    }
+    *elem = 4;
+    *count = 1;
+    if (dst) {
+      if (cap < 4) return PG_ERR_CAPACITY;
+      std::memcpy(dst, &v, 4);
+    }
+    return PG_OK;
+  }
+  uint32_t nTup = ec.apcM >= kTupleBins ? kTupleBins - 1 : ec.nTuples;
+  if (n == "xx") return copyOut(c, s, ws.xx + w0, nw, dst, cap, count, elem);
+  if (n == "yy") return copyOut(c, s, ws.yy + w0, nw, dst, cap, count, elem);
+  if (n == "adc") return copyOut(c, s, ws.adc + w0, nw, dst, cap, count, elem);
+  if (n == "moduleInd") return copyOut(c, s, ws.moduleInd + w0, nw, dst, cap, count, elem);
+  if (n == "clus") return copyOut(c, s, ws.clus + w0, nw, dst, cap, count, elem);
+  if (n == "pdigi") return copyOut(c, s, ws.pdigi + w0, nw, dst, cap, count, elem);
+  if (n == "rawIdArr") return copyOut(c, s, ws.rawIdArr + w0, nw, dst, cap, count, elem);
+  if (n == "errors") return copyOut(c, s, ws.errors + size_t(k) * kErrCap, std::min<size_t>(ec.nErrors, kErrCap), dst, cap, count, elem);
+  if (n == "moduleStart") return copyOut(c, s, ws.moduleStart + mb, kMaxModules + 1, dst, cap, count, elem);
+  if (n == "clusInModule") return copyOut(c, s, ws.clusInModule + mb, kMaxModules, dst, cap, count, elem);
+  if (n == "moduleId") return copyOut(c, s, ws.moduleId + mb, kMaxModules, dst, cap, count, elem);
+  if (n == "clusModuleStart") return copyOut(c, s, ws.clusModuleStart + mb, kMaxModules + 1, dst, cap, count, elem);
+  if (n == "xl") return copyOut(c, s, ws.xl + hb, nh, dst, cap, count, elem);
+  if (n == "yl") return copyOut(c, s, ws.yl + hb, nh, dst, cap, count, elem);
+  if (n == "xerr") return copyOut(c, s, ws.xerr + hb, nh, dst, cap, count, elem);
+  if (n == "yerr") return copyOut(c, s, ws.yerr + hb, nh, dst, cap, count, elem);
+  if (n == "xg") return copyOut(c, s, ws.xg + hb, nh, dst, cap, count, elem);
+  if (n == "yg") return copyOut(c, s, ws.yg + hb, nh, dst, cap, count, elem);
+  if (n == "zg") return copyOut(c, s, ws.zg + hb, nh, dst, cap, count, elem);
+  if (n == "rg") return copyOut(c, s, ws.rg + hb, nh, dst, cap, count, elem);
+  if (n == "charge") return copyOut(c, s, ws.charge + hb, nh, dst, cap, count, elem);
+  if (n == "iphi") return copyOut(c, s, ws.iphi + hb, nh, dst, cap, count, elem);
+  if (n == "xsize") return copyOut(c, s, ws.xsize + hb, nh, dst, cap, count, elem);
+  if (n == "ysize") return copyOut(c, s, ws.ysize + hb, nh, dst, cap, count, elem);
+  if (n == "detInd") return copyOut(c, s, ws.detInd + hb, nh, dst, cap, count, elem);
+  if (n == "hitsLayerStart") return copyOut(c, s, &ws.ev[k].layerStart[0], 11, dst, cap, count, elem);
+  if (n == "phiOff") return copyOut(c, s, ws.phiOff + size_t(k) * kPhiStride, kPhiTot, dst, cap, count, elem);
+  if (n == "phiBins") return copyOut(c, s, ws.phiBins + hb, nh, dst, cap, count, elem);
+  if (n == "cellInner") return copyOut(c, s, ws.cellInner + cb, nc, dst, cap, count, elem);
+  if (n == "cellOuter") return copyOut(c, s, ws.cellOuter + cb, nc, dst, cap, count, elem);
+  if (n == "cellUsed") return copyOut(c, s, ws.cellUsed + cb, nc, dst, cap, count, elem);
+  if (n == "cellDoubletId") return copyOut(c, s, ws.cellDoubletId + cb, nc, dst, cap, count, elem);
+  if (n == "cellLayerPair") return copyOut(c, s, ws.cellPair + cb, nc, dst, cap, count, elem);
+  if (n == "outerHitOffRaw") return copyOut(c, s, ws.ohOff + size_t(k) * (kHitCap + 1), nh + 1, dst, cap, count, elem);
+  if (n == "outerHitCellsRaw") return copyOut(c, s, ws.ohCells + cb, nc, dst, cap, count, elem);
+  if (n == "cellNbrOffRaw") return copyOut(c, s, ws.nbrOff + size_t(k) * (kCellCap + 1), nc + 1, dst, cap, count, elem);
+  if (n == "cellNbrRaw") return copyOut(c, s, ws.nbr + size_t(k) * kEdgeCap, std::min(ec.nEdges, kEdgeCap), dst, cap, count, elem);
+  if (n == "cellTrkOffRaw") return copyOut(c, s, ws.trkOff + size_t(k) * (kCellCap + 1), nc + 1, dst, cap, count, elem);
+  if (n == "cellTrkRaw") {
+    uint32_t tot = 0;
+    cudaMemcpy(&tot, ws.trkOff + size_t(k) * (kCellCap + 1) + nc, 4, cudaMemcpyDeviceToHost);
+    return copyOut(c, s, ws.trk + size_t(k) * kTupleCellCap, tot, dst, cap, count, elem);
+  }
+  if (n == "tupleOff") return copyOut(c, s, ws.tupleOff + size_t(k) * (kTupleBins + 1), nTup + 1, dst, cap, count, elem);
+  if (n == "tupleHits" || n == "tupleDet") {
+    uint32_t tot = 0;
+    cudaMemcpy(&tot, ws.tupleOff + size_t(k) * (kTupleBins + 1) + nTup, 4, cudaMemcpyDeviceToHost);
+    if (n == "tupleHits") return copyOut(c, s, ws.tupleHits + size_t(k) * kTupleHitCap, tot, dst, cap, count, elem);
+    return copyOut(c, s, ws.tupleDet + size_t(k) * kTupleHitCap, tot, dst, cap, count, elem);
+  }
+  if (n == "quality") return copyOut(c, s, ws.quality + tb, nTup, dst, cap, count, elem);
+  if (n == "state") return copyOut(c, s, ws.state + tb * 5, size_t(nTup) * 5, dst, cap, count, elem);
+  if (n == "cov") return copyOut(c, s, ws.cov + tb * 15, size_t(nTup) * 15, dst, cap, count, elem);
+  if (n == "pt") return copyOut(c, s, ws.pt + tb, nTup, dst, cap, count, elem);
+  if (n == "eta") return copyOut(c, s, ws.eta + tb, nTup, dst, cap, count, elem);
+  if (n == "chi2") return copyOut(c, s, ws.chi2 + tb, nTup, dst, cap, count, elem);
+  if (n == "zv") return copyOut(c, s, ws.zv + vb, ec.nVertices, dst, cap, count, elem);
+  if (n == "wv") return copyOut(c, s, ws.wv + vb, ec.nVertices, dst, cap, count, elem);
+  if (n == "vchi2") return copyOut(c, s, ws.vchi2 + vb, ec.nVertices, dst, cap, count, elem);
+  if (n == "ptv2") return copyOut(c, s, ws.ptv2 + vb, ec.nVertices, dst, cap, count, elem);
+  if (n == "ndof") return copyOut(c, s, ws.ndof + vb, ec.nVertices, dst, cap, count, elem);
+  if (n == "sortInd") return copyOut(c, s, ws.sortInd + vb, ec.nVertices, dst, cap, count, elem);
+  if (n == "idv") return copyOut(c, s, ws.idv + tb, nTup, dst, cap, count, elem);
+  return fail(c, PG_ERR_NOTFOUND, "unknown product " + n);
+}
+
+int pg_fit_broken_line(pg_ctx* c, int N, uint32_t n, const double* hits, const float* ge, double B, float* state,
+                       float* cov, float* pt, float* eta, float* chi2, void* stream) {
+  if (!c || (N != 3 && N != 4)) return PG_ERR_ARG;
+  cudaError_t e = fitDirect(N, n, hits, ge, B, state, cov, pt, eta, chi2, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cudaFail(c, e, "fit launch");
+  return PG_OK;
+}
+
+}  // extern "C"

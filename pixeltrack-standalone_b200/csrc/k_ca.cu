@@ -1,0 +1,952 @@
+// Cellular automaton on B200: doublets, isOuterHitOfCell lists, CA links,
+// early fishbone, n-tuplet search, cell->track lists, duplicate removers,
+// tuple multiplicity, classification and the hit->tuple cleaner.
+//
+// Reference behaviour followed (src/serial paths):
+//   doubletsFromHisto        plugin-PixelTriplets/gpuPixelDoubletsAlgos.h:25-238 (+ gpuPixelDoublets.h:14-66)
+//   kernel_connect           plugin-PixelTriplets/CAHitNtupletGeneratorKernelsImpl.h:191-262
+//                            with GPUCACell::areAlignedRZ/dcaCut (GPUCACell.h:175-206), CircleEq.h:23-107
+//   fishbone (early)         plugin-PixelTriplets/gpuFishbone.h:21-90
+//   kernel_find_ntuplets     CAHitNtupletGeneratorKernelsImpl.h:264-292, GPUCACell.h:278-331
+//   finalizeBulk             CUDACore/HistoContainer.h:193-204
+//   earlyDuplicateRemover, count/fillMultiplicity, fillHitDetIndices, classifyTracks,
+//   fastDuplicateRemover, count/fillHitInTracks, tripletCleaner   CAHitNtupletGeneratorKernelsImpl.h
+//   configuration            CAHitNtupletGeneratorOnGPU.cc:21-65
+//
+// Serial order is reproduced exactly: doublets are numbered by a count/scan/
+// write pass over (layer pair, inner hit, phi window, bin content), every
+// per-object list is built by counting sort and then ordered per segment, the
+// DFS numbers tuples by prefix sums over starting cells, and the one
+// order-dependent cleaner (fastDuplicateRemover) runs as rounds over the
+// dependency graph of cells that share a track.
+#include "device_utils.cuh"
+#include "pixgpu_internal.cuh"
+
+namespace pixgpu {
+
+namespace {
+
+constexpr int kNPairs = 19;
+__constant__ uint8_t cLayerPairs[2 * kNPairs] = {0, 1, 0, 4, 0, 7, 1, 2, 1, 4, 1, 7, 4, 5, 7, 8, 2, 3, 2, 4,
+                                                 2, 7, 5, 6, 8, 9, 0, 2, 1, 3, 0, 5, 0, 8, 4, 6, 7, 9};
+__constant__ int16_t cPhiCuts[kNPairs] = {522, 730, 730, 522, 626, 626, 522, 522, 626, 626,
+                                          626, 522, 522, 522, 522, 522, 522, 522, 522};
+__constant__ float cMinZ[kNPairs] = {-20., 0., -30., -22., 10., -30., -70., -70., -22., 15.,
+                                     -30,  -70., -70., -20., -22., 0,   -30., -70., -70.};
+__constant__ float cMaxZ[kNPairs] = {20., 30., 0., 22., 30., -10., 70., 70., 22., 30.,
+                                     -15., 70., 70., 20., 22., 30., 0., 70., 70.};
+__constant__ float cMaxR[kNPairs] = {20., 9., 9., 20., 7., 7., 5., 5., 20., 6., 6., 5., 5., 20., 20., 9., 9., 9., 9.};
+
+constexpr float kPtMin = 0.899999976158f;
+constexpr float kThetaCutBarrel = 0.00200000009499f;
+constexpr float kThetaCutForward = 0.00300000002608f;
+constexpr float kHardCurvCut = 0.0328407224959f;
+constexpr float kDcaCutInner = 0.15000000596f;
+constexpr float kDcaCutOuter = 0.25f;
+constexpr uint32_t kMinHits = 3;
+constexpr uint8_t kBad = 0, kDup = 1, kLoose = 2;
+
+__device__ __forceinline__ uint32_t phiBin(int16_t t) { return uint32_t((int(t) >> 9) & 127); }
+
+struct HitsView {
+  const float *xg, *yg, *zg, *rg;
+  const int16_t *iphi, *ysize;
+  const uint16_t* detInd;
+  const uint32_t* phiOff;
+  const uint16_t* phiBins;
+};
+__device__ __forceinline__ HitsView hitsOf(const Workspace& ws, uint32_t e) {
+  size_t hb = size_t(e) * kHitCap;
+  return {ws.xg + hb, ws.yg + hb, ws.zg + hb, ws.rg + hb, ws.iphi + hb, ws.ysize + hb, ws.detInd + hb,
+          ws.phiOff + size_t(e) * kPhiStride, ws.phiBins + hb};
+}
+
+// ------------------------------------------------------------------ doublets
+
+__global__ void kDoubletSetup(Workspace ws, uint32_t nEvents) {
+  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nEvents) return;
+  EventCounters* c = ws.ev + e;
+  uint32_t cum = 0;
+  if (c->nHits == 0) {
+    for (int p = 0; p < kNPairs; ++p) c->pairCum[p] = 0;
+    c->ntot = 0;
+    return;
+  }
+  for (int p = 0; p < kNPairs; ++p) {
+    uint8_t li = cLayerPairs[2 * p];
+    cum += c->layerStart[li + 1] - c->layerStart[li];
+    c->pairCum[p] = cum;
+  }
+  if (cum > kJCap) {
+    c->flags |= kFlagJOverflow;
+    cum = kJCap;
+  }
+  c->ntot = cum;
+}
+
+// Visit the doublet candidates of inner-hit slot j in serial order.  F(oi)
+// is called for each accepted outer hit.
+template <typename F>
+__device__ __forceinline__ void forEachDoublet(const EventCounters* c, const HitsView& hh, uint32_t j,
+                                               uint32_t& pairOut, uint32_t& innerOut, F&& f) {
+  uint32_t pair = 0;
+  while (j >= c->pairCum[pair]) ++pair;
+  uint8_t inner = cLayerPairs[2 * pair], outer = cLayerPairs[2 * pair + 1];
+  uint32_t i = (0 == pair) ? j : j - c->pairCum[pair - 1];
+  i += c->layerStart[inner];
+  pairOut = pair;
+  innerOut = i;
+  uint16_t mi = hh.detInd[i];
+  if (mi > 2000) return;
+  float mez = hh.zg[i];
+  if (mez < cMinZ[pair] || mez > cMaxZ[pair]) return;
+  int16_t mes = hh.ysize[i];  // ideal conditions: every ladder is treated as outer
+  if (inner == 0 && outer > 3)
+    if (mes > 0 && mes < 36) return;
+  if (inner == 1 && outer > 3)
+    if (mes > 0 && mes < 28) return;
+  int16_t mep = hh.iphi[i];
+  float mer = hh.rg[i];
+  int16_t iphicut = cPhiCuts[pair];
+  uint32_t kl = phiBin(int16_t(mep - iphicut)), kh = phiBin(int16_t(mep + iphicut));
+  uint32_t hoff = 128 * outer;
+  uint32_t khh = (kh + 1) & 127;
+  constexpr float z0cut = 12.f;
+  constexpr float minRadius = 0.5f * 87.78f;
+  constexpr float minRadius2T4 = 4.f * minRadius * minRadius;
+  constexpr float dzdrFact = 8 * 0.0285 / 0.015;
+  constexpr float i2p = 3.14159265358979323846 / 32768;
+  const float maxr = cMaxR[pair];
+  for (uint32_t kk = kl; kk != khh; kk = (kk + 1) & 127) {
+    uint32_t b = kk + hoff;
+    for (uint32_t p = hh.phiOff[b], pe = hh.phiOff[b + 1]; p < pe; ++p) {
+      uint16_t oi = hh.phiBins[p];
+      if (hh.detInd[oi] > 2000) continue;
+      float zo = hh.zg[oi], ro = hh.rg[oi];
+      float dr = ro - mer;
+      if (dr > maxr || dr < 0 || fabsf((mez * ro - mer * zo)) > z0cut * dr) continue;
+      int16_t mop = hh.iphi[oi];
+      uint16_t idphi = uint16_t(min(abs(int(int16_t(mop - mep))), abs(int(int16_t(mep - mop)))));
+      if (idphi > iphicut) continue;
+      {
+        int16_t so = hh.ysize[oi];
+        bool cut = (outer < 4) ? (mes > 0 && so > 0 && abs(so - mes) > (inner == 0 ? 28 : 20))
+                               : ((inner < 4) && mes > 0 &&
+                                  abs(mes - int(fabsf((mez - zo) / (mer - ro)) * dzdrFact + 0.5f)) > 20);
+        if (cut) continue;
+      }
+      {
+        float dphi = float(short(idphi)) * i2p;
+        if (dphi * dphi * (minRadius2T4 - mer * ro) > (ro - mer) * (ro - mer)) continue;
+      }
+      f(oi);
+    }
+  }
+}
+
+__global__ void kDoubletCount(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  const EventCounters* c = ws.ev + e;
+  uint32_t ntot = c->ntot;
+  HitsView hh = hitsOf(ws, e);
+  uint32_t* cnt = ws.jCount + size_t(e) * (kJCap + 1);
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < ntot; j += gridDim.x * blockDim.x) {
+    uint32_t n = 0, pair, inner;
+    forEachDoublet(c, hh, j, pair, inner, [&](uint16_t) { ++n; });
+    cnt[j] = n;
+  }
+}
+
+__global__ void kDoubletWrite(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  EventCounters* c = ws.ev + e;
+  uint32_t ntot = c->ntot;
+  HitsView hh = hitsOf(ws, e);
+  const uint32_t* off = ws.jOffset + size_t(e) * (kJCap + 1);
+  size_t cb = size_t(e) * kCellCap;
+  uint32_t* ohc = ws.ohCount + size_t(e) * (kHitCap + 1);
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < ntot; j += gridDim.x * blockDim.x) {
+    uint32_t idx = off[j];
+    if (idx >= kCellCap) continue;
+    uint32_t pair, inner;
+    forEachDoublet(c, hh, j, pair, inner, [&](uint16_t oi) {
+      if (idx < kCellCap) {
+        ws.cellInner[cb + idx] = uint16_t(inner);
+        ws.cellOuter[cb + idx] = oi;
+        ws.cellPair[cb + idx] = uint8_t(pair);
+        ws.cellDoubletId[cb + idx] = int32_t(idx);
+        ws.cellUsed[cb + idx] = 0;
+        ws.cellInnerZ[cb + idx] = hh.zg[inner];
+        ws.cellInnerR[cb + idx] = hh.rg[inner];
+        atomicAdd(&ohc[oi], 1u);
+      }
+      ++idx;
+    });
+  }
+}
+
+__global__ void kCellsTotal(Workspace ws, uint32_t nEvents) {
+  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nEvents) return;
+  EventCounters* c = ws.ev + e;
+  uint32_t raw = ws.jOffset[size_t(e) * (kJCap + 1) + c->ntot];
+  c->nCellsRaw = raw;
+  c->nCells = min(raw, kCellCap);
+  if (raw >= kCellCap) c->flags |= kFlagCellOverflow;
+}
+
+// generic CSR helpers ------------------------------------------------------
+
+// zero n entries of each event's array
+__global__ void kZero(uint32_t* p, size_t stride, uint32_t n, const uint32_t* lenPtr, uint32_t lenStride) {
+  uint32_t e = blockIdx.y;
+  uint32_t len = lenPtr ? min(n, lenPtr[size_t(e) * lenStride] + 1) : n;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x)
+    p[size_t(e) * stride + i] = 0;
+}
+
+// isOuterHitOfCell fill (unordered), then per-hit ascending order
+__global__ void kOuterHitFill(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  uint32_t n = ws.ev[e].nCells;
+  size_t cb = size_t(e) * kCellCap;
+  const uint32_t* off = ws.ohOff + size_t(e) * (kHitCap + 1);
+  uint32_t* cur = ws.ohCount + size_t(e) * (kHitCap + 1);
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    uint16_t oi = ws.cellOuter[cb + c];
+    uint32_t p = atomicAdd(&cur[oi], 1u);
+    ws.ohCells[cb + off[oi] + p] = c;
+  }
+}
+
+template <typename T>
+__global__ void kSortSegments(T* data, size_t dataStride, const uint32_t* off, size_t offStride,
+                              const uint32_t* lenPtr, uint32_t lenStride, uint32_t fixedLen, bool desc,
+                              uint32_t dataCap) {
+  uint32_t e = blockIdx.y;
+  uint32_t nseg = lenPtr ? lenPtr[size_t(e) * lenStride] : fixedLen;
+  const uint32_t* o = off + size_t(e) * offStride;
+  T* d = data + size_t(e) * dataStride;
+  uint32_t warpsPerBlock = blockDim.x >> 5;
+  for (uint32_t s = blockIdx.x * warpsPerBlock + (threadIdx.x >> 5); s < nseg; s += gridDim.x * warpsPerBlock) {
+    uint32_t b = min(o[s], dataCap), en = min(o[s + 1], dataCap);
+    warpSortSegment(d + b, en - b, desc);
+  }
+}
+
+// ------------------------------------------------------------------ connect
+
+// GPUCACell::areAlignedRZ: fabs(float) binds to the double overload in the
+// serial build, so the left-hand product is formed in double precision
+__device__ __forceinline__ bool alignedRZ(float r1, float z1, float ri, float zi, float ro, float zo, float thetaCut) {
+  float radius_diff = fabsf(r1 - ro);
+  float distance_13_squared = radius_diff * radius_diff + (z1 - zo) * (z1 - zo);
+  float pMin = kPtMin * sqrtf(distance_13_squared);
+  double lhs = fabs(double(z1 * (ri - ro) + zi * (ro - r1) + zo * (r1 - ri)));
+  return lhs * double(pMin) <= double(thetaCut * distance_13_squared * radius_diff);
+}
+
+__device__ __forceinline__ bool dcaCut(float x1, float y1, float x2, float y2, float x3, float y3, float region) {
+  bool noflip = fabsf(x3 - x1) < fabsf(y3 - y1);
+  float x1p = noflip ? x1 - x2 : y1 - y2;
+  float y1p = noflip ? y1 - y2 : x1 - x2;
+  float d12 = x1p * x1p + y1p * y1p;
+  float x3p = noflip ? x3 - x2 : y3 - y2;
+  float y3p = noflip ? y3 - y2 : x3 - x2;
+  float d32 = x3p * x3p + y3p * y3p;
+  float num = x1p * y3p - y1p * x3p;
+  float det = d12 * y3p - d32 * y1p;
+  float st2 = (d12 * x3p - d32 * x1p);
+  float seq = det * det + st2 * st2;
+  float al2 = 1.f / sqrtf(seq);
+  float be2 = -st2 * al2;
+  float ct = 2.f * num * al2;
+  al2 *= det;
+  float cc = noflip ? ct : -ct;
+  float alpha = noflip ? al2 : -be2;
+  float beta = noflip ? be2 : -al2;
+  if (cc > kHardCurvCut) return false;
+  float xx = cc * x2 + alpha;
+  float yy = cc * y2 + beta;
+  float dca0 = sqrtf(xx * xx + yy * yy) - 1.f;
+  return fabsf(dca0) < region * fabsf(cc);
+}
+
+// one thread per (cell); appends CA links (oc <- idx) unordered
+__global__ void kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
+  uint32_t e = blockIdx.y;
+  EventCounters* c = ws.ev + e;
+  uint32_t n = c->nCells;
+  HitsView hh = hitsOf(ws, e);
+  size_t cb = size_t(e) * kCellCap;
+  const uint32_t* ohOff = ws.ohOff + size_t(e) * (kHitCap + 1);
+  const uint32_t* ohCells = ws.ohCells + cb;
+  uint32_t* nbrCnt = ws.nbrCount + size_t(e) * (kCellCap + 1);
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+    uint16_t innerHit = ws.cellInner[cb + idx];
+    uint16_t outerHit = ws.cellOuter[cb + idx];
+    uint32_t b = ohOff[innerHit], cnt = min(ohOff[innerHit + 1] - b, uint32_t(PF_MAX_CELLS_PER_HIT));
+    if (cnt == 0) continue;
+    float ri = ws.cellInnerR[cb + idx], zi = ws.cellInnerZ[cb + idx];
+    float ro = hh.rg[outerHit], zo = hh.zg[outerHit];
+    bool isBarrel = hh.detInd[innerHit] < 1184;
+    float x2 = hh.xg[innerHit], y2 = hh.yg[innerHit], x3 = hh.xg[outerHit], y3 = hh.yg[outerHit];
+    bool any = false;
+    for (uint32_t jj = 0; jj < cnt; ++jj) {
+      uint32_t oc = ohCells[b + jj];
+      float r1 = ws.cellInnerR[cb + oc], z1 = ws.cellInnerZ[cb + oc];
+      if (!alignedRZ(r1, z1, ri, zi, ro, zo, isBarrel ? kThetaCutBarrel : kThetaCutForward)) continue;
+      uint16_t ih = ws.cellInner[cb + oc];
+      float region = hh.detInd[ih] < 96 ? kDcaCutInner : kDcaCutOuter;
+      if (!dcaCut(hh.xg[ih], hh.yg[ih], x2, y2, x3, y3, region)) continue;
+      any = true;
+      ws.cellUsed[cb + oc] = 1;
+      atomicAdd(&nbrCnt[oc], 1u);
+      uint32_t k = atomicAdd(&c->nEdges, 1u);
+      if (k < kEdgeCap) {
+        edgeOc[size_t(e) * kEdgeCap + k] = oc;
+        edgeIdx[size_t(e) * kEdgeCap + k] = idx;
+      } else {
+        atomicOr(&c->flags, kFlagEdgeOverflow);
+      }
+    }
+    if (any) ws.cellUsed[cb + idx] = 1;
+  }
+}
+
+__global__ void kEdgeScatter(Workspace ws, const uint32_t* edgeOc, const uint32_t* edgeIdx) {
+  uint32_t e = blockIdx.y;
+  EventCounters* c = ws.ev + e;
+  uint32_t n = min(c->nEdges, kEdgeCap);
+  const uint32_t* off = ws.nbrOff + size_t(e) * (kCellCap + 1);
+  uint32_t* cur = ws.nbrCount + size_t(e) * (kCellCap + 1);
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    uint32_t oc = edgeOc[size_t(e) * kEdgeCap + k];
+    uint32_t p = atomicAdd(&cur[oc], 1u);
+    if (off[oc] + p < kEdgeCap) ws.nbr[size_t(e) * kEdgeCap + off[oc] + p] = edgeIdx[size_t(e) * kEdgeCap + k];
+  }
+}
+
+// cells with at least one CA link must fit the 65535-list pool of the reference
+__global__ void kNbrPool(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  EventCounters* c = ws.ev + e;
+  uint32_t n = c->nCells;
+  const uint32_t* off = ws.nbrOff + size_t(e) * (kCellCap + 1);
+  uint32_t local = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    local += (off[i + 1] > off[i]) ? 1u : 0u;
+  local = __reduce_add_sync(0xffffffffu, local);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(&c->nNbrLists, local);
+}
+
+// ------------------------------------------------------------------ fishbone
+
+// one warp per hit with >= 2 cells ending on it
+__global__ void kFishbone(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  const EventCounters* c = ws.ev + e;
+  uint32_t nHits = c->nHits;
+  if (nHits < 2) return;
+  HitsView hh = hitsOf(ws, e);
+  size_t cb = size_t(e) * kCellCap;
+  const uint32_t* ohOff = ws.ohOff + size_t(e) * (kHitCap + 1);
+  const uint32_t* ohCells = ws.ohCells + cb;
+  uint32_t wpb = blockDim.x >> 5;
+  for (uint32_t h = blockIdx.x * wpb + (threadIdx.x >> 5); h < nHits; h += gridDim.x * wpb) {
+    uint32_t b = ohOff[h], s = min(ohOff[h + 1] - b, uint32_t(PF_MAX_CELLS_PER_HIT));
+    if (s < 2) continue;
+    uint16_t oh = ws.cellOuter[cb + ohCells[b]];
+    float xo = hh.xg[oh], yo = hh.yg[oh], zo = hh.zg[oh];
+    for (uint32_t ic = laneId(); ic < s; ic += 32) {
+      uint32_t ci = ohCells[b + ic];
+      if (0 == ws.cellUsed[cb + ci]) continue;
+      uint16_t ih = ws.cellInner[cb + ci];
+      uint16_t di = hh.detInd[ih];
+      float xi = hh.xg[ih] - xo, yi = hh.yg[ih] - yo, zi = ws.cellInnerZ[cb + ci] - zo;
+      float ni = xi * xi + yi * yi + zi * zi;
+      for (uint32_t jc = ic + 1; jc < s; ++jc) {
+        uint32_t cj = ohCells[b + jc];
+        if (0 == ws.cellUsed[cb + cj]) continue;
+        uint16_t jh = ws.cellInner[cb + cj];
+        uint16_t dj = hh.detInd[jh];
+        float xj = hh.xg[jh] - xo, yj = hh.yg[jh] - yo, zj = ws.cellInnerZ[cb + cj] - zo;
+        float nj = xj * xj + yj * yj + zj * zj;
+        float cos12 = xi * xj + yi * yj + zi * zj;
+        if (di != dj && cos12 * cos12 >= 0.99999f * ni * nj) {
+          if (ni > nj) {
+            ws.cellDoubletId[cb + ci] = -1;
+            break;
+          } else {
+            ws.cellDoubletId[cb + cj] = -1;
+          }
+        }
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ n-tuplets
+
+// DFS of GPUCACell::find_ntuplets from one starting cell, in serial order.
+// Emit(depth, cells[], outerHitOfLast) is called for every saved tuple.
+template <typename Emit>
+__device__ __forceinline__ bool dfsNtuplets(uint32_t start, const int32_t* doubletId, const uint32_t* nbrOff,
+                                            const uint32_t* nbr, Emit&& emit) {
+  uint32_t stack[5], pos[5];
+  int depth = 0;
+  stack[0] = start;
+  pos[0] = 0;
+  bool anyAlive0 = false;
+  bool last[5];
+  last[0] = true;
+  (void)anyAlive0;
+  while (depth >= 0) {
+    uint32_t cell = stack[depth];
+    uint32_t b = nbrOff[cell];
+    uint32_t cnt = min(nbrOff[cell + 1] - b, uint32_t(PF_MAX_CELL_NEIGHBORS));
+    bool descended = false;
+    while (pos[depth] < cnt) {
+      uint32_t other = nbr[b + pos[depth]];
+      pos[depth]++;
+      if (doubletId[other] < 0) continue;
+      last[depth] = false;
+      if (depth + 1 >= 4) return false;  // a path longer than five hits
+      ++depth;
+      stack[depth] = other;
+      pos[depth] = 0;
+      last[depth] = true;
+      descended = true;
+      break;
+    }
+    if (descended) continue;
+    if (last[depth] && uint32_t(depth + 1) >= kMinHits - 1) emit(depth + 1, stack);
+    --depth;
+  }
+  return true;
+}
+
+__device__ __forceinline__ bool isStartCell(const Workspace& ws, size_t cb, uint32_t idx) {
+  if (ws.cellDoubletId[cb + idx] < 0) return false;
+  int pid = ws.cellPair[cb + idx];
+  return kMinHits > 3 ? pid < 3 : (pid < 8 || pid > 12);
+}
+
+__global__ void kNtupletCount(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  EventCounters* c = ws.ev + e;
+  uint32_t n = c->nCells;
+  size_t cb = size_t(e) * kCellCap;
+  const uint32_t* nbrOff = ws.nbrOff + size_t(e) * (kCellCap + 1);
+  const uint32_t* nbr = ws.nbr + size_t(e) * kEdgeCap;
+  uint32_t* tc = ws.startTupleCount + size_t(e) * (kCellCap + 1);
+  uint32_t* hc = ws.startHitCount + size_t(e) * (kCellCap + 1);
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+    uint32_t nt = 0, nh = 0;
+    if (isStartCell(ws, cb, idx)) {
+      bool ok = dfsNtuplets(idx, ws.cellDoubletId + cb, nbrOff, nbr, [&](int ncells, const uint32_t*) {
+        ++nt;
+        nh += uint32_t(ncells) + 1;
+      });
+      if (!ok) atomicOr(&c->flags, kFlagDeepTuple);
+    }
+    tc[idx] = nt;
+    hc[idx] = nh;
+  }
+}
+
+__global__ void kNtupletWrite(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  EventCounters* c = ws.ev + e;
+  uint32_t n = c->nCells;
+  size_t cb = size_t(e) * kCellCap;
+  const uint32_t* nbrOff = ws.nbrOff + size_t(e) * (kCellCap + 1);
+  const uint32_t* nbr = ws.nbr + size_t(e) * kEdgeCap;
+  const uint32_t* to = ws.startTupleOff + size_t(e) * (kCellCap + 1);
+  const uint32_t* ho = ws.startHitOff + size_t(e) * (kCellCap + 1);
+  uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  uint16_t* th = ws.tupleHits + size_t(e) * kTupleHitCap;
+  uint32_t* tcell = ws.tupleCells + size_t(e) * kTupleCellCap;
+  uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+    if (!isStartCell(ws, cb, idx)) continue;
+    uint32_t m = to[idx], off = ho[idx];
+    if (m >= kTupleBins) continue;
+    dfsNtuplets(idx, ws.cellDoubletId + cb, nbrOff, nbr, [&](int ncells, const uint32_t* cells) {
+      if (m < kTupleBins) {
+        toff[m] = off;
+        for (int k = 0; k < ncells; ++k) {
+          th[off + k] = ws.cellInner[cb + cells[k]];
+          tcell[4 * m + k] = cells[k];
+        }
+        th[off + ncells] = ws.cellOuter[cb + cells[ncells - 1]];
+        for (int k = ncells; k < 4; ++k) tcell[4 * m + k] = 0xffffffffu;
+        q[m] = kBad;
+      }
+      ++m;
+      off += uint32_t(ncells) + 1;
+    });
+  }
+}
+
+// bulkFinalizeFill and the stored-tuple count
+__global__ void kTupleFinalize(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  EventCounters* c = ws.ev + e;
+  uint32_t m = c->apcM, nh = c->apcN;
+  uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  if (m >= kTupleBins) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      toff[kTupleBins] = toff[kTupleBins - 1];
+      c->flags |= kFlagTupleOverflow;
+    }
+  } else {
+    for (uint32_t i = m + blockIdx.x * blockDim.x + threadIdx.x; i <= kTupleBins; i += gridDim.x * blockDim.x)
+      toff[i] = nh;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) c->nTuples = min(m, kTupleBins);
+}
+
+__device__ __forceinline__ uint32_t tupleSize(const uint32_t* toff, uint32_t t) { return toff[t + 1] - toff[t]; }
+
+// cell -> track lists: count, (scan), fill, order
+__global__ void kTrackCount(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  EventCounters* c = ws.ev + e;
+  uint32_t nt = c->nTuples;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  const uint32_t* tcell = ws.tupleCells + size_t(e) * kTupleCellCap;
+  uint32_t* cnt = ws.trkCount + size_t(e) * (kCellCap + 1);
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    if (tupleSize(toff, t) == 0) continue;
+    uint32_t ncell = tupleSize(toff, t) - 1;
+    for (uint32_t k = 0; k < ncell; ++k) atomicAdd(&cnt[tcell[4 * t + k]], 1u);
+  }
+}
+
+__global__ void kTrackFill(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  EventCounters* c = ws.ev + e;
+  uint32_t nt = c->nTuples;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  const uint32_t* tcell = ws.tupleCells + size_t(e) * kTupleCellCap;
+  const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
+  uint32_t* cur = ws.trkCount + size_t(e) * (kCellCap + 1);
+  uint16_t* trk = ws.trk + size_t(e) * kTupleCellCap;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    if (tupleSize(toff, t) == 0) continue;
+    uint32_t ncell = tupleSize(toff, t) - 1;
+    for (uint32_t k = 0; k < ncell; ++k) {
+      uint32_t cc = tcell[4 * t + k];
+      uint32_t p = atomicAdd(&cur[cc], 1u);
+      trk[off[cc] + p] = uint16_t(t);
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t trkListSize(const uint32_t* off, uint32_t cell) {
+  return min(off[cell + 1] - off[cell], uint32_t(PF_MAX_CELL_TRACKS));
+}
+
+// pool usage of the cell->track lists; candidate flags for the duplicate removers
+__global__ void kTrackPool(Workspace ws, uint32_t* candFlag) {
+  uint32_t e = blockIdx.y;
+  EventCounters* c = ws.ev + e;
+  uint32_t n = c->nCells;
+  const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
+  uint32_t* flag = candFlag + size_t(e) * (kCellCap + 1);
+  uint32_t local = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t s = off[i + 1] - off[i];
+    local += s > 0 ? 1u : 0u;
+    flag[i] = min(s, uint32_t(PF_MAX_CELL_TRACKS)) >= 2 ? 1u : 0u;
+  }
+  local = __reduce_add_sync(0xffffffffu, local);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(&c->nTrkLists, local);
+}
+
+__global__ void kCandidateScatter(Workspace ws, const uint32_t* candFlag, const uint32_t* candOff) {
+  uint32_t e = blockIdx.y;
+  uint32_t n = ws.ev[e].nCells;
+  const uint32_t* f = candFlag + size_t(e) * (kCellCap + 1);
+  const uint32_t* o = candOff + size_t(e) * (kCellCap + 1);
+  uint32_t* cand = ws.candidates + size_t(e) * kCellCap;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (f[i]) cand[o[i]] = i;
+}
+
+// kernel_earlyDuplicateRemover: per cell with >= 2 tracks
+__global__ void kEarlyDup(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  EventCounters* c = ws.ev + e;
+  uint32_t nc = c->nCandidates;
+  const uint32_t* cand = ws.candidates + size_t(e) * kCellCap;
+  const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
+  const uint16_t* trk = ws.trk + size_t(e) * kTupleCellCap;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x) {
+    uint32_t cell = cand[k];
+    uint32_t b = off[cell], s = trkListSize(off, cell);
+    uint32_t maxNh = 0;
+    for (uint32_t j = 0; j < s; ++j) maxNh = max(maxNh, tupleSize(toff, trk[b + j]));
+    for (uint32_t j = 0; j < s; ++j)
+      if (tupleSize(toff, trk[b + j]) != maxNh) q[trk[b + j]] = kDup;
+  }
+}
+
+// tuple hits -> detector indices (kernel_fillHitDetIndices)
+__global__ void kTupleDet(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  uint32_t n = toff[kTupleBins];
+  const uint16_t* th = ws.tupleHits + size_t(e) * kTupleHitCap;
+  uint16_t* td = ws.tupleDet + size_t(e) * kTupleHitCap;
+  const uint16_t* det = ws.detInd + size_t(e) * kHitCap;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) td[k] = det[th[k]];
+}
+
+// TupleMultiplicity: counts per hit multiplicity, then fill (order irrelevant to the fits)
+__global__ void kMultiplicityCount(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  uint32_t nt = ws.ev[e].nTuples;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  uint32_t* tm = ws.tmOff + size_t(e) * 16;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    uint32_t nh = tupleSize(toff, t);
+    if (nh < 3 || q[t] == kDup) continue;
+    atomicAdd(&tm[nh], 1u);
+  }
+}
+__global__ void kMultiplicityScan(Workspace ws, uint32_t nEvents) {
+  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nEvents) return;
+  uint32_t* tm = ws.tmOff + size_t(e) * 16;
+  uint32_t acc = 0;
+  for (int b = 0; b < 8; ++b) {
+    uint32_t v = tm[b];
+    tm[8 + b] = acc;  // start of bin b
+    if (v > PF_MAX_TUPLES) ws.ev[e].flags |= kFlagFitBinOverflow;
+    acc += v;
+    tm[b] = 0;        // reused as fill cursor
+  }
+  if (acc > PF_MAX_TUPLES) ws.ev[e].flags |= kFlagTmOverflow;
+}
+__global__ void kMultiplicityFill(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  uint32_t nt = ws.ev[e].nTuples;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  uint32_t* tm = ws.tmOff + size_t(e) * 16;
+  uint16_t* bins = ws.tmBins + size_t(e) * kTupleBins;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    uint32_t nh = tupleSize(toff, t);
+    if (nh < 3 || q[t] == kDup) continue;
+    uint32_t p = atomicAdd(&tm[nh], 1u);
+    uint32_t pos = tm[8 + nh] + p;
+    if (pos < kTupleBins) bins[pos] = uint16_t(t);
+  }
+}
+
+// ------------------------------------------------------------------ after the fit
+
+// kernel_classifyTracks with makeQualityCuts
+__global__ void kClassify(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  uint32_t nt = ws.ev[e].nTuples;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  const float* st = ws.state + size_t(e) * kTupleBins * 5;
+  const float* pt = ws.pt + size_t(e) * kTupleBins;
+  const float* chi2 = ws.chi2 + size_t(e) * kTupleBins;
+  const float c0 = float(0.68177776), c1 = float(0.74609577), c2 = float(-0.08035491), c3 = float(0.00315399);
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    uint32_t nh = tupleSize(toff, t);
+    if (nh == 0) continue;  // beyond the serial loop's guard (only the overflow tail)
+    if (q[t] == kDup) continue;
+    if (nh < 3) continue;
+    bool isNaN = false;
+    for (int i = 0; i < 5; ++i) isNaN |= isnan(st[size_t(t) * 5 + i]);
+    if (isNaN) continue;
+    float p = fminf(pt[t], 10.f);
+    float chi2Cut = 30.f * (c0 + p * (c1 + p * (c2 + p * c3)));
+    if (3.f * chi2[t] >= chi2Cut) continue;
+    float maxTip = nh > 3 ? 0.5f : 0.3f, minPt = nh > 3 ? 0.3f : 0.5f;
+    bool isOk = (fabsf(st[size_t(t) * 5 + 1]) < maxTip) && (pt[t] > minPt) && (fabsf(st[size_t(t) * 5 + 4]) < 12.f);
+    if (isOk) q[t] = kLoose;
+  }
+}
+
+__device__ __forceinline__ bool inTrkList(const uint32_t* off, const uint16_t* trk, uint32_t cell, uint16_t t) {
+  uint32_t b = off[cell], s = off[cell + 1] - b;
+  if (s <= uint32_t(PF_MAX_CELL_TRACKS)) return true;  // t is known to be in the full list
+  return t <= trk[b + PF_MAX_CELL_TRACKS - 1];
+}
+
+// kernel_fastDuplicateRemover in serial semantics.  Candidate cells (>= 2
+// tracks) are processed in rounds: a cell is processed once every earlier
+// candidate sharing one of its tracks has been processed, so every cell sees
+// the track qualities that the serial loop over cells would see.
+__global__ void kFastDupInDegree(Workspace ws, uint32_t* indeg, const uint32_t* candFlag) {
+  uint32_t e = blockIdx.y;
+  uint32_t nc = ws.ev[e].nCandidates;
+  const uint32_t* cand = ws.candidates + size_t(e) * kCellCap;
+  const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
+  const uint16_t* trk = ws.trk + size_t(e) * kTupleCellCap;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  const uint32_t* tcell = ws.tupleCells + size_t(e) * kTupleCellCap;
+  const uint32_t* flag = candFlag + size_t(e) * (kCellCap + 1);
+  uint32_t* deg = indeg + size_t(e) * kCellCap;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x) {
+    uint32_t cell = cand[k];
+    uint32_t b = off[cell], s = trkListSize(off, cell);
+    uint32_t d = 0;
+    for (uint32_t j = 0; j < s; ++j) {
+      uint16_t t = trk[b + j];
+      uint32_t ncell = tupleSize(toff, t) - 1;
+      for (uint32_t q = 0; q < ncell; ++q) {
+        uint32_t o = tcell[4 * t + q];
+        if (o < cell && flag[o] && inTrkList(off, trk, o, t)) ++d;
+      }
+    }
+    deg[k] = d;
+  }
+}
+
+__device__ __forceinline__ uint32_t candIndex(const uint32_t* cand, uint32_t nc, uint32_t cell) {
+  uint32_t lo = 0, hi = nc;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (cand[mid] < cell)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+constexpr int kFastDupThreads = 1024;
+__global__ void __launch_bounds__(kFastDupThreads) kFastDupRounds(Workspace ws, uint32_t* indeg, uint8_t* state,
+                                                                   const uint32_t* candFlag) {
+  uint32_t e = blockIdx.x;
+  uint32_t nc = ws.ev[e].nCandidates;
+  const uint32_t* cand = ws.candidates + size_t(e) * kCellCap;
+  const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
+  const uint16_t* trk = ws.trk + size_t(e) * kTupleCellCap;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  const uint32_t* tcell = ws.tupleCells + size_t(e) * kTupleCellCap;
+  const uint32_t* flag = candFlag + size_t(e) * (kCellCap + 1);
+  uint32_t* deg = indeg + size_t(e) * kCellCap;
+  uint8_t* st = state + size_t(e) * kCellCap;  // 0 pending, 1 ready this round, 2 done
+  uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  const float* tip = ws.state + size_t(e) * kTupleBins * 5 + 1;
+  for (uint32_t k = threadIdx.x; k < nc; k += blockDim.x) st[k] = 0;
+  __syncthreads();
+  for (uint32_t round = 0; round < nc + 1; ++round) {
+    int any = 0;
+    for (uint32_t k = threadIdx.x; k < nc; k += blockDim.x) {
+      if (st[k] == 0 && deg[k] == 0) {
+        st[k] = 1;
+        any = 1;
+      }
+    }
+    if (!__syncthreads_or(any)) break;
+    for (uint32_t k = threadIdx.x; k < nc; k += blockDim.x) {
+      if (st[k] != 1) continue;
+      uint32_t cell = cand[k];
+      uint32_t b = off[cell], s = trkListSize(off, cell);
+      float mc = 10000.f;
+      uint16_t im = 60000;
+      for (uint32_t j = 0; j < s; ++j) {
+        uint16_t t = trk[b + j];
+        float score = fabsf(tip[size_t(t) * 5]);
+        if (q[t] == kLoose && score < mc) {
+          mc = score;
+          im = t;
+        }
+      }
+      for (uint32_t j = 0; j < s; ++j) {
+        uint16_t t = trk[b + j];
+        if (q[t] != kBad && t != im) q[t] = kDup;
+      }
+      // release later candidates sharing a track
+      for (uint32_t j = 0; j < s; ++j) {
+        uint16_t t = trk[b + j];
+        uint32_t ncell = tupleSize(toff, t) - 1;
+        for (uint32_t qq = 0; qq < ncell; ++qq) {
+          uint32_t o = tcell[4 * t + qq];
+          if (o > cell && flag[o] && inTrkList(off, trk, o, t)) atomicSub(&deg[candIndex(cand, nc, o)], 1u);
+        }
+      }
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < nc; k += blockDim.x)
+      if (st[k] == 1) st[k] = 2;
+    __syncthreads();
+  }
+}
+
+// hit -> loose tuples (HitToTuple), order: descending tuple index
+__global__ void kHitToTupleCount(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  uint32_t nt = ws.ev[e].nTuples;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  const uint16_t* th = ws.tupleHits + size_t(e) * kTupleHitCap;
+  const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  uint32_t* cnt = ws.h2tCount + size_t(e) * (kHitCap + 1);
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    if (tupleSize(toff, t) == 0 || q[t] != kLoose) continue;
+    for (uint32_t k = toff[t]; k < toff[t + 1]; ++k) atomicAdd(&cnt[th[k]], 1u);
+  }
+}
+__global__ void kHitToTupleFill(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  EventCounters* c = ws.ev + e;
+  uint32_t nt = c->nTuples;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  const uint16_t* th = ws.tupleHits + size_t(e) * kTupleHitCap;
+  const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  const uint32_t* off = ws.h2tOff + size_t(e) * (kHitCap + 1);
+  uint32_t* cur = ws.h2tCount + size_t(e) * (kHitCap + 1);
+  uint16_t* h2t = ws.h2t + size_t(e) * kH2TCap;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    if (tupleSize(toff, t) == 0 || q[t] != kLoose) continue;
+    for (uint32_t k = toff[t]; k < toff[t + 1]; ++k) {
+      uint16_t h = th[k];
+      uint32_t p = atomicAdd(&cur[h], 1u);
+      uint32_t pos = off[h] + p;
+      if (pos < kH2TCap)
+        h2t[pos] = uint16_t(t);
+      else
+        atomicOr(&c->flags, kFlagH2TOverflow);
+    }
+  }
+}
+
+// kernel_tripletCleaner: one thread per hit with >= 2 loose tuples
+__global__ void kTripletCleaner(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  const uint32_t* off = ws.h2tOff + size_t(e) * (kHitCap + 1);
+  const uint16_t* h2t = ws.h2t + size_t(e) * kH2TCap;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  const float* tip = ws.state + size_t(e) * kTupleBins * 5 + 1;
+  for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < kHitCap; h += gridDim.x * blockDim.x) {
+    uint32_t b = off[h], en = min(off[h + 1], kH2TCap);
+    if (en <= b || en - b < 2) continue;
+    uint32_t maxNh = 0;
+    for (uint32_t p = b; p < en; ++p) maxNh = max(maxNh, tupleSize(toff, h2t[p]));
+    for (uint32_t p = b; p < en; ++p)
+      if (tupleSize(toff, h2t[p]) != maxNh) q[h2t[p]] = kDup;
+    if (maxNh > 3) continue;
+    float mc = 10000.f;
+    uint16_t im = 60000;
+    for (uint32_t p = b; p < en; ++p) {
+      uint16_t t = h2t[p];
+      float s = fabsf(tip[size_t(t) * 5]);
+      if (q[t] != kBad && s < mc) {
+        mc = s;
+        im = t;
+      }
+    }
+    for (uint32_t p = b; p < en; ++p) {
+      uint16_t t = h2t[p];
+      if (q[t] != kBad && t != im) q[t] = kDup;
+    }
+  }
+}
+
+__global__ void kCopyCount(uint32_t* dst, uint32_t dstStride, const uint32_t* src, uint32_t srcStride,
+                           uint32_t nEvents) {
+  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < nEvents) dst[size_t(e) * dstStride] = src[size_t(e) * srcStride];
+}
+
+}  // namespace
+
+#define EVF(field) (&ws.ev[0].field), (sizeof(EventCounters) / 4)
+
+cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
+  (void)es;
+  const uint32_t gx = nEvents >= 32 ? 16 : (nEvents >= 8 ? 64 : 296);  // blocks per event for flat loops
+  dim3 g(gx, nEvents);
+  // ---- doublets: count per inner-hit slot, scan, write in serial order
+  kDoubletSetup<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents);
+  kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.ohCount, kHitCap + 1, kHitCap + 1, nullptr, 0);
+  kDoubletCount<<<g, 128, 0, stream>>>(ws);
+  segScan(ws.jCount, ws.jOffset, kJCap + 1, EVF(ntot), kJCap, nullptr, 0, ws.scanTmp, nEvents, stream);
+  kDoubletWrite<<<g, 128, 0, stream>>>(ws);
+  kCellsTotal<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents);
+  // ---- isOuterHitOfCell: scan of the per-hit counts, unordered fill, order per hit
+  segScan(ws.ohCount, ws.ohOff, kHitCap + 1, EVF(nHits), kHitCap, nullptr, 0, ws.scanTmp, nEvents, stream);
+  kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.ohCount, kHitCap + 1, kHitCap + 1, nullptr, 0);
+  kOuterHitFill<<<g, 256, 0, stream>>>(ws);
+  kSortSegments<uint32_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.ohCells, kCellCap, ws.ohOff, kHitCap + 1,
+                                                                     EVF(nHits), 0, false, kCellCap);
+  // ---- CA links: edges appended unordered, then CSR by inner cell, ordered ascending
+  kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbrCount, kCellCap + 1, kCellCap + 1, EVF(nCells));
+  kConnect<<<g, 128, 0, stream>>>(ws, ws.scratchA, ws.scratchB);
+  segScan(ws.nbrCount, ws.nbrOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanTmp, nEvents, stream);
+  kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbrCount, kCellCap + 1, kCellCap + 1, EVF(nCells));
+  kEdgeScatter<<<g, 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB);
+  kSortSegments<uint32_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbr, kEdgeCap, ws.nbrOff, kCellCap + 1,
+                                                                     EVF(nCells), 0, false, kEdgeCap);
+  kNbrPool<<<g, 256, 0, stream>>>(ws);
+  // ---- early fishbone
+  kFishbone<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws);
+  // ---- n-tuplets: DFS count, scans, DFS write, finalize
+  kNtupletCount<<<g, 128, 0, stream>>>(ws);
+  segScan(ws.startTupleCount, ws.startTupleOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcM), ws.scanTmp, nEvents,
+          stream);
+  segScan(ws.startHitCount, ws.startHitOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcN), ws.scanTmp, nEvents,
+          stream);
+  kNtupletWrite<<<g, 128, 0, stream>>>(ws);
+  kTupleFinalize<<<dim3(32, nEvents), 1024, 0, stream>>>(ws);
+  // ---- cell -> track lists
+  kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trkCount, kCellCap + 1, kCellCap + 1, EVF(nCells));
+  kTrackCount<<<g, 256, 0, stream>>>(ws);
+  segScan(ws.trkCount, ws.trkOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanTmp, nEvents, stream);
+  kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trkCount, kCellCap + 1, kCellCap + 1, EVF(nCells));
+  kTrackFill<<<g, 256, 0, stream>>>(ws);
+  kSortSegments<uint16_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trk, kTupleCellCap, ws.trkOff, kCellCap + 1,
+                                                                     EVF(nCells), 0, false, kTupleCellCap);
+  uint32_t* candFlag = ws.startTupleCount;  // scratch
+  uint32_t* candOff = ws.startHitCount;
+  kTrackPool<<<g, 256, 0, stream>>>(ws, candFlag);
+  segScan(candFlag, candOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(nCandidates), ws.scanTmp, nEvents, stream);
+  kCandidateScatter<<<g, 256, 0, stream>>>(ws, candFlag, candOff);
+  kEarlyDup<<<g, 256, 0, stream>>>(ws);
+  kTupleDet<<<g, 256, 0, stream>>>(ws);
+  // ---- tuple multiplicity for the fits
+  kZero<<<dim3(1, nEvents), 32, 0, stream>>>(ws.tmOff, 16, 16, nullptr, 0);
+  kMultiplicityCount<<<g, 256, 0, stream>>>(ws);
+  kMultiplicityScan<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents);
+  kMultiplicityFill<<<g, 256, 0, stream>>>(ws);
+  return cudaGetLastError();
+}
+
+cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
+  const uint32_t gx = nEvents >= 32 ? 16 : (nEvents >= 8 ? 64 : 296);
+  dim3 g(gx, nEvents);
+  kClassify<<<g, 256, 0, stream>>>(ws);
+  // fastDuplicateRemover (candFlag survives in startTupleCount from runCA)
+  uint32_t* candFlag = ws.startTupleCount;
+  uint32_t* indeg = ws.scratchA;                                 // [maxEvents][kEdgeCap] >= kCellCap
+  uint8_t* state = reinterpret_cast<uint8_t*>(ws.scratchB);
+  kFastDupInDegree<<<g, 256, 0, stream>>>(ws, indeg, candFlag);
+  kFastDupRounds<<<nEvents, kFastDupThreads, 0, stream>>>(ws, indeg, state, candFlag);
+  // hit -> tuple map and triplet cleaner
+  kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, nullptr, 0);
+  kHitToTupleCount<<<g, 256, 0, stream>>>(ws);
+  segScan(ws.h2tCount, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, nullptr, 0, ws.scanTmp, nEvents, stream);
+  kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, nullptr, 0);
+  kHitToTupleFill<<<g, 256, 0, stream>>>(ws);
+  kSortSegments<uint16_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.h2t, kH2TCap, ws.h2tOff, kHitCap + 1,
+                                                                     nullptr, 0, kHitCap, true, kH2TCap);
+  kTripletCleaner<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws);
+  return cudaGetLastError();
+}
+
+}  // namespace pixgpu

@@ -1,0 +1,838 @@
+// Local reconstruction on B200: FED words -> digis (decode + gain calibration
+// fused), module runs, clustering with the charge cut fused, hit-module
+// starts, CPE rechits and the phi-binned hit histogram.
+//
+// Reference behaviour followed (src/serial paths):
+//   RawToDigi_kernel         plugin-SiPixelClusterizer/SiPixelRawToClusterGPUKernel.cc:342-462
+//   calibDigis               plugin-SiPixelClusterizer/gpuCalibPixel.h:22-66
+//   countModules             plugin-SiPixelClusterizer/gpuClustering.h:19-37
+//   findClus                 plugin-SiPixelClusterizer/gpuClustering.h:40-273
+//   clusterChargeCut         plugin-SiPixelClusterizer/gpuClusterChargeCut.h:14-114
+//   fillHitsModuleStart      plugin-SiPixelClusterizer/SiPixelRawToClusterGPUKernel.cc:464-506
+//   getHits + CPE            plugin-SiPixelRecHits/gpuPixelRecHits.h:16-207, CondFormats/pixelCPEforGPU.h:118-340
+//   setHitsLayerStart / phi histogram  plugin-SiPixelRecHits/PixelRecHits.cc:15-53, CUDACore/HistoContainer.h:18-73
+//
+// Ordering: every ordered product is produced in the serial backend's order
+// (module runs by word index, clusters by their lowest pixel index, phi-bin
+// contents by descending hit index) with scans and per-segment sorts instead
+// of atomics whose order depends on scheduling.
+#include <cstdio>
+
+#include "device_utils.cuh"
+#include "pixgpu_internal.cuh"
+
+namespace pixgpu {
+
+namespace {
+
+constexpr uint16_t kInvId = PF_INV_ID;
+
+// ------------------------------------------------------------------ helpers
+
+__device__ __forceinline__ uint32_t eventOfWord(const uint32_t* off, uint32_t nEvents, uint32_t g) {
+  return upperBoundIdx(off, nEvents, g);
+}
+
+__device__ __forceinline__ uint32_t cablingIndex(uint32_t fed, uint32_t link, uint32_t roc) {
+  return fed * PF_MAX_LINK * PF_MAX_ROC + (link - 1) * PF_MAX_ROC + roc;
+}
+
+__device__ uint8_t checkROC(uint32_t w, uint8_t fedId, uint32_t link, const PfCablingMap* cab) {
+  uint8_t errorType = (w >> 21) & 0x1f;
+  if (errorType < 25) return 0;
+  bool found = false;
+  switch (errorType) {
+    case 25: {
+      found = true;
+      uint32_t index = cablingIndex(fedId, link, 1);
+      if (index > 1 && index <= cab->size)
+        if (!(link == cab->link[index] && 1 == cab->roc[index])) found = false;
+      break;
+    }
+    case 26:
+    case 27:
+    case 28:
+    case 29:
+    case 31:
+      found = true;
+      break;
+    case 30:
+      if (((w >> 8) & 0xf) == 1) errorType = 40;
+      found = true;
+      break;
+    default:
+      found = false;
+  }
+  return found ? errorType : 0;
+}
+
+__device__ uint32_t getErrRawID(uint8_t fedId, uint32_t w, uint32_t errorType, const PfCablingMap* cab) {
+  uint32_t rID = 0xffffffffu;
+  uint32_t link = 0, roc = 1;
+  switch (errorType) {
+    case 25:
+    case 30:
+    case 31:
+    case 36:
+    case 40:
+      link = (w >> 26) & 0x3f;
+      break;
+    case 29: {
+      int localCH = 0;
+      for (int k = 0; k < 5; ++k) localCH += (k + 1) * int((w >> k) & 1);
+      int block = (w >> 8) & 0x7;
+      int chan = (block % 2 == 0) ? (block / 2) * 9 + localCH : ((block - 1) / 2) * 9 + 4 + localCH;
+      if (chan < 1 || chan > 36) return rID;
+      link = uint32_t(chan);
+      break;
+    }
+    case 37:
+    case 38:
+      roc = (w >> 21) & 0x1f;
+      link = (w >> 26) & 0x3f;
+      break;
+    default:
+      return rID;
+  }
+  uint32_t t = cab->rawId[cablingIndex(fedId, link, roc)];
+  if (t != 9999) rID = t;
+  return rID;
+}
+
+// Geometry/phase1PixelTopology.h:115-158
+__device__ __forceinline__ uint16_t divu52(uint16_t n) {
+  n = n >> 2;
+  uint16_t q = (n >> 1) + (n >> 4);
+  q = q + (q >> 4) + (q >> 5);
+  q = q >> 3;
+  uint16_t r = n - q * 13;
+  return q + ((r + 3) >> 4);
+}
+__device__ __forceinline__ bool isBigPixX(uint16_t px) { return (px == 79) | (px == 80); }
+__device__ __forceinline__ bool isBigPixY(uint16_t py) {
+  uint16_t ly = py - 52 * divu52(py);
+  return (ly == 0) | (ly == 51);
+}
+__device__ __forceinline__ uint16_t localX(uint16_t px) {
+  int shift = 0;
+  if (px > 79) shift += 1;
+  if (px > 80) shift += 1;
+  return px + shift;
+}
+__device__ __forceinline__ uint16_t localY(uint16_t py) {
+  uint16_t roc = divu52(py);
+  int shift = 2 * roc;
+  int yInRoc = py - 52 * roc;
+  if (yInRoc > 0) shift += 1;
+  return py + shift;
+}
+
+__device__ float cpeCorrection(int sizeM1, int Q_f, int Q_l, uint16_t upper_edge_first_pix,
+                               uint16_t lower_edge_last_pix, float lorentz_shift, float theThickness,
+                               float cot_angle, float pitch, bool first_is_big, bool last_is_big) {
+  if (0 == sizeM1) return 0;
+  float W_eff = 0;
+  bool simple = true;
+  if (1 == sizeM1) {
+    float W_inner = pitch * float(lower_edge_last_pix - upper_edge_first_pix);
+    float W_pred = theThickness * cot_angle - lorentz_shift;
+    W_eff = fabsf(W_pred) - W_inner;
+    simple = (W_eff < 0.0f) | (W_eff > pitch);
+  }
+  if (simple) {
+    float sum_of_edge = 2.0f;
+    if (first_is_big) sum_of_edge += 1.0f;
+    if (last_is_big) sum_of_edge += 1.0f;
+    W_eff = pitch * 0.5f * sum_of_edge;
+  }
+  float Qdiff = Q_l - Q_f;
+  float Qsum = Q_l + Q_f;
+  if (Qsum == 0) Qsum = 1.0f;
+  return 0.5f * (Qdiff / Qsum) * W_eff;
+}
+
+// DataFormats/approx_atan2.h:245-263, degree 7 (the reference's coefficients)
+__device__ __forceinline__ int16_t unsafeAtan2s7(float y, float x) {
+  float r = (fabsf(x) - fabsf(y)) / (fabsf(x) + fabsf(y));
+  if (x < 0) r = -r;
+  float z = r * r;
+  float p = r * ((-10422.177734375f) + z * (3349.97412109375f + z * ((-1525.589599609375f) + z * 406.64190673828125f)));
+  short angle = (x >= 0) ? short(8192) : short(24576);
+  angle += short(p);
+  return (y < 0) ? short(-angle) : angle;
+}
+
+// ------------------------------------------------------------------ kernels
+
+// per-event initialisation of counters and module tables
+__global__ void kInitEvents(Workspace ws, uint32_t nEvents) {
+  uint32_t e = blockIdx.x;
+  if (e >= nEvents) return;
+  EventCounters* c = ws.ev + e;
+  if (threadIdx.x == 0) {
+    c->wordStart = ws.wordOffsets[e];
+    c->nWords = ws.wordOffsets[e + 1] - ws.wordOffsets[e];
+    c->nModules = 0;
+    c->nHits = 0;
+    c->ntot = 0;
+    c->nCellsRaw = c->nCells = c->nEdges = 0;
+    c->nNbrLists = c->nTrkLists = 1;
+    c->apcM = c->apcN = c->nTuples = c->nTupleCells = 0;
+    c->nCandidates = c->nLoose = 0;
+    c->nVertices = c->nErrors = c->nVtxTracks = 0;
+    c->flags = c->nWords > kMaxFedWords ? kFlagTooManyWords : 0u;
+  }
+  uint32_t* cim = ws.clusInModule + size_t(e) * kModStride;
+  for (uint32_t i = threadIdx.x; i < kModStride; i += blockDim.x) {
+    cim[i] = 0;
+    ws.moduleId[size_t(e) * kModStride + i] = 0;
+    ws.moduleStart[size_t(e) * kModStride + i] = 0;
+  }
+}
+
+// RawToDigi_kernel + calibDigis for every word of the batch
+__global__ void kRawToDigi(DeviceES es, Workspace ws, uint32_t nEvents) {
+  const uint32_t total = ws.wordOffsets[nEvents];
+  const PfCablingMap* cab = es.cab;
+  const PfGainHeader* gh = es.gainHdr;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    uint32_t e = eventOfWord(ws.wordOffsets, nEvents, g);
+    uint32_t start = ws.wordOffsets[e];
+    uint32_t i = g - start;
+    uint8_t fedId = ws.fedIds[g >> 1];
+    uint16_t xx = 0, yy = 0, adc = 0, mid = 9999;
+    uint32_t pdigi = 0, rawIdOut = 0;
+    uint32_t ww = ws.words[g];
+    bool err = false;
+    PfPixelError perr;
+    if (ww != 0) {
+      uint32_t link = (ww >> 26) & 0x3f;
+      uint32_t roc = (ww >> 21) & 0x1f;
+      uint32_t index = cablingIndex(fedId, link, roc);
+      if (link == 0 || index >= uint32_t(PF_MAX_SIZE)) {
+        // outside the cabling tables (the reference reads out of bounds here)
+        atomicOr(&ws.ev[e].flags, kFlagBadInput);
+        ww = 0;
+      }
+    }
+    if (ww != 0) {
+      uint32_t link = (ww >> 26) & 0x3f;
+      uint32_t roc = (ww >> 21) & 0x1f;
+      uint32_t index = cablingIndex(fedId, link, roc);
+      uint8_t errorType = checkROC(ww, fedId, link, cab);
+      bool skipROC = (roc < 8) ? false : (errorType != 0);
+      if (skipROC) {
+        err = true;
+        perr = {getErrRawID(fedId, ww, errorType, cab), ww, errorType, fedId};
+      } else {
+        uint32_t rawId = cab->rawId[index];
+        uint32_t rocInDet = cab->rocInDet[index];
+        uint32_t moduleId = cab->moduleId[index];
+        bool barrel = 1 == ((rawId >> 25) & 0x7);
+        if (!cab->badRocs[index] && !es.modToUnp[index]) {
+          uint32_t layer = 0;
+          int side;
+          if (barrel) {
+            layer = (rawId >> 20) & 0xf;
+            int module = (rawId >> 2) & 0x3ff;
+            side = (module < 5) ? -1 : 1;
+          } else {
+            int panel = (rawId >> 10) & 0x3;
+            side = (panel == 1) ? -1 : 1;
+          }
+          uint32_t row, col;
+          bool bad;
+          if (layer == 1) {
+            col = (ww >> 15) & 0x3f;
+            row = (ww >> 8) & 0x7f;
+            bad = !((row < 80) & (col < 52));
+          } else {
+            uint32_t dcol = (ww >> 16) & 0x1f;
+            uint32_t pxid = (ww >> 8) & 0xff;
+            row = 80 - pxid / 2;
+            col = dcol * 2 + pxid % 2;
+            bad = !((dcol < 26) & (2 <= pxid) & (pxid < 162));
+          }
+          if (bad) {
+            err = true;
+            perr = {rawId, ww, 37, fedId};
+          } else {
+            // frameConversion (:72-138)
+            bool minusSide = barrel ? (side == -1 && layer != 1) : true;
+            int slopeRow, slopeCol, rowOffset, colOffset;
+            if (minusSide == (rocInDet < 8)) {
+              slopeRow = 1;
+              slopeCol = -1;
+              rowOffset = 0;
+              colOffset = (minusSide ? 8 : 16) * 52 - int(rocInDet) * 52 - 1;
+            } else {
+              slopeRow = -1;
+              slopeCol = 1;
+              rowOffset = 159;
+              colOffset = (minusSide ? int(rocInDet) - 8 : int(rocInDet)) * 52;
+            }
+            uint32_t gRow = rowOffset + slopeRow * int(row);
+            uint32_t gCol = colOffset + slopeCol * int(col);
+            xx = uint16_t(gRow);
+            yy = uint16_t(gCol);
+            adc = uint16_t(ww & 0xff);
+            pdigi = gRow | (gCol << 11) | (min(uint32_t(adc), 1023u) << 22);
+            mid = uint16_t(moduleId);
+            rawIdOut = rawId;
+          }
+        }
+      }
+    }
+    ws.pdigi[g] = pdigi;
+    ws.rawIdArr[g] = rawIdOut;
+    if (mid != kInvId && (mid >= kMaxModules || xx > 159 || yy > 415)) {
+      atomicOr(&ws.ev[e].flags, kFlagBadInput);
+      mid = kInvId;
+    }
+    // calibDigis (isRun2)
+    if (mid != kInvId) {
+      float conversionFactor = mid < 96 ? 50.f : 47.f;
+      float offset = mid < 96 ? -670.f : -60.f;
+      const PfRangeAndCols rc = gh->rangeAndCols[mid];
+      unsigned int lengthOfColumnData = (rc.second - rc.first) / rc.nCols;
+      unsigned int blocks = xx / gh->numberOfRowsAveragedOver;
+      uint32_t o = rc.first + yy * lengthOfColumnData + 2 * blocks;
+      if (o + 1 >= es.gainPayloadSize) o = 0;  // malformed gain ranges (validated at upload)
+      uint8_t gb = es.gainPayload[o], pb = es.gainPayload[o + 1];
+      float pedestal = float(unsigned(pb)) * gh->pedPrecision + gh->minPed;
+      float gain = float(unsigned(gb)) * gh->gainPrecision + gh->minGain;
+      if ((pb == gh->deadFlag) | (pb == gh->noisyFlag)) {
+        mid = kInvId;
+        adc = 0;
+      } else {
+        float vcal = float(int(adc)) * gain - pedestal * gain;
+        adc = uint16_t(max(100, int(vcal * conversionFactor + offset)));
+      }
+    }
+    ws.xx[g] = xx;
+    ws.yy[g] = yy;
+    ws.adc[g] = adc;
+    ws.moduleInd[g] = mid;
+    ws.clus[g] = int32_t(i);
+    if (err) {
+      uint32_t k = atomicAdd(&ws.ev[e].nErrors, 1u);
+      if (k < kErrCap) {
+        ws.errors[size_t(e) * kErrCap + k] = perr;
+        ws.errWordIdx[size_t(e) * kErrCap + k] = i;
+      } else {
+        atomicOr(&ws.ev[e].flags, kFlagErrOverflow);
+      }
+    }
+  }
+}
+
+// module-run boundaries (countModules), appended unordered then sorted per event
+__global__ void kModuleBoundaries(Workspace ws, uint32_t nEvents) {
+  const uint32_t total = ws.wordOffsets[nEvents];
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    uint16_t id = ws.moduleInd[g];
+    if (id == kInvId) continue;
+    uint32_t e = eventOfWord(ws.wordOffsets, nEvents, g);
+    uint32_t start = ws.wordOffsets[e];
+    int j = int(g) - 1;
+    while (j >= int(start) && ws.moduleInd[j] == kInvId) --j;
+    if (j < int(start) || ws.moduleInd[j] != id) {
+      uint32_t loc = atomicAdd(&ws.ev[e].nModules, 1u);
+      if (loc < kMaxModules) ws.moduleStart[size_t(e) * kModStride + 1 + loc] = g - start;
+    }
+  }
+}
+
+// sort the module-run starts of each event (<= 2000) ascending, bitonic in shared memory
+__global__ void kSortModules(Workspace ws, uint32_t nEvents) {
+  __shared__ uint32_t s[2048];
+  uint32_t e = blockIdx.x;
+  EventCounters* c = ws.ev + e;
+  uint32_t n = c->nModules;
+  if (n > kMaxModules) {
+    n = kMaxModules;
+  }
+  uint32_t* ms = ws.moduleStart + size_t(e) * kModStride;
+  for (uint32_t i = threadIdx.x; i < 2048; i += blockDim.x) s[i] = i < n ? ms[1 + i] : 0xffffffffu;
+  __syncthreads();
+  for (uint32_t k = 2; k <= 2048; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = threadIdx.x; i < 2048; i += blockDim.x) {
+        uint32_t ixj = i ^ j;
+        if (ixj > i) {
+          bool up = (i & k) == 0;
+          uint32_t a = s[i], b = s[ixj];
+          if ((a > b) == up) {
+            s[i] = b;
+            s[ixj] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) ms[1 + i] = s[i];
+  if (threadIdx.x == 0) {
+    ms[0] = n;
+    if (c->nModules > kMaxModules) {
+      c->nModules = kMaxModules;
+      c->flags |= kFlagModuleTooBig;
+    }
+  }
+}
+
+// findClus + clusterChargeCut: one block per (module run, event)
+constexpr int kClusThreads = 256;
+__global__ void __launch_bounds__(kClusThreads) kFindClusters(Workspace ws) {
+  __shared__ uint16_t sx[PF_MAX_PIX_IN_MODULE], sy[PF_MAX_PIX_IN_MODULE];
+  __shared__ int32_t lab[PF_MAX_PIX_IN_MODULE];
+  __shared__ uint16_t colList[PF_MAX_PIX_IN_MODULE];
+  __shared__ uint32_t colStart[420];
+  __shared__ int32_t charge[PF_MAX_CLUS_PER_MODULE];
+  __shared__ uint32_t scanSh[33];
+  __shared__ uint32_t sFound, sNewTotal;
+
+  const uint32_t e = blockIdx.y, module = blockIdx.x;
+  const EventCounters* c = ws.ev + e;
+  const uint32_t nModules = c->nModules;
+  if (module >= nModules) return;
+  const uint32_t start = c->wordStart, nW = c->nWords;
+  const uint32_t* ms = ws.moduleStart + size_t(e) * kModStride;
+  const uint32_t firstPixel = ms[1 + module];
+  uint32_t msize = (module + 1 < nModules) ? ms[2 + module] : nW;
+  const uint16_t thisModuleId = ws.moduleInd[start + firstPixel];
+  if (thisModuleId >= kMaxModules) return;
+  if (msize - firstPixel > PF_MAX_PIX_IN_MODULE) {
+    if (threadIdx.x == 0) atomicOr(&ws.ev[e].flags, kFlagModuleTooBig);
+    msize = firstPixel + PF_MAX_PIX_IN_MODULE;
+  }
+  const uint32_t np = msize - firstPixel;
+  uint16_t* gmid = ws.moduleInd + start + firstPixel;
+  int32_t* gclus = ws.clus + start + firstPixel;
+
+  for (uint32_t k = threadIdx.x; k < 420; k += blockDim.x) colStart[k] = 0;
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
+    bool valid = gmid[k] != kInvId;
+    uint16_t y = ws.yy[start + firstPixel + k];
+    sx[k] = ws.xx[start + firstPixel + k];
+    sy[k] = valid ? y : uint16_t(0xffff);
+    lab[k] = int32_t(k);
+    if (valid) atomicAdd(&colStart[y + 1], 1u);
+  }
+  __syncthreads();
+  // column offsets (exclusive), 419 entries
+  {
+    uint32_t carry = 0;
+    for (uint32_t b0 = 0; b0 < 420; b0 += blockDim.x) {
+      uint32_t b = b0 + threadIdx.x;
+      uint32_t v = b < 420 ? colStart[b] : 0u;
+      uint32_t tot;
+      uint32_t inc = blockExclusiveScan(v, scanSh, &tot) + v;
+      if (b < 420) colStart[b] = carry + inc;
+      carry += tot;
+      __syncthreads();
+    }
+  }
+  // fill column lists (order inside a column is irrelevant for components)
+  for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
+    uint16_t y = sy[k];
+    if (y == 0xffff) continue;
+    uint32_t pos = atomicAdd(&colStart[y], 1u);
+    colList[pos] = uint16_t(k);
+  }
+  __syncthreads();
+  // after the fill colStart[y] points at the end of column y; column y spans
+  // [colStart[y-1], colStart[y]) with colStart[-1] = 0
+  auto colBegin = [&](uint32_t y) { return y == 0 ? 0u : colStart[y - 1]; };
+  auto find = [&](int32_t a) {
+    while (true) {
+      int32_t p = lab[a];
+      if (p == a) return a;
+      int32_t gp = lab[p];
+      if (gp != p) lab[a] = gp;  // path halving (benign race: only ever lowers towards a root)
+      a = p;
+    }
+  };
+  // union of 8-neighbours (|dx| <= 1, dy in {0, 1}); roots hook under the smaller index
+  for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
+    uint16_t y = sy[k];
+    if (y == 0xffff) continue;
+    int xk = sx[k];
+    for (uint32_t yy = y; yy <= uint32_t(y) + 1 && yy < 418; ++yy) {
+      uint32_t b = colBegin(yy), en = colStart[yy];
+      for (uint32_t p = b; p < en; ++p) {
+        uint32_t m = colList[p];
+        if (yy == y && m <= k) continue;
+        if (abs(int(sx[m]) - xk) > 1) continue;
+        int32_t a = int32_t(k), bb = int32_t(m);
+        while (true) {
+          a = find(a);
+          bb = find(bb);
+          if (a == bb) break;
+          if (a > bb) {
+            int32_t t = a;
+            a = bb;
+            bb = t;
+          }
+          int32_t old = atomicCAS(&lab[bb], bb, a);
+          if (old == bb) break;
+          bb = old;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < np; k += blockDim.x)
+    if (sy[k] != 0xffff) lab[k] = find(int32_t(k));
+  __syncthreads();
+  // number the roots in ascending pixel order
+  {
+    uint32_t carry = 0;
+    for (uint32_t k0 = 0; k0 < np; k0 += blockDim.x) {
+      uint32_t k = k0 + threadIdx.x;
+      uint32_t isRoot = (k < np && sy[k] != 0xffff && lab[k] == int32_t(k)) ? 1u : 0u;
+      uint32_t tot;
+      uint32_t pre = blockExclusiveScan(isRoot, scanSh, &tot);
+      if (isRoot) colList[k] = uint16_t(carry + pre);  // colList reused as root rank
+      carry += tot;
+    }
+    if (threadIdx.x == 0) sFound = carry;
+  }
+  __syncthreads();
+  const uint32_t found = sFound;
+  // cluster id of each pixel (serial findClus numbering)
+  for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
+    if (sy[k] == 0xffff) continue;
+    lab[k] = int32_t(colList[lab[k]]);
+  }
+  for (uint32_t k = threadIdx.x; k < PF_MAX_CLUS_PER_MODULE; k += blockDim.x) charge[k] = 0;
+  __syncthreads();
+  // ---- clusterChargeCut
+  uint32_t nclus = found;
+  if (nclus > uint32_t(PF_MAX_CLUS_PER_MODULE)) {
+    for (uint32_t k = threadIdx.x; k < np; k += blockDim.x)
+      if (sy[k] != 0xffff && lab[k] >= PF_MAX_CLUS_PER_MODULE) {
+        sy[k] = 0xfffe;  // becomes invalid with cluster id InvId
+      }
+    if (threadIdx.x == 0) atomicOr(&ws.ev[e].flags, kFlagModuleTooBig);
+    nclus = PF_MAX_CLUS_PER_MODULE;
+  }
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < np; k += blockDim.x)
+    if (sy[k] < 0xfffe) atomicAdd(&charge[lab[k]], int32_t(ws.adc[start + firstPixel + k]));
+  __syncthreads();
+  const int chargeCut = thisModuleId < 96 ? 2000 : 4000;
+  // inclusive scan of ok flags -> new ids (stored back into charge[] as id+1, 0 = bad)
+  {
+    uint32_t carry = 0;
+    for (uint32_t k0 = 0; k0 < nclus; k0 += blockDim.x) {
+      uint32_t k = k0 + threadIdx.x;
+      uint32_t ok = (k < nclus && charge[k] > chargeCut) ? 1u : 0u;
+      uint32_t tot;
+      uint32_t pre = blockExclusiveScan(ok, scanSh, &tot);
+      if (k < nclus) charge[k] = ok ? int32_t(carry + pre + 1) : 0;
+      carry += tot;
+    }
+    if (threadIdx.x == 0) sNewTotal = carry;
+  }
+  __syncthreads();
+  const uint32_t newTotal = sNewTotal;
+  const bool allGood = (nclus == newTotal);
+  for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
+    uint16_t y = sy[k];
+    if (y == 0xffff) {
+      gclus[k] = -9999;
+    } else if (y == 0xfffe) {
+      gmid[k] = kInvId;
+      gclus[k] = kInvId;
+    } else if (allGood) {
+      gclus[k] = lab[k];
+    } else {
+      int32_t nid = charge[lab[k]];
+      if (nid == 0) {
+        gclus[k] = kInvId;
+        gmid[k] = kInvId;
+      } else {
+        gclus[k] = nid - 1;
+      }
+    }
+  }
+  if (threadIdx.x == 0) {
+    ws.clusInModule[size_t(e) * kModStride + thisModuleId] = (found == 0 || allGood) ? found : newTotal;
+    ws.moduleId[size_t(e) * kModStride + module] = thisModuleId;
+  }
+}
+
+// fillHitsModuleStart + setHitsLayerStart + beam-spot corrected average geometry
+__global__ void kHitsModuleStart(DeviceES es, Workspace ws) {
+  __shared__ uint32_t scanSh[33];
+  uint32_t e = blockIdx.x;
+  const uint32_t* cim = ws.clusInModule + size_t(e) * kModStride;
+  uint32_t* cms = ws.clusModuleStart + size_t(e) * kModStride;
+  uint32_t carry = 0;
+  for (uint32_t i0 = 0; i0 < kMaxModules; i0 += blockDim.x) {
+    uint32_t i = i0 + threadIdx.x;
+    uint32_t v = i < kMaxModules ? min(uint32_t(PF_MAX_CLUS_PER_MODULE), cim[i]) : 0u;
+    uint32_t tot;
+    uint32_t inc = blockExclusiveScan(v, scanSh, &tot) + v;
+    if (i < kMaxModules) cms[i + 1] = min(carry + inc, uint32_t(PF_MAX_HITS));
+    carry += tot;
+  }
+  if (threadIdx.x == 0) cms[0] = 0;
+  __syncthreads();
+  EventCounters* c = ws.ev + e;
+  if (threadIdx.x == 0) {
+    c->nHits = cms[kMaxModules];
+    if (carry > PF_MAX_HITS) c->flags |= kFlagHitOverflow;
+  }
+  if (threadIdx.x < 11) c->layerStart[threadIdx.x] = cms[es.lg->layerStart[threadIdx.x]];
+  PfAverageGeometry* agc = ws.agc + e;
+  const PfAverageGeometry* ag = es.ag;
+  const PfBeamSpot* bs = es.bs;
+  for (uint32_t il = threadIdx.x; il < PF_N_LADDERS_BARREL; il += blockDim.x) {
+    agc->ladderZ[il] = ag->ladderZ[il] - bs->z;
+    agc->ladderX[il] = ag->ladderX[il] - bs->x;
+    agc->ladderY[il] = ag->ladderY[il] - bs->y;
+    agc->ladderR[il] = sqrtf(agc->ladderX[il] * agc->ladderX[il] + agc->ladderY[il] * agc->ladderY[il]);
+    agc->ladderMinZ[il] = ag->ladderMinZ[il] - bs->z;
+    agc->ladderMaxZ[il] = ag->ladderMaxZ[il] - bs->z;
+  }
+  if (threadIdx.x == 0) {
+    agc->endCapZ[0] = ag->endCapZ[0] - bs->z;
+    agc->endCapZ[1] = ag->endCapZ[1] - bs->z;
+  }
+}
+
+// getHits: one block per (module run, event); all clusters of a module in one pass
+constexpr int kHitThreads = 128;
+constexpr int kHitBatch = 256;
+__global__ void __launch_bounds__(kHitThreads) kGetHits(DeviceES es, Workspace ws) {
+  __shared__ uint32_t minRow[kHitBatch], maxRow[kHitBatch], minCol[kHitBatch], maxCol[kHitBatch];
+  __shared__ int32_t Qfx[kHitBatch], Qlx[kHitBatch], Qfy[kHitBatch], Qly[kHitBatch], chg[kHitBatch];
+  const uint32_t e = blockIdx.y, module = blockIdx.x;
+  const EventCounters* c = ws.ev + e;
+  const uint32_t nModules = c->nModules;
+  if (module >= nModules) return;
+  const uint32_t me = ws.moduleId[size_t(e) * kModStride + module];
+  const int nclus = int(ws.clusInModule[size_t(e) * kModStride + me]);
+  if (nclus == 0) return;
+  const uint32_t start = c->wordStart, nW = c->nWords;
+  const uint32_t* ms = ws.moduleStart + size_t(e) * kModStride;
+  const uint32_t first = ms[1 + module];
+  const uint32_t last = (module + 1 < nModules) ? ms[2 + module] : nW;
+  if (ws.moduleInd[start + first] != me || me >= es.nDet) return;
+  const PfDetParams& dp = es.det[me];
+  const PfCommonParams& cp = *es.common;
+  const PfBeamSpot& bs = *es.bs;
+  const size_t hb = size_t(e) * kHitCap;
+  const uint32_t cmsMe = ws.clusModuleStart[size_t(e) * kModStride + me];
+  for (int startClus = 0; startClus < nclus; startClus += kHitBatch) {
+    int nIn = min(kHitBatch, nclus - startClus);
+    int lastClus = startClus + nIn;
+    for (int k = threadIdx.x; k < nIn; k += blockDim.x) {
+      minRow[k] = minCol[k] = 0xffffffffu;
+      maxRow[k] = maxCol[k] = 0;
+      chg[k] = Qfx[k] = Qlx[k] = Qfy[k] = Qly[k] = 0;
+    }
+    __syncthreads();
+    for (uint32_t i = first + threadIdx.x; i < last; i += blockDim.x) {
+      uint16_t id = ws.moduleInd[start + i];
+      if (id == kInvId || id != me) continue;
+      int cl = ws.clus[start + i];
+      if (cl < startClus || cl >= lastClus) continue;
+      cl -= startClus;
+      uint32_t x = ws.xx[start + i], y = ws.yy[start + i];
+      atomicMin(&minRow[cl], x);
+      atomicMax(&maxRow[cl], x);
+      atomicMin(&minCol[cl], y);
+      atomicMax(&maxCol[cl], y);
+    }
+    __syncthreads();
+    for (uint32_t i = first + threadIdx.x; i < last; i += blockDim.x) {
+      uint16_t id = ws.moduleInd[start + i];
+      if (id == kInvId || id != me) continue;
+      int cl = ws.clus[start + i];
+      if (cl < startClus || cl >= lastClus) continue;
+      cl -= startClus;
+      uint32_t x = ws.xx[start + i], y = ws.yy[start + i];
+      int32_t ch = ws.adc[start + i];
+      atomicAdd(&chg[cl], ch);
+      if (minRow[cl] == x) atomicAdd(&Qfx[cl], ch);
+      if (maxRow[cl] == x) atomicAdd(&Qlx[cl], ch);
+      if (minCol[cl] == y) atomicAdd(&Qfy[cl], ch);
+      if (maxCol[cl] == y) atomicAdd(&Qly[cl], ch);
+    }
+    __syncthreads();
+    for (int ic = threadIdx.x; ic < nIn; ic += blockDim.x) {
+      uint32_t h = cmsMe + startClus + ic;
+      if (h >= uint32_t(PF_MAX_HITS)) continue;
+      uint16_t llx = uint16_t(minRow[ic] + 1), lly = uint16_t(minCol[ic] + 1);
+      uint16_t urx = uint16_t(maxRow[ic]), ury = uint16_t(maxCol[ic]);
+      uint16_t llxl = localX(llx), llyl = localY(lly), urxl = localX(urx), uryl = localY(ury);
+      int mx = llxl + urxl, my = llyl + uryl;
+      int xsize = int(urxl) + 2 - int(llxl);
+      int ysize = int(uryl) + 2 - int(llyl);
+      bool bigMinX = isBigPixX(uint16_t(minRow[ic])), bigMaxX = isBigPixX(uint16_t(maxRow[ic]));
+      bool bigMinY = isBigPixY(uint16_t(minCol[ic])), bigMaxY = isBigPixY(uint16_t(maxCol[ic]));
+      if (bigMinX) ++xsize;
+      if (bigMaxX) ++xsize;
+      if (bigMinY) ++ysize;
+      if (bigMaxY) ++ysize;
+      // the reference computes these ratios in double precision
+      int unbalanceX = int(8. * double(fabsf(float(Qfx[ic] - Qlx[ic]))) / double(float(Qfx[ic] + Qlx[ic])));
+      int unbalanceY = int(8. * double(fabsf(float(Qfy[ic] - Qly[ic]))) / double(float(Qfy[ic] + Qly[ic])));
+      xsize = 8 * xsize - unbalanceX;
+      ysize = 8 * ysize - unbalanceY;
+      int16_t sxv = int16_t(min(xsize, 1023)), syv = int16_t(min(ysize, 1023));
+      if (minRow[ic] == 0 || maxRow[ic] == 159) sxv = int16_t(-sxv);
+      if (minCol[ic] == 0 || maxCol[ic] == 415) syv = int16_t(-syv);
+      float xPos = dp.shiftX + cp.pitchX * (0.5f * float(mx) + float(-81));
+      float yPos = dp.shiftY + cp.pitchY * (0.5f * float(my) + float(-216));
+      float gvz = -1.f / dp.z0;
+      float cotalpha = (xPos - dp.x0) * gvz, cotbeta = (yPos - dp.y0) * gvz;
+      float thickness = dp.isBarrel ? cp.thicknessB : cp.thicknessE;
+      float xcorr = cpeCorrection(int(maxRow[ic] - minRow[ic]), Qfx[ic], Qlx[ic], llxl, urxl, dp.chargeWidthX,
+                                  thickness, cotalpha, cp.pitchX, bigMinX, bigMaxX);
+      float ycorr = cpeCorrection(int(maxCol[ic] - minCol[ic]), Qfy[ic], Qly[ic], llyl, uryl, dp.chargeWidthY,
+                                  thickness, cotbeta, cp.pitchY, bigMinY, bigMaxY);
+      float xpos = xPos + xcorr, ypos = yPos + ycorr;
+      float xerr = 0.0050f, yerr = 0.0085f;
+      uint32_t sx = maxRow[ic] - minRow[ic], sy = maxCol[ic] - minCol[ic];
+      bool isEdgeX = minRow[ic] == 0 || maxRow[ic] == 159;
+      bool isEdgeY = minCol[ic] == 0 || maxCol[ic] == 415;
+      uint32_t ix = (0 == sx), iy = (0 == sy);
+      ix += (0 == sx) && bigMinX;
+      iy += (0 == sy) && bigMinY;
+      if (!isEdgeX) xerr = dp.sx[ix];
+      if (!isEdgeY) yerr = dp.sy[iy];
+      const PfFrame& f = dp.frame;
+      float xg = f.R11 * xpos + f.R21 * ypos;
+      float yg = f.R12 * xpos + f.R22 * ypos;
+      float zg = f.R13 * xpos + f.R23 * ypos;
+      xg += f.px;
+      yg += f.py;
+      zg += f.pz;
+      xg -= bs.x;
+      yg -= bs.y;
+      zg -= bs.z;
+      ws.charge[hb + h] = chg[ic];
+      ws.detInd[hb + h] = uint16_t(me);
+      ws.xl[hb + h] = xpos;
+      ws.yl[hb + h] = ypos;
+      ws.xsize[hb + h] = sxv;
+      ws.ysize[hb + h] = syv;
+      ws.xerr[hb + h] = xerr * xerr;
+      ws.yerr[hb + h] = yerr * yerr;
+      ws.xg[hb + h] = xg;
+      ws.yg[hb + h] = yg;
+      ws.zg[hb + h] = zg;
+      ws.rg[hb + h] = sqrtf(xg * xg + yg * yg);
+      ws.iphi[hb + h] = unsafeAtan2s7(yg, xg);
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ uint32_t phiBinOf(int16_t t) { return uint32_t((int(t) >> 9) & 127); }
+__device__ __forceinline__ uint32_t layerOfHit(const uint32_t* ls, uint32_t i) {
+  uint32_t l = 0;
+#pragma unroll
+  for (int k = 1; k < 10; ++k) l += (i >= ls[k]) ? 1u : 0u;
+  return l;
+}
+
+// phi histogram: count per (layer, bin)
+__global__ void kPhiCount(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  const EventCounters* c = ws.ev + e;
+  uint32_t nt = c->layerStart[10];
+  uint32_t* off = ws.phiOff + size_t(e) * kPhiStride;
+  const int16_t* iphi = ws.iphi + size_t(e) * kHitCap;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
+    uint32_t b = phiBinOf(iphi[i]) + 128 * layerOfHit(c->layerStart, i);
+    atomicAdd(&off[b], 1u);
+  }
+}
+
+// fill (unordered within a bin); off holds the exclusive scan, cursor counts
+__global__ void kPhiFill(Workspace ws, uint32_t* cursor) {
+  uint32_t e = blockIdx.y;
+  const EventCounters* c = ws.ev + e;
+  uint32_t nt = c->layerStart[10];
+  const uint32_t* off = ws.phiOff + size_t(e) * kPhiStride;
+  uint32_t* cur = cursor + size_t(e) * kPhiStride;
+  const int16_t* iphi = ws.iphi + size_t(e) * kHitCap;
+  uint16_t* bins = ws.phiBins + size_t(e) * kHitCap;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
+    uint32_t b = phiBinOf(iphi[i]) + 128 * layerOfHit(c->layerStart, i);
+    uint32_t p = atomicAdd(&cur[b], 1u);
+    bins[off[b] + p] = uint16_t(i);
+  }
+}
+
+// order every bin by descending hit index (the serial fill order); one warp per bin
+__global__ void kPhiSort(Workspace ws) {
+  uint32_t e = blockIdx.y;
+  uint32_t b = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (b >= kPhiTot - 1) return;
+  if (ws.ev[e].nHits == 0) return;
+  const uint32_t* off = ws.phiOff + size_t(e) * kPhiStride;
+  uint16_t* bins = ws.phiBins + size_t(e) * kHitCap;
+  warpSortSegment(bins + off[b], off[b + 1] - off[b], true);
+}
+
+__global__ void kZeroU32(uint32_t* p, size_t stride, uint32_t n, uint32_t nEvents) {
+  uint32_t e = blockIdx.y;
+  if (e >= nEvents) return;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[e * stride + i] = 0;
+}
+
+// order each event's error list by word index (the serial push order)
+__global__ void kSortErrors(Workspace ws) {
+  uint32_t e = blockIdx.x;
+  uint32_t n = min(ws.ev[e].nErrors, kErrCap);
+  if (threadIdx.x == 0) {
+    PfPixelError* er = ws.errors + size_t(e) * kErrCap;
+    uint32_t* wi = ws.errWordIdx + size_t(e) * kErrCap;
+    for (uint32_t i = 1; i < n; ++i) {
+      PfPixelError x = er[i];
+      uint32_t k = wi[i];
+      int j = int(i) - 1;
+      while (j >= 0 && wi[j] > k) {
+        er[j + 1] = er[j];
+        wi[j + 1] = wi[j];
+        --j;
+      }
+      er[j + 1] = x;
+      wi[j + 1] = k;
+    }
+    if (ws.ev[e].nErrors > kErrCap) ws.ev[e].nErrors = kErrCap;
+  }
+}
+
+}  // namespace
+
+cudaError_t runLocal(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
+  kInitEvents<<<nEvents, 256, 0, stream>>>(ws, nEvents);
+  const int flatBlocks = 148 * 8;
+  kRawToDigi<<<flatBlocks, 256, 0, stream>>>(es, ws, nEvents);
+  kModuleBoundaries<<<flatBlocks, 256, 0, stream>>>(ws, nEvents);
+  kSortModules<<<nEvents, 1024, 0, stream>>>(ws, nEvents);
+  kSortErrors<<<nEvents, 32, 0, stream>>>(ws);
+  kFindClusters<<<dim3(kMaxModules, nEvents), kClusThreads, 0, stream>>>(ws);
+  kHitsModuleStart<<<nEvents, 1024, 0, stream>>>(es, ws);
+  kGetHits<<<dim3(kMaxModules, nEvents), kHitThreads, 0, stream>>>(es, ws);
+  // phi histogram: count, exclusive scan, unordered fill, per-bin ordering
+  uint32_t* cursor = ws.jCount;  // scratch: the doublet counters are not in use yet
+  kZeroU32<<<dim3(2, nEvents), 1024, 0, stream>>>(ws.phiOff, kPhiStride, kPhiStride, nEvents);
+  kZeroU32<<<dim3(2, nEvents), 1024, 0, stream>>>(cursor, kPhiStride, kPhiStride, nEvents);
+  kPhiCount<<<dim3(16, nEvents), 256, 0, stream>>>(ws);
+  // in place exclusive scan of the 1280 counters; the total lands in the extra bin
+  segScan(ws.phiOff, ws.phiOff, kPhiStride, nullptr, 0, kPhiTot - 1, nullptr, 0, ws.scanTmp, nEvents, stream);
+  kPhiFill<<<dim3(16, nEvents), 256, 0, stream>>>(ws, cursor);
+  kPhiSort<<<dim3((kPhiTot - 1 + 7) / 8, nEvents), 256, 0, stream>>>(ws);
+  return cudaGetLastError();
+}
+
+}  // namespace pixgpu

@@ -1,0 +1,444 @@
+// Pixel vertexing on B200: one block per event runs loadTracks,
+// clusterTracksByDensity, fitVertices(50), splitVertices(9),
+// fitVertices(5000) and sortByPt2 with the PixelVertexProducerCUDA
+// configuration (minT=2, eps=0.07, errmax=0.01, chi2max=9, ptMin=0.5).
+// Reference: plugin-PixelVertexFinding/gpuVertexFinderImpl.h:10-43,
+// gpuClusterTracksByDensity.h:20-207, gpuFitVertices.h:15-98,
+// gpuSplitVertices.h:15-125, gpuSortByPt2.h:15-55,
+// PixelVertexProducerCUDA.cc:16-26.
+//
+// All float sums run sequentially per vertex in ascending track order (the
+// serial order), histogram bins are scanned in the serial storage order
+// (descending track index inside a bin) and new split vertices are numbered
+// by a prefix over the parent vertex index.
+#include "device_utils.cuh"
+#include "pixgpu_internal.cuh"
+
+namespace pixgpu {
+
+namespace {
+
+constexpr uint32_t kMaxVtxTracks = 32 * 1024;
+constexpr int kVtxThreads = 1024;
+
+struct VtxScratch {
+  float *zt, *ezt2, *ptt2, *zz;
+  uint16_t* itrk;
+  uint8_t *izt, *newV;
+  int32_t *iv, *nn, *root;
+  uint32_t* list;    // tracks grouped by vertex
+  uint16_t* hbins;   // z-histogram content
+};
+
+__device__ __forceinline__ VtxScratch scratchOf(const Workspace& ws, uint32_t e) {
+  // carve per-event scratch out of scratchA/scratchB (kEdgeCap words each)
+  uint32_t* a = ws.scratchA + size_t(e) * kEdgeCap;
+  uint32_t* b = ws.scratchB + size_t(e) * kEdgeCap;
+  VtxScratch s;
+  s.zt = reinterpret_cast<float*>(a);
+  s.ezt2 = reinterpret_cast<float*>(a + kMaxVtxTracks);
+  s.ptt2 = reinterpret_cast<float*>(a + 2 * kMaxVtxTracks);
+  s.zz = reinterpret_cast<float*>(a + 3 * kMaxVtxTracks);
+  s.iv = reinterpret_cast<int32_t*>(a + 4 * kMaxVtxTracks);
+  s.nn = reinterpret_cast<int32_t*>(a + 5 * kMaxVtxTracks);
+  s.root = reinterpret_cast<int32_t*>(a + 6 * kMaxVtxTracks);
+  s.list = a + 7 * kMaxVtxTracks;
+  s.itrk = reinterpret_cast<uint16_t*>(b);
+  s.hbins = reinterpret_cast<uint16_t*>(b) + kMaxVtxTracks;
+  s.izt = reinterpret_cast<uint8_t*>(b + kMaxVtxTracks);
+  s.newV = reinterpret_cast<uint8_t*>(b + kMaxVtxTracks) + kMaxVtxTracks;
+  return s;
+}
+
+// group tracks by vertex id (ascending track order inside each vertex)
+__device__ void groupByVertex(const VtxScratch& s, uint32_t nt, uint32_t nv, uint32_t* vOff, uint32_t* vCur,
+                              uint32_t* scanSh) {
+  for (uint32_t v = threadIdx.x; v <= nv; v += blockDim.x) {
+    vOff[v] = 0;
+    vCur[v] = 0;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+    int32_t v = s.iv[i];
+    if (v >= 0 && uint32_t(v) < nv) atomicAdd(&vOff[v], 1u);
+  }
+  __syncthreads();
+  uint32_t carry = 0;
+  for (uint32_t v0 = 0; v0 <= nv; v0 += blockDim.x) {
+    uint32_t v = v0 + threadIdx.x;
+    uint32_t c = v <= nv ? vOff[v] : 0u;
+    uint32_t tot;
+    uint32_t pre = blockExclusiveScan(c, scanSh, &tot);
+    if (v <= nv) vOff[v] = carry + pre;
+    carry += tot;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+    int32_t v = s.iv[i];
+    if (v >= 0 && uint32_t(v) < nv) s.list[vOff[v] + atomicAdd(&vCur[v], 1u)] = i;
+  }
+  __syncthreads();
+  for (uint32_t v = threadIdx.x; v < nv; v += blockDim.x) {
+    uint32_t b = vOff[v], n = vOff[v + 1] - b;
+    for (uint32_t k = 1; k < n; ++k) {
+      uint32_t x = s.list[b + k];
+      int j = int(k) - 1;
+      while (j >= 0 && s.list[b + j] > x) {
+        s.list[b + j + 1] = s.list[b + j];
+        --j;
+      }
+      s.list[b + j + 1] = x;
+    }
+  }
+  __syncthreads();
+}
+
+// fitVertices: weighted z, chi2 outlier rejection (iv = 9999), ndof and weight
+__device__ void fitVertices(const VtxScratch& s, uint32_t nt, uint32_t nv, float chi2Max, float* zv, float* wv,
+                            float* chi2, int32_t* ndof, uint32_t* vOff, uint32_t* vCur, uint32_t* scanSh) {
+  groupByVertex(s, nt, nv, vOff, vCur, scanSh);
+  for (uint32_t v = threadIdx.x; v < nv; v += blockDim.x) {
+    uint32_t b = vOff[v], n = vOff[v + 1] - b;
+    float z = 0, w = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+      uint32_t i = s.list[b + k];
+      float wi = 1.f / s.ezt2[i];
+      z += s.zt[i] * wi;
+      w += wi;
+    }
+    z /= w;
+    int32_t nd = -1;
+    float c2s = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+      uint32_t i = s.list[b + k];
+      float c2 = z - s.zt[i];
+      c2 *= c2 / s.ezt2[i];
+      if (c2 > chi2Max) {
+        s.iv[i] = 9999;
+        continue;
+      }
+      c2s += c2;
+      nd++;
+    }
+    if (nd > 0) w *= float(nd) / c2s;
+    zv[v] = z;
+    wv[v] = w;
+    chi2[v] = c2s;
+    ndof[v] = nd;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
+  __shared__ uint32_t scanSh[33];
+  __shared__ uint32_t hoff[257], hcur[257];
+  __shared__ uint32_t vOff[kMaxVtx + 1], vCur[kMaxVtx + 1];
+  __shared__ uint32_t sNt, sFound, sGuard, sNv;
+  const uint32_t e = blockIdx.x;
+  EventCounters* c = ws.ev + e;
+  VtxScratch s = scratchOf(ws, e);
+  const uint32_t nTuples = c->nTuples;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  const float* pt = ws.pt + size_t(e) * kTupleBins;
+  const float* st = ws.state + size_t(e) * kTupleBins * 5;
+  const float* cov = ws.cov + size_t(e) * kTupleBins * 15;
+  int16_t* idv = ws.idv + size_t(e) * kTupleBins;
+  float* zv = ws.zv + size_t(e) * kMaxVtx;
+  float* wv = ws.wv + size_t(e) * kMaxVtx;
+  float* vchi2 = ws.vchi2 + size_t(e) * kMaxVtx;
+  float* ptv2 = ws.ptv2 + size_t(e) * kMaxVtx;
+  int32_t* ndof = ws.ndof + size_t(e) * kMaxVtx;
+  uint16_t* sortInd = ws.sortInd + size_t(e) * kMaxVtx;
+
+  // ---- loadTracks: the serial loop stops at the first empty tuple
+  if (threadIdx.x == 0) {
+    uint32_t g = nTuples;
+    if (nTuples == kTupleBins && toff[kTupleBins] == toff[kTupleBins - 1]) g = kTupleBins - 1;
+    sGuard = g;
+  }
+  __syncthreads();
+  const uint32_t guard = sGuard;
+  {
+    uint32_t carry = 0;
+    for (uint32_t t0 = 0; t0 < guard; t0 += blockDim.x) {
+      uint32_t t = t0 + threadIdx.x;
+      uint32_t sel = 0;
+      if (t < guard) {
+        idv[t] = -1;
+        uint32_t nh = toff[t + 1] - toff[t];
+        sel = (nh >= 4 && q[t] == 2 && !(pt[t] < 0.5f)) ? 1u : 0u;
+      }
+      uint32_t tot;
+      uint32_t pre = blockExclusiveScan(sel, scanSh, &tot);
+      if (sel) {
+        uint32_t it = carry + pre;
+        if (it < kMaxVtxTracks) {
+          s.itrk[it] = uint16_t(t);
+          s.zt[it] = st[size_t(t) * 5 + 4];
+          s.ezt2[it] = cov[size_t(t) * 15 + 14];
+          s.ptt2[it] = pt[t] * pt[t];
+        }
+      }
+      carry += tot;
+    }
+    if (threadIdx.x == 0) sNt = min(carry, kMaxVtxTracks);
+  }
+  __syncthreads();
+  const uint32_t nt = sNt;
+  const float eps = 0.07f, errmax = 0.01f, chi2max = 9.f;
+  const float er2mx = errmax * errmax;
+
+  // ---- clusterTracksByDensity: z histogram (256 bins of 1 mm)
+  for (uint32_t b = threadIdx.x; b < 257; b += blockDim.x) {
+    hoff[b] = 0;
+    hcur[b] = 0;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+    int iz = int(double(s.zt[i]) * 10.);
+    iz = min(max(iz, -128), 127);
+    s.izt[i] = uint8_t(iz + 128);
+    atomicAdd(&hoff[s.izt[i]], 1u);
+    s.iv[i] = int32_t(i);
+    s.nn[i] = 0;
+  }
+  __syncthreads();
+  {
+    uint32_t carry = 0;
+    for (uint32_t b0 = 0; b0 < 257; b0 += blockDim.x) {
+      uint32_t b = b0 + threadIdx.x;
+      uint32_t v = b < 257 ? hoff[b] : 0u;
+      uint32_t tot;
+      uint32_t pre = blockExclusiveScan(v, scanSh, &tot);
+      if (b < 257) hoff[b] = carry + pre;
+      carry += tot;
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+    uint32_t b = s.izt[i];
+    s.hbins[hoff[b] + atomicAdd(&hcur[b], 1u)] = uint16_t(i);
+  }
+  __syncthreads();
+  // the serial fill stores each bin in descending track order
+  for (uint32_t b = threadIdx.x; b < 256; b += blockDim.x) {
+    uint32_t o = hoff[b], n = hoff[b + 1] - o;
+    for (uint32_t k = 1; k < n; ++k) {
+      uint16_t x = s.hbins[o + k];
+      int j = int(k) - 1;
+      while (j >= 0 && s.hbins[o + j] < x) {
+        s.hbins[o + j + 1] = s.hbins[o + j];
+        --j;
+      }
+      s.hbins[o + j + 1] = x;
+    }
+  }
+  __syncthreads();
+  // neighbour counts
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+    if (s.ezt2[i] > er2mx) continue;
+    int bs = s.izt[i];
+    int be = min(255, bs + 1);
+    bs = max(0, bs - 1);
+    int32_t cnt = 0;
+    for (uint32_t p = hoff[bs]; p < hoff[be + 1]; ++p) {
+      uint32_t j = s.hbins[p];
+      if (i == j) continue;
+      float dist = fabsf(s.zt[i] - s.zt[j]);
+      if (dist > eps) continue;
+      if (dist * dist > chi2max * (s.ezt2[i] + s.ezt2[j])) continue;
+      ++cnt;
+    }
+    s.nn[i] = cnt;
+  }
+  __syncthreads();
+  // closest denser neighbour (ties resolved by the serial iteration order)
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+    float mdist = eps;
+    int bs = s.izt[i];
+    int be = min(255, bs + 1);
+    bs = max(0, bs - 1);
+    int32_t best = int32_t(i);
+    for (uint32_t p = hoff[bs]; p < hoff[be + 1]; ++p) {
+      uint32_t j = s.hbins[p];
+      if (s.nn[j] < s.nn[i]) continue;
+      if (s.nn[j] == s.nn[i] && s.zt[j] >= s.zt[i]) continue;
+      float dist = fabsf(s.zt[i] - s.zt[j]);
+      if (dist > mdist) continue;
+      if (dist * dist > chi2max * (s.ezt2[i] + s.ezt2[j])) continue;
+      mdist = dist;
+      best = int32_t(j);
+    }
+    s.iv[i] = best;
+  }
+  __syncthreads();
+  // percolate to the seed
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+    int32_t m = s.iv[i];
+    while (m != s.iv[m]) m = s.iv[m];
+    s.root[i] = m;
+  }
+  __syncthreads();
+  // number the seeds with nn >= minT in ascending track order
+  {
+    uint32_t carry = 0;
+    for (uint32_t i0 = 0; i0 < nt; i0 += blockDim.x) {
+      uint32_t i = i0 + threadIdx.x;
+      uint32_t seed = (i < nt && s.root[i] == int32_t(i) && s.nn[i] >= 2) ? 1u : 0u;
+      uint32_t tot;
+      uint32_t pre = blockExclusiveScan(seed, scanSh, &tot);
+      if (seed) s.iv[i] = int32_t(carry + pre);  // rank of the seed
+      carry += tot;
+    }
+    if (threadIdx.x == 0) sFound = carry;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+    int32_t r = s.root[i];
+    // seeds hold their rank in iv[r]; noise seeds end as 9997 (= -(-9998) - 1)
+    s.zz[i] = 0;
+    s.newV[i] = 0;
+    int32_t v = (s.nn[r] >= 2) ? s.iv[r] : 9997;
+    s.root[i] = v;  // staged: iv of a seed is still read by other threads in this loop
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) s.iv[i] = s.root[i];
+  __syncthreads();
+  uint32_t found = sFound;
+  if (found >= kMaxVtx) {
+    if (threadIdx.x == 0) atomicOr(&c->flags, kFlagVtxOverflow);
+    found = kMaxVtx - 1;
+  }
+
+  // ---- fitVertices(50)
+  fitVertices(s, nt, found, 50.f, zv, wv, vchi2, ndof, vOff, vCur, scanSh);
+
+  // ---- splitVertices(9): tracks of each vertex are the list built by the fit
+  //      minus the ones rejected there (iv = 9999)
+  if (threadIdx.x == 0) sNv = found;
+  __syncthreads();
+  for (uint32_t kv = threadIdx.x; kv < found; kv += blockDim.x) {
+    vCur[kv] = 0;  // split flag
+    if (ndof[kv] < 4) continue;
+    if (vchi2[kv] < 9.f * float(ndof[kv])) continue;
+    if (ndof[kv] >= 512) {
+      atomicOr(&c->flags, kFlagVtxOverflow);
+      continue;
+    }
+    uint32_t b = vOff[kv], n = vOff[kv + 1] - b;
+    for (uint32_t k = 0; k < n; ++k) {
+      uint32_t i = s.list[b + k];
+      if (s.iv[i] != int32_t(kv)) continue;
+      s.zz[i] = s.zt[i] - zv[kv];
+      s.newV[i] = s.zz[i] < 0 ? 0 : 1;
+    }
+    float znew[2], wnew[2];
+    int maxiter = 20;
+    bool more = true;
+    while (more) {
+      more = false;
+      znew[0] = znew[1] = 0;
+      wnew[0] = wnew[1] = 0;
+      for (uint32_t k = 0; k < n; ++k) {
+        uint32_t i = s.list[b + k];
+        if (s.iv[i] != int32_t(kv)) continue;
+        int w = s.newV[i];
+        float ww = 1.f / s.ezt2[i];
+        znew[w] += s.zz[i] * ww;
+        wnew[w] += ww;
+      }
+      znew[0] /= wnew[0];
+      znew[1] /= wnew[1];
+      for (uint32_t k = 0; k < n; ++k) {
+        uint32_t i = s.list[b + k];
+        if (s.iv[i] != int32_t(kv)) continue;
+        float d0 = fabsf(s.zz[i] - znew[0]);
+        float d1 = fabsf(s.zz[i] - znew[1]);
+        uint8_t newer = d0 < d1 ? 0 : 1;
+        more |= newer != s.newV[i];
+        s.newV[i] = newer;
+      }
+      --maxiter;
+      if (maxiter <= 0) more = false;
+    }
+    if (0 == wnew[0] || 0 == wnew[1]) continue;
+    float dist2 = (znew[0] - znew[1]) * (znew[0] - znew[1]);
+    float chi2Dist = dist2 / (1.f / wnew[0] + 1.f / wnew[1]);
+    if (chi2Dist < 4) continue;
+    vCur[kv] = 1;
+  }
+  __syncthreads();
+  // new vertex numbers in ascending order of the vertex that was split
+  {
+    uint32_t carry = 0;
+    for (uint32_t k0 = 0; k0 < found; k0 += blockDim.x) {
+      uint32_t kv = k0 + threadIdx.x;
+      uint32_t f = kv < found ? vCur[kv] : 0u;
+      uint32_t tot;
+      uint32_t pre = blockExclusiveScan(f, scanSh, &tot);
+      if (kv < found) vCur[kv] = f ? (found + carry + pre + 1) : 0u;  // 0: no split, else igv+1
+      carry += tot;
+    }
+    if (threadIdx.x == 0) sNv = found + carry;
+  }
+  __syncthreads();
+  for (uint32_t kv = threadIdx.x; kv < found; kv += blockDim.x) {
+    if (vCur[kv] == 0) continue;
+    uint32_t igv = vCur[kv] - 1;
+    uint32_t b = vOff[kv], n = vOff[kv + 1] - b;
+    for (uint32_t k = 0; k < n; ++k) {
+      uint32_t i = s.list[b + k];
+      if (s.iv[i] == int32_t(kv) && s.newV[i] == 1) s.iv[i] = int32_t(igv);
+    }
+  }
+  __syncthreads();
+  uint32_t nv = sNv;
+  if (nv >= kMaxVtx) {
+    if (threadIdx.x == 0) atomicOr(&c->flags, kFlagVtxOverflow);
+    nv = kMaxVtx - 1;
+  }
+
+  // ---- fitVertices(5000)
+  fitVertices(s, nt, nv, 5000.f, zv, wv, vchi2, ndof, vOff, vCur, scanSh);
+
+  // ---- sortByPt2
+  if (threadIdx.x == 0) c->nVertices = nv;
+  if (nv < 1) return;
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) idv[s.itrk[i]] = int16_t(s.iv[i]);
+  // the fit above left every vertex's accepted tracks in vOff/list order
+  for (uint32_t v = threadIdx.x; v < nv; v += blockDim.x) {
+    uint32_t b = vOff[v], n = vOff[v + 1] - b;
+    float p2 = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+      uint32_t i = s.list[b + k];
+      if (s.iv[i] > 9990) continue;
+      p2 += s.ptt2[i];
+    }
+    ptv2[v] = p2;
+  }
+  __syncthreads();
+  if (nv == 1) {
+    if (threadIdx.x == 0) sortInd[0] = 0;
+    return;
+  }
+  for (uint32_t v = threadIdx.x; v < nv; v += blockDim.x) {
+    float p = ptv2[v];
+    uint32_t r = 0;
+    for (uint32_t u = 0; u < nv; ++u) {
+      float o = ptv2[u];
+      r += (o < p || (o == p && u < v)) ? 1u : 0u;
+    }
+    sortInd[r] = uint16_t(v);
+  }
+  if (threadIdx.x == 0) c->nVtxTracks = nt;
+}
+
+}  // namespace
+
+cudaError_t runVertices(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
+  kVertices<<<nEvents, kVtxThreads, 0, stream>>>(ws);
+  return cudaGetLastError();
+}
+
+}  // namespace pixgpu

@@ -1,0 +1,191 @@
+// Internal declarations of the B200 pixel chain: device ES tables, the batch
+// workspace (per-event fixed strides, ragged FED words) and small device
+// primitives shared by the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pixfmt.h"
+
+namespace pixgpu {
+
+// ---------------------------------------------------------------- capacities
+constexpr uint32_t kMaxModules = PF_MAX_MODULES;         // 2000
+constexpr uint32_t kModStride = 2048;                    // per-event stride of module arrays
+constexpr uint32_t kHitCap = PF_MAX_HITS;                // 49152 hits per event
+constexpr uint32_t kPhiTot = 10 * PF_PHI_BINS + 1;       // 1281
+constexpr uint32_t kPhiStride = 1288;
+constexpr uint32_t kJCap = 6 * kHitCap;                  // doublet inner-hit slots (sum of inner layer sizes)
+constexpr uint32_t kCellCap = PF_MAX_DOUBLETS_PARAM;     // 458752 doublets per event
+constexpr uint32_t kEdgeCap = 2 * kCellCap;              // CA neighbour links kept per event
+constexpr uint32_t kTupleBins = PF_TRACK_STRIDE;         // 32768 tuples (HitContainer bins)
+constexpr uint32_t kTupleHitCap = 5 * kTupleBins;        // 163840
+constexpr uint32_t kTupleCellCap = 4 * kTupleBins;       // cells per tuple <= 4
+constexpr uint32_t kH2TCap = 4 * PF_MAX_TUPLES;          // HitToTuple capacity (98304)
+constexpr uint32_t kMaxVtx = PF_MAX_VTX;
+constexpr uint32_t kErrCap = 4096;                       // digi errors kept per event
+constexpr uint32_t kMaxFedWords = PF_MAX_FED_WORDS;      // 300000 words per event
+
+// flag bits in EventCounters::flags (capacity conditions where the result no
+// longer follows the reference's truncation order exactly)
+enum : uint32_t {
+  kFlagModuleTooBig = 1u << 0,      // > 4000 pixels in a module (reference behaviour undefined)
+  kFlagEdgeOverflow = 1u << 1,      // more CA links than kEdgeCap
+  kFlagNbrPoolOverflow = 1u << 2,   // more cells with neighbours than the 65535-list pool
+  kFlagTrkPoolOverflow = 1u << 3,   // more cells with tracks than the 65535-list pool
+  kFlagFitBinOverflow = 1u << 4,    // > 24576 tuples of one multiplicity (fit order dependent)
+  kFlagTupleOverflow = 1u << 5,     // > 32768 tuples (reference drops the tail)
+  kFlagCellOverflow = 1u << 6,      // doublet capacity reached (reference truncates; reproduced)
+  kFlagHitOverflow = 1u << 7,       // > 49152 clusters (reference truncates; reproduced)
+  kFlagErrOverflow = 1u << 8,       // more digi errors than kErrCap
+  kFlagTooManyWords = 1u << 9,      // event larger than kMaxFedWords
+  kFlagH2TOverflow = 1u << 10,      // hit-to-tuple capacity exceeded
+  kFlagTmOverflow = 1u << 11,       // tuple multiplicity capacity exceeded
+  kFlagVtxOverflow = 1u << 12,      // split vertex with >= 512 tracks or > 1024 vertices
+  kFlagDeepTuple = 1u << 13,        // a CA path longer than 5 hits (reference aborts)
+  kFlagJOverflow = 1u << 14,        // more doublet inner-hit slots than kJCap
+  kFlagBadInput = 1u << 15          // words/cabling entries outside the tables (ignored)
+};
+
+struct EventCounters {
+  uint32_t wordStart, nWords;   // input slice of the batch word buffer
+  uint32_t nModules;            // module runs found (moduleStart[0])
+  uint32_t nHits;               // clusModuleStart[2000]
+  uint32_t layerStart[11];      // hitsLayerStart
+  uint32_t ntot;                // doublet candidates (inner hits over all layer pairs)
+  uint32_t pairCum[20];         // cumulative inner layer sizes per pair
+  uint32_t nCellsRaw;           // doublets found before the capacity cut
+  uint32_t nCells;              // doublets kept
+  uint32_t nEdges;              // CA links
+  uint32_t nNbrLists, nTrkLists;  // pool usage (including the reserved empty list)
+  uint32_t apcM, apcN;          // tuples attempted and their hits
+  uint32_t nTuples;             // tuples stored (min(apcM, 32768))
+  uint32_t nTupleCells;         // entries of the tuple->cell table
+  uint32_t nCandidates;         // cells with >= 2 tracks
+  uint32_t nLoose;              // loose tuples
+  uint32_t nVertices;
+  uint32_t nErrors;
+  uint32_t nVtxTracks;
+  uint32_t flags;
+  uint32_t pad[2];
+};
+
+// ---------------------------------------------------------------- ES on device
+struct DeviceES {
+  const PfCablingMap* cab;
+  const uint8_t* modToUnp;
+  const PfGainHeader* gainHdr;
+  const uint8_t* gainPayload;
+  const PfCommonParams* common;
+  const PfDetParams* det;
+  const PfAverageGeometry* ag;
+  const PfLayerGeometry* lg;
+  const PfBeamSpot* bs;
+  uint32_t nDet;             // entries of det[]
+  uint32_t gainPayloadSize;  // bytes of gainPayload
+};
+
+// ---------------------------------------------------------------- batch workspace
+struct Workspace {
+  uint32_t maxEvents;
+  uint32_t wordCap;          // words over the whole batch
+  // input
+  uint32_t* words;
+  uint8_t* fedIds;
+  uint32_t* wordOffsets;     // [maxEvents + 1]
+  EventCounters* ev;         // [maxEvents]
+  // digis (flat, batch word index)
+  uint16_t *xx, *yy, *adc, *moduleInd;
+  int32_t* clus;
+  uint32_t *pdigi, *rawIdArr;
+  PfPixelError* errors;      // [maxEvents][kErrCap]
+  uint32_t* errWordIdx;      // [maxEvents][kErrCap]
+  // clusters [maxEvents][kModStride]
+  uint32_t *moduleStart, *clusInModule, *moduleId, *clusModuleStart;
+  // hits [maxEvents][kHitCap]
+  float *xl, *yl, *xerr, *yerr, *xg, *yg, *zg, *rg;
+  int32_t* charge;
+  int16_t *iphi, *xsize, *ysize;
+  uint16_t* detInd;
+  uint32_t* phiOff;          // [maxEvents][kPhiStride]
+  uint16_t* phiBins;         // [maxEvents][kHitCap]
+  PfAverageGeometry* agc;    // [maxEvents]
+  // doublets
+  uint32_t* jCount;          // [maxEvents][kJCap + 1]
+  uint32_t* jOffset;         // [maxEvents][kJCap + 1]
+  uint16_t *cellInner, *cellOuter;   // [maxEvents][kCellCap]
+  uint8_t* cellPair;
+  int32_t* cellDoubletId;
+  uint8_t* cellUsed;
+  float *cellInnerZ, *cellInnerR;
+  // cells by outer hit (isOuterHitOfCell), CSR sorted ascending
+  uint32_t* ohCount;         // [maxEvents][kHitCap + 1]
+  uint32_t* ohOff;           // [maxEvents][kHitCap + 1]
+  uint32_t* ohCells;         // [maxEvents][kCellCap]
+  // CA neighbour links (outerNeighbors), CSR sorted ascending
+  uint32_t* nbrCount;        // [maxEvents][kCellCap + 1]
+  uint32_t* nbrOff;          // [maxEvents][kCellCap + 1]
+  uint32_t* nbr;             // [maxEvents][kEdgeCap]
+  // tuples
+  uint32_t* startTupleCount; // [maxEvents][kCellCap + 1]
+  uint32_t* startTupleOff;   // [maxEvents][kCellCap + 1]
+  uint32_t* startHitCount;   // [maxEvents][kCellCap + 1]
+  uint32_t* startHitOff;     // [maxEvents][kCellCap + 1]
+  uint32_t* tupleOff;        // [maxEvents][kTupleBins + 1]
+  uint16_t* tupleHits;       // [maxEvents][kTupleHitCap]
+  uint16_t* tupleDet;        // [maxEvents][kTupleHitCap]
+  uint32_t* tupleCells;      // [maxEvents][kTupleCellCap]  (4 slots per tuple)
+  uint8_t* quality;          // [maxEvents][kTupleBins]
+  // cell -> tracks, CSR sorted ascending
+  uint32_t* trkCount;        // [maxEvents][kCellCap + 1]
+  uint32_t* trkOff;          // [maxEvents][kCellCap + 1]
+  uint16_t* trk;             // [maxEvents][kTupleCellCap]
+  uint32_t* candidates;      // [maxEvents][kCellCap] cells with >= 2 tracks, ascending
+  // tuple multiplicity
+  uint32_t* tmOff;           // [maxEvents][16]
+  uint16_t* tmBins;          // [maxEvents][kTupleBins]
+  // fit results [maxEvents][kTupleBins * k]
+  float *state, *cov, *pt, *eta, *chi2;
+  // hit -> tuple
+  uint32_t* h2tCount;        // [maxEvents][kHitCap + 1]
+  uint32_t* h2tOff;          // [maxEvents][kHitCap + 1]
+  uint16_t* h2t;             // [maxEvents][kH2TCap]
+  // vertices
+  float *zv, *wv, *vchi2, *ptv2;  // [maxEvents][kMaxVtx]
+  int32_t* ndof;             // [maxEvents][kMaxVtx]
+  uint16_t* sortInd;         // [maxEvents][kMaxVtx]
+  int16_t* idv;              // [maxEvents][kTupleBins]
+  // scratch: CA link lists before ordering, cleaner state
+  uint32_t* scratchA;        // [maxEvents][kEdgeCap]
+  uint32_t* scratchB;        // [maxEvents][kEdgeCap]
+  // scan scratch
+  uint32_t* scanTmp;         // [maxEvents][kScanTmpStride]
+};
+
+constexpr uint32_t kScanChunk = 4096;
+constexpr uint32_t kScanTmpStride = 1024;
+
+// ---------------------------------------------------------------- launch API (host)
+size_t workspaceBytes(uint32_t maxEvents, uint32_t wordCap);
+void workspaceCarve(Workspace& ws, void* base, uint32_t maxEvents, uint32_t wordCap);
+
+// Runs the whole chain on events [0, nEvents) of ws, on `stream`.  The
+// word/fedId/offset inputs must already be in ws.  Returns a CUDA error code.
+cudaError_t runChain(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream);
+// Individual stages (used by runChain and by the stage-level tests)
+cudaError_t runLocal(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream);
+cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream);
+cudaError_t runFits(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream);
+cudaError_t runVertices(Workspace& ws, uint32_t nEvents, cudaStream_t stream);
+cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream);
+
+// batched segmented exclusive scan: out[e*stride + i] = sum_{k<i} in[e*stride + k]
+// for i <= n_e, where n_e = lenPtr[e*lenStride] (device) or maxLen when lenPtr is
+// null; n_e <= maxLen.  The total lands at out[e*stride + n_e] and, if totalPtr,
+// at totalPtr[e*totalStride].  in may equal out.
+void segScan(const uint32_t* in, uint32_t* out, uint32_t stride, const uint32_t* lenPtr, uint32_t lenStride,
+             uint32_t maxLen, uint32_t* totalPtr, uint32_t totalStride, uint32_t* tmp, uint32_t nEvents,
+             cudaStream_t stream);
+
+}  // namespace pixgpu

@@ -1,0 +1,347 @@
+"""Python access to the B200 pixel chain (include/pixgpu.h), the synthetic
+event generator (include/pixsynth.h) and, for tests only, the CPU oracle and
+the checker build of the reference.
+
+The product path is libpixgpu.so; this module only marshals buffers.  If the
+library is missing it is built (nvcc cross-compiles without a GPU); a context
+cannot be created without a CUDA device, and every failure raises.
+"""
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+LIB = os.path.join(PKG, "lib")
+sys.path.insert(0, PKG)
+import build as _build  # noqa: E402
+
+U8P = ctypes.POINTER(ctypes.c_uint8)
+
+# products and their element types (names follow the reference's SoA members)
+_TYPES = {
+    "xx": np.uint16, "yy": np.uint16, "adc": np.uint16, "moduleInd": np.uint16, "clus": np.int32,
+    "pdigi": np.uint32, "rawIdArr": np.uint32, "moduleStart": np.uint32, "clusInModule": np.uint32,
+    "moduleId": np.uint32, "clusModuleStart": np.uint32, "xl": np.float32, "yl": np.float32,
+    "xerr": np.float32, "yerr": np.float32, "xg": np.float32, "yg": np.float32, "zg": np.float32,
+    "rg": np.float32, "charge": np.int32, "iphi": np.int16, "xsize": np.int16, "ysize": np.int16,
+    "detInd": np.uint16, "hitsLayerStart": np.uint32, "phiOff": np.uint32, "phiBins": np.uint16,
+    "agcLadderR": np.float32, "cellInner": np.uint16, "cellOuter": np.uint16, "cellLayerPair": np.int16,
+    "cellDoubletId": np.int32, "cellUsed": np.uint16, "cellNbrOff": np.uint32, "cellNbr": np.uint32,
+    "cellTrkOff": np.uint32, "cellTrk": np.uint16, "outerHitOff": np.uint32, "outerHitCells": np.uint32,
+    "tupleOff": np.uint32, "tupleHits": np.uint16, "tupleDet": np.uint16, "quality": np.uint8,
+    "state": np.float32, "cov": np.float32, "pt": np.float32, "eta": np.float32, "chi2": np.float32,
+    "zv": np.float32, "wv": np.float32, "vchi2": np.float32, "ptv2": np.float32, "ndof": np.int32,
+    "sortInd": np.uint16, "idv": np.int16,
+    "outerHitOffRaw": np.uint32, "outerHitCellsRaw": np.uint32, "cellNbrOffRaw": np.uint32,
+    "cellNbrRaw": np.uint32, "cellTrkOffRaw": np.uint32, "cellTrkRaw": np.uint16,
+}
+SCALARS = ["nDigis", "nModules", "nClusters", "nHits", "nCells", "nTuples", "nVertices", "nNbrLists",
+           "nTrkLists"]
+ERROR_DTYPE = np.dtype([("rawId", "<u4"), ("word", "<u4"), ("errorType", "u1"), ("fedId", "u1"),
+                        ("pad", "u1", 2)])
+FLOAT_PRODUCTS = {"xl", "yl", "xerr", "yerr", "xg", "yg", "zg", "rg", "agcLadderR", "state", "cov", "pt", "eta",
+                  "chi2", "zv", "wv", "vchi2", "ptv2"}
+B_FIELD = 0.0114256972711507
+
+
+def _as_array(buf, name, elem):
+    if name == "errors":
+        return np.frombuffer(buf, dtype=ERROR_DTYPE).copy()
+    if name in SCALARS:
+        return int(np.frombuffer(buf, dtype=np.uint32)[0])
+    dt = _TYPES.get(name)
+    if dt is None or np.dtype(dt).itemsize != elem:
+        dt = {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[elem]
+    return np.frombuffer(buf, dtype=dt).copy()
+
+
+def _load(path, builder):
+    if not os.path.exists(path):
+        builder()
+    return ctypes.CDLL(path)
+
+
+# --------------------------------------------------------------------- generator
+_synth = None
+
+
+def synth():
+    global _synth
+    if _synth is None:
+        _synth = _load(os.path.join(LIB, "libpixsynth.so"), _build.build_synth)
+        _synth.ps_event_generate.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double, ctypes.c_void_p,
+                                             ctypes.POINTER(ctypes.c_void_p)]
+        _synth.ps_event_raw.argtypes = [ctypes.c_void_p, ctypes.POINTER(U8P), ctypes.POINTER(ctypes.c_size_t)]
+        _synth.ps_event_destroy.argtypes = [ctypes.c_void_p]
+        _synth.ps_detector_es.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(U8P),
+                                          ctypes.POINTER(ctypes.c_size_t)]
+        _synth.ps_detector_write.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        _synth.ps_detector_destroy.argtypes = [ctypes.c_void_p]
+        _synth.ps_fit_tuples.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_void_p]
+    return _synth
+
+
+class DetectorConfig(ctypes.Structure):
+    _fields_ = [("seed", ctypes.c_uint64), ("dead_column_frac", ctypes.c_double), ("bad_roc_frac", ctypes.c_double)]
+
+
+class EventConfig(ctypes.Structure):
+    _fields_ = [("tracks_per_vertex", ctypes.c_double), ("pt_min", ctypes.c_double), ("pt_index", ctypes.c_double),
+                ("eta_max", ctypes.c_double), ("noise_frac", ctypes.c_double), ("inject_errors", ctypes.c_int),
+                ("fixed_pu", ctypes.c_int)]
+
+
+class Truth(ctypes.Structure):
+    _fields_ = [("n_vertices", ctypes.c_uint32), ("n_tracks", ctypes.c_uint32), ("n_sim_hits", ctypes.c_uint32),
+                ("n_digis", ctypes.c_uint32), ("vertex_z", ctypes.c_void_p), ("track_pt", ctypes.c_void_p),
+                ("track_eta", ctypes.c_void_p), ("track_phi", ctypes.c_void_p), ("track_q", ctypes.c_void_p),
+                ("track_vertex", ctypes.c_void_p), ("track_nhits", ctypes.c_void_p)]
+
+
+ES_NAMES = ["cablingMap.bin", "gain.bin", "cpefast.bin", "beamspot.bin", "fedIds.bin"]
+BASE_SEED = 20261203
+
+
+class Detector:
+    """Seeded synthetic Phase-1 detector: ES file images and raw events."""
+
+    def __init__(self, seed=BASE_SEED, dead_column_frac=0.0, bad_roc_frac=0.0):
+        lib = synth()
+        cfg = DetectorConfig(seed, dead_column_frac, bad_roc_frac)
+        self._h = ctypes.c_void_p()
+        if lib.ps_detector_create(ctypes.byref(cfg), ctypes.byref(self._h)) != 0:
+            raise RuntimeError("ps_detector_create failed")
+        self.es = []
+        for k in range(5):
+            p = U8P()
+            n = ctypes.c_size_t()
+            lib.ps_detector_es(self._h, k, ctypes.byref(p), ctypes.byref(n))
+            self.es.append(ctypes.string_at(p, n.value))
+
+    def write(self, directory):
+        os.makedirs(directory, exist_ok=True)
+        if synth().ps_detector_write(self._h, directory.encode()) != 0:
+            raise RuntimeError("ps_detector_write failed")
+
+    def event(self, seed, pu, tracks_per_vertex=None, inject_errors=0, noise_frac=None, fixed_pu=True,
+              with_truth=False):
+        lib = synth()
+        cfg = EventConfig()
+        lib.ps_default_event_config(ctypes.byref(cfg))
+        if tracks_per_vertex is not None:
+            cfg.tracks_per_vertex = tracks_per_vertex
+        if noise_frac is not None:
+            cfg.noise_frac = noise_frac
+        cfg.inject_errors = inject_errors
+        cfg.fixed_pu = 1 if fixed_pu else 0
+        ev = ctypes.c_void_p()
+        if lib.ps_event_generate(self._h, seed, float(pu), ctypes.byref(cfg), ctypes.byref(ev)) != 0:
+            raise RuntimeError("ps_event_generate failed")
+        try:
+            p = U8P()
+            n = ctypes.c_size_t()
+            lib.ps_event_raw(ev, ctypes.byref(p), ctypes.byref(n))
+            raw = ctypes.string_at(p, n.value)
+            truth = None
+            if with_truth:
+                t = Truth()
+                lib.ps_event_truth(ev, ctypes.byref(t))
+                truth = {"n_vertices": t.n_vertices, "n_tracks": t.n_tracks, "n_sim_hits": t.n_sim_hits,
+                         "n_digis": t.n_digis}
+        finally:
+            lib.ps_event_destroy(ev)
+        return (raw, truth) if with_truth else raw
+
+    def __del__(self):
+        try:
+            synth().ps_detector_destroy(self._h)
+        except Exception:
+            pass
+
+
+def fit_tuples(seed, n, nhits):
+    """Seeded n tuples of nhits hits (MS-smeared helices) for the fit workload."""
+    hits = np.zeros((n, nhits, 3), dtype=np.float64)
+    ge = np.zeros((n, nhits, 6), dtype=np.float32)
+    truth = np.zeros((n, 5), dtype=np.float64)
+    rc = synth().ps_fit_tuples(seed, n, nhits, hits.ctypes.data, ge.ctypes.data, truth.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("ps_fit_tuples failed")
+    return hits, ge, truth
+
+
+# --------------------------------------------------------------------- GPU chain
+_gpu = None
+
+
+class ESImages(ctypes.Structure):
+    _fields_ = [("cabling", ctypes.c_char_p), ("cabling_size", ctypes.c_size_t), ("gain", ctypes.c_char_p),
+                ("gain_size", ctypes.c_size_t), ("cpe", ctypes.c_char_p), ("cpe_size", ctypes.c_size_t),
+                ("beamspot", ctypes.c_char_p), ("beamspot_size", ctypes.c_size_t), ("fedids", ctypes.c_char_p),
+                ("fedids_size", ctypes.c_size_t)]
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("max_events", ctypes.c_uint32), ("max_words_per_batch", ctypes.c_uint32),
+                ("slots", ctypes.c_uint32)]
+
+
+class EventCounts(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("n_words", "n_modules", "n_digi_errors", "n_hits", "n_cells",
+                                                "n_tuples", "n_loose", "n_vertices", "flags")]
+
+
+def gpu_lib():
+    """libpixgpu.so (built if missing)."""
+    global _gpu
+    if _gpu is None:
+        _gpu = _load(os.path.join(LIB, "libpixgpu.so"), _build.build_gpu)
+        _gpu.pg_create.argtypes = [ctypes.POINTER(ESImages), ctypes.POINTER(Config), ctypes.POINTER(ctypes.c_void_p)]
+        _gpu.pg_destroy.argtypes = [ctypes.c_void_p]
+        _gpu.pg_last_error.argtypes = [ctypes.c_void_p]
+        _gpu.pg_last_error.restype = ctypes.c_char_p
+        _gpu.pg_slot_bytes.argtypes = [ctypes.c_void_p]
+        _gpu.pg_slot_bytes.restype = ctypes.c_size_t
+        _gpu.pg_process_batch.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_char_p),
+                                          ctypes.POINTER(ctypes.c_size_t)]
+        _gpu.pg_stage_batch.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
+                                        ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_size_t)]
+        _gpu.pg_run_staged.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
+        _gpu.pg_sync.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
+        _gpu.pg_slot_stream.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
+        _gpu.pg_slot_stream.restype = ctypes.c_void_p
+        _gpu.pg_event_counts_get.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(EventCounts)]
+        _gpu.pg_get_product.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_char_p, ctypes.c_void_p,
+                                        ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int)]
+        _gpu.pg_unpack_raw.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
+        _gpu.pg_fit_broken_line.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32] + [ctypes.c_void_p] * 2 + \
+            [ctypes.c_double] + [ctypes.c_void_p] * 6
+    return _gpu
+
+
+def _raw_arrays(raws):
+    n = len(raws)
+    ptrs = (ctypes.c_char_p * n)(*raws)
+    sizes = (ctypes.c_size_t * n)(*[len(r) for r in raws])
+    return ptrs, sizes
+
+
+class Chain:
+    """A device context: resident conditions plus batch slots."""
+
+    def __init__(self, es_images, max_events=64, max_words_per_batch=None, slots=1, device=0):
+        lib = gpu_lib()
+        self._keep = list(es_images)
+        img = ESImages(*[x for b in self._keep for x in (b, len(b))])
+        if max_words_per_batch is None:
+            max_words_per_batch = max_events * 160000
+        cfg = Config(device, max_events, max_words_per_batch, slots)
+        self._h = ctypes.c_void_p()
+        rc = lib.pg_create(ctypes.byref(img), ctypes.byref(cfg), ctypes.byref(self._h))
+        if rc != 0:
+            raise RuntimeError("pg_create failed with status %d" % rc)
+        self.max_events = max_events
+
+    def _check(self, rc, what):
+        if rc != 0:
+            msg = gpu_lib().pg_last_error(self._h)
+            raise RuntimeError("%s failed (%d): %s" % (what, rc, msg.decode() if msg else ""))
+
+    def process(self, raws):
+        ptrs, sizes = _raw_arrays(raws)
+        self._check(gpu_lib().pg_process_batch(self._h, len(raws), ptrs, sizes), "pg_process_batch")
+
+    def stage(self, raws, slot=0):
+        ptrs, sizes = _raw_arrays(raws)
+        self._check(gpu_lib().pg_stage_batch(self._h, slot, len(raws), ptrs, sizes), "pg_stage_batch")
+
+    def run_staged(self, slot=0):
+        self._check(gpu_lib().pg_run_staged(self._h, slot), "pg_run_staged")
+
+    def sync(self, slot=0):
+        self._check(gpu_lib().pg_sync(self._h, slot), "pg_sync")
+
+    def stream(self, slot=0):
+        return gpu_lib().pg_slot_stream(self._h, slot)
+
+    def counts(self, k):
+        c = EventCounts()
+        self._check(gpu_lib().pg_event_counts_get(self._h, k, ctypes.byref(c)), "pg_event_counts_get")
+        return {n: getattr(c, n) for n, _ in EventCounts._fields_}
+
+    def product(self, k, name):
+        lib = gpu_lib()
+        count = ctypes.c_size_t()
+        elem = ctypes.c_int()
+        self._check(lib.pg_get_product(self._h, k, name.encode(), None, 0, ctypes.byref(count), ctypes.byref(elem)),
+                    "pg_get_product(%s)" % name)
+        buf = ctypes.create_string_buffer(max(1, count.value * elem.value))
+        self._check(lib.pg_get_product(self._h, k, name.encode(), buf, len(buf), ctypes.byref(count),
+                                       ctypes.byref(elem)), "pg_get_product(%s)" % name)
+        return _as_array(buf.raw[:count.value * elem.value], name, elem.value)
+
+    def products(self, k):
+        """All products of event k in the oracle's naming, CA lists capped as in the reference."""
+        out = {}
+        for n in SCALARS:
+            out[n] = self.product(k, n)
+        for n in ["xx", "yy", "adc", "moduleInd", "clus", "pdigi", "rawIdArr", "errors", "moduleStart", "clusInModule",
+                  "moduleId", "clusModuleStart", "xl", "yl", "xerr", "yerr", "xg", "yg", "zg", "rg", "charge", "iphi",
+                  "xsize", "ysize", "detInd", "cellInner", "cellOuter", "cellLayerPair", "cellDoubletId", "cellUsed",
+                  "tupleOff", "tupleHits", "tupleDet", "quality", "state", "cov", "pt", "eta", "chi2", "zv", "wv",
+                  "vchi2", "ptv2", "ndof", "sortInd", "idv"]:
+            out[n] = self.product(k, n)
+        if out["nHits"]:
+            for n in ["hitsLayerStart", "phiOff", "phiBins"]:
+                out[n] = self.product(k, n)
+        out["cellLayerPair"] = out["cellLayerPair"].view(np.uint8).astype(np.int16)
+        out["cellUsed"] = out["cellUsed"].view(np.uint8).astype(np.uint16)
+        # CSR lists with the reference's per-object capacities
+        def capped(off, val, cap):
+            off = off.astype(np.int64)
+            sizes = np.minimum(np.diff(off), cap)
+            newoff = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint32)
+            parts = [val[off[i]:off[i] + sizes[i]] for i in range(len(sizes))]
+            return newoff, (np.concatenate(parts) if parts else val[:0]).astype(val.dtype)
+        out["outerHitOff"], out["outerHitCells"] = capped(self.product(k, "outerHitOffRaw"),
+                                                          self.product(k, "outerHitCellsRaw"), 128)
+        if out["nHits"] == 0:
+            out["outerHitOff"] = np.zeros(1, np.uint32)
+        out["cellNbrOff"], out["cellNbr"] = capped(self.product(k, "cellNbrOffRaw"), self.product(k, "cellNbrRaw"), 36)
+        out["cellTrkOff"], out["cellTrk"] = capped(self.product(k, "cellTrkOffRaw"), self.product(k, "cellTrkRaw"), 48)
+        return out
+
+    def fit(self, N, hits, ge, B=B_FIELD):
+        """Broken-line fit of host arrays hits[n, N, 3] (f64), ge[n, N, 6] (f32) on the device."""
+        import torch
+        n = hits.shape[0]
+        dh = torch.from_numpy(np.ascontiguousarray(hits[:, :N, :])).cuda()
+        dg = torch.from_numpy(np.ascontiguousarray(ge[:, :N, :])).cuda()
+        st = torch.empty((n, 5), dtype=torch.float32, device="cuda")
+        cv = torch.empty((n, 15), dtype=torch.float32, device="cuda")
+        pt = torch.empty(n, dtype=torch.float32, device="cuda")
+        eta = torch.empty(n, dtype=torch.float32, device="cuda")
+        chi2 = torch.empty(n, dtype=torch.float32, device="cuda")
+        s = torch.cuda.current_stream().cuda_stream
+        self._check(gpu_lib().pg_fit_broken_line(self._h, N, n, dh.data_ptr(), dg.data_ptr(), B, st.data_ptr(),
+                                                 cv.data_ptr(), pt.data_ptr(), eta.data_ptr(), chi2.data_ptr(), s),
+                    "pg_fit_broken_line")
+        torch.cuda.synchronize()
+        return {"state": st.cpu().numpy(), "cov": cv.cpu().numpy(), "pt": pt.cpu().numpy(), "eta": eta.cpu().numpy(),
+                "chi2": chi2.cpu().numpy()}
+
+    def close(self):
+        if self._h:
+            gpu_lib().pg_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,91 @@
+"""The B200 chain (libpixgpu.so through its C ABI) against the golden
+fixtures of the reference and against the CPU oracle.
+
+Integers, indices and orderings (digis, clusters, hits sizes and iphi, phi
+histogram, doublets, CA links, tuples, track lists, qualities, vertex
+assignments) must be identical; floating-point products must agree within
+1e-5 relative (the tolerance the fits and vertices are specified with).
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_event, load_golden
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def chain(default_detector):
+    import pixgpu
+    c = pixgpu.Chain(default_detector.es, max_events=8, max_words_per_batch=8 * 200000)
+    yield c
+    c.close()
+
+
+def _report(diffs):
+    return "\n".join("%s: %s" % d for d in diffs)
+
+
+@pytest.mark.parametrize("name", ["pu3", "pu8", "pu5_errors", "pu5_deadcols"])
+def test_matches_reference_fixture(name, golden_meta, detectors):
+    import oracle
+    import pixgpu
+    m = [x for x in golden_meta if x["name"] == name][0]
+    det, raw = golden_event(m, detectors)
+    c = pixgpu.Chain(det.es, max_events=1, max_words_per_batch=300000)
+    try:
+        c.process([raw])
+        got = c.products(0)
+    finally:
+        c.close()
+    diffs = oracle.compare(load_golden(name), got, rtol=RTOL)
+    assert diffs == [], _report(diffs)
+
+
+@pytest.mark.parametrize("seed,pu", [(11, 20), (12, 50), (13, 50)])
+def test_matches_oracle(chain, default_detector, seed, pu):
+    import oracle
+    raw = default_detector.event(seed, pu)
+    want = oracle.Oracle(default_detector.es).process(raw)
+    chain.process([raw])
+    got = chain.products(0)
+    diffs = oracle.compare(want, got, rtol=RTOL)
+    assert diffs == [], _report(diffs)
+
+
+def test_batch_results_equal_single_event_results(chain, default_detector):
+    """Each event's products are the same alone and inside a mixed-PU batch."""
+    import oracle
+    raws = [default_detector.event(30 + k, pu) for k, pu in enumerate([5, 50, 20, 80, 1, 35])]
+    chain.process(raws)
+    mixed = [chain.products(k) for k in range(len(raws))]
+    for k, raw in enumerate(raws):
+        chain.process([raw])
+        alone = chain.products(0)
+        diffs = oracle.compare(alone, mixed[k], rtol=0.0)
+        assert diffs == [], "event %d: %s" % (k, _report(diffs))
+
+
+def test_empty_and_tiny_events(chain, default_detector):
+    import oracle
+    raws = [default_detector.event(50, 0), default_detector.event(51, 1)]
+    chain.process(raws)
+    orc = oracle.Oracle(default_detector.es)
+    for k, raw in enumerate(raws):
+        diffs = oracle.compare(orc.process(raw), chain.products(k), rtol=RTOL)
+        assert diffs == [], _report(diffs)
+
+
+@pytest.mark.parametrize("nhits,N", [(3, 3), (4, 4), (5, 4)])
+def test_broken_line_fit_matches_oracle(chain, nhits, N):
+    import oracle
+    import pixgpu
+    hits, ge, _ = pixgpu.fit_tuples(777 + nhits, 4096, nhits)
+    want = oracle.Oracle(pixgpu.Detector().es).fit(N, hits, ge)
+    got = chain.fit(N, hits, ge)
+    for k in want:
+        a, b = want[k].astype(np.float64), got[k].astype(np.float64)
+        den = np.maximum(np.maximum(np.abs(a), np.abs(b)), 1e-30)
+        rel = np.abs(a - b) / den
+        assert rel.max() <= RTOL, (k, float(rel.max()))

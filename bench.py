@@ -1,0 +1,465 @@
+#!/usr/bin/env python
+"""Throughput and latency of the B200 pixel reconstruction chain at PU50.
+
+One JSON line (rank 0):
+  value      events/s of the batched chain (64 events per launch sequence,
+             captured CUDA graph), inputs resident in a device pool when the
+             timed region starts, results packed into mapped host memory;
+  e2e        the same through the public C ABI (pg_submit) from host raw
+             records: FED scan on the host, H2D of the words, chain, results
+             written to host memory, every step inside the timed region;
+  per_event  the plain one-event-per-launch chain (no graph), for the
+             batched-vs-per-event ratio;
+  serving    the continuous-batching serving loop (pg_serve): Poisson
+             arrivals, p50/p99 latency from arrival to completion;
+  roofline   the dominant kernel (largest share of device time, found by a
+             timed census of every kernel) against the measured HBM copy
+             bandwidth, its duration measured with timing events captured
+             into the graphs of the timed region;
+  cpu_baseline  the reference's serial chain (checker build of its own
+             sources, or the oracle port when that build is absent) on the
+             host cores.
+
+`--impl reference` times the reference's CPU implementation of the chain on
+the same workload and prints the same line with "impl": "reference".
+
+Multi-GPU (torchrun): replicas, one process per GPU, each running the same
+per-GPU workload; value = all events / max-over-ranks time ("scaling": "weak").
+"""
+import argparse
+import collections
+import concurrent.futures as cf
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "pixeltrack-standalone_b200")
+sys.path.insert(0, PKG)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "events/s and p50/p99 latency at PU50: batched serving vs per-event chain, one B200"
+DATA = ("synthetic: seeded Phase-1 pixel events (1856 modules, 108 FEDs, helices in 3.8 T, Landau charge), "
+        "PU50 ~61k digis/event, packed into FED words through the generated cabling map")
+PU = 50
+SEED0 = 20261203
+
+# Algorithmic bytes per unit of each kernel (each column read once by the
+# consuming stage and written once at its declared width; ES tables resident
+# and excluded).  Units: W digis (FED words), H hits, C doublets, E CA links,
+# Sh hits over tuples, N tuples, M active modules.
+KERNEL_BYTES = {
+    "kRawToDigi": lambda u: 50.5 * u["W"],            # raw-to-digi 38.5*W + calibration 12*W (fused)
+    "kModuleBoundaries": lambda u: 6.0 * u["W"],
+    "kFindClusters": lambda u: 24.0 * u["W"],         # findClus 10*W + charge cut 14*W (fused)
+    "kGetHits": lambda u: 12.0 * u["W"] + 44.0 * u["H"] + 112.0 * u["M"],
+    "kDoubletWrite": lambda u: 14.0 * u["H"] + 44.0 * u["C"],
+    "kConnect": lambda u: 40.0 * u["C"] + 8.0 * u["E"],
+    "kFishbone": lambda u: 16.0 * u["C"],
+    "kNtupletWrite": lambda u: 2.0 * u["Sh"] + 9.0 * u["N"],
+    "kBLFit": lambda u: 68.0 * u["Sh"] + 92.0 * u["N"],
+    "kVertices": lambda u: 16.0 * u["N"],
+    # list ordering: read + write of every ordered entry (cells by outer hit,
+    # CA links, tracks per cell, tuples per hit)
+    "kSortSegments": lambda u: 2 * (4.0 * u["C"] + 4.0 * u["E"] + 2.0 * u["Sh"] + 2.0 * u["Sh"]),
+}
+
+
+def chain_bytes(u):
+    """Whole-chain algorithmic bytes: 92.5 W + 64 H + 100 C + 8 E + 76 Sh + 42 N + 92 T (T = N fitted)."""
+    return 92.5 * u["W"] + 64 * u["H"] + 100 * u["C"] + 8 * u["E"] + 76 * u["Sh"] + 42 * u["N"] + 92 * u["N"]
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--batch", type=int, default=64, help="events per launch sequence")
+    p.add_argument("--events", type=int, default=576, help="distinct PU50 events (inputs > L2)")
+    p.add_argument("--slots", type=int, default=2, help="batches in flight")
+    p.add_argument("--per-event", type=int, default=256, help="events for the one-event-per-launch leg")
+    p.add_argument("--serve", type=int, default=4000, help="requests for the serving leg (0: skip)")
+    p.add_argument("--serve-batch", type=int, default=16, help="max events per serving batch")
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------------------- helpers
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+def make_events(det, n, pu=PU, base=SEED0 + 100000):
+    """n distinct seeded events, generated on all host cores."""
+    with cf.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+        return list(ex.map(lambda k: det.event(base + k, pu), range(n)))
+
+
+class Clocks:
+    """nvidia-smi samples during a timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.out.close()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def units_of(summary):
+    return {"W": summary["n_digis"], "H": summary["n_hits"], "C": summary["n_cells"], "E": summary["n_edges"],
+            "Sh": summary["n_tuple_hits"], "N": summary["n_tuples"], "M": summary["n_modules"]}
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(a):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    import pixgpu
+    det = pixgpu.Detector()
+    cores = os.cpu_count() or 1
+    n_distinct = 64
+    raws = make_events(det, n_distinct)
+    if oracle.ref_available():
+        kind = "reference"
+        d = tempfile.mkdtemp()
+        det.write(d)
+        timer = lambda evs: oracle.ref_time_events(d, evs, cores)[0]  # noqa: E731
+    else:
+        kind = "port"
+        orc = oracle.Oracle(det.es)
+        timer = lambda evs: orc.time_events(evs, cores)[0]  # noqa: E731
+    # pilot: size each step so that the whole run stays within a few minutes
+    pilot = timer(raws[:min(len(raws), 2 * cores)])
+    rate = min(len(raws), 2 * cores) / pilot
+    per_step = int(max(cores, min(n_distinct, rate * 120.0 / max(1, a.steps + a.warmup))))
+    for i in range(a.warmup):
+        timer([raws[(i * per_step + k) % n_distinct] for k in range(per_step)])
+    tot = 0.0
+    for i in range(a.steps):
+        tot += timer([raws[(i * per_step + k) % n_distinct] for k in range(per_step)])
+    value = a.steps * per_step / tot
+    line = {"metric": METRIC, "value": value, "unit": "events/s", "impl": "reference", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * tot / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u16/u32 int, f32 hits and cuts, f64 fits",
+            "data": DATA,
+            "config": {"workload": "PU50 pixel chain, events processed on host threads (one chain instance "
+                                   "per thread, the reference's event-level concurrency)",
+                       "pu": PU, "events_per_step": per_step, "distinct_events": n_distinct},
+            "cpu_baseline": {"value": value, "unit": "events/s", "cores": cores, "kind": kind,
+                             "sample": "%d PU50 events per step x %d steps" % (per_step, a.steps)},
+            "e2e": {"value": value, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- our arm
+def pipeline(chain, torch, n_steps, submit, on_done):
+    """Runs n_steps submissions over the chain's slots, keeping every slot busy;
+    returns device milliseconds between a start event joined into every slot
+    stream and an end event joined from all of them."""
+    streams = [torch.cuda.ExternalStream(chain.stream(s)) for s in range(chain.slots)]
+    side = torch.cuda.Stream()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(side)
+    for s in streams:
+        s.wait_event(start)
+    inflight = collections.deque()
+    for i in range(n_steps):
+        while True:
+            slot = submit(i)
+            if slot is not None:
+                break
+            s0 = inflight.popleft()
+            chain.wait(s0)
+            on_done(s0)
+            chain.release(s0)
+        inflight.append(slot)
+    while inflight:
+        s0 = inflight.popleft()
+        chain.wait(s0)
+        on_done(s0)
+        chain.release(s0)
+    for s in streams:
+        e = torch.cuda.Event()
+        e.record(s)
+        side.wait_event(e)
+    end.record(side)
+    end.synchronize()
+    return start.elapsed_time(end)
+
+
+def run_ours(a):
+    import torch
+    import pixgpu
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    dev = local
+    B = a.batch
+    det = pixgpu.Detector()
+    raws = make_events(det, a.events)
+    nw = [len(r) // 4 for r in raws]  # upper bound of FED words per event
+    max_words = int(max(nw)) * B + 1024
+    input_bytes = sum(len(r) for r in raws)
+
+    # ------------------------------------------------------------ batched, device-resident
+    chain = pixgpu.Chain(det.es, max_events=B, max_words_per_batch=max_words, slots=a.slots, device=dev,
+                         pool_words=sum(nw) + 64 * len(nw) + 4096)
+    handles = []
+    for r in raws:
+        h = chain.pool_put(r)
+        while h is None:  # staging buffers in flight
+            time.sleep(0.001)
+            h = chain.pool_put(r)
+        handles.append(h)
+    nb = len(handles) // B
+    batches = [handles[(i % nb) * B:(i % nb) * B + B] for i in range(max(nb, 1))]
+
+    # census: every kernel timed once, to find the dominant one
+    chain.set_probe("*")
+    s = chain.submit_pooled(batches[0], keep=True)
+    chain.wait(s)
+    census = collections.defaultdict(float)
+    launches = collections.Counter()
+    for name, ms in chain.probe_read(s):
+        census[name] += ms
+        launches[name] += 1
+    sums = chain.summary(s)
+    chain.release(s)
+    launches_per_batch = sum(launches.values()) + 1  # + the pool gather
+    total_ms = sum(census.values())
+    top = max(census, key=census.get)
+    chain.set_probe(top)
+    chain.prepare(B)
+
+    probe_ms = []
+    units = collections.Counter()
+    result_bytes = [0]
+
+    def done(slot):
+        probe_ms.extend(ms for _, ms in chain.probe_read(slot))
+        sm = chain.summary(slot)
+        units.update(units_of(sm))
+        result_bytes[0] += sm["result_bytes"]
+
+    sub = lambda i: chain.submit_pooled(batches[i % len(batches)], keep=True)  # noqa: E731
+    pipeline(chain, torch, a.warmup, sub, lambda s: None)
+    probe_ms.clear()
+    with Clocks(dev) as clk:
+        ms = pipeline(chain, torch, a.steps, sub, done)
+    clocks = clk.summary()
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    events = a.steps * B
+    value = world * events / (ms / 1e3)
+    kernel_ms = float(np.mean(probe_ms)) if probe_ms else None
+    launches_of_top = launches[top]
+    hbm, peak_kind = peaks()
+    u_evt = {k: v / events for k, v in units.items()}
+    roof = None
+    if kernel_ms and top in KERNEL_BYTES:
+        # bytes of one launch: the kernel processes the whole batch (B events) per launch,
+        # split evenly over its launches per batch
+        bytes_per_launch = KERNEL_BYTES[top](u_evt) * B / launches_of_top
+        ach = bytes_per_launch / (kernel_ms / 1e3) / 1e9
+        roof = {"bound": "hbm", "kernel": top, "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "traffic": None, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_kind == "measured" else "fallback 6650 GB/s",
+                "bytes_per_launch": bytes_per_launch, "launch_ms": kernel_ms, "launches_timed": len(probe_ms)}
+    chain_ach = chain_bytes(u_evt) * value / world / 1e9
+    chain.set_probe(None)
+    chain.close()
+
+    out = {"metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "u16/u32 int, f32 hits and cuts, f64 fits", "data": DATA,
+           "config": {"workload": "PU50 batched chain: %d events per launch sequence (captured graph), %d batches "
+                                  "in flight, inputs in a device-resident pool" % (B, a.slots),
+                      "pu": PU, "events_per_step": B, "distinct_events": len(raws),
+                      "input_bytes": input_bytes,
+                      "l2": "inputs larger than L2: %d distinct events, %.0f MB of raw records, cycled"
+                            % (len(raws), input_bytes / 1e6),
+                      "parallelism": "replicas (events shard across GPUs, no collective)"},
+           "gpu_launches": launches_per_batch * a.steps,
+           "clocks": clocks,
+           "roofline": roof,
+           "chain_roofline": {"achieved": chain_ach, "peak": hbm, "unit": "GB/s", "frac": chain_ach / hbm,
+                              "bytes_per_event": chain_bytes(u_evt)},
+           "units_per_event": u_evt,
+           "kernel_shares": {k: round(v / total_ms, 4) for k, v in
+                             sorted(census.items(), key=lambda x: -x[1])[:12]},
+           "result_bytes_per_step": result_bytes[0] / max(1, a.steps)}
+
+    # ------------------------------------------------------------ end to end through pg_submit
+    e2e_chain = pixgpu.Chain(det.es, max_events=B, max_words_per_batch=max_words, slots=a.slots, device=dev)
+    e2e_chain.prepare(B)
+    nbh = len(raws) // B
+    host_batches = [raws[(i % nbh) * B:(i % nbh) * B + B] for i in range(nbh)]
+    h2d = [0]
+    d2h = [0]
+
+    def e2e_done(slot):
+        sm = e2e_chain.summary(slot)
+        d2h[0] += sm["result_bytes"]
+        h2d[0] += 4 * sm["n_digis"] + sm["n_digis"] // 2 + 4 * (sm["n_events"] + 1)
+
+    e2e_sub = lambda i: e2e_chain.submit(host_batches[i % nbh])  # noqa: E731
+    pipeline(e2e_chain, torch, a.warmup, e2e_sub, lambda s: None)
+    t0 = time.perf_counter()
+    ems = pipeline(e2e_chain, torch, a.steps, e2e_sub, e2e_done)
+    wall = time.perf_counter() - t0
+    e2e_chain.close()
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ems], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+    out["e2e"] = {"value": world * events / (ems / 1e3), "unit": "events/s",
+                  "h2d_bytes_per_step": h2d[0] / a.steps, "d2h_bytes_per_step": d2h[0] / a.steps,
+                  "host_wall_events_per_s": events / wall,
+                  "path": "pg_submit: host FED scan + H2D of words + chain + results into mapped host memory"}
+
+    if rank == 0 and world == 1:
+        # ------------------------------------------------------------ one event per launch (plain chain)
+        pe = {}
+        for label, slots, graphs in (("1 stream", 1, False), ("4 streams", 4, False)):
+            c1 = pixgpu.Chain(det.es, max_events=1, max_words_per_batch=int(max(nw)) + 1024, slots=slots,
+                              device=dev, use_graphs=graphs, pool_words=sum(nw) + 64 * len(nw) + 4096)
+            hs = [c1.pool_put(r) for r in raws[:64]]
+            sub1 = lambda i: c1.submit_pooled([hs[i % len(hs)]], keep=True)  # noqa: E731
+            pipeline(c1, torch, 8, sub1, lambda s: None)
+            pms = pipeline(c1, torch, a.per_event, sub1, lambda s: None)
+            c1.close()
+            pe[label] = a.per_event / (pms / 1e3)
+        best = max(pe.values())
+        out["per_event"] = {"events_per_s": pe, "mode": "one event per launch sequence, plain launches (no graph), "
+                                                          "device-resident inputs"}
+        out["batched_vs_per_event"] = value / best
+
+        # ------------------------------------------------------------ serving loop
+        if a.serve:
+            sv = {}
+            sc = pixgpu.Chain(det.es, max_events=a.serve_batch, max_words_per_batch=int(max(nw)) * a.serve_batch,
+                              slots=4, device=dev, pool_words=64 * 1000 * 1000)
+            sc.prepare(a.serve_batch)
+            for frac in (0.5, 0.8):
+                rate = frac * value
+                st, lat = sc.serve(raws, a.serve, rate_hz=rate, max_batch=a.serve_batch, seed=11, upload_threads=4)
+                sv["%.0f%% of batched throughput" % (100 * frac)] = {
+                    "offered_hz": st["offered_hz"], "events_per_s": st["events_per_s"], "p50_ms": st["p50_ms"],
+                    "p99_ms": st["p99_ms"], "mean_batch": st["mean_batch"], "batches": st["batches"],
+                    "admission_waits": st["admission_waits"]}
+            sc.close()
+            out["serving"] = {"pu": PU, "requests": a.serve, "max_batch": a.serve_batch, "slots": 4, "points": sv}
+
+        # ------------------------------------------------------------ CPU baseline
+        import oracle
+        cores = os.cpu_count() or 1
+        n_cpu = int(max(cores, min(len(raws), a.cpu_seconds * 9.0 * cores)))
+        sample = raws[:n_cpu]
+        if oracle.ref_available():
+            d = tempfile.mkdtemp()
+            det.write(d)
+            wall_c, _ = oracle.ref_time_events(d, sample, cores)
+            kind = "reference"
+        else:
+            wall_c, _ = oracle.Oracle(det.es).time_events(sample, cores)
+            kind = "port"
+        out["cpu_baseline"] = {"value": len(sample) / wall_c, "unit": "events/s", "cores": cores, "kind": kind,
+                               "sample": "%d distinct PU50 events, one chain instance per thread" % len(sample)}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

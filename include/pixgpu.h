@@ -23,6 +23,13 @@
  *                        TrackingRecHit2DCPU, PixelTrackHeterogeneous, ZVertexHeterogeneous
  *                        (the *SoAFromCUDA transfer modules of the CUDA program)
  *   pg_fit_broken_line   HelixFitOnGPU::launchBrokenLineKernels (BrokenLineFitOnGPU.cc:3-68)
+ *   pg_submit / pg_query / pg_wait / pg_result / pg_release
+ *                        the acquire()/produce() split of the CUDA modules (ExternalWork:
+ *                        work queued on the event's stream, the framework told when done)
+ *                        and the SoA-from-CUDA transfer modules
+ *   pg_pool_* / pg_serve the reference has no counterpart: its EventProcessor runs one event
+ *                        per stream; these are the batching and admission layer above
+ *                        the same chain
  */
 #ifndef PIXGPU_H
 #define PIXGPU_H
@@ -59,7 +66,11 @@ typedef struct pg_config {
   int device;                    /* CUDA device ordinal */
   uint32_t max_events;           /* events per batch */
   uint32_t max_words_per_batch;  /* FED payload words over a whole batch */
-  uint32_t slots;                /* independent batch slots (streams + workspaces) */
+  uint32_t slots;                /* independent batch slots (streams + workspaces); 0: as many as fit in
+                                    hbm_fraction of the free device memory, at most 16 */
+  uint32_t use_graphs;           /* 1: the chain for each batch size is captured once as a CUDA graph */
+  uint64_t pool_words;           /* device-resident input pool, in FED words (0: no pool) */
+  double hbm_fraction;           /* share of free device memory the slots may take when slots == 0 */
 } pg_config;
 
 typedef struct pg_event_counts {
@@ -70,6 +81,8 @@ typedef struct pg_event_counts {
 
 void pg_default_config(pg_config* cfg);
 int pg_create(const pg_es_images* es, const pg_config* cfg, pg_ctx** out);
+/* the configuration in force (slots resolved when created with slots == 0) */
+int pg_get_config(const pg_ctx* ctx, pg_config* out);
 void pg_destroy(pg_ctx* ctx);
 const char* pg_last_error(const pg_ctx* ctx);
 /* device bytes held by one batch slot */
@@ -105,6 +118,116 @@ int pg_stage_batch(pg_ctx* ctx, uint32_t slot, uint32_t n_events, const uint8_t*
 int pg_run_staged(pg_ctx* ctx, uint32_t slot);
 int pg_sync(pg_ctx* ctx, uint32_t slot);
 void* pg_slot_stream(pg_ctx* ctx, uint32_t slot);
+
+/* Compact per-event result of an asynchronous batch: the loose tracks (quality >= loose)
+ * in tuple order and the vertices, the content of PixelTrackHeterogeneous /
+ * ZVertexHeterogeneous that a consumer reads (PixelTrackSoAFromCUDA.cc,
+ * PixelVertexSoAFromCUDA.cc).  Written by the device into mapped pinned host memory;
+ * the pointers stay valid until pg_release of the slot. */
+typedef struct pg_result_view {
+  uint32_t n_tracks;       /* loose tracks stored (at most 8192) */
+  uint32_t n_loose_all;    /* loose tracks found */
+  uint32_t n_vertices, n_hits, n_tuples, n_digis, n_cells;
+  uint32_t flags;          /* capacity flags; bit 16: more loose tracks than stored */
+  const uint32_t* tuple_index;   /* [n_tracks] index of the tuple in the full track SoA */
+  const uint8_t* track_n_hits;   /* [n_tracks] */
+  const uint8_t* quality;        /* [n_tracks] */
+  const float* state;            /* [n_tracks][5] phi, Tip, 1/pt*q, cot(theta), Zip */
+  const float* cov;              /* [n_tracks][15] */
+  const float* pt;               /* [n_tracks] */
+  const float* eta;
+  const float* chi2;
+  const uint16_t* hits;          /* [n_tracks][5] hit indices, 0xffff past n_hits */
+  const int16_t* vertex;         /* [n_tracks] vertex index or -1 */
+  const float* zv;               /* [n_vertices] */
+  const float* wv;
+  const float* vchi2;
+  const float* ptv2;
+  const int32_t* ndof;
+  const uint16_t* sort_ind;      /* vertices by decreasing sum pt^2 */
+} pg_result_view;
+
+/* Asynchronous batches.  pg_submit unpacks, copies and launches on a free slot
+ * and returns its index (PG_ERR_BUSY when every slot is in use); pg_query returns
+ * PG_OK when the batch has finished and PG_ERR_BUSY while it runs; pg_wait blocks;
+ * pg_result gives the view of event k; pg_release makes the slot free again. */
+int pg_submit(pg_ctx* ctx, uint32_t n_events, const uint8_t* const* raws, const size_t* raw_sizes,
+              uint32_t* slot);
+int pg_query(pg_ctx* ctx, uint32_t slot);
+int pg_wait(pg_ctx* ctx, uint32_t slot);
+int pg_result(pg_ctx* ctx, uint32_t slot, uint32_t k, pg_result_view* view);
+int pg_release(pg_ctx* ctx, uint32_t slot);
+
+/* Totals over the finished batch on a slot: result sizes (the bytes the device
+ * wrote into host memory) and the per-event counts the roofline model uses. */
+typedef struct pg_batch_summary {
+  uint32_t n_events, flags;          /* flags: OR over the events */
+  uint64_t n_tracks, n_vertices, result_bytes;
+  uint64_t n_digis, n_modules, n_hits, n_cells, n_edges, n_tuples, n_tuple_hits;
+} pg_batch_summary;
+int pg_batch_summary_get(pg_ctx* ctx, uint32_t slot, pg_batch_summary* out);
+
+/* Device-resident input pool (contexts created with pool_words > 0).  pg_pool_put
+ * unpacks one event, copies its words into the pool on the upload stream and
+ * returns a handle; PG_ERR_NOMEM means the pool has no room now (admission
+ * refused), PG_ERR_BUSY that all pinned staging buffers are in flight.
+ * pg_submit_pooled gathers the given events into a free slot and launches the
+ * chain; their pool space is released once the gather has run, unless flags has
+ * PG_POOL_KEEP (the events stay resident and may be submitted again).
+ * pg_pool_release drops an event that is not part of a pending batch. */
+#define PG_POOL_KEEP 1u
+int pg_pool_put(pg_ctx* ctx, const uint8_t* raw, size_t raw_size, uint32_t* handle);
+int pg_pool_release(pg_ctx* ctx, uint32_t handle);
+int pg_pool_info(pg_ctx* ctx, uint64_t* cap_words, uint64_t* free_words, uint32_t* live_events);
+int pg_submit_pooled(pg_ctx* ctx, uint32_t n_events, const uint32_t* handles, uint32_t flags, uint32_t* slot);
+
+/* Captures the chain of every batch size 1..max_batch on every slot (graphs are
+ * otherwise captured on first use). */
+int pg_prepare(pg_ctx* ctx, uint32_t max_batch);
+
+/* Serving loop with continuous batching over a device-resident pool.  Request i
+ * arrives at arrivals[i] seconds (or on a Poisson schedule of rate_hz when
+ * arrivals is NULL) and carries raw event request_event[i] (or i % n_raw).
+ * Arrivals are unpacked by upload_threads host threads and admitted into the pool
+ * while it has room; whenever a slot is free, all admitted events waiting (up to
+ * max_batch and the slot's word capacity) are dispatched as one batch.  Latency is
+ * measured from arrival to the host seeing the batch complete.  fn, when given, is
+ * called on the calling thread for every request with its result view. */
+typedef struct pg_serve_config {
+  uint32_t n_requests;
+  double rate_hz;
+  uint64_t seed;
+  uint32_t max_batch;        /* 0: max_events */
+  uint32_t upload_threads;
+} pg_serve_config;
+
+typedef struct pg_serve_stats {
+  uint32_t completed, batches, max_batch_seen, admission_waits;
+  double wall_s;             /* first arrival to last completion */
+  double events_per_s;
+  double mean_batch;
+  double offered_hz;
+  double p50_ms, p90_ms, p99_ms, mean_ms, max_ms;
+} pg_serve_stats;
+
+typedef void (*pg_result_fn)(void* user, uint32_t request, uint32_t event, const pg_result_view* view);
+
+void pg_default_serve_config(pg_serve_config* cfg);
+int pg_serve(pg_ctx* ctx, uint32_t n_raw, const uint8_t* const* raws, const size_t* raw_sizes,
+             const pg_serve_config* cfg, const double* arrivals, const uint32_t* request_event,
+             pg_serve_stats* stats, double* latencies, pg_result_fn fn, void* user);
+
+/* Kernel timing.  pg_set_probe(ctx, name) brackets every launch of the named
+ * kernel ("*": every kernel, NULL: none) with timing events, in plain launches
+ * and inside graphs captured afterwards (existing graphs are dropped; every slot
+ * must be free).  pg_probe_read gives the device time of each timed launch of
+ * the last finished batch on a slot. */
+typedef struct pg_probe_entry {
+  const char* kernel;
+  float ms;
+} pg_probe_entry;
+int pg_set_probe(pg_ctx* ctx, const char* kernel);
+int pg_probe_read(pg_ctx* ctx, uint32_t slot, uint32_t max, pg_probe_entry* out, uint32_t* n);
 
 /* Broken-line fits of n tuples of N (3 or 4) hits already on the device:
  * hits[(t*N+i)*3+k], ge[(t*N+i)*6+k]; outputs state[t*5+k], cov[t*15+k],

@@ -38,6 +38,7 @@
 #include <stdexcept>
 #include <iomanip>
 #include <chrono>
+#include <thread>
 
 #include "Eigen/Core"
 
@@ -268,6 +269,7 @@ int pr_process(void* p, const uint8_t* raw, size_t nraw, int dump) {
   ZVertexHeterogeneous vertices = h.vtx->make(tracks.get(), 0.5f);
   auto t1 = std::chrono::steady_clock::now();
   h.lastSeconds = std::chrono::duration<double>(t1 - t0).count();
+  if (dump < 0) return 0;  // timing only: no product copies
 
   // ---- record products
   uint32_t nDigis = digis.nDigis();
@@ -447,6 +449,45 @@ int pr_names(void* p, char* buf, size_t n) {
 // Seconds spent in the chain (excluding input parsing and product recording)
 // during the last pr_process call.
 double pr_last_seconds(void* p) { return static_cast<RefChain*>(p)->lastSeconds; }
+
+// Event-level parallel timing, the reference's own concurrency model (one
+// chain instance per stream, README.md:222-226): `threads` host threads, each
+// with its own instance, take events from a shared counter.  Returns the wall
+// seconds over all events (instances created beforehand), or < 0 on failure;
+// lat[k] receives event k's chain seconds.
+double pr_time_events(const char* datadir, const uint8_t* const* raws, const size_t* sizes, int n, int threads,
+                      double* lat) {
+  if (threads < 1) threads = 1;
+  std::vector<void*> chains;
+  try {
+    for (int t = 0; t < threads; ++t) chains.push_back(pr_create(datadir));
+  } catch (std::exception&) {
+    for (void* c : chains) pr_destroy(c);
+    return -1.0;
+  }
+  std::atomic<int> next{0}, failed{0};
+  std::vector<std::thread> pool;
+  auto t0 = std::chrono::steady_clock::now();
+  for (int t = 0; t < threads; ++t) {
+    pool.emplace_back([&, t]() {
+      for (;;) {
+        int k = next.fetch_add(1);
+        if (k >= n) break;
+        try {
+          if (pr_process(chains[t], raws[k], sizes[k], -1) != 0) failed++;
+        } catch (std::exception&) {
+          failed++;
+        }
+        if (lat) lat[k] = static_cast<RefChain*>(chains[t])->lastSeconds;
+      }
+    });
+  }
+  for (auto& th : pool) th.join();
+  auto t1 = std::chrono::steady_clock::now();
+  for (void* c : chains) pr_destroy(c);
+  if (failed) return -1.0;
+  return std::chrono::duration<double>(t1 - t0).count();
+}
 
 }  // extern "C"
 

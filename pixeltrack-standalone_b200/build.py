@@ -26,7 +26,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # and bit-exact cluster/hit/doublet/tuple results depend on it.
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-I", INC, "-I", CSRC,
            "--expt-relaxed-constexpr"] + ARCH
-CU_SOURCES = ["scan.cu", "k_local.cu", "k_ca.cu", "k_fit.cu", "k_vertex.cu", "chain.cu", "capi.cu"]
+CU_SOURCES = ["scan.cu", "k_local.cu", "k_ca.cu", "k_fit.cu", "k_vertex.cu", "k_pack.cu", "chain.cu", "capi.cu",
+              "pool.cu", "serve.cu"]
 
 
 def _run(cmd):

@@ -1,53 +1,18 @@
 // C ABI of the B200 pixel chain (include/pixgpu.h): context, ES upload,
-// host FED scan, batch slots and product access.
+// host FED scan, batch slots, captured graphs, asynchronous batches and
+// product access.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
-#include <mutex>
 #include <string>
 #include <vector>
 
-#include "pixgpu.h"
-#include "pixgpu_internal.cuh"
+#include "runtime.h"
 
 namespace pixgpu {
 cudaError_t fitDirect(int N, uint32_t n, const double* hits, const float* ge, double B, float* state, float* cov,
                       float* pt, float* eta, float* chi2, cudaStream_t stream);
-}
-
-using namespace pixgpu;
-
-namespace {
-
-struct HostES {
-  std::vector<uint32_t> fedIds;
-};
-
-struct Slot {
-  void* dmem = nullptr;
-  Workspace ws{};
-  cudaStream_t stream = nullptr;
-  uint32_t* hWords = nullptr;   // pinned staging
-  uint8_t* hFed = nullptr;
-  uint32_t* hOffsets = nullptr;
-  uint32_t nEvents = 0;
-  bool staged = false;
-};
-
-}  // namespace
-
-struct pg_ctx {
-  int device = 0;
-  pg_config cfg{};
-  HostES hes;
-  void* esMem = nullptr;
-  DeviceES des{};
-  std::vector<Slot> slots;
-  std::string err;
-  std::mutex mu;
-};
-
-namespace {
 
 int fail(pg_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;
@@ -56,6 +21,11 @@ int fail(pg_ctx* c, int code, const std::string& msg) {
 int cudaFail(pg_ctx* c, cudaError_t e, const char* where) {
   return fail(c, PG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
+}  // namespace pixgpu
+
+using namespace pixgpu;
+
+namespace {
 
 struct Rd {
   const uint8_t* p;
@@ -77,9 +47,11 @@ struct Rd {
   }
 };
 
+}  // namespace
+
 // FED scan: Source record -> (words, fed index per word pair); follows
 // SiPixelRawToClusterCUDA.cc:78-138 with ErrorChecker.cc:36-91 semantics.
-int unpackRaw(const std::vector<uint32_t>& fedIds, const uint8_t* raw, size_t n, uint32_t* words, uint8_t* fed,
+int pixgpu::unpackRaw(const std::vector<uint32_t>& fedIds, const uint8_t* raw, size_t n, uint32_t* words, uint8_t* fed,
               uint32_t cap, uint32_t* nWordsOut) {
   const uint8_t* fedPtr[4096];
   uint32_t fedSize[4096];
@@ -131,6 +103,8 @@ int unpackRaw(const std::vector<uint32_t>& fedIds, const uint8_t* raw, size_t n,
   *nWordsOut = wc;
   return PG_OK;
 }
+
+namespace {
 
 int uploadES(pg_ctx* c, const pg_es_images* es) {
   Rd cab{es->cabling, es->cabling_size}, gain{es->gain, es->gain_size}, cpe{es->cpe, es->cpe_size},
@@ -240,6 +214,32 @@ int stage(pg_ctx* c, Slot& s, uint32_t nEvents, const uint8_t* const* raws, cons
   return PG_OK;
 }
 
+// Captures runChain + result packing for `n` events on the slot's stream.
+int captureGraph(pg_ctx* c, Slot& s, uint32_t n, cudaGraphExec_t* out) {
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cudaFail(c, e, "begin capture");
+  KernelProbe* pr = c->probeName.empty() ? nullptr : s.probe;
+  if (pr) pr->used = 0;
+  tProbe = pr;
+  cudaError_t le = runChain(c->des, s.ws, n, s.stream);
+  if (le == cudaSuccess) {
+    launchPack(s.ws, n, s.dRes, s.stream);
+    le = cudaGetLastError();
+  }
+  tProbe = nullptr;
+  s.probeUsed[n] = pr ? pr->used : 0;
+  e = cudaStreamEndCapture(s.stream, &g);
+  if (le != cudaSuccess || e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return cudaFail(c, le != cudaSuccess ? le : e, "graph capture");
+  }
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cudaFail(c, e, "graph instantiate");
+  return PG_OK;
+}
+
 template <typename T>
 int copyOut(pg_ctx* c, Slot& s, const T* src, size_t n, void* dst, size_t cap, size_t* count, int* elem) {
   *elem = int(sizeof(T));
@@ -255,6 +255,45 @@ int copyOut(pg_ctx* c, Slot& s, const T* src, size_t n, void* dst, size_t cap, s
 
 }  // namespace
 
+int pixgpu::captureGraphFor(pg_ctx* c, Slot& s, uint32_t n) {
+  if (s.graphs.count(n)) return PG_OK;
+  cudaGraphExec_t g = nullptr;
+  int rc = captureGraph(c, s, n, &g);
+  if (rc != PG_OK) return rc;
+  s.graphs.emplace(n, g);
+  return PG_OK;
+}
+
+int pixgpu::launchBatch(pg_ctx* c, Slot& s) {
+  cudaError_t e;
+  if (c->cfg.use_graphs) {
+    int rc = captureGraphFor(c, s, s.nEvents);
+    if (rc != PG_OK) return rc;
+    s.lastProbeUsed = s.probeUsed[s.nEvents];
+    e = cudaGraphLaunch(s.graphs[s.nEvents], s.stream);
+    if (e != cudaSuccess) return cudaFail(c, e, "graph launch");
+  } else {
+    KernelProbe* pr = c->probeName.empty() ? nullptr : s.probe;
+    if (pr) pr->used = 0;
+    tProbe = pr;
+    e = runChain(c->des, s.ws, s.nEvents, s.stream);
+    if (e == cudaSuccess) launchPack(s.ws, s.nEvents, s.dRes, s.stream);
+    tProbe = nullptr;
+    s.lastProbeUsed = pr ? pr->used : 0;
+    if (e != cudaSuccess) return cudaFail(c, e, "chain launch");
+  }
+  e = cudaEventRecord(s.done, s.stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return cudaFail(c, e, "chain launch");
+  return PG_OK;
+}
+
+int pixgpu::findFreeSlot(pg_ctx* c) {
+  for (size_t i = 0; i < c->slots.size(); ++i)
+    if (c->slots[i].state == SlotState::kFree) return int(i);
+  return -1;
+}
+
 extern "C" {
 
 void pg_default_config(pg_config* cfg) {
@@ -262,7 +301,58 @@ void pg_default_config(pg_config* cfg) {
   cfg->max_events = 64;
   cfg->max_words_per_batch = 64u * 160000u;
   cfg->slots = 1;
+  cfg->use_graphs = 1;
+  cfg->pool_words = 0;
+  cfg->hbm_fraction = 0.5;
 }
+
+namespace {
+
+int createSlot(pg_ctx* c, Slot& s, size_t bytes) {
+  const uint32_t E = c->cfg.max_events;
+  if (cudaMalloc(&s.dmem, bytes) != cudaSuccess) return fail(c, PG_ERR_NOMEM, "slot workspace");
+  workspaceCarve(s.ws, s.dmem, E, c->cfg.max_words_per_batch);
+  if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s.gathered, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMallocHost(&s.hWords, size_t(c->cfg.max_words_per_batch) * 4) != cudaSuccess ||
+      cudaMallocHost(&s.hFed, size_t(c->cfg.max_words_per_batch) / 2 + 16) != cudaSuccess ||
+      cudaMallocHost(&s.hOffsets, size_t(E + 1) * 4) != cudaSuccess ||
+      cudaMallocHost(&s.hRefs, size_t(E) * sizeof(PoolRef)) != cudaSuccess ||
+      cudaMalloc(&s.dRefs, size_t(E) * sizeof(PoolRef)) != cudaSuccess ||
+      cudaHostAlloc(&s.hRes, size_t(E) * kResultStride, cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer(reinterpret_cast<void**>(&s.dRes), s.hRes, 0) != cudaSuccess)
+    return fail(c, PG_ERR_NOMEM, "slot stream, events or pinned buffers");
+  // the kernels read the batch input through this descriptor
+  launchSetInput(s.ws, s.ws.words, s.ws.fedIds, s.stream);
+  cudaError_t e = cudaStreamSynchronize(s.stream);
+  if (e != cudaSuccess) return cudaFail(c, e, "slot set-up");
+  return PG_OK;
+}
+
+void destroySlot(Slot& s) {
+  if (s.stream) cudaStreamSynchronize(s.stream);
+  for (auto& g : s.graphs) cudaGraphExecDestroy(g.second);
+  s.graphs.clear();
+  if (s.probe) {
+    for (auto& ev : s.probe->ev)
+      if (ev) cudaEventDestroy(ev);
+    delete s.probe;
+    s.probe = nullptr;
+  }
+  if (s.dmem) cudaFree(s.dmem);
+  if (s.dRefs) cudaFree(s.dRefs);
+  if (s.done) cudaEventDestroy(s.done);
+  if (s.gathered) cudaEventDestroy(s.gathered);
+  if (s.stream) cudaStreamDestroy(s.stream);
+  if (s.hWords) cudaFreeHost(s.hWords);
+  if (s.hFed) cudaFreeHost(s.hFed);
+  if (s.hOffsets) cudaFreeHost(s.hOffsets);
+  if (s.hRefs) cudaFreeHost(s.hRefs);
+  if (s.hRes) cudaFreeHost(s.hRes);
+}
+
+}  // namespace
 
 int pg_create(const pg_es_images* es, const pg_config* cfgIn, pg_ctx** out) {
   if (!es || !out) return PG_ERR_ARG;
@@ -272,7 +362,9 @@ int pg_create(const pg_es_images* es, const pg_config* cfgIn, pg_ctx** out) {
     c->cfg = *cfgIn;
   else
     pg_default_config(&c->cfg);
-  if (c->cfg.max_events == 0 || c->cfg.slots == 0 || c->cfg.max_words_per_batch == 0) return PG_ERR_ARG;
+  if (c->cfg.max_events == 0 || c->cfg.max_words_per_batch == 0 || c->cfg.max_words_per_batch > (1u << 30))
+    return PG_ERR_ARG;
+  c->device = c->cfg.device;
   cudaError_t e = cudaSetDevice(c->cfg.device);
   if (e != cudaSuccess) return PG_ERR_CUDA;
   int rc = uploadES(c.get(), es);
@@ -280,20 +372,33 @@ int pg_create(const pg_es_images* es, const pg_config* cfgIn, pg_ctx** out) {
     if (c->esMem) cudaFree(c->esMem);
     return rc;
   }
-  size_t bytes = workspaceBytes(c->cfg.max_events, c->cfg.max_words_per_batch);
-  c->slots.resize(c->cfg.slots);
-  for (auto& s : c->slots) {
-    if ((e = cudaMalloc(&s.dmem, bytes)) != cudaSuccess) {
+  if (c->cfg.pool_words) {
+    rc = poolCreate(c.get(), c->cfg.pool_words);
+    if (rc != PG_OK) {
       pg_destroy(c.release());
-      return PG_ERR_NOMEM;
+      return rc;
     }
-    workspaceCarve(s.ws, s.dmem, c->cfg.max_events, c->cfg.max_words_per_batch);
-    if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMallocHost(&s.hWords, size_t(c->cfg.max_words_per_batch) * 4) != cudaSuccess ||
-        cudaMallocHost(&s.hFed, size_t(c->cfg.max_words_per_batch) / 2 + 16) != cudaSuccess ||
-        cudaMallocHost(&s.hOffsets, size_t(c->cfg.max_events + 1) * 4) != cudaSuccess) {
+  }
+  size_t bytes = workspaceBytes(c->cfg.max_events, c->cfg.max_words_per_batch);
+  uint32_t nSlots = c->cfg.slots;
+  if (nSlots == 0) {
+    // admission by free HBM: as many slots as fit in the given share of the free memory
+    size_t freeB = 0, totalB = 0;
+    if ((e = cudaMemGetInfo(&freeB, &totalB)) != cudaSuccess) {
       pg_destroy(c.release());
-      return PG_ERR_NOMEM;
+      return PG_ERR_CUDA;
+    }
+    double frac = c->cfg.hbm_fraction > 0 && c->cfg.hbm_fraction <= 0.95 ? c->cfg.hbm_fraction : 0.5;
+    size_t fit = size_t(double(freeB) * frac) / bytes;
+    nSlots = uint32_t(std::min<size_t>(std::max<size_t>(fit, 1), 16));
+    c->cfg.slots = nSlots;
+  }
+  c->slots.resize(nSlots);
+  for (auto& s : c->slots) {
+    if ((rc = createSlot(c.get(), s, bytes)) != PG_OK) {
+      std::string msg = c->err;
+      pg_destroy(c.release());
+      return rc;
     }
   }
   *out = c.release();
@@ -303,16 +408,16 @@ int pg_create(const pg_es_images* es, const pg_config* cfgIn, pg_ctx** out) {
 void pg_destroy(pg_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->cfg.device);
-  for (auto& s : c->slots) {
-    if (s.stream) cudaStreamSynchronize(s.stream);
-    if (s.dmem) cudaFree(s.dmem);
-    if (s.stream) cudaStreamDestroy(s.stream);
-    if (s.hWords) cudaFreeHost(s.hWords);
-    if (s.hFed) cudaFreeHost(s.hFed);
-    if (s.hOffsets) cudaFreeHost(s.hOffsets);
-  }
+  for (auto& s : c->slots) destroySlot(s);
+  poolDestroy(c);
   if (c->esMem) cudaFree(c->esMem);
   delete c;
+}
+
+int pg_get_config(const pg_ctx* c, pg_config* out) {
+  if (!c || !out) return PG_ERR_ARG;
+  *out = c->cfg;
+  return PG_OK;
 }
 
 const char* pg_last_error(const pg_ctx* c) { return c ? c->err.c_str() : "null context"; }
@@ -329,16 +434,14 @@ int pg_unpack_raw(const pg_ctx* c, const uint8_t* raw, size_t n, uint32_t* words
 
 int pg_stage_batch(pg_ctx* c, uint32_t slot, uint32_t nEvents, const uint8_t* const* raws, const size_t* sizes) {
   if (!c || slot >= c->slots.size() || !raws || !sizes) return PG_ERR_ARG;
+  if (c->slots[slot].state != SlotState::kFree) return fail(c, PG_ERR_BUSY, "slot holds an asynchronous batch");
   cudaSetDevice(c->cfg.device);
   return stage(c, c->slots[slot], nEvents, raws, sizes);
 }
 
 int pg_run_staged(pg_ctx* c, uint32_t slot) {
   if (!c || slot >= c->slots.size() || !c->slots[slot].staged) return PG_ERR_ARG;
-  Slot& s = c->slots[slot];
-  cudaError_t e = runChain(c->des, s.ws, s.nEvents, s.stream);
-  if (e != cudaSuccess) return cudaFail(c, e, "chain launch");
-  return PG_OK;
+  return launchBatch(c, c->slots[slot]);
 }
 
 int pg_sync(pg_ctx* c, uint32_t slot) {
@@ -480,6 +583,163 @@ int pg_get_product(pg_ctx* c, uint32_t k, const char* name, void* dst, size_t ca
   if (n == "sortInd") return copyOut(c, s, ws.sortInd + vb, ec.nVertices, dst, cap, count, elem);
   if (n == "idv") return copyOut(c, s, ws.idv + tb, nTup, dst, cap, count, elem);
   return fail(c, PG_ERR_NOTFOUND, "unknown product " + n);
+}
+
+int pg_submit(pg_ctx* c, uint32_t nEvents, const uint8_t* const* raws, const size_t* sizes, uint32_t* slotOut) {
+  if (!c || !raws || !sizes || !slotOut) return PG_ERR_ARG;
+  cudaSetDevice(c->cfg.device);
+  int k;
+  {
+    std::lock_guard<std::mutex> lk(c->mu);
+    k = findFreeSlot(c);
+    if (k < 0) return fail(c, PG_ERR_BUSY, "no free slot");
+    c->slots[k].state = SlotState::kBusy;
+  }
+  Slot& s = c->slots[k];
+  int rc = stage(c, s, nEvents, raws, sizes);
+  if (rc == PG_OK) rc = launchBatch(c, s);
+  if (rc != PG_OK) {
+    cudaStreamSynchronize(s.stream);
+    s.state = SlotState::kFree;
+    return rc;
+  }
+  *slotOut = uint32_t(k);
+  return PG_OK;
+}
+
+int pg_query(pg_ctx* c, uint32_t slot) {
+  if (!c || slot >= c->slots.size() || c->slots[slot].state != SlotState::kBusy) return PG_ERR_ARG;
+  cudaError_t e = cudaEventQuery(c->slots[slot].done);
+  if (e == cudaErrorNotReady) return PG_ERR_BUSY;
+  if (e != cudaSuccess) return cudaFail(c, e, "batch");
+  return PG_OK;
+}
+
+int pg_wait(pg_ctx* c, uint32_t slot) {
+  if (!c || slot >= c->slots.size() || c->slots[slot].state != SlotState::kBusy) return PG_ERR_ARG;
+  cudaError_t e = cudaEventSynchronize(c->slots[slot].done);
+  if (e != cudaSuccess) return cudaFail(c, e, "batch");
+  return PG_OK;
+}
+
+int pg_result(pg_ctx* c, uint32_t slot, uint32_t k, pg_result_view* v) {
+  if (!c || !v || slot >= c->slots.size()) return PG_ERR_ARG;
+  Slot& s = c->slots[slot];
+  if (s.state != SlotState::kBusy || k >= s.nEvents) return PG_ERR_ARG;
+  if (cudaEventQuery(s.done) != cudaSuccess) return fail(c, PG_ERR_BUSY, "batch not finished");
+  uint8_t* base = s.hRes + size_t(k) * kResultStride;
+  const ResultHeader* h = reinterpret_cast<const ResultHeader*>(base);
+  ResultTracks t = resultTracks(base);
+  ResultVertices vx = resultVertices(base);
+  v->n_tracks = h->nTracks;
+  v->n_loose_all = h->nLooseAll;
+  v->n_vertices = h->nVertices;
+  v->n_hits = h->nHits;
+  v->n_tuples = h->nTuples;
+  v->n_digis = h->nDigis;
+  v->n_cells = h->nCells;
+  v->flags = h->flags;
+  v->tuple_index = t.tupleIndex;
+  v->track_n_hits = t.nHits;
+  v->quality = t.quality;
+  v->state = t.state;
+  v->cov = t.cov;
+  v->pt = t.pt;
+  v->eta = t.eta;
+  v->chi2 = t.chi2;
+  v->hits = t.hits;
+  v->vertex = t.vertex;
+  v->zv = vx.zv;
+  v->wv = vx.wv;
+  v->vchi2 = vx.chi2;
+  v->ptv2 = vx.ptv2;
+  v->ndof = vx.ndof;
+  v->sort_ind = vx.sortInd;
+  return PG_OK;
+}
+
+int pg_batch_summary_get(pg_ctx* c, uint32_t slot, pg_batch_summary* out) {
+  if (!c || !out || slot >= c->slots.size()) return PG_ERR_ARG;
+  Slot& s = c->slots[slot];
+  if (s.state != SlotState::kBusy) return PG_ERR_ARG;
+  if (cudaEventQuery(s.done) != cudaSuccess) return fail(c, PG_ERR_BUSY, "batch not finished");
+  *out = pg_batch_summary{};
+  out->n_events = s.nEvents;
+  for (uint32_t k = 0; k < s.nEvents; ++k) {
+    const ResultHeader* h = reinterpret_cast<const ResultHeader*>(s.hRes + size_t(k) * kResultStride);
+    out->flags |= h->flags;
+    out->n_tracks += h->nTracks;
+    out->n_vertices += h->nVertices;
+    out->result_bytes += sizeof(ResultHeader) + h->nTracks * kResultTrackBytes + h->nVertices * kResultVertexBytes;
+    out->n_digis += h->nDigis;
+    out->n_modules += h->nModules;
+    out->n_hits += h->nHits;
+    out->n_cells += h->nCells;
+    out->n_edges += h->nEdges;
+    out->n_tuples += h->nTuples;
+    out->n_tuple_hits += h->nTupleHits;
+  }
+  return PG_OK;
+}
+
+int pg_release(pg_ctx* c, uint32_t slot) {
+  if (!c || slot >= c->slots.size()) return PG_ERR_ARG;
+  Slot& s = c->slots[slot];
+  if (s.state != SlotState::kBusy) return PG_ERR_ARG;
+  cudaError_t e = cudaEventSynchronize(s.done);
+  poolReclaimSlot(c, s);
+  std::lock_guard<std::mutex> lk(c->mu);
+  s.state = SlotState::kFree;
+  if (e != cudaSuccess) return cudaFail(c, e, "batch");
+  return PG_OK;
+}
+
+int pg_set_probe(pg_ctx* c, const char* kernel) {
+  if (!c) return PG_ERR_ARG;
+  std::lock_guard<std::mutex> lk(c->mu);
+  for (auto& s : c->slots)
+    if (s.state != SlotState::kFree) return fail(c, PG_ERR_BUSY, "pg_set_probe needs every slot free");
+  std::string name = kernel ? kernel : "";
+  if (name.size() >= sizeof(KernelProbe::name)) return fail(c, PG_ERR_ARG, "kernel name too long");
+  cudaSetDevice(c->cfg.device);
+  for (auto& s : c->slots) {
+    cudaStreamSynchronize(s.stream);
+    for (auto& g : s.graphs) cudaGraphExecDestroy(g.second);
+    s.graphs.clear();
+    s.probeUsed.clear();
+    s.lastProbeUsed = 0;
+    if (!name.empty() && !s.probe) {
+      s.probe = new KernelProbe();
+      std::memset(s.probe, 0, sizeof(KernelProbe));
+      for (auto& ev : s.probe->ev)
+        if (cudaEventCreate(&ev) != cudaSuccess) return fail(c, PG_ERR_CUDA, "probe events");
+    }
+    if (s.probe) std::snprintf(s.probe->name, sizeof(s.probe->name), "%s", name.c_str());
+  }
+  c->probeName = name;
+  return PG_OK;
+}
+
+int pg_probe_read(pg_ctx* c, uint32_t slot, uint32_t max, pg_probe_entry* out, uint32_t* n) {
+  if (!c || !n || slot >= c->slots.size()) return PG_ERR_ARG;
+  Slot& s = c->slots[slot];
+  *n = 0;
+  if (c->probeName.empty() || !s.probe) return PG_OK;
+  cudaError_t e = cudaEventQuery(s.done);
+  if (e == cudaErrorNotReady) return fail(c, PG_ERR_BUSY, "batch not finished");
+  if (e != cudaSuccess) return cudaFail(c, e, "batch");
+  uint32_t k = std::min(s.lastProbeUsed, max);
+  for (uint32_t i = 0; i < k; ++i) {
+    float ms = 0;
+    e = cudaEventElapsedTime(&ms, s.probe->ev[2 * i], s.probe->ev[2 * i + 1]);
+    if (e != cudaSuccess) return cudaFail(c, e, "probe elapsed time");
+    if (out) {
+      out[i].kernel = s.probe->launched[i];
+      out[i].ms = ms;
+    }
+  }
+  *n = k;
+  return PG_OK;
 }
 
 int pg_fit_broken_line(pg_ctx* c, int N, uint32_t n, const double* hits, const float* ge, double B, float* state,

@@ -1,5 +1,6 @@
 // Batch workspace layout and the launch sequence of the whole chain.
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 #include "pixgpu_internal.cuh"
@@ -25,6 +26,7 @@ void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W) {
   c.take(ws.words, W);
   c.take(ws.fedIds, W / 2 + 2);
   c.take(ws.wordOffsets, E + 1);
+  c.take(ws.input, 1);
   c.take(ws.ev, E);
   c.take(ws.xx, W);
   c.take(ws.yy, W);
@@ -110,7 +112,32 @@ void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W) {
   c.take(ws.scanTmp, size_t(E + 1) * kScanTmpStride);
 }
 
+// the pair opened by probeBegin when its name matched (-1: none).  Records use
+// cudaEventRecordExternal so that under stream capture they become event
+// record nodes of the graph rather than capture-internal dependencies.
+thread_local int tProbeOpen = -1;
+
 }  // namespace
+
+thread_local KernelProbe* tProbe = nullptr;
+
+void probeBegin(const char* name, cudaStream_t s) {
+  tProbeOpen = -1;
+  KernelProbe* p = tProbe;
+  if (!p || p->used >= kProbeMax) return;
+  if (!(p->name[0] == '*' && p->name[1] == 0) && std::strcmp(p->name, name) != 0) return;
+  tProbeOpen = int(p->used);
+  p->launched[p->used] = name;
+  cudaEventRecordWithFlags(p->ev[2 * p->used], s, cudaEventRecordExternal);
+}
+
+void probeEnd(cudaStream_t s) {
+  KernelProbe* p = tProbe;
+  if (!p || tProbeOpen < 0) return;
+  cudaEventRecordWithFlags(p->ev[2 * tProbeOpen + 1], s, cudaEventRecordExternal);
+  p->used = uint32_t(tProbeOpen) + 1;
+  tProbeOpen = -1;
+}
 
 size_t workspaceBytes(uint32_t maxEvents, uint32_t wordCap) {
   Workspace ws;

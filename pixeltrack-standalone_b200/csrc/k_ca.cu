@@ -873,79 +873,79 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   const uint32_t gx = nEvents >= 32 ? 16 : (nEvents >= 8 ? 64 : 296);  // blocks per event for flat loops
   dim3 g(gx, nEvents);
   // ---- doublets: count per inner-hit slot, scan, write in serial order
-  kDoubletSetup<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents);
-  kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.ohCount, kHitCap + 1, kHitCap + 1, nullptr, 0);
-  kDoubletCount<<<g, 128, 0, stream>>>(ws);
+  PG_PROBED("kDoubletSetup", stream, kDoubletSetup<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents));
+  PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.ohCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
+  PG_PROBED("kDoubletCount", stream, kDoubletCount<<<g, 128, 0, stream>>>(ws));
   segScan(ws.jCount, ws.jOffset, kJCap + 1, EVF(ntot), kJCap, nullptr, 0, ws.scanTmp, nEvents, stream);
-  kDoubletWrite<<<g, 128, 0, stream>>>(ws);
-  kCellsTotal<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents);
+  PG_PROBED("kDoubletWrite", stream, kDoubletWrite<<<g, 128, 0, stream>>>(ws));
+  PG_PROBED("kCellsTotal", stream, kCellsTotal<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents));
   // ---- isOuterHitOfCell: scan of the per-hit counts, unordered fill, order per hit
   segScan(ws.ohCount, ws.ohOff, kHitCap + 1, EVF(nHits), kHitCap, nullptr, 0, ws.scanTmp, nEvents, stream);
-  kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.ohCount, kHitCap + 1, kHitCap + 1, nullptr, 0);
-  kOuterHitFill<<<g, 256, 0, stream>>>(ws);
-  kSortSegments<uint32_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.ohCells, kCellCap, ws.ohOff, kHitCap + 1,
-                                                                     EVF(nHits), 0, false, kCellCap);
+  PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.ohCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
+  PG_PROBED("kOuterHitFill", stream, kOuterHitFill<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kSortSegments", stream, kSortSegments<uint32_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.ohCells, kCellCap, ws.ohOff, kHitCap + 1,
+                                                                     EVF(nHits), 0, false, kCellCap));
   // ---- CA links: edges appended unordered, then CSR by inner cell, ordered ascending
-  kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbrCount, kCellCap + 1, kCellCap + 1, EVF(nCells));
-  kConnect<<<g, 128, 0, stream>>>(ws, ws.scratchA, ws.scratchB);
+  PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbrCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
+  PG_PROBED("kConnect", stream, kConnect<<<g, 128, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
   segScan(ws.nbrCount, ws.nbrOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanTmp, nEvents, stream);
-  kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbrCount, kCellCap + 1, kCellCap + 1, EVF(nCells));
-  kEdgeScatter<<<g, 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB);
-  kSortSegments<uint32_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbr, kEdgeCap, ws.nbrOff, kCellCap + 1,
-                                                                     EVF(nCells), 0, false, kEdgeCap);
-  kNbrPool<<<g, 256, 0, stream>>>(ws);
+  PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbrCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
+  PG_PROBED("kEdgeScatter", stream, kEdgeScatter<<<g, 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
+  PG_PROBED("kSortSegments", stream, kSortSegments<uint32_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbr, kEdgeCap, ws.nbrOff, kCellCap + 1,
+                                                                     EVF(nCells), 0, false, kEdgeCap));
+  PG_PROBED("kNbrPool", stream, kNbrPool<<<g, 256, 0, stream>>>(ws));
   // ---- early fishbone
-  kFishbone<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws);
+  PG_PROBED("kFishbone", stream, kFishbone<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws));
   // ---- n-tuplets: DFS count, scans, DFS write, finalize
-  kNtupletCount<<<g, 128, 0, stream>>>(ws);
+  PG_PROBED("kNtupletCount", stream, kNtupletCount<<<g, 128, 0, stream>>>(ws));
   segScan(ws.startTupleCount, ws.startTupleOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcM), ws.scanTmp, nEvents,
           stream);
   segScan(ws.startHitCount, ws.startHitOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcN), ws.scanTmp, nEvents,
           stream);
-  kNtupletWrite<<<g, 128, 0, stream>>>(ws);
-  kTupleFinalize<<<dim3(32, nEvents), 1024, 0, stream>>>(ws);
+  PG_PROBED("kNtupletWrite", stream, kNtupletWrite<<<g, 128, 0, stream>>>(ws));
+  PG_PROBED("kTupleFinalize", stream, kTupleFinalize<<<dim3(32, nEvents), 1024, 0, stream>>>(ws));
   // ---- cell -> track lists
-  kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trkCount, kCellCap + 1, kCellCap + 1, EVF(nCells));
-  kTrackCount<<<g, 256, 0, stream>>>(ws);
+  PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trkCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
+  PG_PROBED("kTrackCount", stream, kTrackCount<<<g, 256, 0, stream>>>(ws));
   segScan(ws.trkCount, ws.trkOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanTmp, nEvents, stream);
-  kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trkCount, kCellCap + 1, kCellCap + 1, EVF(nCells));
-  kTrackFill<<<g, 256, 0, stream>>>(ws);
-  kSortSegments<uint16_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trk, kTupleCellCap, ws.trkOff, kCellCap + 1,
-                                                                     EVF(nCells), 0, false, kTupleCellCap);
+  PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trkCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
+  PG_PROBED("kTrackFill", stream, kTrackFill<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kSortSegments", stream, kSortSegments<uint16_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trk, kTupleCellCap, ws.trkOff, kCellCap + 1,
+                                                                     EVF(nCells), 0, false, kTupleCellCap));
   uint32_t* candFlag = ws.startTupleCount;  // scratch
   uint32_t* candOff = ws.startHitCount;
-  kTrackPool<<<g, 256, 0, stream>>>(ws, candFlag);
+  PG_PROBED("kTrackPool", stream, kTrackPool<<<g, 256, 0, stream>>>(ws, candFlag));
   segScan(candFlag, candOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(nCandidates), ws.scanTmp, nEvents, stream);
-  kCandidateScatter<<<g, 256, 0, stream>>>(ws, candFlag, candOff);
-  kEarlyDup<<<g, 256, 0, stream>>>(ws);
-  kTupleDet<<<g, 256, 0, stream>>>(ws);
+  PG_PROBED("kCandidateScatter", stream, kCandidateScatter<<<g, 256, 0, stream>>>(ws, candFlag, candOff));
+  PG_PROBED("kEarlyDup", stream, kEarlyDup<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kTupleDet", stream, kTupleDet<<<g, 256, 0, stream>>>(ws));
   // ---- tuple multiplicity for the fits
-  kZero<<<dim3(1, nEvents), 32, 0, stream>>>(ws.tmOff, 16, 16, nullptr, 0);
-  kMultiplicityCount<<<g, 256, 0, stream>>>(ws);
-  kMultiplicityScan<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents);
-  kMultiplicityFill<<<g, 256, 0, stream>>>(ws);
+  PG_PROBED("kZero", stream, kZero<<<dim3(1, nEvents), 32, 0, stream>>>(ws.tmOff, 16, 16, nullptr, 0));
+  PG_PROBED("kMultiplicityCount", stream, kMultiplicityCount<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kMultiplicityScan", stream, kMultiplicityScan<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents));
+  PG_PROBED("kMultiplicityFill", stream, kMultiplicityFill<<<g, 256, 0, stream>>>(ws));
   return cudaGetLastError();
 }
 
 cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   const uint32_t gx = nEvents >= 32 ? 16 : (nEvents >= 8 ? 64 : 296);
   dim3 g(gx, nEvents);
-  kClassify<<<g, 256, 0, stream>>>(ws);
+  PG_PROBED("kClassify", stream, kClassify<<<g, 256, 0, stream>>>(ws));
   // fastDuplicateRemover (candFlag survives in startTupleCount from runCA)
   uint32_t* candFlag = ws.startTupleCount;
   uint32_t* indeg = ws.scratchA;                                 // [maxEvents][kEdgeCap] >= kCellCap
   uint8_t* state = reinterpret_cast<uint8_t*>(ws.scratchB);
-  kFastDupInDegree<<<g, 256, 0, stream>>>(ws, indeg, candFlag);
-  kFastDupRounds<<<nEvents, kFastDupThreads, 0, stream>>>(ws, indeg, state, candFlag);
+  PG_PROBED("kFastDupInDegree", stream, kFastDupInDegree<<<g, 256, 0, stream>>>(ws, indeg, candFlag));
+  PG_PROBED("kFastDupRounds", stream, kFastDupRounds<<<nEvents, kFastDupThreads, 0, stream>>>(ws, indeg, state, candFlag));
   // hit -> tuple map and triplet cleaner
-  kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, nullptr, 0);
-  kHitToTupleCount<<<g, 256, 0, stream>>>(ws);
+  PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
+  PG_PROBED("kHitToTupleCount", stream, kHitToTupleCount<<<g, 256, 0, stream>>>(ws));
   segScan(ws.h2tCount, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, nullptr, 0, ws.scanTmp, nEvents, stream);
-  kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, nullptr, 0);
-  kHitToTupleFill<<<g, 256, 0, stream>>>(ws);
-  kSortSegments<uint16_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.h2t, kH2TCap, ws.h2tOff, kHitCap + 1,
-                                                                     nullptr, 0, kHitCap, true, kH2TCap);
-  kTripletCleaner<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws);
+  PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
+  PG_PROBED("kHitToTupleFill", stream, kHitToTupleFill<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kSortSegments", stream, kSortSegments<uint16_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.h2t, kH2TCap, ws.h2tOff, kHitCap + 1,
+                                                                     nullptr, 0, kHitCap, true, kH2TCap));
+  PG_PROBED("kTripletCleaner", stream, kTripletCleaner<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws));
   return cudaGetLastError();
 }
 

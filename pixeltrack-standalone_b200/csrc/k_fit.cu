@@ -587,10 +587,10 @@ __global__ void kBLFitDirect(uint32_t n, const double* hits, const float* hge, d
 cudaError_t runFits(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   const uint32_t gx = nEvents >= 32 ? 8 : (nEvents >= 8 ? 32 : 148);
   dim3 g(gx, nEvents);
-  kFitZero<<<g, 256, 0, stream>>>(ws);
-  kBLFit<3><<<g, 64, 0, stream>>>(es, ws, 3);
-  kBLFit<4><<<g, 64, 0, stream>>>(es, ws, 4);
-  kBLFit<4><<<g, 64, 0, stream>>>(es, ws, 5);
+  PG_PROBED("kFitZero", stream, kFitZero<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kBLFit", stream, kBLFit<3><<<g, 64, 0, stream>>>(es, ws, 3));
+  PG_PROBED("kBLFit", stream, kBLFit<4><<<g, 64, 0, stream>>>(es, ws, 4));
+  PG_PROBED("kBLFit", stream, kBLFit<4><<<g, 64, 0, stream>>>(es, ws, 5));
   return cudaGetLastError();
 }
 
@@ -600,9 +600,9 @@ cudaError_t fitDirect(int N, uint32_t n, const double* hits, const float* ge, do
   if (blocks > 148 * 16) blocks = 148 * 16;
   if (blocks == 0) return cudaSuccess;
   if (N == 3)
-    kBLFitDirect<3><<<blocks, 128, 0, stream>>>(n, hits, ge, B, state, cov, pt, eta, chi2);
+    PG_PROBED("kBLFitDirect", stream, kBLFitDirect<3><<<blocks, 128, 0, stream>>>(n, hits, ge, B, state, cov, pt, eta, chi2));
   else
-    kBLFitDirect<4><<<blocks, 128, 0, stream>>>(n, hits, ge, B, state, cov, pt, eta, chi2);
+    PG_PROBED("kBLFitDirect", stream, kBLFitDirect<4><<<blocks, 128, 0, stream>>>(n, hits, ge, B, state, cov, pt, eta, chi2));
   return cudaGetLastError();
 }
 

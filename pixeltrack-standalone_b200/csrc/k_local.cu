@@ -195,14 +195,16 @@ __global__ void kRawToDigi(DeviceES es, Workspace ws, uint32_t nEvents) {
   const uint32_t total = ws.wordOffsets[nEvents];
   const PfCablingMap* cab = es.cab;
   const PfGainHeader* gh = es.gainHdr;
+  const uint32_t* words = ws.input->words;
+  const uint8_t* fedIds = ws.input->fedIds;
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
     uint32_t e = eventOfWord(ws.wordOffsets, nEvents, g);
     uint32_t start = ws.wordOffsets[e];
     uint32_t i = g - start;
-    uint8_t fedId = ws.fedIds[g >> 1];
+    uint8_t fedId = fedIds[g >> 1];
     uint16_t xx = 0, yy = 0, adc = 0, mid = 9999;
     uint32_t pdigi = 0, rawIdOut = 0;
-    uint32_t ww = ws.words[g];
+    uint32_t ww = words[g];
     bool err = false;
     PfPixelError perr;
     if (ww != 0) {
@@ -401,7 +403,10 @@ __global__ void __launch_bounds__(kClusThreads) kFindClusters(Workspace ws) {
   const uint32_t firstPixel = ms[1 + module];
   uint32_t msize = (module + 1 < nModules) ? ms[2 + module] : nW;
   const uint16_t thisModuleId = ws.moduleInd[start + firstPixel];
-  if (thisModuleId >= kMaxModules) return;
+  if (thisModuleId >= kMaxModules) {
+    if (threadIdx.x == 0) ws.moduleId[size_t(e) * kModStride + module] = 0xffffffffu;
+    return;
+  }
   if (msize - firstPixel > PF_MAX_PIX_IN_MODULE) {
     if (threadIdx.x == 0) atomicOr(&ws.ev[e].flags, kFlagModuleTooBig);
     msize = firstPixel + PF_MAX_PIX_IN_MODULE;
@@ -621,7 +626,7 @@ __global__ void __launch_bounds__(kHitThreads) kGetHits(DeviceES es, Workspace w
   const uint32_t* ms = ws.moduleStart + size_t(e) * kModStride;
   const uint32_t first = ms[1 + module];
   const uint32_t last = (module + 1 < nModules) ? ms[2 + module] : nW;
-  if (ws.moduleInd[start + first] != me || me >= es.nDet) return;
+  if (me >= es.nDet) return;  // runs the clustering rejected carry no valid module id
   const PfDetParams& dp = es.det[me];
   const PfCommonParams& cp = *es.common;
   const PfBeamSpot& bs = *es.bs;
@@ -814,24 +819,24 @@ __global__ void kSortErrors(Workspace ws) {
 }  // namespace
 
 cudaError_t runLocal(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
-  kInitEvents<<<nEvents, 256, 0, stream>>>(ws, nEvents);
+  PG_PROBED("kInitEvents", stream, kInitEvents<<<nEvents, 256, 0, stream>>>(ws, nEvents));
   const int flatBlocks = 148 * 8;
-  kRawToDigi<<<flatBlocks, 256, 0, stream>>>(es, ws, nEvents);
-  kModuleBoundaries<<<flatBlocks, 256, 0, stream>>>(ws, nEvents);
-  kSortModules<<<nEvents, 1024, 0, stream>>>(ws, nEvents);
-  kSortErrors<<<nEvents, 32, 0, stream>>>(ws);
-  kFindClusters<<<dim3(kMaxModules, nEvents), kClusThreads, 0, stream>>>(ws);
-  kHitsModuleStart<<<nEvents, 1024, 0, stream>>>(es, ws);
-  kGetHits<<<dim3(kMaxModules, nEvents), kHitThreads, 0, stream>>>(es, ws);
+  PG_PROBED("kRawToDigi", stream, kRawToDigi<<<flatBlocks, 256, 0, stream>>>(es, ws, nEvents));
+  PG_PROBED("kModuleBoundaries", stream, kModuleBoundaries<<<flatBlocks, 256, 0, stream>>>(ws, nEvents));
+  PG_PROBED("kSortModules", stream, kSortModules<<<nEvents, 1024, 0, stream>>>(ws, nEvents));
+  PG_PROBED("kSortErrors", stream, kSortErrors<<<nEvents, 32, 0, stream>>>(ws));
+  PG_PROBED("kFindClusters", stream, kFindClusters<<<dim3(kMaxModules, nEvents), kClusThreads, 0, stream>>>(ws));
+  PG_PROBED("kHitsModuleStart", stream, kHitsModuleStart<<<nEvents, 1024, 0, stream>>>(es, ws));
+  PG_PROBED("kGetHits", stream, kGetHits<<<dim3(kMaxModules, nEvents), kHitThreads, 0, stream>>>(es, ws));
   // phi histogram: count, exclusive scan, unordered fill, per-bin ordering
   uint32_t* cursor = ws.jCount;  // scratch: the doublet counters are not in use yet
-  kZeroU32<<<dim3(2, nEvents), 1024, 0, stream>>>(ws.phiOff, kPhiStride, kPhiStride, nEvents);
-  kZeroU32<<<dim3(2, nEvents), 1024, 0, stream>>>(cursor, kPhiStride, kPhiStride, nEvents);
-  kPhiCount<<<dim3(16, nEvents), 256, 0, stream>>>(ws);
+  PG_PROBED("kZeroU32", stream, kZeroU32<<<dim3(2, nEvents), 1024, 0, stream>>>(ws.phiOff, kPhiStride, kPhiStride, nEvents));
+  PG_PROBED("kZeroU32", stream, kZeroU32<<<dim3(2, nEvents), 1024, 0, stream>>>(cursor, kPhiStride, kPhiStride, nEvents));
+  PG_PROBED("kPhiCount", stream, kPhiCount<<<dim3(16, nEvents), 256, 0, stream>>>(ws));
   // in place exclusive scan of the 1280 counters; the total lands in the extra bin
   segScan(ws.phiOff, ws.phiOff, kPhiStride, nullptr, 0, kPhiTot - 1, nullptr, 0, ws.scanTmp, nEvents, stream);
-  kPhiFill<<<dim3(16, nEvents), 256, 0, stream>>>(ws, cursor);
-  kPhiSort<<<dim3((kPhiTot - 1 + 7) / 8, nEvents), 256, 0, stream>>>(ws);
+  PG_PROBED("kPhiFill", stream, kPhiFill<<<dim3(16, nEvents), 256, 0, stream>>>(ws, cursor));
+  PG_PROBED("kPhiSort", stream, kPhiSort<<<dim3((kPhiTot - 1 + 7) / 8, nEvents), 256, 0, stream>>>(ws));
   return cudaGetLastError();
 }
 

@@ -437,7 +437,7 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
 }  // namespace
 
 cudaError_t runVertices(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
-  kVertices<<<nEvents, kVtxThreads, 0, stream>>>(ws);
+  PG_PROBED("kVertices", stream, kVertices<<<nEvents, kVtxThreads, 0, stream>>>(ws));
   return cudaGetLastError();
 }
 

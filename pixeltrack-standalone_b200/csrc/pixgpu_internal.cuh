@@ -87,6 +87,14 @@ struct DeviceES {
 };
 
 // ---------------------------------------------------------------- batch workspace
+// where the batch's FED words live (the slot's staging buffer or a slice of
+// the device-resident pool); read by the kernels so that a captured graph
+// does not depend on it
+struct BatchInput {
+  const uint32_t* words;
+  const uint8_t* fedIds;
+};
+
 struct Workspace {
   uint32_t maxEvents;
   uint32_t wordCap;          // words over the whole batch
@@ -94,6 +102,7 @@ struct Workspace {
   uint32_t* words;
   uint8_t* fedIds;
   uint32_t* wordOffsets;     // [maxEvents + 1]
+  BatchInput* input;         // device-resident descriptor of the batch input
   EventCounters* ev;         // [maxEvents]
   // digis (flat, batch word index)
   uint16_t *xx, *yy, *adc, *moduleInd;
@@ -166,6 +175,29 @@ struct Workspace {
 constexpr uint32_t kScanChunk = 4096;
 constexpr uint32_t kScanTmpStride = 1024;
 
+// ---------------------------------------------------------------- kernel timing probe
+// While a probe is installed on the launching host thread, every launch whose
+// kernel name matches (or every launch, for "*") is bracketed by a pair of
+// timing events on its stream.  Under stream capture the event records
+// become graph nodes, so each replay of the graph re-times the kernel.
+constexpr uint32_t kProbeMax = 256;
+struct KernelProbe {
+  char name[64];                 // kernel name, "*" for all
+  cudaEvent_t ev[2 * kProbeMax];
+  const char* launched[kProbeMax];
+  uint32_t used;                 // pairs recorded by the launch sequence
+};
+extern thread_local KernelProbe* tProbe;
+void probeBegin(const char* name, cudaStream_t s);
+void probeEnd(cudaStream_t s);
+#define PG_PROBED(name, stream, ...)                         \
+  do {                                                       \
+    const bool pgProbeOn_ = tProbe != nullptr;               \
+    if (pgProbeOn_) probeBegin(name, stream);                \
+    __VA_ARGS__;                                             \
+    if (pgProbeOn_) probeEnd(stream);                        \
+  } while (0)
+
 // ---------------------------------------------------------------- launch API (host)
 size_t workspaceBytes(uint32_t maxEvents, uint32_t wordCap);
 void workspaceCarve(Workspace& ws, void* base, uint32_t maxEvents, uint32_t wordCap);
@@ -179,6 +211,10 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
 cudaError_t runFits(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream);
 cudaError_t runVertices(Workspace& ws, uint32_t nEvents, cudaStream_t stream);
 cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream);
+
+// batch input descriptor and compact results (k_pack.cu)
+void launchSetInput(Workspace& ws, const uint32_t* words, const uint8_t* fedIds, cudaStream_t s);
+void launchPack(Workspace& ws, uint32_t nEvents, uint8_t* out, cudaStream_t s);
 
 // batched segmented exclusive scan: out[e*stride + i] = sum_{k<i} in[e*stride + k]
 // for i <= n_e, where n_e = lenPtr[e*lenStride] (device) or maxLen when lenPtr is

@@ -81,9 +81,9 @@ void segScan(const uint32_t* in, uint32_t* out, uint32_t stride, const uint32_t*
              cudaStream_t stream) {
   uint32_t nChunks = (maxLen + 1 + kScanChunk - 1) / kScanChunk;
   dim3 g(nChunks, nEvents);
-  scanChunks<<<g, kThreads, 0, stream>>>(in, out, stride, lenPtr, lenStride, maxLen, tmp);
-  scanTotals<<<nEvents, 1024, 0, stream>>>(tmp, lenPtr, lenStride, maxLen, totalPtr, totalStride);
-  scanAdd<<<g, 256, 0, stream>>>(out, stride, lenPtr, lenStride, maxLen, tmp);
+  PG_PROBED("scanChunks", stream, scanChunks<<<g, kThreads, 0, stream>>>(in, out, stride, lenPtr, lenStride, maxLen, tmp));
+  PG_PROBED("scanTotals", stream, scanTotals<<<nEvents, 1024, 0, stream>>>(tmp, lenPtr, lenStride, maxLen, totalPtr, totalStride));
+  PG_PROBED("scanAdd", stream, scanAdd<<<g, 256, 0, stream>>>(out, stride, lenPtr, lenStride, maxLen, tmp));
 }
 
 }  // namespace pixgpu

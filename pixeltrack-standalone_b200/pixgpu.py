@@ -187,7 +187,61 @@ class ESImages(ctypes.Structure):
 
 class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("max_events", ctypes.c_uint32), ("max_words_per_batch", ctypes.c_uint32),
-                ("slots", ctypes.c_uint32)]
+                ("slots", ctypes.c_uint32), ("use_graphs", ctypes.c_uint32), ("pool_words", ctypes.c_uint64),
+                ("hbm_fraction", ctypes.c_double)]
+
+
+class ResultView(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("n_tracks", "n_loose_all", "n_vertices", "n_hits", "n_tuples",
+                                                "n_digis", "n_cells", "flags")] + \
+        [(n, ctypes.c_void_p) for n in ("tuple_index", "track_n_hits", "quality", "state", "cov", "pt", "eta", "chi2",
+                                        "hits", "vertex", "zv", "wv", "vchi2", "ptv2", "ndof", "sort_ind")]
+
+
+class ServeConfig(ctypes.Structure):
+    _fields_ = [("n_requests", ctypes.c_uint32), ("rate_hz", ctypes.c_double), ("seed", ctypes.c_uint64),
+                ("max_batch", ctypes.c_uint32), ("upload_threads", ctypes.c_uint32)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("completed", "batches", "max_batch_seen", "admission_waits")] + \
+        [(n, ctypes.c_double) for n in ("wall_s", "events_per_s", "mean_batch", "offered_hz", "p50_ms", "p90_ms",
+                                        "p99_ms", "mean_ms", "max_ms")]
+
+
+class BatchSummary(ctypes.Structure):
+    _fields_ = [("n_events", ctypes.c_uint32), ("flags", ctypes.c_uint32)] + \
+        [(n, ctypes.c_uint64) for n in ("n_tracks", "n_vertices", "result_bytes", "n_digis", "n_modules", "n_hits",
+                                        "n_cells", "n_edges", "n_tuples", "n_tuple_hits")]
+
+
+class ProbeEntry(ctypes.Structure):
+    _fields_ = [("kernel", ctypes.c_char_p), ("ms", ctypes.c_float)]
+
+
+RESULT_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ResultView))
+
+# (field, dtype, elements per track / vertex)
+_TRACK_FIELDS = [("tuple_index", np.uint32, 1), ("track_n_hits", np.uint8, 1), ("quality", np.uint8, 1),
+                 ("state", np.float32, 5), ("cov", np.float32, 15), ("pt", np.float32, 1), ("eta", np.float32, 1),
+                 ("chi2", np.float32, 1), ("hits", np.uint16, 5), ("vertex", np.int16, 1)]
+_VERTEX_FIELDS = [("zv", np.float32), ("wv", np.float32), ("vchi2", np.float32), ("ptv2", np.float32),
+                  ("ndof", np.int32), ("sort_ind", np.uint16)]
+
+
+def result_from_view(v):
+    """Copies a pg_result_view into numpy arrays."""
+    out = {n: getattr(v, n) for n in ("n_tracks", "n_loose_all", "n_vertices", "n_hits", "n_tuples", "n_digis",
+                                       "n_cells", "flags")}
+    nt, nv = v.n_tracks, v.n_vertices
+    for name, dt, k in _TRACK_FIELDS:
+        nb = nt * k * np.dtype(dt).itemsize
+        a = np.frombuffer(ctypes.string_at(getattr(v, name), nb), dtype=dt) if nb else np.zeros(0, dt)
+        out[name] = a.reshape(nt, k) if k > 1 else a
+    for name, dt in _VERTEX_FIELDS:
+        nb = nv * np.dtype(dt).itemsize
+        out[name] = np.frombuffer(ctypes.string_at(getattr(v, name), nb), dtype=dt) if nb else np.zeros(0, dt)
+    return out
 
 
 class EventCounts(ctypes.Structure):
@@ -221,6 +275,29 @@ def gpu_lib():
                                        ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
         _gpu.pg_fit_broken_line.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32] + [ctypes.c_void_p] * 2 + \
             [ctypes.c_double] + [ctypes.c_void_p] * 6
+        _gpu.pg_get_config.argtypes = [ctypes.c_void_p, ctypes.POINTER(Config)]
+        _gpu.pg_default_config.argtypes = [ctypes.POINTER(Config)]
+        _gpu.pg_submit.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_char_p),
+                                   ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_uint32)]
+        for f in ("pg_query", "pg_wait", "pg_release"):
+            getattr(_gpu, f).argtypes = [ctypes.c_void_p, ctypes.c_uint32]
+        _gpu.pg_result.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ResultView)]
+        _gpu.pg_pool_put.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint32)]
+        _gpu.pg_pool_release.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
+        _gpu.pg_pool_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                      ctypes.POINTER(ctypes.c_uint32)]
+        _gpu.pg_submit_pooled.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
+                                          ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
+        _gpu.pg_set_probe.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        _gpu.pg_batch_summary_get.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(BatchSummary)]
+        _gpu.pg_probe_read.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ProbeEntry),
+                                       ctypes.POINTER(ctypes.c_uint32)]
+        _gpu.pg_prepare.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
+        _gpu.pg_default_serve_config.argtypes = [ctypes.POINTER(ServeConfig)]
+        _gpu.pg_serve.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_char_p),
+                                  ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ServeConfig), ctypes.c_void_p,
+                                  ctypes.c_void_p, ctypes.POINTER(ServeStats), ctypes.c_void_p, RESULT_FN,
+                                  ctypes.c_void_p]
     return _gpu
 
 
@@ -234,18 +311,22 @@ def _raw_arrays(raws):
 class Chain:
     """A device context: resident conditions plus batch slots."""
 
-    def __init__(self, es_images, max_events=64, max_words_per_batch=None, slots=1, device=0):
+    def __init__(self, es_images, max_events=64, max_words_per_batch=None, slots=1, device=0, use_graphs=True,
+                 pool_words=0, hbm_fraction=0.5):
         lib = gpu_lib()
         self._keep = list(es_images)
         img = ESImages(*[x for b in self._keep for x in (b, len(b))])
         if max_words_per_batch is None:
             max_words_per_batch = max_events * 160000
-        cfg = Config(device, max_events, max_words_per_batch, slots)
+        cfg = Config(device, max_events, max_words_per_batch, slots, 1 if use_graphs else 0, pool_words, hbm_fraction)
         self._h = ctypes.c_void_p()
         rc = lib.pg_create(ctypes.byref(img), ctypes.byref(cfg), ctypes.byref(self._h))
         if rc != 0:
             raise RuntimeError("pg_create failed with status %d" % rc)
+        got = Config()
+        lib.pg_get_config(self._h, ctypes.byref(got))
         self.max_events = max_events
+        self.slots = got.slots
 
     def _check(self, rc, what):
         if rc != 0:
@@ -315,6 +396,117 @@ class Chain:
         out["cellNbrOff"], out["cellNbr"] = capped(self.product(k, "cellNbrOffRaw"), self.product(k, "cellNbrRaw"), 36)
         out["cellTrkOff"], out["cellTrk"] = capped(self.product(k, "cellTrkOffRaw"), self.product(k, "cellTrkRaw"), 48)
         return out
+
+    # ------------------------------------------------------------ asynchronous batches
+    def submit(self, raws):
+        """Launches a batch on a free slot and returns the slot (None when all are busy)."""
+        ptrs, sizes = _raw_arrays(raws)
+        slot = ctypes.c_uint32()
+        rc = gpu_lib().pg_submit(self._h, len(raws), ptrs, sizes, ctypes.byref(slot))
+        if rc == -5:
+            return None
+        self._check(rc, "pg_submit")
+        return slot.value
+
+    def query(self, slot):
+        rc = gpu_lib().pg_query(self._h, slot)
+        if rc == -5:
+            return False
+        self._check(rc, "pg_query")
+        return True
+
+    def wait(self, slot):
+        self._check(gpu_lib().pg_wait(self._h, slot), "pg_wait")
+
+    def result(self, slot, k):
+        v = ResultView()
+        self._check(gpu_lib().pg_result(self._h, slot, k, ctypes.byref(v)), "pg_result")
+        return result_from_view(v)
+
+    def summary(self, slot):
+        """Totals over the finished batch on `slot` (result bytes, event counts)."""
+        b = BatchSummary()
+        self._check(gpu_lib().pg_batch_summary_get(self._h, slot, ctypes.byref(b)), "pg_batch_summary_get")
+        return {n: getattr(b, n) for n, _ in BatchSummary._fields_}
+
+    def release(self, slot):
+        self._check(gpu_lib().pg_release(self._h, slot), "pg_release")
+
+    # ------------------------------------------------------------ device-resident pool
+    def pool_put(self, raw):
+        """Admits one event into the pool; None when the pool has no room now."""
+        h = ctypes.c_uint32()
+        rc = gpu_lib().pg_pool_put(self._h, raw, len(raw), ctypes.byref(h))
+        if rc in (-5, -6):
+            return None
+        self._check(rc, "pg_pool_put")
+        return h.value
+
+    def pool_release(self, handle):
+        self._check(gpu_lib().pg_pool_release(self._h, handle), "pg_pool_release")
+
+    def pool_info(self):
+        cap, free, live = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint32()
+        self._check(gpu_lib().pg_pool_info(self._h, ctypes.byref(cap), ctypes.byref(free), ctypes.byref(live)),
+                    "pg_pool_info")
+        return {"cap_words": cap.value, "free_words": free.value, "live_events": live.value}
+
+    def submit_pooled(self, handles, keep=False):
+        """Gathers pooled events into a free slot and launches; None when all slots are busy.
+        keep=True leaves the events resident for later batches."""
+        arr = (ctypes.c_uint32 * len(handles))(*handles)
+        slot = ctypes.c_uint32()
+        rc = gpu_lib().pg_submit_pooled(self._h, len(handles), arr, 1 if keep else 0, ctypes.byref(slot))
+        if rc == -5:
+            return None
+        self._check(rc, "pg_submit_pooled")
+        return slot.value
+
+    def set_probe(self, kernel):
+        """Times every launch of `kernel` ("*" = all kernels, None = off) from now on."""
+        self._check(gpu_lib().pg_set_probe(self._h, kernel.encode() if kernel else None), "pg_set_probe")
+
+    def probe_read(self, slot):
+        """[(kernel, ms)] of the timed launches of the last finished batch on `slot`."""
+        buf = (ProbeEntry * 256)()
+        n = ctypes.c_uint32()
+        self._check(gpu_lib().pg_probe_read(self._h, slot, 256, buf, ctypes.byref(n)), "pg_probe_read")
+        return [(buf[i].kernel.decode(), buf[i].ms) for i in range(n.value)]
+
+    def prepare(self, max_batch=0):
+        self._check(gpu_lib().pg_prepare(self._h, max_batch), "pg_prepare")
+
+    def serve(self, raws, n_requests, rate_hz=None, arrivals=None, request_event=None, max_batch=0, seed=1,
+              upload_threads=2, on_result=None):
+        """Runs the serving loop; returns (stats dict, per-request latency seconds)."""
+        lib = gpu_lib()
+        ptrs, sizes = _raw_arrays(raws)
+        cfg = ServeConfig()
+        lib.pg_default_serve_config(ctypes.byref(cfg))
+        cfg.n_requests = n_requests
+        if rate_hz is not None:
+            cfg.rate_hz = rate_hz
+        cfg.seed = seed
+        cfg.max_batch = max_batch
+        cfg.upload_threads = upload_threads
+        arr = None
+        if arrivals is not None:
+            arr = np.ascontiguousarray(arrivals, dtype=np.float64)
+            assert arr.shape == (n_requests,)
+        rev = None
+        if request_event is not None:
+            rev = np.ascontiguousarray(request_event, dtype=np.uint32)
+            assert rev.shape == (n_requests,)
+        lat = np.zeros(n_requests, dtype=np.float64)
+        st = ServeStats()
+        fn = RESULT_FN(0)
+        if on_result is not None:
+            fn = RESULT_FN(lambda user, req, ev, view: on_result(req, ev, result_from_view(view.contents)))
+        rc = lib.pg_serve(self._h, len(raws), ptrs, sizes, ctypes.byref(cfg),
+                          arr.ctypes.data if arr is not None else None, rev.ctypes.data if rev is not None else None,
+                          ctypes.byref(st), lat.ctypes.data, fn, None)
+        self._check(rc, "pg_serve")
+        return {n: getattr(st, n) for n, _ in ServeStats._fields_}, lat
 
     def fit(self, N, hits, ge, B=B_FIELD):
         """Broken-line fit of host arrays hits[n, N, 3] (f64), ge[n, N, 6] (f32) on the device."""

@@ -57,6 +57,7 @@ void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W) {
   c.take(ws.detInd, H);
   c.take(ws.phiOff, size_t(E) * kPhiStride);
   c.take(ws.phiBins, H);
+  c.take(ws.phiRec, H);
   c.take(ws.agc, E);
   c.take(ws.jCount, size_t(E) * (kJCap + 1));
   c.take(ws.jOffset, size_t(E) * (kJCap + 1));
@@ -71,6 +72,7 @@ void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W) {
   c.take(ws.ohCount, size_t(E) * (kHitCap + 1));
   c.take(ws.ohOff, size_t(E) * (kHitCap + 1));
   c.take(ws.ohCells, C);
+  c.take(ws.ohRec, C);
   size_t C1 = size_t(E) * (kCellCap + 1);
   c.take(ws.nbrCount, C1);
   c.take(ws.nbrOff, C1);
@@ -110,6 +112,7 @@ void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W) {
   c.take(ws.scratchA, size_t(E) * kEdgeCap);
   c.take(ws.scratchB, size_t(E) * kEdgeCap);
   c.take(ws.scanTmp, size_t(E + 1) * kScanTmpStride);
+  c.take(ws.bigSeg, size_t(E) * kBigSegCap);
 }
 
 // the pair opened by probeBegin when its name matched (-1: none).  Records use

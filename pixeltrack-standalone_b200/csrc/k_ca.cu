@@ -20,6 +20,7 @@
 // order-dependent cleaner (fastDuplicateRemover) runs as rounds over the
 // dependency graph of cells that share a track.
 #include "device_utils.cuh"
+#include "segsort.cuh"
 #include "pixgpu_internal.cuh"
 
 namespace pixgpu {
@@ -85,103 +86,168 @@ __global__ void kDoubletSetup(Workspace ws, uint32_t nEvents) {
   c->ntot = cum;
 }
 
-// Visit the doublet candidates of inner-hit slot j in serial order.  F(oi)
-// is called for each accepted outer hit.
-template <typename F>
-__device__ __forceinline__ void forEachDoublet(const EventCounters* c, const HitsView& hh, uint32_t j,
-                                               uint32_t& pairOut, uint32_t& innerOut, F&& f) {
+// Doublet search for inner-hit slot j (gpuPixelDoubletsAlgos.h:25-238 with
+// the PixelTriplets defaults): the per-inner-hit cuts, then the outer layer's
+// phi window as one or two contiguous ranges of the phi histogram.  The
+// serial order of the candidates is the window's bin order with each bin's
+// stored order, i.e. the order of these ranges.
+struct DoubletSeed {
+  uint32_t pair, inner, outer, i;
+  float mez, mer;
+  int16_t mep, mes, iphicut;
+  float maxr;
+  uint32_t b0, e0, b1, e1;  // candidate ranges in phiBins
+};
+
+// per-event layer offsets staged in shared memory by each block
+struct PairTable {
+  uint32_t pairCum[kNPairs];
+  uint32_t layerStart[11];
+};
+
+__device__ __forceinline__ void loadPairTable(const EventCounters* c, PairTable& t) {
+  if (threadIdx.x < kNPairs) t.pairCum[threadIdx.x] = c->pairCum[threadIdx.x];
+  if (threadIdx.x < 11) t.layerStart[threadIdx.x] = c->layerStart[threadIdx.x];
+  __syncthreads();
+}
+
+__device__ __forceinline__ bool doubletSeed(const PairTable& c, const HitsView& hh, uint32_t j, DoubletSeed& d) {
   uint32_t pair = 0;
-  while (j >= c->pairCum[pair]) ++pair;
-  uint8_t inner = cLayerPairs[2 * pair], outer = cLayerPairs[2 * pair + 1];
-  uint32_t i = (0 == pair) ? j : j - c->pairCum[pair - 1];
-  i += c->layerStart[inner];
-  pairOut = pair;
-  innerOut = i;
-  uint16_t mi = hh.detInd[i];
-  if (mi > 2000) return;
-  float mez = hh.zg[i];
-  if (mez < cMinZ[pair] || mez > cMaxZ[pair]) return;
-  int16_t mes = hh.ysize[i];  // ideal conditions: every ladder is treated as outer
+  while (j >= c.pairCum[pair]) ++pair;
+  const uint8_t inner = cLayerPairs[2 * pair], outer = cLayerPairs[2 * pair + 1];
+  uint32_t i = (0 == pair) ? j : j - c.pairCum[pair - 1];
+  i += c.layerStart[inner];
+  d.pair = pair;
+  d.inner = inner;
+  d.outer = outer;
+  d.i = i;
+  if (hh.detInd[i] > 2000) return false;
+  d.mez = hh.zg[i];
+  if (d.mez < cMinZ[pair] || d.mez > cMaxZ[pair]) return false;
+  d.mes = hh.ysize[i];  // ideal conditions: every ladder is treated as outer
   if (inner == 0 && outer > 3)
-    if (mes > 0 && mes < 36) return;
+    if (d.mes > 0 && d.mes < 36) return false;
   if (inner == 1 && outer > 3)
-    if (mes > 0 && mes < 28) return;
-  int16_t mep = hh.iphi[i];
-  float mer = hh.rg[i];
-  int16_t iphicut = cPhiCuts[pair];
-  uint32_t kl = phiBin(int16_t(mep - iphicut)), kh = phiBin(int16_t(mep + iphicut));
-  uint32_t hoff = 128 * outer;
-  uint32_t khh = (kh + 1) & 127;
+    if (d.mes > 0 && d.mes < 28) return false;
+  d.mep = hh.iphi[i];
+  d.mer = hh.rg[i];
+  d.iphicut = cPhiCuts[pair];
+  d.maxr = cMaxR[pair];
+  const uint32_t kl = phiBin(int16_t(d.mep - d.iphicut)), kh = phiBin(int16_t(d.mep + d.iphicut));
+  const uint32_t khh = (kh + 1) & 127;
+  const uint32_t* off = hh.phiOff + 128 * outer;
+  d.b0 = d.e0 = d.b1 = d.e1 = 0;
+  if (kl == khh) return false;  // the serial bin loop runs no iteration
+  if (kl <= kh) {
+    d.b0 = off[kl];
+    d.e0 = off[kh + 1];
+  } else {
+    d.b0 = off[kl];
+    d.e0 = off[128];
+    d.b1 = off[0];
+    d.e1 = off[kh + 1];
+  }
+  return true;
+}
+
+// candidate test on a packed hit record (kPhiRec layout)
+__device__ __forceinline__ bool doubletAccept(const DoubletSeed& d, const uint4 rec) {
   constexpr float z0cut = 12.f;
   constexpr float minRadius = 0.5f * 87.78f;
   constexpr float minRadius2T4 = 4.f * minRadius * minRadius;
   constexpr float dzdrFact = 8 * 0.0285 / 0.015;
   constexpr float i2p = 3.14159265358979323846 / 32768;
-  const float maxr = cMaxR[pair];
-  for (uint32_t kk = kl; kk != khh; kk = (kk + 1) & 127) {
-    uint32_t b = kk + hoff;
-    for (uint32_t p = hh.phiOff[b], pe = hh.phiOff[b + 1]; p < pe; ++p) {
-      uint16_t oi = hh.phiBins[p];
-      if (hh.detInd[oi] > 2000) continue;
-      float zo = hh.zg[oi], ro = hh.rg[oi];
-      float dr = ro - mer;
-      if (dr > maxr || dr < 0 || fabsf((mez * ro - mer * zo)) > z0cut * dr) continue;
-      int16_t mop = hh.iphi[oi];
-      uint16_t idphi = uint16_t(min(abs(int(int16_t(mop - mep))), abs(int(int16_t(mep - mop)))));
-      if (idphi > iphicut) continue;
-      {
-        int16_t so = hh.ysize[oi];
-        bool cut = (outer < 4) ? (mes > 0 && so > 0 && abs(so - mes) > (inner == 0 ? 28 : 20))
-                               : ((inner < 4) && mes > 0 &&
-                                  abs(mes - int(fabsf((mez - zo) / (mer - ro)) * dzdrFact + 0.5f)) > 20);
-        if (cut) continue;
+  if ((rec.w & 0xffffu) > 2000) return false;
+  const float zo = __uint_as_float(rec.x), ro = __uint_as_float(rec.y);
+  const float dr = ro - d.mer;
+  if (dr > d.maxr || dr < 0 || fabsf((d.mez * ro - d.mer * zo)) > z0cut * dr) return false;
+  const int16_t mop = int16_t(rec.z & 0xffffu);
+  const uint16_t idphi = uint16_t(min(abs(int(int16_t(mop - d.mep))), abs(int(int16_t(d.mep - mop)))));
+  if (idphi > d.iphicut) return false;
+  const int16_t so = int16_t(rec.z >> 16);
+  const bool cut = (d.outer < 4) ? (d.mes > 0 && so > 0 && abs(so - d.mes) > (d.inner == 0 ? 28 : 20))
+                                 : ((d.inner < 4) && d.mes > 0 &&
+                                    abs(d.mes - int(fabsf((d.mez - zo) / (d.mer - ro)) * dzdrFact + 0.5f)) > 20);
+  if (cut) return false;
+  const float dphi = float(short(idphi)) * i2p;
+  if (dphi * dphi * (minRadius2T4 - d.mer * ro) > (ro - d.mer) * (ro - d.mer)) return false;
+  return true;
+}
+
+// One warp per inner-hit slot: lanes test consecutive candidates of the
+// window; the ballots give the count (pass 1) and the serial positions
+// (pass 2).  F(position among the slot's doublets, outer hit).
+template <typename F>
+__device__ __forceinline__ uint32_t warpDoublets(const DoubletSeed& d, const uint4* rec, F&& f) {
+  const uint32_t lane = laneId();
+  uint32_t n = 0;
+  for (int r = 0; r < 2; ++r) {
+    const uint32_t b = r ? d.b1 : d.b0, en = r ? d.e1 : d.e0;
+    for (uint32_t p0 = b; p0 < en; p0 += 32) {
+      const uint32_t p = p0 + lane;
+      uint16_t oi = 0;
+      bool ok = false;
+      if (p < en) {
+        const uint4 h = rec[p];
+        oi = uint16_t(h.w >> 16);
+        ok = doubletAccept(d, h);
       }
-      {
-        float dphi = float(short(idphi)) * i2p;
-        if (dphi * dphi * (minRadius2T4 - mer * ro) > (ro - mer) * (ro - mer)) continue;
-      }
-      f(oi);
+      const uint32_t m = __ballot_sync(0xffffffffu, ok);
+      if (ok) f(n + __popc(m & lanemaskLt()), oi);
+      n += __popc(m);
     }
   }
+  return n;
 }
 
 __global__ void kDoubletCount(Workspace ws) {
-  uint32_t e = blockIdx.y;
+  __shared__ PairTable pt;
+  const uint32_t e = blockIdx.y;
   const EventCounters* c = ws.ev + e;
-  uint32_t ntot = c->ntot;
-  HitsView hh = hitsOf(ws, e);
+  const uint32_t ntot = c->ntot;
+  loadPairTable(c, pt);
+  const HitsView hh = hitsOf(ws, e);
+  const uint4* rec = ws.phiRec + size_t(e) * kHitCap;
   uint32_t* cnt = ws.jCount + size_t(e) * (kJCap + 1);
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < ntot; j += gridDim.x * blockDim.x) {
-    uint32_t n = 0, pair, inner;
-    forEachDoublet(c, hh, j, pair, inner, [&](uint16_t) { ++n; });
-    cnt[j] = n;
+  const uint32_t wpb = blockDim.x >> 5;
+  for (uint32_t j = blockIdx.x * wpb + (threadIdx.x >> 5); j < ntot; j += gridDim.x * wpb) {
+    DoubletSeed d;
+    uint32_t n = 0;
+    if (doubletSeed(pt, hh, j, d)) n = warpDoublets(d, rec, [](uint32_t, uint16_t) {});
+    if (laneId() == 0) cnt[j] = n;
   }
 }
 
 __global__ void kDoubletWrite(Workspace ws) {
-  uint32_t e = blockIdx.y;
-  EventCounters* c = ws.ev + e;
-  uint32_t ntot = c->ntot;
-  HitsView hh = hitsOf(ws, e);
+  __shared__ PairTable pt;
+  const uint32_t e = blockIdx.y;
+  const EventCounters* c = ws.ev + e;
+  const uint32_t ntot = c->ntot;
+  loadPairTable(c, pt);
+  const HitsView hh = hitsOf(ws, e);
+  const uint4* rec = ws.phiRec + size_t(e) * kHitCap;
   const uint32_t* off = ws.jOffset + size_t(e) * (kJCap + 1);
-  size_t cb = size_t(e) * kCellCap;
+  const size_t cb = size_t(e) * kCellCap;
   uint32_t* ohc = ws.ohCount + size_t(e) * (kHitCap + 1);
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < ntot; j += gridDim.x * blockDim.x) {
-    uint32_t idx = off[j];
-    if (idx >= kCellCap) continue;
-    uint32_t pair, inner;
-    forEachDoublet(c, hh, j, pair, inner, [&](uint16_t oi) {
+  const uint32_t wpb = blockDim.x >> 5;
+  for (uint32_t j = blockIdx.x * wpb + (threadIdx.x >> 5); j < ntot; j += gridDim.x * wpb) {
+    const uint32_t base = off[j];
+    if (base >= kCellCap || off[j + 1] == base) continue;
+    DoubletSeed d;
+    if (!doubletSeed(pt, hh, j, d)) continue;
+    const float zi = hh.zg[d.i], ri = hh.rg[d.i];
+    warpDoublets(d, rec, [&](uint32_t k, uint16_t oi) {
+      const uint32_t idx = base + k;
       if (idx < kCellCap) {
-        ws.cellInner[cb + idx] = uint16_t(inner);
+        ws.cellInner[cb + idx] = uint16_t(d.i);
         ws.cellOuter[cb + idx] = oi;
-        ws.cellPair[cb + idx] = uint8_t(pair);
+        ws.cellPair[cb + idx] = uint8_t(d.pair);
         ws.cellDoubletId[cb + idx] = int32_t(idx);
         ws.cellUsed[cb + idx] = 0;
-        ws.cellInnerZ[cb + idx] = hh.zg[inner];
-        ws.cellInnerR[cb + idx] = hh.rg[inner];
+        ws.cellInnerZ[cb + idx] = zi;
+        ws.cellInnerR[cb + idx] = ri;
         atomicAdd(&ohc[oi], 1u);
       }
-      ++idx;
     });
   }
 }
@@ -217,21 +283,6 @@ __global__ void kOuterHitFill(Workspace ws) {
     uint16_t oi = ws.cellOuter[cb + c];
     uint32_t p = atomicAdd(&cur[oi], 1u);
     ws.ohCells[cb + off[oi] + p] = c;
-  }
-}
-
-template <typename T>
-__global__ void kSortSegments(T* data, size_t dataStride, const uint32_t* off, size_t offStride,
-                              const uint32_t* lenPtr, uint32_t lenStride, uint32_t fixedLen, bool desc,
-                              uint32_t dataCap) {
-  uint32_t e = blockIdx.y;
-  uint32_t nseg = lenPtr ? lenPtr[size_t(e) * lenStride] : fixedLen;
-  const uint32_t* o = off + size_t(e) * offStride;
-  T* d = data + size_t(e) * dataStride;
-  uint32_t warpsPerBlock = blockDim.x >> 5;
-  for (uint32_t s = blockIdx.x * warpsPerBlock + (threadIdx.x >> 5); s < nseg; s += gridDim.x * warpsPerBlock) {
-    uint32_t b = min(o[s], dataCap), en = min(o[s + 1], dataCap);
-    warpSortSegment(d + b, en - b, desc);
   }
 }
 
@@ -273,45 +324,93 @@ __device__ __forceinline__ bool dcaCut(float x1, float y1, float x2, float y2, f
   return fabsf(dca0) < region * fabsf(cc);
 }
 
-// one thread per (cell); appends CA links (oc <- idx) unordered
+// inner-hit coordinates of every ohCells entry, in ohCells order, so that
+// kConnect reads the candidate cells of a hit as one contiguous range; the
+// sign of r carries the dca region of the candidate (negative: innermost
+// barrel layer, dca cut 0.15 instead of 0.25)
+__global__ void kOhRec(Workspace ws) {
+  const uint32_t e = blockIdx.y;
+  const uint32_t n = ws.ev[e].nCells;
+  const size_t cb = size_t(e) * kCellCap, hb = size_t(e) * kHitCap;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const uint32_t oc = ws.ohCells[cb + p];
+    const uint16_t ih = ws.cellInner[cb + oc];
+    const float r = ws.cellInnerR[cb + oc];
+    ws.ohRec[cb + p] = make_float4(ws.xg[hb + ih], ws.yg[hb + ih], ws.cellInnerZ[cb + oc],
+                                   ws.detInd[hb + ih] < 96 ? -r : r);
+  }
+}
+
+// kernel_connect (CAHitNtupletGeneratorKernelsImpl.h:191-262) by doublet
+// slot: the cells of slot j share their inner hit h, so they share the
+// candidate list (cells ending on h, first 128 in ascending order).  A warp
+// takes a slot: each lane holds up to one candidate per round of 32 and the
+// slot's cells are visited one after the other.  Accepted links (oc <- idx)
+// are appended unordered, one atomic per warp and cell.
 __global__ void kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
-  uint32_t e = blockIdx.y;
+  const uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
-  uint32_t n = c->nCells;
-  HitsView hh = hitsOf(ws, e);
-  size_t cb = size_t(e) * kCellCap;
+  const uint32_t ntot = c->ntot;
+  const uint32_t nCells = c->nCells;
+  const HitsView hh = hitsOf(ws, e);
+  const size_t cb = size_t(e) * kCellCap;
+  const uint32_t* joff = ws.jOffset + size_t(e) * (kJCap + 1);
   const uint32_t* ohOff = ws.ohOff + size_t(e) * (kHitCap + 1);
   const uint32_t* ohCells = ws.ohCells + cb;
+  const float4* ohRec = ws.ohRec + cb;
   uint32_t* nbrCnt = ws.nbrCount + size_t(e) * (kCellCap + 1);
-  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
-    uint16_t innerHit = ws.cellInner[cb + idx];
-    uint16_t outerHit = ws.cellOuter[cb + idx];
-    uint32_t b = ohOff[innerHit], cnt = min(ohOff[innerHit + 1] - b, uint32_t(PF_MAX_CELLS_PER_HIT));
-    if (cnt == 0) continue;
-    float ri = ws.cellInnerR[cb + idx], zi = ws.cellInnerZ[cb + idx];
-    float ro = hh.rg[outerHit], zo = hh.zg[outerHit];
-    bool isBarrel = hh.detInd[innerHit] < 1184;
-    float x2 = hh.xg[innerHit], y2 = hh.yg[innerHit], x3 = hh.xg[outerHit], y3 = hh.yg[outerHit];
-    bool any = false;
-    for (uint32_t jj = 0; jj < cnt; ++jj) {
-      uint32_t oc = ohCells[b + jj];
-      float r1 = ws.cellInnerR[cb + oc], z1 = ws.cellInnerZ[cb + oc];
-      if (!alignedRZ(r1, z1, ri, zi, ro, zo, isBarrel ? kThetaCutBarrel : kThetaCutForward)) continue;
-      uint16_t ih = ws.cellInner[cb + oc];
-      float region = hh.detInd[ih] < 96 ? kDcaCutInner : kDcaCutOuter;
-      if (!dcaCut(hh.xg[ih], hh.yg[ih], x2, y2, x3, y3, region)) continue;
-      any = true;
-      ws.cellUsed[cb + oc] = 1;
-      atomicAdd(&nbrCnt[oc], 1u);
-      uint32_t k = atomicAdd(&c->nEdges, 1u);
-      if (k < kEdgeCap) {
-        edgeOc[size_t(e) * kEdgeCap + k] = oc;
-        edgeIdx[size_t(e) * kEdgeCap + k] = idx;
-      } else {
-        atomicOr(&c->flags, kFlagEdgeOverflow);
+  uint32_t* eOc = edgeOc + size_t(e) * kEdgeCap;
+  uint32_t* eIdx = edgeIdx + size_t(e) * kEdgeCap;
+  const uint32_t lane = laneId(), wpb = blockDim.x >> 5;
+  for (uint32_t j = blockIdx.x * wpb + (threadIdx.x >> 5); j < ntot; j += gridDim.x * wpb) {
+    const uint32_t base = joff[j];
+    const uint32_t end = min(joff[j + 1], nCells);
+    if (base >= end) continue;
+    const uint16_t h = ws.cellInner[cb + base];
+    const uint32_t ob = ohOff[h];
+    const uint32_t m = min(ohOff[h + 1] - ob, uint32_t(PF_MAX_CELLS_PER_HIT));
+    if (m == 0) continue;
+    const float ri = ws.cellInnerR[cb + base], zi = ws.cellInnerZ[cb + base];
+    const float thetaCut = hh.detInd[h] < 1184 ? kThetaCutBarrel : kThetaCutForward;
+    const float x2 = hh.xg[h], y2 = hh.yg[h];
+    for (uint32_t k0 = 0; k0 < m; k0 += 32) {
+      const uint32_t k = k0 + lane;
+      float4 r1 = make_float4(0.f, 0.f, 0.f, 0.f);
+      uint32_t oc = 0;
+      if (k < m) {
+        r1 = ohRec[ob + k];
+        oc = ohCells[ob + k];
       }
+      const float region = r1.w < 0.f ? kDcaCutInner : kDcaCutOuter;
+      const float rr1 = fabsf(r1.w);
+      bool usedOc = false;
+      for (uint32_t idx = base; idx < end; ++idx) {
+        const uint16_t oh = ws.cellOuter[cb + idx];
+        const float ro = hh.rg[oh], zo = hh.zg[oh], x3 = hh.xg[oh], y3 = hh.yg[oh];
+        const bool ok = k < m && alignedRZ(rr1, r1.z, ri, zi, ro, zo, thetaCut) &&
+                        dcaCut(r1.x, r1.y, x2, y2, x3, y3, region);
+        const uint32_t mask = __ballot_sync(0xffffffffu, ok);
+        if (mask == 0) continue;
+        uint32_t at = 0;
+        if (lane == 0) {
+          at = atomicAdd(&c->nEdges, uint32_t(__popc(mask)));
+          ws.cellUsed[cb + idx] = 1;
+        }
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if (ok) {
+          usedOc = true;
+          atomicAdd(&nbrCnt[oc], 1u);
+          const uint32_t slot = at + __popc(mask & lanemaskLt());
+          if (slot < kEdgeCap) {
+            eOc[slot] = oc;
+            eIdx[slot] = idx;
+          } else {
+            atomicOr(&c->flags, kFlagEdgeOverflow);
+          }
+        }
+      }
+      if (usedOc) ws.cellUsed[cb + oc] = 1;
     }
-    if (any) ws.cellUsed[cb + idx] = 1;
   }
 }
 
@@ -875,24 +974,23 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   // ---- doublets: count per inner-hit slot, scan, write in serial order
   PG_PROBED("kDoubletSetup", stream, kDoubletSetup<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents));
   PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.ohCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
-  PG_PROBED("kDoubletCount", stream, kDoubletCount<<<g, 128, 0, stream>>>(ws));
+  PG_PROBED("kDoubletCount", stream, kDoubletCount<<<dim3(gx * 4, nEvents), 256, 0, stream>>>(ws));
   segScan(ws.jCount, ws.jOffset, kJCap + 1, EVF(ntot), kJCap, nullptr, 0, ws.scanTmp, nEvents, stream);
-  PG_PROBED("kDoubletWrite", stream, kDoubletWrite<<<g, 128, 0, stream>>>(ws));
+  PG_PROBED("kDoubletWrite", stream, kDoubletWrite<<<dim3(gx * 4, nEvents), 256, 0, stream>>>(ws));
   PG_PROBED("kCellsTotal", stream, kCellsTotal<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents));
   // ---- isOuterHitOfCell: scan of the per-hit counts, unordered fill, order per hit
   segScan(ws.ohCount, ws.ohOff, kHitCap + 1, EVF(nHits), kHitCap, nullptr, 0, ws.scanTmp, nEvents, stream);
   PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.ohCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
   PG_PROBED("kOuterHitFill", stream, kOuterHitFill<<<g, 256, 0, stream>>>(ws));
-  PG_PROBED("kSortSegments", stream, kSortSegments<uint32_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.ohCells, kCellCap, ws.ohOff, kHitCap + 1,
-                                                                     EVF(nHits), 0, false, kCellCap));
+  sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.ohCells, kCellCap, ws.ohOff, kHitCap + 1, EVF(nHits), 0, false, kCellCap, 0);
+  PG_PROBED("kOhRec", stream, kOhRec<<<g, 256, 0, stream>>>(ws));
   // ---- CA links: edges appended unordered, then CSR by inner cell, ordered ascending
   PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbrCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
-  PG_PROBED("kConnect", stream, kConnect<<<g, 128, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
+  PG_PROBED("kConnect", stream, kConnect<<<dim3(gx * 4, nEvents), 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
   segScan(ws.nbrCount, ws.nbrOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanTmp, nEvents, stream);
   PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbrCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
   PG_PROBED("kEdgeScatter", stream, kEdgeScatter<<<g, 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
-  PG_PROBED("kSortSegments", stream, kSortSegments<uint32_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbr, kEdgeCap, ws.nbrOff, kCellCap + 1,
-                                                                     EVF(nCells), 0, false, kEdgeCap));
+  sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.nbr, kEdgeCap, ws.nbrOff, kCellCap + 1, EVF(nCells), 0, false, kEdgeCap, 1);
   PG_PROBED("kNbrPool", stream, kNbrPool<<<g, 256, 0, stream>>>(ws));
   // ---- early fishbone
   PG_PROBED("kFishbone", stream, kFishbone<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws));
@@ -910,8 +1008,7 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   segScan(ws.trkCount, ws.trkOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanTmp, nEvents, stream);
   PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trkCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
   PG_PROBED("kTrackFill", stream, kTrackFill<<<g, 256, 0, stream>>>(ws));
-  PG_PROBED("kSortSegments", stream, kSortSegments<uint16_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trk, kTupleCellCap, ws.trkOff, kCellCap + 1,
-                                                                     EVF(nCells), 0, false, kTupleCellCap));
+  sortSegments<uint16_t>(ws, nEvents, stream, gx * 2, ws.trk, kTupleCellCap, ws.trkOff, kCellCap + 1, EVF(nCells), 0, false, kTupleCellCap, 2);
   uint32_t* candFlag = ws.startTupleCount;  // scratch
   uint32_t* candOff = ws.startHitCount;
   PG_PROBED("kTrackPool", stream, kTrackPool<<<g, 256, 0, stream>>>(ws, candFlag));
@@ -943,8 +1040,7 @@ cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   segScan(ws.h2tCount, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, nullptr, 0, ws.scanTmp, nEvents, stream);
   PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
   PG_PROBED("kHitToTupleFill", stream, kHitToTupleFill<<<g, 256, 0, stream>>>(ws));
-  PG_PROBED("kSortSegments", stream, kSortSegments<uint16_t><<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.h2t, kH2TCap, ws.h2tOff, kHitCap + 1,
-                                                                     nullptr, 0, kHitCap, true, kH2TCap));
+  sortSegments<uint16_t>(ws, nEvents, stream, gx * 2, ws.h2t, kH2TCap, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, true, kH2TCap, 3);
   PG_PROBED("kTripletCleaner", stream, kTripletCleaner<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws));
   return cudaGetLastError();
 }

@@ -180,6 +180,7 @@ __global__ void kInitEvents(Workspace ws, uint32_t nEvents) {
     c->apcM = c->apcN = c->nTuples = c->nTupleCells = 0;
     c->nCandidates = c->nLoose = 0;
     c->nVertices = c->nErrors = c->nVtxTracks = 0;
+    c->nBig[0] = c->nBig[1] = c->nBig[2] = c->nBig[3] = 0;
     c->flags = c->nWords > kMaxFedWords ? kFlagTooManyWords : 0u;
   }
   uint32_t* cim = ws.clusInModule + size_t(e) * kModStride;
@@ -488,8 +489,14 @@ __global__ void __launch_bounds__(kClusThreads) kFindClusters(Workspace ws) {
     }
   }
   __syncthreads();
-  for (uint32_t k = threadIdx.x; k < np; k += blockDim.x)
-    if (sy[k] != 0xffff) lab[k] = find(int32_t(k));
+  // flatten: read-only walk to the root (path halving here would race with
+  // the final root writes of other threads and could leave a non-root label)
+  for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
+    if (sy[k] == 0xffff) continue;
+    int32_t r = lab[k];
+    while (lab[r] != r) r = lab[r];
+    lab[k] = r;
+  }
   __syncthreads();
   // number the roots in ascending pixel order
   {
@@ -787,6 +794,24 @@ __global__ void kPhiSort(Workspace ws) {
   warpSortSegment(bins + off[b], off[b + 1] - off[b], true);
 }
 
+// packed copy of the hits in phi-histogram order, read as contiguous
+// candidate ranges by the doublet search
+__global__ void kPhiRec(Workspace ws) {
+  const uint32_t e = blockIdx.y;
+  const uint32_t n = ws.phiOff[size_t(e) * kPhiStride + kPhiTot - 1];
+  const size_t hb = size_t(e) * kHitCap;
+  const uint16_t* bins = ws.phiBins + hb;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const uint32_t h = bins[p];
+    uint4 r;
+    r.x = __float_as_uint(ws.zg[hb + h]);
+    r.y = __float_as_uint(ws.rg[hb + h]);
+    r.z = uint32_t(uint16_t(ws.iphi[hb + h])) | (uint32_t(uint16_t(ws.ysize[hb + h])) << 16);
+    r.w = uint32_t(ws.detInd[hb + h]) | (h << 16);
+    ws.phiRec[hb + p] = r;
+  }
+}
+
 __global__ void kZeroU32(uint32_t* p, size_t stride, uint32_t n, uint32_t nEvents) {
   uint32_t e = blockIdx.y;
   if (e >= nEvents) return;
@@ -837,6 +862,7 @@ cudaError_t runLocal(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaSt
   segScan(ws.phiOff, ws.phiOff, kPhiStride, nullptr, 0, kPhiTot - 1, nullptr, 0, ws.scanTmp, nEvents, stream);
   PG_PROBED("kPhiFill", stream, kPhiFill<<<dim3(16, nEvents), 256, 0, stream>>>(ws, cursor));
   PG_PROBED("kPhiSort", stream, kPhiSort<<<dim3((kPhiTot - 1 + 7) / 8, nEvents), 256, 0, stream>>>(ws));
+  PG_PROBED("kPhiRec", stream, kPhiRec<<<dim3(16, nEvents), 256, 0, stream>>>(ws));
   return cudaGetLastError();
 }
 

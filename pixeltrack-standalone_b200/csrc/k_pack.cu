@@ -19,15 +19,35 @@ __global__ void kSetInput(BatchInput* in, const uint32_t* words, const uint8_t* 
   in->fedIds = fedIds;
 }
 
-__global__ void kPackResults(Workspace ws, uint8_t* out) {
+// 32-bit word w of a byte (or 16-bit) array assembled from its elements
+template <typename F>
+__device__ __forceinline__ uint32_t packBytes(uint32_t w, uint32_t n, F&& get) {
+  uint32_t x = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < 4; ++k) {
+    const uint32_t i = 4 * w + k;
+    x |= (i < n ? uint32_t(get(i)) & 0xffu : 0u) << (8 * k);
+  }
+  return x;
+}
+template <typename F>
+__device__ __forceinline__ uint32_t packHalves(uint32_t w, uint32_t n, F&& get) {
+  const uint32_t i = 2 * w;
+  const uint32_t lo = i < n ? uint32_t(get(i)) & 0xffffu : 0u;
+  const uint32_t hi = i + 1 < n ? uint32_t(get(i + 1)) & 0xffffu : 0u;
+  return lo | (hi << 16);
+}
+
+// One block per event.  The destination is host memory reached over the
+// bus, so every array is written as consecutive 32-bit words by consecutive
+// threads (whole lines per warp); the gathers come from device memory.
+__global__ void __launch_bounds__(512) kPackResults(Workspace ws, uint8_t* out) {
   __shared__ uint32_t scanSh[33];
+  __shared__ uint16_t sIdx[kResultTracks];
   __shared__ uint32_t sGuard;
   const uint32_t e = blockIdx.x;
   const EventCounters* c = ws.ev + e;
   uint8_t* base = out + size_t(e) * kResultStride;
-  ResultHeader* hdr = reinterpret_cast<ResultHeader*>(base);
-  ResultTracks trk = resultTracks(base);
-  ResultVertices vtx = resultVertices(base);
   const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
   const uint16_t* th = ws.tupleHits + size_t(e) * kTupleHitCap;
   const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
@@ -41,48 +61,71 @@ __global__ void kPackResults(Workspace ws, uint8_t* out) {
   const uint32_t guard = sGuard;
   uint32_t carry = 0;
   for (uint32_t t0 = 0; t0 < guard; t0 += blockDim.x) {
-    uint32_t t = t0 + threadIdx.x;
-    uint32_t loose = (t < guard && q[t] >= 2) ? 1u : 0u;
+    const uint32_t t = t0 + threadIdx.x;
+    const uint32_t loose = (t < guard && q[t] >= 2) ? 1u : 0u;
     uint32_t tot;
-    uint32_t pre = blockExclusiveScan(loose, scanSh, &tot);
-    uint32_t p = carry + pre;
-    if (loose && p < kResultTracks) {
-      uint32_t nh = toff[t + 1] - toff[t];
-      trk.tupleIndex[p] = t;
-      trk.nHits[p] = uint8_t(nh);
-      trk.quality[p] = q[t];
-      for (int k = 0; k < 5; ++k) trk.state[5 * p + k] = ws.state[tb * 5 + size_t(t) * 5 + k];
-      for (int k = 0; k < 15; ++k) trk.cov[15 * p + k] = ws.cov[tb * 15 + size_t(t) * 15 + k];
-      trk.pt[p] = ws.pt[tb + t];
-      trk.eta[p] = ws.eta[tb + t];
-      trk.chi2[p] = ws.chi2[tb + t];
-      for (uint32_t k = 0; k < 5; ++k) trk.hits[5 * p + k] = k < nh ? th[toff[t] + k] : uint16_t(0xffff);
-      trk.vertex[p] = c->nVertices > 0 ? ws.idv[tb + t] : int16_t(-1);
-    }
+    const uint32_t p = carry + blockExclusiveScan(loose, scanSh, &tot);
+    if (loose && p < kResultTracks) sIdx[p] = uint16_t(t);
     carry += tot;
   }
+  __syncthreads();
+  const uint32_t n = min(carry, kResultTracks);
+  const uint32_t T = blockDim.x;
+  uint32_t* w32 = reinterpret_cast<uint32_t*>(base + kResOffTupleIndex);
+  for (uint32_t j = threadIdx.x; j < n; j += T) w32[j] = sIdx[j];
+  w32 = reinterpret_cast<uint32_t*>(base + kResOffNHits);
+  for (uint32_t w = threadIdx.x; w < (n + 3) / 4; w += T)
+    w32[w] = packBytes(w, n, [&](uint32_t i) { return toff[sIdx[i] + 1] - toff[sIdx[i]]; });
+  w32 = reinterpret_cast<uint32_t*>(base + kResOffQuality);
+  for (uint32_t w = threadIdx.x; w < (n + 3) / 4; w += T)
+    w32[w] = packBytes(w, n, [&](uint32_t i) { return q[sIdx[i]]; });
+  float* f = reinterpret_cast<float*>(base + kResOffState);
+  for (uint32_t j = threadIdx.x; j < 5 * n; j += T) f[j] = ws.state[tb * 5 + size_t(sIdx[j / 5]) * 5 + j % 5];
+  f = reinterpret_cast<float*>(base + kResOffCov);
+  for (uint32_t j = threadIdx.x; j < 15 * n; j += T) f[j] = ws.cov[tb * 15 + size_t(sIdx[j / 15]) * 15 + j % 15];
+  f = reinterpret_cast<float*>(base + kResOffPt);
+  for (uint32_t j = threadIdx.x; j < n; j += T) f[j] = ws.pt[tb + sIdx[j]];
+  f = reinterpret_cast<float*>(base + kResOffEta);
+  for (uint32_t j = threadIdx.x; j < n; j += T) f[j] = ws.eta[tb + sIdx[j]];
+  f = reinterpret_cast<float*>(base + kResOffChi2);
+  for (uint32_t j = threadIdx.x; j < n; j += T) f[j] = ws.chi2[tb + sIdx[j]];
+  w32 = reinterpret_cast<uint32_t*>(base + kResOffHits);
+  for (uint32_t w = threadIdx.x; w < (5 * n + 1) / 2; w += T)
+    w32[w] = packHalves(w, 5 * n, [&](uint32_t i) {
+      const uint32_t t = sIdx[i / 5], k = i % 5;
+      return k < toff[t + 1] - toff[t] ? uint32_t(th[toff[t] + k]) : 0xffffu;
+    });
+  const bool hasVtx = c->nVertices > 0;
+  w32 = reinterpret_cast<uint32_t*>(base + kResOffVertex);
+  for (uint32_t w = threadIdx.x; w < (n + 1) / 2; w += T)
+    w32[w] = packHalves(w, n, [&](uint32_t i) { return hasVtx ? uint32_t(uint16_t(ws.idv[tb + sIdx[i]])) : 0xffffu; });
   const uint32_t nv = min(c->nVertices, uint32_t(kMaxVtx));
   const size_t vb = size_t(e) * kMaxVtx;
-  for (uint32_t v = threadIdx.x; v < nv; v += blockDim.x) {
+  ResultVertices vtx = resultVertices(base);
+  for (uint32_t v = threadIdx.x; v < nv; v += T) {
     vtx.zv[v] = ws.zv[vb + v];
     vtx.wv[v] = ws.wv[vb + v];
     vtx.chi2[v] = ws.vchi2[vb + v];
     vtx.ptv2[v] = ws.ptv2[vb + v];
     vtx.ndof[v] = ws.ndof[vb + v];
-    vtx.sortInd[v] = ws.sortInd[vb + v];
   }
+  w32 = reinterpret_cast<uint32_t*>(base + kResOffSortInd);
+  for (uint32_t w = threadIdx.x; w < (nv + 1) / 2; w += T)
+    w32[w] = packHalves(w, nv, [&](uint32_t i) { return uint32_t(ws.sortInd[vb + i]); });
   if (threadIdx.x == 0) {
-    hdr->nTracks = min(carry, kResultTracks);
-    hdr->nLooseAll = carry;
-    hdr->nVertices = nv;
-    hdr->nHits = c->nHits;
-    hdr->nTuples = guard;
-    hdr->nDigis = c->nWords;
-    hdr->nCells = c->nCells;
-    hdr->flags = c->flags | (carry > kResultTracks ? kFlagResultOverflow : 0u);
-    hdr->nEdges = c->nEdges;
-    hdr->nTupleHits = toff[guard];
-    hdr->nModules = c->nModules;
+    ResultHeader h{};
+    h.nTracks = n;
+    h.nLooseAll = carry;
+    h.nVertices = nv;
+    h.nHits = c->nHits;
+    h.nTuples = guard;
+    h.nDigis = c->nWords;
+    h.nCells = c->nCells;
+    h.flags = c->flags | (carry > kResultTracks ? kFlagResultOverflow : 0u);
+    h.nEdges = c->nEdges;
+    h.nTupleHits = toff[guard];
+    h.nModules = c->nModules;
+    *reinterpret_cast<ResultHeader*>(base) = h;
   }
 }
 
@@ -93,7 +136,7 @@ void launchSetInput(Workspace& ws, const uint32_t* words, const uint8_t* fedIds,
 }
 
 void launchPack(Workspace& ws, uint32_t nEvents, uint8_t* out, cudaStream_t s) {
-  PG_PROBED("kPackResults", s, kPackResults<<<nEvents, 256, 0, s>>>(ws, out));
+  PG_PROBED("kPackResults", s, kPackResults<<<nEvents, 512, 0, s>>>(ws, out));
 }
 
 }  // namespace pixgpu

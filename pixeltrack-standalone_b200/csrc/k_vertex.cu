@@ -11,6 +11,8 @@
 // serial order), histogram bins are scanned in the serial storage order
 // (descending track index inside a bin) and new split vertices are numbered
 // by a prefix over the parent vertex index.
+#include <atomic>
+
 #include "device_utils.cuh"
 #include "pixgpu_internal.cuh"
 
@@ -20,6 +22,11 @@ namespace {
 
 constexpr uint32_t kMaxVtxTracks = 32 * 1024;
 constexpr int kVtxThreads = 1024;
+// events with at most this many vertex tracks keep every per-track array in
+// shared memory (38 bytes per track); larger ones use the global scratch
+constexpr uint32_t kSmemTracks = 4096;
+constexpr size_t kTrackBytes = 8 * 4 + 2 * 2 + 2;
+constexpr size_t kVtxSmemBytes = kSmemTracks * kTrackBytes;
 
 struct VtxScratch {
   float *zt, *ezt2, *ptt2, *zz;
@@ -29,6 +36,23 @@ struct VtxScratch {
   uint32_t* list;    // tracks grouped by vertex
   uint16_t* hbins;   // z-histogram content
 };
+
+__device__ __forceinline__ VtxScratch carve(char* p, uint32_t cap) {
+  VtxScratch s;
+  s.zt = reinterpret_cast<float*>(p);
+  s.ezt2 = s.zt + cap;
+  s.ptt2 = s.ezt2 + cap;
+  s.zz = s.ptt2 + cap;
+  s.iv = reinterpret_cast<int32_t*>(s.zz + cap);
+  s.nn = s.iv + cap;
+  s.root = s.nn + cap;
+  s.list = reinterpret_cast<uint32_t*>(s.root + cap);
+  s.itrk = reinterpret_cast<uint16_t*>(s.list + cap);
+  s.hbins = s.itrk + cap;
+  s.izt = reinterpret_cast<uint8_t*>(s.hbins + cap);
+  s.newV = s.izt + cap;
+  return s;
+}
 
 __device__ __forceinline__ VtxScratch scratchOf(const Workspace& ws, uint32_t e) {
   // carve per-event scratch out of scratchA/scratchB (kEdgeCap words each)
@@ -73,21 +97,17 @@ __device__ void groupByVertex(const VtxScratch& s, uint32_t nt, uint32_t nv, uin
     carry += tot;
   }
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
-    int32_t v = s.iv[i];
-    if (v >= 0 && uint32_t(v) < nv) s.list[vOff[v] + atomicAdd(&vCur[v], 1u)] = i;
-  }
-  __syncthreads();
-  for (uint32_t v = threadIdx.x; v < nv; v += blockDim.x) {
-    uint32_t b = vOff[v], n = vOff[v + 1] - b;
-    for (uint32_t k = 1; k < n; ++k) {
-      uint32_t x = s.list[b + k];
-      int j = int(k) - 1;
-      while (j >= 0 && s.list[b + j] > x) {
-        s.list[b + j + 1] = s.list[b + j];
-        --j;
-      }
-      s.list[b + j + 1] = x;
+  // ordered fill: one warp per vertex walks the tracks in ascending order
+  const uint32_t lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (uint32_t v = threadIdx.x >> 5; v < nv; v += nw) {
+    uint32_t pos = vOff[v];
+    const uint32_t end = vOff[v + 1];
+    for (uint32_t i0 = 0; i0 < nt && pos < end; i0 += 32) {
+      const uint32_t i = i0 + lane;
+      const bool in = i < nt && s.iv[i] == int32_t(v);
+      const uint32_t m = __ballot_sync(0xffffffffu, in);
+      if (in) s.list[pos + __popc(m & lanemaskLt())] = i;
+      pos += __popc(m);
     }
   }
   __syncthreads();
@@ -130,13 +150,14 @@ __device__ void fitVertices(const VtxScratch& s, uint32_t nt, uint32_t nv, float
 }
 
 __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
+  extern __shared__ __align__(16) char vsm[];
   __shared__ uint32_t scanSh[33];
   __shared__ uint32_t hoff[257], hcur[257];
   __shared__ uint32_t vOff[kMaxVtx + 1], vCur[kMaxVtx + 1];
   __shared__ uint32_t sNt, sFound, sGuard, sNv;
   const uint32_t e = blockIdx.x;
+  const uint32_t lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   EventCounters* c = ws.ev + e;
-  VtxScratch s = scratchOf(ws, e);
   const uint32_t nTuples = c->nTuples;
   const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
   const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
@@ -159,20 +180,37 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
   }
   __syncthreads();
   const uint32_t guard = sGuard;
+  auto selected = [&](uint32_t t) {
+    const uint32_t nh = toff[t + 1] - toff[t];
+    return nh >= 4 && q[t] == 2 && !(pt[t] < 0.5f);
+  };
+  // count first: the count decides where the per-track arrays live
   {
     uint32_t carry = 0;
     for (uint32_t t0 = 0; t0 < guard; t0 += blockDim.x) {
-      uint32_t t = t0 + threadIdx.x;
+      const uint32_t t = t0 + threadIdx.x;
       uint32_t sel = 0;
       if (t < guard) {
         idv[t] = -1;
-        uint32_t nh = toff[t + 1] - toff[t];
-        sel = (nh >= 4 && q[t] == 2 && !(pt[t] < 0.5f)) ? 1u : 0u;
+        sel = selected(t) ? 1u : 0u;
       }
       uint32_t tot;
-      uint32_t pre = blockExclusiveScan(sel, scanSh, &tot);
+      blockExclusiveScan(sel, scanSh, &tot);
+      carry += tot;
+    }
+    if (threadIdx.x == 0) sNt = min(carry, kMaxVtxTracks);
+  }
+  __syncthreads();
+  const VtxScratch s = sNt <= kSmemTracks ? carve(vsm, kSmemTracks) : scratchOf(ws, e);
+  {
+    uint32_t carry = 0;
+    for (uint32_t t0 = 0; t0 < guard; t0 += blockDim.x) {
+      const uint32_t t = t0 + threadIdx.x;
+      const uint32_t sel = (t < guard && selected(t)) ? 1u : 0u;
+      uint32_t tot;
+      const uint32_t pre = blockExclusiveScan(sel, scanSh, &tot);
       if (sel) {
-        uint32_t it = carry + pre;
+        const uint32_t it = carry + pre;
         if (it < kMaxVtxTracks) {
           s.itrk[it] = uint16_t(t);
           s.zt[it] = st[size_t(t) * 5 + 4];
@@ -182,7 +220,6 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
       }
       carry += tot;
     }
-    if (threadIdx.x == 0) sNt = min(carry, kMaxVtxTracks);
   }
   __syncthreads();
   const uint32_t nt = sNt;
@@ -216,22 +253,17 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
     }
   }
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
-    uint32_t b = s.izt[i];
-    s.hbins[hoff[b] + atomicAdd(&hcur[b], 1u)] = uint16_t(i);
-  }
-  __syncthreads();
-  // the serial fill stores each bin in descending track order
-  for (uint32_t b = threadIdx.x; b < 256; b += blockDim.x) {
-    uint32_t o = hoff[b], n = hoff[b + 1] - o;
-    for (uint32_t k = 1; k < n; ++k) {
-      uint16_t x = s.hbins[o + k];
-      int j = int(k) - 1;
-      while (j >= 0 && s.hbins[o + j] < x) {
-        s.hbins[o + j + 1] = s.hbins[o + j];
-        --j;
-      }
-      s.hbins[o + j + 1] = x;
+  // the serial fill stores each bin in descending track order: one warp per
+  // bin walks the tracks from the last one down
+  for (uint32_t b = threadIdx.x >> 5; b < 256; b += nw) {
+    uint32_t pos = hoff[b];
+    const uint32_t end = hoff[b + 1];
+    for (uint32_t r0 = 0; r0 < nt && pos < end; r0 += 32) {
+      const uint32_t r = r0 + lane;
+      const bool in = r < nt && s.izt[nt - 1 - r] == b;
+      const uint32_t m = __ballot_sync(0xffffffffu, in);
+      if (in) s.hbins[pos + __popc(m & lanemaskLt())] = uint16_t(nt - 1 - r);
+      pos += __popc(m);
     }
   }
   __syncthreads();
@@ -437,7 +469,17 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
 }  // namespace
 
 cudaError_t runVertices(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
-  PG_PROBED("kVertices", stream, kVertices<<<nEvents, kVtxThreads, 0, stream>>>(ws));
+  // opt in to the large shared-memory carve-out, once per device
+  static std::atomic<uint64_t> configured{0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const uint64_t bit = uint64_t(1) << (dev & 63);
+  if (!(configured.load() & bit)) {
+    cudaError_t e = cudaFuncSetAttribute(kVertices, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kVtxSmemBytes));
+    if (e != cudaSuccess) return e;
+    configured.fetch_or(bit);
+  }
+  PG_PROBED("kVertices", stream, kVertices<<<nEvents, kVtxThreads, kVtxSmemBytes, stream>>>(ws));
   return cudaGetLastError();
 }
 

@@ -26,6 +26,7 @@ constexpr uint32_t kH2TCap = 4 * PF_MAX_TUPLES;          // HitToTuple capacity 
 constexpr uint32_t kMaxVtx = PF_MAX_VTX;
 constexpr uint32_t kErrCap = 4096;                       // digi errors kept per event
 constexpr uint32_t kMaxFedWords = PF_MAX_FED_WORDS;      // 300000 words per event
+constexpr uint32_t kBigSegCap = 8192;                    // long list segments queued per event and sort
 
 // flag bits in EventCounters::flags (capacity conditions where the result no
 // longer follows the reference's truncation order exactly)
@@ -68,6 +69,7 @@ struct EventCounters {
   uint32_t nErrors;
   uint32_t nVtxTracks;
   uint32_t flags;
+  uint32_t nBig[4];             // long segments queued by each list ordering
   uint32_t pad[2];
 };
 
@@ -119,6 +121,7 @@ struct Workspace {
   uint16_t* detInd;
   uint32_t* phiOff;          // [maxEvents][kPhiStride]
   uint16_t* phiBins;         // [maxEvents][kHitCap]
+  uint4* phiRec;             // [maxEvents][kHitCap] hit records in phiBins order: z, r, iphi|ysize<<16, detInd|hit<<16
   PfAverageGeometry* agc;    // [maxEvents]
   // doublets
   uint32_t* jCount;          // [maxEvents][kJCap + 1]
@@ -132,6 +135,7 @@ struct Workspace {
   uint32_t* ohCount;         // [maxEvents][kHitCap + 1]
   uint32_t* ohOff;           // [maxEvents][kHitCap + 1]
   uint32_t* ohCells;         // [maxEvents][kCellCap]
+  float4* ohRec;             // [maxEvents][kCellCap] inner hit of each ohCells entry: x, y, z, +-r (- : dca region inner)
   // CA neighbour links (outerNeighbors), CSR sorted ascending
   uint32_t* nbrCount;        // [maxEvents][kCellCap + 1]
   uint32_t* nbrOff;          // [maxEvents][kCellCap + 1]
@@ -170,6 +174,7 @@ struct Workspace {
   uint32_t* scratchB;        // [maxEvents][kEdgeCap]
   // scan scratch
   uint32_t* scanTmp;         // [maxEvents][kScanTmpStride]
+  uint32_t* bigSeg;          // [maxEvents][kBigSegCap] long segments awaiting the block sort
 };
 
 constexpr uint32_t kScanChunk = 4096;

@@ -73,6 +73,7 @@ void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W) {
   c.take(ws.ohOff, size_t(E) * (kHitCap + 1));
   c.take(ws.ohCells, C);
   c.take(ws.ohRec, C);
+  c.take(ws.ohDet, C);
   size_t C1 = size_t(E) * (kCellCap + 1);
   c.take(ws.nbrCount, C1);
   c.take(ws.nbrOff, C1);

@@ -200,6 +200,44 @@ __device__ __forceinline__ uint32_t warpDoublets(const DoubletSeed& d, const uin
   return n;
 }
 
+// Each warp looks at 32 slots at once: every lane evaluates one slot's seed
+// cuts, then the warp walks the candidate ranges of the surviving slots one
+// after the other.  Warp w takes slots w, w + S, w + 2S, ... (S warps per
+// event), so that dense runs of consecutive slots spread over the warps.
+template <typename PerSlot>
+__device__ __forceinline__ void forSeedSlots(const PairTable& pt, const HitsView& hh, uint32_t ntot,
+                                             PerSlot&& perSlot) {
+  const uint32_t lane = laneId(), wpb = blockDim.x >> 5;
+  const uint32_t S = gridDim.x * wpb, w = blockIdx.x * wpb + (threadIdx.x >> 5);
+  for (uint32_t r0 = 0; w + r0 * S < ntot; r0 += 32) {
+    const uint32_t j = w + (r0 + lane) * S;
+    DoubletSeed d;
+    const bool live = j < ntot && doubletSeed(pt, hh, j, d) && (d.e0 > d.b0 || d.e1 > d.b1);
+    uint32_t m = __ballot_sync(0xffffffffu, live);
+    perSlot(j, live, d, 0u);  // every lane sees its own slot first
+    while (m) {
+      const int l = __ffs(m) - 1;
+      m &= m - 1;
+      DoubletSeed ds;
+      ds.pair = __shfl_sync(0xffffffffu, d.pair, l);
+      ds.inner = __shfl_sync(0xffffffffu, d.inner, l);
+      ds.outer = __shfl_sync(0xffffffffu, d.outer, l);
+      ds.i = __shfl_sync(0xffffffffu, d.i, l);
+      ds.mez = __shfl_sync(0xffffffffu, d.mez, l);
+      ds.mer = __shfl_sync(0xffffffffu, d.mer, l);
+      ds.mep = int16_t(__shfl_sync(0xffffffffu, int(d.mep), l));
+      ds.mes = int16_t(__shfl_sync(0xffffffffu, int(d.mes), l));
+      ds.iphicut = int16_t(__shfl_sync(0xffffffffu, int(d.iphicut), l));
+      ds.maxr = __shfl_sync(0xffffffffu, d.maxr, l);
+      ds.b0 = __shfl_sync(0xffffffffu, d.b0, l);
+      ds.e0 = __shfl_sync(0xffffffffu, d.e0, l);
+      ds.b1 = __shfl_sync(0xffffffffu, d.b1, l);
+      ds.e1 = __shfl_sync(0xffffffffu, d.e1, l);
+      perSlot(w + (r0 + uint32_t(l)) * S, true, ds, 1u + uint32_t(l));
+    }
+  }
+}
+
 __global__ void kDoubletCount(Workspace ws) {
   __shared__ PairTable pt;
   const uint32_t e = blockIdx.y;
@@ -209,13 +247,14 @@ __global__ void kDoubletCount(Workspace ws) {
   const HitsView hh = hitsOf(ws, e);
   const uint4* rec = ws.phiRec + size_t(e) * kHitCap;
   uint32_t* cnt = ws.jCount + size_t(e) * (kJCap + 1);
-  const uint32_t wpb = blockDim.x >> 5;
-  for (uint32_t j = blockIdx.x * wpb + (threadIdx.x >> 5); j < ntot; j += gridDim.x * wpb) {
-    DoubletSeed d;
-    uint32_t n = 0;
-    if (doubletSeed(pt, hh, j, d)) n = warpDoublets(d, rec, [](uint32_t, uint16_t) {});
-    if (laneId() == 0) cnt[j] = n;
-  }
+  forSeedSlots(pt, hh, ntot, [&](uint32_t j, bool live, const DoubletSeed& d, uint32_t phase) {
+    if (phase == 0) {
+      if (j < ntot && !live) cnt[j] = 0;
+      return;
+    }
+    const uint32_t n = warpDoublets(d, rec, [](uint32_t, uint16_t) {});
+    if (laneId() == phase - 1) cnt[j] = n;
+  });
 }
 
 __global__ void kDoubletWrite(Workspace ws) {
@@ -229,12 +268,10 @@ __global__ void kDoubletWrite(Workspace ws) {
   const uint32_t* off = ws.jOffset + size_t(e) * (kJCap + 1);
   const size_t cb = size_t(e) * kCellCap;
   uint32_t* ohc = ws.ohCount + size_t(e) * (kHitCap + 1);
-  const uint32_t wpb = blockDim.x >> 5;
-  for (uint32_t j = blockIdx.x * wpb + (threadIdx.x >> 5); j < ntot; j += gridDim.x * wpb) {
+  forSeedSlots(pt, hh, ntot, [&](uint32_t j, bool live, const DoubletSeed& d, uint32_t phase) {
+    if (phase == 0) return;
     const uint32_t base = off[j];
-    if (base >= kCellCap || off[j + 1] == base) continue;
-    DoubletSeed d;
-    if (!doubletSeed(pt, hh, j, d)) continue;
+    if (base >= kCellCap || off[j + 1] == base) return;
     const float zi = hh.zg[d.i], ri = hh.rg[d.i];
     warpDoublets(d, rec, [&](uint32_t k, uint16_t oi) {
       const uint32_t idx = base + k;
@@ -249,7 +286,7 @@ __global__ void kDoubletWrite(Workspace ws) {
         atomicAdd(&ohc[oi], 1u);
       }
     });
-  }
+  });
 }
 
 __global__ void kCellsTotal(Workspace ws, uint32_t nEvents) {
@@ -336,17 +373,20 @@ __global__ void kOhRec(Workspace ws) {
     const uint32_t oc = ws.ohCells[cb + p];
     const uint16_t ih = ws.cellInner[cb + oc];
     const float r = ws.cellInnerR[cb + oc];
-    ws.ohRec[cb + p] = make_float4(ws.xg[hb + ih], ws.yg[hb + ih], ws.cellInnerZ[cb + oc],
-                                   ws.detInd[hb + ih] < 96 ? -r : r);
+    const uint16_t det = ws.detInd[hb + ih];
+    ws.ohRec[cb + p] = make_float4(ws.xg[hb + ih], ws.yg[hb + ih], ws.cellInnerZ[cb + oc], det < 96 ? -r : r);
+    ws.ohDet[cb + p] = det;
   }
 }
 
 // kernel_connect (CAHitNtupletGeneratorKernelsImpl.h:191-262) by doublet
 // slot: the cells of slot j share their inner hit h, so they share the
 // candidate list (cells ending on h, first 128 in ascending order).  A warp
-// takes a slot: each lane holds up to one candidate per round of 32 and the
-// slot's cells are visited one after the other.  Accepted links (oc <- idx)
-// are appended unordered, one atomic per warp and cell.
+// looks at 32 slots at once (warp w: slots w, w + S, ...) and takes the
+// non-empty ones in turn; for a slot, lane t stages the outer hit of cell t,
+// lane k holds candidate k of the current round of 32, and the cells are
+// tested one after the other against all candidates.  Accepted links
+// (oc <- idx) are appended unordered with one atomic per warp and cell.
 __global__ void kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
   const uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
@@ -362,54 +402,81 @@ __global__ void kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
   uint32_t* eOc = edgeOc + size_t(e) * kEdgeCap;
   uint32_t* eIdx = edgeIdx + size_t(e) * kEdgeCap;
   const uint32_t lane = laneId(), wpb = blockDim.x >> 5;
-  for (uint32_t j = blockIdx.x * wpb + (threadIdx.x >> 5); j < ntot; j += gridDim.x * wpb) {
-    const uint32_t base = joff[j];
-    const uint32_t end = min(joff[j + 1], nCells);
-    if (base >= end) continue;
-    const uint16_t h = ws.cellInner[cb + base];
-    const uint32_t ob = ohOff[h];
-    const uint32_t m = min(ohOff[h + 1] - ob, uint32_t(PF_MAX_CELLS_PER_HIT));
-    if (m == 0) continue;
-    const float ri = ws.cellInnerR[cb + base], zi = ws.cellInnerZ[cb + base];
-    const float thetaCut = hh.detInd[h] < 1184 ? kThetaCutBarrel : kThetaCutForward;
-    const float x2 = hh.xg[h], y2 = hh.yg[h];
-    for (uint32_t k0 = 0; k0 < m; k0 += 32) {
-      const uint32_t k = k0 + lane;
-      float4 r1 = make_float4(0.f, 0.f, 0.f, 0.f);
-      uint32_t oc = 0;
-      if (k < m) {
-        r1 = ohRec[ob + k];
-        oc = ohCells[ob + k];
+  const uint32_t S = gridDim.x * wpb, w = blockIdx.x * wpb + (threadIdx.x >> 5);
+  for (uint32_t r0 = 0; w + r0 * S < ntot; r0 += 32) {
+    const uint32_t jl = w + (r0 + lane) * S;
+    uint32_t myBase = 0, myEnd = 0, myOb = 0, myM = 0;
+    if (jl < ntot) {
+      myBase = joff[jl];
+      myEnd = min(joff[jl + 1], nCells);
+      if (myBase < myEnd) {
+        const uint16_t h = ws.cellInner[cb + myBase];
+        myOb = ohOff[h];
+        myM = min(ohOff[h + 1] - myOb, uint32_t(PF_MAX_CELLS_PER_HIT));
       }
-      const float region = r1.w < 0.f ? kDcaCutInner : kDcaCutOuter;
-      const float rr1 = fabsf(r1.w);
-      bool usedOc = false;
-      for (uint32_t idx = base; idx < end; ++idx) {
-        const uint16_t oh = ws.cellOuter[cb + idx];
-        const float ro = hh.rg[oh], zo = hh.zg[oh], x3 = hh.xg[oh], y3 = hh.yg[oh];
-        const bool ok = k < m && alignedRZ(rr1, r1.z, ri, zi, ro, zo, thetaCut) &&
-                        dcaCut(r1.x, r1.y, x2, y2, x3, y3, region);
-        const uint32_t mask = __ballot_sync(0xffffffffu, ok);
-        if (mask == 0) continue;
-        uint32_t at = 0;
-        if (lane == 0) {
-          at = atomicAdd(&c->nEdges, uint32_t(__popc(mask)));
-          ws.cellUsed[cb + idx] = 1;
+    }
+    uint32_t live = __ballot_sync(0xffffffffu, myBase < myEnd && myM > 0);
+    while (live) {
+      const int l = __ffs(live) - 1;
+      live &= live - 1;
+      const uint32_t base = __shfl_sync(0xffffffffu, myBase, l);
+      const uint32_t end = __shfl_sync(0xffffffffu, myEnd, l);
+      const uint32_t ob = __shfl_sync(0xffffffffu, myOb, l);
+      const uint32_t m = __shfl_sync(0xffffffffu, myM, l);
+      const uint16_t h = ws.cellInner[cb + base];
+      const float ri = ws.cellInnerR[cb + base], zi = ws.cellInnerZ[cb + base];
+      const float thetaCut = hh.detInd[h] < 1184 ? kThetaCutBarrel : kThetaCutForward;
+      const float x2 = hh.xg[h], y2 = hh.yg[h];
+      for (uint32_t c0 = base; c0 < end; c0 += 32) {
+        const uint32_t nc = min(32u, end - c0);
+        float sro = 0.f, szo = 0.f, sx3 = 0.f, sy3 = 0.f;
+        if (lane < nc) {
+          const uint16_t oh = ws.cellOuter[cb + c0 + lane];
+          sro = hh.rg[oh];
+          szo = hh.zg[oh];
+          sx3 = hh.xg[oh];
+          sy3 = hh.yg[oh];
         }
-        at = __shfl_sync(0xffffffffu, at, 0);
-        if (ok) {
-          usedOc = true;
-          atomicAdd(&nbrCnt[oc], 1u);
-          const uint32_t slot = at + __popc(mask & lanemaskLt());
-          if (slot < kEdgeCap) {
-            eOc[slot] = oc;
-            eIdx[slot] = idx;
-          } else {
-            atomicOr(&c->flags, kFlagEdgeOverflow);
+        for (uint32_t k0 = 0; k0 < m; k0 += 32) {
+          const uint32_t k = k0 + lane;
+          float4 r1 = make_float4(0.f, 0.f, 0.f, 0.f);
+          uint32_t oc = 0;
+          if (k < m) {
+            r1 = ohRec[ob + k];
+            oc = ohCells[ob + k];
           }
+          const float region = r1.w < 0.f ? kDcaCutInner : kDcaCutOuter;
+          const float rr1 = fabsf(r1.w);
+          bool usedOc = false;
+          for (uint32_t t = 0; t < nc; ++t) {
+            const float ro = __shfl_sync(0xffffffffu, sro, t), zo = __shfl_sync(0xffffffffu, szo, t);
+            const float x3 = __shfl_sync(0xffffffffu, sx3, t), y3 = __shfl_sync(0xffffffffu, sy3, t);
+            const bool ok = k < m && alignedRZ(rr1, r1.z, ri, zi, ro, zo, thetaCut) &&
+                            dcaCut(r1.x, r1.y, x2, y2, x3, y3, region);
+            const uint32_t mask = __ballot_sync(0xffffffffu, ok);
+            if (mask == 0) continue;
+            const uint32_t idx = c0 + t;
+            uint32_t at = 0;
+            if (lane == 0) {
+              at = atomicAdd(&c->nEdges, uint32_t(__popc(mask)));
+              ws.cellUsed[cb + idx] = 1;
+            }
+            at = __shfl_sync(0xffffffffu, at, 0);
+            if (ok) {
+              usedOc = true;
+              atomicAdd(&nbrCnt[oc], 1u);
+              const uint32_t slot = at + __popc(mask & lanemaskLt());
+              if (slot < kEdgeCap) {
+                eOc[slot] = oc;
+                eIdx[slot] = idx;
+              } else {
+                atomicOr(&c->flags, kFlagEdgeOverflow);
+              }
+            }
+          }
+          if (usedOc) ws.cellUsed[cb + oc] = 1;
         }
       }
-      if (usedOc) ws.cellUsed[cb + oc] = 1;
     }
   }
 }
@@ -442,47 +509,68 @@ __global__ void kNbrPool(Workspace ws) {
 
 // ------------------------------------------------------------------ fishbone
 
-// one warp per hit with >= 2 cells ending on it
-__global__ void kFishbone(Workspace ws) {
-  uint32_t e = blockIdx.y;
+// gpuFishbone.h:21-90 (early fishbone), one warp per hit with >= 2 cells
+// ending on it.  The hit's cells (first 128, ascending) are staged in shared
+// memory from the isOuterHitOfCell-ordered records; lane ic compares cell ic
+// with every later cell, as the serial double loop does.  Kills only write
+// doubletId = -1 and never change the `used` flags the loop reads, so the
+// lanes are independent.
+constexpr int kFishWarps = 8;
+__global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws) {
+  __shared__ float sxA[kFishWarps][PF_MAX_CELLS_PER_HIT], syA[kFishWarps][PF_MAX_CELLS_PER_HIT],
+      szA[kFishWarps][PF_MAX_CELLS_PER_HIT];
+  __shared__ uint16_t sdA[kFishWarps][PF_MAX_CELLS_PER_HIT];
+  __shared__ uint8_t suA[kFishWarps][PF_MAX_CELLS_PER_HIT];
+  const uint32_t e = blockIdx.y;
   const EventCounters* c = ws.ev + e;
-  uint32_t nHits = c->nHits;
+  const uint32_t nHits = c->nHits;
   if (nHits < 2) return;
-  HitsView hh = hitsOf(ws, e);
-  size_t cb = size_t(e) * kCellCap;
+  const HitsView hh = hitsOf(ws, e);
+  const size_t cb = size_t(e) * kCellCap;
   const uint32_t* ohOff = ws.ohOff + size_t(e) * (kHitCap + 1);
   const uint32_t* ohCells = ws.ohCells + cb;
-  uint32_t wpb = blockDim.x >> 5;
-  for (uint32_t h = blockIdx.x * wpb + (threadIdx.x >> 5); h < nHits; h += gridDim.x * wpb) {
-    uint32_t b = ohOff[h], s = min(ohOff[h + 1] - b, uint32_t(PF_MAX_CELLS_PER_HIT));
+  const float4* ohRec = ws.ohRec + cb;
+  const uint16_t* ohDet = ws.ohDet + cb;
+  const uint32_t w = threadIdx.x >> 5, lane = laneId();
+  float* sx = sxA[w];
+  float* sy = syA[w];
+  float* sz = szA[w];
+  uint16_t* sd = sdA[w];
+  uint8_t* su = suA[w];
+  for (uint32_t h = blockIdx.x * kFishWarps + w; h < nHits; h += gridDim.x * kFishWarps) {
+    const uint32_t b = ohOff[h], s = min(ohOff[h + 1] - b, uint32_t(PF_MAX_CELLS_PER_HIT));
     if (s < 2) continue;
-    uint16_t oh = ws.cellOuter[cb + ohCells[b]];
-    float xo = hh.xg[oh], yo = hh.yg[oh], zo = hh.zg[oh];
-    for (uint32_t ic = laneId(); ic < s; ic += 32) {
-      uint32_t ci = ohCells[b + ic];
-      if (0 == ws.cellUsed[cb + ci]) continue;
-      uint16_t ih = ws.cellInner[cb + ci];
-      uint16_t di = hh.detInd[ih];
-      float xi = hh.xg[ih] - xo, yi = hh.yg[ih] - yo, zi = ws.cellInnerZ[cb + ci] - zo;
-      float ni = xi * xi + yi * yi + zi * zi;
+    const float xo = hh.xg[h], yo = hh.yg[h], zo = hh.zg[h];
+    for (uint32_t k = lane; k < s; k += 32) {
+      const float4 r = ohRec[b + k];
+      sx[k] = r.x - xo;
+      sy[k] = r.y - yo;
+      sz[k] = r.z - zo;
+      sd[k] = ohDet[b + k];
+      su[k] = ws.cellUsed[cb + ohCells[b + k]];
+    }
+    __syncwarp();
+    for (uint32_t ic = lane; ic < s; ic += 32) {
+      if (0 == su[ic]) continue;
+      const float xi = sx[ic], yi = sy[ic], zi = sz[ic];
+      const uint16_t di = sd[ic];
+      const float ni = xi * xi + yi * yi + zi * zi;
       for (uint32_t jc = ic + 1; jc < s; ++jc) {
-        uint32_t cj = ohCells[b + jc];
-        if (0 == ws.cellUsed[cb + cj]) continue;
-        uint16_t jh = ws.cellInner[cb + cj];
-        uint16_t dj = hh.detInd[jh];
-        float xj = hh.xg[jh] - xo, yj = hh.yg[jh] - yo, zj = ws.cellInnerZ[cb + cj] - zo;
-        float nj = xj * xj + yj * yj + zj * zj;
-        float cos12 = xi * xj + yi * yj + zi * zj;
-        if (di != dj && cos12 * cos12 >= 0.99999f * ni * nj) {
+        if (0 == su[jc]) continue;
+        const float xj = sx[jc], yj = sy[jc], zj = sz[jc];
+        const float nj = xj * xj + yj * yj + zj * zj;
+        const float cos12 = xi * xj + yi * yj + zi * zj;
+        if (di != sd[jc] && cos12 * cos12 >= 0.99999f * ni * nj) {
           if (ni > nj) {
-            ws.cellDoubletId[cb + ci] = -1;
+            ws.cellDoubletId[cb + ohCells[b + ic]] = -1;
             break;
           } else {
-            ws.cellDoubletId[cb + cj] = -1;
+            ws.cellDoubletId[cb + ohCells[b + jc]] = -1;
           }
         }
       }
     }
+    __syncwarp();
   }
 }
 
@@ -814,75 +902,71 @@ __global__ void kFastDupInDegree(Workspace ws, uint32_t* indeg, const uint32_t* 
   }
 }
 
-__device__ __forceinline__ uint32_t candIndex(const uint32_t* cand, uint32_t nc, uint32_t cell) {
-  uint32_t lo = 0, hi = nc;
-  while (lo < hi) {
-    uint32_t mid = (lo + hi) >> 1;
-    if (cand[mid] < cell)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  return lo;
-}
-
+// One block per event.  A worklist holds the candidates whose earlier
+// track-sharing candidates are all done; cells of one round share no track,
+// so they are processed in parallel, and each releases its later neighbours
+// (the in-degree reaching zero queues them for the next round).
 constexpr int kFastDupThreads = 1024;
-__global__ void __launch_bounds__(kFastDupThreads) kFastDupRounds(Workspace ws, uint32_t* indeg, uint8_t* state,
-                                                                   const uint32_t* candFlag) {
-  uint32_t e = blockIdx.x;
-  uint32_t nc = ws.ev[e].nCandidates;
+__global__ void __launch_bounds__(kFastDupThreads) kFastDupRounds(Workspace ws, uint32_t* indeg, uint32_t* lists,
+                                                                   const uint32_t* candFlag, const uint32_t* candOff) {
+  __shared__ uint32_t sN[2];
+  const uint32_t e = blockIdx.x;
+  const uint32_t nc = ws.ev[e].nCandidates;
   const uint32_t* cand = ws.candidates + size_t(e) * kCellCap;
   const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
   const uint16_t* trk = ws.trk + size_t(e) * kTupleCellCap;
   const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
   const uint32_t* tcell = ws.tupleCells + size_t(e) * kTupleCellCap;
   const uint32_t* flag = candFlag + size_t(e) * (kCellCap + 1);
+  const uint32_t* cidx = candOff + size_t(e) * (kCellCap + 1);
   uint32_t* deg = indeg + size_t(e) * kCellCap;
-  uint8_t* st = state + size_t(e) * kCellCap;  // 0 pending, 1 ready this round, 2 done
+  uint32_t* L[2] = {lists + size_t(e) * kEdgeCap, lists + size_t(e) * kEdgeCap + kCellCap};
   uint8_t* q = ws.quality + size_t(e) * kTupleBins;
   const float* tip = ws.state + size_t(e) * kTupleBins * 5 + 1;
-  for (uint32_t k = threadIdx.x; k < nc; k += blockDim.x) st[k] = 0;
+  if (threadIdx.x < 2) sN[threadIdx.x] = 0;
   __syncthreads();
-  for (uint32_t round = 0; round < nc + 1; ++round) {
-    int any = 0;
-    for (uint32_t k = threadIdx.x; k < nc; k += blockDim.x) {
-      if (st[k] == 0 && deg[k] == 0) {
-        st[k] = 1;
-        any = 1;
-      }
-    }
-    if (!__syncthreads_or(any)) break;
-    for (uint32_t k = threadIdx.x; k < nc; k += blockDim.x) {
-      if (st[k] != 1) continue;
-      uint32_t cell = cand[k];
-      uint32_t b = off[cell], s = trkListSize(off, cell);
+  for (uint32_t k = threadIdx.x; k < nc; k += blockDim.x)
+    if (deg[k] == 0) L[0][atomicAdd(&sN[0], 1u)] = k;
+  __syncthreads();
+  int cur = 0;
+  for (;;) {
+    const uint32_t n = sN[cur];
+    if (n == 0) break;
+    const uint32_t* Lc = L[cur];
+    uint32_t* Ln = L[cur ^ 1];
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+      const uint32_t cell = cand[Lc[i]];
+      const uint32_t b = off[cell], s = trkListSize(off, cell);
       float mc = 10000.f;
       uint16_t im = 60000;
       for (uint32_t j = 0; j < s; ++j) {
-        uint16_t t = trk[b + j];
-        float score = fabsf(tip[size_t(t) * 5]);
+        const uint16_t t = trk[b + j];
+        const float score = fabsf(tip[size_t(t) * 5]);
         if (q[t] == kLoose && score < mc) {
           mc = score;
           im = t;
         }
       }
       for (uint32_t j = 0; j < s; ++j) {
-        uint16_t t = trk[b + j];
+        const uint16_t t = trk[b + j];
         if (q[t] != kBad && t != im) q[t] = kDup;
       }
       // release later candidates sharing a track
       for (uint32_t j = 0; j < s; ++j) {
-        uint16_t t = trk[b + j];
-        uint32_t ncell = tupleSize(toff, t) - 1;
+        const uint16_t t = trk[b + j];
+        const uint32_t ncell = tupleSize(toff, t) - 1;
         for (uint32_t qq = 0; qq < ncell; ++qq) {
-          uint32_t o = tcell[4 * t + qq];
-          if (o > cell && flag[o] && inTrkList(off, trk, o, t)) atomicSub(&deg[candIndex(cand, nc, o)], 1u);
+          const uint32_t o = tcell[4 * t + qq];
+          if (o > cell && flag[o] && inTrkList(off, trk, o, t)) {
+            const uint32_t ko = cidx[o];
+            if (atomicSub(&deg[ko], 1u) == 1u) Ln[atomicAdd(&sN[cur ^ 1], 1u)] = ko;
+          }
         }
       }
     }
     __syncthreads();
-    for (uint32_t k = threadIdx.x; k < nc; k += blockDim.x)
-      if (st[k] == 1) st[k] = 2;
+    if (threadIdx.x == 0) sN[cur] = 0;
+    cur ^= 1;
     __syncthreads();
   }
 }
@@ -995,12 +1079,12 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   // ---- early fishbone
   PG_PROBED("kFishbone", stream, kFishbone<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws));
   // ---- n-tuplets: DFS count, scans, DFS write, finalize
-  PG_PROBED("kNtupletCount", stream, kNtupletCount<<<g, 128, 0, stream>>>(ws));
+  PG_PROBED("kNtupletCount", stream, kNtupletCount<<<dim3(gx * 8, nEvents), 128, 0, stream>>>(ws));
   segScan(ws.startTupleCount, ws.startTupleOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcM), ws.scanTmp, nEvents,
           stream);
   segScan(ws.startHitCount, ws.startHitOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcN), ws.scanTmp, nEvents,
           stream);
-  PG_PROBED("kNtupletWrite", stream, kNtupletWrite<<<g, 128, 0, stream>>>(ws));
+  PG_PROBED("kNtupletWrite", stream, kNtupletWrite<<<dim3(gx * 8, nEvents), 128, 0, stream>>>(ws));
   PG_PROBED("kTupleFinalize", stream, kTupleFinalize<<<dim3(32, nEvents), 1024, 0, stream>>>(ws));
   // ---- cell -> track lists
   PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trkCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
@@ -1030,10 +1114,11 @@ cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   PG_PROBED("kClassify", stream, kClassify<<<g, 256, 0, stream>>>(ws));
   // fastDuplicateRemover (candFlag survives in startTupleCount from runCA)
   uint32_t* candFlag = ws.startTupleCount;
-  uint32_t* indeg = ws.scratchA;                                 // [maxEvents][kEdgeCap] >= kCellCap
-  uint8_t* state = reinterpret_cast<uint8_t*>(ws.scratchB);
+  uint32_t* candOff = ws.startHitCount;  // candidate index of each cell, from runCA
+  uint32_t* indeg = ws.scratchA;        // [maxEvents][kEdgeCap] >= kCellCap
+  uint32_t* lists = ws.scratchB;        // two worklists of kCellCap per event
   PG_PROBED("kFastDupInDegree", stream, kFastDupInDegree<<<g, 256, 0, stream>>>(ws, indeg, candFlag));
-  PG_PROBED("kFastDupRounds", stream, kFastDupRounds<<<nEvents, kFastDupThreads, 0, stream>>>(ws, indeg, state, candFlag));
+  PG_PROBED("kFastDupRounds", stream, kFastDupRounds<<<nEvents, kFastDupThreads, 0, stream>>>(ws, indeg, lists, candFlag, candOff));
   // hit -> tuple map and triplet cleaner
   PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
   PG_PROBED("kHitToTupleCount", stream, kHitToTupleCount<<<g, 256, 0, stream>>>(ws));

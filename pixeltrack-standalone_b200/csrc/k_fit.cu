@@ -500,11 +500,18 @@ __device__ void blFit(const double* H3, const float* ge, double B, FitOut& out) 
 }
 
 // zero the fit results of every stored tuple (the reference's TrackSoA is value-initialised)
+// Tuples that no fit writes get zero fit results: those kept out of the
+// multiplicity bins (duplicates), and every tuple of an event whose bins
+// overflowed (the fits then cover an order-dependent subset).
 __global__ void kFitZero(Workspace ws) {
-  uint32_t e = blockIdx.y;
-  uint32_t nt = ws.ev[e].nTuples;
-  size_t tb = size_t(e) * kTupleBins;
+  const uint32_t e = blockIdx.y;
+  const uint32_t nt = ws.ev[e].nTuples;
+  const bool all = (ws.ev[e].flags & (kFlagFitBinOverflow | kFlagTmOverflow)) != 0;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
+  const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  const size_t tb = size_t(e) * kTupleBins;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    if (!all && toff[t + 1] - toff[t] >= 3 && q[t] != 1) continue;  // 1: duplicate
     for (int k = 0; k < 5; ++k) ws.state[tb * 5 + size_t(t) * 5 + k] = 0.f;
     for (int k = 0; k < 15; ++k) ws.cov[tb * 15 + size_t(t) * 15 + k] = 0.f;
     ws.pt[tb + t] = 0.f;
@@ -515,7 +522,7 @@ __global__ void kFitZero(Workspace ws) {
 
 // one thread per (tuple of the multiplicity bin nh); fits the first N hits
 template <int N>
-__global__ void kBLFit(DeviceES es, Workspace ws, uint32_t nh) {
+__device__ __forceinline__ void blFitBin(const DeviceES& es, const Workspace& ws, uint32_t nh) {
   uint32_t e = blockIdx.y;
   const uint32_t* tm = ws.tmOff + size_t(e) * 16;
   uint32_t size = min(tm[nh], uint32_t(PF_MAX_TUPLES));
@@ -559,6 +566,15 @@ __global__ void kBLFit(DeviceES es, Workspace ws, uint32_t nh) {
   }
 }
 
+// the three multiplicity bins in one launch: blockIdx.z = 0, 1, 2 fits the
+// 3-hit tuples, the 4-hit tuples and the first 4 hits of the 5-hit tuples
+__global__ void __launch_bounds__(128) kBLFit(DeviceES es, Workspace ws) {
+  if (blockIdx.z == 0)
+    blFitBin<3>(es, ws, 3);
+  else
+    blFitBin<4>(es, ws, 3 + blockIdx.z);
+}
+
 // standalone fit of externally supplied tuples (fit workload and tests)
 template <int N>
 __global__ void kBLFitDirect(uint32_t n, const double* hits, const float* hge, double B, float* state, float* cov,
@@ -588,9 +604,9 @@ cudaError_t runFits(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStr
   const uint32_t gx = nEvents >= 32 ? 8 : (nEvents >= 8 ? 32 : 148);
   dim3 g(gx, nEvents);
   PG_PROBED("kFitZero", stream, kFitZero<<<g, 256, 0, stream>>>(ws));
-  PG_PROBED("kBLFit", stream, kBLFit<3><<<g, 64, 0, stream>>>(es, ws, 3));
-  PG_PROBED("kBLFit", stream, kBLFit<4><<<g, 64, 0, stream>>>(es, ws, 4));
-  PG_PROBED("kBLFit", stream, kBLFit<4><<<g, 64, 0, stream>>>(es, ws, 5));
+  // FP64-bound: enough warps per SM to cover the double-precision latency
+  const uint32_t fx = nEvents >= 32 ? 16 : (nEvents >= 8 ? 64 : 296);
+  PG_PROBED("kBLFit", stream, kBLFit<<<dim3(fx, nEvents, 3), 128, 0, stream>>>(es, ws));
   return cudaGetLastError();
 }
 

@@ -181,6 +181,7 @@ __global__ void kInitEvents(Workspace ws, uint32_t nEvents) {
     c->nCandidates = c->nLoose = 0;
     c->nVertices = c->nErrors = c->nVtxTracks = 0;
     c->nBig[0] = c->nBig[1] = c->nBig[2] = c->nBig[3] = 0;
+    c->nBigMod = 0;
     c->flags = c->nWords > kMaxFedWords ? kFlagTooManyWords : 0u;
   }
   uint32_t* cim = ws.clusInModule + size_t(e) * kModStride;
@@ -386,7 +387,13 @@ __global__ void kSortModules(Workspace ws, uint32_t nEvents) {
 
 // findClus + clusterChargeCut: one block per (module run, event)
 constexpr int kClusThreads = 256;
-__global__ void __launch_bounds__(kClusThreads) kFindClusters(Workspace ws) {
+constexpr uint32_t kSmallPix = 128;  // modules up to this many pixels are clustered by one warp
+constexpr int kSmallWarps = 8;
+
+// findClus + clusterChargeCut of one module run by the whole block (modules
+// with more than kSmallPix pixels): column histogram, union-find with roots
+// hooked under the smaller pixel index, numbering by ascending root.
+__device__ void clusterModuleBlock(const Workspace& ws, uint32_t e, uint32_t module) {
   __shared__ uint16_t sx[PF_MAX_PIX_IN_MODULE], sy[PF_MAX_PIX_IN_MODULE];
   __shared__ int32_t lab[PF_MAX_PIX_IN_MODULE];
   __shared__ uint16_t colList[PF_MAX_PIX_IN_MODULE];
@@ -395,7 +402,6 @@ __global__ void __launch_bounds__(kClusThreads) kFindClusters(Workspace ws) {
   __shared__ uint32_t scanSh[33];
   __shared__ uint32_t sFound, sNewTotal;
 
-  const uint32_t e = blockIdx.y, module = blockIdx.x;
   const EventCounters* c = ws.ev + e;
   const uint32_t nModules = c->nModules;
   if (module >= nModules) return;
@@ -571,6 +577,152 @@ __global__ void __launch_bounds__(kClusThreads) kFindClusters(Workspace ws) {
     }
   }
   if (threadIdx.x == 0) {
+    ws.clusInModule[size_t(e) * kModStride + thisModuleId] = (found == 0 || allGood) ? found : newTotal;
+    ws.moduleId[size_t(e) * kModStride + module] = thisModuleId;
+  }
+  __syncthreads();
+}
+
+// the modules queued by kFindClustersSmall, one block each
+__global__ void __launch_bounds__(kClusThreads) kFindClustersBig(Workspace ws) {
+  const uint32_t e = blockIdx.y;
+  const uint32_t n = min(ws.ev[e].nBigMod, kMaxModules);
+  const uint32_t* list = ws.bigSeg + size_t(e) * kBigSegCap;
+  for (uint32_t k = blockIdx.x; k < n; k += gridDim.x) clusterModuleBlock(ws, e, list[k]);
+}
+
+// One warp per module run.  Runs of at most kSmallPix pixels are clustered
+// here: neighbours (|dx| <= 1, |dy| <= 1) found by a direct pair scan,
+// union-find in shared memory, roots ranked by ascending pixel index, then
+// the charge cut with renumbering -- the same numbering as the block path.
+// Larger runs are queued for kFindClustersBig.
+__global__ void __launch_bounds__(kSmallWarps * 32) kFindClustersSmall(Workspace ws) {
+  __shared__ uint16_t sxA[kSmallWarps][kSmallPix], syA[kSmallWarps][kSmallPix], rkA[kSmallWarps][kSmallPix];
+  __shared__ int32_t labA[kSmallWarps][kSmallPix], chgA[kSmallWarps][kSmallPix];
+  const uint32_t e = blockIdx.y, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t module = blockIdx.x * kSmallWarps + w;
+  EventCounters* c = ws.ev + e;
+  const uint32_t nModules = c->nModules;
+  if (module >= nModules || module >= kMaxModules) return;
+  const uint32_t start = c->wordStart, nW = c->nWords;
+  const uint32_t* ms = ws.moduleStart + size_t(e) * kModStride;
+  const uint32_t firstPixel = ms[1 + module];
+  const uint32_t msize = (module + 1 < nModules) ? ms[2 + module] : nW;
+  const uint16_t thisModuleId = ws.moduleInd[start + firstPixel];
+  if (thisModuleId >= kMaxModules) {
+    if (lane == 0) ws.moduleId[size_t(e) * kModStride + module] = 0xffffffffu;
+    return;
+  }
+  const uint32_t np = msize - firstPixel;
+  if (np > kSmallPix) {
+    if (lane == 0) {
+      const uint32_t k = atomicAdd(&c->nBigMod, 1u);
+      if (k < kMaxModules) ws.bigSeg[size_t(e) * kBigSegCap + k] = module;
+    }
+    return;
+  }
+  uint16_t* sx = sxA[w];
+  uint16_t* sy = syA[w];
+  uint16_t* rk = rkA[w];
+  int32_t* lab = labA[w];
+  int32_t* chg = chgA[w];
+  uint16_t* gmid = ws.moduleInd + start + firstPixel;
+  int32_t* gclus = ws.clus + start + firstPixel;
+  for (uint32_t k = lane; k < np; k += 32) {
+    const bool valid = gmid[k] != kInvId;
+    sx[k] = ws.xx[start + firstPixel + k];
+    sy[k] = valid ? ws.yy[start + firstPixel + k] : uint16_t(0xffff);
+    lab[k] = int32_t(k);
+  }
+  __syncwarp();
+  auto find = [&](int32_t a) {
+    while (true) {
+      const int32_t p = lab[a];
+      if (p == a) return a;
+      const int32_t gp = lab[p];
+      if (gp != p) lab[a] = gp;  // path halving: only ever moves towards a root
+      a = p;
+    }
+  };
+  for (uint32_t k = lane; k < np; k += 32) {
+    const uint16_t yk = sy[k];
+    if (yk == 0xffff) continue;
+    const int xk = sx[k];
+    for (uint32_t m = k + 1; m < np; ++m) {
+      const uint16_t ym = sy[m];
+      if (ym == 0xffff || abs(int(ym) - int(yk)) > 1 || abs(int(sx[m]) - xk) > 1) continue;
+      int32_t a = int32_t(k), bb = int32_t(m);
+      while (true) {
+        a = find(a);
+        bb = find(bb);
+        if (a == bb) break;
+        if (a > bb) {
+          const int32_t t = a;
+          a = bb;
+          bb = t;
+        }
+        const int32_t old = atomicCAS(&lab[bb], bb, a);
+        if (old == bb) break;
+        bb = old;
+      }
+    }
+  }
+  __syncwarp();
+  // flatten by a read-only walk (path halving here could race with the root
+  // writes of other lanes)
+  for (uint32_t k = lane; k < np; k += 32) {
+    if (sy[k] == 0xffff) continue;
+    int32_t r = lab[k];
+    while (lab[r] != r) r = lab[r];
+    lab[k] = r;
+  }
+  __syncwarp();
+  // rank the roots in ascending pixel order
+  uint32_t found = 0;
+  for (uint32_t k0 = 0; k0 < np; k0 += 32) {
+    const uint32_t k = k0 + lane;
+    const bool isRoot = k < np && sy[k] != 0xffff && lab[k] == int32_t(k);
+    const uint32_t m = __ballot_sync(0xffffffffu, isRoot);
+    if (isRoot) rk[k] = uint16_t(found + __popc(m & lanemaskLt()));
+    found += __popc(m);
+  }
+  for (uint32_t k = lane; k < found; k += 32) chg[k] = 0;
+  __syncwarp();
+  for (uint32_t k = lane; k < np; k += 32) {
+    if (sy[k] == 0xffff) continue;
+    const int32_t id = rk[lab[k]];
+    lab[k] = id;
+    atomicAdd(&chg[id], int32_t(ws.adc[start + firstPixel + k]));
+  }
+  __syncwarp();
+  // charge cut: new ids (stored as id + 1, 0 = removed)
+  const int chargeCut = thisModuleId < 96 ? 2000 : 4000;
+  uint32_t newTotal = 0;
+  for (uint32_t k0 = 0; k0 < found; k0 += 32) {
+    const uint32_t k = k0 + lane;
+    const bool ok = k < found && chg[k] > chargeCut;
+    const uint32_t m = __ballot_sync(0xffffffffu, ok);
+    if (k < found) chg[k] = ok ? int32_t(newTotal + __popc(m & lanemaskLt()) + 1) : 0;
+    newTotal += __popc(m);
+  }
+  __syncwarp();
+  const bool allGood = (found == newTotal);
+  for (uint32_t k = lane; k < np; k += 32) {
+    if (sy[k] == 0xffff) {
+      gclus[k] = -9999;
+    } else if (allGood) {
+      gclus[k] = lab[k];
+    } else {
+      const int32_t nid = chg[lab[k]];
+      if (nid == 0) {
+        gclus[k] = kInvId;
+        gmid[k] = kInvId;
+      } else {
+        gclus[k] = nid - 1;
+      }
+    }
+  }
+  if (lane == 0) {
     ws.clusInModule[size_t(e) * kModStride + thisModuleId] = (found == 0 || allGood) ? found : newTotal;
     ws.moduleId[size_t(e) * kModStride + module] = thisModuleId;
   }
@@ -850,7 +1002,10 @@ cudaError_t runLocal(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaSt
   PG_PROBED("kModuleBoundaries", stream, kModuleBoundaries<<<flatBlocks, 256, 0, stream>>>(ws, nEvents));
   PG_PROBED("kSortModules", stream, kSortModules<<<nEvents, 1024, 0, stream>>>(ws, nEvents));
   PG_PROBED("kSortErrors", stream, kSortErrors<<<nEvents, 32, 0, stream>>>(ws));
-  PG_PROBED("kFindClusters", stream, kFindClusters<<<dim3(kMaxModules, nEvents), kClusThreads, 0, stream>>>(ws));
+  PG_PROBED("kFindClusters", stream,
+            kFindClustersSmall<<<dim3((kMaxModules + kSmallWarps - 1) / kSmallWarps, nEvents), kSmallWarps * 32, 0,
+                                 stream>>>(ws));
+  PG_PROBED("kFindClustersBig", stream, kFindClustersBig<<<dim3(64, nEvents), kClusThreads, 0, stream>>>(ws));
   PG_PROBED("kHitsModuleStart", stream, kHitsModuleStart<<<nEvents, 1024, 0, stream>>>(es, ws));
   PG_PROBED("kGetHits", stream, kGetHits<<<dim3(kMaxModules, nEvents), kHitThreads, 0, stream>>>(es, ws));
   // phi histogram: count, exclusive scan, unordered fill, per-bin ordering

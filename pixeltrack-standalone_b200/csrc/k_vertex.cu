@@ -113,38 +113,65 @@ __device__ void groupByVertex(const VtxScratch& s, uint32_t nt, uint32_t nv, uin
   __syncthreads();
 }
 
-// fitVertices: weighted z, chi2 outlier rejection (iv = 9999), ndof and weight
+// Float sums that must follow the serial order (ascending track order inside
+// a vertex) are formed by a warp: the lanes evaluate 32 consecutive terms at
+// once and every lane adds them in order from the shuffles.  Terms of tracks
+// that the serial loop skips are +0.0, which leaves a sum unchanged (a sum
+// that starts at +0.0 never becomes -0.0 under round-to-nearest).
+
+// fitVertices: weighted z, chi2 outlier rejection (iv = 9999), ndof and weight;
+// one warp per vertex
 __device__ void fitVertices(const VtxScratch& s, uint32_t nt, uint32_t nv, float chi2Max, float* zv, float* wv,
                             float* chi2, int32_t* ndof, uint32_t* vOff, uint32_t* vCur, uint32_t* scanSh) {
   groupByVertex(s, nt, nv, vOff, vCur, scanSh);
-  for (uint32_t v = threadIdx.x; v < nv; v += blockDim.x) {
-    uint32_t b = vOff[v], n = vOff[v + 1] - b;
+  const uint32_t lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (uint32_t v = threadIdx.x >> 5; v < nv; v += nw) {
+    const uint32_t b = vOff[v], n = vOff[v + 1] - b;
     float z = 0, w = 0;
-    for (uint32_t k = 0; k < n; ++k) {
-      uint32_t i = s.list[b + k];
-      float wi = 1.f / s.ezt2[i];
-      z += s.zt[i] * wi;
-      w += wi;
+    for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+      const uint32_t k = k0 + lane;
+      float tz = 0.f, tw = 0.f;
+      if (k < n) {
+        const uint32_t i = s.list[b + k];
+        const float wi = 1.f / s.ezt2[i];
+        tz = s.zt[i] * wi;
+        tw = wi;
+      }
+      const uint32_t cnt = min(32u, n - k0);
+      for (uint32_t l = 0; l < cnt; ++l) {
+        z += __shfl_sync(0xffffffffu, tz, l);
+        w += __shfl_sync(0xffffffffu, tw, l);
+      }
     }
     z /= w;
     int32_t nd = -1;
     float c2s = 0;
-    for (uint32_t k = 0; k < n; ++k) {
-      uint32_t i = s.list[b + k];
-      float c2 = z - s.zt[i];
-      c2 *= c2 / s.ezt2[i];
-      if (c2 > chi2Max) {
-        s.iv[i] = 9999;
-        continue;
+    for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+      const uint32_t k = k0 + lane;
+      float t = 0.f;
+      bool acc = false;
+      if (k < n) {
+        const uint32_t i = s.list[b + k];
+        float c2 = z - s.zt[i];
+        c2 *= c2 / s.ezt2[i];
+        if (c2 > chi2Max) {
+          s.iv[i] = 9999;
+        } else {
+          acc = true;
+          t = c2;
+        }
       }
-      c2s += c2;
-      nd++;
+      nd += __popc(__ballot_sync(0xffffffffu, acc));
+      const uint32_t cnt = min(32u, n - k0);
+      for (uint32_t l = 0; l < cnt; ++l) c2s += __shfl_sync(0xffffffffu, t, l);
     }
     if (nd > 0) w *= float(nd) / c2s;
-    zv[v] = z;
-    wv[v] = w;
-    chi2[v] = c2s;
-    ndof[v] = nd;
+    if (lane == 0) {
+      zv[v] = z;
+      wv[v] = w;
+      chi2[v] = c2s;
+      ndof[v] = nd;
+    }
   }
   __syncthreads();
 }
@@ -184,41 +211,31 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
     const uint32_t nh = toff[t + 1] - toff[t];
     return nh >= 4 && q[t] == 2 && !(pt[t] < 0.5f);
   };
-  // count first: the count decides where the per-track arrays live
-  {
-    uint32_t carry = 0;
-    for (uint32_t t0 = 0; t0 < guard; t0 += blockDim.x) {
-      const uint32_t t = t0 + threadIdx.x;
-      uint32_t sel = 0;
-      if (t < guard) {
-        idv[t] = -1;
-        sel = selected(t) ? 1u : 0u;
-      }
-      uint32_t tot;
-      blockExclusiveScan(sel, scanSh, &tot);
-      carry += tot;
-    }
-    if (threadIdx.x == 0) sNt = min(carry, kMaxVtxTracks);
+  // each thread takes a contiguous chunk of tuples: its selected tracks keep
+  // ascending order, one block scan places them, and the loads of a chunk
+  // are independent of each other
+  const uint32_t chunk = (guard + blockDim.x - 1) / blockDim.x;
+  const uint32_t t0 = min(guard, threadIdx.x * chunk), t1 = min(guard, t0 + chunk);
+  uint32_t mine = 0;
+  for (uint32_t t = t0; t < t1; ++t) {
+    idv[t] = -1;
+    mine += selected(t) ? 1u : 0u;
   }
+  uint32_t total;
+  const uint32_t first = blockExclusiveScan(mine, scanSh, &total);
+  if (threadIdx.x == 0) sNt = min(total, kMaxVtxTracks);
   __syncthreads();
+  // the count decides where the per-track arrays live
   const VtxScratch s = sNt <= kSmemTracks ? carve(vsm, kSmemTracks) : scratchOf(ws, e);
   {
-    uint32_t carry = 0;
-    for (uint32_t t0 = 0; t0 < guard; t0 += blockDim.x) {
-      const uint32_t t = t0 + threadIdx.x;
-      const uint32_t sel = (t < guard && selected(t)) ? 1u : 0u;
-      uint32_t tot;
-      const uint32_t pre = blockExclusiveScan(sel, scanSh, &tot);
-      if (sel) {
-        const uint32_t it = carry + pre;
-        if (it < kMaxVtxTracks) {
-          s.itrk[it] = uint16_t(t);
-          s.zt[it] = st[size_t(t) * 5 + 4];
-          s.ezt2[it] = cov[size_t(t) * 15 + 14];
-          s.ptt2[it] = pt[t] * pt[t];
-        }
-      }
-      carry += tot;
+    uint32_t it = first;
+    for (uint32_t t = t0; t < t1 && it < kMaxVtxTracks; ++t) {
+      if (!selected(t)) continue;
+      s.itrk[it] = uint16_t(t);
+      s.zt[it] = st[size_t(t) * 5 + 4];
+      s.ezt2[it] = cov[size_t(t) * 15 + 14];
+      s.ptt2[it] = pt[t] * pt[t];
+      ++it;
     }
   }
   __syncthreads();
@@ -267,42 +284,77 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
     }
   }
   __syncthreads();
-  // neighbour counts
-  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
-    if (s.ezt2[i] > er2mx) continue;
-    int bs = s.izt[i];
-    int be = min(255, bs + 1);
-    bs = max(0, bs - 1);
-    int32_t cnt = 0;
-    for (uint32_t p = hoff[bs]; p < hoff[be + 1]; ++p) {
-      uint32_t j = s.hbins[p];
-      if (i == j) continue;
-      float dist = fabsf(s.zt[i] - s.zt[j]);
-      if (dist > eps) continue;
-      if (dist * dist > chi2max * (s.ezt2[i] + s.ezt2[j])) continue;
-      ++cnt;
+  // neighbour counts: one warp per track, the lanes take 32 consecutive
+  // entries of the track's three bins at a time
+  for (uint32_t i = threadIdx.x >> 5; i < nt; i += nw) {
+    if (s.ezt2[i] > er2mx) {
+      if (lane == 0) s.nn[i] = 0;
+      continue;
     }
-    s.nn[i] = cnt;
+    const int b0 = max(0, int(s.izt[i]) - 1), b1 = min(255, int(s.izt[i]) + 1);
+    const uint32_t pb = hoff[b0], pe = hoff[b1 + 1];
+    const float zi = s.zt[i], ei = s.ezt2[i];
+    int32_t cnt = 0;
+    for (uint32_t p0 = pb; p0 < pe; p0 += 32) {
+      const uint32_t p = p0 + lane;
+      bool ok = false;
+      if (p < pe) {
+        const uint32_t j = s.hbins[p];
+        const float dist = fabsf(zi - s.zt[j]);
+        ok = i != j && !(dist > eps) && !(dist * dist > chi2max * (ei + s.ezt2[j]));
+      }
+      cnt += __popc(__ballot_sync(0xffffffffu, ok));
+    }
+    if (lane == 0) s.nn[i] = cnt;
   }
   __syncthreads();
-  // closest denser neighbour (ties resolved by the serial iteration order)
-  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
-    float mdist = eps;
-    int bs = s.izt[i];
-    int be = min(255, bs + 1);
-    bs = max(0, bs - 1);
-    int32_t best = int32_t(i);
-    for (uint32_t p = hoff[bs]; p < hoff[be + 1]; ++p) {
-      uint32_t j = s.hbins[p];
-      if (s.nn[j] < s.nn[i]) continue;
-      if (s.nn[j] == s.nn[i] && s.zt[j] >= s.zt[i]) continue;
-      float dist = fabsf(s.zt[i] - s.zt[j]);
-      if (dist > mdist) continue;
-      if (dist * dist > chi2max * (s.ezt2[i] + s.ezt2[j])) continue;
-      mdist = dist;
-      best = int32_t(j);
+  // Closest denser neighbour.  The serial loop (mdist starts at eps; a
+  // candidate is taken when denser, not farther than mdist and
+  // chi2-compatible) ends on the last candidate of minimal distance among the
+  // qualifying ones -- unless a candidate with a NaN distance qualifies: from
+  // then on every denser, chi2-compatible candidate is taken, so the result
+  // is the last of those.  The warp evaluates both, the first as the minimum
+  // of (distance, reversed position).
+  for (uint32_t i = threadIdx.x >> 5; i < nt; i += nw) {
+    const int b0 = max(0, int(s.izt[i]) - 1), b1 = min(255, int(s.izt[i]) + 1);
+    const uint32_t pb = hoff[b0], pe = hoff[b1 + 1];
+    const float zi = s.zt[i], ei = s.ezt2[i];
+    const int32_t ni = s.nn[i];
+    unsigned long long bestKey = ~0ull;
+    bool anyNaN = false;
+    int32_t lastOk = -1;
+    for (uint32_t p0 = pb; p0 < pe; p0 += 32) {
+      const uint32_t p = p0 + lane;
+      unsigned long long key = ~0ull;
+      bool nan = false, dc = false;
+      if (p < pe) {
+        const uint32_t j = s.hbins[p];
+        const int32_t nj = s.nn[j];
+        const float zj = s.zt[j];
+        const float dist = fabsf(zi - zj);
+        const bool dens = !(nj < ni) && !(nj == ni && zj >= zi);
+        dc = dens && !(dist * dist > chi2max * (ei + s.ezt2[j]));
+        nan = dens && isnan(dist);
+        if (dc && !(dist > eps)) key = (uint64_t(__float_as_uint(dist)) << 32) | uint64_t(0xffffffffu - p);
+      }
+      anyNaN |= __any_sync(0xffffffffu, nan);
+      const uint32_t m = __ballot_sync(0xffffffffu, dc);
+      if (m) lastOk = int32_t(p0 + 31 - __clz(m));
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+        key = other < key ? other : key;
+      }
+      bestKey = key < bestKey ? key : bestKey;
     }
-    s.iv[i] = best;
+    if (lane == 0) {
+      int32_t best = int32_t(i);
+      if (anyNaN)
+        best = int32_t(s.hbins[lastOk]);
+      else if (bestKey != ~0ull)
+        best = int32_t(s.hbins[0xffffffffu - uint32_t(bestKey & 0xffffffffu)]);
+      s.iv[i] = best;
+    }
   }
   __syncthreads();
   // percolate to the seed
@@ -350,21 +402,22 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
   //      minus the ones rejected there (iv = 9999)
   if (threadIdx.x == 0) sNv = found;
   __syncthreads();
-  for (uint32_t kv = threadIdx.x; kv < found; kv += blockDim.x) {
-    vCur[kv] = 0;  // split flag
+  for (uint32_t kv = threadIdx.x >> 5; kv < found; kv += nw) {
+    if (lane == 0) vCur[kv] = 0;  // split flag
     if (ndof[kv] < 4) continue;
     if (vchi2[kv] < 9.f * float(ndof[kv])) continue;
     if (ndof[kv] >= 512) {
-      atomicOr(&c->flags, kFlagVtxOverflow);
+      if (lane == 0) atomicOr(&c->flags, kFlagVtxOverflow);
       continue;
     }
-    uint32_t b = vOff[kv], n = vOff[kv + 1] - b;
-    for (uint32_t k = 0; k < n; ++k) {
-      uint32_t i = s.list[b + k];
+    const uint32_t b = vOff[kv], n = vOff[kv + 1] - b;
+    for (uint32_t k = lane; k < n; k += 32) {
+      const uint32_t i = s.list[b + k];
       if (s.iv[i] != int32_t(kv)) continue;
       s.zz[i] = s.zt[i] - zv[kv];
       s.newV[i] = s.zz[i] < 0 ? 0 : 1;
     }
+    __syncwarp();
     float znew[2], wnew[2];
     int maxiter = 20;
     bool more = true;
@@ -372,33 +425,53 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
       more = false;
       znew[0] = znew[1] = 0;
       wnew[0] = wnew[1] = 0;
-      for (uint32_t k = 0; k < n; ++k) {
-        uint32_t i = s.list[b + k];
-        if (s.iv[i] != int32_t(kv)) continue;
-        int w = s.newV[i];
-        float ww = 1.f / s.ezt2[i];
-        znew[w] += s.zz[i] * ww;
-        wnew[w] += ww;
+      for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+        const uint32_t k = k0 + lane;
+        float z0 = 0.f, w0 = 0.f, z1 = 0.f, w1 = 0.f;
+        if (k < n) {
+          const uint32_t i = s.list[b + k];
+          if (s.iv[i] == int32_t(kv)) {
+            const float ww = 1.f / s.ezt2[i];
+            const float p = s.zz[i] * ww;
+            if (s.newV[i]) {
+              z1 = p;
+              w1 = ww;
+            } else {
+              z0 = p;
+              w0 = ww;
+            }
+          }
+        }
+        const uint32_t cnt = min(32u, n - k0);
+        for (uint32_t l = 0; l < cnt; ++l) {
+          znew[0] += __shfl_sync(0xffffffffu, z0, l);
+          wnew[0] += __shfl_sync(0xffffffffu, w0, l);
+          znew[1] += __shfl_sync(0xffffffffu, z1, l);
+          wnew[1] += __shfl_sync(0xffffffffu, w1, l);
+        }
       }
       znew[0] /= wnew[0];
       znew[1] /= wnew[1];
-      for (uint32_t k = 0; k < n; ++k) {
-        uint32_t i = s.list[b + k];
+      bool changed = false;
+      for (uint32_t k = lane; k < n; k += 32) {
+        const uint32_t i = s.list[b + k];
         if (s.iv[i] != int32_t(kv)) continue;
-        float d0 = fabsf(s.zz[i] - znew[0]);
-        float d1 = fabsf(s.zz[i] - znew[1]);
-        uint8_t newer = d0 < d1 ? 0 : 1;
-        more |= newer != s.newV[i];
+        const float d0 = fabsf(s.zz[i] - znew[0]);
+        const float d1 = fabsf(s.zz[i] - znew[1]);
+        const uint8_t newer = d0 < d1 ? 0 : 1;
+        changed |= newer != s.newV[i];
         s.newV[i] = newer;
       }
+      more = __any_sync(0xffffffffu, changed);
+      __syncwarp();
       --maxiter;
       if (maxiter <= 0) more = false;
     }
     if (0 == wnew[0] || 0 == wnew[1]) continue;
-    float dist2 = (znew[0] - znew[1]) * (znew[0] - znew[1]);
-    float chi2Dist = dist2 / (1.f / wnew[0] + 1.f / wnew[1]);
+    const float dist2 = (znew[0] - znew[1]) * (znew[0] - znew[1]);
+    const float chi2Dist = dist2 / (1.f / wnew[0] + 1.f / wnew[1]);
     if (chi2Dist < 4) continue;
-    vCur[kv] = 1;
+    if (lane == 0) vCur[kv] = 1;
   }
   __syncthreads();
   // new vertex numbers in ascending order of the vertex that was split
@@ -439,15 +512,20 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
   if (nv < 1) return;
   for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) idv[s.itrk[i]] = int16_t(s.iv[i]);
   // the fit above left every vertex's accepted tracks in vOff/list order
-  for (uint32_t v = threadIdx.x; v < nv; v += blockDim.x) {
-    uint32_t b = vOff[v], n = vOff[v + 1] - b;
+  for (uint32_t v = threadIdx.x >> 5; v < nv; v += nw) {
+    const uint32_t b = vOff[v], n = vOff[v + 1] - b;
     float p2 = 0;
-    for (uint32_t k = 0; k < n; ++k) {
-      uint32_t i = s.list[b + k];
-      if (s.iv[i] > 9990) continue;
-      p2 += s.ptt2[i];
+    for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+      const uint32_t k = k0 + lane;
+      float t = 0.f;
+      if (k < n) {
+        const uint32_t i = s.list[b + k];
+        if (s.iv[i] <= 9990) t = s.ptt2[i];
+      }
+      const uint32_t cnt = min(32u, n - k0);
+      for (uint32_t l = 0; l < cnt; ++l) p2 += __shfl_sync(0xffffffffu, t, l);
     }
-    ptv2[v] = p2;
+    if (lane == 0) ptv2[v] = p2;
   }
   __syncthreads();
   if (nv == 1) {

@@ -70,7 +70,8 @@ struct EventCounters {
   uint32_t nVtxTracks;
   uint32_t flags;
   uint32_t nBig[4];             // long segments queued by each list ordering
-  uint32_t pad[2];
+  uint32_t nBigMod;             // modules queued for the block clusterizer
+  uint32_t pad[1];
 };
 
 // ---------------------------------------------------------------- ES on device
@@ -136,6 +137,7 @@ struct Workspace {
   uint32_t* ohOff;           // [maxEvents][kHitCap + 1]
   uint32_t* ohCells;         // [maxEvents][kCellCap]
   float4* ohRec;             // [maxEvents][kCellCap] inner hit of each ohCells entry: x, y, z, +-r (- : dca region inner)
+  uint16_t* ohDet;           // [maxEvents][kCellCap] module index of that inner hit
   // CA neighbour links (outerNeighbors), CSR sorted ascending
   uint32_t* nbrCount;        // [maxEvents][kCellCap + 1]
   uint32_t* nbrOff;          // [maxEvents][kCellCap + 1]

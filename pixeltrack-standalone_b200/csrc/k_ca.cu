@@ -383,10 +383,11 @@ __global__ void kOhRec(Workspace ws) {
 // slot: the cells of slot j share their inner hit h, so they share the
 // candidate list (cells ending on h, first 128 in ascending order).  A warp
 // looks at 32 slots at once (warp w: slots w, w + S, ...) and takes the
-// non-empty ones in turn; for a slot, lane t stages the outer hit of cell t,
-// lane k holds candidate k of the current round of 32, and the cells are
-// tested one after the other against all candidates.  Accepted links
-// (oc <- idx) are appended unordered with one atomic per warp and cell.
+// non-empty ones in turn; for a slot, lane t stages the outer hit of cell t
+// and the lanes form groups of G candidates (G the power of two covering the
+// list, at most 32), each group testing another cell of the slot, so short
+// candidate lists still keep the lanes busy.  Accepted links (oc <- idx) are
+// appended unordered with one atomic per warp and round.
 __global__ void kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
   const uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
@@ -427,6 +428,9 @@ __global__ void kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
       const float ri = ws.cellInnerR[cb + base], zi = ws.cellInnerZ[cb + base];
       const float thetaCut = hh.detInd[h] < 1184 ? kThetaCutBarrel : kThetaCutForward;
       const float x2 = hh.xg[h], y2 = hh.yg[h];
+      // lanes form 32/G groups of G >= m candidates; each group tests one cell
+      const uint32_t G = m > 16 ? 32u : (m > 8 ? 16u : (m > 4 ? 8u : (m > 2 ? 4u : (m > 1 ? 2u : 1u))));
+      const uint32_t R = 32u / G, grp = lane / G, kk = lane % G;
       for (uint32_t c0 = base; c0 < end; c0 += 32) {
         const uint32_t nc = min(32u, end - c0);
         float sro = 0.f, szo = 0.f, sx3 = 0.f, sy3 = 0.f;
@@ -437,8 +441,8 @@ __global__ void kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
           sx3 = hh.xg[oh];
           sy3 = hh.yg[oh];
         }
-        for (uint32_t k0 = 0; k0 < m; k0 += 32) {
-          const uint32_t k = k0 + lane;
+        for (uint32_t k0 = 0; k0 < m; k0 += G) {
+          const uint32_t k = k0 + kk;
           float4 r1 = make_float4(0.f, 0.f, 0.f, 0.f);
           uint32_t oc = 0;
           if (k < m) {
@@ -448,22 +452,22 @@ __global__ void kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
           const float region = r1.w < 0.f ? kDcaCutInner : kDcaCutOuter;
           const float rr1 = fabsf(r1.w);
           bool usedOc = false;
-          for (uint32_t t = 0; t < nc; ++t) {
-            const float ro = __shfl_sync(0xffffffffu, sro, t), zo = __shfl_sync(0xffffffffu, szo, t);
-            const float x3 = __shfl_sync(0xffffffffu, sx3, t), y3 = __shfl_sync(0xffffffffu, sy3, t);
-            const bool ok = k < m && alignedRZ(rr1, r1.z, ri, zi, ro, zo, thetaCut) &&
+          for (uint32_t t0 = 0; t0 < nc; t0 += R) {
+            const uint32_t t = t0 + grp;
+            const uint32_t src = t < nc ? t : 0u;
+            const float ro = __shfl_sync(0xffffffffu, sro, src), zo = __shfl_sync(0xffffffffu, szo, src);
+            const float x3 = __shfl_sync(0xffffffffu, sx3, src), y3 = __shfl_sync(0xffffffffu, sy3, src);
+            const bool ok = t < nc && k < m && alignedRZ(rr1, r1.z, ri, zi, ro, zo, thetaCut) &&
                             dcaCut(r1.x, r1.y, x2, y2, x3, y3, region);
             const uint32_t mask = __ballot_sync(0xffffffffu, ok);
             if (mask == 0) continue;
-            const uint32_t idx = c0 + t;
             uint32_t at = 0;
-            if (lane == 0) {
-              at = atomicAdd(&c->nEdges, uint32_t(__popc(mask)));
-              ws.cellUsed[cb + idx] = 1;
-            }
+            if (lane == 0) at = atomicAdd(&c->nEdges, uint32_t(__popc(mask)));
             at = __shfl_sync(0xffffffffu, at, 0);
             if (ok) {
+              const uint32_t idx = c0 + t;
               usedOc = true;
+              ws.cellUsed[cb + idx] = 1;
               atomicAdd(&nbrCnt[oc], 1u);
               const uint32_t slot = at + __popc(mask & lanemaskLt());
               if (slot < kEdgeCap) {

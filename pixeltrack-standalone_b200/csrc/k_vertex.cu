@@ -294,18 +294,14 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
     const int b0 = max(0, int(s.izt[i]) - 1), b1 = min(255, int(s.izt[i]) + 1);
     const uint32_t pb = hoff[b0], pe = hoff[b1 + 1];
     const float zi = s.zt[i], ei = s.ezt2[i];
-    int32_t cnt = 0;
-    for (uint32_t p0 = pb; p0 < pe; p0 += 32) {
-      const uint32_t p = p0 + lane;
-      bool ok = false;
-      if (p < pe) {
-        const uint32_t j = s.hbins[p];
-        const float dist = fabsf(zi - s.zt[j]);
-        ok = i != j && !(dist > eps) && !(dist * dist > chi2max * (ei + s.ezt2[j]));
-      }
-      cnt += __popc(__ballot_sync(0xffffffffu, ok));
+    uint32_t cnt = 0;  // per lane, summed once per track
+    for (uint32_t p = pb + lane; p < pe; p += 32) {
+      const uint32_t j = s.hbins[p];
+      const float dist = fabsf(zi - s.zt[j]);
+      cnt += (i != j && !(dist > eps) && !(dist * dist > chi2max * (ei + s.ezt2[j]))) ? 1u : 0u;
     }
-    if (lane == 0) s.nn[i] = cnt;
+    cnt = __reduce_add_sync(0xffffffffu, cnt);
+    if (lane == 0) s.nn[i] = int32_t(cnt);
   }
   __syncthreads();
   // Closest denser neighbour.  The serial loop (mdist starts at eps; a
@@ -320,32 +316,32 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
     const uint32_t pb = hoff[b0], pe = hoff[b1 + 1];
     const float zi = s.zt[i], ei = s.ezt2[i];
     const int32_t ni = s.nn[i];
+    // per-lane running results, combined once per track
     unsigned long long bestKey = ~0ull;
-    bool anyNaN = false;
+    bool nanLane = false;
     int32_t lastOk = -1;
-    for (uint32_t p0 = pb; p0 < pe; p0 += 32) {
-      const uint32_t p = p0 + lane;
-      unsigned long long key = ~0ull;
-      bool nan = false, dc = false;
-      if (p < pe) {
-        const uint32_t j = s.hbins[p];
-        const int32_t nj = s.nn[j];
-        const float zj = s.zt[j];
-        const float dist = fabsf(zi - zj);
-        const bool dens = !(nj < ni) && !(nj == ni && zj >= zi);
-        dc = dens && !(dist * dist > chi2max * (ei + s.ezt2[j]));
-        nan = dens && isnan(dist);
-        if (dc && !(dist > eps)) key = (uint64_t(__float_as_uint(dist)) << 32) | uint64_t(0xffffffffu - p);
+    for (uint32_t p = pb + lane; p < pe; p += 32) {
+      const uint32_t j = s.hbins[p];
+      const int32_t nj = s.nn[j];
+      const float zj = s.zt[j];
+      const float dist = fabsf(zi - zj);
+      const bool dens = !(nj < ni) && !(nj == ni && zj >= zi);
+      const bool dc = dens && !(dist * dist > chi2max * (ei + s.ezt2[j]));
+      nanLane |= dens && isnan(dist);
+      if (dc) {
+        lastOk = int32_t(p);
+        if (!(dist > eps)) {
+          const unsigned long long key = (uint64_t(__float_as_uint(dist)) << 32) | uint64_t(0xffffffffu - p);
+          bestKey = key < bestKey ? key : bestKey;
+        }
       }
-      anyNaN |= __any_sync(0xffffffffu, nan);
-      const uint32_t m = __ballot_sync(0xffffffffu, dc);
-      if (m) lastOk = int32_t(p0 + 31 - __clz(m));
+    }
+    const bool anyNaN = __any_sync(0xffffffffu, nanLane);
+    lastOk = __reduce_max_sync(0xffffffffu, lastOk);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
-        key = other < key ? other : key;
-      }
-      bestKey = key < bestKey ? key : bestKey;
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long other = __shfl_xor_sync(0xffffffffu, bestKey, o);
+      bestKey = other < bestKey ? other : bestKey;
     }
     if (lane == 0) {
       int32_t best = int32_t(i);

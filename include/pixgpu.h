@@ -229,6 +229,29 @@ typedef struct pg_probe_entry {
 int pg_set_probe(pg_ctx* ctx, const char* kernel);
 int pg_probe_read(pg_ctx* ctx, uint32_t slot, uint32_t max, pg_probe_entry* out, uint32_t* n);
 
+/* Vertex finding without device allocation.  No counterpart in the reference:
+ * it exists for callers that cannot allocate device memory where they need the
+ * vertices, e.g. a per-event module inside a framework that owns all device
+ * memory through its own caching allocator (cudaFree synchronises the whole
+ * device), or a latency-critical path that must not stall on the allocator.
+ * It runs the chain's vertex finder on one event's track SoA given by the
+ * caller in device memory: tuple_off[n_tuples+1], quality[n_tuples],
+ * pt[n_tuples], state[n_tuples*5], cov[n_tuples*15]; it writes idv[n_tuples] and
+ * zv, wv, chi2, ptv2, ndof, sort_ind (1024 entries each) and returns the vertex
+ * count (and the capacity flags) on the host.  All temporaries live in one
+ * static device array of 1.25 MB that every GPU loading the library keeps until
+ * exit; nothing is allocated and no context is needed.  n_tuples must be at most
+ * 32767 (PG_ERR_CAPACITY otherwise).  The first call on a device looks up the
+ * array's device address and sets the kernel's shared-memory attribute, so make
+ * it before any stream capture on that device.  Every call shares the array:
+ * calls that overlap on the GPU (other streams, other threads) race, so
+ * serialise them.  The call waits for its work on `stream` before returning.
+ * msg (msg_cap bytes, may be NULL) receives an error text. */
+int pg_vertices_noalloc(const uint32_t* tuple_off, const uint8_t* quality, const float* pt, const float* state,
+                        const float* cov, uint32_t n_tuples, int16_t* idv, float* zv, float* wv, float* chi2,
+                        float* ptv2, int32_t* ndof, uint16_t* sort_ind, uint32_t* n_vertices, uint32_t* flags,
+                        void* stream, char* msg, size_t msg_cap);
+
 /* Broken-line fits of n tuples of N (3 or 4) hits already on the device:
  * hits[(t*N+i)*3+k], ge[(t*N+i)*6+k]; outputs state[t*5+k], cov[t*15+k],
  * pt[t], eta[t], chi2[t]; B in GeV/cm (0.0114256972711507 in the reference). */

@@ -113,6 +113,26 @@ class Oracle(_Named):
             raise RuntimeError("oracle fit failed")
         return out
 
+    def vertices(self, tupleOff, quality, pt, state, cov):
+        """The serial vertex finder on a given track SoA (n tuples)."""
+        n = len(quality)
+        out = {"idv": np.zeros(max(n, 1), np.int16), "zv": np.zeros(1024, np.float32),
+               "wv": np.zeros(1024, np.float32), "vchi2": np.zeros(1024, np.float32),
+               "ptv2": np.zeros(1024, np.float32), "ndof": np.zeros(1024, np.int32),
+               "sortInd": np.zeros(1024, np.uint16)}
+        nv = ctypes.c_uint32()
+        args = [np.ascontiguousarray(a) for a in (tupleOff, quality, pt, state, cov)]
+        self.lib.or_vertices.argtypes = [ctypes.c_uint32] + [ctypes.c_void_p] * 13
+        rc = self.lib.or_vertices(n, *[a.ctypes.data for a in args],
+                                  *[out[k].ctypes.data for k in ("idv", "zv", "wv", "vchi2", "ptv2", "ndof",
+                                                                 "sortInd")], ctypes.addressof(nv))
+        if rc != 0:
+            raise RuntimeError("oracle vertexing failed")
+        k = nv.value
+        return {"nVertices": k, "idv": out["idv"][:n], "zv": out["zv"][:k], "wv": out["wv"][:k],
+                "vchi2": out["vchi2"][:k], "ptv2": out["ptv2"][:k], "ndof": out["ndof"][:k],
+                "sortInd": out["sortInd"][:k]}
+
     def __del__(self):
         try:
             self.lib.or_destroy(self._h)

@@ -1,6 +1,7 @@
 // C entry points of the oracle library (checker only; see oracle.h).
 // Products are exposed by name with the same names the checker build of the
 // reference (oracle/ref/ref_driver.cc) uses, so tests compare them directly.
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cstring>
@@ -236,6 +237,42 @@ int or_fit(int N, uint32_t n, const double* hits, const float* ge, double B, flo
   for (uint32_t t = 0; t < n; ++t)
     oracle::brokenLineFit(N, hits + size_t(t) * N * 3, ge + size_t(t) * N * 6, B, state + size_t(t) * 5,
                           cov + size_t(t) * 15, pt + t, eta + t, chi2 + t);
+  return 0;
+}
+
+// Vertexing of a given track SoA (n tuples): tuple_off[n+1], quality[n],
+// pt[n], state[n*5], cov[n*15]; outputs idv[n], zv/wv/chi2/ptv2/ndof/sortInd
+// (1024 each) and the vertex count.  Test infrastructure for the vertex
+// finder run on tracks that do not come from an event.
+int or_vertices(uint32_t n, const uint32_t* tupleOff, const uint8_t* quality, const float* pt, const float* state,
+                const float* cov, int16_t* idv, float* zv, float* wv, float* chi2, float* ptv2, int32_t* ndof,
+                uint16_t* sortInd, uint32_t* nVertices) {
+  if (n >= PF_TRACK_STRIDE) return -1;
+  oracle::CA ca;
+  ca.tupleOff.assign(PF_TRACK_STRIDE + 1, tupleOff[n]);
+  std::copy(tupleOff, tupleOff + n + 1, ca.tupleOff.begin());
+  ca.quality.assign(PF_TRACK_STRIDE, 0);
+  std::copy(quality, quality + n, ca.quality.begin());
+  ca.pt.assign(PF_TRACK_STRIDE, 0.f);
+  std::copy(pt, pt + n, ca.pt.begin());
+  ca.state.assign(size_t(PF_TRACK_STRIDE) * 5, 0.f);
+  std::copy(state, state + size_t(n) * 5, ca.state.begin());
+  ca.cov.assign(size_t(PF_TRACK_STRIDE) * 15, 0.f);
+  std::copy(cov, cov + size_t(n) * 15, ca.cov.begin());
+  oracle::Vertices v;
+  try {
+    oracle::makeVertices(ca, v);
+  } catch (std::exception&) {
+    return -1;
+  }
+  std::copy(v.idv.begin(), v.idv.begin() + n, idv);
+  std::copy(v.zv.begin(), v.zv.begin() + 1024, zv);
+  std::copy(v.wv.begin(), v.wv.begin() + 1024, wv);
+  std::copy(v.chi2.begin(), v.chi2.begin() + 1024, chi2);
+  std::copy(v.ptv2.begin(), v.ptv2.begin() + 1024, ptv2);
+  std::copy(v.ndof.begin(), v.ndof.begin() + 1024, ndof);
+  std::copy(v.sortInd.begin(), v.sortInd.begin() + 1024, sortInd);
+  *nVertices = v.nvFinal;
   return 0;
 }
 

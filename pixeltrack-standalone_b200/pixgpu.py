@@ -298,7 +298,26 @@ def gpu_lib():
                                   ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ServeConfig), ctypes.c_void_p,
                                   ctypes.c_void_p, ctypes.POINTER(ServeStats), ctypes.c_void_p, RESULT_FN,
                                   ctypes.c_void_p]
+        _gpu.pg_vertices_noalloc.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_uint32] + [ctypes.c_void_p] * 10 + \
+            [ctypes.c_char_p, ctypes.c_size_t]
     return _gpu
+
+
+def vertices_noalloc(tuple_off, quality, pt, state, cov, idv, zv, wv, chi2, ptv2, ndof, sort_ind, stream=None):
+    """pg_vertices_noalloc on device tensors (torch): one event's track SoA in,
+    the vertices out; returns (n_vertices, flags).  Allocates nothing on the
+    device; raises with the library's message on failure."""
+    n = int(quality.numel())
+    nv = ctypes.c_uint32()
+    fl = ctypes.c_uint32()
+    msg = ctypes.create_string_buffer(256)
+    rc = gpu_lib().pg_vertices_noalloc(tuple_off.data_ptr(), quality.data_ptr(), pt.data_ptr(), state.data_ptr(),
+                                       cov.data_ptr(), n, idv.data_ptr(), zv.data_ptr(), wv.data_ptr(),
+                                       chi2.data_ptr(), ptv2.data_ptr(), ndof.data_ptr(), sort_ind.data_ptr(),
+                                       ctypes.addressof(nv), ctypes.addressof(fl), stream, msg, len(msg))
+    if rc != 0:
+        raise RuntimeError("pg_vertices_noalloc failed (%d): %s" % (rc, msg.value.decode()))
+    return nv.value, fl.value
 
 
 def _raw_arrays(raws):

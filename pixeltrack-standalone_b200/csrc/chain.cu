@@ -114,6 +114,7 @@ void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W) {
   c.take(ws.scratchB, size_t(E) * kEdgeCap);
   c.take(ws.scanTmp, size_t(E + 1) * kScanTmpStride);
   c.take(ws.bigSeg, size_t(E) * kBigSegCap);
+  c.take(ws.segList, size_t(E) * kCellCap);
 }
 
 // the pair opened by probeBegin when its name matched (-1: none).  Records use

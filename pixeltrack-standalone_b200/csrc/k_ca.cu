@@ -320,6 +320,7 @@ __global__ void kOuterHitFill(Workspace ws) {
     uint16_t oi = ws.cellOuter[cb + c];
     uint32_t p = atomicAdd(&cur[oi], 1u);
     ws.ohCells[cb + off[oi] + p] = c;
+    if (p == 1) noteSegment(ws, e, 0, oi);
   }
 }
 
@@ -495,6 +496,7 @@ __global__ void kEdgeScatter(Workspace ws, const uint32_t* edgeOc, const uint32_
     uint32_t oc = edgeOc[size_t(e) * kEdgeCap + k];
     uint32_t p = atomicAdd(&cur[oc], 1u);
     if (off[oc] + p < kEdgeCap) ws.nbr[size_t(e) * kEdgeCap + off[oc] + p] = edgeIdx[size_t(e) * kEdgeCap + k];
+    if (p == 1) noteSegment(ws, e, 1, oc);
   }
 }
 
@@ -732,6 +734,7 @@ __global__ void kTrackFill(Workspace ws) {
       uint32_t cc = tcell[4 * t + k];
       uint32_t p = atomicAdd(&cur[cc], 1u);
       trk[off[cc] + p] = uint16_t(t);
+      if (p == 1) noteSegment(ws, e, 2, cc);
     }
   }
 }
@@ -1004,6 +1007,7 @@ __global__ void kHitToTupleFill(Workspace ws) {
       uint16_t h = th[k];
       uint32_t p = atomicAdd(&cur[h], 1u);
       uint32_t pos = off[h] + p;
+      if (p == 1) noteSegment(ws, e, 3, h);
       if (pos < kH2TCap)
         h2t[pos] = uint16_t(t);
       else

@@ -182,6 +182,7 @@ __global__ void kInitEvents(Workspace ws, uint32_t nEvents) {
     c->nVertices = c->nErrors = c->nVtxTracks = 0;
     c->nBig[0] = c->nBig[1] = c->nBig[2] = c->nBig[3] = 0;
     c->nBigMod = 0;
+    c->nSegList[0] = c->nSegList[1] = c->nSegList[2] = c->nSegList[3] = 0;
     c->flags = c->nWords > kMaxFedWords ? kFlagTooManyWords : 0u;
   }
   uint32_t* cim = ws.clusInModule + size_t(e) * kModStride;

@@ -71,6 +71,7 @@ struct EventCounters {
   uint32_t flags;
   uint32_t nBig[4];             // long segments queued by each list ordering
   uint32_t nBigMod;             // modules queued for the block clusterizer
+  uint32_t nSegList[4];         // list segments that received a second entry, per list ordering
   uint32_t pad[1];
 };
 
@@ -177,10 +178,21 @@ struct Workspace {
   // scan scratch
   uint32_t* scanTmp;         // [maxEvents][kScanTmpStride]
   uint32_t* bigSeg;          // [maxEvents][kBigSegCap] long segments awaiting the block sort
+  uint32_t* segList;         // [maxEvents][kCellCap] segments with >= 2 entries (the ones to order)
 };
 
 constexpr uint32_t kScanChunk = 4096;
 constexpr uint32_t kScanTmpStride = 1024;
+
+// A CSR fill notes segment s when it places s's second entry: only those
+// segments need ordering.  `list` selects the counter of the list ordering
+// that follows the fill (0 cells by outer hit, 1 CA links, 2 tracks per
+// cell, 3 tuples per hit); the lists share ws.segList, each consumed before
+// the next fill.
+__device__ __forceinline__ void noteSegment(const Workspace& ws, uint32_t e, int list, uint32_t s) {
+  const uint32_t k = atomicAdd(&ws.ev[e].nSegList[list], 1u);
+  ws.segList[size_t(e) * kCellCap + k] = s;
+}
 
 // ---------------------------------------------------------------- kernel timing probe
 // While a probe is installed on the launching host thread, every launch whose

@@ -4,9 +4,10 @@
 // order, which is the order restored here (keys inside one segment are
 // distinct).
 //
-//  kSortSmall  one thread per segment: n <= 16 sorted in registers by a
-//              bitonic network; 16 < n <= 256 handed to the warp (rank sort,
-//              one segment at a time, ballot over the lanes that hold one);
+//  kSortListed one thread per segment the fill noted (the segments that got
+//              a second entry): n <= 16 sorted in registers by a bitonic
+//              network; 16 < n <= 256 handed to the warp (rank sort, one
+//              segment at a time, ballot over the lanes that hold one);
 //              n > 256 appended to a per-event list for kSortBig.
 //  kSortBig    one block per long segment: rank sort in shared memory.
 #pragma once
@@ -61,17 +62,19 @@ __device__ void serialSort(T* seg, uint32_t n, bool desc) {
 }
 
 template <typename T>
-__global__ void kSortSmall(T* data, size_t dataStride, const uint32_t* off, size_t offStride, const uint32_t* lenPtr,
-                           uint32_t lenStride, uint32_t fixedLen, bool desc, uint32_t dataCap, uint32_t* big,
-                           uint32_t* nBig, uint32_t nBigStride) {
+__global__ void kSortListed(T* data, size_t dataStride, const uint32_t* off, size_t offStride, const uint32_t* list,
+                            const uint32_t* nList, uint32_t nListStride, bool desc, uint32_t dataCap, uint32_t* big,
+                            uint32_t* nBig, uint32_t nBigStride) {
   const uint32_t e = blockIdx.y;
-  const uint32_t nseg = lenPtr ? lenPtr[size_t(e) * lenStride] : fixedLen;
+  const uint32_t nseg = nList[size_t(e) * nListStride];
   const uint32_t* o = off + size_t(e) * offStride;
+  const uint32_t* L = list + size_t(e) * kCellCap;
   T* d = data + size_t(e) * dataStride;
   for (uint32_t s0 = blockIdx.x * blockDim.x; s0 < nseg; s0 += gridDim.x * blockDim.x) {
-    const uint32_t s = s0 + threadIdx.x;
-    uint32_t b = 0, n = 0;
-    if (s < nseg) {
+    const uint32_t k = s0 + threadIdx.x;
+    uint32_t b = 0, n = 0, s = 0;
+    if (k < nseg) {
+      s = L[k];
       b = min(o[s], dataCap);
       n = min(o[s + 1], dataCap) - b;
     }
@@ -84,9 +87,9 @@ __global__ void kSortSmall(T* data, size_t dataStride, const uint32_t* off, size
       warpSortSegment(d + bb, nn, desc);
     }
     if (n > 256) {
-      const uint32_t k = atomicAdd(&nBig[size_t(e) * nBigStride], 1u);
-      if (k < kBigSegCap)
-        big[size_t(e) * kBigSegCap + k] = s;
+      const uint32_t q = atomicAdd(&nBig[size_t(e) * nBigStride], 1u);
+      if (q < kBigSegCap)
+        big[size_t(e) * kBigSegCap + q] = s;
       else
         serialSort(d + b, n, desc);  // more long segments than the list holds
     }
@@ -120,18 +123,23 @@ __global__ void kSortBig(T* data, size_t dataStride, const uint32_t* off, size_t
   }
 }
 
-// Orders segment s = [off[s], off[s+1]) of data for s < nseg_e, per event e;
-// nseg_e = lenPtr[e*lenStride] or fixedLen.  `slot` picks one of the
-// per-event long-segment counters (distinct per call site).
+// Orders segment s = [off[s], off[s+1]) of data for every segment the
+// preceding fill noted in list `slot` (those with >= 2 entries); `slot` also
+// picks the per-event long-segment counter.  lenPtr/fixedLen (the number of
+// segments) are kept for the callers' readability only.
 template <typename T>
 void sortSegments(Workspace& ws, uint32_t nEvents, cudaStream_t stream, uint32_t gx, T* data, size_t dataStride,
                   const uint32_t* off, size_t offStride, const uint32_t* lenPtr, uint32_t lenStride, uint32_t fixedLen,
                   bool desc, uint32_t dataCap, int slot) {
   uint32_t* nBig = &ws.ev[0].nBig[slot];
   const uint32_t stride = sizeof(EventCounters) / 4;
+  (void)lenPtr;
+  (void)lenStride;
+  (void)fixedLen;
   PG_PROBED("kSortSegments", stream,
-            kSortSmall<T><<<dim3(gx, nEvents), 256, 0, stream>>>(data, dataStride, off, offStride, lenPtr, lenStride,
-                                                                 fixedLen, desc, dataCap, ws.bigSeg, nBig, stride));
+            kSortListed<T><<<dim3(gx, nEvents), 256, 0, stream>>>(data, dataStride, off, offStride, ws.segList,
+                                                                  &ws.ev[0].nSegList[slot], stride, desc, dataCap,
+                                                                  ws.bigSeg, nBig, stride));
   PG_PROBED("kSortBig", stream,
             kSortBig<T><<<dim3(8, nEvents), 256, 0, stream>>>(data, dataStride, off, offStride, desc, dataCap,
                                                               ws.bigSeg, nBig, stride));

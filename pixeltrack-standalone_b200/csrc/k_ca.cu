@@ -331,9 +331,16 @@ __global__ void kOuterHitFill(Workspace ws) {
 __device__ __forceinline__ bool alignedRZ(float r1, float z1, float ri, float zi, float ro, float zo, float thetaCut) {
   float radius_diff = fabsf(r1 - ro);
   float distance_13_squared = radius_diff * radius_diff + (z1 - zo) * (z1 - zo);
+  const float area = z1 * (ri - ro) + zi * (ro - r1) + zo * (r1 - ri);
+  const float rhs = thetaCut * distance_13_squared * radius_diff;
+  // cheap rejection: the squared inequality in float, with a relative margin
+  // far above its rounding error, rejects only pairs the exact test rejects
+  // (NaN operands, and right-hand sides small enough for the squares to lose
+  // precision as subnormals, fall through to the exact test)
+  if (rhs > 1e-15f && area * area * (kPtMin * kPtMin) * distance_13_squared > 1.0001f * rhs * rhs) return false;
   float pMin = kPtMin * sqrtf(distance_13_squared);
-  double lhs = fabs(double(z1 * (ri - ro) + zi * (ro - r1) + zo * (r1 - ri)));
-  return lhs * double(pMin) <= double(thetaCut * distance_13_squared * radius_diff);
+  double lhs = fabs(double(area));
+  return lhs * double(pMin) <= double(rhs);
 }
 
 __device__ __forceinline__ bool dcaCut(float x1, float y1, float x2, float y2, float x3, float y3, float region) {

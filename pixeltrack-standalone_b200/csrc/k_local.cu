@@ -183,6 +183,7 @@ __global__ void kInitEvents(Workspace ws, uint32_t nEvents) {
     c->nBig[0] = c->nBig[1] = c->nBig[2] = c->nBig[3] = 0;
     c->nBigMod = 0;
     c->nSegList[0] = c->nSegList[1] = c->nSegList[2] = c->nSegList[3] = 0;
+    c->nBigHitMod = 0;
     c->flags = c->nWords > kMaxFedWords ? kFlagTooManyWords : 0u;
   }
   uint32_t* cim = ws.clusInModule + size_t(e) * kModStride;
@@ -770,23 +771,98 @@ __global__ void kHitsModuleStart(DeviceES es, Workspace ws) {
 }
 
 // getHits: one block per (module run, event); all clusters of a module in one pass
+// gpuPixelRecHits.h:100-207 for one cluster: sizes, CPE position and
+// errors, global position, iphi; written to hit slot h of event e
+__device__ __forceinline__ void writeHit(const Workspace& ws, size_t hb, uint32_t h, uint32_t me,
+                                         const PfDetParams& dp, const PfCommonParams& cp, const PfBeamSpot& bs,
+                                         uint32_t minRow, uint32_t maxRow, uint32_t minCol, uint32_t maxCol,
+                                         int32_t Qfx, int32_t Qlx, int32_t Qfy, int32_t Qly, int32_t chg) {
+  uint16_t llx = uint16_t(minRow + 1), lly = uint16_t(minCol + 1);
+  uint16_t urx = uint16_t(maxRow), ury = uint16_t(maxCol);
+  uint16_t llxl = localX(llx), llyl = localY(lly), urxl = localX(urx), uryl = localY(ury);
+  int mx = llxl + urxl, my = llyl + uryl;
+  int xsize = int(urxl) + 2 - int(llxl);
+  int ysize = int(uryl) + 2 - int(llyl);
+  bool bigMinX = isBigPixX(uint16_t(minRow)), bigMaxX = isBigPixX(uint16_t(maxRow));
+  bool bigMinY = isBigPixY(uint16_t(minCol)), bigMaxY = isBigPixY(uint16_t(maxCol));
+  if (bigMinX) ++xsize;
+  if (bigMaxX) ++xsize;
+  if (bigMinY) ++ysize;
+  if (bigMaxY) ++ysize;
+  // the reference computes these ratios in double precision
+  int unbalanceX = int(8. * double(fabsf(float(Qfx - Qlx))) / double(float(Qfx + Qlx)));
+  int unbalanceY = int(8. * double(fabsf(float(Qfy - Qly))) / double(float(Qfy + Qly)));
+  xsize = 8 * xsize - unbalanceX;
+  ysize = 8 * ysize - unbalanceY;
+  int16_t sxv = int16_t(min(xsize, 1023)), syv = int16_t(min(ysize, 1023));
+  if (minRow == 0 || maxRow == 159) sxv = int16_t(-sxv);
+  if (minCol == 0 || maxCol == 415) syv = int16_t(-syv);
+  float xPos = dp.shiftX + cp.pitchX * (0.5f * float(mx) + float(-81));
+  float yPos = dp.shiftY + cp.pitchY * (0.5f * float(my) + float(-216));
+  float gvz = -1.f / dp.z0;
+  float cotalpha = (xPos - dp.x0) * gvz, cotbeta = (yPos - dp.y0) * gvz;
+  float thickness = dp.isBarrel ? cp.thicknessB : cp.thicknessE;
+  float xcorr = cpeCorrection(int(maxRow - minRow), Qfx, Qlx, llxl, urxl, dp.chargeWidthX,
+                              thickness, cotalpha, cp.pitchX, bigMinX, bigMaxX);
+  float ycorr = cpeCorrection(int(maxCol - minCol), Qfy, Qly, llyl, uryl, dp.chargeWidthY,
+                              thickness, cotbeta, cp.pitchY, bigMinY, bigMaxY);
+  float xpos = xPos + xcorr, ypos = yPos + ycorr;
+  float xerr = 0.0050f, yerr = 0.0085f;
+  uint32_t sx = maxRow - minRow, sy = maxCol - minCol;
+  bool isEdgeX = minRow == 0 || maxRow == 159;
+  bool isEdgeY = minCol == 0 || maxCol == 415;
+  uint32_t ix = (0 == sx), iy = (0 == sy);
+  ix += (0 == sx) && bigMinX;
+  iy += (0 == sy) && bigMinY;
+  if (!isEdgeX) xerr = dp.sx[ix];
+  if (!isEdgeY) yerr = dp.sy[iy];
+  const PfFrame& f = dp.frame;
+  float xg = f.R11 * xpos + f.R21 * ypos;
+  float yg = f.R12 * xpos + f.R22 * ypos;
+  float zg = f.R13 * xpos + f.R23 * ypos;
+  xg += f.px;
+  yg += f.py;
+  zg += f.pz;
+  xg -= bs.x;
+  yg -= bs.y;
+  zg -= bs.z;
+  ws.charge[hb + h] = chg;
+  ws.detInd[hb + h] = uint16_t(me);
+  ws.xl[hb + h] = xpos;
+  ws.yl[hb + h] = ypos;
+  ws.xsize[hb + h] = sxv;
+  ws.ysize[hb + h] = syv;
+  ws.xerr[hb + h] = xerr * xerr;
+  ws.yerr[hb + h] = yerr * yerr;
+  ws.xg[hb + h] = xg;
+  ws.yg[hb + h] = yg;
+  ws.zg[hb + h] = zg;
+  ws.rg[hb + h] = sqrtf(xg * xg + yg * yg);
+  ws.iphi[hb + h] = unsafeAtan2s7(yg, xg);
+}
+
 constexpr int kHitThreads = 128;
 constexpr int kHitBatch = 256;
-__global__ void __launch_bounds__(kHitThreads) kGetHits(DeviceES es, Workspace ws) {
+constexpr uint32_t kSmallClus = 32;  // modules with at most this many clusters are handled by one warp
+constexpr int kHitWarps = 8;
+
+// getHits for one module run by the whole block (modules with more than
+// kSmallClus clusters): per-cluster extremes and edge charges by shared
+// atomics, in batches of kHitBatch clusters
+__device__ void hitsModuleBlock(const DeviceES& es, const Workspace& ws, uint32_t e, uint32_t module) {
   __shared__ uint32_t minRow[kHitBatch], maxRow[kHitBatch], minCol[kHitBatch], maxCol[kHitBatch];
   __shared__ int32_t Qfx[kHitBatch], Qlx[kHitBatch], Qfy[kHitBatch], Qly[kHitBatch], chg[kHitBatch];
-  const uint32_t e = blockIdx.y, module = blockIdx.x;
   const EventCounters* c = ws.ev + e;
   const uint32_t nModules = c->nModules;
   if (module >= nModules) return;
   const uint32_t me = ws.moduleId[size_t(e) * kModStride + module];
+  if (me >= es.nDet) return;  // runs the clustering rejected carry no valid module id
   const int nclus = int(ws.clusInModule[size_t(e) * kModStride + me]);
   if (nclus == 0) return;
   const uint32_t start = c->wordStart, nW = c->nWords;
   const uint32_t* ms = ws.moduleStart + size_t(e) * kModStride;
   const uint32_t first = ms[1 + module];
   const uint32_t last = (module + 1 < nModules) ? ms[2 + module] : nW;
-  if (me >= es.nDet) return;  // runs the clustering rejected carry no valid module id
   const PfDetParams& dp = es.det[me];
   const PfCommonParams& cp = *es.common;
   const PfBeamSpot& bs = *es.bs;
@@ -832,70 +908,95 @@ __global__ void __launch_bounds__(kHitThreads) kGetHits(DeviceES es, Workspace w
     for (int ic = threadIdx.x; ic < nIn; ic += blockDim.x) {
       uint32_t h = cmsMe + startClus + ic;
       if (h >= uint32_t(PF_MAX_HITS)) continue;
-      uint16_t llx = uint16_t(minRow[ic] + 1), lly = uint16_t(minCol[ic] + 1);
-      uint16_t urx = uint16_t(maxRow[ic]), ury = uint16_t(maxCol[ic]);
-      uint16_t llxl = localX(llx), llyl = localY(lly), urxl = localX(urx), uryl = localY(ury);
-      int mx = llxl + urxl, my = llyl + uryl;
-      int xsize = int(urxl) + 2 - int(llxl);
-      int ysize = int(uryl) + 2 - int(llyl);
-      bool bigMinX = isBigPixX(uint16_t(minRow[ic])), bigMaxX = isBigPixX(uint16_t(maxRow[ic]));
-      bool bigMinY = isBigPixY(uint16_t(minCol[ic])), bigMaxY = isBigPixY(uint16_t(maxCol[ic]));
-      if (bigMinX) ++xsize;
-      if (bigMaxX) ++xsize;
-      if (bigMinY) ++ysize;
-      if (bigMaxY) ++ysize;
-      // the reference computes these ratios in double precision
-      int unbalanceX = int(8. * double(fabsf(float(Qfx[ic] - Qlx[ic]))) / double(float(Qfx[ic] + Qlx[ic])));
-      int unbalanceY = int(8. * double(fabsf(float(Qfy[ic] - Qly[ic]))) / double(float(Qfy[ic] + Qly[ic])));
-      xsize = 8 * xsize - unbalanceX;
-      ysize = 8 * ysize - unbalanceY;
-      int16_t sxv = int16_t(min(xsize, 1023)), syv = int16_t(min(ysize, 1023));
-      if (minRow[ic] == 0 || maxRow[ic] == 159) sxv = int16_t(-sxv);
-      if (minCol[ic] == 0 || maxCol[ic] == 415) syv = int16_t(-syv);
-      float xPos = dp.shiftX + cp.pitchX * (0.5f * float(mx) + float(-81));
-      float yPos = dp.shiftY + cp.pitchY * (0.5f * float(my) + float(-216));
-      float gvz = -1.f / dp.z0;
-      float cotalpha = (xPos - dp.x0) * gvz, cotbeta = (yPos - dp.y0) * gvz;
-      float thickness = dp.isBarrel ? cp.thicknessB : cp.thicknessE;
-      float xcorr = cpeCorrection(int(maxRow[ic] - minRow[ic]), Qfx[ic], Qlx[ic], llxl, urxl, dp.chargeWidthX,
-                                  thickness, cotalpha, cp.pitchX, bigMinX, bigMaxX);
-      float ycorr = cpeCorrection(int(maxCol[ic] - minCol[ic]), Qfy[ic], Qly[ic], llyl, uryl, dp.chargeWidthY,
-                                  thickness, cotbeta, cp.pitchY, bigMinY, bigMaxY);
-      float xpos = xPos + xcorr, ypos = yPos + ycorr;
-      float xerr = 0.0050f, yerr = 0.0085f;
-      uint32_t sx = maxRow[ic] - minRow[ic], sy = maxCol[ic] - minCol[ic];
-      bool isEdgeX = minRow[ic] == 0 || maxRow[ic] == 159;
-      bool isEdgeY = minCol[ic] == 0 || maxCol[ic] == 415;
-      uint32_t ix = (0 == sx), iy = (0 == sy);
-      ix += (0 == sx) && bigMinX;
-      iy += (0 == sy) && bigMinY;
-      if (!isEdgeX) xerr = dp.sx[ix];
-      if (!isEdgeY) yerr = dp.sy[iy];
-      const PfFrame& f = dp.frame;
-      float xg = f.R11 * xpos + f.R21 * ypos;
-      float yg = f.R12 * xpos + f.R22 * ypos;
-      float zg = f.R13 * xpos + f.R23 * ypos;
-      xg += f.px;
-      yg += f.py;
-      zg += f.pz;
-      xg -= bs.x;
-      yg -= bs.y;
-      zg -= bs.z;
-      ws.charge[hb + h] = chg[ic];
-      ws.detInd[hb + h] = uint16_t(me);
-      ws.xl[hb + h] = xpos;
-      ws.yl[hb + h] = ypos;
-      ws.xsize[hb + h] = sxv;
-      ws.ysize[hb + h] = syv;
-      ws.xerr[hb + h] = xerr * xerr;
-      ws.yerr[hb + h] = yerr * yerr;
-      ws.xg[hb + h] = xg;
-      ws.yg[hb + h] = yg;
-      ws.zg[hb + h] = zg;
-      ws.rg[hb + h] = sqrtf(xg * xg + yg * yg);
-      ws.iphi[hb + h] = unsafeAtan2s7(yg, xg);
+      writeHit(ws, hb, h, me, dp, cp, bs, minRow[ic], maxRow[ic], minCol[ic], maxCol[ic], Qfx[ic], Qlx[ic], Qfy[ic],
+               Qly[ic], chg[ic]);
     }
     __syncthreads();
+  }
+}
+
+// the modules queued by kGetHitsSmall, one block each
+__global__ void __launch_bounds__(kHitThreads) kGetHitsBig(DeviceES es, Workspace ws) {
+  const uint32_t e = blockIdx.y;
+  const uint32_t n = min(ws.ev[e].nBigHitMod, kMaxModules);
+  const uint32_t* list = ws.bigSeg + size_t(e) * kBigSegCap;
+  for (uint32_t k = blockIdx.x; k < n; k += gridDim.x) hitsModuleBlock(es, ws, e, list[k]);
+}
+
+// One warp per module run with at most kSmallClus clusters (the others are
+// queued for kGetHitsBig): lanes walk the pixels, the per-cluster extremes
+// and edge charges collect in per-warp shared arrays, lane k writes hit k.
+__global__ void __launch_bounds__(kHitWarps * 32) kGetHitsSmall(DeviceES es, Workspace ws) {
+  __shared__ uint32_t mnR[kHitWarps][kSmallClus], mxR[kHitWarps][kSmallClus], mnC[kHitWarps][kSmallClus],
+      mxC[kHitWarps][kSmallClus];
+  __shared__ int32_t qfx[kHitWarps][kSmallClus], qlx[kHitWarps][kSmallClus], qfy[kHitWarps][kSmallClus],
+      qly[kHitWarps][kSmallClus], chA[kHitWarps][kSmallClus];
+  const uint32_t e = blockIdx.y, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t module = blockIdx.x * kHitWarps + w;
+  EventCounters* c = ws.ev + e;
+  const uint32_t nModules = c->nModules;
+  if (module >= nModules || module >= kMaxModules) return;
+  const uint32_t me = ws.moduleId[size_t(e) * kModStride + module];
+  if (me >= es.nDet) return;  // runs the clustering rejected carry no valid module id
+  const uint32_t nclus = ws.clusInModule[size_t(e) * kModStride + me];
+  if (nclus == 0) return;
+  if (nclus > kSmallClus) {
+    if (lane == 0) {
+      const uint32_t k = atomicAdd(&c->nBigHitMod, 1u);
+      if (k < kMaxModules) ws.bigSeg[size_t(e) * kBigSegCap + k] = module;
+    }
+    return;
+  }
+  const uint32_t start = c->wordStart, nW = c->nWords;
+  const uint32_t* ms = ws.moduleStart + size_t(e) * kModStride;
+  const uint32_t first = ms[1 + module];
+  const uint32_t last = (module + 1 < nModules) ? ms[2 + module] : nW;
+  uint32_t* minRow = mnR[w];
+  uint32_t* maxRow = mxR[w];
+  uint32_t* minCol = mnC[w];
+  uint32_t* maxCol = mxC[w];
+  int32_t* Qfx = qfx[w];
+  int32_t* Qlx = qlx[w];
+  int32_t* Qfy = qfy[w];
+  int32_t* Qly = qly[w];
+  int32_t* chg = chA[w];
+  if (lane < nclus) {
+    minRow[lane] = minCol[lane] = 0xffffffffu;
+    maxRow[lane] = maxCol[lane] = 0;
+    chg[lane] = Qfx[lane] = Qlx[lane] = Qfy[lane] = Qly[lane] = 0;
+  }
+  __syncwarp();
+  for (uint32_t i = first + lane; i < last; i += 32) {
+    const uint16_t id = ws.moduleInd[start + i];
+    if (id == kInvId || id != me) continue;
+    const int cl = ws.clus[start + i];
+    if (cl < 0 || cl >= int(nclus)) continue;
+    const uint32_t x = ws.xx[start + i], y = ws.yy[start + i];
+    atomicMin(&minRow[cl], x);
+    atomicMax(&maxRow[cl], x);
+    atomicMin(&minCol[cl], y);
+    atomicMax(&maxCol[cl], y);
+  }
+  __syncwarp();
+  for (uint32_t i = first + lane; i < last; i += 32) {
+    const uint16_t id = ws.moduleInd[start + i];
+    if (id == kInvId || id != me) continue;
+    const int cl = ws.clus[start + i];
+    if (cl < 0 || cl >= int(nclus)) continue;
+    const uint32_t x = ws.xx[start + i], y = ws.yy[start + i];
+    const int32_t ch = ws.adc[start + i];
+    atomicAdd(&chg[cl], ch);
+    if (minRow[cl] == x) atomicAdd(&Qfx[cl], ch);
+    if (maxRow[cl] == x) atomicAdd(&Qlx[cl], ch);
+    if (minCol[cl] == y) atomicAdd(&Qfy[cl], ch);
+    if (maxCol[cl] == y) atomicAdd(&Qly[cl], ch);
+  }
+  __syncwarp();
+  if (lane < nclus) {
+    const uint32_t h = ws.clusModuleStart[size_t(e) * kModStride + me] + lane;
+    if (h < uint32_t(PF_MAX_HITS))
+      writeHit(ws, size_t(e) * kHitCap, h, me, es.det[me], *es.common, *es.bs, minRow[lane], maxRow[lane],
+               minCol[lane], maxCol[lane], Qfx[lane], Qlx[lane], Qfy[lane], Qly[lane], chg[lane]);
   }
 }
 
@@ -1008,7 +1109,10 @@ cudaError_t runLocal(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaSt
                                  stream>>>(ws));
   PG_PROBED("kFindClustersBig", stream, kFindClustersBig<<<dim3(64, nEvents), kClusThreads, 0, stream>>>(ws));
   PG_PROBED("kHitsModuleStart", stream, kHitsModuleStart<<<nEvents, 1024, 0, stream>>>(es, ws));
-  PG_PROBED("kGetHits", stream, kGetHits<<<dim3(kMaxModules, nEvents), kHitThreads, 0, stream>>>(es, ws));
+  PG_PROBED("kGetHits", stream,
+            kGetHitsSmall<<<dim3((kMaxModules + kHitWarps - 1) / kHitWarps, nEvents), kHitWarps * 32, 0, stream>>>(es,
+                                                                                                               ws));
+  PG_PROBED("kGetHitsBig", stream, kGetHitsBig<<<dim3(64, nEvents), kHitThreads, 0, stream>>>(es, ws));
   // phi histogram: count, exclusive scan, unordered fill, per-bin ordering
   uint32_t* cursor = ws.jCount;  // scratch: the doublet counters are not in use yet
   PG_PROBED("kZeroU32", stream, kZeroU32<<<dim3(2, nEvents), 1024, 0, stream>>>(ws.phiOff, kPhiStride, kPhiStride, nEvents));

@@ -72,7 +72,7 @@ struct EventCounters {
   uint32_t nBig[4];             // long segments queued by each list ordering
   uint32_t nBigMod;             // modules queued for the block clusterizer
   uint32_t nSegList[4];         // list segments that received a second entry, per list ordering
-  uint32_t pad[1];
+  uint32_t nBigHitMod;          // modules queued for the block rechit kernel
 };
 
 // ---------------------------------------------------------------- ES on device

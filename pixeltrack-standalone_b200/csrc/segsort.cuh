@@ -5,8 +5,8 @@
 // distinct).
 //
 //  kSortListed one thread per segment the fill noted (the segments that got
-//              a second entry): n <= 16 sorted in registers by a bitonic
-//              network; 16 < n <= 256 handed to the warp (rank sort, one
+//              a second entry): n <= 32 sorted in registers by a bitonic
+//              network; 32 < n <= 256 handed to the warp (rank sort, one
 //              segment at a time, ballot over the lanes that hold one);
 //              n > 256 appended to a per-event list for kSortBig.
 //  kSortBig    one block per long segment: rank sort in shared memory.
@@ -19,18 +19,19 @@ namespace pixgpu {
 
 constexpr uint32_t kBigSort = 4096;  // longest segment ordered in shared memory
 
-template <typename T>
-__device__ __forceinline__ void sortRegs16(T* seg, uint32_t n, bool desc) {
-  T v[16];
+// bitonic network over N registers (N a power of two, n <= N elements)
+template <uint32_t N, typename T>
+__device__ __forceinline__ void sortRegs(T* seg, uint32_t n, bool desc) {
+  T v[N];
   const T pad = desc ? T(0) : T(~T(0));
 #pragma unroll
-  for (uint32_t i = 0; i < 16; ++i) v[i] = i < n ? seg[i] : pad;
+  for (uint32_t i = 0; i < N; ++i) v[i] = i < n ? seg[i] : pad;
 #pragma unroll
-  for (uint32_t k = 2; k <= 16; k <<= 1) {
+  for (uint32_t k = 2; k <= N; k <<= 1) {
 #pragma unroll
     for (uint32_t j = k >> 1; j > 0; j >>= 1) {
 #pragma unroll
-      for (uint32_t i = 0; i < 16; ++i) {
+      for (uint32_t i = 0; i < N; ++i) {
         const uint32_t l = i ^ j;
         if (l > i) {
           const bool up = (i & k) == 0;
@@ -44,8 +45,8 @@ __device__ __forceinline__ void sortRegs16(T* seg, uint32_t n, bool desc) {
   }
   // ascending with the pads last; descending reads it backwards (pads are 0)
 #pragma unroll
-  for (uint32_t i = 0; i < 16; ++i)
-    if (i < n) seg[i] = desc ? v[15 - i] : v[i];
+  for (uint32_t i = 0; i < N; ++i)
+    if (i < n) seg[i] = desc ? v[N - 1 - i] : v[i];
 }
 
 template <typename T>
@@ -78,8 +79,11 @@ __global__ void kSortListed(T* data, size_t dataStride, const uint32_t* off, siz
       b = min(o[s], dataCap);
       n = min(o[s + 1], dataCap) - b;
     }
-    if (n >= 2 && n <= 16) sortRegs16(d + b, n, desc);
-    uint32_t m = __ballot_sync(0xffffffffu, n > 16 && n <= 256);
+    if (n >= 2 && n <= 16)
+      sortRegs<16>(d + b, n, desc);
+    else if (n > 16 && n <= 32)
+      sortRegs<32>(d + b, n, desc);
+    uint32_t m = __ballot_sync(0xffffffffu, n > 32 && n <= 256);
     while (m) {
       const int l = __ffs(m) - 1;
       m &= m - 1;

@@ -13,6 +13,8 @@
 namespace pixgpu {
 cudaError_t fitDirect(int N, uint32_t n, const double* hits, const float* ge, double B, float* state, float* cov,
                       float* pt, float* eta, float* chi2, cudaStream_t stream);
+cudaError_t fitDirectMixed(int N, uint32_t n, const double* hits, const float* ge, double B, float* state, float* cov,
+                           float* pt, float* eta, float* chi2, cudaStream_t stream);
 
 int fail(pg_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;
@@ -746,6 +748,14 @@ int pg_fit_broken_line(pg_ctx* c, int N, uint32_t n, const double* hits, const f
                        float* cov, float* pt, float* eta, float* chi2, void* stream) {
   if (!c || (N != 3 && N != 4)) return PG_ERR_ARG;
   cudaError_t e = fitDirect(N, n, hits, ge, B, state, cov, pt, eta, chi2, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cudaFail(c, e, "fit launch");
+  return PG_OK;
+}
+
+int pg_fit_broken_line_mixed(pg_ctx* c, int N, uint32_t n, const double* hits, const float* ge, double B, float* state,
+                       float* cov, float* pt, float* eta, float* chi2, void* stream) {
+  if (!c || (N != 3 && N != 4)) return PG_ERR_ARG;
+  cudaError_t e = fitDirectMixed(N, n, hits, ge, B, state, cov, pt, eta, chi2, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cudaFail(c, e, "fit launch");
   return PG_OK;
 }

@@ -598,6 +598,8 @@ __global__ void kBLFitDirect(uint32_t n, const double* hits, const float* hge, d
   }
 }
 
+#include "k_fit_mixed.cuh"
+
 }  // namespace
 
 cudaError_t runFits(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
@@ -619,6 +621,20 @@ cudaError_t fitDirect(int N, uint32_t n, const double* hits, const float* ge, do
     PG_PROBED("kBLFitDirect", stream, kBLFitDirect<3><<<blocks, 128, 0, stream>>>(n, hits, ge, B, state, cov, pt, eta, chi2));
   else
     PG_PROBED("kBLFitDirect", stream, kBLFitDirect<4><<<blocks, 128, 0, stream>>>(n, hits, ge, B, state, cov, pt, eta, chi2));
+  return cudaGetLastError();
+}
+
+cudaError_t fitDirectMixed(int N, uint32_t n, const double* hits, const float* ge, double B, float* state, float* cov,
+                           float* pt, float* eta, float* chi2, cudaStream_t stream) {
+  uint32_t blocks = (n + 127) / 128;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks == 0) return cudaSuccess;
+  if (N == 3)
+    PG_PROBED("kBLFitDirectMixed", stream,
+              kBLFitDirectMixed<3><<<blocks, 128, 0, stream>>>(n, hits, ge, B, state, cov, pt, eta, chi2));
+  else
+    PG_PROBED("kBLFitDirectMixed", stream,
+              kBLFitDirectMixed<4><<<blocks, 128, 0, stream>>>(n, hits, ge, B, state, cov, pt, eta, chi2));
   return cudaGetLastError();
 }
 

@@ -471,6 +471,23 @@ def run_ours(a):
                     "admission_waits": st["admission_waits"]}
             sc.close()
             out["serving"] = {"pu": PU, "requests": a.serve, "max_batch": a.serve_batch, "slots": 4, "points": sv}
+            # uneven pileup: PU log-uniform in [30, 250], Poisson arrivals
+            rng = np.random.default_rng(7)
+            pus = np.exp(rng.uniform(np.log(30), np.log(250), 96))
+            with cf.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+                mraws = list(ex.map(lambda k: det.event(SEED0 + 300000 + k, float(pus[k])), range(len(pus))))
+            mc = pixgpu.Chain(det.es, max_events=a.serve_batch, max_words_per_batch=a.serve_batch * 300000, slots=4,
+                              device=dev, pool_words=128 * 1000 * 1000)
+            mc.prepare(a.serve_batch)
+            mv = {}
+            for rate in (1000.0, 2000.0):
+                st, _ = mc.serve(mraws, a.serve // 2, rate_hz=rate, max_batch=a.serve_batch, seed=13, upload_threads=4)
+                mv["%.0f Hz" % rate] = {"offered_hz": st["offered_hz"], "events_per_s": st["events_per_s"],
+                                        "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_batch": st["mean_batch"],
+                                        "admission_waits": st["admission_waits"]}
+            mc.close()
+            out["serving_mixed_pu"] = {"pu": "log-uniform 30-250", "distinct_events": len(mraws),
+                                       "requests": a.serve // 2, "points": mv}
 
         # ------------------------------------------------------------ fits: FP64 and mixed precision
         out["fits"] = fit_leg(det, dev, torch)

@@ -44,6 +44,36 @@ __device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* sh,
   return r;
 }
 
+// The same for 64-bit values (several packed counters scanned at once);
+// `sh` holds >= 33 uint64_t.
+__device__ __forceinline__ uint64_t blockExclusiveScan64(uint64_t v, uint64_t* sh, uint64_t* total) {
+  uint32_t w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  uint64_t inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint64_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (laneId() >= uint32_t(o)) inc += t;
+  }
+  if (laneId() == 31) sh[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    uint64_t x = laneId() < nw ? sh[laneId()] : 0;
+    uint64_t xi = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint64_t t = __shfl_up_sync(0xffffffffu, xi, o);
+      if (laneId() >= uint32_t(o)) xi += t;
+    }
+    if (laneId() < nw) sh[laneId()] = xi - x;
+    if (laneId() == nw - 1) sh[32] = xi;
+  }
+  __syncthreads();
+  uint64_t r = sh[w] + inc - v;
+  *total = sh[32];
+  __syncthreads();
+  return r;
+}
+
 // Orders the n elements of seg[] in place (ascending, or descending if desc),
 // using one warp: rank of each element = number of smaller elements.  Keys
 // are distinct.  For n <= 32*kPer only; larger segments fall back to a

@@ -809,45 +809,56 @@ __global__ void kTupleDet(Workspace ws) {
 }
 
 // TupleMultiplicity: counts per hit multiplicity, then fill (order irrelevant to the fits)
-__global__ void kMultiplicityCount(Workspace ws) {
-  uint32_t e = blockIdx.y;
-  uint32_t nt = ws.ev[e].nTuples;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
-  const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
-  uint32_t* tm = ws.tmOff + size_t(e) * 16;
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
-    uint32_t nh = tupleSize(toff, t);
-    if (nh < 3 || q[t] == kDup) continue;
-    atomicAdd(&tm[nh], 1u);
-  }
-}
-__global__ void kMultiplicityScan(Workspace ws, uint32_t nEvents) {
-  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= nEvents) return;
-  uint32_t* tm = ws.tmOff + size_t(e) * 16;
-  uint32_t acc = 0;
-  for (int b = 0; b < 8; ++b) {
-    uint32_t v = tm[b];
-    tm[8 + b] = acc;  // start of bin b
-    if (v > PF_MAX_TUPLES) ws.ev[e].flags |= kFlagFitBinOverflow;
-    acc += v;
-    tm[b] = 0;        // reused as fill cursor
-  }
-  if (acc > PF_MAX_TUPLES) ws.ev[e].flags |= kFlagTmOverflow;
-}
-__global__ void kMultiplicityFill(Workspace ws) {
-  uint32_t e = blockIdx.y;
-  uint32_t nt = ws.ev[e].nTuples;
+// TupleMultiplicity (countMultiplicity/fillMultiplicity, Impl.h:304-338):
+// one block per event counts the non-duplicate tuples of 3, 4 and 5 hits,
+// places the bins, and fills them in ascending tuple order (the serial fill
+// order) with one scan of the three counters packed into 64 bits, so that
+// the content stays deterministic when a bin overflows.
+__global__ void __launch_bounds__(1024) kMultiplicity(Workspace ws) {
+  __shared__ uint32_t cnt[8], start[8];
+  __shared__ uint64_t scanSh[33];
+  const uint32_t e = blockIdx.x;
+  EventCounters* c = ws.ev + e;
+  const uint32_t nt = c->nTuples;
   const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
   const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
   uint32_t* tm = ws.tmOff + size_t(e) * 16;
   uint16_t* bins = ws.tmBins + size_t(e) * kTupleBins;
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
-    uint32_t nh = tupleSize(toff, t);
-    if (nh < 3 || q[t] == kDup) continue;
-    uint32_t p = atomicAdd(&tm[nh], 1u);
-    uint32_t pos = tm[8 + nh] + p;
-    if (pos < kTupleBins) bins[pos] = uint16_t(t);
+  auto binOf = [&](uint32_t t) -> uint32_t {  // 0: not binned
+    const uint32_t nh = tupleSize(toff, t);
+    return (nh < 3 || nh > 5 || q[t] == kDup) ? 0u : nh;
+  };
+  if (threadIdx.x < 8) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  for (uint32_t t = threadIdx.x; t < nt; t += blockDim.x) {
+    const uint32_t b = binOf(t);
+    if (b) atomicAdd(&cnt[b], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (int b = 0; b < 8; ++b) {
+      start[b] = acc;
+      tm[8 + b] = acc;  // start of bin b
+      tm[b] = cnt[b];
+      if (cnt[b] > PF_MAX_TUPLES) c->flags |= kFlagFitBinOverflow;
+      acc += cnt[b];
+    }
+    if (acc > PF_MAX_TUPLES) c->flags |= kFlagTmOverflow;
+  }
+  __syncthreads();
+  uint64_t carry = 0;
+  for (uint32_t t0 = 0; t0 < nt; t0 += blockDim.x) {
+    const uint32_t t = t0 + threadIdx.x;
+    const uint32_t b = t < nt ? binOf(t) : 0u;
+    const uint64_t key = b ? (uint64_t(1) << (20 * (b - 3))) : 0ull;
+    uint64_t tot;
+    const uint64_t pre = blockExclusiveScan64(key, scanSh, &tot) + carry;
+    if (b) {
+      const uint32_t pos = start[b] + uint32_t((pre >> (20 * (b - 3))) & 0xfffffu);
+      if (pos < kTupleBins) bins[pos] = uint16_t(t);
+    }
+    carry += tot;
   }
 }
 
@@ -1116,10 +1127,7 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   PG_PROBED("kEarlyDup", stream, kEarlyDup<<<g, 256, 0, stream>>>(ws));
   PG_PROBED("kTupleDet", stream, kTupleDet<<<g, 256, 0, stream>>>(ws));
   // ---- tuple multiplicity for the fits
-  PG_PROBED("kZero", stream, kZero<<<dim3(1, nEvents), 32, 0, stream>>>(ws.tmOff, 16, 16, nullptr, 0));
-  PG_PROBED("kMultiplicityCount", stream, kMultiplicityCount<<<g, 256, 0, stream>>>(ws));
-  PG_PROBED("kMultiplicityScan", stream, kMultiplicityScan<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents));
-  PG_PROBED("kMultiplicityFill", stream, kMultiplicityFill<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kMultiplicity", stream, kMultiplicity<<<nEvents, 1024, 0, stream>>>(ws));
   return cudaGetLastError();
 }
 

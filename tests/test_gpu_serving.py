@@ -158,3 +158,32 @@ def test_serving_results_same_alone_and_in_the_mix(default_detector, events, alo
     assert stats["mean_batch"] >= 1.0
     if rate_hz > 100000:
         assert stats["max_batch_seen"] > 1
+
+
+def test_mixed_pileup_batch_equals_alone(default_detector):
+    """A batch of uneven events with pileup from 20 to 200 (the capacities
+    saturate above ~PU80 and the events carry overflow flags): every event's
+    result is the same inside the batch as alone."""
+    import pixgpu
+    pus = [20, 200, 120, 60, 180, 35, 90, 150]
+    raws = [default_detector.event(700 + k, pu) for k, pu in enumerate(pus)]
+    c1 = pixgpu.Chain(default_detector.es, max_events=1, max_words_per_batch=300000, use_graphs=False)
+    alone = []
+    try:
+        for r in raws:
+            s = c1.submit([r])
+            c1.wait(s)
+            alone.append(c1.result(s, 0))
+            c1.release(s)
+    finally:
+        c1.close()
+    c = pixgpu.Chain(default_detector.es, max_events=8, max_words_per_batch=8 * 300000)
+    try:
+        s = c.submit(raws)
+        c.wait(s)
+        for k in range(len(raws)):
+            assert same(c.result(s, k), alone[k]) == [], (k, pus[k])
+        assert any(c.result(s, k)["flags"] for k in range(len(raws)))  # the dense events do overflow
+        c.release(s)
+    finally:
+        c.close()

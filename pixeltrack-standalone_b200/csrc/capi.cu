@@ -555,7 +555,20 @@ int pg_get_product(pg_ctx* c, uint32_t k, const char* name, void* dst, size_t ca
   if (n == "cellDoubletId") return copyOut(c, s, ws.cellDoubletId + cb, nc, dst, cap, count, elem);
   if (n == "cellLayerPair") return copyOut(c, s, ws.cellPair + cb, nc, dst, cap, count, elem);
   if (n == "outerHitOffRaw") return copyOut(c, s, ws.ohOff + size_t(k) * (kHitCap + 1), nh + 1, dst, cap, count, elem);
-  if (n == "outerHitCellsRaw") return copyOut(c, s, ws.ohCells + cb, nc, dst, cap, count, elem);
+  if (n == "outerHitCellsRaw") {
+    // the device orders only lists longer than the 128 the CA reads; the
+    // product gives every list in ascending order, as the serial fill does
+    int rc = copyOut(c, s, ws.ohCells + cb, nc, dst, cap, count, elem);
+    if (rc != PG_OK || !dst || nc == 0) return rc;
+    std::vector<uint32_t> off(size_t(nh) + 1);
+    cudaError_t e2 = cudaMemcpy(off.data(), ws.ohOff + size_t(k) * (kHitCap + 1), off.size() * 4,
+                                cudaMemcpyDeviceToHost);
+    if (e2 != cudaSuccess) return cudaFail(c, e2, "D2H outer-hit offsets");
+    uint32_t* cells = static_cast<uint32_t*>(dst);
+    for (uint32_t h = 0; h < nh; ++h)
+      std::sort(cells + std::min<size_t>(off[h], nc), cells + std::min<size_t>(off[h + 1], nc));
+    return PG_OK;
+  }
   if (n == "cellNbrOffRaw") return copyOut(c, s, ws.nbrOff + size_t(k) * (kCellCap + 1), nc + 1, dst, cap, count, elem);
   if (n == "cellNbrRaw") return copyOut(c, s, ws.nbr + size_t(k) * kEdgeCap, std::min(ec.nEdges, kEdgeCap), dst, cap, count, elem);
   if (n == "cellTrkOffRaw") return copyOut(c, s, ws.trkOff + size_t(k) * (kCellCap + 1), nc + 1, dst, cap, count, elem);

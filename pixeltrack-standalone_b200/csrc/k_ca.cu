@@ -309,7 +309,7 @@ __global__ void kZero(uint32_t* p, size_t stride, uint32_t n, const uint32_t* le
     p[size_t(e) * stride + i] = 0;
 }
 
-// isOuterHitOfCell fill (unordered), then per-hit ascending order
+// isOuterHitOfCell fill (unordered; lists longer than 128 are ordered after)
 __global__ void kOuterHitFill(Workspace ws) {
   uint32_t e = blockIdx.y;
   uint32_t n = ws.ev[e].nCells;
@@ -320,7 +320,9 @@ __global__ void kOuterHitFill(Workspace ws) {
     uint16_t oi = ws.cellOuter[cb + c];
     uint32_t p = atomicAdd(&cur[oi], 1u);
     ws.ohCells[cb + off[oi] + p] = c;
-    if (p == 1) noteSegment(ws, e, 0, oi);
+    // connect and fishbone read the first 128 cells of a hit (ascending):
+    // only longer lists need ordering here; fishbone orders the rest itself
+    if (p == PF_MAX_CELLS_PER_HIT) noteSegment(ws, e, 0, oi);
   }
 }
 
@@ -523,8 +525,8 @@ __global__ void kNbrPool(Workspace ws) {
 // ------------------------------------------------------------------ fishbone
 
 // gpuFishbone.h:21-90 (early fishbone), one warp per hit with >= 2 cells
-// ending on it.  The hit's cells (first 128, ascending) are staged in shared
-// memory from the isOuterHitOfCell-ordered records; lane ic compares cell ic
+// ending on it.  The hit's cells (first 128, put in ascending order here)
+// are staged in shared memory from the isOuterHitOfCell records; lane ic compares cell ic
 // with every later cell, as the serial double loop does.  Kills only write
 // doubletId = -1 and never change the `used` flags the loop reads, so the
 // lanes are independent.
@@ -534,6 +536,7 @@ __global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws) {
       szA[kFishWarps][PF_MAX_CELLS_PER_HIT];
   __shared__ uint16_t sdA[kFishWarps][PF_MAX_CELLS_PER_HIT];
   __shared__ uint8_t suA[kFishWarps][PF_MAX_CELLS_PER_HIT];
+  __shared__ uint32_t rawA[kFishWarps][PF_MAX_CELLS_PER_HIT], scA[kFishWarps][PF_MAX_CELLS_PER_HIT];
   const uint32_t e = blockIdx.y;
   const EventCounters* c = ws.ev + e;
   const uint32_t nHits = c->nHits;
@@ -550,17 +553,31 @@ __global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws) {
   float* sz = szA[w];
   uint16_t* sd = sdA[w];
   uint8_t* su = suA[w];
+  uint32_t* raw = rawA[w];
+  uint32_t* sc = scA[w];
   for (uint32_t h = blockIdx.x * kFishWarps + w; h < nHits; h += gridDim.x * kFishWarps) {
     const uint32_t b = ohOff[h], s = min(ohOff[h + 1] - b, uint32_t(PF_MAX_CELLS_PER_HIT));
     if (s < 2) continue;
     const float xo = hh.xg[h], yo = hh.yg[h], zo = hh.zg[h];
-    for (uint32_t k = lane; k < s; k += 32) {
-      const float4 r = ohRec[b + k];
-      sx[k] = r.x - xo;
-      sy[k] = r.y - yo;
-      sz[k] = r.z - zo;
-      sd[k] = ohDet[b + k];
-      su[k] = ws.cellUsed[cb + ohCells[b + k]];
+    // stage the hit's cells in ascending cell order (the list is filled
+    // unordered; up to 128 entries, at most 4 per lane)
+    for (uint32_t k = lane; k < s; k += 32) raw[k] = ohCells[b + k];
+    __syncwarp();
+#pragma unroll
+    for (uint32_t j = 0; j < PF_MAX_CELLS_PER_HIT / 32; ++j) {
+      const uint32_t k = lane + 32 * j;
+      if (k < s) {
+        const uint32_t cell = raw[k];
+        uint32_t r = 0;
+        for (uint32_t m = 0; m < s; ++m) r += raw[m] < cell ? 1u : 0u;
+        const float4 rec = ohRec[b + k];
+        sx[r] = rec.x - xo;
+        sy[r] = rec.y - yo;
+        sz[r] = rec.z - zo;
+        sd[r] = ohDet[b + k];
+        su[r] = ws.cellUsed[cb + cell];
+        sc[r] = cell;
+      }
     }
     __syncwarp();
     for (uint32_t ic = lane; ic < s; ic += 32) {
@@ -575,10 +592,10 @@ __global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws) {
         const float cos12 = xi * xj + yi * yj + zi * zj;
         if (di != sd[jc] && cos12 * cos12 >= 0.99999f * ni * nj) {
           if (ni > nj) {
-            ws.cellDoubletId[cb + ohCells[b + ic]] = -1;
+            ws.cellDoubletId[cb + sc[ic]] = -1;
             break;
           } else {
-            ws.cellDoubletId[cb + ohCells[b + jc]] = -1;
+            ws.cellDoubletId[cb + sc[jc]] = -1;
           }
         }
       }

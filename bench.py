@@ -71,6 +71,12 @@ KERNEL_BYTES = {
 }
 
 
+# DRAM bytes per event of a kernel (dram__bytes_read.sum + dram__bytes_write.sum
+# of one ncu capture on 16 PU50 events, divided by 16; traffic scales with the
+# events of a launch).  Source: profiles/kConnect_kDoubletWrite_kFishbone_pu50_b16.md
+NCU_DRAM_BYTES_PER_EVENT = {"kConnect": 9.35e6, "kDoubletWrite": 3.45e6, "kFishbone": 8.37e6}
+
+
 def chain_bytes(u):
     """Whole-chain algorithmic bytes: 92.5 W + 64 H + 100 C + 8 E + 76 Sh + 42 N + 92 T (T = N fitted)."""
     return 92.5 * u["W"] + 64 * u["H"] + 100 * u["C"] + 8 * u["E"] + 76 * u["Sh"] + 42 * u["N"] + 92 * u["N"]
@@ -383,7 +389,9 @@ def run_ours(a):
         bytes_per_launch = KERNEL_BYTES[top](u_evt) * B / launches_of_top
         ach = bytes_per_launch / (kernel_ms / 1e3) / 1e9
         roof = {"bound": "hbm", "kernel": top, "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                "traffic": None, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
+                "traffic": (NCU_DRAM_BYTES_PER_EVENT[top] * B / launches_of_top
+                            if top in NCU_DRAM_BYTES_PER_EVENT else None),
+                "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback 6650 GB/s",
                 "bytes_per_launch": bytes_per_launch, "launch_ms": kernel_ms, "launches_timed": len(probe_ms)}
     chain_ach = chain_bytes(u_evt) * value / world / 1e9

@@ -124,6 +124,10 @@ void makeVertices(const CA& ca, Vertices& v);
 void brokenLineFit(int N, const double* hits /*3xN col-major*/, const float* hits_ge /*6xN*/, double B,
                    float* state5, float* cov15, float* pt, float* eta, float* chi2);
 
+// Riemann fit of one tuple of N (3 or 4) hits; same I/O as brokenLineFit
+void riemannFit(int N, const double* hits /*3xN col-major*/, const float* hits_ge /*6xN*/, double B, float* state5,
+                float* cov15, float* pt, float* eta, float* chi2);
+
 // whole chain for one raw.bin event record
 void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev);
 

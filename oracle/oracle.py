@@ -72,6 +72,7 @@ class Oracle(_Named):
         self.lib.or_time_events.restype = ctypes.c_double
         self.lib.or_fit.argtypes = [ctypes.c_int, ctypes.c_uint32] + [ctypes.c_void_p] * 2 + [ctypes.c_double] + \
             [ctypes.c_void_p] * 5
+        self.lib.or_fit_riemann.argtypes = self.lib.or_fit.argtypes
         self.lib.or_destroy.argtypes = [ctypes.c_void_p]
         self._keep = list(es_images)
         args = []
@@ -101,13 +102,14 @@ class Oracle(_Named):
             raise RuntimeError("oracle failed while timing")
         return wall, lat
 
-    def fit(self, N, hits, ge, B=0.0114256972711507):
+    def fit(self, N, hits, ge, B=0.0114256972711507, riemann=False):
         n = hits.shape[0]
         h = np.ascontiguousarray(hits[:, :N, :], dtype=np.float64)
         g = np.ascontiguousarray(ge[:, :N, :], dtype=np.float32)
         out = {"state": np.zeros((n, 5), np.float32), "cov": np.zeros((n, 15), np.float32),
                "pt": np.zeros(n, np.float32), "eta": np.zeros(n, np.float32), "chi2": np.zeros(n, np.float32)}
-        rc = self.lib.or_fit(N, n, h.ctypes.data, g.ctypes.data, B, out["state"].ctypes.data, out["cov"].ctypes.data,
+        fn = self.lib.or_fit_riemann if riemann else self.lib.or_fit
+        rc = fn(N, n, h.ctypes.data, g.ctypes.data, B, out["state"].ctypes.data, out["cov"].ctypes.data,
                              out["pt"].ctypes.data, out["eta"].ctypes.data, out["chi2"].ctypes.data)
         if rc != 0:
             raise RuntimeError("oracle fit failed")
@@ -169,6 +171,23 @@ class Reference(_Named):
 
     def last_seconds(self):
         return self.lib.pr_last_seconds(self._h)
+
+
+def ref_fit_riemann(N, hits, ge, B=0.0114256972711507):
+    """The reference's own Riemann fit (RiemannFit.h through the checker
+    build) on standalone tuples, in the layout of Oracle.fit."""
+    lib = ctypes.CDLL(REF_LIB)
+    lib.pr_fit_riemann.argtypes = [ctypes.c_int, ctypes.c_uint32] + [ctypes.c_void_p] * 2 + [ctypes.c_double] + \
+        [ctypes.c_void_p] * 5
+    n = hits.shape[0]
+    h = np.ascontiguousarray(hits[:, :N, :], dtype=np.float64)
+    g = np.ascontiguousarray(ge[:, :N, :], dtype=np.float32)
+    out = {"state": np.zeros((n, 5), np.float32), "cov": np.zeros((n, 15), np.float32),
+           "pt": np.zeros(n, np.float32), "eta": np.zeros(n, np.float32), "chi2": np.zeros(n, np.float32)}
+    if lib.pr_fit_riemann(N, n, h.ctypes.data, g.ctypes.data, B, out["state"].ctypes.data, out["cov"].ctypes.data,
+                          out["pt"].ctypes.data, out["eta"].ctypes.data, out["chi2"].ctypes.data) != 0:
+        raise RuntimeError("reference Riemann fit failed")
+    return out
 
 
 def ref_time_events(datadir, raws, threads=1):

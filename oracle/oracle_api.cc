@@ -240,6 +240,16 @@ int or_fit(int N, uint32_t n, const double* hits, const float* ge, double B, flo
   return 0;
 }
 
+// Riemann fit of n tuples, same layout as or_fit.
+int or_fit_riemann(int N, uint32_t n, const double* hits, const float* ge, double B, float* state, float* cov,
+                   float* pt, float* eta, float* chi2) {
+  if (N != 3 && N != 4) return -1;
+  for (uint32_t t = 0; t < n; ++t)
+    oracle::riemannFit(N, hits + size_t(t) * N * 3, ge + size_t(t) * N * 6, B, state + size_t(t) * 5,
+                       cov + size_t(t) * 15, pt + t, eta + t, chi2 + t);
+  return 0;
+}
+
 // Vertexing of a given track SoA (n tuples): tuple_off[n+1], quality[n],
 // pt[n], state[n*5], cov[n*15]; outputs idv[n], zv/wv/chi2/ptv2/ndof/sortInd
 // (1024 each) and the vertex count.  Test infrastructure for the vertex

@@ -73,6 +73,7 @@
 #include "plugin-SiPixelClusterizer/SiPixelRawToClusterGPUKernel.h"
 #include "plugin-SiPixelRecHits/PixelRecHits.h"
 #include "plugin-PixelVertexFinding/gpuVertexFinder.h"
+#include "plugin-PixelTriplets/RiemannFit.h"
 
 namespace {
 
@@ -491,9 +492,47 @@ double pr_time_events(const char* datadir, const uint8_t* const* raws, const siz
 
 }  // extern "C"
 
-// The Riemann fit sources need a 3x3 symmetric eigen-solver that the shim
-// does not provide; the default configuration (useRiemannFit=false,
-// CAHitNtupletGeneratorOnGPU.cc:49) never calls this entry.
-void HelixFitOnGPU::launchRiemannKernelsOnCPU(HitsView const*, uint32_t, uint32_t) {
-  throw std::runtime_error("Riemann fit is not part of the checker build");
+// Riemann fit of n standalone tuples of N (3 or 4) hits through the
+// reference's own Rfit functions, in the order of kernelFastFit,
+// kernelCircleFit and kernelLineFit (RiemannFitOnGPU.h:20-162), with the
+// result packing of kernelLineFit (:156-162).  Layout as the oracle's or_fit:
+// hits[(t*N+i)*3+k], ge[(t*N+i)*6+k]; outputs state[t*5], cov[t*15],
+// pt/eta/chi2[t].
+template <int N>
+static void refRiemann(uint32_t n, const double* hits, const float* ge, double B, float* state, float* cov, float* pt,
+                       float* eta, float* chi2) {
+  auto soa = std::make_unique<pixelTrack::TrackSoA>();
+  for (uint32_t t = 0; t < n; ++t) {
+    Rfit::Matrix3xNd<N> h;
+    Eigen::Matrix<float, 6, N> g;
+    for (int i = 0; i < N; ++i) {
+      for (int k = 0; k < 3; ++k) h(k, i) = hits[(size_t(t) * N + i) * 3 + k];
+      for (int k = 0; k < 6; ++k) g(k, i) = ge[(size_t(t) * N + i) * 6 + k];
+    }
+    Rfit::Vector4d fast_fit;
+    Rfit::Fast_fit(h, fast_fit);
+    Rfit::VectorNd<N> rad = (h.block(0, 0, 2, N).colwise().norm());
+    Rfit::Matrix2Nd<N> hits_cov = Rfit::Matrix2Nd<N>::Zero();
+    Rfit::loadCovariance2D(g, hits_cov);
+    Rfit::circle_fit circle = Rfit::Circle_fit(h.block(0, 0, 2, N), hits_cov, fast_fit, rad, B, true);
+    auto const& line = Rfit::Line_fit(h, g, circle, fast_fit, B, true);
+    Rfit::fromCircleToPerigee(circle);
+    soa->stateAtBS.copyFromCircle(circle.par, circle.cov, line.par, line.cov, 1.f / float(B), 0);
+    for (int k = 0; k < 5; ++k) state[size_t(t) * 5 + k] = soa->stateAtBS.state(0)(k);
+    for (int k = 0; k < 15; ++k) cov[size_t(t) * 15 + k] = soa->stateAtBS.covariance(0)(k);
+    pt[t] = B / std::abs(circle.par(2));
+    eta[t] = asinhf(line.par(0));
+    chi2[t] = (circle.chi2 + line.chi2) / (2 * N - 5);
+  }
+}
+
+extern "C" int pr_fit_riemann(int N, uint32_t n, const double* hits, const float* ge, double B, float* state,
+                              float* cov, float* pt, float* eta, float* chi2) {
+  if (N == 3)
+    refRiemann<3>(n, hits, ge, B, state, cov, pt, eta, chi2);
+  else if (N == 4)
+    refRiemann<4>(n, hits, ge, B, state, cov, pt, eta, chi2);
+  else
+    return -1;
+  return 0;
 }

@@ -80,10 +80,10 @@ def build_synth():
 
 def build_oracle():
     d = os.path.join(ROOT, "oracle")
-    srcs = [os.path.join(d, f) for f in ("oracle_local.cc", "oracle_ca.cc", "oracle_fit.cc", "oracle_vertex.cc",
-                                         "oracle_api.cc")]
+    srcs = [os.path.join(d, f) for f in ("oracle_local.cc", "oracle_ca.cc", "oracle_fit.cc", "oracle_riemann.cc",
+                                         "oracle_vertex.cc", "oracle_api.cc")]
     target = os.path.join(d, "liboracle.so")
-    if _stale(target, srcs + [os.path.join(d, "oracle.h")] + _headers(INC)):
+    if _stale(target, srcs + [os.path.join(d, h) for h in ("oracle.h", "oracle_mat.h", "sym_eigen.h")] + _headers(INC)):
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-pthread", "-I", INC] + srcs + ["-o", target])
     return target
 

@@ -264,45 +264,57 @@ def pipeline(chain, torch, n_steps, submit, on_done):
 
 
 def fit_leg(det, dev, torch, n=1000000):
-    """1M seeded MS-smeared tuples of 3 and of 4 hits: broken-line fits per
-    second in FP64 (the reference's precision) and in the mixed-precision
-    variant, and the variant's deviation from the FP64 result."""
+    """1M seeded MS-smeared tuples of 3 and of 4 hits: broken-line and Riemann
+    fits per second in FP64 (the reference's precision) and in their
+    mixed-precision variants, and each variant's deviation from its FP64
+    result (max and rms over the tuples)."""
     import pixgpu
     c = pixgpu.Chain(det.es, max_events=1, max_words_per_batch=300000, device=dev)
     lib = pixgpu.gpu_lib()
+    methods = {"broken_line": (lib.pg_fit_broken_line, lib.pg_fit_broken_line_mixed),
+               "riemann": (lib.pg_fit_riemann, lib.pg_fit_riemann_mixed)}
     res = {}
     for nh in (3, 4):
         hits, ge, _ = pixgpu.fit_tuples(20261203 + nh, n, nh)
         dh = torch.from_numpy(np.ascontiguousarray(hits)).cuda()
         dg = torch.from_numpy(np.ascontiguousarray(ge)).cuda()
-        outs = {}
-        rates = {}
-        for label, fn in (("fp64", lib.pg_fit_broken_line), ("mixed", lib.pg_fit_broken_line_mixed)):
-            o = [torch.empty(n * k, dtype=torch.float32, device="cuda") for k in (5, 15, 1, 1, 1)]
-            st = torch.cuda.current_stream().cuda_stream
-            args = (c._h, nh, n, dh.data_ptr(), dg.data_ptr(), pixgpu.B_FIELD, *[x.data_ptr() for x in o], st)
-            for _ in range(2):
-                fn(*args)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize()
-            e0.record()
-            for _ in range(5):
-                fn(*args)
-            e1.record()
-            e1.synchronize()
-            rates[label] = n / (e0.elapsed_time(e1) / 5 / 1e3)
-            outs[label] = [x.cpu().numpy().astype(np.float64) for x in o]
-        sa, sb = outs["fp64"][0].reshape(n, 5), outs["mixed"][0].reshape(n, 5)
-        dk = np.abs(1 / outs["mixed"][2] - 1 / outs["fp64"][2])
-        d = np.abs(sb - sa)
-        err = {"inv_pt_per_gev": dk, "phi": d[:, 0], "d0_cm": d[:, 1], "cot_theta": d[:, 3], "z0_cm": d[:, 4]}
-        res["%d_hits" % nh] = {"fits_per_s": rates,
-                               "mixed_vs_fp64": {k: {"max": float(v.max()), "rms": float(np.sqrt((v ** 2).mean()))}
-                                                 for k, v in err.items()}}
+        per = {}
+        for method, fns in methods.items():
+            outs = {}
+            rates = {}
+            for label, fn in zip(("fp64", "mixed"), fns):
+                o = [torch.empty(n * k, dtype=torch.float32, device="cuda") for k in (5, 15, 1, 1, 1)]
+                st = torch.cuda.current_stream().cuda_stream
+                args = (c._h, nh, n, dh.data_ptr(), dg.data_ptr(), pixgpu.B_FIELD, *[x.data_ptr() for x in o], st)
+                for _ in range(2):
+                    if fn(*args) != 0:
+                        raise RuntimeError("fit launch failed")
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                for _ in range(5):
+                    fn(*args)
+                e1.record()
+                e1.synchronize()
+                rates[label] = n / (e0.elapsed_time(e1) / 5 / 1e3)
+                outs[label] = [x.cpu().numpy().astype(np.float64) for x in o]
+            sa, sb = outs["fp64"][0].reshape(n, 5), outs["mixed"][0].reshape(n, 5)
+            fin = np.isfinite(sa).all(axis=1) & np.isfinite(sb).all(axis=1)
+            dk = np.abs(1 / outs["mixed"][2] - 1 / outs["fp64"][2])[fin]
+            d = np.abs(sb - sa)[fin]
+            err = {"inv_pt_per_gev": dk, "phi": d[:, 0], "d0_cm": d[:, 1], "cot_theta": d[:, 3], "z0_cm": d[:, 4]}
+            per[method] = {"fits_per_s": rates, "both_finite": int(fin.sum()),
+                           "mixed_vs_fp64": {k: {"max": float(v.max()), "rms": float(np.sqrt((v ** 2).mean()))}
+                                             for k, v in err.items()}}
+        res["%d_hits" % nh] = per
     c.close()
     return {"tuples": n, "per_multiplicity": res,
-            "mixed": "FP32 arithmetic; FP64 for the reference circle, radial residuals, Cholesky solves and "
-                     "covariance propagation"}
+            "mixed": {"broken_line": "FP32 arithmetic; FP64 for the reference circle, radial residuals, Cholesky "
+                                     "solves and covariance propagation",
+                      "riemann": "FP32 for the multiple-scattering models, the s-z projection and the "
+                                 "single-precision eigen-solves of the numerical Jacobian; FP64 for the prefit "
+                                 "circle, the radiation-length path lengths, the Riemann matrix and its smallest "
+                                 "eigenvector, the Cholesky solves and the covariance propagation"}}
 
 
 def run_ours(a):

@@ -23,6 +23,7 @@
  *                        TrackingRecHit2DCPU, PixelTrackHeterogeneous, ZVertexHeterogeneous
  *                        (the *SoAFromCUDA transfer modules of the CUDA program)
  *   pg_fit_broken_line   HelixFitOnGPU::launchBrokenLineKernels (BrokenLineFitOnGPU.cc:3-68)
+ *   pg_fit_riemann       HelixFitOnGPU::launchRiemannKernelsOnCPU (RiemannFitOnGPU.cc:3-110)
  *   pg_submit / pg_query / pg_wait / pg_result / pg_release
  *                        the acquire()/produce() split of the CUDA modules (ExternalWork:
  *                        work queued on the event's stream, the framework told when done)
@@ -264,6 +265,23 @@ int pg_fit_broken_line(pg_ctx* ctx, int N, uint32_t n, const double* hits, const
  * the FP64 result is measured in tests/test_gpu_fit_mixed.py. */
 int pg_fit_broken_line_mixed(pg_ctx* ctx, int N, uint32_t n, const double* hits, const float* ge, double B, float* state,
                        float* cov, float* pt, float* eta, float* chi2, void* stream);
+
+/* Riemann fits of n tuples of N (3 or 4) hits already on the device, same
+ * layout as pg_fit_broken_line.  Replaces HelixFitOnGPU::launchRiemannKernelsOnCPU
+ * (RiemannFitOnGPU.cc:3-110; kernelFastFit/kernelCircleFit/kernelLineFit,
+ * RiemannFitOnGPU.h:20-162), the fit that CAHitNtupletGeneratorOnGPU selects
+ * with useRiemannFit (CAHitNtupletGeneratorOnGPU.cc:49). */
+int pg_fit_riemann(pg_ctx* ctx, int N, uint32_t n, const double* hits, const float* ge, double B, float* state,
+                   float* cov, float* pt, float* eta, float* chi2, void* stream);
+
+/* The Riemann fits in mixed precision: FP32 for the multiple-scattering
+ * models, the s-z projection and the single-precision eigen-solves of the
+ * numerical Jacobian; FP64 for the prefit circle, the path lengths of the
+ * radiation-length model, the Riemann matrix and its smallest eigenvector,
+ * the Cholesky inversions with their solves and the covariance propagation.  A variant beside the FP64 fit; its deviation from the FP64
+ * result is measured in tests/test_gpu_riemann.py. */
+int pg_fit_riemann_mixed(pg_ctx* ctx, int N, uint32_t n, const double* hits, const float* ge, double B, float* state,
+                         float* cov, float* pt, float* eta, float* chi2, void* stream);
 
 #ifdef __cplusplus
 }

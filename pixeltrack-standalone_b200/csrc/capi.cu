@@ -15,6 +15,8 @@ cudaError_t fitDirect(int N, uint32_t n, const double* hits, const float* ge, do
                       float* pt, float* eta, float* chi2, cudaStream_t stream);
 cudaError_t fitDirectMixed(int N, uint32_t n, const double* hits, const float* ge, double B, float* state, float* cov,
                            float* pt, float* eta, float* chi2, cudaStream_t stream);
+cudaError_t fitDirectRiemann(int N, uint32_t n, const double* hits, const float* ge, double B, float* state,
+                             float* cov, float* pt, float* eta, float* chi2, bool mixed, cudaStream_t stream);
 
 int fail(pg_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;
@@ -769,6 +771,24 @@ int pg_fit_broken_line_mixed(pg_ctx* c, int N, uint32_t n, const double* hits, c
                        float* cov, float* pt, float* eta, float* chi2, void* stream) {
   if (!c || (N != 3 && N != 4)) return PG_ERR_ARG;
   cudaError_t e = fitDirectMixed(N, n, hits, ge, B, state, cov, pt, eta, chi2, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cudaFail(c, e, "fit launch");
+  return PG_OK;
+}
+
+int pg_fit_riemann(pg_ctx* c, int N, uint32_t n, const double* hits, const float* ge, double B, float* state,
+                   float* cov, float* pt, float* eta, float* chi2, void* stream) {
+  if (!c || (N != 3 && N != 4)) return PG_ERR_ARG;
+  cudaError_t e =
+      fitDirectRiemann(N, n, hits, ge, B, state, cov, pt, eta, chi2, false, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cudaFail(c, e, "fit launch");
+  return PG_OK;
+}
+
+int pg_fit_riemann_mixed(pg_ctx* c, int N, uint32_t n, const double* hits, const float* ge, double B, float* state,
+                         float* cov, float* pt, float* eta, float* chi2, void* stream) {
+  if (!c || (N != 3 && N != 4)) return PG_ERR_ARG;
+  cudaError_t e =
+      fitDirectRiemann(N, n, hits, ge, B, state, cov, pt, eta, chi2, true, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cudaFail(c, e, "fit launch");
   return PG_OK;
 }

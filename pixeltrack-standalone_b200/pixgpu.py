@@ -276,6 +276,8 @@ def gpu_lib():
         _gpu.pg_fit_broken_line.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32] + [ctypes.c_void_p] * 2 + \
             [ctypes.c_double] + [ctypes.c_void_p] * 6
         _gpu.pg_fit_broken_line_mixed.argtypes = _gpu.pg_fit_broken_line.argtypes
+        _gpu.pg_fit_riemann.argtypes = _gpu.pg_fit_broken_line.argtypes
+        _gpu.pg_fit_riemann_mixed.argtypes = _gpu.pg_fit_broken_line.argtypes
         _gpu.pg_get_config.argtypes = [ctypes.c_void_p, ctypes.POINTER(Config)]
         _gpu.pg_default_config.argtypes = [ctypes.POINTER(Config)]
         _gpu.pg_submit.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_char_p),
@@ -528,9 +530,10 @@ class Chain:
         self._check(rc, "pg_serve")
         return {n: getattr(st, n) for n, _ in ServeStats._fields_}, lat
 
-    def fit(self, N, hits, ge, B=B_FIELD, mixed=False):
+    def fit(self, N, hits, ge, B=B_FIELD, mixed=False, riemann=False):
         """Broken-line fit of host arrays hits[n, N, 3] (f64), ge[n, N, 6] (f32) on the device;
-        mixed=True runs the FP32 variant with FP64 Cholesky solves and covariance propagation."""
+        mixed=True runs the FP32 variant with FP64 Cholesky solves and covariance propagation;
+        riemann=True runs the Riemann fit instead (with mixed=True, its mixed-precision variant)."""
         import torch
         n = hits.shape[0]
         dh = torch.from_numpy(np.ascontiguousarray(hits[:, :N, :])).cuda()
@@ -541,9 +544,16 @@ class Chain:
         eta = torch.empty(n, dtype=torch.float32, device="cuda")
         chi2 = torch.empty(n, dtype=torch.float32, device="cuda")
         s = torch.cuda.current_stream().cuda_stream
-        fn = gpu_lib().pg_fit_broken_line_mixed if mixed else gpu_lib().pg_fit_broken_line
+        if riemann and mixed:
+            fn, name = gpu_lib().pg_fit_riemann_mixed, "pg_fit_riemann_mixed"
+        elif riemann:
+            fn, name = gpu_lib().pg_fit_riemann, "pg_fit_riemann"
+        elif mixed:
+            fn, name = gpu_lib().pg_fit_broken_line_mixed, "pg_fit_broken_line_mixed"
+        else:
+            fn, name = gpu_lib().pg_fit_broken_line, "pg_fit_broken_line"
         self._check(fn(self._h, N, n, dh.data_ptr(), dg.data_ptr(), B, st.data_ptr(), cv.data_ptr(), pt.data_ptr(),
-                       eta.data_ptr(), chi2.data_ptr(), s), "pg_fit_broken_line")
+                       eta.data_ptr(), chi2.data_ptr(), s), name)
         torch.cuda.synchronize()
         return {"state": st.cpu().numpy(), "cov": cv.cpu().numpy(), "pt": pt.cpu().numpy(), "eta": eta.cpu().numpy(),
                 "chi2": chi2.cpu().numpy()}

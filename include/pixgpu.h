@@ -72,6 +72,8 @@ typedef struct pg_config {
   uint32_t use_graphs;           /* 1: the chain for each batch size is captured once as a CUDA graph */
   uint64_t pool_words;           /* device-resident input pool, in FED words (0: no pool) */
   double hbm_fraction;           /* share of free device memory the slots may take when slots == 0 */
+  uint32_t riemann_fit;          /* 1: Riemann fits in place of broken-line fits (the useRiemannFit
+                                    parameter of CAHitNtupletGeneratorOnGPU.cc:49, default off) */
 } pg_config;
 
 typedef struct pg_event_counts {

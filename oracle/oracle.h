@@ -116,7 +116,9 @@ void makeClusters(const ES& es, const Words& w, Digis& d, Clusters& c);
 // PixelRecHitGPUKernel::makeHits (plugin-SiPixelRecHits/PixelRecHits.cc:33-53)
 void makeHits(const ES& es, const Digis& d, const Clusters& c, Hits& h);
 // CAHitNtupletGeneratorOnGPU::makeTuples (plugin-PixelTriplets/CAHitNtupletGeneratorOnGPU.cc:96-126)
-void makeTuples(const ES& es, const Hits& h, CA& ca);
+// useRiemannFit selects the Riemann fit in place of the broken-line fit
+// (CAHitNtupletGeneratorOnGPU.cc:116-120; the reference's default is off)
+void makeTuples(const ES& es, const Hits& h, CA& ca, bool useRiemannFit = false);
 // gpuVertexFinder::Producer::make (plugin-PixelVertexFinding/gpuVertexFinderImpl.h:84-111)
 void makeVertices(const CA& ca, Vertices& v);
 
@@ -129,7 +131,7 @@ void riemannFit(int N, const double* hits /*3xN col-major*/, const float* hits_g
                 float* cov15, float* pt, float* eta, float* chi2);
 
 // whole chain for one raw.bin event record
-void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev);
+void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev, bool useRiemannFit = false);
 
 }  // namespace oracle
 

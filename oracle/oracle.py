@@ -54,7 +54,7 @@ class _Named:
 class Oracle(_Named):
     """Sequential restatement of the serial chain (oracle/*.cc)."""
 
-    def __init__(self, es_images):
+    def __init__(self, es_images, riemann_fit=False):
         path = os.path.join(HERE, "liboracle.so")
         if not os.path.exists(path):
             _build.build_oracle()
@@ -74,6 +74,7 @@ class Oracle(_Named):
             [ctypes.c_void_p] * 5
         self.lib.or_fit_riemann.argtypes = self.lib.or_fit.argtypes
         self.lib.or_destroy.argtypes = [ctypes.c_void_p]
+        self.lib.or_set_riemann.argtypes = [ctypes.c_void_p, ctypes.c_int]
         self._keep = list(es_images)
         args = []
         for b in self._keep:
@@ -82,6 +83,7 @@ class Oracle(_Named):
         if not self._h.value:
             raise RuntimeError("oracle: malformed ES images")
         self._get = self.lib.or_get
+        self.lib.or_set_riemann(self._h, 1 if riemann_fit else 0)
 
     def process(self, raw, names=None):
         if self.lib.or_process(self._h, raw, len(raw)) != 0:
@@ -152,7 +154,7 @@ def ref_available():
 class Reference(_Named):
     """The reference's own serial chain, compiled from its sources (checker build)."""
 
-    def __init__(self, datadir):
+    def __init__(self, datadir, riemann_fit=False):
         self.lib = ctypes.CDLL(REF_LIB)
         self.lib.pr_create.restype = ctypes.c_void_p
         self.lib.pr_create.argtypes = [ctypes.c_char_p]
@@ -163,6 +165,8 @@ class Reference(_Named):
         self.lib.pr_last_seconds.restype = ctypes.c_double
         self._h = ctypes.c_void_p(self.lib.pr_create(datadir.encode()))
         self._get = self.lib.pr_get
+        self.lib.pr_set_riemann.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        self.lib.pr_set_riemann(self._h, 1 if riemann_fit else 0)
 
     def process(self, raw, names=None, internals=True):
         if self.lib.pr_process(self._h, raw, len(raw), 1 if internals else 0) != 0:

@@ -25,6 +25,7 @@ struct Handle {
   oracle::Event ev;
   std::map<std::string, Blob> out;
   double lastSeconds = 0;
+  bool useRiemannFit = false;
   std::string error;
 
   template <typename T>
@@ -140,11 +141,11 @@ void record(Handle& h) {
 }  // namespace
 
 namespace oracle {
-void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev) {
+void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev, bool useRiemannFit) {
   fedLoop(es, raw, n, ev.words);
   makeClusters(es, ev.words, ev.digis, ev.clusters);
   makeHits(es, ev.digis, ev.clusters, ev.hits);
-  makeTuples(es, ev.hits, ev.ca);
+  makeTuples(es, ev.hits, ev.ca, useRiemannFit);
   makeVertices(ev.ca, ev.vtx);
 }
 }  // namespace oracle
@@ -167,12 +168,15 @@ void* or_create(const uint8_t* cabling, size_t ncab, const uint8_t* gain, size_t
 
 void or_destroy(void* p) { delete static_cast<Handle*>(p); }
 
+// useRiemannFit of the CA module configuration (off by default, as in the reference)
+void or_set_riemann(void* p, int on) { static_cast<Handle*>(p)->useRiemannFit = on != 0; }
+
 // Runs the chain on one raw.bin event record; 0 on success.
 int or_process(void* p, const uint8_t* raw, size_t n) {
   Handle& h = *static_cast<Handle*>(p);
   try {
     auto t0 = std::chrono::steady_clock::now();
-    oracle::processEvent(h.es, raw, n, h.ev);
+    oracle::processEvent(h.es, raw, n, h.ev, h.useRiemannFit);
     auto t1 = std::chrono::steady_clock::now();
     h.lastSeconds = std::chrono::duration<double>(t1 - t0).count();
     record(h);
@@ -214,7 +218,7 @@ double or_time_events(void* p, const uint8_t* const* raws, const size_t* sizes, 
         if (k >= n) break;
         auto a = std::chrono::steady_clock::now();
         try {
-          oracle::processEvent(h.es, raws[k], sizes[k], ev);
+          oracle::processEvent(h.es, raws[k], sizes[k], ev, h.useRiemannFit);
         } catch (std::exception&) {
           failed++;
         }

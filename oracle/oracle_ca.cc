@@ -94,7 +94,7 @@ inline float dca0(const Circle& e) {
 
 }  // namespace
 
-void makeTuples(const ES& es, const Hits& hh, CA& ca) {
+void makeTuples(const ES& es, const Hits& hh, CA& ca, bool useRiemannFit) {
   const uint32_t nHits = hh.nHits;
   // ---- allocateOnGPU / launchZero (CAHitNtupletGeneratorKernelsAlloc.h:4-25) and tuples zero
   ca.nCells = 0;
@@ -374,7 +374,8 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca) {
 
   if (0 == nHits) return;
 
-  // ---- broken-line fits (BrokenLineFitOnGPU.cc:3-68): N=3, 4, and 5 fitted as 4
+  // ---- broken-line fits (BrokenLineFitOnGPU.cc:3-68), or with useRiemannFit
+  // the Riemann fits (RiemannFitOnGPU.cc:3-110): N=3, 4, and 5 fitted as 4
   const double B = double(float(0.0114256972711507));
   auto fitBin = [&](uint32_t nHitsBin, int N) {
     uint32_t sz = ca.tmOff[nHitsBin + 1] - ca.tmOff[nHitsBin];
@@ -400,8 +401,12 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca) {
         hits[3 * i + 1] = hh.yg[hit];
         hits[3 * i + 2] = hh.zg[hit];
       }
-      brokenLineFit(N, hits, ge, B, &ca.state[size_t(tkid) * 5], &ca.cov[size_t(tkid) * 15], &ca.pt[tkid],
-                    &ca.eta[tkid], &ca.chi2[tkid]);
+      if (useRiemannFit)
+        riemannFit(N, hits, ge, B, &ca.state[size_t(tkid) * 5], &ca.cov[size_t(tkid) * 15], &ca.pt[tkid],
+                   &ca.eta[tkid], &ca.chi2[tkid]);
+      else
+        brokenLineFit(N, hits, ge, B, &ca.state[size_t(tkid) * 5], &ca.cov[size_t(tkid) * 15], &ca.pt[tkid],
+                      &ca.eta[tkid], &ca.chi2[tkid]);
     }
   };
   fitBin(3, 3);

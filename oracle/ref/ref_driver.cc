@@ -94,6 +94,10 @@ struct RefChain {
   std::unique_ptr<pixelgpudetails::SiPixelRawToClusterGPUKernel::WordFedAppender> appender;
   std::map<std::string, Blob> out;
   double lastSeconds = 0;
+  // the fit choice of a configuration with useRiemannFit=true; the
+  // reference's own configuration fixes it to false
+  // (CAHitNtupletGeneratorOnGPU.cc:49)
+  bool useRiemannFit = false;
 
   template <typename T>
   void put(const std::string& name, const T* p, size_t n) {
@@ -259,7 +263,7 @@ int pr_process(void* p, const uint8_t* raw, size_t nraw, int dump) {
   if (0 != hits.nHits()) {
     HelixFitOnGPU fitter(bfield, h.caGen->m_params.fit5as4_);
     fitter.allocateOnGPU(&(soa->hitIndices), kernels.tupleMultiplicity(), soa);
-    if (h.caGen->m_params.useRiemannFit_)
+    if (h.caGen->m_params.useRiemannFit_ || h.useRiemannFit)
       fitter.launchRiemannKernelsOnCPU(hits.view(), hits.nHits(), CAConstants::maxNumberOfQuadruplets());
     else
       fitter.launchBrokenLineKernelsOnCPU(hits.view(), hits.nHits(), CAConstants::maxNumberOfQuadruplets());
@@ -450,6 +454,8 @@ int pr_names(void* p, char* buf, size_t n) {
 // Seconds spent in the chain (excluding input parsing and product recording)
 // during the last pr_process call.
 double pr_last_seconds(void* p) { return static_cast<RefChain*>(p)->lastSeconds; }
+
+void pr_set_riemann(void* p, int on) { static_cast<RefChain*>(p)->useRiemannFit = on != 0; }
 
 // Event-level parallel timing, the reference's own concurrency model (one
 // chain instance per stream, README.md:222-226): `threads` host threads, each

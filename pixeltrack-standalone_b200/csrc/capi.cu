@@ -226,7 +226,7 @@ int captureGraph(pg_ctx* c, Slot& s, uint32_t n, cudaGraphExec_t* out) {
   KernelProbe* pr = c->probeName.empty() ? nullptr : s.probe;
   if (pr) pr->used = 0;
   tProbe = pr;
-  cudaError_t le = runChain(c->des, s.ws, n, s.stream);
+  cudaError_t le = runChain(c->des, s.ws, n, s.stream, c->cfg.riemann_fit != 0);
   if (le == cudaSuccess) {
     launchPack(s.ws, n, s.dRes, s.stream);
     le = cudaGetLastError();
@@ -280,7 +280,7 @@ int pixgpu::launchBatch(pg_ctx* c, Slot& s) {
     KernelProbe* pr = c->probeName.empty() ? nullptr : s.probe;
     if (pr) pr->used = 0;
     tProbe = pr;
-    e = runChain(c->des, s.ws, s.nEvents, s.stream);
+    e = runChain(c->des, s.ws, s.nEvents, s.stream, c->cfg.riemann_fit != 0);
     if (e == cudaSuccess) launchPack(s.ws, s.nEvents, s.dRes, s.stream);
     tProbe = nullptr;
     s.lastProbeUsed = pr ? pr->used : 0;
@@ -308,6 +308,7 @@ void pg_default_config(pg_config* cfg) {
   cfg->use_graphs = 1;
   cfg->pool_words = 0;
   cfg->hbm_fraction = 0.5;
+  cfg->riemann_fit = 0;
 }
 
 namespace {

@@ -17,6 +17,7 @@ namespace pixgpu {
 namespace {
 
 #include "fit_linalg.cuh"
+#include "k_fit_riemann.cuh"
 
 __device__ __forceinline__ double multScatt(double length, double B, double R, double slope) {
   double pt2 = fmin(20., B * R);
@@ -367,7 +368,7 @@ __global__ void kFitZero(Workspace ws) {
 }
 
 // one thread per (tuple of the multiplicity bin nh); fits the first N hits
-template <int N>
+template <int N, bool kRiemann = false>
 __device__ __forceinline__ void blFitBin(const DeviceES& es, const Workspace& ws, uint32_t nh) {
   uint32_t e = blockIdx.y;
   const uint32_t* tm = ws.tmOff + size_t(e) * 16;
@@ -401,7 +402,10 @@ __device__ __forceinline__ void blFitBin(const DeviceES& es, const Workspace& ws
       H[3 * i + 2] = ws.zg[hb + hit];
     }
     FitOut o;
-    blFit<N>(H, ge, B, o);
+    if constexpr (kRiemann)
+      rfFit<N, double>(H, ge, B, o);
+    else
+      blFit<N>(H, ge, B, o);
 #pragma unroll
     for (int j = 0; j < 5; ++j) ws.state[tb * 5 + size_t(tkid) * 5 + j] = o.state[j];
 #pragma unroll
@@ -419,6 +423,15 @@ __global__ void __launch_bounds__(128) kBLFit(DeviceES es, Workspace ws) {
     blFitBin<3>(es, ws, 3);
   else
     blFitBin<4>(es, ws, 3 + blockIdx.z);
+}
+
+// the same bins through the Riemann fit (useRiemannFit,
+// CAHitNtupletGeneratorOnGPU.cc:116-120; RiemannFitOnGPU.cc:3-110)
+__global__ void __launch_bounds__(128) kRiemannFit(DeviceES es, Workspace ws) {
+  if (blockIdx.z == 0)
+    blFitBin<3, true>(es, ws, 3);
+  else
+    blFitBin<4, true>(es, ws, 3 + blockIdx.z);
 }
 
 // standalone fit of externally supplied tuples (fit workload and tests)
@@ -445,17 +458,19 @@ __global__ void kBLFitDirect(uint32_t n, const double* hits, const float* hge, d
 }
 
 #include "k_fit_mixed.cuh"
-#include "k_fit_riemann.cuh"
 
 }  // namespace
 
-cudaError_t runFits(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
+cudaError_t runFits(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream, bool riemann) {
   const uint32_t gx = nEvents >= 32 ? 8 : (nEvents >= 8 ? 32 : 148);
   dim3 g(gx, nEvents);
   PG_PROBED("kFitZero", stream, kFitZero<<<g, 256, 0, stream>>>(ws));
   // FP64-bound: enough warps per SM to cover the double-precision latency
   const uint32_t fx = nEvents >= 32 ? 16 : (nEvents >= 8 ? 64 : 296);
-  PG_PROBED("kBLFit", stream, kBLFit<<<dim3(fx, nEvents, 3), 128, 0, stream>>>(es, ws));
+  if (riemann)
+    PG_PROBED("kRiemannFit", stream, kRiemannFit<<<dim3(fx, nEvents, 3), 128, 0, stream>>>(es, ws));
+  else
+    PG_PROBED("kBLFit", stream, kBLFit<<<dim3(fx, nEvents, 3), 128, 0, stream>>>(es, ws));
   return cudaGetLastError();
 }
 

@@ -223,11 +223,12 @@ void workspaceCarve(Workspace& ws, void* base, uint32_t maxEvents, uint32_t word
 
 // Runs the whole chain on events [0, nEvents) of ws, on `stream`.  The
 // word/fedId/offset inputs must already be in ws.  Returns a CUDA error code.
-cudaError_t runChain(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream);
+// riemann: the Riemann fit in place of the broken-line fit (useRiemannFit)
+cudaError_t runChain(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream, bool riemann = false);
 // Individual stages (used by runChain and by the stage-level tests)
 cudaError_t runLocal(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream);
 cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream);
-cudaError_t runFits(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream);
+cudaError_t runFits(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream, bool riemann = false);
 cudaError_t runVertices(Workspace& ws, uint32_t nEvents, cudaStream_t stream);
 cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream);
 

@@ -111,3 +111,52 @@ def test_mixed_riemann_fit_within_bounds_of_fp64(chain, nhits, N):
     assert d[:, 1].max() < md0, d[:, 1].max()
     assert np.sqrt((d[:, 3] ** 2).mean()) < rcot
     assert np.sqrt((d[:, 4] ** 2).mean()) < rz0
+
+
+def _d0_cancellation(p):
+    """Per track, var(R) / var(d0): the transverse impact parameter of the
+    Riemann fit is |centre| - R (FitUtils.h:198-214), so its variance is the
+    difference of terms of the size of var(R); for a stiff track (R of
+    10^3-10^5 cm) FP64 keeps only eps * var(R) / var(d0) of it."""
+    nt = p["nTuples"]
+    st = p["state"].reshape(-1, 5)[:nt].astype(np.float64)
+    cov = p["cov"].reshape(-1, 15)[:nt].astype(np.float64)
+    with np.errstate(all="ignore"):
+        pt = 1.0 / np.abs(st[:, 2])
+        k = cov[:, 9] * pt ** 4 / 0.0114256972711507 ** 2 / np.abs(cov[:, 5])
+    return np.nan_to_num(k, nan=0.0, posinf=1e300)
+
+
+@pytest.mark.parametrize("seed,pu", [(211, 20), (212, 50)])
+def test_riemann_chain_matches_oracle(default_detector, seed, pu):
+    """The whole chain configured with useRiemannFit (pg_config.riemann_fit)
+    against the oracle chain configured the same way: integer products
+    exact, floating-point ones within 1e-5 relative.  A track's covariance
+    and chi2 may also differ by 8 eps times its d0 cancellation factor
+    (_d0_cancellation): on these events every difference beyond 1e-5 sits in
+    a stiff triplet with a factor above 1e10 and stays below 3 eps times it,
+    the last bits of FP64 terms that cancel, where the device and host
+    transcendental functions round differently."""
+    import oracle
+    import pixgpu
+    raw = default_detector.event(seed, pu)
+    want = oracle.Oracle(default_detector.es, riemann_fit=True).process(raw)
+    c = pixgpu.Chain(default_detector.es, max_events=1, max_words_per_batch=300000, riemann_fit=True)
+    try:
+        c.process([raw])
+        got = c.products(0)
+    finally:
+        c.close()
+    names = [n for n in oracle.PRODUCTS if n not in ("chi2", "cov")]
+    diffs = oracle.compare(want, got, names=names, rtol=RTOL)
+    assert diffs == [], "\n".join("%s: %s" % d for d in diffs)
+    nt = want["nTuples"]
+    tol = RTOL + 8 * 2.220446e-16 * _d0_cancellation(want)
+    for name, width in (("cov", 15), ("chi2", 1)):
+        a = want[name].reshape(-1, width)[:nt].astype(np.float64)
+        b = got[name].reshape(-1, width)[:nt].astype(np.float64)
+        both_nan = np.isnan(a) & np.isnan(b)
+        bad = (np.abs(a - b) > tol[:, None] * np.maximum(np.abs(a), np.abs(b))) & ~both_nan
+        if name == "chi2":
+            bad &= np.abs(a - b) > 2e-7
+        assert not bad.any(), (name, np.nonzero(bad.any(axis=1))[0][:10].tolist())

@@ -55,3 +55,22 @@ def test_riemann_and_broken_line_agree_on_the_helix(orc):
     d = r["state"].astype(np.float64) - b["state"]
     sig = np.sqrt(r["cov"][:, [0, 5, 9, 12, 14]].astype(np.float64))
     assert np.median(np.abs(d) / sig, axis=0).max() < 0.5
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="checker build of the reference not present")
+@pytest.mark.parametrize("seed,pu", [(201, 20), (202, 50)])
+def test_riemann_chain_oracle_equals_reference(default_detector, seed, pu):
+    """The whole chain with useRiemannFit: tracks and vertices of the oracle
+    equal the reference's own serial chain configured the same way."""
+    import tempfile
+    d = tempfile.mkdtemp()
+    default_detector.write(d)
+    orc = oracle.Oracle(default_detector.es, riemann_fit=True)
+    ref = oracle.Reference(d, riemann_fit=True)
+    raw = default_detector.event(seed, pu)
+    want = ref.process(raw)
+    got = orc.process(raw)
+    assert oracle.compare(want, got, rtol=0.0) == []
+    # the fit choice reached both chains: the broken-line tracks differ
+    bl = oracle.Oracle(default_detector.es).process(raw)
+    assert not np.array_equal(bl["state"], got["state"])

@@ -19,6 +19,8 @@
 // DFS numbers tuples by prefix sums over starting cells, and the one
 // order-dependent cleaner (fastDuplicateRemover) runs as rounds over the
 // dependency graph of cells that share a track.
+#include <cooperative_groups.h>
+
 #include "device_utils.cuh"
 #include "segsort.cuh"
 #include "pixgpu_internal.cuh"
@@ -944,15 +946,23 @@ __global__ void kFastDupInDegree(Workspace ws, uint32_t* indeg, const uint32_t* 
   }
 }
 
-// One block per event.  A worklist holds the candidates whose earlier
-// track-sharing candidates are all done; cells of one round share no track,
-// so they are processed in parallel, and each releases its later neighbours
-// (the in-degree reaching zero queues them for the next round).
+// One thread-block cluster of P CTAs per event (kFastDupCtas for small
+// batches, 1 for large ones).  A worklist
+// holds the candidates whose earlier track-sharing candidates are all done;
+// cells of one round share no track, so the cluster's threads process them in
+// parallel, and each releases its later neighbours (the in-degree reaching
+// zero queues them for the next round).  The rounds are separated by cluster
+// barriers; the two worklist counters live in the shared memory of rank 0.
 constexpr int kFastDupThreads = 1024;
-__global__ void __launch_bounds__(kFastDupThreads) kFastDupRounds(Workspace ws, uint32_t* indeg, uint32_t* lists,
-                                                                   const uint32_t* candFlag, const uint32_t* candOff) {
+constexpr uint32_t kFastDupCtas = 8;
+__global__ void __launch_bounds__(kFastDupThreads)
+    kFastDupRounds(Workspace ws, uint32_t* indeg, uint32_t* lists, const uint32_t* candFlag, const uint32_t* candOff) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const uint32_t r = cl.block_rank(), P = cl.num_blocks();
   __shared__ uint32_t sN[2];
-  const uint32_t e = blockIdx.x;
+  uint32_t* N = cl.map_shared_rank(sN, 0);
+  const uint32_t e = blockIdx.y;
   const uint32_t nc = ws.ev[e].nCandidates;
   const uint32_t* cand = ws.candidates + size_t(e) * kCellCap;
   const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
@@ -965,18 +975,23 @@ __global__ void __launch_bounds__(kFastDupThreads) kFastDupRounds(Workspace ws, 
   uint32_t* L[2] = {lists + size_t(e) * kEdgeCap, lists + size_t(e) * kEdgeCap + kCellCap};
   uint8_t* q = ws.quality + size_t(e) * kTupleBins;
   const float* tip = ws.state + size_t(e) * kTupleBins * 5 + 1;
-  if (threadIdx.x < 2) sN[threadIdx.x] = 0;
-  __syncthreads();
-  for (uint32_t k = threadIdx.x; k < nc; k += blockDim.x)
-    if (deg[k] == 0) L[0][atomicAdd(&sN[0], 1u)] = k;
-  __syncthreads();
+  const uint32_t gtid = r * blockDim.x + threadIdx.x, gstride = P * blockDim.x;
+  if (r == 0 && threadIdx.x < 2) sN[threadIdx.x] = 0;
+  cl.sync();
+  for (uint32_t k = gtid; k < nc; k += gstride)
+    if (deg[k] == 0) L[0][atomicAdd(&N[0], 1u)] = k;
+  cl.sync();
   int cur = 0;
   for (;;) {
-    const uint32_t n = sN[cur];
+    const uint32_t n = N[cur];
+    // every CTA has read the count: it may be reset, and rank 0's shared
+    // memory is not read after the last round
+    cl.sync();
     if (n == 0) break;
+    if (r == 0 && threadIdx.x == 0) N[cur] = 0;
     const uint32_t* Lc = L[cur];
     uint32_t* Ln = L[cur ^ 1];
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    for (uint32_t i = gtid; i < n; i += gstride) {
       const uint32_t cell = cand[Lc[i]];
       const uint32_t b = off[cell], s = trkListSize(off, cell);
       float mc = 10000.f;
@@ -1001,15 +1016,14 @@ __global__ void __launch_bounds__(kFastDupThreads) kFastDupRounds(Workspace ws, 
           const uint32_t o = tcell[4 * t + qq];
           if (o > cell && flag[o] && inTrkList(off, trk, o, t)) {
             const uint32_t ko = cidx[o];
-            if (atomicSub(&deg[ko], 1u) == 1u) Ln[atomicAdd(&sN[cur ^ 1], 1u)] = ko;
+            if (atomicSub(&deg[ko], 1u) == 1u) Ln[atomicAdd(&N[cur ^ 1], 1u)] = ko;
           }
         }
       }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) sN[cur] = 0;
     cur ^= 1;
-    __syncthreads();
+    // the round's quality writes and the next worklist are complete
+    cl.sync();
   }
 }
 
@@ -1102,20 +1116,18 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   PG_PROBED("kDoubletSetup", stream, kDoubletSetup<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents));
   PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.ohCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
   PG_PROBED("kDoubletCount", stream, kDoubletCount<<<dim3(gx * 4, nEvents), 256, 0, stream>>>(ws));
-  segScan(ws.jCount, ws.jOffset, kJCap + 1, EVF(ntot), kJCap, nullptr, 0, ws.scanTmp, nEvents, stream);
+  segScan(ws.jCount, ws.jOffset, kJCap + 1, EVF(ntot), kJCap, nullptr, 0, nEvents, stream);
   PG_PROBED("kDoubletWrite", stream, kDoubletWrite<<<dim3(gx * 4, nEvents), 256, 0, stream>>>(ws));
   PG_PROBED("kCellsTotal", stream, kCellsTotal<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents));
   // ---- isOuterHitOfCell: scan of the per-hit counts, unordered fill, order per hit
-  segScan(ws.ohCount, ws.ohOff, kHitCap + 1, EVF(nHits), kHitCap, nullptr, 0, ws.scanTmp, nEvents, stream);
-  PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.ohCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
+  segScan(ws.ohCount, ws.ohOff, kHitCap + 1, EVF(nHits), kHitCap, nullptr, 0, nEvents, stream, true);
   PG_PROBED("kOuterHitFill", stream, kOuterHitFill<<<g, 256, 0, stream>>>(ws));
   sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.ohCells, kCellCap, ws.ohOff, kHitCap + 1, EVF(nHits), 0, false, kCellCap, 0);
   PG_PROBED("kOhRec", stream, kOhRec<<<g, 256, 0, stream>>>(ws));
   // ---- CA links: edges appended unordered, then CSR by inner cell, ordered ascending
   PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbrCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
   PG_PROBED("kConnect", stream, kConnect<<<dim3(gx * 4, nEvents), 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
-  segScan(ws.nbrCount, ws.nbrOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanTmp, nEvents, stream);
-  PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbrCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
+  segScan(ws.nbrCount, ws.nbrOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, nEvents, stream, true);
   PG_PROBED("kEdgeScatter", stream, kEdgeScatter<<<g, 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
   sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.nbr, kEdgeCap, ws.nbrOff, kCellCap + 1, EVF(nCells), 0, false, kEdgeCap, 1);
   PG_PROBED("kNbrPool", stream, kNbrPool<<<g, 256, 0, stream>>>(ws));
@@ -1123,23 +1135,20 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   PG_PROBED("kFishbone", stream, kFishbone<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws));
   // ---- n-tuplets: DFS count, scans, DFS write, finalize
   PG_PROBED("kNtupletCount", stream, kNtupletCount<<<dim3(gx * 8, nEvents), 128, 0, stream>>>(ws));
-  segScan(ws.startTupleCount, ws.startTupleOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcM), ws.scanTmp, nEvents,
-          stream);
-  segScan(ws.startHitCount, ws.startHitOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcN), ws.scanTmp, nEvents,
-          stream);
+  segScan(ws.startTupleCount, ws.startTupleOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcM), nEvents, stream);
+  segScan(ws.startHitCount, ws.startHitOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcN), nEvents, stream);
   PG_PROBED("kNtupletWrite", stream, kNtupletWrite<<<dim3(gx * 8, nEvents), 128, 0, stream>>>(ws));
   PG_PROBED("kTupleFinalize", stream, kTupleFinalize<<<dim3(32, nEvents), 1024, 0, stream>>>(ws));
   // ---- cell -> track lists
   PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trkCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
   PG_PROBED("kTrackCount", stream, kTrackCount<<<g, 256, 0, stream>>>(ws));
-  segScan(ws.trkCount, ws.trkOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanTmp, nEvents, stream);
-  PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trkCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
+  segScan(ws.trkCount, ws.trkOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, nEvents, stream, true);
   PG_PROBED("kTrackFill", stream, kTrackFill<<<g, 256, 0, stream>>>(ws));
   sortSegments<uint16_t>(ws, nEvents, stream, gx * 2, ws.trk, kTupleCellCap, ws.trkOff, kCellCap + 1, EVF(nCells), 0, false, kTupleCellCap, 2);
   uint32_t* candFlag = ws.startTupleCount;  // scratch
   uint32_t* candOff = ws.startHitCount;
   PG_PROBED("kTrackPool", stream, kTrackPool<<<g, 256, 0, stream>>>(ws, candFlag));
-  segScan(candFlag, candOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(nCandidates), ws.scanTmp, nEvents, stream);
+  segScan(candFlag, candOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(nCandidates), nEvents, stream);
   PG_PROBED("kCandidateScatter", stream, kCandidateScatter<<<g, 256, 0, stream>>>(ws, candFlag, candOff));
   PG_PROBED("kEarlyDup", stream, kEarlyDup<<<g, 256, 0, stream>>>(ws));
   PG_PROBED("kTupleDet", stream, kTupleDet<<<g, 256, 0, stream>>>(ws));
@@ -1158,12 +1167,16 @@ cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   uint32_t* indeg = ws.scratchA;        // [maxEvents][kEdgeCap] >= kCellCap
   uint32_t* lists = ws.scratchB;        // two worklists of kCellCap per event
   PG_PROBED("kFastDupInDegree", stream, kFastDupInDegree<<<g, 256, 0, stream>>>(ws, indeg, candFlag));
-  PG_PROBED("kFastDupRounds", stream, kFastDupRounds<<<nEvents, kFastDupThreads, 0, stream>>>(ws, indeg, lists, candFlag, candOff));
+  const uint32_t P = nEvents <= kClusterMaxEvents ? kFastDupCtas : 1;
+  cudaError_t le = cudaSuccess;
+  PG_PROBED("kFastDupRounds", stream,
+            le = launchClustered(kFastDupRounds, P, nEvents, kFastDupThreads, 0, stream, ws, indeg, lists, candFlag,
+                                 candOff));
+  if (le != cudaSuccess) return le;
   // hit -> tuple map and triplet cleaner
   PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
   PG_PROBED("kHitToTupleCount", stream, kHitToTupleCount<<<g, 256, 0, stream>>>(ws));
-  segScan(ws.h2tCount, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, nullptr, 0, ws.scanTmp, nEvents, stream);
-  PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
+  segScan(ws.h2tCount, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, nullptr, 0, nEvents, stream, true);
   PG_PROBED("kHitToTupleFill", stream, kHitToTupleFill<<<g, 256, 0, stream>>>(ws));
   sortSegments<uint16_t>(ws, nEvents, stream, gx * 2, ws.h2t, kH2TCap, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, true, kH2TCap, 3);
   PG_PROBED("kTripletCleaner", stream, kTripletCleaner<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws));

@@ -6,6 +6,8 @@
 // loose, in tuple order) with their fit state, covariance, hits and vertex
 // assignment, and the vertices.  The destination is mapped pinned host memory,
 // so the transfer is exact-sized and needs no host synchronisation.
+#include <cooperative_groups.h>
+
 #include "device_utils.cuh"
 #include "pixgpu_internal.cuh"
 #include "pixgpu_results.h"
@@ -38,71 +40,113 @@ __device__ __forceinline__ uint32_t packHalves(uint32_t w, uint32_t n, F&& get) 
   return lo | (hi << 16);
 }
 
-// One block per event.  The destination is host memory reached over the
-// bus, so every array is written as consecutive 32-bit words by consecutive
-// threads (whole lines per warp); the gathers come from device memory.
+// One thread-block cluster of P CTAs per event (P = 1 for large batches, where
+// the bus, not the SMs, bounds the copy).  Each CTA compacts
+// the loose tuples of one slice of the tuple range; the slices' counts give
+// the offsets (read across the cluster from distributed shared memory), and
+// every CTA gathers the whole list into its own shared memory.  Each CTA then
+// writes one slice of every output array.  The destination is host memory
+// reached over the bus: every array is written as consecutive 32-bit words
+// by consecutive threads (whole lines per warp), from all the cluster's SMs
+// at once; the gathers come from device memory.
+constexpr uint32_t kPackCtas = 8;  // CTAs per event in a small batch
+
 __global__ void __launch_bounds__(512) kPackResults(Workspace ws, uint8_t* out) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const uint32_t r = cl.block_rank(), P = cl.num_blocks();
   __shared__ uint32_t scanSh[33];
+  __shared__ uint16_t sLocal[kResultTracks];
   __shared__ uint16_t sIdx[kResultTracks];
-  __shared__ uint32_t sGuard;
-  const uint32_t e = blockIdx.x;
+  __shared__ uint32_t sCount;
+  __shared__ uint32_t sOff[kPackCtas + 1];  // P <= kPackCtas
+  const uint32_t e = blockIdx.y;
   const EventCounters* c = ws.ev + e;
   uint8_t* base = out + size_t(e) * kResultStride;
   const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
   const uint16_t* th = ws.tupleHits + size_t(e) * kTupleHitCap;
   const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
   const size_t tb = size_t(e) * kTupleBins;
-  if (threadIdx.x == 0) {
-    uint32_t g = c->nTuples;
-    if (c->apcM >= kTupleBins) g = kTupleBins - 1;
-    sGuard = g;
-  }
-  __syncthreads();
-  const uint32_t guard = sGuard;
+  const uint32_t guard = c->apcM >= kTupleBins ? kTupleBins - 1 : c->nTuples;
+  // ---- this CTA's slice of the tuples: loose ones in tuple order
+  const uint32_t chunk = (guard + P - 1) / P;
+  const uint32_t lo = min(guard, r * chunk), hi = min(guard, lo + chunk);
   uint32_t carry = 0;
-  for (uint32_t t0 = 0; t0 < guard; t0 += blockDim.x) {
+  for (uint32_t t0 = lo; t0 < hi; t0 += blockDim.x) {
     const uint32_t t = t0 + threadIdx.x;
-    const uint32_t loose = (t < guard && q[t] >= 2) ? 1u : 0u;
+    const uint32_t loose = (t < hi && q[t] >= 2) ? 1u : 0u;
     uint32_t tot;
     const uint32_t p = carry + blockExclusiveScan(loose, scanSh, &tot);
-    if (loose && p < kResultTracks) sIdx[p] = uint16_t(t);
+    if (loose && p < kResultTracks) sLocal[p] = uint16_t(t);
     carry += tot;
   }
+  if (threadIdx.x == 0) sCount = carry;
+  cl.sync();
+  if (threadIdx.x == 0) {
+    uint32_t o = 0;
+    for (uint32_t k = 0; k < P; ++k) {
+      sOff[k] = o;
+      o += *cl.map_shared_rank(&sCount, k);
+    }
+    sOff[P] = o;
+  }
   __syncthreads();
-  const uint32_t n = min(carry, kResultTracks);
+  const uint32_t nLoose = sOff[P];
+  const uint32_t n = min(nLoose, kResultTracks);
+  // ---- the whole list, gathered from the cluster's shared memories
+  for (uint32_t k = 0; k < P; ++k) {
+    const uint16_t* src = cl.map_shared_rank(sLocal, k);
+    const uint32_t o = sOff[k], m = min(sOff[k + 1], n) > o ? min(sOff[k + 1], n) - o : 0u;
+    for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) sIdx[o + j] = src[j];
+  }
+  // no CTA may leave (and release its shared memory) before all have read
+  cl.sync();
+  // ---- this CTA's slice of every output array
+  auto sl = [&](uint32_t len, uint32_t& a, uint32_t& b) {
+    a = uint32_t(uint64_t(len) * r / P);
+    b = uint32_t(uint64_t(len) * (r + 1) / P);
+  };
   const uint32_t T = blockDim.x;
+  uint32_t a, b;
   uint32_t* w32 = reinterpret_cast<uint32_t*>(base + kResOffTupleIndex);
-  for (uint32_t j = threadIdx.x; j < n; j += T) w32[j] = sIdx[j];
+  sl(n, a, b);
+  for (uint32_t j = a + threadIdx.x; j < b; j += T) w32[j] = sIdx[j];
   w32 = reinterpret_cast<uint32_t*>(base + kResOffNHits);
-  for (uint32_t w = threadIdx.x; w < (n + 3) / 4; w += T)
+  sl((n + 3) / 4, a, b);
+  for (uint32_t w = a + threadIdx.x; w < b; w += T)
     w32[w] = packBytes(w, n, [&](uint32_t i) { return toff[sIdx[i] + 1] - toff[sIdx[i]]; });
   w32 = reinterpret_cast<uint32_t*>(base + kResOffQuality);
-  for (uint32_t w = threadIdx.x; w < (n + 3) / 4; w += T)
-    w32[w] = packBytes(w, n, [&](uint32_t i) { return q[sIdx[i]]; });
+  for (uint32_t w = a + threadIdx.x; w < b; w += T) w32[w] = packBytes(w, n, [&](uint32_t i) { return q[sIdx[i]]; });
   float* f = reinterpret_cast<float*>(base + kResOffState);
-  for (uint32_t j = threadIdx.x; j < 5 * n; j += T) f[j] = ws.state[tb * 5 + size_t(sIdx[j / 5]) * 5 + j % 5];
+  sl(5 * n, a, b);
+  for (uint32_t j = a + threadIdx.x; j < b; j += T) f[j] = ws.state[tb * 5 + size_t(sIdx[j / 5]) * 5 + j % 5];
   f = reinterpret_cast<float*>(base + kResOffCov);
-  for (uint32_t j = threadIdx.x; j < 15 * n; j += T) f[j] = ws.cov[tb * 15 + size_t(sIdx[j / 15]) * 15 + j % 15];
+  sl(15 * n, a, b);
+  for (uint32_t j = a + threadIdx.x; j < b; j += T) f[j] = ws.cov[tb * 15 + size_t(sIdx[j / 15]) * 15 + j % 15];
+  sl(n, a, b);
   f = reinterpret_cast<float*>(base + kResOffPt);
-  for (uint32_t j = threadIdx.x; j < n; j += T) f[j] = ws.pt[tb + sIdx[j]];
+  for (uint32_t j = a + threadIdx.x; j < b; j += T) f[j] = ws.pt[tb + sIdx[j]];
   f = reinterpret_cast<float*>(base + kResOffEta);
-  for (uint32_t j = threadIdx.x; j < n; j += T) f[j] = ws.eta[tb + sIdx[j]];
+  for (uint32_t j = a + threadIdx.x; j < b; j += T) f[j] = ws.eta[tb + sIdx[j]];
   f = reinterpret_cast<float*>(base + kResOffChi2);
-  for (uint32_t j = threadIdx.x; j < n; j += T) f[j] = ws.chi2[tb + sIdx[j]];
+  for (uint32_t j = a + threadIdx.x; j < b; j += T) f[j] = ws.chi2[tb + sIdx[j]];
   w32 = reinterpret_cast<uint32_t*>(base + kResOffHits);
-  for (uint32_t w = threadIdx.x; w < (5 * n + 1) / 2; w += T)
+  sl((5 * n + 1) / 2, a, b);
+  for (uint32_t w = a + threadIdx.x; w < b; w += T)
     w32[w] = packHalves(w, 5 * n, [&](uint32_t i) {
       const uint32_t t = sIdx[i / 5], k = i % 5;
       return k < toff[t + 1] - toff[t] ? uint32_t(th[toff[t] + k]) : 0xffffu;
     });
   const bool hasVtx = c->nVertices > 0;
   w32 = reinterpret_cast<uint32_t*>(base + kResOffVertex);
-  for (uint32_t w = threadIdx.x; w < (n + 1) / 2; w += T)
+  sl((n + 1) / 2, a, b);
+  for (uint32_t w = a + threadIdx.x; w < b; w += T)
     w32[w] = packHalves(w, n, [&](uint32_t i) { return hasVtx ? uint32_t(uint16_t(ws.idv[tb + sIdx[i]])) : 0xffffu; });
   const uint32_t nv = min(c->nVertices, uint32_t(kMaxVtx));
   const size_t vb = size_t(e) * kMaxVtx;
   ResultVertices vtx = resultVertices(base);
-  for (uint32_t v = threadIdx.x; v < nv; v += T) {
+  sl(nv, a, b);
+  for (uint32_t v = a + threadIdx.x; v < b; v += T) {
     vtx.zv[v] = ws.zv[vb + v];
     vtx.wv[v] = ws.wv[vb + v];
     vtx.chi2[v] = ws.vchi2[vb + v];
@@ -110,18 +154,19 @@ __global__ void __launch_bounds__(512) kPackResults(Workspace ws, uint8_t* out) 
     vtx.ndof[v] = ws.ndof[vb + v];
   }
   w32 = reinterpret_cast<uint32_t*>(base + kResOffSortInd);
-  for (uint32_t w = threadIdx.x; w < (nv + 1) / 2; w += T)
+  sl((nv + 1) / 2, a, b);
+  for (uint32_t w = a + threadIdx.x; w < b; w += T)
     w32[w] = packHalves(w, nv, [&](uint32_t i) { return uint32_t(ws.sortInd[vb + i]); });
-  if (threadIdx.x == 0) {
+  if (r == 0 && threadIdx.x == 0) {
     ResultHeader h{};
     h.nTracks = n;
-    h.nLooseAll = carry;
+    h.nLooseAll = nLoose;
     h.nVertices = nv;
     h.nHits = c->nHits;
     h.nTuples = guard;
     h.nDigis = c->nWords;
     h.nCells = c->nCells;
-    h.flags = c->flags | (carry > kResultTracks ? kFlagResultOverflow : 0u);
+    h.flags = c->flags | (nLoose > kResultTracks ? kFlagResultOverflow : 0u);
     h.nEdges = c->nEdges;
     h.nTupleHits = toff[guard];
     h.nModules = c->nModules;
@@ -136,7 +181,10 @@ void launchSetInput(Workspace& ws, const uint32_t* words, const uint8_t* fedIds,
 }
 
 void launchPack(Workspace& ws, uint32_t nEvents, uint8_t* out, cudaStream_t s) {
-  PG_PROBED("kPackResults", s, kPackResults<<<nEvents, 512, 0, s>>>(ws, out));
+  const uint32_t P = nEvents <= kClusterMaxEvents ? kPackCtas : 1;
+  cudaError_t le = cudaSuccess;
+  PG_PROBED("kPackResults", s, le = launchClustered(kPackResults, P, nEvents, 512, 0, s, ws, out));
+  (void)le;  // a failed launch is reported by the stream's next error check
 }
 
 }  // namespace pixgpu

@@ -13,6 +13,8 @@
 // by a prefix over the parent vertex index.
 #include <atomic>
 
+#include <cooperative_groups.h>
+
 #include "device_utils.cuh"
 #include "pixgpu_internal.cuh"
 
@@ -27,6 +29,7 @@ constexpr int kVtxThreads = 1024;
 constexpr uint32_t kSmemTracks = 4096;
 constexpr size_t kTrackBytes = 8 * 4 + 2 * 2 + 2;
 constexpr size_t kVtxSmemBytes = kSmemTracks * kTrackBytes;
+constexpr uint32_t kVtxCtas = 4;  // CTAs per event in a small batch
 
 struct VtxScratch {
   float *zt, *ezt2, *ptt2, *zz;
@@ -176,13 +179,21 @@ __device__ void fitVertices(const VtxScratch& s, uint32_t nt, uint32_t nv, float
   __syncthreads();
 }
 
+// Launched as a cluster of P CTAs per event (P = 1 for large batches).  With
+// P > 1 and the per-track arrays in shared memory, every CTA builds the track
+// arrays and the z histogram, the two neighbour searches are divided among the
+// CTAs by track, each result written into every CTA's shared memory, and rank
+// 0 alone continues from there.
 __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const uint32_t rank = cl.block_rank(), P = cl.num_blocks();
   extern __shared__ __align__(16) char vsm[];
   __shared__ uint32_t scanSh[33];
   __shared__ uint32_t hoff[257], hcur[257];
   __shared__ uint32_t vOff[kMaxVtx + 1], vCur[kMaxVtx + 1];
   __shared__ uint32_t sNt, sFound, sGuard, sNv;
-  const uint32_t e = blockIdx.x;
+  const uint32_t e = blockIdx.y;
   const uint32_t lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   EventCounters* c = ws.ev + e;
   const uint32_t nTuples = c->nTuples;
@@ -218,16 +229,20 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
   const uint32_t t0 = min(guard, threadIdx.x * chunk), t1 = min(guard, t0 + chunk);
   uint32_t mine = 0;
   for (uint32_t t = t0; t < t1; ++t) {
-    idv[t] = -1;
+    if (rank == 0) idv[t] = -1;
     mine += selected(t) ? 1u : 0u;
   }
   uint32_t total;
   const uint32_t first = blockExclusiveScan(mine, scanSh, &total);
   if (threadIdx.x == 0) sNt = min(total, kMaxVtxTracks);
   __syncthreads();
-  // the count decides where the per-track arrays live
+  // the count decides where the per-track arrays live; the neighbour
+  // searches are split among the cluster's CTAs when they are in shared memory
   const VtxScratch s = sNt <= kSmemTracks ? carve(vsm, kSmemTracks) : scratchOf(ws, e);
-  {
+  const bool split = P > 1 && sNt <= kSmemTracks;
+  const bool active = split || rank == 0;
+  const uint32_t wFirst = split ? rank * nw : 0, wStride = split ? P * nw : nw;
+  if (active) {
     uint32_t it = first;
     for (uint32_t t = t0; t < t1 && it < kMaxVtxTracks; ++t) {
       if (!selected(t)) continue;
@@ -243,6 +258,7 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
   const float eps = 0.07f, errmax = 0.01f, chi2max = 9.f;
   const float er2mx = errmax * errmax;
 
+  if (active) {
   // ---- clusterTracksByDensity: z histogram (256 bins of 1 mm)
   for (uint32_t b = threadIdx.x; b < 257; b += blockDim.x) {
     hoff[b] = 0;
@@ -286,9 +302,9 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
   __syncthreads();
   // neighbour counts: one warp per track, the lanes take 32 consecutive
   // entries of the track's three bins at a time
-  for (uint32_t i = threadIdx.x >> 5; i < nt; i += nw) {
+  for (uint32_t i = wFirst + (threadIdx.x >> 5); i < nt; i += wStride) {
     if (s.ezt2[i] > er2mx) {
-      if (lane == 0) s.nn[i] = 0;
+      if (split ? lane < P : lane == 0) *(split ? cl.map_shared_rank(s.nn, lane) + i : s.nn + i) = 0;
       continue;
     }
     const int b0 = max(0, int(s.izt[i]) - 1), b1 = min(255, int(s.izt[i]) + 1);
@@ -301,9 +317,12 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
       cnt += (i != j && !(dist > eps) && !(dist * dist > chi2max * (ei + s.ezt2[j]))) ? 1u : 0u;
     }
     cnt = __reduce_add_sync(0xffffffffu, cnt);
-    if (lane == 0) s.nn[i] = int32_t(cnt);
+    if (split ? lane < P : lane == 0) *(split ? cl.map_shared_rank(s.nn, lane) + i : s.nn + i) = int32_t(cnt);
   }
-  __syncthreads();
+  }
+  // every CTA holds every neighbour count
+  cl.sync();
+  if (active) {
   // Closest denser neighbour.  The serial loop (mdist starts at eps; a
   // candidate is taken when denser, not farther than mdist and
   // chi2-compatible) ends on the last candidate of minimal distance among the
@@ -311,7 +330,7 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
   // then on every denser, chi2-compatible candidate is taken, so the result
   // is the last of those.  The warp evaluates both, the first as the minimum
   // of (distance, reversed position).
-  for (uint32_t i = threadIdx.x >> 5; i < nt; i += nw) {
+  for (uint32_t i = wFirst + (threadIdx.x >> 5); i < nt; i += wStride) {
     const int b0 = max(0, int(s.izt[i]) - 1), b1 = min(255, int(s.izt[i]) + 1);
     const uint32_t pb = hoff[b0], pe = hoff[b1 + 1];
     const float zi = s.zt[i], ei = s.ezt2[i];
@@ -343,16 +362,18 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
       const unsigned long long other = __shfl_xor_sync(0xffffffffu, bestKey, o);
       bestKey = other < bestKey ? other : bestKey;
     }
-    if (lane == 0) {
-      int32_t best = int32_t(i);
-      if (anyNaN)
-        best = int32_t(s.hbins[lastOk]);
-      else if (bestKey != ~0ull)
-        best = int32_t(s.hbins[0xffffffffu - uint32_t(bestKey & 0xffffffffu)]);
-      s.iv[i] = best;
-    }
+    int32_t best = int32_t(i);
+    if (anyNaN)
+      best = int32_t(s.hbins[lastOk]);
+    else if (bestKey != ~0ull)
+      best = int32_t(s.hbins[0xffffffffu - uint32_t(bestKey & 0xffffffffu)]);
+    if (split ? lane < P : lane == 0) *(split ? cl.map_shared_rank(s.iv, lane) + i : s.iv + i) = best;
   }
-  __syncthreads();
+  }
+  // every CTA holds every closest denser neighbour; only rank 0 goes on,
+  // and no CTA reads another CTA's shared memory after this point
+  cl.sync();
+  if (rank != 0) return;
   // percolate to the seed
   for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
     int32_t m = s.iv[i];
@@ -553,7 +574,13 @@ cudaError_t runVertices(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
     if (e != cudaSuccess) return e;
     configured.fetch_or(bit);
   }
-  PG_PROBED("kVertices", stream, kVertices<<<nEvents, kVtxThreads, kVtxSmemBytes, stream>>>(ws));
+  // small batches: a cluster of kVtxCtas CTAs per event shortens the event's
+  // latency; large batches: one CTA per event keeps the SMs for other events
+  const uint32_t P = nEvents <= kClusterMaxEvents ? kVtxCtas : 1;
+  cudaError_t le = cudaSuccess;
+  PG_PROBED("kVertices", stream,
+            le = launchClustered(kVertices, P, nEvents, kVtxThreads, kVtxSmemBytes, stream, ws));
+  if (le != cudaSuccess) return le;
   return cudaGetLastError();
 }
 

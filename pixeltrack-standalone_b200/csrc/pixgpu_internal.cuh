@@ -175,14 +175,9 @@ struct Workspace {
   // scratch: CA link lists before ordering, cleaner state
   uint32_t* scratchA;        // [maxEvents][kEdgeCap]
   uint32_t* scratchB;        // [maxEvents][kEdgeCap]
-  // scan scratch
-  uint32_t* scanTmp;         // [maxEvents][kScanTmpStride]
   uint32_t* bigSeg;          // [maxEvents][kBigSegCap] long segments awaiting the block sort
   uint32_t* segList;         // [maxEvents][kCellCap] segments with >= 2 entries (the ones to order)
 };
-
-constexpr uint32_t kScanChunk = 4096;
-constexpr uint32_t kScanTmpStride = 1024;
 
 // A CSR fill notes segment s when it places s's second entry: only those
 // segments need ordering.  `list` selects the counter of the list ordering
@@ -221,6 +216,32 @@ void probeEnd(cudaStream_t s);
 size_t workspaceBytes(uint32_t maxEvents, uint32_t wordCap);
 void workspaceCarve(Workspace& ws, void* base, uint32_t maxEvents, uint32_t wordCap);
 
+// Batches up to this many events run the per-event cooperative kernels
+// (result packing, duplicate rounds, vertexing) as clusters of several CTAs
+// per event, for latency; larger batches give each event one CTA, which
+// leaves the other SMs to the concurrently running batch.
+constexpr uint32_t kClusterMaxEvents = 16;
+
+// Launch of kernel k on a grid of (x, nEvents) CTAs grouped in clusters of x
+// CTAs along the first dimension.
+template <typename... KArgs, typename... Args>
+cudaError_t launchClustered(void (*k)(KArgs...), uint32_t x, uint32_t nEvents, uint32_t threads, size_t smem,
+                            cudaStream_t stream, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(x, nEvents);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = x;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, KArgs(args)...);
+}
+
 // Runs the whole chain on events [0, nEvents) of ws, on `stream`.  The
 // word/fedId/offset inputs must already be in ws.  Returns a CUDA error code.
 // riemann: the Riemann fit in place of the broken-line fit (useRiemannFit)
@@ -239,9 +260,10 @@ void launchPack(Workspace& ws, uint32_t nEvents, uint8_t* out, cudaStream_t s);
 // batched segmented exclusive scan: out[e*stride + i] = sum_{k<i} in[e*stride + k]
 // for i <= n_e, where n_e = lenPtr[e*lenStride] (device) or maxLen when lenPtr is
 // null; n_e <= maxLen.  The total lands at out[e*stride + n_e] and, if totalPtr,
-// at totalPtr[e*totalStride].  in may equal out.
-void segScan(const uint32_t* in, uint32_t* out, uint32_t stride, const uint32_t* lenPtr, uint32_t lenStride,
-             uint32_t maxLen, uint32_t* totalPtr, uint32_t totalStride, uint32_t* tmp, uint32_t nEvents,
-             cudaStream_t stream);
+// at totalPtr[e*totalStride].  in may equal out unless zeroIn, which leaves
+// in[0..n_e) zero (the count arrays are reused as fill cursors).
+void segScan(uint32_t* in, uint32_t* out, uint32_t stride, const uint32_t* lenPtr, uint32_t lenStride,
+             uint32_t maxLen, uint32_t* totalPtr, uint32_t totalStride, uint32_t nEvents, cudaStream_t stream,
+             bool zeroIn = false);
 
 }  // namespace pixgpu

@@ -112,6 +112,7 @@ void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W) {
   c.take(ws.idv, T);
   c.take(ws.scratchA, size_t(E) * kEdgeCap);
   c.take(ws.scratchB, size_t(E) * kEdgeCap);
+  c.take(ws.scanSums, size_t(E) * kScanMaxSlices);
   c.take(ws.bigSeg, size_t(E) * kBigSegCap);
   c.take(ws.segList, size_t(E) * kCellCap);
 }

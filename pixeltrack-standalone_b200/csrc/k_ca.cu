@@ -1116,18 +1116,18 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   PG_PROBED("kDoubletSetup", stream, kDoubletSetup<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents));
   PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.ohCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
   PG_PROBED("kDoubletCount", stream, kDoubletCount<<<dim3(gx * 4, nEvents), 256, 0, stream>>>(ws));
-  segScan(ws.jCount, ws.jOffset, kJCap + 1, EVF(ntot), kJCap, nullptr, 0, nEvents, stream);
+  segScan(ws.jCount, ws.jOffset, kJCap + 1, EVF(ntot), kJCap, nullptr, 0, ws.scanSums, nEvents, stream);
   PG_PROBED("kDoubletWrite", stream, kDoubletWrite<<<dim3(gx * 4, nEvents), 256, 0, stream>>>(ws));
   PG_PROBED("kCellsTotal", stream, kCellsTotal<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents));
   // ---- isOuterHitOfCell: scan of the per-hit counts, unordered fill, order per hit
-  segScan(ws.ohCount, ws.ohOff, kHitCap + 1, EVF(nHits), kHitCap, nullptr, 0, nEvents, stream, true);
+  segScan(ws.ohCount, ws.ohOff, kHitCap + 1, EVF(nHits), kHitCap, nullptr, 0, ws.scanSums, nEvents, stream, true);
   PG_PROBED("kOuterHitFill", stream, kOuterHitFill<<<g, 256, 0, stream>>>(ws));
   sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.ohCells, kCellCap, ws.ohOff, kHitCap + 1, EVF(nHits), 0, false, kCellCap, 0);
   PG_PROBED("kOhRec", stream, kOhRec<<<g, 256, 0, stream>>>(ws));
   // ---- CA links: edges appended unordered, then CSR by inner cell, ordered ascending
   PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbrCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
   PG_PROBED("kConnect", stream, kConnect<<<dim3(gx * 4, nEvents), 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
-  segScan(ws.nbrCount, ws.nbrOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, nEvents, stream, true);
+  segScan(ws.nbrCount, ws.nbrOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanSums, nEvents, stream, true);
   PG_PROBED("kEdgeScatter", stream, kEdgeScatter<<<g, 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
   sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.nbr, kEdgeCap, ws.nbrOff, kCellCap + 1, EVF(nCells), 0, false, kEdgeCap, 1);
   PG_PROBED("kNbrPool", stream, kNbrPool<<<g, 256, 0, stream>>>(ws));
@@ -1135,20 +1135,20 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   PG_PROBED("kFishbone", stream, kFishbone<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws));
   // ---- n-tuplets: DFS count, scans, DFS write, finalize
   PG_PROBED("kNtupletCount", stream, kNtupletCount<<<dim3(gx * 8, nEvents), 128, 0, stream>>>(ws));
-  segScan(ws.startTupleCount, ws.startTupleOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcM), nEvents, stream);
-  segScan(ws.startHitCount, ws.startHitOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcN), nEvents, stream);
+  segScan(ws.startTupleCount, ws.startTupleOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcM), ws.scanSums, nEvents, stream);
+  segScan(ws.startHitCount, ws.startHitOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcN), ws.scanSums, nEvents, stream);
   PG_PROBED("kNtupletWrite", stream, kNtupletWrite<<<dim3(gx * 8, nEvents), 128, 0, stream>>>(ws));
   PG_PROBED("kTupleFinalize", stream, kTupleFinalize<<<dim3(32, nEvents), 1024, 0, stream>>>(ws));
   // ---- cell -> track lists
   PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trkCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
   PG_PROBED("kTrackCount", stream, kTrackCount<<<g, 256, 0, stream>>>(ws));
-  segScan(ws.trkCount, ws.trkOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, nEvents, stream, true);
+  segScan(ws.trkCount, ws.trkOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanSums, nEvents, stream, true);
   PG_PROBED("kTrackFill", stream, kTrackFill<<<g, 256, 0, stream>>>(ws));
   sortSegments<uint16_t>(ws, nEvents, stream, gx * 2, ws.trk, kTupleCellCap, ws.trkOff, kCellCap + 1, EVF(nCells), 0, false, kTupleCellCap, 2);
   uint32_t* candFlag = ws.startTupleCount;  // scratch
   uint32_t* candOff = ws.startHitCount;
   PG_PROBED("kTrackPool", stream, kTrackPool<<<g, 256, 0, stream>>>(ws, candFlag));
-  segScan(candFlag, candOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(nCandidates), nEvents, stream);
+  segScan(candFlag, candOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(nCandidates), ws.scanSums, nEvents, stream);
   PG_PROBED("kCandidateScatter", stream, kCandidateScatter<<<g, 256, 0, stream>>>(ws, candFlag, candOff));
   PG_PROBED("kEarlyDup", stream, kEarlyDup<<<g, 256, 0, stream>>>(ws));
   PG_PROBED("kTupleDet", stream, kTupleDet<<<g, 256, 0, stream>>>(ws));
@@ -1176,7 +1176,7 @@ cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   // hit -> tuple map and triplet cleaner
   PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
   PG_PROBED("kHitToTupleCount", stream, kHitToTupleCount<<<g, 256, 0, stream>>>(ws));
-  segScan(ws.h2tCount, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, nullptr, 0, nEvents, stream, true);
+  segScan(ws.h2tCount, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, nullptr, 0, ws.scanSums, nEvents, stream, true);
   PG_PROBED("kHitToTupleFill", stream, kHitToTupleFill<<<g, 256, 0, stream>>>(ws));
   sortSegments<uint16_t>(ws, nEvents, stream, gx * 2, ws.h2t, kH2TCap, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, true, kH2TCap, 3);
   PG_PROBED("kTripletCleaner", stream, kTripletCleaner<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws));

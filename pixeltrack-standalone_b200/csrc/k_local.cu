@@ -1119,7 +1119,7 @@ cudaError_t runLocal(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaSt
   PG_PROBED("kZeroU32", stream, kZeroU32<<<dim3(2, nEvents), 1024, 0, stream>>>(cursor, kPhiStride, kPhiStride, nEvents));
   PG_PROBED("kPhiCount", stream, kPhiCount<<<dim3(16, nEvents), 256, 0, stream>>>(ws));
   // in place exclusive scan of the 1280 counters; the total lands in the extra bin
-  segScan(ws.phiOff, ws.phiOff, kPhiStride, nullptr, 0, kPhiTot - 1, nullptr, 0, nEvents, stream);
+  segScan(ws.phiOff, ws.phiOff, kPhiStride, nullptr, 0, kPhiTot - 1, nullptr, 0, ws.scanSums, nEvents, stream);
   PG_PROBED("kPhiFill", stream, kPhiFill<<<dim3(16, nEvents), 256, 0, stream>>>(ws, cursor));
   PG_PROBED("kPhiSort", stream, kPhiSort<<<dim3((kPhiTot - 1 + 7) / 8, nEvents), 256, 0, stream>>>(ws));
   PG_PROBED("kPhiRec", stream, kPhiRec<<<dim3(16, nEvents), 256, 0, stream>>>(ws));

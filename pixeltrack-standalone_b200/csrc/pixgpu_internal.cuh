@@ -99,6 +99,8 @@ struct BatchInput {
   const uint8_t* fedIds;
 };
 
+constexpr uint32_t kScanMaxSlices = 64;  // slices of one event's array in the segmented scan
+
 struct Workspace {
   uint32_t maxEvents;
   uint32_t wordCap;          // words over the whole batch
@@ -175,6 +177,7 @@ struct Workspace {
   // scratch: CA link lists before ordering, cleaner state
   uint32_t* scratchA;        // [maxEvents][kEdgeCap]
   uint32_t* scratchB;        // [maxEvents][kEdgeCap]
+  uint32_t* scanSums;        // [maxEvents][kScanMaxSlices] slice totals of the segmented scans
   uint32_t* bigSeg;          // [maxEvents][kBigSegCap] long segments awaiting the block sort
   uint32_t* segList;         // [maxEvents][kCellCap] segments with >= 2 entries (the ones to order)
 };
@@ -262,8 +265,9 @@ void launchPack(Workspace& ws, uint32_t nEvents, uint8_t* out, cudaStream_t s);
 // null; n_e <= maxLen.  The total lands at out[e*stride + n_e] and, if totalPtr,
 // at totalPtr[e*totalStride].  in may equal out unless zeroIn, which leaves
 // in[0..n_e) zero (the count arrays are reused as fill cursors).
+// sums: [nEvents][kScanMaxSlices] scratch for the slice totals.
 void segScan(uint32_t* in, uint32_t* out, uint32_t stride, const uint32_t* lenPtr, uint32_t lenStride,
-             uint32_t maxLen, uint32_t* totalPtr, uint32_t totalStride, uint32_t nEvents, cudaStream_t stream,
-             bool zeroIn = false);
+             uint32_t maxLen, uint32_t* totalPtr, uint32_t totalStride, uint32_t* sums, uint32_t nEvents,
+             cudaStream_t stream, bool zeroIn = false);
 
 }  // namespace pixgpu

@@ -240,6 +240,13 @@ __device__ __forceinline__ void forSeedSlots(const PairTable& pt, const HitsView
   }
 }
 
+constexpr uint32_t kNoTemp = 0xffffffffu;  // the slot's doublets did not fit its warp's staging region
+
+// Pass 1: count each slot's doublets and stage their outer hits, in serial
+// order, in the staging region of the warp that found them (scratchA as
+// 16-bit entries, an equal share per warp: no atomics); the slot's staging
+// offset goes to scratchB.  A slot whose window could overflow the region is
+// only counted, and pass 2 tests its candidates again.
 __global__ void kDoubletCount(Workspace ws) {
   __shared__ PairTable pt;
   const uint32_t e = blockIdx.y;
@@ -249,16 +256,33 @@ __global__ void kDoubletCount(Workspace ws) {
   const HitsView hh = hitsOf(ws, e);
   const uint4* rec = ws.phiRec + size_t(e) * kHitCap;
   uint32_t* cnt = ws.jCount + size_t(e) * (kJCap + 1);
+  uint16_t* stage = reinterpret_cast<uint16_t*>(ws.scratchA + size_t(e) * kEdgeCap);
+  uint32_t* slotStage = ws.scratchB + size_t(e) * kEdgeCap;
+  const uint32_t wpb = blockDim.x >> 5;
+  const uint32_t S = gridDim.x * wpb, w = blockIdx.x * wpb + (threadIdx.x >> 5);
+  const uint32_t R = 2 * kEdgeCap / S;  // staging entries per warp
+  uint32_t used = 0;                     // warp-uniform
   forSeedSlots(pt, hh, ntot, [&](uint32_t j, bool live, const DoubletSeed& d, uint32_t phase) {
     if (phase == 0) {
       if (j < ntot && !live) cnt[j] = 0;
       return;
     }
-    const uint32_t n = warpDoublets(d, rec, [](uint32_t, uint16_t) {});
-    if (laneId() == phase - 1) cnt[j] = n;
+    const uint32_t window = (d.e0 - d.b0) + (d.e1 - d.b1);
+    const uint32_t at = used + window <= R ? w * R + used : kNoTemp;
+    const uint32_t n = warpDoublets(d, rec, [&](uint32_t k, uint16_t oi) {
+      if (at != kNoTemp) stage[at + k] = oi;
+    });
+    if (at != kNoTemp) used += n;
+    if (laneId() == phase - 1) {
+      cnt[j] = n;
+      slotStage[j] = at;
+    }
   });
 }
 
+// Pass 2: each slot's doublets from its staging entries to their serial
+// positions (the scan of the counts); slots that were not staged are found
+// again.  Lanes take 32 slots, the warp serves the non-empty ones in turn.
 __global__ void kDoubletWrite(Workspace ws) {
   __shared__ PairTable pt;
   const uint32_t e = blockIdx.y;
@@ -270,25 +294,50 @@ __global__ void kDoubletWrite(Workspace ws) {
   const uint32_t* off = ws.jOffset + size_t(e) * (kJCap + 1);
   const size_t cb = size_t(e) * kCellCap;
   uint32_t* ohc = ws.ohCount + size_t(e) * (kHitCap + 1);
-  forSeedSlots(pt, hh, ntot, [&](uint32_t j, bool live, const DoubletSeed& d, uint32_t phase) {
-    if (phase == 0) return;
-    const uint32_t base = off[j];
-    if (base >= kCellCap || off[j + 1] == base) return;
-    const float zi = hh.zg[d.i], ri = hh.rg[d.i];
-    warpDoublets(d, rec, [&](uint32_t k, uint16_t oi) {
-      const uint32_t idx = base + k;
-      if (idx < kCellCap) {
-        ws.cellInner[cb + idx] = uint16_t(d.i);
+  const uint16_t* stage = reinterpret_cast<const uint16_t*>(ws.scratchA + size_t(e) * kEdgeCap);
+  const uint32_t* slotStage = ws.scratchB + size_t(e) * kEdgeCap;
+  const uint32_t lane = laneId(), wpb = blockDim.x >> 5;
+  const uint32_t S = gridDim.x * wpb, w = blockIdx.x * wpb + (threadIdx.x >> 5);
+  for (uint32_t r0 = 0; w + r0 * S < ntot; r0 += 32) {
+    const uint32_t jl = w + (r0 + lane) * S;
+    uint32_t myBase = 0, myN = 0;
+    if (jl < ntot) {
+      myBase = off[jl];
+      myN = myBase < kCellCap ? min(off[jl + 1], kCellCap) - myBase : 0u;
+    }
+    uint32_t live = __ballot_sync(0xffffffffu, myN > 0);
+    while (live) {
+      const int l = __ffs(live) - 1;
+      live &= live - 1;
+      const uint32_t j = w + (r0 + uint32_t(l)) * S;
+      const uint32_t base = __shfl_sync(0xffffffffu, myBase, l), n = __shfl_sync(0xffffffffu, myN, l);
+      uint32_t pair = 0;
+      while (j >= pt.pairCum[pair]) ++pair;
+      const uint32_t i = (0 == pair ? j : j - pt.pairCum[pair - 1]) + pt.layerStart[cLayerPairs[2 * pair]];
+      const float zi = hh.zg[i], ri = hh.rg[i];
+      auto put = [&](uint32_t k, uint16_t oi) {
+        const uint32_t idx = base + k;
+        ws.cellInner[cb + idx] = uint16_t(i);
         ws.cellOuter[cb + idx] = oi;
-        ws.cellPair[cb + idx] = uint8_t(d.pair);
+        ws.cellPair[cb + idx] = uint8_t(pair);
         ws.cellDoubletId[cb + idx] = int32_t(idx);
         ws.cellUsed[cb + idx] = 0;
         ws.cellInnerZ[cb + idx] = zi;
         ws.cellInnerR[cb + idx] = ri;
         atomicAdd(&ohc[oi], 1u);
+      };
+      const uint32_t at = slotStage[j];
+      if (at != kNoTemp) {
+        for (uint32_t k = lane; k < n; k += 32) put(k, stage[at + k]);
+      } else {
+        DoubletSeed d;
+        doubletSeed(pt, hh, j, d);
+        warpDoublets(d, rec, [&](uint32_t k, uint16_t oi) {
+          if (k < n) put(k, oi);
+        });
       }
-    });
-  });
+    }
+  }
 }
 
 __global__ void kCellsTotal(Workspace ws, uint32_t nEvents) {

@@ -5,8 +5,13 @@ chain.  Events are generated once, uploaded into the device pool, and the
 chain is launched `--repeat` times over batches of `--batch` events.
 
   python pixeltrack-standalone_b200/run_events.py --events 64 --batch 64 --pu 50 --repeat 3
+
+--probe adds, after the timed loop, the median wall latency of one batch
+(submit to results on the host) and the device time of every kernel of a
+batch, timed with events captured around each launch (pg_set_probe).
 """
 import argparse
+import collections
 import concurrent.futures as cf
 import os
 import sys
@@ -25,6 +30,7 @@ def main():
     p.add_argument("--slots", type=int, default=1)
     p.add_argument("--seed", type=int, default=pixgpu.BASE_SEED + 1000)
     p.add_argument("--no-graphs", action="store_true")
+    p.add_argument("--probe", action="store_true", help="per-kernel device times of a batch")
     a = p.parse_args()
     det = pixgpu.Detector()
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
@@ -46,6 +52,29 @@ def main():
             chain.release(s)
     dt = time.perf_counter() - t0
     print("processed %d events (PU %g, batches of %d) in %.3f s: %.1f events/s" % (done, a.pu, a.batch, dt, done / dt))
+    if a.probe:
+        lat = []
+        for b in batches * 3:
+            t1 = time.perf_counter()
+            s = chain.submit_pooled(b, keep=True)
+            chain.wait(s)
+            lat.append(time.perf_counter() - t1)
+            chain.release(s)
+        lat.sort()
+        census, launches = collections.defaultdict(float), collections.Counter()
+        chain.set_probe("*")
+        for b in batches:
+            s = chain.submit_pooled(b, keep=True)
+            chain.wait(s)
+            for name, ms in chain.probe_read(s):
+                census[name] += ms / len(batches)
+                launches[name] += 1
+            chain.release(s)
+        chain.set_probe(None)
+        print("batch wall latency: median %.3f ms; kernel launches per batch %d, device time %.3f ms" %
+              (1e3 * lat[len(lat) // 2], sum(launches.values()) // len(batches), sum(census.values())))
+        for name, ms in sorted(census.items(), key=lambda x: -x[1]):
+            print("  %-22s %8.1f us  x%d" % (name, 1e3 * ms, launches[name] // len(batches)))
     chain.close()
 
 

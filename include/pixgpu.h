@@ -74,6 +74,8 @@ typedef struct pg_config {
   double hbm_fraction;           /* share of free device memory the slots may take when slots == 0 */
   uint32_t riemann_fit;          /* 1: Riemann fits in place of broken-line fits (the useRiemannFit
                                     parameter of CAHitNtupletGeneratorOnGPU.cc:49, default off) */
+  uint32_t vertex_algo;          /* vertex clusterer of PixelVertexProducerCUDA.cc:26-35: 0 useDensity
+                                    (the default), 1 useDBSCAN, 2 useIterative */
 } pg_config;
 
 typedef struct pg_event_counts {

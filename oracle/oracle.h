@@ -119,8 +119,10 @@ void makeHits(const ES& es, const Digis& d, const Clusters& c, Hits& h);
 // useRiemannFit selects the Riemann fit in place of the broken-line fit
 // (CAHitNtupletGeneratorOnGPU.cc:116-120; the reference's default is off)
 void makeTuples(const ES& es, const Hits& h, CA& ca, bool useRiemannFit = false);
-// gpuVertexFinder::Producer::make (plugin-PixelVertexFinding/gpuVertexFinderImpl.h:84-111)
-void makeVertices(const CA& ca, Vertices& v);
+// gpuVertexFinder::Producer::make (plugin-PixelVertexFinding/gpuVertexFinderImpl.h:84-111);
+// algo: 0 clusterTracksByDensity (the PixelVertexProducerCUDA default),
+// 1 clusterTracksDBSCAN, 2 clusterTracksIterative
+void makeVertices(const CA& ca, Vertices& v, int algo = 0);
 
 // broken-line fit of one tuple of N (3 or 4) hits; results in the TrackSoA layout
 void brokenLineFit(int N, const double* hits /*3xN col-major*/, const float* hits_ge /*6xN*/, double B,
@@ -131,7 +133,8 @@ void riemannFit(int N, const double* hits /*3xN col-major*/, const float* hits_g
                 float* cov15, float* pt, float* eta, float* chi2);
 
 // whole chain for one raw.bin event record
-void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev, bool useRiemannFit = false);
+void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev, bool useRiemannFit = false,
+                  int vertexAlgo = 0);
 
 }  // namespace oracle
 

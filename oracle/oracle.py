@@ -54,7 +54,7 @@ class _Named:
 class Oracle(_Named):
     """Sequential restatement of the serial chain (oracle/*.cc)."""
 
-    def __init__(self, es_images, riemann_fit=False):
+    def __init__(self, es_images, riemann_fit=False, vertex_algo=0):
         path = os.path.join(HERE, "liboracle.so")
         if not os.path.exists(path):
             _build.build_oracle()
@@ -84,6 +84,9 @@ class Oracle(_Named):
             raise RuntimeError("oracle: malformed ES images")
         self._get = self.lib.or_get
         self.lib.or_set_riemann(self._h, 1 if riemann_fit else 0)
+        self.lib.or_set_vertex_algo.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        if self.lib.or_set_vertex_algo(self._h, int(vertex_algo)) != 0:
+            raise ValueError("vertex_algo: 0 density, 1 DBSCAN, 2 iterative")
 
     def process(self, raw, names=None):
         if self.lib.or_process(self._h, raw, len(raw)) != 0:
@@ -154,7 +157,7 @@ def ref_available():
 class Reference(_Named):
     """The reference's own serial chain, compiled from its sources (checker build)."""
 
-    def __init__(self, datadir, riemann_fit=False):
+    def __init__(self, datadir, riemann_fit=False, vertex_algo=0):
         self.lib = ctypes.CDLL(REF_LIB)
         self.lib.pr_create.restype = ctypes.c_void_p
         self.lib.pr_create.argtypes = [ctypes.c_char_p]
@@ -167,6 +170,9 @@ class Reference(_Named):
         self._get = self.lib.pr_get
         self.lib.pr_set_riemann.argtypes = [ctypes.c_void_p, ctypes.c_int]
         self.lib.pr_set_riemann(self._h, 1 if riemann_fit else 0)
+        self.lib.pr_set_vertex_algo.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        if self.lib.pr_set_vertex_algo(self._h, int(vertex_algo)) != 0:
+            raise ValueError("vertex_algo: 0 density, 1 DBSCAN, 2 iterative")
 
     def process(self, raw, names=None, internals=True):
         if self.lib.pr_process(self._h, raw, len(raw), 1 if internals else 0) != 0:

@@ -26,6 +26,7 @@ struct Handle {
   std::map<std::string, Blob> out;
   double lastSeconds = 0;
   bool useRiemannFit = false;
+  int vertexAlgo = 0;
   std::string error;
 
   template <typename T>
@@ -141,12 +142,12 @@ void record(Handle& h) {
 }  // namespace
 
 namespace oracle {
-void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev, bool useRiemannFit) {
+void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev, bool useRiemannFit, int vertexAlgo) {
   fedLoop(es, raw, n, ev.words);
   makeClusters(es, ev.words, ev.digis, ev.clusters);
   makeHits(es, ev.digis, ev.clusters, ev.hits);
   makeTuples(es, ev.hits, ev.ca, useRiemannFit);
-  makeVertices(ev.ca, ev.vtx);
+  makeVertices(ev.ca, ev.vtx, vertexAlgo);
 }
 }  // namespace oracle
 
@@ -171,12 +172,19 @@ void or_destroy(void* p) { delete static_cast<Handle*>(p); }
 // useRiemannFit of the CA module configuration (off by default, as in the reference)
 void or_set_riemann(void* p, int on) { static_cast<Handle*>(p)->useRiemannFit = on != 0; }
 
+// vertex clustering of PixelVertexProducerCUDA: 0 density (default), 1 DBSCAN, 2 iterative
+int or_set_vertex_algo(void* p, int algo) {
+  if (algo < 0 || algo > 2) return -1;
+  static_cast<Handle*>(p)->vertexAlgo = algo;
+  return 0;
+}
+
 // Runs the chain on one raw.bin event record; 0 on success.
 int or_process(void* p, const uint8_t* raw, size_t n) {
   Handle& h = *static_cast<Handle*>(p);
   try {
     auto t0 = std::chrono::steady_clock::now();
-    oracle::processEvent(h.es, raw, n, h.ev, h.useRiemannFit);
+    oracle::processEvent(h.es, raw, n, h.ev, h.useRiemannFit, h.vertexAlgo);
     auto t1 = std::chrono::steady_clock::now();
     h.lastSeconds = std::chrono::duration<double>(t1 - t0).count();
     record(h);
@@ -218,7 +226,7 @@ double or_time_events(void* p, const uint8_t* const* raws, const size_t* sizes, 
         if (k >= n) break;
         auto a = std::chrono::steady_clock::now();
         try {
-          oracle::processEvent(h.es, raws[k], sizes[k], ev, h.useRiemannFit);
+          oracle::processEvent(h.es, raws[k], sizes[k], ev, h.useRiemannFit, h.vertexAlgo);
         } catch (std::exception&) {
           failed++;
         }

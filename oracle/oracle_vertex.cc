@@ -1,6 +1,8 @@
 // Oracle (checker only): pixel vertexing, restating
 // plugin-PixelVertexFinding/gpuVertexFinderImpl.h:10-43 (loadTracks),
-// gpuClusterTracksByDensity.h:20-207, gpuFitVertices.h:15-98,
+// gpuClusterTracksByDensity.h:20-207 (or, configured,
+// gpuClusterTracksDBSCAN.h:16-227 / gpuClusterTracksIterative.h:16-201; the
+// choice of gpuVertexFinderImpl.h:96-102), gpuFitVertices.h:15-98,
 // gpuSplitVertices.h:15-125 and gpuSortByPt2.h:15-55 with the
 // PixelVertexProducerCUDA configuration (PixelVertexProducerCUDA.cc:16-26):
 // minT=2, eps=0.07, errmax=0.01, chi2max=9, ptMin=0.5.  See oracle.h.
@@ -13,7 +15,7 @@
 
 namespace oracle {
 
-void makeVertices(const CA& ca, Vertices& v) {
+void makeVertices(const CA& ca, Vertices& v, int algo) {
   constexpr uint32_t MAXTRACKS = 32 * 1024, MAXVTX = PF_MAX_VTX;
   const int minT = 2;
   const float eps = 0.07f, errmax = 0.01f, chi2max = 9.f, ptMin = 0.5f;
@@ -47,7 +49,7 @@ void makeVertices(const CA& ca, Vertices& v) {
   int32_t* nn = v.ndof.data();
   uint32_t nvIntermediate = 0;
 
-  // ---- clusterTracksByDensity
+  // ---- clustering: histogram common to the three algorithms
   {
     float er2mx = errmax * errmax;
     std::vector<uint8_t> izt(nt);
@@ -73,32 +75,97 @@ void makeVertices(const CA& ca, Vertices& v) {
       bs = std::max(0, bs - 1);
       for (uint32_t p = off[bs]; p < off[be + 1]; ++p) f(uint32_t(bins[p]));
     };
+    // neighbour counts (DBSCAN: no chi2 compatibility)
     for (uint32_t i = 0; i < nt; ++i) {
       if (ezt2[i] > er2mx) continue;
       forEach(i, [&](uint32_t j) {
         if (i == j) return;
         float dist = std::abs(zt[i] - zt[j]);
         if (dist > eps) return;
-        if (dist * dist > chi2max * (ezt2[i] + ezt2[j])) return;
+        if (algo != 1 && dist * dist > chi2max * (ezt2[i] + ezt2[j])) return;
         nn[i]++;
       });
     }
-    for (uint32_t i = 0; i < nt; ++i) {
-      float mdist = eps;
-      forEach(i, [&](uint32_t j) {
-        if (nn[j] < nn[i]) return;
-        if (nn[j] == nn[i] && zt[j] >= zt[i]) return;
-        float dist = std::abs(zt[i] - zt[j]);
-        if (dist > mdist) return;
-        if (dist * dist > chi2max * (ezt2[i] + ezt2[j])) return;
-        mdist = dist;
-        iv[i] = int32_t(j);
-      });
-    }
-    for (uint32_t i = 0; i < nt; ++i) {
-      int32_t m = iv[i];
-      while (m != iv[m]) m = iv[m];
-      iv[i] = m;
+    auto percolate = [&]() {
+      for (uint32_t i = 0; i < nt; ++i) {
+        int32_t m = iv[i];
+        while (m != iv[m]) m = iv[m];
+        iv[i] = m;
+      }
+    };
+    // DBSCAN/Iterative edge rule: a non-core track joins its closest
+    // chi2-compatible core neighbour
+    auto edges = [&]() {
+      for (uint32_t i = 0; i < nt; ++i) {
+        if (nn[i] >= minT) continue;
+        float mdist = eps;
+        forEach(i, [&](uint32_t j) {
+          if (nn[j] < minT) return;
+          float dist = std::abs(zt[i] - zt[j]);
+          if (dist > mdist) return;
+          if (dist * dist > chi2max * (ezt2[i] + ezt2[j])) return;
+          mdist = dist;
+          iv[i] = iv[j];
+        });
+      }
+    };
+    if (algo == 0) {  // gpuClusterTracksByDensity.h:20-207: closest denser neighbour
+      for (uint32_t i = 0; i < nt; ++i) {
+        float mdist = eps;
+        forEach(i, [&](uint32_t j) {
+          if (nn[j] < nn[i]) return;
+          if (nn[j] == nn[i] && zt[j] >= zt[i]) return;
+          float dist = std::abs(zt[i] - zt[j]);
+          if (dist > mdist) return;
+          if (dist * dist > chi2max * (ezt2[i] + ezt2[j])) return;
+          mdist = dist;
+          iv[i] = int32_t(j);
+        });
+      }
+      percolate();
+    } else if (algo == 1) {  // gpuClusterTracksDBSCAN.h:16-227: core links to the lowest-z core neighbour
+      for (uint32_t i = 0; i < nt; ++i) {
+        if (nn[i] < minT) continue;
+        float mz = zt[i];
+        forEach(i, [&](uint32_t j) {
+          if (zt[j] >= mz) return;
+          if (nn[j] < minT) return;
+          float dist = std::abs(zt[i] - zt[j]);
+          if (dist > eps) return;
+          mz = zt[j];
+          iv[i] = int32_t(j);
+        });
+      }
+      percolate();
+      edges();
+    } else {  // gpuClusterTracksIterative.h:16-201: min-label propagation over compatible cores
+      int nloops = 0;
+      bool more = true;
+      while (more) {
+        if (1 == nloops % 2) {
+          percolate();
+        } else {
+          more = false;
+          for (uint32_t k = 0; k < nt; ++k) {
+            const uint32_t i = bins[k];
+            const int be = std::min(int(izt[i]) + 1, 255);
+            if (nn[i] < minT) continue;
+            for (uint32_t p = k + 1; p < off[be + 1]; ++p) {
+              const uint32_t j = bins[p];
+              if (nn[j] < minT) continue;
+              float dist = std::abs(zt[i] - zt[j]);
+              if (dist > eps) continue;
+              if (dist * dist > chi2max * (ezt2[i] + ezt2[j])) continue;
+              const int32_t old = iv[j];  // the serial atomicMin
+              if (iv[i] < old) iv[j] = iv[i];
+              if (old != iv[i]) more = true;
+              if (old < iv[i]) iv[i] = old;
+            }
+          }
+        }
+        ++nloops;
+      }
+      edges();
     }
     uint32_t found = 0;
     for (uint32_t i = 0; i < nt; ++i) {

@@ -457,6 +457,16 @@ double pr_last_seconds(void* p) { return static_cast<RefChain*>(p)->lastSeconds;
 
 void pr_set_riemann(void* p, int on) { static_cast<RefChain*>(p)->useRiemannFit = on != 0; }
 
+// The vertex finder of a PixelVertexProducerCUDA configured with useDensity
+// (0, the reference's own configuration), useDBSCAN (1) or useIterative (2);
+// the other parameters as in PixelVertexProducerCUDA.cc:26-35.
+int pr_set_vertex_algo(void* p, int algo) {
+  if (algo < 0 || algo > 2) return -1;
+  static_cast<RefChain*>(p)->vtx =
+      std::make_unique<gpuVertexFinder::Producer>(true, algo == 0, algo == 1, algo == 2, 2, 0.07, 0.01, 9);
+  return 0;
+}
+
 // Event-level parallel timing, the reference's own concurrency model (one
 // chain instance per stream, README.md:222-226): `threads` host threads, each
 // with its own instance, take events from a shared counter.  Returns the wall

@@ -226,7 +226,7 @@ int captureGraph(pg_ctx* c, Slot& s, uint32_t n, cudaGraphExec_t* out) {
   KernelProbe* pr = c->probeName.empty() ? nullptr : s.probe;
   if (pr) pr->used = 0;
   tProbe = pr;
-  cudaError_t le = runChain(c->des, s.ws, n, s.stream, c->cfg.riemann_fit != 0);
+  cudaError_t le = runChain(c->des, s.ws, n, s.stream, c->cfg.riemann_fit != 0, int(c->cfg.vertex_algo));
   if (le == cudaSuccess) {
     launchPack(s.ws, n, s.dRes, s.stream);
     le = cudaGetLastError();
@@ -280,7 +280,7 @@ int pixgpu::launchBatch(pg_ctx* c, Slot& s) {
     KernelProbe* pr = c->probeName.empty() ? nullptr : s.probe;
     if (pr) pr->used = 0;
     tProbe = pr;
-    e = runChain(c->des, s.ws, s.nEvents, s.stream, c->cfg.riemann_fit != 0);
+    e = runChain(c->des, s.ws, s.nEvents, s.stream, c->cfg.riemann_fit != 0, int(c->cfg.vertex_algo));
     if (e == cudaSuccess) launchPack(s.ws, s.nEvents, s.dRes, s.stream);
     tProbe = nullptr;
     s.lastProbeUsed = pr ? pr->used : 0;
@@ -309,6 +309,7 @@ void pg_default_config(pg_config* cfg) {
   cfg->pool_words = 0;
   cfg->hbm_fraction = 0.5;
   cfg->riemann_fit = 0;
+  cfg->vertex_algo = 0;
 }
 
 namespace {
@@ -367,7 +368,8 @@ int pg_create(const pg_es_images* es, const pg_config* cfgIn, pg_ctx** out) {
     c->cfg = *cfgIn;
   else
     pg_default_config(&c->cfg);
-  if (c->cfg.max_events == 0 || c->cfg.max_words_per_batch == 0 || c->cfg.max_words_per_batch > (1u << 30))
+  if (c->cfg.max_events == 0 || c->cfg.max_words_per_batch == 0 || c->cfg.max_words_per_batch > (1u << 30) ||
+      c->cfg.vertex_algo > 2)
     return PG_ERR_ARG;
   c->device = c->cfg.device;
   cudaError_t e = cudaSetDevice(c->cfg.device);

@@ -156,13 +156,14 @@ void workspaceCarve(Workspace& ws, void* base, uint32_t maxEvents, uint32_t word
   layout(ws, c, maxEvents, wordCap);
 }
 
-cudaError_t runChain(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream, bool riemann) {
+cudaError_t runChain(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream, bool riemann,
+                     int vertexAlgo) {
   cudaError_t err;
   if ((err = runLocal(es, ws, nEvents, stream)) != cudaSuccess) return err;
   if ((err = runCA(es, ws, nEvents, stream)) != cudaSuccess) return err;
   if ((err = runFits(es, ws, nEvents, stream, riemann)) != cudaSuccess) return err;
   if ((err = runCleaners(ws, nEvents, stream)) != cudaSuccess) return err;
-  if ((err = runVertices(ws, nEvents, stream)) != cudaSuccess) return err;
+  if ((err = runVertices(ws, nEvents, stream, vertexAlgo)) != cudaSuccess) return err;
   return cudaSuccess;
 }
 

@@ -179,12 +179,169 @@ __device__ void fitVertices(const VtxScratch& s, uint32_t nt, uint32_t nv, float
   __syncthreads();
 }
 
+// order-preserving map of a float to unsigned (negative values reversed)
+__device__ __forceinline__ uint32_t orderedBits(float x) {
+  const uint32_t u = __float_as_uint(x);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// DBSCAN (gpuClusterTracksDBSCAN.h:16-227) and iterative
+// (gpuClusterTracksIterative.h:16-201) clustering after the neighbour counts:
+// iv[i] left pointing at track i's root (the numbering that follows is the
+// one of the density clusterer).  One block; warp per track for the
+// neighbour loops, whose serial order is reproduced by (key, position)
+// reductions; a track whose candidates include a NaN is done by lane 0
+// literally.
+__device__ void clusterCoresAndEdges(const VtxScratch& s, uint32_t nt, const uint32_t* hoff, int algo, float eps,
+                                     float chi2max, int32_t minT, int* sFlag) {
+  const uint32_t lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  auto range = [&](uint32_t i, uint32_t& pb, uint32_t& pe) {
+    const int b0 = max(0, int(s.izt[i]) - 1), b1 = min(255, int(s.izt[i]) + 1);
+    pb = hoff[b0];
+    pe = hoff[b1 + 1];
+  };
+  auto percolate = [&]() {
+    for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+      int32_t m = s.iv[i];
+      while (m != s.iv[m]) m = s.iv[m];
+      s.root[i] = m;
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) s.iv[i] = s.root[i];
+    __syncthreads();
+  };
+  if (algo == 1) {
+    // core tracks: the core neighbour of lowest z below the track's own
+    // (first in bin order among equal z)
+    for (uint32_t i = threadIdx.x >> 5; i < nt; i += nw) {
+      if (s.nn[i] < minT) continue;
+      uint32_t pb, pe;
+      range(i, pb, pe);
+      const float zi = s.zt[i];
+      unsigned long long best = ~0ull;
+      bool nan = isnan(zi);
+      for (uint32_t p = pb + lane; p < pe; p += 32) {
+        const uint32_t j = s.hbins[p];
+        const float zj = s.zt[j];
+        nan |= isnan(zj);
+        if (!(zj < zi) || s.nn[j] < minT || fabsf(zi - zj) > eps) continue;
+        const unsigned long long key = (uint64_t(orderedBits(zj)) << 32) | p;
+        best = key < best ? key : best;
+      }
+      if (__any_sync(0xffffffffu, nan)) {
+        if (lane == 0) {  // the serial loop as written
+          float mz = zi;
+          for (uint32_t p = pb; p < pe; ++p) {
+            const uint32_t j = s.hbins[p];
+            if (s.zt[j] >= mz || s.nn[j] < minT || fabsf(zi - s.zt[j]) > eps) continue;
+            mz = s.zt[j];
+            s.iv[i] = int32_t(j);
+          }
+        }
+        continue;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
+        best = other < best ? other : best;
+      }
+      if (lane == 0 && best != ~0ull) s.iv[i] = int32_t(s.hbins[uint32_t(best & 0xffffffffu)]);
+    }
+    __syncthreads();
+    percolate();
+  } else {
+    // connected components of the compatible core tracks: every label
+    // becomes the lowest track index of its component, the fixed point of the
+    // reference's alternating min-propagation and percolation
+    for (uint32_t it = 0; it <= nt + 1; ++it) {
+      if (threadIdx.x == 0) *sFlag = 0;
+      __syncthreads();
+      for (uint32_t i = threadIdx.x >> 5; i < nt; i += nw) {
+        if (s.nn[i] < minT) continue;
+        uint32_t pb, pe;
+        range(i, pb, pe);
+        const float zi = s.zt[i], ei = s.ezt2[i];
+        int32_t m = s.iv[i];
+        for (uint32_t p = pb + lane; p < pe; p += 32) {
+          const uint32_t j = s.hbins[p];
+          if (j == i || s.nn[j] < minT) continue;
+          const float dist = fabsf(zi - s.zt[j]);
+          if (dist > eps || dist * dist > chi2max * (ei + s.ezt2[j])) continue;
+          m = min(m, s.iv[j]);
+        }
+        m = __reduce_min_sync(0xffffffffu, m);
+        if (lane == 0 && m < s.iv[i]) {
+          atomicMin(&s.iv[i], m);
+          *sFlag = 1;
+        }
+      }
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+        const int32_t l = s.iv[i], ll = s.iv[l];
+        if (ll < l) {
+          atomicMin(&s.iv[i], ll);
+          *sFlag = 1;
+        }
+      }
+      __syncthreads();
+      const int more = *sFlag;
+      __syncthreads();
+      if (!more) break;
+    }
+  }
+  // edge rule: a non-core track joins its closest chi2-compatible core
+  // neighbour (last in bin order among equal distances)
+  for (uint32_t i = threadIdx.x >> 5; i < nt; i += nw) {
+    if (s.nn[i] >= minT) continue;
+    uint32_t pb, pe;
+    range(i, pb, pe);
+    const float zi = s.zt[i], ei = s.ezt2[i];
+    unsigned long long best = ~0ull;
+    bool nan = false;
+    for (uint32_t p = pb + lane; p < pe; p += 32) {
+      const uint32_t j = s.hbins[p];
+      if (s.nn[j] < minT) continue;
+      const float dist = fabsf(zi - s.zt[j]);
+      nan |= isnan(dist) || isnan(chi2max * (ei + s.ezt2[j]));
+      if (dist > eps || dist * dist > chi2max * (ei + s.ezt2[j])) continue;
+      const unsigned long long key = (uint64_t(__float_as_uint(dist)) << 32) | uint64_t(0xffffffffu - p);
+      best = key < best ? key : best;
+    }
+    if (__any_sync(0xffffffffu, nan)) {
+      if (lane == 0) {
+        s.root[i] = s.iv[i];
+        float mdist = eps;
+        for (uint32_t p = pb; p < pe; ++p) {
+          const uint32_t j = s.hbins[p];
+          if (s.nn[j] < minT) continue;
+          const float dist = fabsf(zi - s.zt[j]);
+          if (dist > mdist || dist * dist > chi2max * (ei + s.ezt2[j])) continue;
+          mdist = dist;
+          s.root[i] = s.iv[j];
+        }
+      }
+      continue;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
+      best = other < best ? other : best;
+    }
+    if (lane == 0) s.root[i] = best != ~0ull ? s.iv[s.hbins[0xffffffffu - uint32_t(best & 0xffffffffu)]] : s.iv[i];
+  }
+  __syncthreads();
+  // edge tracks take their core's root; the others keep theirs
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x)
+    if (s.nn[i] < minT) s.iv[i] = s.root[i];
+  __syncthreads();
+}
+
 // Launched as a cluster of P CTAs per event (P = 1 for large batches).  With
 // P > 1 and the per-track arrays in shared memory, every CTA builds the track
 // arrays and the z histogram, the two neighbour searches are divided among the
 // CTAs by track, each result written into every CTA's shared memory, and rank
 // 0 alone continues from there.
-__global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
+__global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   const uint32_t rank = cl.block_rank(), P = cl.num_blocks();
@@ -193,6 +350,7 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
   __shared__ uint32_t hoff[257], hcur[257];
   __shared__ uint32_t vOff[kMaxVtx + 1], vCur[kMaxVtx + 1];
   __shared__ uint32_t sNt, sFound, sGuard, sNv;
+  __shared__ int sFlag;
   const uint32_t e = blockIdx.y;
   const uint32_t lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   EventCounters* c = ws.ev + e;
@@ -239,7 +397,7 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
   // the count decides where the per-track arrays live; the neighbour
   // searches are split among the cluster's CTAs when they are in shared memory
   const VtxScratch s = sNt <= kSmemTracks ? carve(vsm, kSmemTracks) : scratchOf(ws, e);
-  const bool split = P > 1 && sNt <= kSmemTracks;
+  const bool split = P > 1 && sNt <= kSmemTracks && algo == 0;
   const bool active = split || rank == 0;
   const uint32_t wFirst = split ? rank * nw : 0, wStride = split ? P * nw : nw;
   if (active) {
@@ -314,7 +472,7 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
     for (uint32_t p = pb + lane; p < pe; p += 32) {
       const uint32_t j = s.hbins[p];
       const float dist = fabsf(zi - s.zt[j]);
-      cnt += (i != j && !(dist > eps) && !(dist * dist > chi2max * (ei + s.ezt2[j]))) ? 1u : 0u;
+      cnt += (i != j && !(dist > eps) && (algo == 1 || !(dist * dist > chi2max * (ei + s.ezt2[j])))) ? 1u : 0u;
     }
     cnt = __reduce_add_sync(0xffffffffu, cnt);
     if (split ? lane < P : lane == 0) *(split ? cl.map_shared_rank(s.nn, lane) + i : s.nn + i) = int32_t(cnt);
@@ -322,7 +480,8 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
   }
   // every CTA holds every neighbour count
   cl.sync();
-  if (active) {
+  if (active && algo != 0) clusterCoresAndEdges(s, nt, hoff, algo, eps, chi2max, 2, &sFlag);
+  if (active && algo == 0) {
   // Closest denser neighbour.  The serial loop (mdist starts at eps; a
   // candidate is taken when denser, not farther than mdist and
   // chi2-compatible) ends on the last candidate of minimal distance among the
@@ -563,7 +722,7 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws) {
 
 }  // namespace
 
-cudaError_t runVertices(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
+cudaError_t runVertices(Workspace& ws, uint32_t nEvents, cudaStream_t stream, int algo) {
   // opt in to the large shared-memory carve-out, once per device
   static std::atomic<uint64_t> configured{0};
   int dev = 0;
@@ -579,7 +738,7 @@ cudaError_t runVertices(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   const uint32_t P = nEvents <= kClusterMaxEvents ? kVtxCtas : 1;
   cudaError_t le = cudaSuccess;
   PG_PROBED("kVertices", stream,
-            le = launchClustered(kVertices, P, nEvents, kVtxThreads, kVtxSmemBytes, stream, ws));
+            le = launchClustered(kVertices, P, nEvents, kVtxThreads, kVtxSmemBytes, stream, ws, algo));
   if (le != cudaSuccess) return le;
   return cudaGetLastError();
 }

@@ -247,13 +247,16 @@ cudaError_t launchClustered(void (*k)(KArgs...), uint32_t x, uint32_t nEvents, u
 
 // Runs the whole chain on events [0, nEvents) of ws, on `stream`.  The
 // word/fedId/offset inputs must already be in ws.  Returns a CUDA error code.
-// riemann: the Riemann fit in place of the broken-line fit (useRiemannFit)
-cudaError_t runChain(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream, bool riemann = false);
+// riemann: the Riemann fit in place of the broken-line fit (useRiemannFit);
+// vertexAlgo: the vertex clusterer (runVertices)
+cudaError_t runChain(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream, bool riemann = false,
+                     int vertexAlgo = 0);
 // Individual stages (used by runChain and by the stage-level tests)
 cudaError_t runLocal(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream);
 cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream);
 cudaError_t runFits(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream, bool riemann = false);
-cudaError_t runVertices(Workspace& ws, uint32_t nEvents, cudaStream_t stream);
+// algo: 0 clusterTracksByDensity (default), 1 clusterTracksDBSCAN, 2 clusterTracksIterative
+cudaError_t runVertices(Workspace& ws, uint32_t nEvents, cudaStream_t stream, int algo = 0);
 cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream);
 
 // batch input descriptor and compact results (k_pack.cu)

@@ -76,6 +76,14 @@ typedef struct pg_config {
                                     parameter of CAHitNtupletGeneratorOnGPU.cc:49, default off) */
   uint32_t vertex_algo;          /* vertex clusterer of PixelVertexProducerCUDA.cc:26-35: 0 useDensity
                                     (the default), 1 useDBSCAN, 2 useIterative */
+  /* CAHitNtupletGeneratorOnGPU parameters (CAHitNtupletGeneratorOnGPU.cc:45-66); pg_default_config
+     sets the reference's values */
+  uint32_t min_hits_per_ntuplet;              /* 3 (default) or 4 */
+  uint32_t include_jumping_forward_doublets;  /* 1 */
+  uint32_t early_fishbone;                    /* 1 */
+  uint32_t late_fishbone;                     /* 0; 1 adds the late fishbone and the fishbone cleaner */
+  uint32_t ideal_conditions;                  /* 1 */
+  uint32_t do_cluster_cut, do_z0_cut, do_pt_cut; /* 1, 1, 1 */
 } pg_config;
 
 typedef struct pg_event_counts {
@@ -84,6 +92,7 @@ typedef struct pg_event_counts {
   uint32_t flags;               /* capacity flags (PG_FLAG_*) */
 } pg_event_counts;
 
+/* the reference's configuration; start every pg_config from it */
 void pg_default_config(pg_config* cfg);
 int pg_create(const pg_es_images* es, const pg_config* cfg, pg_ctx** out);
 /* the configuration in force (slots resolved when created with slots == 0) */

@@ -115,10 +115,20 @@ void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w);
 void makeClusters(const ES& es, const Words& w, Digis& d, Clusters& c);
 // PixelRecHitGPUKernel::makeHits (plugin-SiPixelRecHits/PixelRecHits.cc:33-53)
 void makeHits(const ES& es, const Digis& d, const Clusters& c, Hits& h);
+// the CA module's configurable switches (CAHitNtupletGeneratorOnGPU.cc:46-58,
+// defaults as there; the cut values stay the reference's constants)
+struct CAParams {
+  uint32_t minHitsPerNtuplet = 3;              // 3 or 4
+  bool includeJumpingForwardDoublets = true;   // pairs 15..18
+  bool earlyFishbone = true, lateFishbone = false;
+  bool idealConditions = true, doClusterCut = true, doZ0Cut = true, doPtCut = true;
+  bool useRiemannFit = false;                  // Riemann fit in place of the broken-line fit
+  // CAHitNtupletGeneratorKernels.cc:52-57: the layer pairs that are built
+  int nPairs() const { return minHitsPerNtuplet > 3 ? 13 : (includeJumpingForwardDoublets ? 19 : 15); }
+};
+
 // CAHitNtupletGeneratorOnGPU::makeTuples (plugin-PixelTriplets/CAHitNtupletGeneratorOnGPU.cc:96-126)
-// useRiemannFit selects the Riemann fit in place of the broken-line fit
-// (CAHitNtupletGeneratorOnGPU.cc:116-120; the reference's default is off)
-void makeTuples(const ES& es, const Hits& h, CA& ca, bool useRiemannFit = false);
+void makeTuples(const ES& es, const Hits& h, CA& ca, const CAParams& p = CAParams());
 // gpuVertexFinder::Producer::make (plugin-PixelVertexFinding/gpuVertexFinderImpl.h:84-111);
 // algo: 0 clusterTracksByDensity (the PixelVertexProducerCUDA default),
 // 1 clusterTracksDBSCAN, 2 clusterTracksIterative
@@ -133,7 +143,7 @@ void riemannFit(int N, const double* hits /*3xN col-major*/, const float* hits_g
                 float* cov15, float* pt, float* eta, float* chi2);
 
 // whole chain for one raw.bin event record
-void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev, bool useRiemannFit = false,
+void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev, const CAParams& p = CAParams(),
                   int vertexAlgo = 0);
 
 }  // namespace oracle

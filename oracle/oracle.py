@@ -16,6 +16,20 @@ sys.path.insert(0, os.path.join(ROOT, "pixeltrack-standalone_b200"))
 import build as _build  # noqa: E402
 from pixgpu import ERROR_DTYPE, SCALARS, _TYPES  # noqa: E402
 
+# the CA module's switches (CAHitNtupletGeneratorOnGPU.cc:46-58) with the
+# reference's defaults; the same names as the product's pg_config fields
+CA_DEFAULTS = {"min_hits_per_ntuplet": 3, "include_jumping_forward_doublets": 1, "early_fishbone": 1,
+               "late_fishbone": 0, "ideal_conditions": 1, "do_cluster_cut": 1, "do_z0_cut": 1, "do_pt_cut": 1}
+
+
+def _ca_args(ca):
+    p = dict(CA_DEFAULTS)
+    for k, v in (ca or {}).items():
+        if k not in p:
+            raise ValueError("unknown CA parameter %s" % k)
+        p[k] = int(v)
+    return [p[k] for k in CA_DEFAULTS]
+
 PRODUCTS = ["nDigis", "nModules", "xx", "yy", "adc", "moduleInd", "clus", "pdigi", "rawIdArr", "errors", "nClusters",
             "moduleStart", "clusInModule", "moduleId", "clusModuleStart", "nHits", "xl", "yl", "xerr", "yerr", "xg",
             "yg", "zg", "rg", "charge", "iphi", "xsize", "ysize", "detInd", "hitsLayerStart", "phiOff", "phiBins",
@@ -54,7 +68,7 @@ class _Named:
 class Oracle(_Named):
     """Sequential restatement of the serial chain (oracle/*.cc)."""
 
-    def __init__(self, es_images, riemann_fit=False, vertex_algo=0):
+    def __init__(self, es_images, riemann_fit=False, vertex_algo=0, ca=None):
         path = os.path.join(HERE, "liboracle.so")
         if not os.path.exists(path):
             _build.build_oracle()
@@ -87,6 +101,9 @@ class Oracle(_Named):
         self.lib.or_set_vertex_algo.argtypes = [ctypes.c_void_p, ctypes.c_int]
         if self.lib.or_set_vertex_algo(self._h, int(vertex_algo)) != 0:
             raise ValueError("vertex_algo: 0 density, 1 DBSCAN, 2 iterative")
+        self.lib.or_set_ca_params.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 8
+        if self.lib.or_set_ca_params(self._h, *_ca_args(ca)) != 0:
+            raise ValueError("min_hits_per_ntuplet: 3 or 4")
 
     def process(self, raw, names=None):
         if self.lib.or_process(self._h, raw, len(raw)) != 0:
@@ -157,7 +174,7 @@ def ref_available():
 class Reference(_Named):
     """The reference's own serial chain, compiled from its sources (checker build)."""
 
-    def __init__(self, datadir, riemann_fit=False, vertex_algo=0):
+    def __init__(self, datadir, riemann_fit=False, vertex_algo=0, ca=None):
         self.lib = ctypes.CDLL(REF_LIB)
         self.lib.pr_create.restype = ctypes.c_void_p
         self.lib.pr_create.argtypes = [ctypes.c_char_p]
@@ -173,6 +190,10 @@ class Reference(_Named):
         self.lib.pr_set_vertex_algo.argtypes = [ctypes.c_void_p, ctypes.c_int]
         if self.lib.pr_set_vertex_algo(self._h, int(vertex_algo)) != 0:
             raise ValueError("vertex_algo: 0 density, 1 DBSCAN, 2 iterative")
+        if ca:
+            self.lib.pr_set_ca_params.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 8
+            if self.lib.pr_set_ca_params(self._h, *_ca_args(ca)) != 0:
+                raise ValueError("min_hits_per_ntuplet: 3 or 4")
 
     def process(self, raw, names=None, internals=True):
         if self.lib.pr_process(self._h, raw, len(raw), 1 if internals else 0) != 0:

@@ -25,7 +25,7 @@ struct Handle {
   oracle::Event ev;
   std::map<std::string, Blob> out;
   double lastSeconds = 0;
-  bool useRiemannFit = false;
+  oracle::CAParams ca;
   int vertexAlgo = 0;
   std::string error;
 
@@ -142,11 +142,11 @@ void record(Handle& h) {
 }  // namespace
 
 namespace oracle {
-void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev, bool useRiemannFit, int vertexAlgo) {
+void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev, const CAParams& p, int vertexAlgo) {
   fedLoop(es, raw, n, ev.words);
   makeClusters(es, ev.words, ev.digis, ev.clusters);
   makeHits(es, ev.digis, ev.clusters, ev.hits);
-  makeTuples(es, ev.hits, ev.ca, useRiemannFit);
+  makeTuples(es, ev.hits, ev.ca, p);
   makeVertices(ev.ca, ev.vtx, vertexAlgo);
 }
 }  // namespace oracle
@@ -170,7 +170,24 @@ void* or_create(const uint8_t* cabling, size_t ncab, const uint8_t* gain, size_t
 void or_destroy(void* p) { delete static_cast<Handle*>(p); }
 
 // useRiemannFit of the CA module configuration (off by default, as in the reference)
-void or_set_riemann(void* p, int on) { static_cast<Handle*>(p)->useRiemannFit = on != 0; }
+void or_set_riemann(void* p, int on) { static_cast<Handle*>(p)->ca.useRiemannFit = on != 0; }
+
+// the CA module's switches (CAHitNtupletGeneratorOnGPU.cc:46-58); -1 when
+// minHitsPerNtuplet is outside 3..4
+int or_set_ca_params(void* p, int minHitsPerNtuplet, int includeJumpingForwardDoublets, int earlyFishbone,
+                     int lateFishbone, int idealConditions, int doClusterCut, int doZ0Cut, int doPtCut) {
+  if (minHitsPerNtuplet < 3 || minHitsPerNtuplet > 4) return -1;
+  auto& c = static_cast<Handle*>(p)->ca;
+  c.minHitsPerNtuplet = uint32_t(minHitsPerNtuplet);
+  c.includeJumpingForwardDoublets = includeJumpingForwardDoublets != 0;
+  c.earlyFishbone = earlyFishbone != 0;
+  c.lateFishbone = lateFishbone != 0;
+  c.idealConditions = idealConditions != 0;
+  c.doClusterCut = doClusterCut != 0;
+  c.doZ0Cut = doZ0Cut != 0;
+  c.doPtCut = doPtCut != 0;
+  return 0;
+}
 
 // vertex clustering of PixelVertexProducerCUDA: 0 density (default), 1 DBSCAN, 2 iterative
 int or_set_vertex_algo(void* p, int algo) {
@@ -184,7 +201,7 @@ int or_process(void* p, const uint8_t* raw, size_t n) {
   Handle& h = *static_cast<Handle*>(p);
   try {
     auto t0 = std::chrono::steady_clock::now();
-    oracle::processEvent(h.es, raw, n, h.ev, h.useRiemannFit, h.vertexAlgo);
+    oracle::processEvent(h.es, raw, n, h.ev, h.ca, h.vertexAlgo);
     auto t1 = std::chrono::steady_clock::now();
     h.lastSeconds = std::chrono::duration<double>(t1 - t0).count();
     record(h);
@@ -226,7 +243,7 @@ double or_time_events(void* p, const uint8_t* const* raws, const size_t* sizes, 
         if (k >= n) break;
         auto a = std::chrono::steady_clock::now();
         try {
-          oracle::processEvent(h.es, raws[k], sizes[k], ev, h.useRiemannFit, h.vertexAlgo);
+          oracle::processEvent(h.es, raws[k], sizes[k], ev, h.ca, h.vertexAlgo);
         } catch (std::exception&) {
           failed++;
         }

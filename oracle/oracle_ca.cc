@@ -29,8 +29,7 @@ constexpr float kMaxZ[kNPairs] = {20., 30., 0., 22., 30., -10., 70., 70., 22., 3
                                   -15., 70., 70., 20., 22., 30., 0., 70., 70.};
 constexpr float kMaxR[kNPairs] = {20., 9., 9., 20., 7., 7., 5., 5., 20., 6., 6., 5., 5., 20., 20., 9., 9., 9., 9.};
 
-// CAHitNtupletGeneratorOnGPU.cc:45-65 (module configuration)
-constexpr uint32_t kMinHitsPerNtuplet = 3;
+// CAHitNtupletGeneratorOnGPU.cc:45-65 (module configuration; the switches are CAParams)
 constexpr uint32_t kMaxDoublets = PF_MAX_DOUBLETS_PARAM;
 constexpr float kPtMin = 0.899999976158f;
 constexpr float kThetaCutBarrel = 0.00200000009499f;
@@ -94,7 +93,9 @@ inline float dca0(const Circle& e) {
 
 }  // namespace
 
-void makeTuples(const ES& es, const Hits& hh, CA& ca, bool useRiemannFit) {
+void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
+  const bool useRiemannFit = prm.useRiemannFit;
+  const int nPairs = prm.nPairs();
   const uint32_t nHits = hh.nHits;
   // ---- allocateOnGPU / launchZero (CAHitNtupletGeneratorKernelsAlloc.h:4-25) and tuples zero
   ca.nCells = 0;
@@ -129,8 +130,8 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, bool useRiemannFit) {
     auto layerSize = [&](uint8_t li) { return offsets[li + 1] - offsets[li]; };
     uint32_t cum[kNPairs];
     cum[0] = layerSize(kLayerPairs[0]);
-    for (int i = 1; i < kNPairs; ++i) cum[i] = cum[i - 1] + layerSize(kLayerPairs[2 * i]);
-    const uint32_t ntot = cum[kNPairs - 1];
+    for (int i = 1; i < nPairs; ++i) cum[i] = cum[i - 1] + layerSize(kLayerPairs[2 * i]);
+    const uint32_t ntot = cum[nPairs - 1];
     constexpr int minYsizeB1 = 36, minYsizeB2 = 28, maxDYsize12 = 28, maxDYsize = 20, maxDYPred = 20;
     constexpr float dzdrFact = 8 * 0.0285 / 0.015;
     constexpr float z0cut = 12.f;
@@ -149,11 +150,16 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, bool useRiemannFit) {
       if (mi > 2000) continue;
       float mez = hh.zg[i];
       if (mez < kMinZ[pairLayerId] || mez > kMaxZ[pairLayerId]) continue;
-      int16_t mes = hh.ysize[i];  // doClusterCut with ideal conditions: every ladder counts as outer
-      if (inner == 0 && outer > 3)
-        if (mes > 0 && mes < minYsizeB1) continue;
-      if (inner == 1 && outer > 3)
-        if (mes > 0 && mes < minYsizeB2) continue;
+      int16_t mes = -1;
+      if (prm.doClusterCut) {
+        // gpuPixelDoubletsAlgos.h:120-135: with ideal conditions every ladder counts as outer
+        const bool isOuterLadder = prm.idealConditions ? true : 0 == (mi / 8) % 2;
+        mes = inner > 0 || isOuterLadder ? hh.ysize[i] : int16_t(-1);
+        if (inner == 0 && outer > 3)
+          if (mes > 0 && mes < minYsizeB1) continue;
+        if (inner == 1 && outer > 3)
+          if (mes > 0 && mes < minYsizeB2) continue;
+      }
       int16_t mep = hh.iphi[i];
       float mer = hh.rg[i];
       int16_t iphicut = kPhiCuts[pairLayerId];
@@ -167,7 +173,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, bool useRiemannFit) {
           uint16_t mo = hh.detInd[oi];
           if (mo > 2000) continue;
           // z0cutoff
-          {
+          if (prm.doZ0Cut) {
             float zo = hh.zg[oi], ro = hh.rg[oi];
             float dr = ro - mer;
             if (dr > kMaxR[pairLayerId] || dr < 0 || std::abs((mez * ro - mer * zo)) > z0cut * dr) continue;
@@ -176,7 +182,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, bool useRiemannFit) {
           uint16_t idphi = uint16_t(std::min(std::abs(int16_t(mop - mep)), std::abs(int16_t(mep - mop))));
           if (idphi > iphicut) continue;
           // zsizeCut
-          {
+          if (prm.doClusterCut) {
             bool onlyBarrel = outer < 4;
             int16_t so = hh.ysize[oi];
             int dy = inner == 0 ? maxDYsize12 : maxDYsize;
@@ -187,7 +193,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, bool useRiemannFit) {
             if (cut) continue;
           }
           // ptcut
-          {
+          if (prm.doPtCut) {
             float ri = mer, ro = hh.rg[oi];
             float dphi = short2phi(short(idphi));
             if (dphi * dphi * (minRadius2T4 - ri * ro) > (ro - ri) * (ro - ri)) continue;
@@ -244,8 +250,10 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, bool useRiemannFit) {
     }
   }
 
-  // ---- fishbone, early (gpuFishbone.h:21-90), checkTrack = false
-  if (nHits > 1) {
+  // ---- fishbone (gpuFishbone.h:21-90): early (after connect) with checkTrack
+  //      false, late (after the multiplicity fill) with checkTrack true, which
+  //      skips cells that are on no n-tuplet (CAHitNtupletGeneratorKernels.cc:101-134)
+  auto fishbone = [&](bool checkTrack) {
     std::vector<float> x, y, z, n;
     std::vector<uint16_t> d;
     std::vector<uint32_t> cc;
@@ -258,6 +266,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, bool useRiemannFit) {
       for (uint32_t ic = 0; ic < s; ++ic) {
         uint32_t c = vc[ic];
         if (0 == ca.used[c]) continue;
+        if (checkTrack && ca.trk[c].empty()) continue;
         cc.push_back(c);
         d.push_back(uint16_t(float(hh.detInd[ca.inner[c]])));
         float xx = hh.xg[ca.inner[c]] - xo, yy = hh.yg[ca.inner[c]] - yo, zz = ca.innerZ[c] - zo;
@@ -282,7 +291,8 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, bool useRiemannFit) {
         }
       }
     }
-  }
+  };
+  if (nHits > 1 && prm.earlyFishbone) fishbone(false);
 
   // ---- kernel_find_ntuplets (CAHitNtupletGeneratorKernelsImpl.h:264-292) with
   //      GPUCACell::find_ntuplets<6> (GPUCACell.h:278-331) and bulkFill (HistoContainer.h:181-190)
@@ -307,7 +317,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, bool useRiemannFit) {
       last = false;
       dfs(other);
     }
-    if (last && uint32_t(depth) >= kMinHitsPerNtuplet - 1) {
+    if (last && uint32_t(depth) >= prm.minHitsPerNtuplet - 1) {
       uint16_t hits[6];
       uint32_t nh = 0;
       for (int k = 0; k < depth; ++k) hits[nh++] = ca.inner[tmp[k]];
@@ -328,7 +338,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, bool useRiemannFit) {
   for (uint32_t idx = 0; idx < nCells; ++idx) {
     if (ca.doubletId[idx] < 0) continue;
     int pid = ca.layerPair[idx];
-    bool doit = kMinHitsPerNtuplet > 3 ? pid < 3 : pid < 8 || pid > 12;
+    bool doit = prm.minHitsPerNtuplet > 3 ? pid < 3 : pid < 8 || pid > 12;
     if (doit) {
       depth = 0;
       dfs(idx);
@@ -368,6 +378,8 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, bool useRiemannFit) {
     uint32_t w = ca.tmOff[nh]--;
     ca.tmBins[w - 1] = uint16_t(it);
   }
+
+  if (nHits > 1 && prm.lateFishbone) fishbone(true);
 
   // ---- fillHitDetIndices (Impl.h:449-464)
   for (uint32_t k = 0; k < ca.tupleOff[kTupleBins]; ++k) ca.tupleDet[k] = hh.detInd[ca.tupleHits[k]];
@@ -432,6 +444,12 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, bool useRiemannFit) {
     bool isOk = (std::abs(tip) < maxTip) and (ca.pt[it] > minPt) and (std::abs(zip) < maxZip);
     if (isOk) ca.quality[it] = kLoose;
   }
+
+  // ---- kernel_fishboneCleaner (Impl.h:104-116), with lateFishbone only
+  if (prm.lateFishbone)
+    for (uint32_t idx = 0; idx < nCells; ++idx)
+      if (ca.doubletId[idx] < 0)
+        for (auto it : ca.trk[idx]) ca.quality[it] = kBad;
 
   // ---- kernel_fastDuplicateRemover (Impl.h:151-189): sequential over cells
   for (uint32_t idx = 0; idx < nCells; ++idx) {

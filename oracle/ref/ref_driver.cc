@@ -98,6 +98,10 @@ struct RefChain {
   // reference's own configuration fixes it to false
   // (CAHitNtupletGeneratorOnGPU.cc:49)
   bool useRiemannFit = false;
+  // the CA module's switches when set through pr_set_ca_params; otherwise
+  // the reference's own configuration (caGen->m_params)
+  std::unique_ptr<cAHitNtupletGenerator::Params> caParams;
+  const cAHitNtupletGenerator::Params& params() const { return caParams ? *caParams : caGen->m_params; }
 
   template <typename T>
   void put(const std::string& name, const T* p, size_t n) {
@@ -254,16 +258,16 @@ int pr_process(void* p, const uint8_t* raw, size_t nraw, int dump) {
   float bfield = bf;
   PixelTrackHeterogeneous tracks(std::make_unique<pixelTrack::TrackSoA>());
   auto* soa = tracks.get();
-  CAHitNtupletGeneratorKernelsCPU kernels(h.caGen->m_params);
+  CAHitNtupletGeneratorKernelsCPU kernels(h.params());
   kernels.counters_ = h.caGen->m_counters;
   kernels.allocateOnGPU(nullptr);
   kernels.buildDoublets(hits, nullptr);
   kernels.launchKernels(hits, soa, nullptr);
   kernels.fillHitDetIndices(hits.view(), soa, nullptr);
   if (0 != hits.nHits()) {
-    HelixFitOnGPU fitter(bfield, h.caGen->m_params.fit5as4_);
+    HelixFitOnGPU fitter(bfield, h.params().fit5as4_);
     fitter.allocateOnGPU(&(soa->hitIndices), kernels.tupleMultiplicity(), soa);
-    if (h.caGen->m_params.useRiemannFit_ || h.useRiemannFit)
+    if (h.params().useRiemannFit_ || h.useRiemannFit)
       fitter.launchRiemannKernelsOnCPU(hits.view(), hits.nHits(), CAConstants::maxNumberOfQuadruplets());
     else
       fitter.launchBrokenLineKernelsOnCPU(hits.view(), hits.nHits(), CAConstants::maxNumberOfQuadruplets());
@@ -456,6 +460,21 @@ int pr_names(void* p, char* buf, size_t n) {
 double pr_last_seconds(void* p) { return static_cast<RefChain*>(p)->lastSeconds; }
 
 void pr_set_riemann(void* p, int on) { static_cast<RefChain*>(p)->useRiemannFit = on != 0; }
+
+// A CA module configuration that differs from the reference's own in its
+// switches (CAHitNtupletGeneratorOnGPU.cc:46-58); every cut value is kept.
+int pr_set_ca_params(void* p, int minHitsPerNtuplet, int includeJumpingForwardDoublets, int earlyFishbone,
+                     int lateFishbone, int idealConditions, int doClusterCut, int doZ0Cut, int doPtCut) {
+  if (minHitsPerNtuplet < 3 || minHitsPerNtuplet > 4) return -1;
+  auto& h = *static_cast<RefChain*>(p);
+  const auto& d = h.caGen->m_params;
+  h.caParams = std::make_unique<cAHitNtupletGenerator::Params>(
+      d.onGPU_, uint32_t(minHitsPerNtuplet), d.maxNumberOfDoublets_, d.useRiemannFit_, d.fit5as4_,
+      includeJumpingForwardDoublets != 0, earlyFishbone != 0, lateFishbone != 0, idealConditions != 0, d.doStats_,
+      doClusterCut != 0, doZ0Cut != 0, doPtCut != 0, d.ptmin_, d.CAThetaCutBarrel_, d.CAThetaCutForward_,
+      d.hardCurvCut_, d.dcaCutInnerTriplet_, d.dcaCutOuterTriplet_, d.cuts_);
+  return 0;
+}
 
 // The vertex finder of a PixelVertexProducerCUDA configured with useDensity
 // (0, the reference's own configuration), useDBSCAN (1) or useIterative (2);

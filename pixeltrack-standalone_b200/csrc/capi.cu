@@ -310,6 +310,15 @@ void pg_default_config(pg_config* cfg) {
   cfg->hbm_fraction = 0.5;
   cfg->riemann_fit = 0;
   cfg->vertex_algo = 0;
+  // CAHitNtupletGeneratorOnGPU.cc:45-66
+  cfg->min_hits_per_ntuplet = 3;
+  cfg->include_jumping_forward_doublets = 1;
+  cfg->early_fishbone = 1;
+  cfg->late_fishbone = 0;
+  cfg->ideal_conditions = 1;
+  cfg->do_cluster_cut = 1;
+  cfg->do_z0_cut = 1;
+  cfg->do_pt_cut = 1;
 }
 
 namespace {
@@ -318,6 +327,15 @@ int createSlot(pg_ctx* c, Slot& s, size_t bytes) {
   const uint32_t E = c->cfg.max_events;
   if (cudaMalloc(&s.dmem, bytes) != cudaSuccess) return fail(c, PG_ERR_NOMEM, "slot workspace");
   workspaceCarve(s.ws, s.dmem, E, c->cfg.max_words_per_batch);
+  // layer pairs of CAHitNtupletGeneratorKernels.cc:52-57
+  s.ws.ca.nPairs = c->cfg.min_hits_per_ntuplet > 3 ? 13u : (c->cfg.include_jumping_forward_doublets ? 19u : 15u);
+  s.ws.ca.minHits = c->cfg.min_hits_per_ntuplet;
+  s.ws.ca.idealConditions = c->cfg.ideal_conditions != 0;
+  s.ws.ca.doClusterCut = c->cfg.do_cluster_cut != 0;
+  s.ws.ca.doZ0Cut = c->cfg.do_z0_cut != 0;
+  s.ws.ca.doPtCut = c->cfg.do_pt_cut != 0;
+  s.ws.ca.earlyFishbone = c->cfg.early_fishbone != 0;
+  s.ws.ca.lateFishbone = c->cfg.late_fishbone != 0;
   if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&s.gathered, cudaEventDisableTiming) != cudaSuccess ||
@@ -369,7 +387,7 @@ int pg_create(const pg_es_images* es, const pg_config* cfgIn, pg_ctx** out) {
   else
     pg_default_config(&c->cfg);
   if (c->cfg.max_events == 0 || c->cfg.max_words_per_batch == 0 || c->cfg.max_words_per_batch > (1u << 30) ||
-      c->cfg.vertex_algo > 2)
+      c->cfg.vertex_algo > 2 || c->cfg.min_hits_per_ntuplet < 3 || c->cfg.min_hits_per_ntuplet > 4)
     return PG_ERR_ARG;
   c->device = c->cfg.device;
   cudaError_t e = cudaSetDevice(c->cfg.device);

@@ -46,7 +46,6 @@ constexpr float kThetaCutForward = 0.00300000002608f;
 constexpr float kHardCurvCut = 0.0328407224959f;
 constexpr float kDcaCutInner = 0.15000000596f;
 constexpr float kDcaCutOuter = 0.25f;
-constexpr uint32_t kMinHits = 3;
 constexpr uint8_t kBad = 0, kDup = 1, kLoose = 2;
 
 __device__ __forceinline__ uint32_t phiBin(int16_t t) { return uint32_t((int(t) >> 9) & 127); }
@@ -76,10 +75,10 @@ __global__ void kDoubletSetup(Workspace ws, uint32_t nEvents) {
     c->ntot = 0;
     return;
   }
-  for (int p = 0; p < kNPairs; ++p) {
+  for (uint32_t p = 0; p < uint32_t(kNPairs); ++p) {
     uint8_t li = cLayerPairs[2 * p];
-    cum += c->layerStart[li + 1] - c->layerStart[li];
-    c->pairCum[p] = cum;
+    if (p < ws.ca.nPairs) cum += c->layerStart[li + 1] - c->layerStart[li];
+    c->pairCum[p] = cum;  // pairs beyond nPairs own no slots
   }
   if (cum > kJCap) {
     c->flags |= kFlagJOverflow;
@@ -94,6 +93,7 @@ __global__ void kDoubletSetup(Workspace ws, uint32_t nEvents) {
 // serial order of the candidates is the window's bin order with each bin's
 // stored order, i.e. the order of these ranges.
 struct DoubletSeed {
+  uint32_t cuts;  // bit 0 z0 cut, bit 1 cluster-size cut, bit 2 pt cut
   uint32_t pair, inner, outer, i;
   float mez, mer;
   int16_t mep, mes, iphicut;
@@ -101,15 +101,18 @@ struct DoubletSeed {
   uint32_t b0, e0, b1, e1;  // candidate ranges in phiBins
 };
 
-// per-event layer offsets staged in shared memory by each block
+// per-event layer offsets staged in shared memory by each block, with the
+// CA configuration
 struct PairTable {
   uint32_t pairCum[kNPairs];
   uint32_t layerStart[11];
+  CAConfig ca;
 };
 
-__device__ __forceinline__ void loadPairTable(const EventCounters* c, PairTable& t) {
+__device__ __forceinline__ void loadPairTable(const EventCounters* c, PairTable& t, const CAConfig& ca) {
   if (threadIdx.x < kNPairs) t.pairCum[threadIdx.x] = c->pairCum[threadIdx.x];
   if (threadIdx.x < 11) t.layerStart[threadIdx.x] = c->layerStart[threadIdx.x];
+  if (threadIdx.x == 0) t.ca = ca;
   __syncthreads();
 }
 
@@ -119,6 +122,7 @@ __device__ __forceinline__ bool doubletSeed(const PairTable& c, const HitsView& 
   const uint8_t inner = cLayerPairs[2 * pair], outer = cLayerPairs[2 * pair + 1];
   uint32_t i = (0 == pair) ? j : j - c.pairCum[pair - 1];
   i += c.layerStart[inner];
+  d.cuts = (c.ca.doZ0Cut ? 1u : 0u) | (c.ca.doClusterCut ? 2u : 0u) | (c.ca.doPtCut ? 4u : 0u);
   d.pair = pair;
   d.inner = inner;
   d.outer = outer;
@@ -126,11 +130,15 @@ __device__ __forceinline__ bool doubletSeed(const PairTable& c, const HitsView& 
   if (hh.detInd[i] > 2000) return false;
   d.mez = hh.zg[i];
   if (d.mez < cMinZ[pair] || d.mez > cMaxZ[pair]) return false;
-  d.mes = hh.ysize[i];  // ideal conditions: every ladder is treated as outer
-  if (inner == 0 && outer > 3)
-    if (d.mes > 0 && d.mes < 36) return false;
-  if (inner == 1 && outer > 3)
-    if (d.mes > 0 && d.mes < 28) return false;
+  d.mes = -1;
+  if (c.ca.doClusterCut) {
+    const bool isOuterLadder = c.ca.idealConditions ? true : 0 == (hh.detInd[i] / 8) % 2;
+    d.mes = inner > 0 || isOuterLadder ? hh.ysize[i] : int16_t(-1);
+    if (inner == 0 && outer > 3)
+      if (d.mes > 0 && d.mes < 36) return false;
+    if (inner == 1 && outer > 3)
+      if (d.mes > 0 && d.mes < 28) return false;
+  }
   d.mep = hh.iphi[i];
   d.mer = hh.rg[i];
   d.iphicut = cPhiCuts[pair];
@@ -162,7 +170,7 @@ __device__ __forceinline__ bool doubletAccept(const DoubletSeed& d, const uint4 
   if ((rec.w & 0xffffu) > 2000) return false;
   const float zo = __uint_as_float(rec.x), ro = __uint_as_float(rec.y);
   const float dr = ro - d.mer;
-  if (dr > d.maxr || dr < 0 || fabsf((d.mez * ro - d.mer * zo)) > z0cut * dr) return false;
+  if ((d.cuts & 1u) && (dr > d.maxr || dr < 0 || fabsf((d.mez * ro - d.mer * zo)) > z0cut * dr)) return false;
   const int16_t mop = int16_t(rec.z & 0xffffu);
   const uint16_t idphi = uint16_t(min(abs(int(int16_t(mop - d.mep))), abs(int(int16_t(d.mep - mop)))));
   if (idphi > d.iphicut) return false;
@@ -170,9 +178,9 @@ __device__ __forceinline__ bool doubletAccept(const DoubletSeed& d, const uint4 
   const bool cut = (d.outer < 4) ? (d.mes > 0 && so > 0 && abs(so - d.mes) > (d.inner == 0 ? 28 : 20))
                                  : ((d.inner < 4) && d.mes > 0 &&
                                     abs(d.mes - int(fabsf((d.mez - zo) / (d.mer - ro)) * dzdrFact + 0.5f)) > 20);
-  if (cut) return false;
+  if ((d.cuts & 2u) && cut) return false;
   const float dphi = float(short(idphi)) * i2p;
-  if (dphi * dphi * (minRadius2T4 - d.mer * ro) > (ro - d.mer) * (ro - d.mer)) return false;
+  if ((d.cuts & 4u) && dphi * dphi * (minRadius2T4 - d.mer * ro) > (ro - d.mer) * (ro - d.mer)) return false;
   return true;
 }
 
@@ -221,6 +229,7 @@ __device__ __forceinline__ void forSeedSlots(const PairTable& pt, const HitsView
       const int l = __ffs(m) - 1;
       m &= m - 1;
       DoubletSeed ds;
+      ds.cuts = __shfl_sync(0xffffffffu, d.cuts, l);
       ds.pair = __shfl_sync(0xffffffffu, d.pair, l);
       ds.inner = __shfl_sync(0xffffffffu, d.inner, l);
       ds.outer = __shfl_sync(0xffffffffu, d.outer, l);
@@ -252,7 +261,7 @@ __global__ void kDoubletCount(Workspace ws) {
   const uint32_t e = blockIdx.y;
   const EventCounters* c = ws.ev + e;
   const uint32_t ntot = c->ntot;
-  loadPairTable(c, pt);
+  loadPairTable(c, pt, ws.ca);
   const HitsView hh = hitsOf(ws, e);
   const uint4* rec = ws.phiRec + size_t(e) * kHitCap;
   uint32_t* cnt = ws.jCount + size_t(e) * (kJCap + 1);
@@ -288,7 +297,7 @@ __global__ void kDoubletWrite(Workspace ws) {
   const uint32_t e = blockIdx.y;
   const EventCounters* c = ws.ev + e;
   const uint32_t ntot = c->ntot;
-  loadPairTable(c, pt);
+  loadPairTable(c, pt, ws.ca);
   const HitsView hh = hitsOf(ws, e);
   const uint4* rec = ws.phiRec + size_t(e) * kHitCap;
   const uint32_t* off = ws.jOffset + size_t(e) * (kJCap + 1);
@@ -582,7 +591,9 @@ __global__ void kNbrPool(Workspace ws) {
 // doubletId = -1 and never change the `used` flags the loop reads, so the
 // lanes are independent.
 constexpr int kFishWarps = 8;
-__global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws) {
+// checkTrack: the late fishbone (gpuFishbone.h:21-90 with checkTrack), which
+// also skips cells that no tuple goes through
+__global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws, bool checkTrack) {
   __shared__ float sxA[kFishWarps][PF_MAX_CELLS_PER_HIT], syA[kFishWarps][PF_MAX_CELLS_PER_HIT],
       szA[kFishWarps][PF_MAX_CELLS_PER_HIT];
   __shared__ uint16_t sdA[kFishWarps][PF_MAX_CELLS_PER_HIT];
@@ -598,6 +609,7 @@ __global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws) {
   const uint32_t* ohCells = ws.ohCells + cb;
   const float4* ohRec = ws.ohRec + cb;
   const uint16_t* ohDet = ws.ohDet + cb;
+  const uint32_t* trkOff = ws.trkOff + size_t(e) * (kCellCap + 1);
   const uint32_t w = threadIdx.x >> 5, lane = laneId();
   float* sx = sxA[w];
   float* sy = syA[w];
@@ -626,7 +638,7 @@ __global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws) {
         sy[r] = rec.y - yo;
         sz[r] = rec.z - zo;
         sd[r] = ohDet[b + k];
-        su[r] = ws.cellUsed[cb + cell];
+        su[r] = ws.cellUsed[cb + cell] && !(checkTrack && trkOff[cell + 1] == trkOff[cell]) ? 1 : 0;
         sc[r] = cell;
       }
     }
@@ -661,7 +673,7 @@ __global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws) {
 // Emit(depth, cells[], outerHitOfLast) is called for every saved tuple.
 template <typename Emit>
 __device__ __forceinline__ bool dfsNtuplets(uint32_t start, const int32_t* doubletId, const uint32_t* nbrOff,
-                                            const uint32_t* nbr, Emit&& emit) {
+                                            const uint32_t* nbr, uint32_t minHits, Emit&& emit) {
   uint32_t stack[5], pos[5];
   int depth = 0;
   stack[0] = start;
@@ -689,7 +701,7 @@ __device__ __forceinline__ bool dfsNtuplets(uint32_t start, const int32_t* doubl
       break;
     }
     if (descended) continue;
-    if (last[depth] && uint32_t(depth + 1) >= kMinHits - 1) emit(depth + 1, stack);
+    if (last[depth] && uint32_t(depth + 1) >= minHits - 1) emit(depth + 1, stack);
     --depth;
   }
   return true;
@@ -698,7 +710,7 @@ __device__ __forceinline__ bool dfsNtuplets(uint32_t start, const int32_t* doubl
 __device__ __forceinline__ bool isStartCell(const Workspace& ws, size_t cb, uint32_t idx) {
   if (ws.cellDoubletId[cb + idx] < 0) return false;
   int pid = ws.cellPair[cb + idx];
-  return kMinHits > 3 ? pid < 3 : (pid < 8 || pid > 12);
+  return ws.ca.minHits > 3 ? pid < 3 : (pid < 8 || pid > 12);
 }
 
 __global__ void kNtupletCount(Workspace ws) {
@@ -713,7 +725,7 @@ __global__ void kNtupletCount(Workspace ws) {
   for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
     uint32_t nt = 0, nh = 0;
     if (isStartCell(ws, cb, idx)) {
-      bool ok = dfsNtuplets(idx, ws.cellDoubletId + cb, nbrOff, nbr, [&](int ncells, const uint32_t*) {
+      bool ok = dfsNtuplets(idx, ws.cellDoubletId + cb, nbrOff, nbr, ws.ca.minHits, [&](int ncells, const uint32_t*) {
         ++nt;
         nh += uint32_t(ncells) + 1;
       });
@@ -741,7 +753,7 @@ __global__ void kNtupletWrite(Workspace ws) {
     if (!isStartCell(ws, cb, idx)) continue;
     uint32_t m = to[idx], off = ho[idx];
     if (m >= kTupleBins) continue;
-    dfsNtuplets(idx, ws.cellDoubletId + cb, nbrOff, nbr, [&](int ncells, const uint32_t* cells) {
+    dfsNtuplets(idx, ws.cellDoubletId + cb, nbrOff, nbr, ws.ca.minHits, [&](int ncells, const uint32_t* cells) {
       if (m < kTupleBins) {
         toff[m] = off;
         for (int k = 0; k < ncells; ++k) {
@@ -778,17 +790,24 @@ __global__ void kTupleFinalize(Workspace ws) {
 
 __device__ __forceinline__ uint32_t tupleSize(const uint32_t* toff, uint32_t t) { return toff[t + 1] - toff[t]; }
 
+// cells of stored tuple t, from its cell slots: unlike tupleSize this also
+// holds for the last bin of a full container, whose size the finalize sets to
+// zero after the tuple was written and added to its cells' track lists
+__device__ __forceinline__ uint32_t tupleCellCount(const uint32_t* tcell, uint32_t t) {
+  uint32_t n = 0;
+  while (n < 4 && tcell[4 * t + n] != 0xffffffffu) ++n;
+  return n;
+}
+
 // cell -> track lists: count, (scan), fill, order
 __global__ void kTrackCount(Workspace ws) {
   uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   uint32_t nt = c->nTuples;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
   const uint32_t* tcell = ws.tupleCells + size_t(e) * kTupleCellCap;
   uint32_t* cnt = ws.trkCount + size_t(e) * (kCellCap + 1);
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
-    if (tupleSize(toff, t) == 0) continue;
-    uint32_t ncell = tupleSize(toff, t) - 1;
+    const uint32_t ncell = tupleCellCount(tcell, t);
     for (uint32_t k = 0; k < ncell; ++k) atomicAdd(&cnt[tcell[4 * t + k]], 1u);
   }
 }
@@ -797,14 +816,12 @@ __global__ void kTrackFill(Workspace ws) {
   uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   uint32_t nt = c->nTuples;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
   const uint32_t* tcell = ws.tupleCells + size_t(e) * kTupleCellCap;
   const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
   uint32_t* cur = ws.trkCount + size_t(e) * (kCellCap + 1);
   uint16_t* trk = ws.trk + size_t(e) * kTupleCellCap;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
-    if (tupleSize(toff, t) == 0) continue;
-    uint32_t ncell = tupleSize(toff, t) - 1;
+    const uint32_t ncell = tupleCellCount(tcell, t);
     for (uint32_t k = 0; k < ncell; ++k) {
       uint32_t cc = tcell[4 * t + k];
       uint32_t p = atomicAdd(&cur[cc], 1u);
@@ -985,7 +1002,7 @@ __global__ void kFastDupInDegree(Workspace ws, uint32_t* indeg, const uint32_t* 
     uint32_t d = 0;
     for (uint32_t j = 0; j < s; ++j) {
       uint16_t t = trk[b + j];
-      uint32_t ncell = tupleSize(toff, t) - 1;
+      uint32_t ncell = tupleCellCount(tcell, t);
       for (uint32_t q = 0; q < ncell; ++q) {
         uint32_t o = tcell[4 * t + q];
         if (o < cell && flag[o] && inTrkList(off, trk, o, t)) ++d;
@@ -1060,7 +1077,7 @@ __global__ void __launch_bounds__(kFastDupThreads)
       // release later candidates sharing a track
       for (uint32_t j = 0; j < s; ++j) {
         const uint16_t t = trk[b + j];
-        const uint32_t ncell = tupleSize(toff, t) - 1;
+        const uint32_t ncell = tupleCellCount(tcell, t);
         for (uint32_t qq = 0; qq < ncell; ++qq) {
           const uint32_t o = tcell[4 * t + qq];
           if (o > cell && flag[o] && inTrkList(off, trk, o, t)) {
@@ -1153,6 +1170,22 @@ __global__ void kCopyCount(uint32_t* dst, uint32_t dstStride, const uint32_t* sr
   if (e < nEvents) dst[size_t(e) * dstStride] = src[size_t(e) * srcStride];
 }
 
+// kernel_fishboneCleaner (CAHitNtupletGeneratorKernelsImpl.h:104-116): the
+// tuples through a cell the late fishbone killed are bad
+__global__ void kFishboneCleaner(Workspace ws) {
+  const uint32_t e = blockIdx.y;
+  const uint32_t n = ws.ev[e].nCells;
+  const size_t cb = size_t(e) * kCellCap;
+  const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
+  const uint16_t* trk = ws.trk + size_t(e) * kTupleCellCap;
+  uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (ws.cellDoubletId[cb + i] >= 0) continue;
+    const uint32_t b = off[i], s = trkListSize(off, i);
+    for (uint32_t j = 0; j < s; ++j) q[trk[b + j]] = kBad;
+  }
+}
+
 }  // namespace
 
 #define EVF(field) (&ws.ev[0].field), (sizeof(EventCounters) / 4)
@@ -1181,7 +1214,8 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.nbr, kEdgeCap, ws.nbrOff, kCellCap + 1, EVF(nCells), 0, false, kEdgeCap, 1);
   PG_PROBED("kNbrPool", stream, kNbrPool<<<g, 256, 0, stream>>>(ws));
   // ---- early fishbone
-  PG_PROBED("kFishbone", stream, kFishbone<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws));
+  if (ws.ca.earlyFishbone)
+    PG_PROBED("kFishbone", stream, kFishbone<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws, false));
   // ---- n-tuplets: DFS count, scans, DFS write, finalize
   PG_PROBED("kNtupletCount", stream, kNtupletCount<<<dim3(gx * 8, nEvents), 128, 0, stream>>>(ws));
   segScan(ws.startTupleCount, ws.startTupleOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcM), ws.scanSums, nEvents, stream);
@@ -1203,6 +1237,9 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   PG_PROBED("kTupleDet", stream, kTupleDet<<<g, 256, 0, stream>>>(ws));
   // ---- tuple multiplicity for the fits
   PG_PROBED("kMultiplicity", stream, kMultiplicity<<<nEvents, 1024, 0, stream>>>(ws));
+  // ---- late fishbone (CAHitNtupletGeneratorKernels.cc:133-136)
+  if (ws.ca.lateFishbone)
+    PG_PROBED("kFishbone", stream, kFishbone<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws, true));
   return cudaGetLastError();
 }
 
@@ -1210,6 +1247,8 @@ cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   const uint32_t gx = nEvents >= 32 ? 16 : (nEvents >= 8 ? 64 : 296);
   dim3 g(gx, nEvents);
   PG_PROBED("kClassify", stream, kClassify<<<g, 256, 0, stream>>>(ws));
+  // kernel_fishboneCleaner with the late fishbone (CAHitNtupletGeneratorKernels.cc:159-162)
+  if (ws.ca.lateFishbone) PG_PROBED("kFishboneCleaner", stream, kFishboneCleaner<<<g, 256, 0, stream>>>(ws));
   // fastDuplicateRemover (candFlag survives in startTupleCount from runCA)
   uint32_t* candFlag = ws.startTupleCount;
   uint32_t* candOff = ws.startHitCount;  // candidate index of each cell, from runCA

@@ -101,9 +101,20 @@ struct BatchInput {
 
 constexpr uint32_t kScanMaxSlices = 64;  // slices of one event's array in the segmented scan
 
+// CAHitNtupletGeneratorOnGPU parameters that select among the algorithm's
+// variants (CAHitNtupletGeneratorOnGPU.cc:45-66; CAHitNtupletGeneratorKernels.cc:52-70)
+struct CAConfig {
+  uint32_t nPairs;           // layer pairs searched: 19; 15 without jumping forward doublets; 13 for quadruplets
+  uint32_t minHits;          // minHitsPerNtuplet (3 or 4)
+  uint32_t idealConditions;  // every ladder treated as outer in the cluster-size cut
+  uint32_t doClusterCut, doZ0Cut, doPtCut;
+  uint32_t earlyFishbone, lateFishbone;
+};
+
 struct Workspace {
   uint32_t maxEvents;
   uint32_t wordCap;          // words over the whole batch
+  CAConfig ca;               // the context's CA configuration
   // input
   uint32_t* words;
   uint8_t* fedIds;

@@ -185,10 +185,15 @@ class ESImages(ctypes.Structure):
                 ("fedids_size", ctypes.c_size_t)]
 
 
+CA_FIELDS = ("min_hits_per_ntuplet", "include_jumping_forward_doublets", "early_fishbone", "late_fishbone",
+             "ideal_conditions", "do_cluster_cut", "do_z0_cut", "do_pt_cut")
+
+
 class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("max_events", ctypes.c_uint32), ("max_words_per_batch", ctypes.c_uint32),
                 ("slots", ctypes.c_uint32), ("use_graphs", ctypes.c_uint32), ("pool_words", ctypes.c_uint64),
-                ("hbm_fraction", ctypes.c_double), ("riemann_fit", ctypes.c_uint32), ("vertex_algo", ctypes.c_uint32)]
+                ("hbm_fraction", ctypes.c_double), ("riemann_fit", ctypes.c_uint32), ("vertex_algo", ctypes.c_uint32)] + \
+        [(n, ctypes.c_uint32) for n in CA_FIELDS]
 
 
 class ResultView(ctypes.Structure):
@@ -334,14 +339,24 @@ class Chain:
     """A device context: resident conditions plus batch slots."""
 
     def __init__(self, es_images, max_events=64, max_words_per_batch=None, slots=1, device=0, use_graphs=True,
-                 pool_words=0, hbm_fraction=0.5, riemann_fit=False, vertex_algo=0):
+                 pool_words=0, hbm_fraction=0.5, riemann_fit=False, vertex_algo=0, ca=None):
+        """ca: CAHitNtupletGeneratorOnGPU parameters overriding the reference's (pg_config field
+        names: min_hits_per_ntuplet, include_jumping_forward_doublets, early_fishbone, late_fishbone,
+        ideal_conditions, do_cluster_cut, do_z0_cut, do_pt_cut)."""
         lib = gpu_lib()
         self._keep = list(es_images)
         img = ESImages(*[x for b in self._keep for x in (b, len(b))])
         if max_words_per_batch is None:
             max_words_per_batch = max_events * 160000
-        cfg = Config(device, max_events, max_words_per_batch, slots, 1 if use_graphs else 0, pool_words, hbm_fraction,
-                     1 if riemann_fit else 0, int(vertex_algo))
+        cfg = Config()
+        lib.pg_default_config(ctypes.byref(cfg))
+        cfg.device, cfg.max_events, cfg.max_words_per_batch, cfg.slots = device, max_events, max_words_per_batch, slots
+        cfg.use_graphs, cfg.pool_words, cfg.hbm_fraction = 1 if use_graphs else 0, pool_words, hbm_fraction
+        cfg.riemann_fit, cfg.vertex_algo = 1 if riemann_fit else 0, int(vertex_algo)
+        for k, v in (ca or {}).items():
+            if k not in CA_FIELDS:
+                raise ValueError("unknown CA parameter %s" % k)
+            setattr(cfg, k, int(v))
         self._h = ctypes.c_void_p()
         rc = lib.pg_create(ctypes.byref(img), ctypes.byref(cfg), ctypes.byref(self._h))
         if rc != 0:

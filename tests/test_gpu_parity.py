@@ -54,6 +54,20 @@ def test_matches_oracle(chain, default_detector, seed, pu):
     assert diffs == [], _report(diffs)
 
 
+def test_matches_oracle_at_saturation(chain, default_detector):
+    """This PU 75 event fills the 458752-doublet capacity and the 32768-tuple
+    container; the last tuple is written and joins its cells' track lists
+    before the finalize empties its bin, as in the reference."""
+    import oracle
+    raw = default_detector.event(105, 75)
+    want = oracle.Oracle(default_detector.es).process(raw)
+    assert want["nCells"] == 458752 and want["nTuples"] == 32767
+    chain.process([raw])
+    got = chain.products(0)
+    diffs = oracle.compare(want, got, rtol=RTOL)
+    assert diffs == [], _report(diffs)
+
+
 def test_batch_results_equal_single_event_results(chain, default_detector):
     """Each event's products are the same alone and inside a mixed-PU batch."""
     import oracle

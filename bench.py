@@ -32,6 +32,7 @@ import concurrent.futures as cf
 import json
 import os
 import shutil
+import struct
 import subprocess
 import sys
 import tempfile
@@ -431,33 +432,50 @@ def run_ours(a):
            "result_bytes_per_step": result_bytes[0] / max(1, a.steps)}
 
     # ------------------------------------------------------------ end to end through pg_submit
-    e2e_chain = pixgpu.Chain(det.es, max_events=B, max_words_per_batch=max_words, slots=a.slots, device=dev)
-    e2e_chain.prepare(B)
     nbh = len(raws) // B
     host_batches = [raws[(i % nbh) * B:(i % nbh) * B + B] for i in range(nbh)]
-    h2d = [0]
-    d2h = [0]
 
-    def e2e_done(slot):
-        sm = e2e_chain.summary(slot)
-        d2h[0] += sm["result_bytes"]
-        h2d[0] += 4 * sm["n_digis"] + sm["n_digis"] // 2 + 4 * (sm["n_events"] + 1)
+    def e2e_leg(scan):
+        ec = pixgpu.Chain(det.es, max_events=B, max_words_per_batch=max_words, slots=a.slots, device=dev,
+                          fed_scan=scan)
+        ec.prepare(B)
+        h2d = [0]
+        d2h = [0]
+        fed_list = struct.unpack_from("<%dI" % struct.unpack_from("<I", det.es[4], 0)[0], det.es[4], 4)
+        n_scan = sum(1 for f in fed_list if f != 40 and f < 4096)  # FED table entries per event
 
-    e2e_sub = lambda i: e2e_chain.submit(host_batches[i % nbh])  # noqa: E731
-    pipeline(e2e_chain, torch, a.warmup, e2e_sub, lambda s: None)
-    t0 = time.perf_counter()
-    ems = pipeline(e2e_chain, torch, a.steps, e2e_sub, e2e_done)
-    wall = time.perf_counter() - t0
-    e2e_chain.close()
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ems], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ems = float(t.item())
-    out["e2e"] = {"value": world * events / (ems / 1e3), "unit": "events/s",
-                  "h2d_bytes_per_step": h2d[0] / a.steps, "d2h_bytes_per_step": d2h[0] / a.steps,
-                  "host_wall_events_per_s": events / wall,
-                  "path": "pg_submit: host FED scan + H2D of words + chain + results into mapped host memory"}
+        def e2e_done(slot):
+            sm = ec.summary(slot)
+            d2h[0] += sm["result_bytes"]
+            if scan == "host":  # words, one FED byte per word pair, offsets
+                h2d[0] += 4 * sm["n_digis"] + sm["n_digis"] // 2 + 4 * (sm["n_events"] + 1)
+
+        sub = lambda i: ec.submit(host_batches[i % nbh])  # noqa: E731
+        pipeline(ec, torch, a.warmup, sub, lambda s: None)
+        t0 = time.perf_counter()
+        ems = pipeline(ec, torch, a.steps, sub, e2e_done)
+        wall = time.perf_counter() - t0
+        ec.close()
+        if scan == "device":  # whole FED blocks (records less their directories) and the FED table
+            for i in range(a.steps):
+                batch = host_batches[i % nbh]
+                h2d[0] += sum(len(r) - 4 - 8 * struct.unpack_from("<I", r, 0)[0] for r in batch)
+                h2d[0] += 8 * n_scan * len(batch)
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        return {"value": world * events / (ems / 1e3), "unit": "events/s",
+                "h2d_bytes_per_step": h2d[0] / a.steps, "d2h_bytes_per_step": d2h[0] / a.steps,
+                "host_wall_events_per_s": events / wall,
+                "path": ("pg_submit: host FED scan + H2D of words" if scan == "host" else
+                         "pg_submit: H2D of whole FED blocks + device FED scan") +
+                        " + chain + results into mapped host memory"}
+
+    legs = {scan: e2e_leg(scan) for scan in ("host", "device")}
+    out["e2e"] = legs[pixgpu.default_config().get("fed_scan") and "device" or "host"]
+    out["e2e_by_fed_scan"] = {k: v["value"] for k, v in legs.items()}
 
     if rank == 0 and world == 1:
         # ------------------------------------------------------------ one event per launch (plain chain)

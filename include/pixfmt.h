@@ -149,6 +149,18 @@ typedef struct PfPixelError {
   uint8_t fedId;
 } PfPixelError;
 
+/* one entry of PixelFormatterErrors (DataFormats/PixelErrors.h:16), the
+   S-Link framing errors of the FED loop (ErrorChecker.cc:38-91): all under
+   the dummy detector id 0xffffffff, in FED-loop order.  SiPixelRawDataError
+   (DataFormats/SiPixelRawDataError.h:16-50) keeps the 64-bit header or
+   trailer word, the error type (32, 33, 34, 39) and the full FED id; its
+   message follows from the type (pg_error_message). */
+typedef struct PfFormatterError {
+  uint64_t word64;
+  uint32_t errorType;
+  uint32_t fedId;
+} PfFormatterError;
+
 #ifdef __cplusplus
 }
 #endif
@@ -161,6 +173,7 @@ static_assert(sizeof(PfAverageGeometry) == 3560, "AverageGeometry image size");
 static_assert(sizeof(PfLayerGeometry) == 160, "LayerGeometry image size");
 static_assert(sizeof(PfBeamSpot) == 44, "BeamSpotPOD image size");
 static_assert(sizeof(PfPixelError) == 12, "PixelErrorCompact image size");
+static_assert(sizeof(PfFormatterError) == 16, "formatter error record size");
 #endif
 
 #endif /* PIXFMT_H */

@@ -53,6 +53,31 @@ enum pg_status {
   PG_ERR_NOTFOUND = -7   /* unknown product name */
 };
 
+/* per-event flag bits (pg_event_counts.flags, the results' flags): conditions
+   where the reference's behaviour is undefined or its truncation order is not
+   reproduced exactly */
+enum pg_flag {
+  PG_FLAG_MODULE_TOO_BIG = 1u << 0,    /* > 4000 pixels in a module */
+  PG_FLAG_EDGE_OVERFLOW = 1u << 1,     /* more CA links than the edge capacity */
+  PG_FLAG_NBR_POOL_OVERFLOW = 1u << 2, /* more cells with neighbours than the list pool */
+  PG_FLAG_TRK_POOL_OVERFLOW = 1u << 3, /* more cells with tracks than the list pool */
+  PG_FLAG_FIT_BIN_OVERFLOW = 1u << 4,  /* > 24576 tuples of one multiplicity */
+  PG_FLAG_TUPLE_OVERFLOW = 1u << 5,    /* > 32768 tuples (the tail is dropped, as in the reference) */
+  PG_FLAG_CELL_OVERFLOW = 1u << 6,     /* doublet capacity reached (truncated as in the reference) */
+  PG_FLAG_HIT_OVERFLOW = 1u << 7,      /* > 49152 clusters (truncated as in the reference) */
+  PG_FLAG_ERR_OVERFLOW = 1u << 8,      /* more digi errors than kept */
+  PG_FLAG_TOO_MANY_WORDS = 1u << 9,    /* event larger than MAX_FED_WORDS */
+  PG_FLAG_H2T_OVERFLOW = 1u << 10,     /* hit-to-tuple capacity exceeded */
+  PG_FLAG_TM_OVERFLOW = 1u << 11,      /* tuple multiplicity capacity exceeded */
+  PG_FLAG_VTX_OVERFLOW = 1u << 12,     /* split vertex with >= 512 tracks or > 1024 vertices */
+  PG_FLAG_DEEP_TUPLE = 1u << 13,       /* a CA path longer than 5 hits (the reference aborts) */
+  PG_FLAG_J_OVERFLOW = 1u << 14,       /* more doublet inner-hit slots than kept */
+  PG_FLAG_BAD_INPUT = 1u << 15,        /* payload words outside the cabling tables (read as padding) */
+  /* bit 16 is the results' "more loose tracks than stored" */
+  PG_FLAG_SPLIT_MODULE = 1u << 17      /* a module's digis in several runs: the later runs are read as
+                                          padding (the reference's result is loop-order dependent) */
+};
+
 typedef struct pg_ctx pg_ctx;
 
 typedef struct pg_es_images {
@@ -84,6 +109,12 @@ typedef struct pg_config {
   uint32_t late_fishbone;                     /* 0; 1 adds the late fishbone and the fishbone cleaner */
   uint32_t ideal_conditions;                  /* 1 */
   uint32_t do_cluster_cut, do_z0_cut, do_pt_cut; /* 1, 1, 1 */
+  /* the FED loop's ErrorChecker (plugin-SiPixelClusterizer/ErrorChecker.cc:38-91) */
+  uint32_t formatter_errors;     /* 1: record its S-Link framing errors (types 32, 33, 34, 39) as the
+                                    "formatterErrors" product; 0 (default): as the reference, whose
+                                    ErrorChecker records none (ErrorChecker.cc:36) */
+  uint32_t fed_scan;             /* 0: the FED header/trailer checks and word concatenation on the host
+                                    (default); 1: on the device, from the whole FED buffers */
 } pg_config;
 
 typedef struct pg_event_counts {

@@ -40,6 +40,7 @@ struct Words {
   std::vector<uint32_t> word;
   std::vector<uint8_t> fedId;  // one per word pair, fedId - 1200
   uint32_t nWords = 0;
+  std::vector<PfFormatterError> formatterErrors;  // with includeErrors in the ErrorChecker
 };
 
 struct Digis {
@@ -109,8 +110,9 @@ struct Event {
   Vertices vtx;
 };
 
-// plugin-SiPixelClusterizer/SiPixelRawToClusterCUDA.cc:78-138 (FED loop, ErrorChecker, WordFedAppender)
-void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w);
+// plugin-SiPixelClusterizer/SiPixelRawToClusterCUDA.cc:78-138 (FED loop, ErrorChecker, WordFedAppender);
+// formatterErrors: the ErrorChecker's includeErrors (false in the reference's ErrorChecker.cc:36)
+void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w, bool formatterErrors = false);
 // SiPixelRawToClusterGPUKernel::makeClusters (SiPixelRawToClusterGPUKernel.cc:509-600)
 void makeClusters(const ES& es, const Words& w, Digis& d, Clusters& c);
 // PixelRecHitGPUKernel::makeHits (plugin-SiPixelRecHits/PixelRecHits.cc:33-53)
@@ -143,8 +145,12 @@ void riemannFit(int N, const double* hits /*3xN col-major*/, const float* hits_g
                 float* cov15, float* pt, float* eta, float* chi2);
 
 // whole chain for one raw.bin event record
-void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev, const CAParams& p = CAParams(),
-                  int vertexAlgo = 0);
+struct Options {
+  CAParams ca;
+  int vertexAlgo = 0;            // see makeVertices
+  bool formatterErrors = false;  // see fedLoop
+};
+void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev, const Options& o = Options());
 
 }  // namespace oracle
 

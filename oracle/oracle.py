@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 sys.path.insert(0, os.path.join(ROOT, "pixeltrack-standalone_b200"))
 import build as _build  # noqa: E402
-from pixgpu import ERROR_DTYPE, SCALARS, _TYPES  # noqa: E402
+from pixgpu import ERROR_DTYPE, FORMATTER_ERROR_DTYPE, SCALARS, _TYPES  # noqa: E402
 
 # the CA module's switches (CAHitNtupletGeneratorOnGPU.cc:46-58) with the
 # reference's defaults; the same names as the product's pg_config fields
@@ -30,7 +30,8 @@ def _ca_args(ca):
         p[k] = int(v)
     return [p[k] for k in CA_DEFAULTS]
 
-PRODUCTS = ["nDigis", "nModules", "xx", "yy", "adc", "moduleInd", "clus", "pdigi", "rawIdArr", "errors", "nClusters",
+PRODUCTS = ["nDigis", "nModules", "xx", "yy", "adc", "moduleInd", "clus", "pdigi", "rawIdArr", "errors",
+            "formatterErrors", "nClusters",
             "moduleStart", "clusInModule", "moduleId", "clusModuleStart", "nHits", "xl", "yl", "xerr", "yerr", "xg",
             "yg", "zg", "rg", "charge", "iphi", "xsize", "ysize", "detInd", "hitsLayerStart", "phiOff", "phiBins",
             "nCells", "cellInner", "cellOuter", "cellLayerPair", "cellDoubletId", "cellUsed", "cellNbrOff",
@@ -42,6 +43,8 @@ PRODUCTS = ["nDigis", "nModules", "xx", "yy", "adc", "moduleInd", "clus", "pdigi
 def _decode(buf, name, elem):
     if name == "errors":
         return np.frombuffer(buf, dtype=ERROR_DTYPE).copy()
+    if name == "formatterErrors":
+        return np.frombuffer(buf, dtype=FORMATTER_ERROR_DTYPE).copy()
     if name in SCALARS:
         return int(np.frombuffer(buf, dtype=np.uint32)[0])
     dt = _TYPES.get(name)
@@ -68,7 +71,7 @@ class _Named:
 class Oracle(_Named):
     """Sequential restatement of the serial chain (oracle/*.cc)."""
 
-    def __init__(self, es_images, riemann_fit=False, vertex_algo=0, ca=None):
+    def __init__(self, es_images, riemann_fit=False, vertex_algo=0, ca=None, formatter_errors=False):
         path = os.path.join(HERE, "liboracle.so")
         if not os.path.exists(path):
             _build.build_oracle()
@@ -104,6 +107,8 @@ class Oracle(_Named):
         self.lib.or_set_ca_params.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 8
         if self.lib.or_set_ca_params(self._h, *_ca_args(ca)) != 0:
             raise ValueError("min_hits_per_ntuplet: 3 or 4")
+        self.lib.or_set_formatter_errors.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        self.lib.or_set_formatter_errors(self._h, 1 if formatter_errors else 0)
 
     def process(self, raw, names=None):
         if self.lib.or_process(self._h, raw, len(raw)) != 0:
@@ -174,7 +179,7 @@ def ref_available():
 class Reference(_Named):
     """The reference's own serial chain, compiled from its sources (checker build)."""
 
-    def __init__(self, datadir, riemann_fit=False, vertex_algo=0, ca=None):
+    def __init__(self, datadir, riemann_fit=False, vertex_algo=0, ca=None, formatter_errors=False):
         self.lib = ctypes.CDLL(REF_LIB)
         self.lib.pr_create.restype = ctypes.c_void_p
         self.lib.pr_create.argtypes = [ctypes.c_char_p]
@@ -190,6 +195,8 @@ class Reference(_Named):
         self.lib.pr_set_vertex_algo.argtypes = [ctypes.c_void_p, ctypes.c_int]
         if self.lib.pr_set_vertex_algo(self._h, int(vertex_algo)) != 0:
             raise ValueError("vertex_algo: 0 density, 1 DBSCAN, 2 iterative")
+        self.lib.pr_set_formatter_errors.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        self.lib.pr_set_formatter_errors(self._h, 1 if formatter_errors else 0)
         if ca:
             self.lib.pr_set_ca_params.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 8
             if self.lib.pr_set_ca_params(self._h, *_ca_args(ca)) != 0:

@@ -25,8 +25,7 @@ struct Handle {
   oracle::Event ev;
   std::map<std::string, Blob> out;
   double lastSeconds = 0;
-  oracle::CAParams ca;
-  int vertexAlgo = 0;
+  oracle::Options opts;
   std::string error;
 
   template <typename T>
@@ -60,6 +59,7 @@ void record(Handle& h) {
   h.put("pdigi", d.pdigi.data(), d.nDigis);
   h.put("rawIdArr", d.rawIdArr.data(), d.nDigis);
   h.put("errors", d.errors.data(), d.errors.size());
+  h.put("formatterErrors", h.ev.words.formatterErrors.data(), h.ev.words.formatterErrors.size());
   h.put1<uint32_t>("nClusters", c.nClusters);
   h.put("moduleStart", c.moduleStart.data(), c.moduleStart.size());
   h.put("clusInModule", c.clusInModule.data(), c.clusInModule.size());
@@ -142,12 +142,12 @@ void record(Handle& h) {
 }  // namespace
 
 namespace oracle {
-void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev, const CAParams& p, int vertexAlgo) {
-  fedLoop(es, raw, n, ev.words);
+void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev, const Options& o) {
+  fedLoop(es, raw, n, ev.words, o.formatterErrors);
   makeClusters(es, ev.words, ev.digis, ev.clusters);
   makeHits(es, ev.digis, ev.clusters, ev.hits);
-  makeTuples(es, ev.hits, ev.ca, p);
-  makeVertices(ev.ca, ev.vtx, vertexAlgo);
+  makeTuples(es, ev.hits, ev.ca, o.ca);
+  makeVertices(ev.ca, ev.vtx, o.vertexAlgo);
 }
 }  // namespace oracle
 
@@ -170,14 +170,14 @@ void* or_create(const uint8_t* cabling, size_t ncab, const uint8_t* gain, size_t
 void or_destroy(void* p) { delete static_cast<Handle*>(p); }
 
 // useRiemannFit of the CA module configuration (off by default, as in the reference)
-void or_set_riemann(void* p, int on) { static_cast<Handle*>(p)->ca.useRiemannFit = on != 0; }
+void or_set_riemann(void* p, int on) { static_cast<Handle*>(p)->opts.ca.useRiemannFit = on != 0; }
 
 // the CA module's switches (CAHitNtupletGeneratorOnGPU.cc:46-58); -1 when
 // minHitsPerNtuplet is outside 3..4
 int or_set_ca_params(void* p, int minHitsPerNtuplet, int includeJumpingForwardDoublets, int earlyFishbone,
                      int lateFishbone, int idealConditions, int doClusterCut, int doZ0Cut, int doPtCut) {
   if (minHitsPerNtuplet < 3 || minHitsPerNtuplet > 4) return -1;
-  auto& c = static_cast<Handle*>(p)->ca;
+  auto& c = static_cast<Handle*>(p)->opts.ca;
   c.minHitsPerNtuplet = uint32_t(minHitsPerNtuplet);
   c.includeJumpingForwardDoublets = includeJumpingForwardDoublets != 0;
   c.earlyFishbone = earlyFishbone != 0;
@@ -192,16 +192,20 @@ int or_set_ca_params(void* p, int minHitsPerNtuplet, int includeJumpingForwardDo
 // vertex clustering of PixelVertexProducerCUDA: 0 density (default), 1 DBSCAN, 2 iterative
 int or_set_vertex_algo(void* p, int algo) {
   if (algo < 0 || algo > 2) return -1;
-  static_cast<Handle*>(p)->vertexAlgo = algo;
+  static_cast<Handle*>(p)->opts.vertexAlgo = algo;
   return 0;
 }
+
+// the ErrorChecker's includeErrors: record the FED loop's framing errors
+// (off in the reference, ErrorChecker.cc:36)
+void or_set_formatter_errors(void* p, int on) { static_cast<Handle*>(p)->opts.formatterErrors = on != 0; }
 
 // Runs the chain on one raw.bin event record; 0 on success.
 int or_process(void* p, const uint8_t* raw, size_t n) {
   Handle& h = *static_cast<Handle*>(p);
   try {
     auto t0 = std::chrono::steady_clock::now();
-    oracle::processEvent(h.es, raw, n, h.ev, h.ca, h.vertexAlgo);
+    oracle::processEvent(h.es, raw, n, h.ev, h.opts);
     auto t1 = std::chrono::steady_clock::now();
     h.lastSeconds = std::chrono::duration<double>(t1 - t0).count();
     record(h);
@@ -243,7 +247,7 @@ double or_time_events(void* p, const uint8_t* const* raws, const size_t* sizes, 
         if (k >= n) break;
         auto a = std::chrono::steady_clock::now();
         try {
-          oracle::processEvent(h.es, raws[k], sizes[k], ev, h.ca, h.vertexAlgo);
+          oracle::processEvent(h.es, raws[k], sizes[k], ev, h.opts);
         } catch (std::exception&) {
           failed++;
         }

@@ -44,6 +44,8 @@ inline uint32_t cablingIndex(uint32_t fed, uint32_t link, uint32_t roc) {
 // :59-67
 DetIdGPU getRawId(const PfCablingMap& cab, uint8_t fed, uint32_t link, uint32_t roc) {
   uint32_t index = cablingIndex(fed, link, roc);
+  if (link == 0 || index >= uint32_t(PF_MAX_SIZE))
+    throw std::runtime_error("undefined in the reference: a word outside the cabling tables");
   return {cab.rawId[index], cab.rocInDet[index], cab.moduleId[index]};
 }
 
@@ -269,8 +271,10 @@ void loadES(ES& es, const uint8_t* cabling, size_t ncab, const uint8_t* gain, si
   }
 }
 
-// SiPixelRawToClusterCUDA.cc:78-138 with ErrorChecker.cc:36-91 (includeErrors=false in the checker)
-void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w) {
+// SiPixelRawToClusterCUDA.cc:78-138 with ErrorChecker.cc:36-91.  The
+// reference's ErrorChecker records no errors (includeErrors = false in its
+// constructor, :36); formatterErrors turns that recording on.
+void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w, bool formatterErrors) {
   // Source.cc:9-21 record layout
   std::vector<std::pair<const uint8_t*, uint32_t>> fedData(4096, {nullptr, 0});
   size_t off = 0;
@@ -291,6 +295,10 @@ void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w) {
   }
   w.word.assign(PF_MAX_FED_WORDS, 0);
   w.fedId.assign(PF_MAX_FED_WORDS, 0);
+  w.formatterErrors.clear();
+  auto record = [&](uint64_t word64, uint32_t type, uint32_t fedId) {
+    if (formatterErrors) w.formatterErrors.push_back({word64, type, fedId});
+  };
   uint32_t wordCounter = 0;
   for (uint32_t fedId : es.fedIds) {
     if (fedId == 40) continue;
@@ -303,35 +311,50 @@ void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w) {
       std::memcpy(&v, data + 8 * size_t(k), 8);
       return v;
     };
-    // CRC bit (FED_CRC_MODIFIED) of the last word
-    if ((word64(nWords - 1) >> 2) & 1) continue;
-    // headers: FEDHeader::check / moreHeaders
+    // checkCRC (:38-48): the CRC-modified bit of the last word drops the FED
+    if ((word64(nWords - 1) >> 2) & 1) {
+      record(word64(nWords - 1), 39, fedId);
+      continue;
+    }
+    // checkHeader (:50-65): FEDHeader::check (start marker 0x5), sourceID,
+    // moreHeaders; a word that fails the check ends the headers unrecorded
     int h = -1;
     bool more = true;
     while (more) {
       ++h;
+      if (h >= nWords) throw std::runtime_error("undefined in the reference: headers run past the FED");
       uint64_t v = word64(h);
       uint32_t sourceid = uint32_t(v), eventid = uint32_t(v >> 32);
-      if (((eventid >> 28) & 0xf) != 0x5)
+      if (((eventid >> 28) & 0xf) != 0x5) {
         more = false;
-      else
+      } else {
+        if (((sourceid >> 8) & 0xfff) != fedId) record(v, 32, fedId);
         more = ((sourceid >> 3) & 1) != 0;
+      }
     }
-    // trailers: FEDTrailer::check / moreTrailers
+    // checkTrailer (:67-91): FEDTrailer::check (end marker 0xa),
+    // fragmentLength against the FED's 64-bit word count, moreTrailers
     int t = nWords;
     more = true;
     while (more) {
       --t;
+      if (t < 0) throw std::runtime_error("undefined in the reference: trailers run past the FED");
       uint64_t v = word64(t);
       uint32_t conscheck = uint32_t(v), eventsize = uint32_t(v >> 32);
-      if (((eventsize >> 28) & 0xf) != 0xa)
+      if (((eventsize >> 28) & 0xf) != 0xa) {
+        record(v, 33, fedId);
         more = false;
-      else
+      } else {
+        if ((eventsize & 0x00ffffffu) != uint32_t(nWords)) record(v, 34, fedId);
         more = ((conscheck >> 3) & 1) != 0;
+      }
     }
+    if (t < h + 1) throw std::runtime_error("undefined in the reference: header and trailer overlap");
     const uint8_t* bw = data + 8 * size_t(h + 1);
     const uint8_t* ew = data + 8 * size_t(t);
     uint32_t length = uint32_t((ew - bw) / 4);
+    if (wordCounter + length > PF_MAX_FED_WORDS)
+      throw std::runtime_error("undefined in the reference: more than MAX_FED_WORDS words");
     // WordFedAppender::initializeWordFed (SiPixelRawToClusterGPUKernel.cc:41-47)
     std::memcpy(w.word.data() + wordCounter, bw, 4 * size_t(length));
     std::memset(w.fedId.data() + wordCounter / 2, int(fedId - 1200), length / 2);
@@ -461,6 +484,16 @@ void makeClusters(const ES& es, const Words& w, Digis& d, Clusters& c) {
     }
   }
   d.nModules = ms[0];
+  // a module in two runs: findClus and the rechits then overwrite its cluster
+  // count and hit slots in loop order (and race in the reference's CUDA build)
+  {
+    std::vector<uint8_t> seen(PF_MAX_MODULES, 0);
+    for (uint32_t module = 0; module < ms[0]; ++module) {
+      uint16_t id = d.moduleInd[ms[1 + module]];
+      if (id < PF_MAX_MODULES && seen[id]++)
+        throw std::runtime_error("undefined in the reference: a module's digis in two separate runs");
+    }
+  }
 
   // ---- findClus (gpuClustering.h:40-273): connected components (|dx|<=1, |dy|<=1)
   // labelled by the lowest pixel index, numbered in ascending order of that index

@@ -50,6 +50,8 @@
 #include "plugin-PixelTriplets/CAHitNtupletGeneratorOnGPU.h"
 #include "plugin-PixelTriplets/CAHitNtupletGeneratorKernels.h"
 #include "plugin-PixelTriplets/GPUCACell.h"
+// and the ErrorChecker's includeErrors switch
+#include "plugin-SiPixelClusterizer/ErrorChecker.h"
 #undef private
 #undef protected
 
@@ -69,7 +71,6 @@
 #include "DataFormats/FEDRawDataCollection.h"
 #include "DataFormats/PixelErrors.h"
 #include "Framework/ProductRegistry.h"
-#include "plugin-SiPixelClusterizer/ErrorChecker.h"
 #include "plugin-SiPixelClusterizer/SiPixelRawToClusterGPUKernel.h"
 #include "plugin-SiPixelRecHits/PixelRecHits.h"
 #include "plugin-PixelVertexFinding/gpuVertexFinder.h"
@@ -98,6 +99,8 @@ struct RefChain {
   // reference's own configuration fixes it to false
   // (CAHitNtupletGeneratorOnGPU.cc:49)
   bool useRiemannFit = false;
+  // the ErrorChecker's includeErrors (false in ErrorChecker.cc:36)
+  bool formatterErrors = false;
   // the CA module's switches when set through pr_set_ca_params; otherwise
   // the reference's own configuration (caGen->m_params)
   std::unique_ptr<cAHitNtupletGenerator::Params> caParams;
@@ -213,6 +216,7 @@ int pr_process(void* p, const uint8_t* raw, size_t nraw, int dump) {
   unsigned int wordCounterGPU = 0, fedCounter = 0;
   bool errorsInEvent = false;
   ErrorChecker errorcheck;
+  errorcheck.includeErrors = h.formatterErrors;
   for (int fedId : h.fedIds) {
     if (fedId == 40) continue;
     assert(fedId >= 1200);
@@ -295,6 +299,16 @@ int pr_process(void* p, const uint8_t* raw, size_t nraw, int dump) {
     auto const* ev = digiErrors.error();
     int ne = ev ? ev->size() : 0;
     h.put("errors", ev ? ev->data() : (const PixelErrorCompact*)nullptr, size_t(ne));
+    // PixelFormatterErrors, flattened in map order (the product's 16-byte records)
+    struct FormatterErrorRecord {
+      uint64_t word64;
+      uint32_t errorType, fedId;
+    };
+    std::vector<FormatterErrorRecord> fe;
+    for (auto const& kv : digiErrors.formatterErrors())
+      for (auto const& er : kv.second)
+        fe.push_back({er.getWord64(), uint32_t(er.getType()), uint32_t(er.getFedId())});
+    h.put("formatterErrors", fe.data(), fe.size());
   }
   h.put1<uint32_t>("nClusters", clusters.nClusters());
   h.put("moduleStart", clusters.moduleStart(), gpuClustering::MaxNumModules + 1);
@@ -458,6 +472,8 @@ int pr_names(void* p, char* buf, size_t n) {
 // Seconds spent in the chain (excluding input parsing and product recording)
 // during the last pr_process call.
 double pr_last_seconds(void* p) { return static_cast<RefChain*>(p)->lastSeconds; }
+
+void pr_set_formatter_errors(void* p, int on) { static_cast<RefChain*>(p)->formatterErrors = on != 0; }
 
 void pr_set_riemann(void* p, int on) { static_cast<RefChain*>(p)->useRiemannFit = on != 0; }
 

@@ -55,11 +55,12 @@ struct Rd {
 
 // FED scan: Source record -> (words, fed index per word pair); follows
 // SiPixelRawToClusterCUDA.cc:78-138 with ErrorChecker.cc:36-91 semantics.
-int pixgpu::unpackRaw(const std::vector<uint32_t>& fedIds, const uint8_t* raw, size_t n, uint32_t* words, uint8_t* fed,
-              uint32_t cap, uint32_t* nWordsOut) {
-  const uint8_t* fedPtr[4096];
-  uint32_t fedSize[4096];
-  std::memset(fedSize, 0, sizeof(fedSize));
+namespace {
+
+// the record's FED directory (Source.cc:9-21): data pointer and byte size of
+// each FED id; PG_ERR_FORMAT for a truncated record or an id >= 4096
+int fedDirectory(const uint8_t* raw, size_t n, const uint8_t** fedPtr, uint32_t* fedSize) {
+  std::memset(fedSize, 0, 4096 * sizeof(uint32_t));
   Rd r{raw, n};
   uint32_t nfeds = r.get<uint32_t>();
   if (!r.ok) return PG_ERR_FORMAT;
@@ -70,6 +71,16 @@ int pixgpu::unpackRaw(const std::vector<uint32_t>& fedIds, const uint8_t* raw, s
     fedSize[id] = size;
     r.off += size;
   }
+  return PG_OK;
+}
+
+}  // namespace
+
+int pixgpu::unpackRaw(const std::vector<uint32_t>& fedIds, const uint8_t* raw, size_t n, uint32_t* words, uint8_t* fed,
+              uint32_t cap, uint32_t* nWordsOut, std::vector<PfFormatterError>* fmt) {
+  const uint8_t* fedPtr[4096];
+  uint32_t fedSize[4096];
+  if (fedDirectory(raw, n, fedPtr, fedSize) != PG_OK) return PG_ERR_FORMAT;
   uint32_t wc = 0;
   for (uint32_t fedId : fedIds) {
     if (fedId == 40 || fedId >= 4096) continue;
@@ -82,22 +93,40 @@ int pixgpu::unpackRaw(const std::vector<uint32_t>& fedIds, const uint8_t* raw, s
       std::memcpy(&v, d + 8 * size_t(k), 8);
       return v;
     };
-    if ((w64(n64 - 1) >> 2) & 1) continue;  // CRC-modified bit
+    auto record = [&](uint64_t v, uint32_t type) {
+      if (fmt) fmt->push_back(PfFormatterError{v, type, fedId});
+    };
+    // checkCRC: the CRC-modified bit of the last word drops the FED
+    if ((w64(n64 - 1) >> 2) & 1) {
+      record(w64(n64 - 1), 39);
+      continue;
+    }
+    // checkHeader: start marker 0x5 (else the headers end, unrecorded),
+    // source id, more-headers bit; bounded by the FED (the reference is not)
     int h = -1;
     bool more = true;
     while (more && h + 1 < n64) {
       ++h;
       uint64_t v = w64(h);
-      more = (((uint32_t(v >> 32)) >> 28) & 0xf) == 0x5 && ((uint32_t(v) >> 3) & 1);
+      if (((uint32_t(v >> 32) >> 28) & 0xf) != 0x5) break;
+      if (((uint32_t(v) >> 8) & 0xfff) != fedId) record(v, 32);
+      more = (uint32_t(v) >> 3) & 1;
     }
+    // checkTrailer: end marker 0xa (else type 33 and the trailers end),
+    // fragment length against the FED's 64-bit words (type 34), more-trailers bit
     int t = n64;
     more = true;
     while (more && t > 0) {
       --t;
       uint64_t v = w64(t);
-      more = (((uint32_t(v >> 32)) >> 28) & 0xf) == 0xa && ((uint32_t(v) >> 3) & 1);
+      if (((uint32_t(v >> 32) >> 28) & 0xf) != 0xa) {
+        record(v, 33);
+        break;
+      }
+      if ((uint32_t(v >> 32) & 0x00ffffffu) != uint32_t(n64)) record(v, 34);
+      more = (uint32_t(v) >> 3) & 1;
     }
-    if (t < h + 1) continue;
+    if (t < h + 1) continue;  // header and trailer overlap (undefined in the reference): no payload
     uint32_t len = uint32_t(t - (h + 1)) * 2;
     if (wc + len > cap) return PG_ERR_CAPACITY;
     std::memcpy(words + wc, d + 8 * size_t(h + 1), 4 * size_t(len));
@@ -111,8 +140,7 @@ int pixgpu::unpackRaw(const std::vector<uint32_t>& fedIds, const uint8_t* raw, s
 namespace {
 
 int uploadES(pg_ctx* c, const pg_es_images* es) {
-  Rd cab{es->cabling, es->cabling_size}, gain{es->gain, es->gain_size}, cpe{es->cpe, es->cpe_size},
-      bs{es->beamspot, es->beamspot_size}, fi{es->fedids, es->fedids_size};
+  Rd cpe{es->cpe, es->cpe_size}, bs{es->beamspot, es->beamspot_size}, fi{es->fedids, es->fedids_size};
   // sizes
   if (es->cabling_size < sizeof(PfCablingMap) + 4) return fail(c, PG_ERR_FORMAT, "cabling image too short");
   uint32_t nUnp;
@@ -144,6 +172,9 @@ int uploadES(pg_ctx* c, const pg_es_images* es) {
   c->hes.fedIds.resize(nf);
   fi.bytes(c->hes.fedIds.data(), nf * 4);
   if (!fi.ok) return fail(c, PG_ERR_FORMAT, "fedIds image truncated");
+  c->hes.scanFeds.clear();
+  for (uint32_t id : c->hes.fedIds)
+    if (id != 40 && id < 4096) c->hes.scanFeds.push_back(id);
   // one device allocation for the resident conditions
   size_t off = 0;
   auto place = [&](size_t bytes) {
@@ -189,15 +220,63 @@ int uploadES(pg_ctx* c, const pg_es_images* es) {
   return PG_OK;
 }
 
+// Device FED scan: copies every FED block of the ES list, header to trailer,
+// to the pinned raw buffer and writes the per-event FED table; the payload
+// words are bounded by two per 64-bit word between one header and one trailer
+// (the exact count for well-formed FEDs), which must fit the event and batch
+// capacities.
+int stageRawBlocks(pg_ctx* c, Slot& s, uint32_t nEvents, const uint8_t* const* raws, const size_t* sizes) {
+  const FedScanBuffers& fs = s.ws.scan;
+  const uint32_t F = fs.nFeds;
+  const uint32_t* ids = c->hes.scanFeds.data();
+  const uint8_t* fedPtr[4096];
+  uint32_t fedSize[4096];
+  uint64_t cursor = 0, batchBound = 0;
+  for (uint32_t k = 0; k < nEvents; ++k) {
+    if (fedDirectory(raws[k], sizes[k], fedPtr, fedSize) != PG_OK) return fail(c, PG_ERR_FORMAT, "malformed raw record");
+    uint64_t bound = 0;
+    uint2* tab = s.hTab + size_t(k) * F;
+    for (uint32_t j = 0; j < F; ++j) {
+      const uint32_t n64 = fedSize[ids[j]] / 8;
+      if (cursor + n64 > fs.rawCap64) return fail(c, PG_ERR_CAPACITY, "raw records larger than the staging buffer");
+      tab[j] = make_uint2(uint32_t(cursor), n64);
+      if (n64) std::memcpy(s.hRaw + cursor, fedPtr[ids[j]], size_t(n64) * 8);
+      cursor += n64;
+      bound += n64 >= 2 ? 2 * uint64_t(n64 - 2) : 0;
+    }
+    if (bound > kMaxFedWords) return fail(c, PG_ERR_CAPACITY, "event or batch too large");
+    batchBound += bound;
+  }
+  if (batchBound > c->cfg.max_words_per_batch) return fail(c, PG_ERR_CAPACITY, "event or batch too large");
+  cudaError_t e;
+  if (cursor && (e = cudaMemcpyAsync(fs.raw64, s.hRaw, size_t(cursor) * 8, cudaMemcpyHostToDevice, s.stream)) !=
+                    cudaSuccess)
+    return cudaFail(c, e, "H2D FED blocks");
+  if ((e = cudaMemcpyAsync(fs.tab, s.hTab, size_t(nEvents) * F * sizeof(uint2), cudaMemcpyHostToDevice,
+                           s.stream)) != cudaSuccess)
+    return cudaFail(c, e, "H2D FED table");
+  s.fmtErrors.clear();
+  s.fmtOff.clear();
+  s.nEvents = nEvents;
+  s.staged = true;
+  return PG_OK;
+}
+
 int stage(pg_ctx* c, Slot& s, uint32_t nEvents, const uint8_t* const* raws, const size_t* sizes) {
   if (nEvents == 0 || nEvents > c->cfg.max_events) return fail(c, PG_ERR_CAPACITY, "batch size");
+  if (s.ws.scan.on) return stageRawBlocks(c, s, nEvents, raws, sizes);
   uint32_t off = 0;
+  const bool fmt = c->cfg.formatter_errors != 0;
+  s.fmtErrors.clear();
+  s.fmtOff.assign(1, 0);
   for (uint32_t k = 0; k < nEvents; ++k) {
     s.hOffsets[k] = off;
     uint32_t nw = 0;
     uint32_t room = c->cfg.max_words_per_batch - off;
     room = room > kMaxFedWords ? kMaxFedWords : room;
-    int rc = unpackRaw(c->hes.fedIds, raws[k], sizes[k], s.hWords + off, s.hFed + off / 2, room, &nw);
+    int rc = unpackRaw(c->hes.fedIds, raws[k], sizes[k], s.hWords + off, s.hFed + off / 2, room, &nw,
+                       fmt ? &s.fmtErrors : nullptr);
+    s.fmtOff.push_back(uint32_t(s.fmtErrors.size()));
     if (rc != PG_OK) return fail(c, rc, rc == PG_ERR_CAPACITY ? "event or batch too large" : "malformed raw record");
     off += nw;
   }
@@ -319,6 +398,8 @@ void pg_default_config(pg_config* cfg) {
   cfg->do_cluster_cut = 1;
   cfg->do_z0_cut = 1;
   cfg->do_pt_cut = 1;
+  cfg->formatter_errors = 0;
+  cfg->fed_scan = 0;
 }
 
 namespace {
@@ -347,6 +428,43 @@ int createSlot(pg_ctx* c, Slot& s, size_t bytes) {
       cudaHostAlloc(&s.hRes, size_t(E) * kResultStride, cudaHostAllocMapped) != cudaSuccess ||
       cudaHostGetDevicePointer(reinterpret_cast<void**>(&s.dRes), s.hRes, 0) != cudaSuccess)
     return fail(c, PG_ERR_NOMEM, "slot stream, events or pinned buffers");
+  if (c->cfg.fed_scan) {
+    // device FED scan buffers (fedscan.cu)
+    FedScanBuffers& fs = s.ws.scan;
+    const uint32_t F = uint32_t(c->hes.scanFeds.size());
+    fs.on = 1;
+    fs.recordErrors = c->cfg.formatter_errors != 0;
+    fs.nFeds = F;
+    // payload plus up to four framing words per FED
+    fs.rawCap64 = c->cfg.max_words_per_batch / 2 + 4 * E * F + 16;
+    const size_t EF = size_t(E) * F;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+      size_t o = off;
+      off = (off + bytes + 255) & ~size_t(255);
+      return o;
+    };
+    const size_t oIds = take(F * 4), oRaw = take(size_t(fs.rawCap64) * 8), oTab = take(EF * sizeof(uint2)),
+                 oLen = take(EF * 4), oSrc = take(EF * 4), oDst = take(EF * 4), oEv = take(size_t(E) * 4),
+                 oFmt = take(size_t(E) * kFmtErrCap * sizeof(PfFormatterError)), oCnt = take(size_t(E) * 4);
+    if (cudaMalloc(&s.dScan, off) != cudaSuccess ||
+        cudaMallocHost(&s.hRaw, size_t(fs.rawCap64) * 8) != cudaSuccess ||
+        cudaMallocHost(&s.hTab, EF * sizeof(uint2) + 8) != cudaSuccess)
+      return fail(c, PG_ERR_NOMEM, "FED scan buffers");
+    char* b = static_cast<char*>(s.dScan);
+    fs.fedIds = reinterpret_cast<const uint32_t*>(b + oIds);
+    fs.raw64 = reinterpret_cast<uint64_t*>(b + oRaw);
+    fs.tab = reinterpret_cast<uint2*>(b + oTab);
+    fs.len = reinterpret_cast<uint32_t*>(b + oLen);
+    fs.src = reinterpret_cast<uint32_t*>(b + oSrc);
+    fs.dst = reinterpret_cast<uint32_t*>(b + oDst);
+    fs.evWords = reinterpret_cast<uint32_t*>(b + oEv);
+    fs.fmt = reinterpret_cast<PfFormatterError*>(b + oFmt);
+    fs.fmtCount = reinterpret_cast<uint32_t*>(b + oCnt);
+    if (F && cudaMemcpyAsync(b + oIds, c->hes.scanFeds.data(), F * 4, cudaMemcpyHostToDevice, s.stream) !=
+                 cudaSuccess)
+      return fail(c, PG_ERR_CUDA, "FED id list");
+  }
   // the kernels read the batch input through this descriptor
   launchSetInput(s.ws, s.ws.words, s.ws.fedIds, s.stream);
   cudaError_t e = cudaStreamSynchronize(s.stream);
@@ -365,6 +483,9 @@ void destroySlot(Slot& s) {
     s.probe = nullptr;
   }
   if (s.dmem) cudaFree(s.dmem);
+  if (s.dScan) cudaFree(s.dScan);
+  if (s.hRaw) cudaFreeHost(s.hRaw);
+  if (s.hTab) cudaFreeHost(s.hTab);
   if (s.dRefs) cudaFree(s.dRefs);
   if (s.done) cudaEventDestroy(s.done);
   if (s.gathered) cudaEventDestroy(s.gathered);
@@ -387,7 +508,8 @@ int pg_create(const pg_es_images* es, const pg_config* cfgIn, pg_ctx** out) {
   else
     pg_default_config(&c->cfg);
   if (c->cfg.max_events == 0 || c->cfg.max_words_per_batch == 0 || c->cfg.max_words_per_batch > (1u << 30) ||
-      c->cfg.vertex_algo > 2 || c->cfg.min_hits_per_ntuplet < 3 || c->cfg.min_hits_per_ntuplet > 4)
+      c->cfg.vertex_algo > 2 || c->cfg.min_hits_per_ntuplet < 3 || c->cfg.min_hits_per_ntuplet > 4 ||
+      c->cfg.fed_scan > 1 || (c->cfg.fed_scan && c->cfg.pool_words))  // the pool stages on the host
     return PG_ERR_ARG;
   c->device = c->cfg.device;
   cudaError_t e = cudaSetDevice(c->cfg.device);
@@ -552,6 +674,23 @@ int pg_get_product(pg_ctx* c, uint32_t k, const char* name, void* dst, size_t ca
   if (n == "pdigi") return copyOut(c, s, ws.pdigi + w0, nw, dst, cap, count, elem);
   if (n == "rawIdArr") return copyOut(c, s, ws.rawIdArr + w0, nw, dst, cap, count, elem);
   if (n == "errors") return copyOut(c, s, ws.errors + size_t(k) * kErrCap, std::min<size_t>(ec.nErrors, kErrCap), dst, cap, count, elem);
+  if (n == "formatterErrors" && ws.scan.on) {
+    uint32_t cnt = 0;
+    e = cudaMemcpy(&cnt, ws.scan.fmtCount + k, 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cudaFail(c, e, "D2H formatter error count");
+    return copyOut(c, s, ws.scan.fmt + size_t(k) * kFmtErrCap, std::min<size_t>(cnt, kFmtErrCap), dst, cap, count,
+                   elem);
+  }
+  if (n == "formatterErrors") {
+    *elem = int(sizeof(PfFormatterError));
+    const bool have = k + 1 < s.fmtOff.size();
+    const size_t b = have ? s.fmtOff[k] : 0, m = have ? s.fmtOff[k + 1] - s.fmtOff[k] : 0;
+    *count = m;
+    if (!dst || m == 0) return PG_OK;
+    if (m * sizeof(PfFormatterError) > cap) return fail(c, PG_ERR_CAPACITY, "product larger than the destination");
+    std::memcpy(dst, s.fmtErrors.data() + b, m * sizeof(PfFormatterError));
+    return PG_OK;
+  }
   if (n == "moduleStart") return copyOut(c, s, ws.moduleStart + mb, kMaxModules + 1, dst, cap, count, elem);
   if (n == "clusInModule") return copyOut(c, s, ws.clusInModule + mb, kMaxModules, dst, cap, count, elem);
   if (n == "moduleId") return copyOut(c, s, ws.moduleId + mb, kMaxModules, dst, cap, count, elem);

@@ -159,6 +159,7 @@ void workspaceCarve(Workspace& ws, void* base, uint32_t maxEvents, uint32_t word
 cudaError_t runChain(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream, bool riemann,
                      int vertexAlgo) {
   cudaError_t err;
+  if (ws.scan.on) launchFedScan(ws, nEvents, stream);
   if ((err = runLocal(es, ws, nEvents, stream)) != cudaSuccess) return err;
   if ((err = runCA(es, ws, nEvents, stream)) != cudaSuccess) return err;
   if ((err = runFits(es, ws, nEvents, stream, riemann)) != cudaSuccess) return err;

@@ -992,7 +992,6 @@ __global__ void kFastDupInDegree(Workspace ws, uint32_t* indeg, const uint32_t* 
   const uint32_t* cand = ws.candidates + size_t(e) * kCellCap;
   const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
   const uint16_t* trk = ws.trk + size_t(e) * kTupleCellCap;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
   const uint32_t* tcell = ws.tupleCells + size_t(e) * kTupleCellCap;
   const uint32_t* flag = candFlag + size_t(e) * (kCellCap + 1);
   uint32_t* deg = indeg + size_t(e) * kCellCap;
@@ -1033,7 +1032,6 @@ __global__ void __launch_bounds__(kFastDupThreads)
   const uint32_t* cand = ws.candidates + size_t(e) * kCellCap;
   const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
   const uint16_t* trk = ws.trk + size_t(e) * kTupleCellCap;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
   const uint32_t* tcell = ws.tupleCells + size_t(e) * kTupleCellCap;
   const uint32_t* flag = candFlag + size_t(e) * (kCellCap + 1);
   const uint32_t* cidx = candOff + size_t(e) * (kCellCap + 1);
@@ -1162,12 +1160,6 @@ __global__ void kTripletCleaner(Workspace ws) {
       if (q[t] != kBad && t != im) q[t] = kDup;
     }
   }
-}
-
-__global__ void kCopyCount(uint32_t* dst, uint32_t dstStride, const uint32_t* src, uint32_t srcStride,
-                           uint32_t nEvents) {
-  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e < nEvents) dst[size_t(e) * dstStride] = src[size_t(e) * srcStride];
 }
 
 // kernel_fishboneCleaner (CAHitNtupletGeneratorKernelsImpl.h:104-116): the

@@ -377,13 +377,76 @@ __global__ void kSortModules(Workspace ws, uint32_t nEvents) {
       __syncthreads();
     }
   }
-  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) ms[1 + i] = s[i];
-  if (threadIdx.x == 0) {
-    ms[0] = n;
-    if (c->nModules > kMaxModules) {
-      c->nModules = kMaxModules;
-      c->flags |= kFlagModuleTooBig;
+  // A module whose digis come in more than one run (only in corrupted data:
+  // a module is read out in one block per link) is clustered run by run by the
+  // reference, whose serial build then overwrites the module's cluster count
+  // and hit slots in loop order and whose CUDA build races on them.  Here the
+  // first run is kept and the later runs are read as padding (zero words);
+  // the event is flagged.
+  __shared__ uint32_t sFirst[kMaxModules];
+  __shared__ uint8_t sDrop[2048];
+  __shared__ uint32_t sNDrop;
+  const uint32_t start = ws.wordOffsets[e];
+  const uint16_t* mind = ws.moduleInd + start;
+  for (uint32_t i = threadIdx.x; i < kMaxModules; i += blockDim.x) sFirst[i] = 0xffffffffu;
+  if (threadIdx.x == 0) sNDrop = 0;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint16_t mid = mind[s[i]];
+    if (mid < kMaxModules) atomicMin(&sFirst[mid], i);
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint16_t mid = mind[s[i]];
+    const bool drop = mid < kMaxModules && sFirst[mid] != i;
+    sDrop[i] = drop ? 1 : 0;
+    if (drop) atomicAdd(&sNDrop, 1u);
+  }
+  __syncthreads();
+  if (sNDrop) {
+    const uint32_t nw = c->nWords;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+      if (!sDrop[i]) continue;
+      const uint16_t mid = mind[s[i]];
+      const uint32_t end = i + 1 < n ? s[i + 1] : nw;
+      for (uint32_t g = s[i]; g < end; ++g) {
+        const size_t w = size_t(start) + g;
+        if (ws.moduleInd[w] != mid) continue;
+        ws.moduleInd[w] = kInvId;
+        ws.xx[w] = ws.yy[w] = ws.adc[w] = 0;
+        ws.pdigi[w] = 0;
+        ws.rawIdArr[w] = 0;
+      }
     }
+    __syncthreads();
+    // drop the later runs from the list (their starts sort past the kept ones)
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+      if (sDrop[i]) s[i] = 0xffffffffu;
+    __syncthreads();
+    for (uint32_t k = 2; k <= 2048; k <<= 1) {
+      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+        for (uint32_t i = threadIdx.x; i < 2048; i += blockDim.x) {
+          uint32_t ixj = i ^ j;
+          if (ixj > i) {
+            bool up = (i & k) == 0;
+            uint32_t a = s[i], b = s[ixj];
+            if ((a > b) == up) {
+              s[i] = b;
+              s[ixj] = a;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+  }
+  const uint32_t kept = n - sNDrop;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) ms[1 + i] = i < kept ? s[i] : 0u;
+  if (threadIdx.x == 0) {
+    ms[0] = kept;
+    if (c->nModules > kMaxModules) c->flags |= kFlagModuleTooBig;
+    c->nModules = kept;
+    if (sNDrop) c->flags |= kFlagSplitModule;
   }
 }
 

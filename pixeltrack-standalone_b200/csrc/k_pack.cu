@@ -182,9 +182,8 @@ void launchSetInput(Workspace& ws, const uint32_t* words, const uint8_t* fedIds,
 
 void launchPack(Workspace& ws, uint32_t nEvents, uint8_t* out, cudaStream_t s) {
   const uint32_t P = nEvents <= kClusterMaxEvents ? kPackCtas : 1;
-  cudaError_t le = cudaSuccess;
-  PG_PROBED("kPackResults", s, le = launchClustered(kPackResults, P, nEvents, 512, 0, s, ws, out));
-  (void)le;  // a failed launch is reported by the stream's next error check
+  // a failed launch is reported by the stream's next error check
+  PG_PROBED("kPackResults", s, (void)launchClustered(kPackResults, P, nEvents, 512, 0, s, ws, out));
 }
 
 }  // namespace pixgpu

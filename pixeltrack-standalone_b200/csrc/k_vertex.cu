@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
   const uint32_t rank = cl.block_rank(), P = cl.num_blocks();
   extern __shared__ __align__(16) char vsm[];
   __shared__ uint32_t scanSh[33];
-  __shared__ uint32_t hoff[257], hcur[257];
+  __shared__ uint32_t hoff[257];
   __shared__ uint32_t vOff[kMaxVtx + 1], vCur[kMaxVtx + 1];
   __shared__ uint32_t sNt, sFound, sGuard, sNv;
   __shared__ int sFlag;
@@ -418,10 +418,7 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
 
   if (active) {
   // ---- clusterTracksByDensity: z histogram (256 bins of 1 mm)
-  for (uint32_t b = threadIdx.x; b < 257; b += blockDim.x) {
-    hoff[b] = 0;
-    hcur[b] = 0;
-  }
+  for (uint32_t b = threadIdx.x; b < 257; b += blockDim.x) hoff[b] = 0;
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
     int iz = int(double(s.zt[i]) * 10.);

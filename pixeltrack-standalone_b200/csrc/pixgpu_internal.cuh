@@ -7,6 +7,7 @@
 #include <stdint.h>
 
 #include "pixfmt.h"
+#include "pixgpu.h"
 
 namespace pixgpu {
 
@@ -46,8 +47,16 @@ enum : uint32_t {
   kFlagVtxOverflow = 1u << 12,      // split vertex with >= 512 tracks or > 1024 vertices
   kFlagDeepTuple = 1u << 13,        // a CA path longer than 5 hits (reference aborts)
   kFlagJOverflow = 1u << 14,        // more doublet inner-hit slots than kJCap
-  kFlagBadInput = 1u << 15          // words/cabling entries outside the tables (ignored)
+  kFlagBadInput = 1u << 15,         // words/cabling entries outside the tables (ignored)
+  kFlagSplitModule = 1u << 17       // a module's digis in several runs (later runs read as padding)
 };
+
+static_assert(uint32_t(kFlagBadInput) == uint32_t(PG_FLAG_BAD_INPUT) &&
+                  uint32_t(kFlagJOverflow) == uint32_t(PG_FLAG_J_OVERFLOW) &&
+                  uint32_t(kFlagTupleOverflow) == uint32_t(PG_FLAG_TUPLE_OVERFLOW) &&
+                  uint32_t(kFlagModuleTooBig) == uint32_t(PG_FLAG_MODULE_TOO_BIG) &&
+                  uint32_t(kFlagSplitModule) == uint32_t(PG_FLAG_SPLIT_MODULE),
+              "flag bits of the ABI");
 
 struct EventCounters {
   uint32_t wordStart, nWords;   // input slice of the batch word buffer
@@ -111,10 +120,30 @@ struct CAConfig {
   uint32_t earlyFishbone, lateFishbone;
 };
 
+// FED scan on the device (fedscan.cu): the batch's whole FED blocks and the
+// per-FED bookkeeping of the header/trailer walk
+constexpr uint32_t kFmtErrCap = 1024;  // framing errors kept per event
+struct FedScanBuffers {
+  uint32_t on;               // 1: the chain starts from raw FED blocks (else from host-unpacked words)
+  uint32_t recordErrors;     // record the framing errors (the ErrorChecker's includeErrors)
+  uint32_t nFeds;            // FEDs of the ES list, in its order (fedId 40 and ids >= 4096 left out)
+  uint32_t rawCap64;         // capacity of raw64, in 64-bit words
+  const uint32_t* fedIds;    // [nFeds]
+  uint64_t* raw64;           // the FED blocks, header to trailer, 8-byte aligned
+  uint2* tab;                // [maxEvents][nFeds] {first 64-bit word in raw64, 64-bit length}
+  uint32_t* len;             // [maxEvents][nFeds] payload words
+  uint32_t* src;             // [maxEvents][nFeds] first payload 64-bit word in raw64
+  uint32_t* dst;             // [maxEvents][nFeds] first payload word within the event
+  uint32_t* evWords;         // [maxEvents]
+  PfFormatterError* fmt;     // [maxEvents][kFmtErrCap]
+  uint32_t* fmtCount;        // [maxEvents] (may exceed kFmtErrCap; the first kFmtErrCap are kept)
+};
+
 struct Workspace {
   uint32_t maxEvents;
   uint32_t wordCap;          // words over the whole batch
   CAConfig ca;               // the context's CA configuration
+  FedScanBuffers scan;       // device FED scan (scan.on == 0: not used)
   // input
   uint32_t* words;
   uint8_t* fedIds;
@@ -272,6 +301,8 @@ cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream);
 
 // batch input descriptor and compact results (k_pack.cu)
 void launchSetInput(Workspace& ws, const uint32_t* words, const uint8_t* fedIds, cudaStream_t s);
+// device FED scan: wordOffsets, words and fedIds of the batch from ws.scan
+void launchFedScan(Workspace& ws, uint32_t nEvents, cudaStream_t stream);
 void launchPack(Workspace& ws, uint32_t nEvents, uint8_t* out, cudaStream_t s);
 
 // batched segmented exclusive scan: out[e*stride + i] = sum_{k<i} in[e*stride + k]

@@ -47,6 +47,14 @@ struct Slot {
   uint32_t nEvents = 0;
   bool staged = false;
   SlotState state = SlotState::kFree;
+  // formatter errors of the current batch, host-scan mode: event k's are
+  // [fmtOff[k], fmtOff[k + 1])
+  std::vector<PfFormatterError> fmtErrors;
+  std::vector<uint32_t> fmtOff;
+  // device FED scan: its device buffers and the pinned FED blocks and table
+  void* dScan = nullptr;
+  uint64_t* hRaw = nullptr;
+  uint2* hTab = nullptr;
 };
 
 // A pinned buffer that holds one unpacked event on its way into the pool.
@@ -85,6 +93,7 @@ struct Pool {
 
 struct HostES {
   std::vector<uint32_t> fedIds;
+  std::vector<uint32_t> scanFeds;  // the FEDs the loop visits, in order (fedId 40 and ids >= 4096 skipped)
 };
 
 struct pg_ctx {
@@ -104,8 +113,10 @@ namespace pixgpu {
 
 int fail(pg_ctx* c, int code, const std::string& msg);
 int cudaFail(pg_ctx* c, cudaError_t e, const char* where);
+// FED loop of one raw record on the host; fmt (may be null) receives the
+// framing errors
 int unpackRaw(const std::vector<uint32_t>& fedIds, const uint8_t* raw, size_t n, uint32_t* words, uint8_t* fed,
-              uint32_t cap, uint32_t* nWordsOut);
+              uint32_t cap, uint32_t* nWordsOut, std::vector<PfFormatterError>* fmt = nullptr);
 // chain + result packing for the slot's current batch (graph or plain launches)
 int launchBatch(pg_ctx* c, Slot& s);
 // captures the chain for n events on slot s once (no-op when present)

@@ -42,6 +42,8 @@ SCALARS = ["nDigis", "nModules", "nClusters", "nHits", "nCells", "nTuples", "nVe
            "nTrkLists"]
 ERROR_DTYPE = np.dtype([("rawId", "<u4"), ("word", "<u4"), ("errorType", "u1"), ("fedId", "u1"),
                         ("pad", "u1", 2)])
+# PfFormatterError: the 64-bit header/trailer word, the error type, the full FED id
+FORMATTER_ERROR_DTYPE = np.dtype([("word64", "<u8"), ("errorType", "<u4"), ("fedId", "<u4")])
 FLOAT_PRODUCTS = {"xl", "yl", "xerr", "yerr", "xg", "yg", "zg", "rg", "agcLadderR", "state", "cov", "pt", "eta",
                   "chi2", "zv", "wv", "vchi2", "ptv2"}
 B_FIELD = 0.0114256972711507
@@ -50,6 +52,8 @@ B_FIELD = 0.0114256972711507
 def _as_array(buf, name, elem):
     if name == "errors":
         return np.frombuffer(buf, dtype=ERROR_DTYPE).copy()
+    if name == "formatterErrors":
+        return np.frombuffer(buf, dtype=FORMATTER_ERROR_DTYPE).copy()
     if name in SCALARS:
         return int(np.frombuffer(buf, dtype=np.uint32)[0])
     dt = _TYPES.get(name)
@@ -104,6 +108,12 @@ class Truth(ctypes.Structure):
 
 ES_NAMES = ["cablingMap.bin", "gain.bin", "cpefast.bin", "beamspot.bin", "fedIds.bin"]
 BASE_SEED = 20261203
+# pg_flag bits (include/pixgpu.h)
+PG_FLAG_TUPLE_OVERFLOW = 1 << 5
+PG_FLAG_CELL_OVERFLOW = 1 << 6
+PG_FLAG_TOO_MANY_WORDS = 1 << 9
+PG_FLAG_BAD_INPUT = 1 << 15
+PG_FLAG_SPLIT_MODULE = 1 << 17
 
 
 class Detector:
@@ -193,7 +203,14 @@ class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("max_events", ctypes.c_uint32), ("max_words_per_batch", ctypes.c_uint32),
                 ("slots", ctypes.c_uint32), ("use_graphs", ctypes.c_uint32), ("pool_words", ctypes.c_uint64),
                 ("hbm_fraction", ctypes.c_double), ("riemann_fit", ctypes.c_uint32), ("vertex_algo", ctypes.c_uint32)] + \
-        [(n, ctypes.c_uint32) for n in CA_FIELDS]
+        [(n, ctypes.c_uint32) for n in CA_FIELDS] + [("formatter_errors", ctypes.c_uint32), ("fed_scan", ctypes.c_uint32)]
+
+
+def default_config():
+    """pg_default_config as a dict (the reference's configuration)."""
+    cfg = Config()
+    gpu_lib().pg_default_config(ctypes.byref(cfg))
+    return {n: getattr(cfg, n) for n, _ in Config._fields_}
 
 
 class ResultView(ctypes.Structure):
@@ -339,10 +356,13 @@ class Chain:
     """A device context: resident conditions plus batch slots."""
 
     def __init__(self, es_images, max_events=64, max_words_per_batch=None, slots=1, device=0, use_graphs=True,
-                 pool_words=0, hbm_fraction=0.5, riemann_fit=False, vertex_algo=0, ca=None):
+                 pool_words=0, hbm_fraction=0.5, riemann_fit=False, vertex_algo=0, ca=None, formatter_errors=False,
+                 fed_scan="host"):
         """ca: CAHitNtupletGeneratorOnGPU parameters overriding the reference's (pg_config field
         names: min_hits_per_ntuplet, include_jumping_forward_doublets, early_fishbone, late_fishbone,
-        ideal_conditions, do_cluster_cut, do_z0_cut, do_pt_cut)."""
+        ideal_conditions, do_cluster_cut, do_z0_cut, do_pt_cut).  formatter_errors: record the FED
+        loop's framing errors ("formatterErrors").  fed_scan: "host", or "device" for the header and
+        trailer checks and the word concatenation on the GPU."""
         lib = gpu_lib()
         self._keep = list(es_images)
         img = ESImages(*[x for b in self._keep for x in (b, len(b))])
@@ -353,6 +373,10 @@ class Chain:
         cfg.device, cfg.max_events, cfg.max_words_per_batch, cfg.slots = device, max_events, max_words_per_batch, slots
         cfg.use_graphs, cfg.pool_words, cfg.hbm_fraction = 1 if use_graphs else 0, pool_words, hbm_fraction
         cfg.riemann_fit, cfg.vertex_algo = 1 if riemann_fit else 0, int(vertex_algo)
+        cfg.formatter_errors = 1 if formatter_errors else 0
+        if fed_scan not in ("host", "device"):
+            raise ValueError("fed_scan: 'host' or 'device'")
+        cfg.fed_scan = 1 if fed_scan == "device" else 0
         for k, v in (ca or {}).items():
             if k not in CA_FIELDS:
                 raise ValueError("unknown CA parameter %s" % k)
@@ -409,7 +433,8 @@ class Chain:
         out = {}
         for n in SCALARS:
             out[n] = self.product(k, n)
-        for n in ["xx", "yy", "adc", "moduleInd", "clus", "pdigi", "rawIdArr", "errors", "moduleStart", "clusInModule",
+        for n in ["xx", "yy", "adc", "moduleInd", "clus", "pdigi", "rawIdArr", "errors", "formatterErrors", "moduleStart",
+                  "clusInModule",
                   "moduleId", "clusModuleStart", "xl", "yl", "xerr", "yerr", "xg", "yg", "zg", "rg", "charge", "iphi",
                   "xsize", "ysize", "detInd", "cellInner", "cellOuter", "cellLayerPair", "cellDoubletId", "cellUsed",
                   "tupleOff", "tupleHits", "tupleDet", "quality", "state", "cov", "pt", "eta", "chi2", "zv", "wv",

@@ -41,8 +41,13 @@ def default_detector(detectors):
 
 
 def load_golden(name):
+    import pixgpu
     d = np.load(os.path.join(GOLDEN, name + ".npz"))
-    return {k: (int(d[k]) if d[k].ndim == 0 else d[k]) for k in d.files}
+    out = {k: (int(d[k]) if d[k].ndim == 0 else d[k]) for k in d.files}
+    # the fixtures come from the reference's configuration, whose ErrorChecker
+    # records no formatter errors
+    out.setdefault("formatterErrors", np.zeros(0, dtype=pixgpu.FORMATTER_ERROR_DTYPE))
+    return out
 
 
 def golden_event(meta_entry, detectors):

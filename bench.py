@@ -42,6 +42,7 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "pixeltrack-standalone_b200")
+TUNE_CACHE = os.path.join(PKG, "tuning", "launch_tuning.txt")
 sys.path.insert(0, PKG)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
@@ -91,11 +92,15 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--batch", type=int, default=64, help="events per launch sequence")
     p.add_argument("--events", type=int, default=576, help="distinct PU50 events (inputs > L2)")
-    p.add_argument("--slots", type=int, default=2, help="batches in flight")
+    p.add_argument("--slots", type=int, default=3, help="batches in flight")
     p.add_argument("--per-event", type=int, default=256, help="events for the one-event-per-launch leg")
     p.add_argument("--serve", type=int, default=4000, help="requests for the serving leg (0: skip)")
     p.add_argument("--serve-batch", type=int, default=16, help="max events per serving batch")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
+    p.add_argument("--mixed-batches", type=int, default=3,
+                   help="distinct 64-event batches with PU uniform in [20, 200] (0: skip that leg)")
+    p.add_argument("--autotune", action="store_true",
+                   help="tune the launch shapes now (else load the committed cache) and write the table")
     return p.parse_args()
 
 
@@ -341,6 +346,7 @@ def run_ours(a):
     # ------------------------------------------------------------ batched, device-resident
     chain = pixgpu.Chain(det.es, max_events=B, max_words_per_batch=max_words, slots=a.slots, device=dev,
                          pool_words=sum(nw) + 64 * len(nw) + 4096)
+    tuning = apply_tuning(chain, B, raws, a)
     handles = []
     for r in raws:
         h = chain.pool_put(r)
@@ -422,6 +428,7 @@ def run_ours(a):
                             % (len(raws), input_bytes / 1e6),
                       "parallelism": "replicas (events shard across GPUs, no collective)"},
            "gpu_launches": launches_per_batch * a.steps,
+           "launch_tuning": tuning,
            "clocks": clocks,
            "roofline": roof,
            "chain_roofline": {"achieved": chain_ach, "peak": hbm, "unit": "GB/s", "frac": chain_ach / hbm,
@@ -431,6 +438,38 @@ def run_ours(a):
                              sorted(census.items(), key=lambda x: -x[1])[:12]},
            "result_bytes_per_step": result_bytes[0] / max(1, a.steps)}
 
+    # ------------------------------------------------------------ batched, uneven pileup
+    # 64 events per launch with PU uniform in [20, 200] (the batched-chain
+    # configuration), device-resident inputs, the same tuning
+    if rank == 0 and world == 1 and a.mixed_batches:
+        rng = np.random.default_rng(3)
+        mpus = rng.uniform(20.0, 200.0, B * a.mixed_batches)
+        with cf.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+            mraws = list(ex.map(lambda k: det.event(SEED0 + 200000 + k, float(mpus[k])), range(len(mpus))))
+        mnw = [len(r) // 4 for r in mraws]
+        mb = [mnw[i * B:(i + 1) * B] for i in range(a.mixed_batches)]
+        mchain = pixgpu.Chain(det.es, max_events=B, max_words_per_batch=max(sum(x) for x in mb) + 1024,
+                              slots=a.slots, device=dev, pool_words=sum(mnw) + 64 * len(mnw) + 4096)
+        for k, v in tuning["grid_scales"].items():
+            mchain.tune_set(B, k, v)
+        mh = []
+        for r in mraws:
+            h = mchain.pool_put(r)
+            while h is None:
+                time.sleep(0.001)
+                h = mchain.pool_put(r)
+            mh.append(h)
+        mbatches = [mh[i * B:(i + 1) * B] for i in range(a.mixed_batches)]
+        mchain.prepare(B)
+        msub = lambda i: mchain.submit_pooled(mbatches[i % len(mbatches)], keep=True)  # noqa: E731
+        pipeline(mchain, torch, a.warmup, msub, lambda s: None)
+        msteps = max(8, a.steps // 2)
+        mms = pipeline(mchain, torch, msteps, msub, lambda s: None)
+        mchain.close()
+        out["batched_mixed_pu"] = {"pu": "uniform 20-200", "events_per_batch": B, "distinct_events": len(mraws),
+                                   "mean_words_per_event": float(np.mean(mnw)), "steps": msteps,
+                                   "events_per_s": msteps * B / (mms / 1e3), "ms_per_step": mms / msteps}
+
     # ------------------------------------------------------------ end to end through pg_submit
     nbh = len(raws) // B
     host_batches = [raws[(i % nbh) * B:(i % nbh) * B + B] for i in range(nbh)]
@@ -438,6 +477,8 @@ def run_ours(a):
     def e2e_leg(scan):
         ec = pixgpu.Chain(det.es, max_events=B, max_words_per_batch=max_words, slots=a.slots, device=dev,
                           fed_scan=scan)
+        for k, v in tuning["grid_scales"].items():
+            ec.tune_set(B, k, v)
         ec.prepare(B)
         h2d = [0]
         d2h = [0]
@@ -551,6 +592,24 @@ def run_ours(a):
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
+
+
+def apply_tuning(chain, B, raws, a):
+    """Launch shapes for B-event batches: the committed cache for this device, or
+    the autotuner's choice (with --autotune, or when the cache has no entry)."""
+    import pixgpu
+    src = "cache"
+    n = chain.tune_load(TUNE_CACHE) if (os.path.exists(TUNE_CACHE) and not a.autotune) else 0
+    gain = None
+    if n == 0:
+        src = "autotuned in this run"
+        gain = chain.autotune(raws[:B], repeats=3)
+        out_dir = os.path.join(ROOT, "gpurun_out")
+        if os.path.isdir(out_dir):
+            chain.tune_save(os.path.join(out_dir, "launch_tuning.txt"))
+    table = {k: v for k, v in chain.tune_table(B).items() if v}
+    return {"source": src, "events_per_batch": B, "grid_scales": table, "tuner_gain_ms_per_batch": gain,
+            "kernels_tunable": len(pixgpu.tune_kernel_names())}
 
 
 def main():

@@ -274,6 +274,27 @@ typedef struct pg_probe_entry {
 int pg_set_probe(pg_ctx* ctx, const char* kernel);
 int pg_probe_read(pg_ctx* ctx, uint32_t slot, uint32_t max, pg_probe_entry* out, uint32_t* n);
 
+/* Launch-shape tuning.  Each tunable kernel loops grid-stride over its
+ * event's work; its grid x-extent is the default for the batch size times
+ * 2^scale, scale in -3..3 (0: default), kept per batch size (a batch uses the
+ * table of its size, else of the largest tuned size below it).  Results do
+ * not depend on the scales.  pg_tune_kernel_name(i) names the i-th tunable
+ * kernel (NULL past the last).  pg_tune_set/pg_tune_load need every slot free
+ * and drop the captured graphs.
+ * pg_autotune times each tunable kernel (kernel probe, median of `repeats`
+ * batches of the first n records) at scales -2..2 and keeps the fastest when
+ * it gains 2%, kernel by kernel; *gain_ms receives the summed saving per batch.
+ * pg_tune_save writes the table as lines "<device name>|<n> <kernel> <scale>";
+ * pg_tune_load applies the lines of this context's device and returns their
+ * number (>= 0), or PG_ERR_NOTFOUND when the file is missing. */
+const char* pg_tune_kernel_name(uint32_t i);
+int pg_tune_set(pg_ctx* ctx, uint32_t n_events, const char* kernel, int scale);
+int pg_tune_get(const pg_ctx* ctx, uint32_t n_events, const char* kernel, int* scale);
+int pg_autotune(pg_ctx* ctx, uint32_t n_events, const uint8_t* const* raws, const size_t* sizes, uint32_t repeats,
+                double* gain_ms);
+int pg_tune_save(const pg_ctx* ctx, const char* path);
+int pg_tune_load(pg_ctx* ctx, const char* path);
+
 /* Vertex finding without device allocation.  No counterpart in the reference:
  * it exists for callers that cannot allocate device memory where they need the
  * vertices, e.g. a per-event module inside a framework that owns all device

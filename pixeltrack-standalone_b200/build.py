@@ -27,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-I", INC, "-I", CSRC,
            "--expt-relaxed-constexpr"] + ARCH
 CU_SOURCES = ["scan.cu", "k_local.cu", "k_ca.cu", "k_fit.cu", "k_vertex.cu", "k_pack.cu", "chain.cu", "capi.cu",
-              "pool.cu", "serve.cu", "noalloc.cu", "fedscan.cu"]
+              "pool.cu", "serve.cu", "noalloc.cu", "fedscan.cu", "tune.cu"]
 
 
 def _run(cmd):

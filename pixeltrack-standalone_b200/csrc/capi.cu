@@ -305,6 +305,7 @@ int captureGraph(pg_ctx* c, Slot& s, uint32_t n, cudaGraphExec_t* out) {
   KernelProbe* pr = c->probeName.empty() ? nullptr : s.probe;
   if (pr) pr->used = 0;
   tProbe = pr;
+  s.ws.tune = tuningFor(c, n);
   cudaError_t le = runChain(c->des, s.ws, n, s.stream, c->cfg.riemann_fit != 0, int(c->cfg.vertex_algo));
   if (le == cudaSuccess) {
     launchPack(s.ws, n, s.dRes, s.stream);
@@ -359,6 +360,7 @@ int pixgpu::launchBatch(pg_ctx* c, Slot& s) {
     KernelProbe* pr = c->probeName.empty() ? nullptr : s.probe;
     if (pr) pr->used = 0;
     tProbe = pr;
+    s.ws.tune = tuningFor(c, s.nEvents);
     e = runChain(c->des, s.ws, s.nEvents, s.stream, c->cfg.riemann_fit != 0, int(c->cfg.vertex_algo));
     if (e == cudaSuccess) launchPack(s.ws, s.nEvents, s.dRes, s.stream);
     tProbe = nullptr;

@@ -169,7 +169,7 @@ void launchFedScan(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   PG_PROBED("kFedScan", stream, kFedScan<<<nEvents, kScanThreads, 0, stream>>>(ws));
   // a few warps per event: ~100 FEDs of a few hundred word pairs each
   const uint32_t sx = nEvents >= 32 ? 2 : (nEvents >= 8 ? 4 : 16);
-  PG_PROBED("kFedCopy", stream, kFedCopy<<<dim3(sx, nEvents), kCopyThreads, 0, stream>>>(ws, nEvents));
+  PG_PROBED("kFedCopy", stream, kFedCopy<<<dim3(tunedGrid(ws, kTuneFedCopy, sx), nEvents), kCopyThreads, 0, stream>>>(ws, nEvents));
 }
 
 }  // namespace pixgpu

@@ -1189,56 +1189,56 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   // ---- doublets: count per inner-hit slot, scan, write in serial order
   PG_PROBED("kDoubletSetup", stream, kDoubletSetup<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents));
   PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.ohCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
-  PG_PROBED("kDoubletCount", stream, kDoubletCount<<<dim3(gx * 4, nEvents), 256, 0, stream>>>(ws));
+  PG_PROBED("kDoubletCount", stream, kDoubletCount<<<dim3(tunedGrid(ws, kTuneDoubletCount, gx * 4), nEvents), 256, 0, stream>>>(ws));
   segScan(ws.jCount, ws.jOffset, kJCap + 1, EVF(ntot), kJCap, nullptr, 0, ws.scanSums, nEvents, stream);
-  PG_PROBED("kDoubletWrite", stream, kDoubletWrite<<<dim3(gx * 4, nEvents), 256, 0, stream>>>(ws));
+  PG_PROBED("kDoubletWrite", stream, kDoubletWrite<<<dim3(tunedGrid(ws, kTuneDoubletWrite, gx * 4), nEvents), 256, 0, stream>>>(ws));
   PG_PROBED("kCellsTotal", stream, kCellsTotal<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents));
   // ---- isOuterHitOfCell: scan of the per-hit counts, unordered fill, order per hit
   segScan(ws.ohCount, ws.ohOff, kHitCap + 1, EVF(nHits), kHitCap, nullptr, 0, ws.scanSums, nEvents, stream, true);
-  PG_PROBED("kOuterHitFill", stream, kOuterHitFill<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kOuterHitFill", stream, kOuterHitFill<<<dim3(tunedGrid(ws, kTuneOuterHitFill, gx), nEvents), 256, 0, stream>>>(ws));
   sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.ohCells, kCellCap, ws.ohOff, kHitCap + 1, EVF(nHits), 0, false, kCellCap, 0);
-  PG_PROBED("kOhRec", stream, kOhRec<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kOhRec", stream, kOhRec<<<dim3(tunedGrid(ws, kTuneOhRec, gx), nEvents), 256, 0, stream>>>(ws));
   // ---- CA links: edges appended unordered, then CSR by inner cell, ordered ascending
   PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbrCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
-  PG_PROBED("kConnect", stream, kConnect<<<dim3(gx * 4, nEvents), 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
+  PG_PROBED("kConnect", stream, kConnect<<<dim3(tunedGrid(ws, kTuneConnect, gx * 4), nEvents), 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
   segScan(ws.nbrCount, ws.nbrOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanSums, nEvents, stream, true);
-  PG_PROBED("kEdgeScatter", stream, kEdgeScatter<<<g, 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
+  PG_PROBED("kEdgeScatter", stream, kEdgeScatter<<<dim3(tunedGrid(ws, kTuneEdgeScatter, gx), nEvents), 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
   sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.nbr, kEdgeCap, ws.nbrOff, kCellCap + 1, EVF(nCells), 0, false, kEdgeCap, 1);
-  PG_PROBED("kNbrPool", stream, kNbrPool<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kNbrPool", stream, kNbrPool<<<dim3(tunedGrid(ws, kTuneNbrPool, gx), nEvents), 256, 0, stream>>>(ws));
   // ---- early fishbone
   if (ws.ca.earlyFishbone)
-    PG_PROBED("kFishbone", stream, kFishbone<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws, false));
+    PG_PROBED("kFishbone", stream, kFishbone<<<dim3(tunedGrid(ws, kTuneFishbone, gx * 2), nEvents), 256, 0, stream>>>(ws, false));
   // ---- n-tuplets: DFS count, scans, DFS write, finalize
-  PG_PROBED("kNtupletCount", stream, kNtupletCount<<<dim3(gx * 8, nEvents), 128, 0, stream>>>(ws));
+  PG_PROBED("kNtupletCount", stream, kNtupletCount<<<dim3(tunedGrid(ws, kTuneNtupletCount, gx * 8), nEvents), 128, 0, stream>>>(ws));
   segScan(ws.startTupleCount, ws.startTupleOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcM), ws.scanSums, nEvents, stream);
   segScan(ws.startHitCount, ws.startHitOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcN), ws.scanSums, nEvents, stream);
-  PG_PROBED("kNtupletWrite", stream, kNtupletWrite<<<dim3(gx * 8, nEvents), 128, 0, stream>>>(ws));
+  PG_PROBED("kNtupletWrite", stream, kNtupletWrite<<<dim3(tunedGrid(ws, kTuneNtupletWrite, gx * 8), nEvents), 128, 0, stream>>>(ws));
   PG_PROBED("kTupleFinalize", stream, kTupleFinalize<<<dim3(32, nEvents), 1024, 0, stream>>>(ws));
   // ---- cell -> track lists
   PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trkCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
-  PG_PROBED("kTrackCount", stream, kTrackCount<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kTrackCount", stream, kTrackCount<<<dim3(tunedGrid(ws, kTuneTrackCount, gx), nEvents), 256, 0, stream>>>(ws));
   segScan(ws.trkCount, ws.trkOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanSums, nEvents, stream, true);
-  PG_PROBED("kTrackFill", stream, kTrackFill<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kTrackFill", stream, kTrackFill<<<dim3(tunedGrid(ws, kTuneTrackFill, gx), nEvents), 256, 0, stream>>>(ws));
   sortSegments<uint16_t>(ws, nEvents, stream, gx * 2, ws.trk, kTupleCellCap, ws.trkOff, kCellCap + 1, EVF(nCells), 0, false, kTupleCellCap, 2);
   uint32_t* candFlag = ws.startTupleCount;  // scratch
   uint32_t* candOff = ws.startHitCount;
-  PG_PROBED("kTrackPool", stream, kTrackPool<<<g, 256, 0, stream>>>(ws, candFlag));
+  PG_PROBED("kTrackPool", stream, kTrackPool<<<dim3(tunedGrid(ws, kTuneTrackPool, gx), nEvents), 256, 0, stream>>>(ws, candFlag));
   segScan(candFlag, candOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(nCandidates), ws.scanSums, nEvents, stream);
-  PG_PROBED("kCandidateScatter", stream, kCandidateScatter<<<g, 256, 0, stream>>>(ws, candFlag, candOff));
-  PG_PROBED("kEarlyDup", stream, kEarlyDup<<<g, 256, 0, stream>>>(ws));
-  PG_PROBED("kTupleDet", stream, kTupleDet<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kCandidateScatter", stream, kCandidateScatter<<<dim3(tunedGrid(ws, kTuneCandidateScatter, gx), nEvents), 256, 0, stream>>>(ws, candFlag, candOff));
+  PG_PROBED("kEarlyDup", stream, kEarlyDup<<<dim3(tunedGrid(ws, kTuneEarlyDup, gx), nEvents), 256, 0, stream>>>(ws));
+  PG_PROBED("kTupleDet", stream, kTupleDet<<<dim3(tunedGrid(ws, kTuneTupleDet, gx), nEvents), 256, 0, stream>>>(ws));
   // ---- tuple multiplicity for the fits
   PG_PROBED("kMultiplicity", stream, kMultiplicity<<<nEvents, 1024, 0, stream>>>(ws));
   // ---- late fishbone (CAHitNtupletGeneratorKernels.cc:133-136)
   if (ws.ca.lateFishbone)
-    PG_PROBED("kFishbone", stream, kFishbone<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws, true));
+    PG_PROBED("kFishbone", stream, kFishbone<<<dim3(tunedGrid(ws, kTuneFishbone, gx * 2), nEvents), 256, 0, stream>>>(ws, true));
   return cudaGetLastError();
 }
 
 cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   const uint32_t gx = nEvents >= 32 ? 16 : (nEvents >= 8 ? 64 : 296);
   dim3 g(gx, nEvents);
-  PG_PROBED("kClassify", stream, kClassify<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kClassify", stream, kClassify<<<dim3(tunedGrid(ws, kTuneClassify, gx), nEvents), 256, 0, stream>>>(ws));
   // kernel_fishboneCleaner with the late fishbone (CAHitNtupletGeneratorKernels.cc:159-162)
   if (ws.ca.lateFishbone) PG_PROBED("kFishboneCleaner", stream, kFishboneCleaner<<<g, 256, 0, stream>>>(ws));
   // fastDuplicateRemover (candFlag survives in startTupleCount from runCA)
@@ -1246,7 +1246,7 @@ cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   uint32_t* candOff = ws.startHitCount;  // candidate index of each cell, from runCA
   uint32_t* indeg = ws.scratchA;        // [maxEvents][kEdgeCap] >= kCellCap
   uint32_t* lists = ws.scratchB;        // two worklists of kCellCap per event
-  PG_PROBED("kFastDupInDegree", stream, kFastDupInDegree<<<g, 256, 0, stream>>>(ws, indeg, candFlag));
+  PG_PROBED("kFastDupInDegree", stream, kFastDupInDegree<<<dim3(tunedGrid(ws, kTuneFastDupInDegree, gx), nEvents), 256, 0, stream>>>(ws, indeg, candFlag));
   const uint32_t P = nEvents <= kClusterMaxEvents ? kFastDupCtas : 1;
   cudaError_t le = cudaSuccess;
   PG_PROBED("kFastDupRounds", stream,
@@ -1255,11 +1255,11 @@ cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   if (le != cudaSuccess) return le;
   // hit -> tuple map and triplet cleaner
   PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
-  PG_PROBED("kHitToTupleCount", stream, kHitToTupleCount<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kHitToTupleCount", stream, kHitToTupleCount<<<dim3(tunedGrid(ws, kTuneHitToTupleCount, gx), nEvents), 256, 0, stream>>>(ws));
   segScan(ws.h2tCount, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, nullptr, 0, ws.scanSums, nEvents, stream, true);
-  PG_PROBED("kHitToTupleFill", stream, kHitToTupleFill<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kHitToTupleFill", stream, kHitToTupleFill<<<dim3(tunedGrid(ws, kTuneHitToTupleFill, gx), nEvents), 256, 0, stream>>>(ws));
   sortSegments<uint16_t>(ws, nEvents, stream, gx * 2, ws.h2t, kH2TCap, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, true, kH2TCap, 3);
-  PG_PROBED("kTripletCleaner", stream, kTripletCleaner<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws));
+  PG_PROBED("kTripletCleaner", stream, kTripletCleaner<<<dim3(tunedGrid(ws, kTuneTripletCleaner, gx * 2), nEvents), 256, 0, stream>>>(ws));
   return cudaGetLastError();
 }
 

@@ -464,13 +464,13 @@ __global__ void kBLFitDirect(uint32_t n, const double* hits, const float* hge, d
 cudaError_t runFits(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream, bool riemann) {
   const uint32_t gx = nEvents >= 32 ? 8 : (nEvents >= 8 ? 32 : 148);
   dim3 g(gx, nEvents);
-  PG_PROBED("kFitZero", stream, kFitZero<<<g, 256, 0, stream>>>(ws));
+  PG_PROBED("kFitZero", stream, kFitZero<<<dim3(tunedGrid(ws, kTuneFitZero, g.x), nEvents), 256, 0, stream>>>(ws));
   // FP64-bound: enough warps per SM to cover the double-precision latency
   const uint32_t fx = nEvents >= 32 ? 16 : (nEvents >= 8 ? 64 : 296);
   if (riemann)
-    PG_PROBED("kRiemannFit", stream, kRiemannFit<<<dim3(fx, nEvents, 3), 128, 0, stream>>>(es, ws));
+    PG_PROBED("kRiemannFit", stream, kRiemannFit<<<dim3(tunedGrid(ws, kTuneFit, fx), nEvents, 3), 128, 0, stream>>>(es, ws));
   else
-    PG_PROBED("kBLFit", stream, kBLFit<<<dim3(fx, nEvents, 3), 128, 0, stream>>>(es, ws));
+    PG_PROBED("kBLFit", stream, kBLFit<<<dim3(tunedGrid(ws, kTuneFit, fx), nEvents, 3), 128, 0, stream>>>(es, ws));
   return cudaGetLastError();
 }
 

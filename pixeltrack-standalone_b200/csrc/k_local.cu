@@ -1163,29 +1163,29 @@ __global__ void kSortErrors(Workspace ws) {
 cudaError_t runLocal(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   PG_PROBED("kInitEvents", stream, kInitEvents<<<nEvents, 256, 0, stream>>>(ws, nEvents));
   const int flatBlocks = 148 * 8;
-  PG_PROBED("kRawToDigi", stream, kRawToDigi<<<flatBlocks, 256, 0, stream>>>(es, ws, nEvents));
-  PG_PROBED("kModuleBoundaries", stream, kModuleBoundaries<<<flatBlocks, 256, 0, stream>>>(ws, nEvents));
+  PG_PROBED("kRawToDigi", stream, kRawToDigi<<<tunedGrid(ws, kTuneRawToDigi, flatBlocks), 256, 0, stream>>>(es, ws, nEvents));
+  PG_PROBED("kModuleBoundaries", stream, kModuleBoundaries<<<tunedGrid(ws, kTuneModuleBoundaries, flatBlocks), 256, 0, stream>>>(ws, nEvents));
   PG_PROBED("kSortModules", stream, kSortModules<<<nEvents, 1024, 0, stream>>>(ws, nEvents));
   PG_PROBED("kSortErrors", stream, kSortErrors<<<nEvents, 32, 0, stream>>>(ws));
   PG_PROBED("kFindClusters", stream,
             kFindClustersSmall<<<dim3((kMaxModules + kSmallWarps - 1) / kSmallWarps, nEvents), kSmallWarps * 32, 0,
                                  stream>>>(ws));
-  PG_PROBED("kFindClustersBig", stream, kFindClustersBig<<<dim3(64, nEvents), kClusThreads, 0, stream>>>(ws));
+  PG_PROBED("kFindClustersBig", stream, kFindClustersBig<<<dim3(tunedGrid(ws, kTuneFindClustersBig, 64), nEvents), kClusThreads, 0, stream>>>(ws));
   PG_PROBED("kHitsModuleStart", stream, kHitsModuleStart<<<nEvents, 1024, 0, stream>>>(es, ws));
   PG_PROBED("kGetHits", stream,
             kGetHitsSmall<<<dim3((kMaxModules + kHitWarps - 1) / kHitWarps, nEvents), kHitWarps * 32, 0, stream>>>(es,
                                                                                                                ws));
-  PG_PROBED("kGetHitsBig", stream, kGetHitsBig<<<dim3(64, nEvents), kHitThreads, 0, stream>>>(es, ws));
+  PG_PROBED("kGetHitsBig", stream, kGetHitsBig<<<dim3(tunedGrid(ws, kTuneGetHitsBig, 64), nEvents), kHitThreads, 0, stream>>>(es, ws));
   // phi histogram: count, exclusive scan, unordered fill, per-bin ordering
   uint32_t* cursor = ws.jCount;  // scratch: the doublet counters are not in use yet
   PG_PROBED("kZeroU32", stream, kZeroU32<<<dim3(2, nEvents), 1024, 0, stream>>>(ws.phiOff, kPhiStride, kPhiStride, nEvents));
   PG_PROBED("kZeroU32", stream, kZeroU32<<<dim3(2, nEvents), 1024, 0, stream>>>(cursor, kPhiStride, kPhiStride, nEvents));
-  PG_PROBED("kPhiCount", stream, kPhiCount<<<dim3(16, nEvents), 256, 0, stream>>>(ws));
+  PG_PROBED("kPhiCount", stream, kPhiCount<<<dim3(tunedGrid(ws, kTunePhiCount, 16), nEvents), 256, 0, stream>>>(ws));
   // in place exclusive scan of the 1280 counters; the total lands in the extra bin
   segScan(ws.phiOff, ws.phiOff, kPhiStride, nullptr, 0, kPhiTot - 1, nullptr, 0, ws.scanSums, nEvents, stream);
-  PG_PROBED("kPhiFill", stream, kPhiFill<<<dim3(16, nEvents), 256, 0, stream>>>(ws, cursor));
+  PG_PROBED("kPhiFill", stream, kPhiFill<<<dim3(tunedGrid(ws, kTunePhiFill, 16), nEvents), 256, 0, stream>>>(ws, cursor));
   PG_PROBED("kPhiSort", stream, kPhiSort<<<dim3((kPhiTot - 1 + 7) / 8, nEvents), 256, 0, stream>>>(ws));
-  PG_PROBED("kPhiRec", stream, kPhiRec<<<dim3(16, nEvents), 256, 0, stream>>>(ws));
+  PG_PROBED("kPhiRec", stream, kPhiRec<<<dim3(tunedGrid(ws, kTunePhiRec, 16), nEvents), 256, 0, stream>>>(ws));
   return cudaGetLastError();
 }
 

@@ -139,11 +139,29 @@ struct FedScanBuffers {
   uint32_t* fmtCount;        // [maxEvents] (may exceed kFmtErrCap; the first kFmtErrCap are kept)
 };
 
+// Launch-shape tuning (tune.cu): the grid x-extent of each tunable launch is
+// its default (a function of the batch size) times 2^scale.  Every tunable
+// kernel loops grid-stride over its event's work, so the scale changes only
+// the speed, never the results.
+enum TuneId : uint32_t {
+  kTuneRawToDigi, kTuneModuleBoundaries, kTuneFindClustersBig, kTuneGetHitsBig, kTunePhiCount, kTunePhiFill,
+  kTunePhiRec, kTuneDoubletCount, kTuneDoubletWrite, kTuneOuterHitFill, kTuneOhRec, kTuneConnect, kTuneEdgeScatter,
+  kTuneNbrPool, kTuneFishbone, kTuneNtupletCount, kTuneNtupletWrite, kTuneTrackCount, kTuneTrackFill,
+  kTuneTrackPool, kTuneCandidateScatter, kTuneEarlyDup, kTuneTupleDet, kTuneClassify, kTuneFastDupInDegree,
+  kTuneHitToTupleCount, kTuneHitToTupleFill, kTuneTripletCleaner, kTuneFitZero, kTuneFit, kTuneFedCopy, kNumTune
+};
+extern const char* const kTuneNames[kNumTune];
+constexpr int kTuneMinScale = -3, kTuneMaxScale = 3;
+struct LaunchTuning {
+  int8_t scale[kNumTune];
+};
+
 struct Workspace {
   uint32_t maxEvents;
   uint32_t wordCap;          // words over the whole batch
   CAConfig ca;               // the context's CA configuration
   FedScanBuffers scan;       // device FED scan (scan.on == 0: not used)
+  LaunchTuning tune;         // grid scales of the tunable launches (host side)
   // input
   uint32_t* words;
   uint8_t* fedIds;
@@ -301,6 +319,13 @@ cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream);
 
 // batch input descriptor and compact results (k_pack.cu)
 void launchSetInput(Workspace& ws, const uint32_t* words, const uint8_t* fedIds, cudaStream_t s);
+// grid x-extent of a tunable launch
+inline uint32_t tunedGrid(const Workspace& ws, TuneId id, uint32_t base) {
+  const int s = ws.tune.scale[id];
+  uint64_t g = s >= 0 ? uint64_t(base) << s : uint64_t(base) >> (-s);
+  return uint32_t(g < 1 ? 1 : (g > 65535 ? 65535 : g));
+}
+
 // device FED scan: wordOffsets, words and fedIds of the batch from ws.scan
 void launchFedScan(Workspace& ws, uint32_t nEvents, cudaStream_t stream);
 void launchPack(Workspace& ws, uint32_t nEvents, uint8_t* out, cudaStream_t s);

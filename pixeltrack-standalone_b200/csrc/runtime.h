@@ -104,6 +104,7 @@ struct pg_ctx {
   pixgpu::DeviceES des{};
   std::vector<pixgpu::Slot> slots;
   pixgpu::Pool pool;
+  std::map<uint32_t, pixgpu::LaunchTuning> tuning;  // launch tuning per batch size (tune.cu)
   std::string probeName;  // kernel timed by the probe ("" = none)
   std::string err;
   std::mutex mu;  // slot bookkeeping (the serving loop's threads share it)
@@ -112,6 +113,8 @@ struct pg_ctx {
 namespace pixgpu {
 
 int fail(pg_ctx* c, int code, const std::string& msg);
+// the launch tuning for batches of n events: n's table, else the largest tuned size below n, else defaults
+LaunchTuning tuningFor(const pg_ctx* c, uint32_t n);
 int cudaFail(pg_ctx* c, cudaError_t e, const char* where);
 // FED loop of one raw record on the host; fmt (may be null) receives the
 // framing errors

@@ -206,6 +206,17 @@ class Config(ctypes.Structure):
         [(n, ctypes.c_uint32) for n in CA_FIELDS] + [("formatter_errors", ctypes.c_uint32), ("fed_scan", ctypes.c_uint32)]
 
 
+def tune_kernel_names():
+    """The kernels whose launch shape the tuner sets."""
+    out, i = [], 0
+    while True:
+        n = gpu_lib().pg_tune_kernel_name(i)
+        if not n:
+            return out
+        out.append(n.decode())
+        i += 1
+
+
 def default_config():
     """pg_default_config as a dict (the reference's configuration)."""
     cfg = Config()
@@ -314,6 +325,14 @@ def gpu_lib():
         _gpu.pg_submit_pooled.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
                                           ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
         _gpu.pg_set_probe.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        _gpu.pg_tune_kernel_name.restype = ctypes.c_char_p
+        _gpu.pg_tune_kernel_name.argtypes = [ctypes.c_uint32]
+        _gpu.pg_tune_set.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_char_p, ctypes.c_int]
+        _gpu.pg_tune_get.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]
+        _gpu.pg_autotune.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_char_p),
+                                     ctypes.POINTER(ctypes.c_size_t), ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]
+        _gpu.pg_tune_save.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        _gpu.pg_tune_load.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         _gpu.pg_batch_summary_get.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(BatchSummary)]
         _gpu.pg_probe_read.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ProbeEntry),
                                        ctypes.POINTER(ctypes.c_uint32)]
@@ -535,6 +554,37 @@ class Chain:
         n = ctypes.c_uint32()
         self._check(gpu_lib().pg_probe_read(self._h, slot, 256, buf, ctypes.byref(n)), "pg_probe_read")
         return [(buf[i].kernel.decode(), buf[i].ms) for i in range(n.value)]
+
+    def tune_set(self, n_events, kernel, scale):
+        """Grid scale of one tunable kernel for batches of n_events (default grid x 2^scale)."""
+        self._check(gpu_lib().pg_tune_set(self._h, n_events, kernel.encode(), int(scale)), "pg_tune_set")
+
+    def tune_table(self, n_events):
+        """{kernel: scale} in force for batches of n_events."""
+        out = {}
+        for name in tune_kernel_names():
+            v = ctypes.c_int()
+            self._check(gpu_lib().pg_tune_get(self._h, n_events, name.encode(), ctypes.byref(v)), "pg_tune_get")
+            out[name] = v.value
+        return out
+
+    def autotune(self, raws, repeats=3):
+        """Tunes the launches for batches of len(raws) events; returns the saving per batch in ms."""
+        ptrs, sizes = _raw_arrays(raws)
+        gain = ctypes.c_double()
+        self._check(gpu_lib().pg_autotune(self._h, len(raws), ptrs, sizes, repeats, ctypes.byref(gain)),
+                    "pg_autotune")
+        return gain.value
+
+    def tune_save(self, path):
+        self._check(gpu_lib().pg_tune_save(self._h, path.encode()), "pg_tune_save")
+
+    def tune_load(self, path):
+        """Applies the cache entries of this device; returns how many."""
+        n = gpu_lib().pg_tune_load(self._h, path.encode())
+        if n < 0:
+            self._check(n, "pg_tune_load")
+        return n
 
     def prepare(self, max_batch=0):
         self._check(gpu_lib().pg_prepare(self._h, max_batch), "pg_prepare")

@@ -12,10 +12,11 @@
 //             id, fragment length, more-headers/trailers bits), the CTA scans
 //             the payload lengths in FED order and writes the event's word
 //             count; the framing errors go to a per-event list in FED order.
-//   kFedCopy  (slices x events): each CTA adds up the counts of the events
-//             before its own (the event's first word), one CTA per event
-//             writes wordOffsets, and each warp copies whole FED payloads as
-//             64-bit word pairs with their one-byte FED index per pair.
+//   kFedCopy  (FED groups x events): each CTA adds up the counts of the
+//             events before its own (the event's first word), one CTA per
+//             event writes wordOffsets, and each warp copies one FED payload
+//             as 64-bit word pairs (four loads in flight per lane) with their
+//             one-byte FED index per pair.
 #include "device_utils.cuh"
 #include "pixgpu_internal.cuh"
 
@@ -156,9 +157,22 @@ __global__ void __launch_bounds__(kCopyThreads) kFedCopy(Workspace ws, uint32_t 
     const uint64_t* s = fs.raw64 + src[j];
     const uint32_t d = (base + dst[j]) / 2;  // word pairs; every payload length is even
     const uint8_t idx = uint8_t(fs.fedIds[j] - 1200u);
-    for (uint32_t i = lane; i < pairs; i += 32) {
-      words64[d + i] = s[i];
-      fed[d + i] = idx;
+    // four independent loads in flight per lane
+    for (uint32_t i0 = 0; i0 < pairs; i0 += 128) {
+      uint64_t v[4];
+#pragma unroll
+      for (uint32_t u = 0; u < 4; ++u) {
+        const uint32_t i = i0 + u * 32 + lane;
+        v[u] = i < pairs ? s[i] : 0ull;
+      }
+#pragma unroll
+      for (uint32_t u = 0; u < 4; ++u) {
+        const uint32_t i = i0 + u * 32 + lane;
+        if (i < pairs) {
+          words64[d + i] = v[u];
+          fed[d + i] = idx;
+        }
+      }
     }
   }
 }
@@ -167,8 +181,8 @@ __global__ void __launch_bounds__(kCopyThreads) kFedCopy(Workspace ws, uint32_t 
 
 void launchFedScan(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   PG_PROBED("kFedScan", stream, kFedScan<<<nEvents, kScanThreads, 0, stream>>>(ws));
-  // a few warps per event: ~100 FEDs of a few hundred word pairs each
-  const uint32_t sx = nEvents >= 32 ? 2 : (nEvents >= 8 ? 4 : 16);
+  // one warp per FED (~100 FEDs of a few hundred word pairs each)
+  const uint32_t sx = max(1u, (ws.scan.nFeds + kCopyThreads / 32 - 1) / (kCopyThreads / 32));
   PG_PROBED("kFedCopy", stream, kFedCopy<<<dim3(tunedGrid(ws, kTuneFedCopy, sx), nEvents), kCopyThreads, 0, stream>>>(ws, nEvents));
 }
 

@@ -31,22 +31,37 @@ def main():
     p.add_argument("--seed", type=int, default=pixgpu.BASE_SEED + 1000)
     p.add_argument("--no-graphs", action="store_true")
     p.add_argument("--probe", action="store_true", help="per-kernel device times of a batch")
+    p.add_argument("--fed-scan", choices=["host", "device"], default="host",
+                   help="device: raw records go to the device whole (pg_submit) and the FED scan runs there; "
+                        "host: records are unpacked once into the device-resident pool")
+    p.add_argument("--tuning", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning",
+                                                    "launch_tuning.txt"),
+                   help="launch-shape cache to load ('' for the default shapes)")
     a = p.parse_args()
     det = pixgpu.Detector()
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
         raws = list(ex.map(lambda k: det.event(a.seed + k, a.pu), range(a.events)))
     words = [len(r) // 4 for r in raws]
+    device_scan = a.fed_scan == "device"
     chain = pixgpu.Chain(det.es, max_events=a.batch, max_words_per_batch=max(words) * a.batch + 1024, slots=a.slots,
-                         use_graphs=not a.no_graphs, pool_words=sum(words) + 64 * len(words) + 4096)
-    handles = [chain.pool_put(r) for r in raws]
-    if any(h is None for h in handles):
-        raise RuntimeError("pool admission failed")
-    batches = [handles[i:i + a.batch] for i in range(0, len(handles), a.batch)]
+                         use_graphs=not a.no_graphs, pool_words=0 if device_scan else sum(words) + 64 * len(words) + 4096,
+                         fed_scan=a.fed_scan)
+    if a.tuning and os.path.exists(a.tuning):
+        chain.tune_load(a.tuning)
+    if device_scan:
+        batches = [raws[i:i + a.batch] for i in range(0, len(raws), a.batch)]
+        submit = lambda b: chain.submit(b)  # noqa: E731
+    else:
+        handles = [chain.pool_put(r) for r in raws]
+        if any(h is None for h in handles):
+            raise RuntimeError("pool admission failed")
+        batches = [handles[i:i + a.batch] for i in range(0, len(handles), a.batch)]
+        submit = lambda b: chain.submit_pooled(b, keep=True)  # noqa: E731
     done = 0
     t0 = time.perf_counter()
     for _ in range(a.repeat):
         for b in batches:
-            s = chain.submit_pooled(b, keep=True)
+            s = submit(b)
             chain.wait(s)
             done += len(b)
             chain.release(s)
@@ -56,7 +71,7 @@ def main():
         lat = []
         for b in batches * 3:
             t1 = time.perf_counter()
-            s = chain.submit_pooled(b, keep=True)
+            s = submit(b)
             chain.wait(s)
             lat.append(time.perf_counter() - t1)
             chain.release(s)
@@ -64,7 +79,7 @@ def main():
         census, launches = collections.defaultdict(float), collections.Counter()
         chain.set_probe("*")
         for b in batches:
-            s = chain.submit_pooled(b, keep=True)
+            s = submit(b)
             chain.wait(s)
             for name, ms in chain.probe_read(s):
                 census[name] += ms / len(batches)

@@ -450,8 +450,7 @@ def run_ours(a):
         mb = [mnw[i * B:(i + 1) * B] for i in range(a.mixed_batches)]
         mchain = pixgpu.Chain(det.es, max_events=B, max_words_per_batch=max(sum(x) for x in mb) + 1024,
                               slots=a.slots, device=dev, pool_words=sum(mnw) + 64 * len(mnw) + 4096)
-        for k, v in tuning["grid_scales"].items():
-            mchain.tune_set(B, k, v)
+        load_tuning(mchain)
         mh = []
         for r in mraws:
             h = mchain.pool_put(r)
@@ -477,8 +476,7 @@ def run_ours(a):
     def e2e_leg(scan):
         ec = pixgpu.Chain(det.es, max_events=B, max_words_per_batch=max_words, slots=a.slots, device=dev,
                           fed_scan=scan)
-        for k, v in tuning["grid_scales"].items():
-            ec.tune_set(B, k, v)
+        load_tuning(ec)
         ec.prepare(B)
         h2d = [0]
         d2h = [0]
@@ -524,6 +522,7 @@ def run_ours(a):
         for label, slots, graphs in (("1 stream", 1, False), ("4 streams", 4, False)):
             c1 = pixgpu.Chain(det.es, max_events=1, max_words_per_batch=int(max(nw)) + 1024, slots=slots,
                               device=dev, use_graphs=graphs, pool_words=sum(nw) + 64 * len(nw) + 4096)
+            load_tuning(c1)
             hs = [c1.pool_put(r) for r in raws[:64]]
             sub1 = lambda i: c1.submit_pooled([hs[i % len(hs)]], keep=True)  # noqa: E731
             pipeline(c1, torch, 8, sub1, lambda s: None)
@@ -540,6 +539,7 @@ def run_ours(a):
             sv = {}
             sc = pixgpu.Chain(det.es, max_events=a.serve_batch, max_words_per_batch=int(max(nw)) * a.serve_batch,
                               slots=4, device=dev, pool_words=64 * 1000 * 1000)
+            load_tuning(sc)
             sc.prepare(a.serve_batch)
             for frac in (0.5, 0.8):
                 rate = frac * value
@@ -557,6 +557,7 @@ def run_ours(a):
                 mraws = list(ex.map(lambda k: det.event(SEED0 + 300000 + k, float(pus[k])), range(len(pus))))
             mc = pixgpu.Chain(det.es, max_events=a.serve_batch, max_words_per_batch=a.serve_batch * 300000, slots=4,
                               device=dev, pool_words=128 * 1000 * 1000)
+            load_tuning(mc)
             mc.prepare(a.serve_batch)
             mv = {}
             for rate in (1000.0, 2000.0):
@@ -592,6 +593,12 @@ def run_ours(a):
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
+
+
+def load_tuning(chain):
+    """The committed launch-shape table (every tuned batch size), when present."""
+    if os.path.exists(TUNE_CACHE):
+        chain.tune_load(TUNE_CACHE)
 
 
 def apply_tuning(chain, B, raws, a):

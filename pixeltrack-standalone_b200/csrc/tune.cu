@@ -110,8 +110,8 @@ int pg_tune_save(const pg_ctx* c, const char* path) {
   const std::string dev = deviceName(c);
   f << "# launch tuning: <device>|<events per batch> <kernel> <grid scale (default x 2^scale)>\n";
   for (const auto& kv : c->tuning)
-    for (uint32_t i = 0; i < kNumTune; ++i)
-      if (kv.second.scale[i]) f << dev << "|" << kv.first << " " << kTuneNames[i] << " " << int(kv.second.scale[i]) << "\n";
+    for (uint32_t i = 0; i < kNumTune; ++i)  // every kernel, so that a tuned size never falls back to another
+      f << dev << "|" << kv.first << " " << kTuneNames[i] << " " << int(kv.second.scale[i]) << "\n";
   return f ? PG_OK : PG_ERR_ARG;
 }
 

@@ -95,7 +95,8 @@ def parse():
     p.add_argument("--slots", type=int, default=3, help="batches in flight")
     p.add_argument("--per-event", type=int, default=256, help="events for the one-event-per-launch leg")
     p.add_argument("--serve", type=int, default=4000, help="requests for the serving leg (0: skip)")
-    p.add_argument("--serve-batch", type=int, default=16, help="max events per serving batch")
+    p.add_argument("--serve-batch", type=int, default=32, help="max events per serving batch")
+    p.add_argument("--serve-slots", type=int, default=6, help="batches in flight in the serving loop")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     p.add_argument("--mixed-batches", type=int, default=3,
                    help="distinct 64-event batches with PU uniform in [20, 200] (0: skip that leg)")
@@ -538,7 +539,7 @@ def run_ours(a):
         if a.serve:
             sv = {}
             sc = pixgpu.Chain(det.es, max_events=a.serve_batch, max_words_per_batch=int(max(nw)) * a.serve_batch,
-                              slots=4, device=dev, pool_words=64 * 1000 * 1000)
+                              slots=a.serve_slots, device=dev, pool_words=64 * 1000 * 1000)
             load_tuning(sc)
             sc.prepare(a.serve_batch)
             for frac in (0.5, 0.8):
@@ -549,13 +550,15 @@ def run_ours(a):
                     "p99_ms": st["p99_ms"], "mean_batch": st["mean_batch"], "batches": st["batches"],
                     "admission_waits": st["admission_waits"]}
             sc.close()
-            out["serving"] = {"pu": PU, "requests": a.serve, "max_batch": a.serve_batch, "slots": 4, "points": sv}
+            out["serving"] = {"pu": PU, "requests": a.serve, "max_batch": a.serve_batch, "slots": a.serve_slots,
+                              "points": sv}
             # uneven pileup: PU log-uniform in [30, 250], Poisson arrivals
             rng = np.random.default_rng(7)
             pus = np.exp(rng.uniform(np.log(30), np.log(250), 96))
             with cf.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
                 mraws = list(ex.map(lambda k: det.event(SEED0 + 300000 + k, float(pus[k])), range(len(pus))))
-            mc = pixgpu.Chain(det.es, max_events=a.serve_batch, max_words_per_batch=a.serve_batch * 300000, slots=4,
+            mc = pixgpu.Chain(det.es, max_events=a.serve_batch, max_words_per_batch=a.serve_batch * 300000,
+                              slots=a.serve_slots,
                               device=dev, pool_words=128 * 1000 * 1000)
             load_tuning(mc)
             mc.prepare(a.serve_batch)

@@ -45,6 +45,7 @@ PKG = os.path.join(ROOT, "pixeltrack-standalone_b200")
 TUNE_CACHE = os.path.join(PKG, "tuning", "launch_tuning.txt")
 sys.path.insert(0, PKG)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import replicas  # noqa: E402
 
 METRIC = "events/s and p50/p99 latency at PU50: batched serving vs per-event chain, one B200"
 DATA = ("synthetic: seeded Phase-1 pixel events (1856 modules, 108 FEDs, helices in 3.8 T, Landau charge), "
@@ -339,7 +340,8 @@ def run_ours(a):
     dev = local
     B = a.batch
     det = pixgpu.Detector()
-    raws = make_events(det, a.events)
+    # each rank its own distinct events (replicas, weak scaling)
+    raws = make_events(det, a.events, base=replicas.shard_seeds(rank, world, a.events, SEED0 + 100000)[0])
     nw = [len(r) // 4 for r in raws]  # upper bound of FED words per event
     max_words = int(max(nw)) * B + 1024
     input_bytes = sum(len(r) for r in raws)
@@ -391,13 +393,8 @@ def run_ours(a):
     with Clocks(dev) as clk:
         ms = pipeline(chain, torch, a.steps, sub, done)
     clocks = clk.summary()
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     events = a.steps * B
-    value = world * events / (ms / 1e3)
+    value, ms = replicas.job_rate(events, ms, device="cuda")
     kernel_ms = float(np.mean(probe_ms)) if probe_ms else None
     launches_of_top = launches[top]
     hbm, peak_kind = peaks()
@@ -501,12 +498,8 @@ def run_ours(a):
                 batch = host_batches[i % nbh]
                 h2d[0] += sum(len(r) - 4 - 8 * struct.unpack_from("<I", r, 0)[0] for r in batch)
                 h2d[0] += 8 * n_scan * len(batch)
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
-        return {"value": world * events / (ems / 1e3), "unit": "events/s",
+        rate, ems = replicas.job_rate(events, ems, device="cuda")
+        return {"value": rate, "unit": "events/s",
                 "h2d_bytes_per_step": h2d[0] / a.steps, "d2h_bytes_per_step": d2h[0] / a.steps,
                 "host_wall_events_per_s": events / wall,
                 "path": ("pg_submit: host FED scan + H2D of words" if scan == "host" else

@@ -307,13 +307,27 @@ def fit_leg(det, dev, torch, n=1000000):
                 rates[label] = n / (e0.elapsed_time(e1) / 5 / 1e3)
                 outs[label] = [x.cpu().numpy().astype(np.float64) for x in o]
             sa, sb = outs["fp64"][0].reshape(n, 5), outs["mixed"][0].reshape(n, 5)
+            cov = outs["fp64"][1].reshape(n, 15)
             fin = np.isfinite(sa).all(axis=1) & np.isfinite(sb).all(axis=1)
             dk = np.abs(1 / outs["mixed"][2] - 1 / outs["fp64"][2])[fin]
+            vk = np.abs(1 / outs["fp64"][2])[fin]
             d = np.abs(sb - sa)[fin]
-            err = {"inv_pt_per_gev": dk, "phi": d[:, 0], "d0_cm": d[:, 1], "cot_theta": d[:, 3], "z0_cm": d[:, 4]}
+            # packed symmetric 5x5 covariance: diagonal entries 0, 2, 5, 9, 14
+            sig = np.sqrt(np.maximum(cov[fin][:, [0, 2, 5, 9, 14]], 0.0))
+            err = {"inv_pt_per_gev": (dk, vk, sig[:, 2]), "phi": (d[:, 0], np.abs(sa[fin][:, 0]), sig[:, 0]),
+                   "d0_cm": (d[:, 1], np.abs(sa[fin][:, 1]), sig[:, 1]),
+                   "cot_theta": (d[:, 3], np.abs(sa[fin][:, 3]), sig[:, 3]),
+                   "z0_cm": (d[:, 4], np.abs(sa[fin][:, 4]), sig[:, 4])}
+
+            def stats(v, ref, sg):
+                rel = v / np.maximum(ref, 1e-30)
+                pull = v / np.maximum(sg, 1e-30)
+                return {"max": float(v.max()), "rms": float(np.sqrt((v ** 2).mean())),
+                        "frac_rel_over_1e-5": float((rel > 1e-5).mean()),
+                        "rel_p999": float(np.quantile(rel, 0.999)),
+                        "max_over_fp64_sigma": float(pull.max()), "p9999_over_fp64_sigma": float(np.quantile(pull, 0.9999))}
             per[method] = {"fits_per_s": rates, "both_finite": int(fin.sum()),
-                           "mixed_vs_fp64": {k: {"max": float(v.max()), "rms": float(np.sqrt((v ** 2).mean()))}
-                                             for k, v in err.items()}}
+                           "mixed_vs_fp64": {k: stats(*v) for k, v in err.items()}}
         res["%d_hits" % nh] = per
     c.close()
     return {"tuples": n, "per_multiplicity": res,

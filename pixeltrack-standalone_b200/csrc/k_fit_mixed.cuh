@@ -2,14 +2,16 @@
 // namespaces, after the FP64 fit whose matrix type and Cholesky inversions it
 // reuses).
 //
-// The arithmetic of the fit runs in FP32: the fast circle fit, arc lengths,
-// multiple-scattering variances, the band matrices, line residuals and chi2.
-// FP64 is kept for the two Cholesky inversions with the solves that use
-// them, for the covariance propagation (Jacobian sandwiches and the Karimaki
-// translation), for the three-point reference circle, and for the radial
-// residuals to that circle, which are differences of numbers of the size of
-// the radius.  The steps follow BrokenLine.h:46-504 exactly as the
-// FP64 path does; only the precision differs.
+// The arithmetic of the fit runs in FP32: the multiple-scattering
+// variances, the rotations and projections of the hit errors, the band
+// matrices, the residual weights and the chi2.  FP64 is kept for the two
+// Cholesky inversions with the solves that use them, for the covariance
+// propagation (Jacobian sandwiches and the Karimaki translation), for the
+// three-point reference circle, and for what is measured from that circle:
+// the arc lengths and the radial residuals, which are small differences and
+// angles of vectors as long as the radius.  The steps follow
+// BrokenLine.h:46-504 exactly as the FP64 path does; only the precision
+// differs.
 
 template <int R, int C>
 struct MF {
@@ -115,6 +117,7 @@ __device__ void blFitMixed(const float* H3, const float* ge, double x0, double y
   // FP64: for a straight-looking track its centre is a ratio of small
   // differences, and every later FP32 step inherits its error
   float ff[4];
+  double fc0, fc1, fc2;  // the circle in FP64, for the arc lengths below
   {
     auto Hd = [&](int r, int c) { return double(H3[3 * c + r]); };
     double ax = Hd(0, n / 2) - Hd(0, 0), ay = Hd(1, n / 2) - Hd(1, 0);
@@ -130,6 +133,9 @@ __device__ void blFitMixed(const float* H3, const float* ge, double x0, double y
     ff[0] = float(f0);
     ff[1] = float(f1);
     ff[2] = float(f2);
+    fc0 = f0;
+    fc1 = f1;
+    fc2 = f2;
     ff[3] = float(f2 * atan2(cross2D(dx, dy, ex, ey), dx * ex + dy * ey) / (Hd(2, n - 1) - Hd(2, 0)));
   }
   int q;
@@ -140,19 +146,26 @@ __device__ void blFitMixed(const float* H3, const float* ge, double x0, double y
     q = cross2DF(dx, dy, ex, ey) > 0 ? -1 : 1;
     const float slope = -q / ff[3];
     MF<2, 2> R = rotationMatrixF(slope);
+    // the arc lengths in FP64: the radius vectors are as long as the radius
+    // (metres for a stiff track) and the angles between them small, so in
+    // FP32 their cross products, and the circle centre itself, would carry
+    // errors of the size of the arc lengths' last digits times the radius
+    double rd[2][N];
 #pragma unroll
     for (int i = 0; i < n; ++i) {
-      radii[0][i] = H(0, i) - ff[0];
-      radii[1][i] = H(1, i) - ff[1];
+      rd[0][i] = double(H(0, i)) - fc0;
+      rd[1][i] = double(H(1, i)) - fc1;
+      radii[0][i] = float(rd[0][i]);
+      radii[1][i] = float(rd[1][i]);
     }
     // the circle centre in the beam-line frame gives the direction of the
     // point of closest approach
-    const float cax = float(double(ff[0]) + x0), cay = float(double(ff[1]) + y0);
-    float nrm = sqrtf(cax * cax + cay * cay);
-    float e0 = (-ff[2] * cax) / nrm, e1 = (-ff[2] * cay) / nrm;
+    const double cax = fc0 + x0, cay = fc1 + y0;
+    const double nrm = sqrt(cax * cax + cay * cay);
+    const double e0 = (-fc2 * cax) / nrm, e1 = (-fc2 * cay) / nrm;
 #pragma unroll
     for (int i = 0; i < n; ++i)
-      s[i] = q * ff[2] * atan2f(cross2DF(radii[0][i], radii[1][i], e0, e1), radii[0][i] * e0 + radii[1][i] * e1);
+      s[i] = float(q * fc2 * atan2(cross2D(rd[0][i], rd[1][i], e0, e1), rd[0][i] * e0 + rd[1][i] * e1));
 #pragma unroll
     for (int i = 0; i < n; ++i) {
       float p0 = s[i], p1 = H(2, i);

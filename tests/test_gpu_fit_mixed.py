@@ -1,23 +1,28 @@
 """Mixed-precision broken-line fit (FP32 arithmetic; FP64 for the reference
-circle, the radial residuals, the Cholesky solves and the covariance
-propagation) against the FP64 fit on the same tuples.
+circle, the arc lengths and radial residuals measured from it, the Cholesky
+solves and the covariance propagation) against the FP64 fit on the same
+tuples.
 
 The FP64 fit equals the oracle within 1e-5 (test_gpu_parity.py); here the
-deviation of the variant is bounded.  Measured on 200k seeded tuples per
-multiplicity (maxima): |d(1/pT)| 4e-6 /GeV, |d phi| 5e-7, |d d0| 2e-6 cm for
-every multiplicity; cot(theta) and z0 rms 5e-5 and 8e-4 cm for triplets,
-5e-7 and 5e-6 cm for quadruplets.  The bounds below leave a margin of ~10.
+deviation of the variant is bounded, absolutely and in units of the FP64
+fit's own uncertainty.  Measured on 1M seeded tuples per multiplicity
+(maxima, 3 / 4 hits): |d(1/pT)| 1.6e-5 / 2.4e-6 /GeV, |d phi| 1.4e-6 / 4.8e-7,
+|d d0| 4.6e-6 / 1.6e-6 cm, |d cot(theta)| 1.9e-5 / 1.4e-5, |d z0| 2.1e-4 /
+2.3e-4 cm; at most 0.07 sigma of the FP64 fit for any parameter.  The bounds
+below leave a margin of ~5-10.
 """
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
-BOUNDS = {  # nhits: (max |d 1/pT|, max |d phi|, max |d d0|, rms d cot, rms d z0)
-    3: (5e-5, 1e-5, 5e-5, 1e-3, 1e-2),
-    4: (5e-5, 1e-5, 5e-5, 1e-5, 1e-4),
-    5: (5e-5, 1e-5, 5e-5, 1e-5, 1e-4),
+BOUNDS = {  # nhits: (max |d 1/pT|, max |d phi|, max |d d0|, max |d cot|, max |d z0|)
+    3: (1e-4, 1e-5, 5e-5, 2e-4, 2e-3),
+    4: (5e-5, 1e-5, 5e-5, 2e-4, 2e-3),
+    5: (5e-5, 1e-5, 5e-5, 2e-4, 2e-3),
 }
+MAX_PULL = 0.5  # max |mixed - FP64| / sigma(FP64) over the five parameters
+DIAG = [0, 2, 5, 9, 14]  # diagonal of the packed 5x5 covariance
 
 
 @pytest.fixture(scope="module")
@@ -38,9 +43,13 @@ def test_mixed_fit_within_bounds_of_fp64(chain, nhits, N):
     assert np.isfinite(sb).all() and np.isfinite(b["pt"]).all()
     dk = np.abs(1.0 / b["pt"].astype(np.float64) - 1.0 / a["pt"].astype(np.float64))
     d = np.abs(sb - sa)
-    mk, mphi, md0, rcot, rz0 = BOUNDS[nhits]
+    mk, mphi, md0, mcot, mz0 = BOUNDS[nhits]
     assert dk.max() < mk, dk.max()
     assert d[:, 0].max() < mphi, d[:, 0].max()
     assert d[:, 1].max() < md0, d[:, 1].max()
-    assert np.sqrt((d[:, 3] ** 2).mean()) < rcot
-    assert np.sqrt((d[:, 4] ** 2).mean()) < rz0
+    assert d[:, 3].max() < mcot, d[:, 3].max()
+    assert d[:, 4].max() < mz0, d[:, 4].max()
+    sig = np.sqrt(np.maximum(a["cov"].astype(np.float64).reshape(-1, 15)[:, DIAG], 0.0))
+    ok = (sig > 0).all(axis=1)
+    pull = (d[ok] / sig[ok]).max()
+    assert pull < MAX_PULL, pull

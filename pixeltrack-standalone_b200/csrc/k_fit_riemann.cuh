@@ -725,8 +725,15 @@ __device__ void rfLineFit(const double* H, const float* ge, const RfCircle& circ
 #pragma unroll
   for (int i = 0; i < n; ++i) {
     A(0, i) = 1.;
-    A(1, i) = S(rot(0, 0)) * sArc[i] + S(rot(0, 1)) * zz[i];
-    zc(i, 0) = S(rot(1, 0)) * sArc[i] + S(rot(1, 1)) * zz[i];
+    if constexpr (std::is_same<S, double>::value) {
+      A(1, i) = S(rot(0, 0)) * sArc[i] + S(rot(0, 1)) * zz[i];
+      zc(i, 0) = S(rot(1, 0)) * sArc[i] + S(rot(1, 1)) * zz[i];
+    } else {
+      // the s-z rotation in FP64 from the FP64 arc lengths: rotating with the
+      // rounded matrix and back with the exact one would tilt the line
+      A(1, i) = rot(0, 0) * sArcD[i] + rot(0, 1) * H[3 * i + 2];
+      zc(i, 0) = rot(1, 0) * sArcD[i] + rot(1, 1) * H[3 * i + 2];
+    }
   }
   M<N, N> Vyi;
   invert(cms, Vyi);

@@ -1012,7 +1012,7 @@ __global__ void kFastDupInDegree(Workspace ws, uint32_t* indeg, const uint32_t* 
 }
 
 // One thread-block cluster of P CTAs per event (kFastDupCtas for small
-// batches, 1 for large ones).  A worklist
+// batches, 2 for large ones).  A worklist
 // holds the candidates whose earlier track-sharing candidates are all done;
 // cells of one round share no track, so the cluster's threads process them in
 // parallel, and each releases its later neighbours (the in-degree reaching
@@ -1247,7 +1247,7 @@ cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   uint32_t* indeg = ws.scratchA;        // [maxEvents][kEdgeCap] >= kCellCap
   uint32_t* lists = ws.scratchB;        // two worklists of kCellCap per event
   PG_PROBED("kFastDupInDegree", stream, kFastDupInDegree<<<dim3(tunedGrid(ws, kTuneFastDupInDegree, gx), nEvents), 256, 0, stream>>>(ws, indeg, candFlag));
-  const uint32_t P = nEvents <= kClusterMaxEvents ? kFastDupCtas : 1;
+  const uint32_t P = nEvents <= kClusterMaxEvents ? kFastDupCtas : 2;
   cudaError_t le = cudaSuccess;
   PG_PROBED("kFastDupRounds", stream,
             le = launchClustered(kFastDupRounds, P, nEvents, kFastDupThreads, 0, stream, ws, indeg, lists, candFlag,

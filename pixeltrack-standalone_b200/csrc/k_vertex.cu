@@ -731,8 +731,9 @@ cudaError_t runVertices(Workspace& ws, uint32_t nEvents, cudaStream_t stream, in
     configured.fetch_or(bit);
   }
   // small batches: a cluster of kVtxCtas CTAs per event shortens the event's
-  // latency; large batches: one CTA per event keeps the SMs for other events
-  const uint32_t P = nEvents <= kClusterMaxEvents ? kVtxCtas : 1;
+  // latency; large batches: pairs of CTAs (measured at 64 PU50 events: 0.52 ->
+  // 0.39 ms per batch and +2 % throughput with three batches in flight)
+  const uint32_t P = nEvents <= kClusterMaxEvents ? kVtxCtas : 2;
   cudaError_t le = cudaSuccess;
   PG_PROBED("kVertices", stream,
             le = launchClustered(kVertices, P, nEvents, kVtxThreads, kVtxSmemBytes, stream, ws, algo));

@@ -292,7 +292,7 @@ __global__ void kDoubletCount(Workspace ws) {
 // Pass 2: each slot's doublets from its staging entries to their serial
 // positions (the scan of the counts); slots that were not staged are found
 // again.  Lanes take 32 slots, the warp serves the non-empty ones in turn.
-__global__ void kDoubletWrite(Workspace ws) {
+__global__ void __launch_bounds__(256, 5) kDoubletWrite(Workspace ws) {
   __shared__ PairTable pt;
   const uint32_t e = blockIdx.y;
   const EventCounters* c = ws.ev + e;
@@ -458,7 +458,7 @@ __global__ void kOhRec(Workspace ws) {
 // list, at most 32), each group testing another cell of the slot, so short
 // candidate lists still keep the lanes busy.  Accepted links (oc <- idx) are
 // appended unordered with one atomic per warp and round.
-__global__ void kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
+__global__ void __launch_bounds__(256, 5) kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
   const uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   const uint32_t ntot = c->ntot;

@@ -418,7 +418,7 @@ __device__ __forceinline__ void blFitBin(const DeviceES& es, const Workspace& ws
 
 // the three multiplicity bins in one launch: blockIdx.z = 0, 1, 2 fits the
 // 3-hit tuples, the 4-hit tuples and the first 4 hits of the 5-hit tuples
-__global__ void __launch_bounds__(128) kBLFit(DeviceES es, Workspace ws) {
+__global__ void __launch_bounds__(128, 4) kBLFit(DeviceES es, Workspace ws) {
   if (blockIdx.z == 0)
     blFitBin<3>(es, ws, 3);
   else

@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(kScanThreads)
   if (threadIdx.x == 0) sums[size_t(e) * kScanMaxSlices + r] = tot;
 }
 
-__global__ void __launch_bounds__(kScanThreads)
+__global__ void __launch_bounds__(kScanThreads, 3)
     kScanSlices(uint32_t* in, uint32_t* out, uint32_t stride, const uint32_t* lenPtr, uint32_t lenStride,
                 uint32_t fixedLen, const uint32_t* sums, uint32_t* totalPtr, uint32_t totalStride, bool zeroIn) {
   __shared__ uint32_t sh[33];

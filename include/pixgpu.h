@@ -74,8 +74,10 @@ enum pg_flag {
   PG_FLAG_J_OVERFLOW = 1u << 14,       /* more doublet inner-hit slots than kept */
   PG_FLAG_BAD_INPUT = 1u << 15,        /* payload words outside the cabling tables (read as padding) */
   /* bit 16 is the results' "more loose tracks than stored" */
-  PG_FLAG_SPLIT_MODULE = 1u << 17      /* a module's digis in several runs: the later runs are read as
+  PG_FLAG_SPLIT_MODULE = 1u << 17,     /* a module's digis in several runs: the later runs are read as
                                           padding (the reference's result is loop-order dependent) */
+  PG_FLAG_TOO_MANY_RUNS = 1u << 18     /* more than 2000 module runs: the first 2000 found are kept (the
+                                          reference's countModules counter wraps, gpuClustering.h:33) */
 };
 
 typedef struct pg_ctx pg_ctx;

@@ -444,7 +444,7 @@ __global__ void kSortModules(Workspace ws, uint32_t nEvents) {
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) ms[1 + i] = i < kept ? s[i] : 0u;
   if (threadIdx.x == 0) {
     ms[0] = kept;
-    if (c->nModules > kMaxModules) c->flags |= kFlagModuleTooBig;
+    if (c->nModules > kMaxModules) c->flags |= kFlagTooManyRuns;
     c->nModules = kept;
     if (sNDrop) c->flags |= kFlagSplitModule;
   }

@@ -48,14 +48,16 @@ enum : uint32_t {
   kFlagDeepTuple = 1u << 13,        // a CA path longer than 5 hits (reference aborts)
   kFlagJOverflow = 1u << 14,        // more doublet inner-hit slots than kJCap
   kFlagBadInput = 1u << 15,         // words/cabling entries outside the tables (ignored)
-  kFlagSplitModule = 1u << 17       // a module's digis in several runs (later runs read as padding)
+  kFlagSplitModule = 1u << 17,      // a module's digis in several runs (later runs read as padding)
+  kFlagTooManyRuns = 1u << 18       // more than 2000 module runs (the reference's counter wraps)
 };
 
 static_assert(uint32_t(kFlagBadInput) == uint32_t(PG_FLAG_BAD_INPUT) &&
                   uint32_t(kFlagJOverflow) == uint32_t(PG_FLAG_J_OVERFLOW) &&
                   uint32_t(kFlagTupleOverflow) == uint32_t(PG_FLAG_TUPLE_OVERFLOW) &&
                   uint32_t(kFlagModuleTooBig) == uint32_t(PG_FLAG_MODULE_TOO_BIG) &&
-                  uint32_t(kFlagSplitModule) == uint32_t(PG_FLAG_SPLIT_MODULE),
+                  uint32_t(kFlagSplitModule) == uint32_t(PG_FLAG_SPLIT_MODULE) &&
+                  uint32_t(kFlagTooManyRuns) == uint32_t(PG_FLAG_TOO_MANY_RUNS),
               "flag bits of the ABI");
 
 struct EventCounters {

@@ -732,8 +732,10 @@ cudaError_t runVertices(Workspace& ws, uint32_t nEvents, cudaStream_t stream, in
   }
   // small batches: a cluster of kVtxCtas CTAs per event shortens the event's
   // latency; large batches: pairs of CTAs (measured at 64 PU50 events: 0.52 ->
-  // 0.39 ms per batch and +2 % throughput with three batches in flight)
-  const uint32_t P = nEvents <= kClusterMaxEvents ? kVtxCtas : 2;
+  // 0.39 ms per batch and +2 % throughput with three batches in flight).  Only
+  // the density clusterer splits its work across the cluster; the others run
+  // on one CTA.
+  const uint32_t P = algo != 0 ? 1u : (nEvents <= kClusterMaxEvents ? kVtxCtas : 2u);
   cudaError_t le = cudaSuccess;
   PG_PROBED("kVertices", stream,
             le = launchClustered(kVertices, P, nEvents, kVtxThreads, kVtxSmemBytes, stream, ws, algo));

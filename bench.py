@@ -101,6 +101,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     p.add_argument("--mixed-batches", type=int, default=3,
                    help="distinct 64-event batches with PU uniform in [20, 200] (0: skip that leg)")
+    p.add_argument("--tune-out", default="", help="where to write the table --autotune finds")
     p.add_argument("--autotune", action="store_true",
                    help="tune the launch shapes now (else load the committed cache) and write the table")
     return p.parse_args()
@@ -621,9 +622,8 @@ def apply_tuning(chain, B, raws, a):
     if n == 0:
         src = "autotuned in this run"
         gain = chain.autotune(raws[:B], repeats=3)
-        out_dir = os.path.join(ROOT, "gpurun_out")
-        if os.path.isdir(out_dir):
-            chain.tune_save(os.path.join(out_dir, "launch_tuning.txt"))
+        if a.tune_out:
+            chain.tune_save(a.tune_out)
     table = {k: v for k, v in chain.tune_table(B).items() if v}
     return {"source": src, "events_per_batch": B, "grid_scales": table, "tuner_gain_ms_per_batch": gain,
             "kernels_tunable": len(pixgpu.tune_kernel_names())}

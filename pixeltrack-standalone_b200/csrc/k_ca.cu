@@ -458,7 +458,7 @@ __global__ void kOhRec(Workspace ws) {
 // list, at most 32), each group testing another cell of the slot, so short
 // candidate lists still keep the lanes busy.  Accepted links (oc <- idx) are
 // appended unordered with one atomic per warp and round.
-__global__ void __launch_bounds__(256, 5) kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
+__global__ void __launch_bounds__(256, 6) kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
   const uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   const uint32_t ntot = c->ntot;

@@ -326,10 +326,13 @@ int pg_vertices_noalloc(const uint32_t* tuple_off, const uint8_t* quality, const
 int pg_fit_broken_line(pg_ctx* ctx, int N, uint32_t n, const double* hits, const float* ge, double B, float* state,
                        float* cov, float* pt, float* eta, float* chi2, void* stream);
 
-/* The same fits in mixed precision: FP32 arithmetic, FP64 only for the circle
- * and line Cholesky inversions with their solves and for the covariance
- * propagation.  A variant beside HelixFitOnGPU's FP64 fit; its deviation from
- * the FP64 result is measured in tests/test_gpu_fit_mixed.py. */
+/* The same fits in mixed precision: FP32 arithmetic for the multiple-scattering
+ * model, the band matrices and the parameter updates; FP64 for the circle and
+ * line Cholesky inversions with their solves, the covariance propagation, and
+ * the three-point reference circle with what is measured from it (the arc
+ * lengths and the radial residuals), which lose the sagitta of stiff tracks
+ * in FP32.  A variant beside HelixFitOnGPU's FP64 fit; its deviation from the
+ * FP64 result is measured in tests/test_gpu_fit_mixed.py. */
 int pg_fit_broken_line_mixed(pg_ctx* ctx, int N, uint32_t n, const double* hits, const float* ge, double B, float* state,
                        float* cov, float* pt, float* eta, float* chi2, void* stream);
 

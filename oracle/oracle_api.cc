@@ -49,6 +49,9 @@ void record(Handle& h) {
   auto& ca = h.ev.ca;
   auto& v = h.ev.vtx;
   h.out.clear();
+  // the FED loop's word stream (WordFedAppender): words and one FED index per word pair
+  h.put("fedWords", h.ev.words.word.data(), h.ev.words.nWords);
+  h.put("fedWordFedIds", h.ev.words.fedId.data(), (h.ev.words.nWords + 1) / 2);
   h.put1<uint32_t>("nDigis", d.nDigis);
   h.put1<uint32_t>("nModules", d.nModules);
   h.put("xx", d.xx.data(), d.nDigis);

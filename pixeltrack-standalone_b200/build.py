@@ -88,9 +88,19 @@ def build_oracle():
     return target
 
 
-def build_ref(reference="/root/reference"):
+def reference_dir():
+    """The reference checkout the checker builds read: $PIXTRACK_REFERENCE, else
+    the container's read-only mount.  None where neither exists (the GPU box)."""
+    for d in (os.environ.get("PIXTRACK_REFERENCE"), "/root/reference"):
+        if d and os.path.isdir(os.path.join(d, "src", "serial")):
+            return d
+    return None
+
+
+def build_ref(reference=None):
     """Checker build of the reference serial sources (skipped where they are absent)."""
-    if not os.path.isdir(os.path.join(reference, "src", "serial")):
+    reference = reference or reference_dir()
+    if reference is None:
         return None
     _run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle", "ref"), "REF=" + reference])
     return os.path.join(ROOT, "oracle", "_ref", "libpixref.so")

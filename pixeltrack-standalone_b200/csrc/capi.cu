@@ -19,8 +19,15 @@ cudaError_t fitDirectRiemann(int N, uint32_t n, const double* hits, const float*
                              float* cov, float* pt, float* eta, float* chi2, bool mixed, cudaStream_t stream);
 
 int fail(pg_ctx* c, int code, const std::string& msg) {
-  if (c) c->err = msg;
+  if (c) {
+    std::lock_guard<std::mutex> lk(c->errMu);
+    c->err = msg;
+  }
   return code;
+}
+std::string lastError(pg_ctx* c) {
+  std::lock_guard<std::mutex> lk(c->errMu);
+  return c->err;
 }
 int cudaFail(pg_ctx* c, cudaError_t e, const char* where) {
   return fail(c, PG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));

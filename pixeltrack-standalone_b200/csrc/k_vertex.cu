@@ -22,7 +22,8 @@ namespace pixgpu {
 
 namespace {
 
-constexpr uint32_t kMaxVtxTracks = 32 * 1024;
+static_assert(kVtxScratchAWords <= kEdgeCap && kVtxScratchBWords <= kEdgeCap,
+              "vertex scratch exceeds the per-event scratchA/scratchB stride");
 constexpr int kVtxThreads = 1024;
 // events with at most this many vertex tracks keep every per-track array in
 // shared memory (38 bytes per track); larger ones use the global scratch
@@ -58,7 +59,8 @@ __device__ __forceinline__ VtxScratch carve(char* p, uint32_t cap) {
 }
 
 __device__ __forceinline__ VtxScratch scratchOf(const Workspace& ws, uint32_t e) {
-  // carve per-event scratch out of scratchA/scratchB (kEdgeCap words each)
+  // carve per-event scratch out of scratchA/scratchB (kEdgeCap words each;
+  // kVtxScratchAWords and kVtxScratchBWords of them are used)
   uint32_t* a = ws.scratchA + size_t(e) * kEdgeCap;
   uint32_t* b = ws.scratchB + size_t(e) * kEdgeCap;
   VtxScratch s;
@@ -70,10 +72,12 @@ __device__ __forceinline__ VtxScratch scratchOf(const Workspace& ws, uint32_t e)
   s.nn = reinterpret_cast<int32_t*>(a + 5 * kMaxVtxTracks);
   s.root = reinterpret_cast<int32_t*>(a + 6 * kMaxVtxTracks);
   s.list = a + 7 * kMaxVtxTracks;
+  static_assert(8 * size_t(kMaxVtxTracks) == kVtxScratchAWords, "scratch A layout");
   s.itrk = reinterpret_cast<uint16_t*>(b);
   s.hbins = reinterpret_cast<uint16_t*>(b) + kMaxVtxTracks;
   s.izt = reinterpret_cast<uint8_t*>(b + kMaxVtxTracks);
   s.newV = reinterpret_cast<uint8_t*>(b + kMaxVtxTracks) + kMaxVtxTracks;
+  static_assert(size_t(kMaxVtxTracks) + 2 * size_t(kMaxVtxTracks) / 4 == kVtxScratchBWords, "scratch B layout");
   return s;
 }
 

@@ -19,14 +19,17 @@ namespace pixgpu {
 namespace {
 
 // Scratch layout: the per-event counters, then the two per-track scratch
-// areas the vertex kernel uses for events above its shared-memory size
-// (8 arrays of kVtxTracksMax 32-bit words, then 16-bit/8-bit arrays).
-constexpr uint32_t kVtxTracksMax = 32768;  // the vertex kernel's own track cap
+// areas the vertex kernel uses for events above its shared-memory size, with
+// the sizes that kernel carves (pixgpu_internal.cuh: kVtxScratchAWords,
+// kVtxScratchBWords for kMaxVtxTracks tracks).
 constexpr size_t kCountersBytes = 256;
-constexpr size_t kScratchABytes = size_t(8) * kVtxTracksMax * 4;
-constexpr size_t kScratchBBytes = (size_t(kVtxTracksMax) + kVtxTracksMax / 2) * 4;
+constexpr size_t kScratchABytes = kVtxScratchAWords * 4;
+constexpr size_t kScratchBBytes = kVtxScratchBWords * 4;
 constexpr size_t kNoAllocBytes = kCountersBytes + kScratchABytes + kScratchBBytes;  // 1.25 MB
 static_assert(sizeof(EventCounters) <= kCountersBytes, "counters do not fit their scratch slot");
+static_assert(kNoAllocBytes <= 1280 * 1024, "the documented 1.25 MB bound of the static scratch");
+// the tuple limit the entry point checks stays within the kernel's track cap
+static_assert(kTupleBins <= kMaxVtxTracks, "n_tuples limit above the vertex scratch");
 
 static __device__ __align__(256) unsigned char gVtxScratch[kNoAllocBytes];
 

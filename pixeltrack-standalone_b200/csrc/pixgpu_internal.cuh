@@ -28,6 +28,14 @@ constexpr uint32_t kMaxVtx = PF_MAX_VTX;
 constexpr uint32_t kErrCap = 4096;                       // digi errors kept per event
 constexpr uint32_t kMaxFedWords = PF_MAX_FED_WORDS;      // 300000 words per event
 constexpr uint32_t kBigSegCap = 8192;                    // long list segments queued per event and sort
+// The vertex finder's track cap (ZVertexSoA MAXTRACKS) and the per-event
+// scratch it carves out of scratchA/scratchB for events above its
+// shared-memory size (k_vertex.cu scratchOf): eight 32-bit arrays in A; two
+// 16-bit and two 8-bit arrays in B.  noalloc.cu sizes its static array from
+// the same numbers.
+constexpr uint32_t kMaxVtxTracks = 32 * 1024;
+constexpr size_t kVtxScratchAWords = size_t(8) * kMaxVtxTracks;
+constexpr size_t kVtxScratchBWords = size_t(kMaxVtxTracks) + kMaxVtxTracks / 2;
 
 // flag bits in EventCounters::flags (capacity conditions where the result no
 // longer follows the reference's truncation order exactly)

@@ -107,12 +107,15 @@ struct pg_ctx {
   std::map<uint32_t, pixgpu::LaunchTuning> tuning;  // launch tuning per batch size (tune.cu)
   std::string probeName;  // kernel timed by the probe ("" = none)
   std::string err;
+  std::mutex errMu;  // guards err: the serving loop's threads report errors concurrently
   std::mutex mu;  // slot bookkeeping (the serving loop's threads share it)
 };
 
 namespace pixgpu {
 
 int fail(pg_ctx* c, int code, const std::string& msg);
+// the context's last error message (a copy taken under errMu)
+std::string lastError(pg_ctx* c);
 // the launch tuning for batches of n events: n's table, else the largest tuned size below n, else defaults
 LaunchTuning tuningFor(const pg_ctx* c, uint32_t n);
 int cudaFail(pg_ctx* c, cudaError_t e, const char* where);

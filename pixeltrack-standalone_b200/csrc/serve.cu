@@ -126,7 +126,7 @@ int pg_serve(pg_ctx* c, uint32_t nRaw, const uint8_t* const* raws, const size_t*
   auto abortWith = [&](int code) {
     std::lock_guard<std::mutex> lk(abortMu);
     if (abortRc.load() == PG_OK) {
-      abortMsg = c->err;
+      abortMsg = lastError(c);
       abortRc.store(code);
     }
   };
@@ -241,6 +241,8 @@ int pg_serve(pg_ctx* c, uint32_t nRaw, const uint8_t* const* raws, const size_t*
       int s = pg_submit_pooled(c, uint32_t(handles.size()), handles.data(), 0, &slot);
       if (s != PG_OK) {
         abortWith(s);
+        // a refused batch leaves its events admitted: give their extents back
+        for (uint32_t h : handles) pg_pool_release(c, h);
         break;
       }
       inflight[slot] = std::move(reqs);
@@ -253,13 +255,13 @@ int pg_serve(pg_ctx* c, uint32_t nRaw, const uint8_t* const* raws, const size_t*
   }
   if (abortRc.load() != PG_OK) nextReq.store(N);
   for (auto& t : ups) t.join();
-  // drain anything still in flight after an abort
+  // drain anything still in flight after an abort, and give back the pool
+  // extents of events that were admitted but never batched
   for (size_t k = 0; k < S; ++k)
     if (!inflight[k].empty()) pg_release(c, uint32_t(k));
-  if (abortRc.load() != PG_OK) {
-    c->err = abortMsg;
-    return abortRc.load();
-  }
+  for (const Ready& r : ready) pg_pool_release(c, r.handle);
+  ready.clear();
+  if (abortRc.load() != PG_OK) return fail(c, abortRc.load(), abortMsg);
 
   std::vector<double> ms(N);
   double sum = 0, mx = 0;

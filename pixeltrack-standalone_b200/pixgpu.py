@@ -347,18 +347,56 @@ def gpu_lib():
     return _gpu
 
 
+NOALLOC_MAX_TUPLES = 32767   # pg_vertices_noalloc's static scratch limit
+NOALLOC_VERTEX_SLOTS = 1024  # entries of the per-vertex outputs (ZVertexSoA::MAXVTX)
+
+
 def vertices_noalloc(tuple_off, quality, pt, state, cov, idv, zv, wv, chi2, ptv2, ndof, sort_ind, stream=None):
     """pg_vertices_noalloc on device tensors (torch): one event's track SoA in,
     the vertices out; returns (n_vertices, flags).  Allocates nothing on the
-    device; raises with the library's message on failure."""
+    device; raises with the library's message on failure.
+
+    Every tensor must be a contiguous CUDA tensor on the same device, with the
+    dtype and length the C entry point reads or writes: n = quality.numel()
+    tuples, tuple_off >= n + 1 (uint32 as int32), pt >= n, state >= 5n,
+    cov >= 15n, idv >= n (int16), and the per-vertex outputs at least 1024
+    entries.  The call runs on `stream` (a CUDA stream handle), by default on
+    torch's current stream of that device."""
+    import torch
     n = int(quality.numel())
+    if n > NOALLOC_MAX_TUPLES:
+        raise ValueError("vertices_noalloc: %d tuples above the limit of %d" % (n, NOALLOC_MAX_TUPLES))
+    spec = (("tuple_off", tuple_off, (torch.int32,), n + 1), ("quality", quality, (torch.uint8,), n),
+            ("pt", pt, (torch.float32,), n), ("state", state, (torch.float32,), 5 * n),
+            ("cov", cov, (torch.float32,), 15 * n), ("idv", idv, (torch.int16,), n),
+            ("zv", zv, (torch.float32,), NOALLOC_VERTEX_SLOTS), ("wv", wv, (torch.float32,), NOALLOC_VERTEX_SLOTS),
+            ("chi2", chi2, (torch.float32,), NOALLOC_VERTEX_SLOTS),
+            ("ptv2", ptv2, (torch.float32,), NOALLOC_VERTEX_SLOTS),
+            ("ndof", ndof, (torch.int32,), NOALLOC_VERTEX_SLOTS),
+            ("sort_ind", sort_ind, (torch.int16, torch.uint16), NOALLOC_VERTEX_SLOTS))
+    dev = quality.device
+    if dev.type != "cuda":
+        raise ValueError("vertices_noalloc: tensors must be on a CUDA device")
+    for name, t, dtypes, need in spec:
+        if t.device != dev:
+            raise ValueError("vertices_noalloc: %s is on %s, quality on %s" % (name, t.device, dev))
+        if t.dtype not in dtypes:
+            raise ValueError("vertices_noalloc: %s has dtype %s, expected %s" % (name, t.dtype, dtypes[0]))
+        if not t.is_contiguous():
+            raise ValueError("vertices_noalloc: %s is not contiguous" % name)
+        if t.numel() < need:
+            raise ValueError("vertices_noalloc: %s has %d entries, needs %d" % (name, t.numel(), need))
     nv = ctypes.c_uint32()
     fl = ctypes.c_uint32()
     msg = ctypes.create_string_buffer(256)
-    rc = gpu_lib().pg_vertices_noalloc(tuple_off.data_ptr(), quality.data_ptr(), pt.data_ptr(), state.data_ptr(),
-                                       cov.data_ptr(), n, idv.data_ptr(), zv.data_ptr(), wv.data_ptr(),
-                                       chi2.data_ptr(), ptv2.data_ptr(), ndof.data_ptr(), sort_ind.data_ptr(),
-                                       ctypes.addressof(nv), ctypes.addressof(fl), stream, msg, len(msg))
+    with torch.cuda.device(dev):
+        if stream is None:
+            stream = torch.cuda.current_stream(dev).cuda_stream
+        rc = gpu_lib().pg_vertices_noalloc(tuple_off.data_ptr(), quality.data_ptr(), pt.data_ptr(),
+                                           state.data_ptr(), cov.data_ptr(), n, idv.data_ptr(), zv.data_ptr(),
+                                           wv.data_ptr(), chi2.data_ptr(), ptv2.data_ptr(), ndof.data_ptr(),
+                                           sort_ind.data_ptr(), ctypes.addressof(nv), ctypes.addressof(fl), stream,
+                                           msg, len(msg))
     if rc != 0:
         raise RuntimeError("pg_vertices_noalloc failed (%d): %s" % (rc, msg.value.decode()))
     return nv.value, fl.value

@@ -28,11 +28,32 @@ def test_exports(header, lib):
     assert missing == []
 
 
-def test_unpack_matches_oracle_word_stream(default_detector):
-    """pg_unpack_raw (host FED scan of the product) needs no device."""
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed,pu,errors", [(7, 5, 3), (11, 50, 0)])
+def test_unpack_matches_oracle_word_stream(default_detector, seed, pu, errors):
+    """pg_unpack_raw (the product's host FED scan, called through the C ABI)
+    gives the oracle FED loop's word stream and per-pair FED indices, on a
+    clean PU50 event and on an event with injected raw-data errors.  A
+    context needs a device, so this runs on the GPU box."""
+    import ctypes
     import numpy as np
+    import oracle
     import pixgpu
-    lib = pixgpu.gpu_lib()
-    raw = default_detector.event(7, 5, inject_errors=3)
-    # a context needs a device; the FED scan is checked through a context-free path
-    assert hasattr(lib, "pg_unpack_raw")
+    raw = default_detector.event(seed, pu, inject_errors=errors)
+    want = oracle.Oracle(default_detector.es)
+    want.process(raw)
+    ww = want._products(["fedWords", "fedWordFedIds"])
+    c = pixgpu.Chain(default_detector.es, max_events=1, max_words_per_batch=300000)
+    try:
+        cap = 300000
+        words = np.zeros(cap, np.uint32)
+        fed = np.zeros(cap // 2 + 2, np.uint8)
+        n = ctypes.c_uint32()
+        rc = pixgpu.gpu_lib().pg_unpack_raw(c._h, raw, len(raw), words.ctypes.data, fed.ctypes.data, cap,
+                                            ctypes.byref(n))
+        assert rc == 0
+    finally:
+        c.close()
+    assert n.value == len(ww["fedWords"]) > 0
+    assert np.array_equal(words[:n.value], ww["fedWords"])
+    assert np.array_equal(fed[:(n.value + 1) // 2], ww["fedWordFedIds"])

@@ -130,6 +130,32 @@ def test_pool_admission_and_gather(default_detector, events, alone):
         c.close()
 
 
+def test_serving_abort_gives_back_the_pool(default_detector):
+    """A request larger than a batch slot aborts the serving loop with
+    PG_ERR_CAPACITY; the events admitted before it (waiting in the ready
+    queue or refused with their batch) must leave the pool, so that the
+    context stays usable."""
+    import pixgpu
+    small = [default_detector.event(700 + k, 3) for k in range(4)]
+    big = default_detector.event(710, 50)
+    assert len(big) // 4 > 40000 > max(len(r) for r in small) // 4
+    c = pixgpu.Chain(default_detector.es, max_events=4, max_words_per_batch=40000, pool_words=600000)
+    try:
+        raws = small + [big]
+        with pytest.raises(RuntimeError, match="larger than a batch slot"):
+            c.serve(raws, n_requests=40, arrivals=np.linspace(0.0, 0.002, 40),
+                    request_event=[k % 4 if k < 30 else 4 for k in range(40)])
+        info = c.pool_info()
+        assert info["live_events"] == 0 and info["free_words"] == info["cap_words"], info
+        # the context serves again afterwards
+        stats, lat = c.serve(small, n_requests=20, rate_hz=5000.0)
+        assert stats["completed"] == 20
+        info = c.pool_info()
+        assert info["live_events"] == 0 and info["free_words"] == info["cap_words"], info
+    finally:
+        c.close()
+
+
 @pytest.mark.parametrize("rate_hz", [2000.0, 200000.0])
 def test_serving_results_same_alone_and_in_the_mix(default_detector, events, alone, rate_hz):
     """Continuous batching: results delivered by the serving loop equal the

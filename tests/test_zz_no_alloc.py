@@ -90,13 +90,40 @@ def test_noalloc_large_track_set_twice(large_track_set):
 
 
 def test_noalloc_rejects_too_many_tuples():
+    """The C entry point refuses more tuples than its static scratch holds,
+    and so does the Python wrapper, before any call."""
+    import ctypes
     import torch
     import pixgpu
     dev = torch.device("cuda", 0)
     n = 32768
     z = lambda k, dt: torch.zeros(k, dtype=dt, device=dev)  # noqa: E731
-    with pytest.raises(RuntimeError, match="32767"):
-        pixgpu.vertices_noalloc(z(n + 1, torch.int32), z(n, torch.uint8), z(n, torch.float32), z(5 * n, torch.float32),
-                                z(15 * n, torch.float32), z(n, torch.int16), z(1024, torch.float32),
-                                z(1024, torch.float32), z(1024, torch.float32), z(1024, torch.float32),
-                                z(1024, torch.int32), z(1024, torch.int16))
+    args = [z(n + 1, torch.int32), z(n, torch.uint8), z(n, torch.float32), z(5 * n, torch.float32),
+            z(15 * n, torch.float32), z(n, torch.int16), z(1024, torch.float32), z(1024, torch.float32),
+            z(1024, torch.float32), z(1024, torch.float32), z(1024, torch.int32), z(1024, torch.int16)]
+    with pytest.raises(ValueError, match="32767"):
+        pixgpu.vertices_noalloc(*args)
+    nv, fl = ctypes.c_uint32(), ctypes.c_uint32()
+    msg = ctypes.create_string_buffer(256)
+    ptrs = [t.data_ptr() for t in args]
+    rc = pixgpu.gpu_lib().pg_vertices_noalloc(*ptrs[:5], n, *ptrs[5:], ctypes.addressof(nv), ctypes.addressof(fl),
+                                               torch.cuda.current_stream(dev).cuda_stream, msg, len(msg))
+    assert rc != 0 and b"32767" in msg.value
+
+
+def test_noalloc_wrapper_checks_its_tensors():
+    """Short outputs, wrong dtypes and host tensors are refused before the call."""
+    import torch
+    import pixgpu
+    dev = torch.device("cuda", 0)
+    n = 10
+    z = lambda k, dt, d=dev: torch.zeros(k, dtype=dt, device=d)  # noqa: E731
+    good = [z(n + 1, torch.int32), z(n, torch.uint8), z(n, torch.float32), z(5 * n, torch.float32),
+            z(15 * n, torch.float32), z(n, torch.int16), z(1024, torch.float32), z(1024, torch.float32),
+            z(1024, torch.float32), z(1024, torch.float32), z(1024, torch.int32), z(1024, torch.int16)]
+    for k, bad in ((6, z(100, torch.float32)), (0, z(n, torch.int32)), (5, z(n - 1, torch.int16)),
+                   (2, z(n, torch.float64)), (3, z(5 * n, torch.float32, "cpu"))):
+        args = list(good)
+        args[k] = bad
+        with pytest.raises(ValueError):
+            pixgpu.vertices_noalloc(*args)

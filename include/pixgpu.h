@@ -117,6 +117,22 @@ typedef struct pg_config {
                                     ErrorChecker records none (ErrorChecker.cc:36) */
   uint32_t fed_scan;             /* 0: the FED header/trailer checks and word concatenation on the host
                                     (default); 1: on the device, from the whole FED buffers */
+  /* Per-event container capacities.  0 keeps the reference's value (given
+     beside each), whose truncation order the results reproduce.  Larger
+     values run the same algorithm on events whose containers would overflow
+     (the reference changes them only by recompiling, CAConstants.h:18-40);
+     indices are 32-bit throughout, and every per-event array of a slot is
+     sized by them (pg_slot_bytes).  Smaller values are refused. */
+  uint32_t cap_fed_words;        /* 300000: MAX_FED_WORDS (SiPixelRawToClusterGPUKernel.cc:34) */
+  uint32_t cap_hits;             /* 49152: maxNumberOfHits (gpuClusteringConstants.h:10,27); <= 2^21 */
+  uint32_t cap_doublets;         /* 458752: maxNumberOfDoublets (CAHitNtupletGeneratorOnGPU.cc:48) */
+  uint32_t cap_lists;            /* 65536: maxNumOfActiveDoublets, the cells that may hold a neighbour
+                                    or a track list (CAConstants.h:40) */
+  uint32_t cap_tuples;           /* 32768: HitContainer bins = TrackSoA stride (PixelTrackHeterogeneous.h:20,62);
+                                    < 2^20 */
+  uint32_t cap_multiplicity;     /* 24576: maxNumberOfTuples, the TupleMultiplicity content and the fits
+                                    per multiplicity (CAConstants.h:22); <= cap_tuples */
+  uint32_t cap_hit_to_tuple;     /* 98304: the HitToTuple content (CAConstants.h:64) */
 } pg_config;
 
 typedef struct pg_event_counts {
@@ -155,6 +171,14 @@ int pg_process_batch(pg_ctx* ctx, uint32_t n_events, const uint8_t* const* raws,
 int pg_event_counts_get(pg_ctx* ctx, uint32_t k, pg_event_counts* out);
 int pg_get_product(pg_ctx* ctx, uint32_t k, const char* name, void* dst, size_t cap_bytes, size_t* count,
                    int* elem_bytes);
+/* The same products of event k of the finished asynchronous batch on `slot`
+ * (after pg_wait, or pg_query returning PG_OK, and before pg_release):
+ * PG_ERR_BUSY while the batch runs.  The full-size products the framework
+ * modules hand to host consumers (SiPixelDigisSoA, SiPixelClustersSoA,
+ * PixelTrackHeterogeneous, ZVertexHeterogeneous) come from here; pg_result
+ * is the compact form. */
+int pg_slot_product(pg_ctx* ctx, uint32_t slot, uint32_t k, const char* name, void* dst, size_t cap_bytes,
+                    size_t* count, int* elem_bytes);
 
 /* Device-resident path (inputs staged once, then the kernels alone):
  * pg_stage_batch unpacks and copies a batch into slot s; pg_run_staged
@@ -184,7 +208,7 @@ typedef struct pg_result_view {
   const float* pt;               /* [n_tracks] */
   const float* eta;
   const float* chi2;
-  const uint16_t* hits;          /* [n_tracks][5] hit indices, 0xffff past n_hits */
+  const uint32_t* hits;          /* [n_tracks][5] hit indices, 0xffffffff past track_n_hits */
   const int16_t* vertex;         /* [n_tracks] vertex index or -1 */
   const float* zv;               /* [n_vertices] */
   const float* wv;

@@ -46,6 +46,12 @@ typedef struct ps_event_config {
   double noise_frac;         /* noise digis as a fraction of signal digis */
   int inject_errors;         /* >0: add that many FED error words per event */
   int fixed_pu;              /* 1: exactly round(pu) vertices; 0: Poisson(pu) */
+  /* soft component per vertex (0 by default: no random numbers drawn, the
+     events of the plain configuration are unchanged) */
+  double soft_per_vertex;    /* Poisson mean of soft tracks per vertex */
+  double soft_pt_min;        /* GeV; soft pT = soft_pt_min + Exp(soft_pt_mean) */
+  double soft_pt_mean;       /* GeV */
+  double secondary_frac;     /* share of soft tracks produced 2-12 cm from the vertex */
 } ps_event_config;
 
 typedef struct ps_truth {
@@ -65,6 +71,12 @@ typedef struct ps_truth {
 /* Fill *cfg with the defaults used by the benchmark workloads. */
 void ps_default_detector_config(ps_detector_config* cfg);
 void ps_default_event_config(ps_event_config* cfg);
+/* The calibrated event model: fewer prompt tracks above 0.5 GeV plus a soft
+ * exponential component, most of it produced displaced, so that a PU50 event
+ * has about 57k digis, 18k hits and 1.6k loose tracks (the benchmark
+ * workload's stated sizes).  The default configuration above is the denser
+ * model of earlier versions (all tracks prompt and above 0.5 GeV). */
+void ps_calibrated_event_config(ps_event_config* cfg);
 
 int ps_detector_create(const ps_detector_config* cfg, ps_detector** out);
 void ps_detector_destroy(ps_detector* det);

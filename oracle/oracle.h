@@ -19,6 +19,34 @@
 
 namespace oracle {
 
+// Container capacities.  The defaults are the reference's compile-time
+// constants and module parameters, whose overflow behaviour parity covers:
+// MAX_FED_WORDS (SiPixelRawToClusterGPUKernel.cc:34), maxNumberOfHits
+// (gpuClusteringConstants.h:10,27), maxNumberOfDoublets (the module parameter,
+// CAHitNtupletGeneratorOnGPU.cc:48), maxNumOfActiveDoublets (CAConstants.h:40,
+// the CellNeighbors and CellTracks pools), the HitContainer bins = TrackSoA
+// stride (PixelTrackHeterogeneous.h:20,62; also the vertex finder's track
+// stride, ZVertexSoA.h:11), maxNumberOfTuples (CAConstants.h:22: the
+// TupleMultiplicity content and the fits' concurrency) and the HitToTuple
+// content (4 x maxNumberOfTuples, CAConstants.h:64).  The reference changes
+// them only by recompiling (CAConstants.h:18-40 selects smaller sets with
+// GPU_SMALL_EVENTS); a larger set runs the same algorithm on events whose
+// containers would overflow, with indices held in 32 bits throughout.
+struct Caps {
+  uint32_t fedWords = PF_MAX_FED_WORDS;
+  uint32_t hits = PF_MAX_HITS;
+  uint32_t doublets = PF_MAX_DOUBLETS_PARAM;
+  uint32_t lists = PF_MAX_ACTIVE_DOUBLETS;
+  uint32_t tuples = PF_TRACK_STRIDE;
+  uint32_t multiplicity = PF_MAX_TUPLES;
+  uint32_t hitToTuple = 4 * PF_MAX_TUPLES;
+  bool isDefault() const {
+    return fedWords == PF_MAX_FED_WORDS && hits == PF_MAX_HITS && doublets == PF_MAX_DOUBLETS_PARAM &&
+           lists == PF_MAX_ACTIVE_DOUBLETS && tuples == PF_TRACK_STRIDE && multiplicity == PF_MAX_TUPLES &&
+           hitToTuple == 4 * PF_MAX_TUPLES;
+  }
+};
+
 struct ES {
   std::unique_ptr<PfCablingMap> cab;
   std::vector<uint8_t> modToUnp;
@@ -64,30 +92,30 @@ struct Hits {
   std::vector<uint16_t> detInd;
   uint32_t layerStart[11] = {};
   std::vector<uint32_t> phiOff;    // 10*128+1
-  std::vector<uint16_t> phiBins;   // nHits
+  std::vector<uint32_t> phiBins;   // nHits
   PfAverageGeometry agc;           // beam-spot corrected average geometry
 };
 
-constexpr uint32_t kTupleBins = PF_TRACK_STRIDE;  // OneToManyAssoc<uint16, 32768, 163840>
-
 struct CA {
   uint32_t nCells = 0;
-  std::vector<uint16_t> inner, outer, used;
+  uint32_t tupleBins = PF_TRACK_STRIDE;              // HitContainer bins (Caps::tuples)
+  std::vector<uint32_t> inner, outer;
+  std::vector<uint16_t> used;
   std::vector<int16_t> layerPair;
   std::vector<int32_t> doubletId;
   std::vector<float> innerZ, innerR;
   std::vector<std::vector<uint32_t>> outerHitCells;  // per hit, capped at 128
   std::vector<std::vector<uint32_t>> nbr;            // per cell, capped at 36
-  std::vector<std::vector<uint16_t>> trk;            // per cell, capped at 48
+  std::vector<std::vector<uint32_t>> trk;            // per cell, capped at 48
   int32_t nbrPool = 1, trkPool = 1;                  // SimpleVector sizes (slot 0 = empty list)
   // tuples
   uint32_t apcM = 0, apcN = 0;                       // AtomicPairCounter {m, n}
-  std::vector<uint32_t> tupleOff;                    // kTupleBins + 1
-  std::vector<uint16_t> tupleHits;                   // 5 * kTupleBins
+  std::vector<uint32_t> tupleOff;                    // tupleBins + 1
+  std::vector<uint32_t> tupleHits;                   // 5 * tupleBins
   std::vector<uint16_t> tupleDet;
-  std::vector<uint8_t> quality;                      // kTupleBins
+  std::vector<uint8_t> quality;                      // tupleBins
   std::vector<uint32_t> tmOff;                       // TupleMultiplicity off[9]
-  std::vector<uint16_t> tmBins;
+  std::vector<uint32_t> tmBins;
   // fit results
   std::vector<float> state, cov, pt, eta, chi2;      // state[i*5+k], cov[i*15+k]
   uint32_t size(uint32_t t) const { return tupleOff[t + 1] - tupleOff[t]; }
@@ -112,11 +140,12 @@ struct Event {
 
 // plugin-SiPixelClusterizer/SiPixelRawToClusterCUDA.cc:78-138 (FED loop, ErrorChecker, WordFedAppender);
 // formatterErrors: the ErrorChecker's includeErrors (false in the reference's ErrorChecker.cc:36)
-void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w, bool formatterErrors = false);
+void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w, bool formatterErrors = false,
+             const Caps& caps = Caps());
 // SiPixelRawToClusterGPUKernel::makeClusters (SiPixelRawToClusterGPUKernel.cc:509-600)
-void makeClusters(const ES& es, const Words& w, Digis& d, Clusters& c);
+void makeClusters(const ES& es, const Words& w, Digis& d, Clusters& c, const Caps& caps = Caps());
 // PixelRecHitGPUKernel::makeHits (plugin-SiPixelRecHits/PixelRecHits.cc:33-53)
-void makeHits(const ES& es, const Digis& d, const Clusters& c, Hits& h);
+void makeHits(const ES& es, const Digis& d, const Clusters& c, Hits& h, const Caps& caps = Caps());
 // the CA module's configurable switches (CAHitNtupletGeneratorOnGPU.cc:46-58,
 // defaults as there; the cut values stay the reference's constants)
 struct CAParams {
@@ -125,6 +154,7 @@ struct CAParams {
   bool earlyFishbone = true, lateFishbone = false;
   bool idealConditions = true, doClusterCut = true, doZ0Cut = true, doPtCut = true;
   bool useRiemannFit = false;                  // Riemann fit in place of the broken-line fit
+  Caps caps;                                   // container capacities
   // CAHitNtupletGeneratorKernels.cc:52-57: the layer pairs that are built
   int nPairs() const { return minHitsPerNtuplet > 3 ? 13 : (includeJumpingForwardDoublets ? 19 : 15); }
 };
@@ -135,6 +165,7 @@ void makeTuples(const ES& es, const Hits& h, CA& ca, const CAParams& p = CAParam
 // algo: 0 clusterTracksByDensity (the PixelVertexProducerCUDA default),
 // 1 clusterTracksDBSCAN, 2 clusterTracksIterative
 void makeVertices(const CA& ca, Vertices& v, int algo = 0);
+// the vertex finder's track stride is the TrackSoA stride (ca.tupleBins)
 
 // broken-line fit of one tuple of N (3 or 4) hits; results in the TrackSoA layout
 void brokenLineFit(int N, const double* hits /*3xN col-major*/, const float* hits_ge /*6xN*/, double B,
@@ -146,7 +177,7 @@ void riemannFit(int N, const double* hits /*3xN col-major*/, const float* hits_g
 
 // whole chain for one raw.bin event record
 struct Options {
-  CAParams ca;
+  CAParams ca;                   // ca.caps: the container capacities of the whole chain
   int vertexAlgo = 0;            // see makeVertices
   bool formatterErrors = false;  // see fedLoop
 };

@@ -30,6 +30,9 @@ def _ca_args(ca):
         p[k] = int(v)
     return [p[k] for k in CA_DEFAULTS]
 
+# container capacities, in the order of or_set_caps (oracle::Caps)
+CAPS_FIELDS = ["fed_words", "hits", "doublets", "lists", "tuples", "multiplicity", "hit_to_tuple"]
+
 PRODUCTS = ["nDigis", "nModules", "xx", "yy", "adc", "moduleInd", "clus", "pdigi", "rawIdArr", "errors",
             "formatterErrors", "nClusters",
             "moduleStart", "clusInModule", "moduleId", "clusModuleStart", "nHits", "xl", "yl", "xerr", "yerr", "xg",
@@ -71,7 +74,8 @@ class _Named:
 class Oracle(_Named):
     """Sequential restatement of the serial chain (oracle/*.cc)."""
 
-    def __init__(self, es_images, riemann_fit=False, vertex_algo=0, ca=None, formatter_errors=False):
+    def __init__(self, es_images, riemann_fit=False, vertex_algo=0, ca=None, formatter_errors=False, caps=None):
+        """caps: container capacities (CAPS_FIELDS names) above the reference's."""
         path = os.path.join(HERE, "liboracle.so")
         if not os.path.exists(path):
             _build.build_oracle()
@@ -109,6 +113,13 @@ class Oracle(_Named):
             raise ValueError("min_hits_per_ntuplet: 3 or 4")
         self.lib.or_set_formatter_errors.argtypes = [ctypes.c_void_p, ctypes.c_int]
         self.lib.or_set_formatter_errors(self._h, 1 if formatter_errors else 0)
+        if caps:
+            self.lib.or_set_caps.argtypes = [ctypes.c_void_p] + [ctypes.c_uint32] * len(CAPS_FIELDS)
+            unknown = set(caps) - set(CAPS_FIELDS)
+            if unknown:
+                raise ValueError("unknown capacities %s" % sorted(unknown))
+            if self.lib.or_set_caps(self._h, *[int(caps.get(k, 0)) for k in CAPS_FIELDS]) != 0:
+                raise ValueError("capacities below the reference's")
 
     def process(self, raw, names=None):
         if self.lib.or_process(self._h, raw, len(raw)) != 0:

@@ -98,7 +98,7 @@ void record(Handle& h) {
   h.put("cellUsed", ca.used.data(), ca.nCells);
   {
     std::vector<uint32_t> off(1, 0), val, toff(1, 0);
-    std::vector<uint16_t> tval;
+    std::vector<uint32_t> tval;
     for (uint32_t c2 = 0; c2 < ca.nCells; ++c2) {
       for (auto x : ca.nbr[c2]) val.push_back(x);
       off.push_back(uint32_t(val.size()));
@@ -121,7 +121,7 @@ void record(Handle& h) {
     h.put1<int32_t>("nTrkLists", ca.trkPool);
   }
   uint32_t nt = 0;
-  while (nt < oracle::kTupleBins && ca.size(nt) > 0) ++nt;
+  while (nt < ca.tupleBins && ca.size(nt) > 0) ++nt;
   h.put1<uint32_t>("nTuples", nt);
   h.put("tupleOff", ca.tupleOff.data(), nt + 1);
   h.put("tupleHits", ca.tupleHits.data(), ca.tupleOff[nt]);
@@ -146,9 +146,9 @@ void record(Handle& h) {
 
 namespace oracle {
 void processEvent(const ES& es, const uint8_t* raw, size_t n, Event& ev, const Options& o) {
-  fedLoop(es, raw, n, ev.words, o.formatterErrors);
-  makeClusters(es, ev.words, ev.digis, ev.clusters);
-  makeHits(es, ev.digis, ev.clusters, ev.hits);
+  fedLoop(es, raw, n, ev.words, o.formatterErrors, o.ca.caps);
+  makeClusters(es, ev.words, ev.digis, ev.clusters, o.ca.caps);
+  makeHits(es, ev.digis, ev.clusters, ev.hits, o.ca.caps);
   makeTuples(es, ev.hits, ev.ca, o.ca);
   makeVertices(ev.ca, ev.vtx, o.vertexAlgo);
 }
@@ -189,6 +189,27 @@ int or_set_ca_params(void* p, int minHitsPerNtuplet, int includeJumpingForwardDo
   c.doClusterCut = doClusterCut != 0;
   c.doZ0Cut = doZ0Cut != 0;
   c.doPtCut = doPtCut != 0;
+  return 0;
+}
+
+// container capacities (oracle::Caps; the reference's values by default).
+// Zero leaves a field unchanged; -1 when a capacity is below the reference's
+// (smaller containers would change results the reference defines).
+int or_set_caps(void* p, uint32_t fedWords, uint32_t hits, uint32_t doublets, uint32_t lists, uint32_t tuples,
+                uint32_t multiplicity, uint32_t hitToTuple) {
+  oracle::Caps c = static_cast<Handle*>(p)->opts.ca.caps;
+  if (fedWords) c.fedWords = fedWords;
+  if (hits) c.hits = hits;
+  if (doublets) c.doublets = doublets;
+  if (lists) c.lists = lists;
+  if (tuples) c.tuples = tuples;
+  if (multiplicity) c.multiplicity = multiplicity;
+  if (hitToTuple) c.hitToTuple = hitToTuple;
+  const oracle::Caps d;
+  if (c.fedWords < d.fedWords || c.hits < d.hits || c.doublets < d.doublets || c.lists < d.lists ||
+      c.tuples < d.tuples || c.multiplicity < d.multiplicity || c.hitToTuple < d.hitToTuple)
+    return -1;
+  static_cast<Handle*>(p)->opts.ca.caps = c;
   return 0;
 }
 

@@ -29,8 +29,8 @@ constexpr float kMaxZ[kNPairs] = {20., 30., 0., 22., 30., -10., 70., 70., 22., 3
                                   -15., 70., 70., 20., 22., 30., 0., 70., 70.};
 constexpr float kMaxR[kNPairs] = {20., 9., 9., 20., 7., 7., 5., 5., 20., 6., 6., 5., 5., 20., 20., 9., 9., 9., 9.};
 
-// CAHitNtupletGeneratorOnGPU.cc:45-65 (module configuration; the switches are CAParams)
-constexpr uint32_t kMaxDoublets = PF_MAX_DOUBLETS_PARAM;
+// CAHitNtupletGeneratorOnGPU.cc:45-65 (module configuration; the switches are
+// CAParams, the container capacities CAParams::caps)
 constexpr float kPtMin = 0.899999976158f;
 constexpr float kThetaCutBarrel = 0.00200000009499f;
 constexpr float kThetaCutForward = 0.00300000002608f;
@@ -95,6 +95,11 @@ inline float dca0(const Circle& e) {
 
 void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
   const bool useRiemannFit = prm.useRiemannFit;
+  const Caps& caps = prm.caps;
+  const uint32_t kTupleBins = caps.tuples;
+  // "no tuple" in the duplicate removers (the reference's 60000 lies above
+  // every tuple index of its 32768 bins; 32-bit indices need a larger one)
+  constexpr uint32_t kNoTuple = 0xffffffffu;
   const int nPairs = prm.nPairs();
   const uint32_t nHits = hh.nHits;
   // ---- allocateOnGPU / launchZero (CAHitNtupletGeneratorKernelsAlloc.h:4-25) and tuples zero
@@ -112,12 +117,13 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
   ca.nbrPool = 1;
   ca.trkPool = 1;
   ca.apcM = ca.apcN = 0;
+  ca.tupleBins = kTupleBins;
   ca.tupleOff.assign(kTupleBins + 1, 0);
   ca.tupleHits.assign(5 * kTupleBins, 0);
   ca.tupleDet.assign(5 * kTupleBins, 0);
   ca.quality.assign(kTupleBins, 0);
   ca.tmOff.assign(9, 0);
-  ca.tmBins.assign(PF_MAX_TUPLES, 0);
+  ca.tmBins.assign(caps.multiplicity, 0);
   ca.state.assign(size_t(kTupleBins) * 5, 0.f);
   ca.cov.assign(size_t(kTupleBins) * 15, 0.f);
   ca.pt.assign(kTupleBins, 0.f);
@@ -169,7 +175,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
       for (uint32_t kk = kl; kk != khh; kk = (kk + 1) % 128) {
         uint32_t b = kk + hoff;
         for (uint32_t p = hh.phiOff[b]; p < hh.phiOff[b + 1]; ++p) {
-          uint16_t oi = hh.phiBins[p];
+          uint32_t oi = hh.phiBins[p];
           uint16_t mo = hh.detInd[oi];
           if (mo > 2000) continue;
           // z0cutoff
@@ -199,9 +205,9 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
             if (dphi * dphi * (minRadius2T4 - ri * ro) > (ro - ri) * (ro - ri)) continue;
           }
           uint32_t ind = ca.nCells;
-          if (ind >= kMaxDoublets) break;
+          if (ind >= caps.doublets) break;
           ca.nCells++;
-          ca.inner.push_back(uint16_t(i));
+          ca.inner.push_back(i);
           ca.outer.push_back(oi);
           ca.layerPair.push_back(int16_t(pairLayerId));
           ca.doubletId.push_back(int32_t(ind));
@@ -220,7 +226,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
 
   // ---- kernel_connect (CAHitNtupletGeneratorKernelsImpl.h:191-262)
   for (uint32_t idx = 0; idx < nCells; ++idx) {
-    uint16_t innerHit = ca.inner[idx];
+    uint32_t innerHit = ca.inner[idx];
     const auto& vi = ca.outerHitCells[innerHit];
     float ri = ca.innerR[idx], zi = ca.innerZ[idx];
     float ro = hh.rg[ca.outer[idx]], zo = hh.zg[ca.outer[idx]];
@@ -239,7 +245,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
       if (!(std::abs(dca0(eq)) < region * std::abs(eq.c))) continue;
       // GPUCACell::addOuterNeighbor (GPUCACell.h:67-86): pool of maxNumOfActiveDoublets lists
       if (ca.nbr[oc].empty() && !hasNbrList[oc]) {
-        if (ca.nbrPool < PF_MAX_ACTIVE_DOUBLETS) {
+        if (ca.nbrPool < int32_t(caps.lists)) {
           ca.nbrPool++;
           hasNbrList[oc] = 1;
         }
@@ -298,9 +304,9 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
   //      GPUCACell::find_ntuplets<6> (GPUCACell.h:278-331) and bulkFill (HistoContainer.h:181-190)
   uint32_t tmp[6];
   int depth = 0;
-  auto addTrack = [&](uint32_t c, uint16_t it) {
+  auto addTrack = [&](uint32_t c, uint32_t it) {
     if (ca.trk[c].empty() && !hasTrkList[c]) {
-      if (ca.trkPool < PF_MAX_ACTIVE_DOUBLETS) {
+      if (ca.trkPool < int32_t(caps.lists)) {
         ca.trkPool++;
         hasTrkList[c] = 1;
       } else
@@ -318,7 +324,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
       dfs(other);
     }
     if (last && uint32_t(depth) >= prm.minHitsPerNtuplet - 1) {
-      uint16_t hits[6];
+      uint32_t hits[6];
       uint32_t nh = 0;
       for (int k = 0; k < depth; ++k) hits[nh++] = ca.inner[tmp[k]];
       hits[nh] = ca.outer[cell];
@@ -329,7 +335,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
       if (m < kTupleBins) {
         ca.tupleOff[m] = off;
         for (uint32_t k = 0; k < n; ++k) ca.tupleHits[off + k] = hits[k];
-        for (int k = 0; k < depth; ++k) addTrack(tmp[k], uint16_t(m));
+        for (int k = 0; k < depth; ++k) addTrack(tmp[k], m);
         ca.quality[m] = kBad;
       }
     }
@@ -370,13 +376,14 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
   }
   for (int b = 1; b < 9; ++b) ca.tmOff[b] += ca.tmOff[b - 1];
   // beyond this capacity the reference writes past TupleMultiplicity::bins
-  if (ca.tmOff[8] > PF_MAX_TUPLES) throw std::runtime_error("undefined in the reference: TupleMultiplicity overflow");
+  if (ca.tmOff[8] > caps.multiplicity)
+    throw std::runtime_error("undefined in the reference: TupleMultiplicity overflow");
   for (uint32_t it = 0; it < kTupleBins; ++it) {
     uint32_t nh = ca.size(it);
     if (nh < 3) continue;
     if (ca.quality[it] == kDup) continue;
     uint32_t w = ca.tmOff[nh]--;
-    ca.tmBins[w - 1] = uint16_t(it);
+    ca.tmBins[w - 1] = it;
   }
 
   if (nHits > 1 && prm.lateFishbone) fishbone(true);
@@ -391,14 +398,14 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
   const double B = double(float(0.0114256972711507));
   auto fitBin = [&](uint32_t nHitsBin, int N) {
     uint32_t sz = ca.tmOff[nHitsBin + 1] - ca.tmOff[nHitsBin];
-    for (uint32_t local = 0; local < PF_MAX_TUPLES; ++local) {
+    for (uint32_t local = 0; local < caps.multiplicity; ++local) {
       if (local >= sz) break;
-      uint16_t tkid = ca.tmBins[ca.tmOff[nHitsBin] + local];
+      uint32_t tkid = ca.tmBins[ca.tmOff[nHitsBin] + local];
       double hits[3 * 5];
       float ge[6 * 5];
-      const uint16_t* hitId = &ca.tupleHits[ca.tupleOff[tkid]];
+      const uint32_t* hitId = &ca.tupleHits[ca.tupleOff[tkid]];
       for (int i = 0; i < N; ++i) {
-        uint16_t hit = hitId[i];
+        uint32_t hit = hitId[i];
         const PfFrame& f = es.det[hh.detInd[hit]].frame;
         // SOAFrame::toGlobal(cxx, cxy, cyy, gl) (DataFormats/SOARotation.h:511-519)
         float cxx = hh.xerr[hit], cxy = 0, cyy = hh.yerr[hit];
@@ -456,7 +463,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
     const auto& tr = ca.trk[idx];
     if (tr.size() < 2) continue;
     float mc = 10000.f;
-    uint16_t im = 60000;
+    uint32_t im = kNoTuple;
     for (auto it : tr) {
       float score = std::abs(ca.state[size_t(it) * 5 + 1]);
       if (ca.quality[it] == kLoose && score < mc) {
@@ -469,8 +476,8 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
   }
 
   // ---- hit -> tuple map (Impl.h:421-447) and kernel_tripletCleaner (:479-534)
-  std::vector<uint32_t> h2tOff(PF_MAX_HITS + 1, 0);
-  std::vector<uint16_t> h2t(4 * PF_MAX_TUPLES, 0);
+  std::vector<uint32_t> h2tOff(caps.hits + 1, 0);
+  std::vector<uint32_t> h2t(caps.hitToTuple, 0);
   for (uint32_t idx = 0; idx < kTupleBins; ++idx) {
     if (ca.size(idx) == 0) break;
     if (ca.quality[idx] != kLoose) continue;
@@ -483,10 +490,10 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
     if (ca.quality[idx] != kLoose) continue;
     for (uint32_t k = ca.tupleOff[idx]; k < ca.tupleOff[idx + 1]; ++k) {
       uint32_t w = h2tOff[ca.tupleHits[k]]--;
-      h2t[w - 1] = uint16_t(idx);
+      h2t[w - 1] = idx;
     }
   }
-  for (uint32_t idx = 0; idx < PF_MAX_HITS; ++idx) {
+  for (uint32_t idx = 0; idx < caps.hits; ++idx) {
     uint32_t b = h2tOff[idx], e = h2tOff[idx + 1];
     if (e - b < 2) continue;
     uint32_t maxNh = 0;
@@ -495,9 +502,9 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
       if (ca.size(h2t[p]) != maxNh) ca.quality[h2t[p]] = kDup;
     if (maxNh > 3) continue;
     float mc = 10000.f;
-    uint16_t im = 60000;
+    uint32_t im = kNoTuple;
     for (uint32_t p = b; p < e; ++p) {
-      uint16_t it = h2t[p];
+      uint32_t it = h2t[p];
       float tip = std::abs(ca.state[size_t(it) * 5 + 1]);
       if (ca.quality[it] != kBad && tip < mc) {
         mc = tip;
@@ -505,7 +512,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
       }
     }
     for (uint32_t p = b; p < e; ++p) {
-      uint16_t it = h2t[p];
+      uint32_t it = h2t[p];
       if (ca.quality[it] != kBad && it != im) ca.quality[it] = kDup;
     }
   }

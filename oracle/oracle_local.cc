@@ -274,7 +274,7 @@ void loadES(ES& es, const uint8_t* cabling, size_t ncab, const uint8_t* gain, si
 // SiPixelRawToClusterCUDA.cc:78-138 with ErrorChecker.cc:36-91.  The
 // reference's ErrorChecker records no errors (includeErrors = false in its
 // constructor, :36); formatterErrors turns that recording on.
-void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w, bool formatterErrors) {
+void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w, bool formatterErrors, const Caps& caps) {
   // Source.cc:9-21 record layout
   std::vector<std::pair<const uint8_t*, uint32_t>> fedData(4096, {nullptr, 0});
   size_t off = 0;
@@ -293,8 +293,8 @@ void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w, bool formatte
     fedData[fedId] = {raw + off, size};
     off += size;
   }
-  w.word.assign(PF_MAX_FED_WORDS, 0);
-  w.fedId.assign(PF_MAX_FED_WORDS, 0);
+  w.word.assign(caps.fedWords, 0);
+  w.fedId.assign(caps.fedWords, 0);
   w.formatterErrors.clear();
   auto record = [&](uint64_t word64, uint32_t type, uint32_t fedId) {
     if (formatterErrors) w.formatterErrors.push_back({word64, type, fedId});
@@ -353,7 +353,7 @@ void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w, bool formatte
     const uint8_t* bw = data + 8 * size_t(h + 1);
     const uint8_t* ew = data + 8 * size_t(t);
     uint32_t length = uint32_t((ew - bw) / 4);
-    if (wordCounter + length > PF_MAX_FED_WORDS)
+    if (wordCounter + length > caps.fedWords)
       throw std::runtime_error("undefined in the reference: more than MAX_FED_WORDS words");
     // WordFedAppender::initializeWordFed (SiPixelRawToClusterGPUKernel.cc:41-47)
     std::memcpy(w.word.data() + wordCounter, bw, 4 * size_t(length));
@@ -363,7 +363,7 @@ void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w, bool formatte
   w.nWords = wordCounter;
 }
 
-void makeClusters(const ES& es, const Words& w, Digis& d, Clusters& c) {
+void makeClusters(const ES& es, const Words& w, Digis& d, Clusters& c, const Caps& caps) {
   const PfCablingMap& cab = *es.cab;
   const uint32_t nW = w.nWords;
   d.nDigis = nW;
@@ -617,11 +617,11 @@ void makeClusters(const ES& es, const Words& w, Digis& d, Clusters& c) {
   for (uint32_t i = 0; i < PF_MAX_MODULES; ++i) cms[i + 1] = std::min<uint32_t>(PF_MAX_CLUS_PER_MODULE, c.clusInModule[i]);
   for (uint32_t i = 1; i < PF_MAX_MODULES + 1; ++i) cms[i] += cms[i - 1];
   for (uint32_t i = 0; i < PF_MAX_MODULES + 1; ++i)
-    if (cms[i] > PF_MAX_HITS) cms[i] = PF_MAX_HITS;
+    if (cms[i] > caps.hits) cms[i] = caps.hits;
   c.nClusters = cms[PF_MAX_MODULES];
 }
 
-void makeHits(const ES& es, const Digis& d, const Clusters& c, Hits& h) {
+void makeHits(const ES& es, const Digis& d, const Clusters& c, Hits& h, const Caps& caps) {
   const uint32_t nHits = c.nClusters;
   h.nHits = nHits;
   h.xl.assign(nHits, 0);
@@ -704,7 +704,7 @@ void makeHits(const ES& es, const Digis& d, const Clusters& c, Hits& h) {
         uint32_t firstHit = c.clusModuleStart[me] + startClus;
         for (int ic = 0; ic < nIn; ++ic) {
           uint32_t hidx = firstHit + ic;
-          if (hidx >= PF_MAX_HITS) break;
+          if (hidx >= caps.hits) break;
           // pixelCPEforGPU::position (pixelCPEforGPU.h:176-259)
           uint16_t llx = uint16_t(minRow[ic] + 1), lly = uint16_t(minCol[ic] + 1);
           uint16_t urx = uint16_t(maxRow[ic]), ury = uint16_t(maxCol[ic]);
@@ -790,7 +790,7 @@ void makeHits(const ES& es, const Digis& d, const Clusters& c, Hits& h) {
     for (uint32_t i = 0; i < nt; ++i) {
       uint32_t b = bin(h.iphi[i]) + 128 * layerOf(i);
       uint32_t w = h.phiOff[b]--;
-      h.phiBins[w - 1] = uint16_t(i);
+      h.phiBins[w - 1] = i;
     }
   }
 }

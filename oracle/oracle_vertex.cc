@@ -6,6 +6,7 @@
 // gpuSplitVertices.h:15-125 and gpuSortByPt2.h:15-55 with the
 // PixelVertexProducerCUDA configuration (PixelVertexProducerCUDA.cc:16-26):
 // minT=2, eps=0.07, errmax=0.01, chi2max=9, ptMin=0.5.  See oracle.h.
+#include <stdexcept>
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -16,7 +17,9 @@
 namespace oracle {
 
 void makeVertices(const CA& ca, Vertices& v, int algo) {
-  constexpr uint32_t MAXTRACKS = 32 * 1024, MAXVTX = PF_MAX_VTX;
+  // the TrackSoA stride (32768 in the reference, ZVertexSoA.h:11)
+  const uint32_t MAXTRACKS = ca.tupleBins;
+  constexpr uint32_t MAXVTX = PF_MAX_VTX;
   const int minT = 2;
   const float eps = 0.07f, errmax = 0.01f, chi2max = 9.f, ptMin = 0.5f;
   v.nvFinal = 0;
@@ -29,7 +32,7 @@ void makeVertices(const CA& ca, Vertices& v, int algo) {
   v.idv.assign(MAXTRACKS, 0);
 
   // ---- loadTracks (quality loose, nHits >= 4, pt >= ptMin)
-  std::vector<uint16_t> itrk;
+  std::vector<uint32_t> itrk;
   std::vector<float> zt, ezt2, ptt2;
   for (uint32_t idx = 0; idx < MAXTRACKS; ++idx) {
     uint32_t nHits = ca.size(idx);
@@ -39,12 +42,14 @@ void makeVertices(const CA& ca, Vertices& v, int algo) {
     if (ca.quality[idx] != 2) continue;
     float pt = ca.pt[idx];
     if (pt < ptMin) continue;
-    itrk.push_back(uint16_t(idx));
+    itrk.push_back(idx);
     zt.push_back(ca.state[size_t(idx) * 5 + 4]);
     ezt2.push_back(ca.cov[size_t(idx) * 15 + 14]);
     ptt2.push_back(pt * pt);
   }
   const uint32_t nt = uint32_t(itrk.size());
+  // ZVertexSoA::MAXTRACKS (ZVertexSoA.h:11): the reference writes past its arrays beyond it
+  if (nt > 32 * 1024) throw std::runtime_error("undefined in the reference: more than 32768 vertex tracks");
   std::vector<int32_t> iv(nt);
   int32_t* nn = v.ndof.data();
   uint32_t nvIntermediate = 0;
@@ -63,10 +68,10 @@ void makeVertices(const CA& ca, Vertices& v, int algo) {
       nn[i] = 0;
     }
     for (int b = 1; b < 257; ++b) off[b] += off[b - 1];
-    std::vector<uint16_t> bins(nt);
+    std::vector<uint32_t> bins(nt);
     for (uint32_t i = 0; i < nt; ++i) {
       uint32_t w = off[izt[i]]--;
-      bins[w - 1] = uint16_t(i);
+      bins[w - 1] = i;
     }
     // forEachInBins(hist, izt[i], 1, f): bins izt-1 .. izt+1, in storage order
     auto forEach = [&](uint32_t i, auto&& f) {

@@ -2,6 +2,8 @@
 
 lib/libpixgpu.so    the B200 chain (CUDA, sm_100a) behind include/pixgpu.h
 lib/libpixsynth.so  the seeded synthetic detector/event generator (include/pixsynth.h)
+lib/pluginPixelB200.so  the chain's modules for the reference framework (framework/), built
+                    against that framework's headers (only where the reference tree exists)
 oracle/liboracle.so the CPU oracle used by the tests (checker only)
 oracle/_ref/        checker build of the reference's serial sources (only where they exist)
 
@@ -97,19 +99,33 @@ def reference_dir():
     return None
 
 
+def build_plugins(reference=None):
+    """The framework modules (framework/Makefile), against the reference framework's headers."""
+    reference = reference or reference_dir()
+    if reference is None:
+        return None
+    _run(["make", "-s", "-j8", "-C", os.path.join(PKG, "framework"), "REF=" + reference])
+    return os.path.join(LIB, "pluginPixelB200.so")
+
+
 def build_ref(reference=None):
-    """Checker build of the reference serial sources (skipped where they are absent)."""
+    """Checker build of the reference serial sources and of its event processor with
+    the plugins (skipped where the reference tree is absent)."""
     reference = reference or reference_dir()
     if reference is None:
         return None
     _run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle", "ref"), "REF=" + reference])
+    if os.path.exists(os.path.join(LIB, "pluginPixelB200.so")):
+        _run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle", "ref"), "REF=" + reference, "fw"])
     return os.path.join(ROOT, "oracle", "_ref", "libpixref.so")
 
 
 def build_all(gpu=True):
-    out = {"synth": build_synth(), "oracle": build_oracle(), "ref": build_ref()}
+    out = {"synth": build_synth(), "oracle": build_oracle()}
     if gpu:
         out["gpu"] = build_gpu()
+        out["plugins"] = build_plugins()
+    out["ref"] = build_ref()
     return out
 
 

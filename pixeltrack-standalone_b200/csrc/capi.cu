@@ -25,6 +25,35 @@ int fail(pg_ctx* c, int code, const std::string& msg) {
   }
   return code;
 }
+bool resolveCaps(const pg_config& cfg, Caps* out) {
+  const Caps r = referenceCaps();
+  Caps c = r;
+  auto pick = [](uint32_t v, uint32_t def) { return v ? v : def; };
+  c.fedWords = pick(cfg.cap_fed_words, r.fedWords);
+  c.hits = pick(cfg.cap_hits, r.hits);
+  c.cells = pick(cfg.cap_doublets, r.cells);
+  c.lists = pick(cfg.cap_lists, r.lists);
+  c.tuples = pick(cfg.cap_tuples, r.tuples);
+  c.multiplicity = pick(cfg.cap_multiplicity, r.multiplicity);
+  c.h2t = pick(cfg.cap_hit_to_tuple, r.h2t);
+  if (c.fedWords < r.fedWords || c.hits < r.hits || c.cells < r.cells || c.lists < r.lists || c.tuples < r.tuples ||
+      c.multiplicity < r.multiplicity || c.h2t < r.h2t)
+    return false;
+  // the doublet search packs hit indices into 21 bits; the multiplicity fill
+  // counts each bin in a 20-bit field
+  if (c.hits > kMaxHitCapLimit || c.tuples >= (1u << 20) || c.multiplicity > c.tuples) return false;
+  if (uint64_t(c.cells) * 2 > 0xffffffffull || uint64_t(c.hits) * 6 > 0xffffffffull) return false;
+  c.jCap = 6 * c.hits;
+  // CA links kept: the reference's 2 x 458752, or one per doublet beyond it
+  c.edges = std::max(r.edges, c.cells);
+  // scratchA/scratchB: CA link staging, two duplicate-round worklists of
+  // cells, the doublet staging (one entry per inner-hit slot in B) and the
+  // vertex finder's per-track arrays
+  c.scratch = std::max<uint32_t>(std::max(std::max(c.edges, 2 * c.cells), c.jCap), uint32_t(kVtxScratchAWords));
+  *out = c;
+  return true;
+}
+
 std::string lastError(pg_ctx* c) {
   std::lock_guard<std::mutex> lk(c->errMu);
   return c->err;
@@ -251,7 +280,7 @@ int stageRawBlocks(pg_ctx* c, Slot& s, uint32_t nEvents, const uint8_t* const* r
       cursor += n64;
       bound += n64 >= 2 ? 2 * uint64_t(n64 - 2) : 0;
     }
-    if (bound > kMaxFedWords) return fail(c, PG_ERR_CAPACITY, "event or batch too large");
+    if (bound > c->caps.fedWords) return fail(c, PG_ERR_CAPACITY, "event or batch too large");
     batchBound += bound;
   }
   if (batchBound > c->cfg.max_words_per_batch) return fail(c, PG_ERR_CAPACITY, "event or batch too large");
@@ -280,7 +309,7 @@ int stage(pg_ctx* c, Slot& s, uint32_t nEvents, const uint8_t* const* raws, cons
     s.hOffsets[k] = off;
     uint32_t nw = 0;
     uint32_t room = c->cfg.max_words_per_batch - off;
-    room = room > kMaxFedWords ? kMaxFedWords : room;
+    room = room > c->caps.fedWords ? c->caps.fedWords : room;
     int rc = unpackRaw(c->hes.fedIds, raws[k], sizes[k], s.hWords + off, s.hFed + off / 2, room, &nw,
                        fmt ? &s.fmtErrors : nullptr);
     s.fmtOff.push_back(uint32_t(s.fmtErrors.size()));
@@ -409,6 +438,9 @@ void pg_default_config(pg_config* cfg) {
   cfg->do_pt_cut = 1;
   cfg->formatter_errors = 0;
   cfg->fed_scan = 0;
+  // the reference's container capacities
+  cfg->cap_fed_words = cfg->cap_hits = cfg->cap_doublets = cfg->cap_lists = 0;
+  cfg->cap_tuples = cfg->cap_multiplicity = cfg->cap_hit_to_tuple = 0;
 }
 
 namespace {
@@ -416,7 +448,7 @@ namespace {
 int createSlot(pg_ctx* c, Slot& s, size_t bytes) {
   const uint32_t E = c->cfg.max_events;
   if (cudaMalloc(&s.dmem, bytes) != cudaSuccess) return fail(c, PG_ERR_NOMEM, "slot workspace");
-  workspaceCarve(s.ws, s.dmem, E, c->cfg.max_words_per_batch);
+  workspaceCarve(s.ws, s.dmem, E, c->cfg.max_words_per_batch, c->caps);
   // layer pairs of CAHitNtupletGeneratorKernels.cc:52-57
   s.ws.ca.nPairs = c->cfg.min_hits_per_ntuplet > 3 ? 13u : (c->cfg.include_jumping_forward_doublets ? 19u : 15u);
   s.ws.ca.minHits = c->cfg.min_hits_per_ntuplet;
@@ -520,6 +552,7 @@ int pg_create(const pg_es_images* es, const pg_config* cfgIn, pg_ctx** out) {
       c->cfg.vertex_algo > 2 || c->cfg.min_hits_per_ntuplet < 3 || c->cfg.min_hits_per_ntuplet > 4 ||
       c->cfg.fed_scan > 1 || (c->cfg.fed_scan && c->cfg.pool_words))  // the pool stages on the host
     return PG_ERR_ARG;
+  if (!resolveCaps(c->cfg, &c->caps)) return PG_ERR_ARG;
   c->device = c->cfg.device;
   cudaError_t e = cudaSetDevice(c->cfg.device);
   if (e != cudaSuccess) return PG_ERR_CUDA;
@@ -535,7 +568,7 @@ int pg_create(const pg_es_images* es, const pg_config* cfgIn, pg_ctx** out) {
       return rc;
     }
   }
-  size_t bytes = workspaceBytes(c->cfg.max_events, c->cfg.max_words_per_batch);
+  size_t bytes = workspaceBytes(c->cfg.max_events, c->cfg.max_words_per_batch, c->caps);
   uint32_t nSlots = c->cfg.slots;
   if (nSlots == 0) {
     // admission by free HBM: as many slots as fit in the given share of the free memory
@@ -579,7 +612,7 @@ int pg_get_config(const pg_ctx* c, pg_config* out) {
 const char* pg_last_error(const pg_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
 size_t pg_slot_bytes(const pg_ctx* c) {
-  return c ? workspaceBytes(c->cfg.max_events, c->cfg.max_words_per_batch) : 0;
+  return c ? workspaceBytes(c->cfg.max_events, c->cfg.max_words_per_batch, c->caps) : 0;
 }
 
 int pg_unpack_raw(const pg_ctx* c, const uint8_t* raw, size_t n, uint32_t* words, uint8_t* fedIds, uint32_t cap,
@@ -638,15 +671,36 @@ int pg_event_counts_get(pg_ctx* c, uint32_t k, pg_event_counts* out) {
   return PG_OK;
 }
 
+namespace {
+int slotProduct(pg_ctx* c, Slot& s, uint32_t k, const char* name, void* dst, size_t cap, size_t* count, int* elem);
+}  // namespace
+
 int pg_get_product(pg_ctx* c, uint32_t k, const char* name, void* dst, size_t cap, size_t* count, int* elem) {
   if (!c || !name || !count || !elem || k >= c->slots[0].nEvents) return PG_ERR_ARG;
-  Slot& s = c->slots[0];
+  return slotProduct(c, c->slots[0], k, name, dst, cap, count, elem);
+}
+
+int pg_slot_product(pg_ctx* c, uint32_t slot, uint32_t k, const char* name, void* dst, size_t cap, size_t* count,
+                    int* elem) {
+  if (!c || !name || !count || !elem || slot >= c->slots.size()) return PG_ERR_ARG;
+  Slot& s = c->slots[slot];
+  if (s.state != SlotState::kBusy || k >= s.nEvents) return fail(c, PG_ERR_ARG, "slot holds no such event");
+  const cudaError_t q = cudaEventQuery(s.done);
+  if (q == cudaErrorNotReady) return PG_ERR_BUSY;
+  if (q != cudaSuccess) return cudaFail(c, q, "batch");
+  return slotProduct(c, s, k, name, dst, cap, count, elem);
+}
+
+namespace {
+int slotProduct(pg_ctx* c, Slot& s, uint32_t k, const char* name, void* dst, size_t cap, size_t* count, int* elem) {
   const Workspace& ws = s.ws;
   EventCounters ec;
   cudaError_t e = cudaMemcpy(&ec, ws.ev + k, sizeof(ec), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cudaFail(c, e, "D2H counters");
   std::string n(name);
   const size_t w0 = ec.wordStart, nw = ec.nWords;
+  const uint32_t kHitCap = ws.cap.hits, kCellCap = ws.cap.cells, kTupleBins = ws.cap.tuples;
+  const uint32_t kTupleHitCap = ws.cap.tupleHits(), kTupleCellCap = ws.cap.tupleCells(), kEdgeCap = ws.cap.edges;
   const size_t hb = size_t(k) * kHitCap, mb = size_t(k) * kModStride, cb = size_t(k) * kCellCap,
                tb = size_t(k) * kTupleBins, vb = size_t(k) * kMaxVtx;
   const uint32_t nh = ec.nHits, nc = ec.nCells;
@@ -770,6 +824,7 @@ int pg_get_product(pg_ctx* c, uint32_t k, const char* name, void* dst, size_t ca
   if (n == "idv") return copyOut(c, s, ws.idv + tb, nTup, dst, cap, count, elem);
   return fail(c, PG_ERR_NOTFOUND, "unknown product " + n);
 }
+}  // namespace
 
 int pg_submit(pg_ctx* c, uint32_t nEvents, const uint8_t* const* raws, const size_t* sizes, uint32_t* slotOut) {
   if (!c || !raws || !sizes || !slotOut) return PG_ERR_ARG;

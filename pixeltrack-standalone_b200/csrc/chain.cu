@@ -20,9 +20,10 @@ struct Carver {
   }
 };
 
-void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W) {
+void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W, const Caps& cap) {
   ws.maxEvents = E;
   ws.wordCap = W;
+  ws.cap = cap;
   c.take(ws.words, W);
   c.take(ws.fedIds, W / 2 + 2);
   c.take(ws.wordOffsets, E + 1);
@@ -41,7 +42,7 @@ void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W) {
   c.take(ws.clusInModule, size_t(E) * kModStride);
   c.take(ws.moduleId, size_t(E) * kModStride);
   c.take(ws.clusModuleStart, size_t(E) * kModStride);
-  size_t H = size_t(E) * kHitCap;
+  size_t H = size_t(E) * cap.hits;
   c.take(ws.xl, H);
   c.take(ws.yl, H);
   c.take(ws.xerr, H);
@@ -59,9 +60,9 @@ void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W) {
   c.take(ws.phiBins, H);
   c.take(ws.phiRec, H);
   c.take(ws.agc, E);
-  c.take(ws.jCount, size_t(E) * (kJCap + 1));
-  c.take(ws.jOffset, size_t(E) * (kJCap + 1));
-  size_t C = size_t(E) * kCellCap;
+  c.take(ws.jCount, size_t(E) * (cap.jCap + 1));
+  c.take(ws.jOffset, size_t(E) * (cap.jCap + 1));
+  size_t C = size_t(E) * cap.cells;
   c.take(ws.cellInner, C);
   c.take(ws.cellOuter, C);
   c.take(ws.cellPair, C);
@@ -69,39 +70,39 @@ void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W) {
   c.take(ws.cellUsed, C);
   c.take(ws.cellInnerZ, C);
   c.take(ws.cellInnerR, C);
-  c.take(ws.ohCount, size_t(E) * (kHitCap + 1));
-  c.take(ws.ohOff, size_t(E) * (kHitCap + 1));
+  c.take(ws.ohCount, size_t(E) * (cap.hits + 1));
+  c.take(ws.ohOff, size_t(E) * (cap.hits + 1));
   c.take(ws.ohCells, C);
   c.take(ws.ohRec, C);
   c.take(ws.ohDet, C);
-  size_t C1 = size_t(E) * (kCellCap + 1);
+  size_t C1 = size_t(E) * (cap.cells + 1);
   c.take(ws.nbrCount, C1);
   c.take(ws.nbrOff, C1);
-  c.take(ws.nbr, size_t(E) * kEdgeCap);
+  c.take(ws.nbr, size_t(E) * cap.edges);
   c.take(ws.startTupleCount, C1);
   c.take(ws.startTupleOff, C1);
   c.take(ws.startHitCount, C1);
   c.take(ws.startHitOff, C1);
-  c.take(ws.tupleOff, size_t(E) * (kTupleBins + 1));
-  c.take(ws.tupleHits, size_t(E) * kTupleHitCap);
-  c.take(ws.tupleDet, size_t(E) * kTupleHitCap);
-  c.take(ws.tupleCells, size_t(E) * kTupleCellCap);
-  c.take(ws.quality, size_t(E) * kTupleBins);
+  c.take(ws.tupleOff, size_t(E) * (cap.tuples + 1));
+  c.take(ws.tupleHits, size_t(E) * cap.tupleHits());
+  c.take(ws.tupleDet, size_t(E) * cap.tupleHits());
+  c.take(ws.tupleCells, size_t(E) * cap.tupleCells());
+  c.take(ws.quality, size_t(E) * cap.tuples);
   c.take(ws.trkCount, C1);
   c.take(ws.trkOff, C1);
-  c.take(ws.trk, size_t(E) * kTupleCellCap);
+  c.take(ws.trk, size_t(E) * cap.tupleCells());
   c.take(ws.candidates, C);
   c.take(ws.tmOff, size_t(E) * 16);
-  c.take(ws.tmBins, size_t(E) * kTupleBins);
-  size_t T = size_t(E) * kTupleBins;
+  c.take(ws.tmBins, size_t(E) * cap.tuples);  // bins beyond cap.multiplicity only under its overflow flag
+  size_t T = size_t(E) * cap.tuples;
   c.take(ws.state, T * 5);
   c.take(ws.cov, T * 15);
   c.take(ws.pt, T);
   c.take(ws.eta, T);
   c.take(ws.chi2, T);
-  c.take(ws.h2tCount, size_t(E) * (kHitCap + 1));
-  c.take(ws.h2tOff, size_t(E) * (kHitCap + 1));
-  c.take(ws.h2t, size_t(E) * kH2TCap);
+  c.take(ws.h2tCount, size_t(E) * (cap.hits + 1));
+  c.take(ws.h2tOff, size_t(E) * (cap.hits + 1));
+  c.take(ws.h2t, size_t(E) * cap.h2t);
   size_t V = size_t(E) * kMaxVtx;
   c.take(ws.zv, V);
   c.take(ws.wv, V);
@@ -110,11 +111,11 @@ void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W) {
   c.take(ws.ndof, V);
   c.take(ws.sortInd, V);
   c.take(ws.idv, T);
-  c.take(ws.scratchA, size_t(E) * kEdgeCap);
-  c.take(ws.scratchB, size_t(E) * kEdgeCap);
+  c.take(ws.scratchA, size_t(E) * cap.scratch);
+  c.take(ws.scratchB, size_t(E) * cap.scratch);
   c.take(ws.scanSums, size_t(E) * kScanMaxSlices);
   c.take(ws.bigSeg, size_t(E) * kBigSegCap);
-  c.take(ws.segList, size_t(E) * kCellCap);
+  c.take(ws.segList, size_t(E) * cap.cells);
 }
 
 // the pair opened by probeBegin when its name matched (-1: none).  Records use
@@ -144,16 +145,16 @@ void probeEnd(cudaStream_t s) {
   tProbeOpen = -1;
 }
 
-size_t workspaceBytes(uint32_t maxEvents, uint32_t wordCap) {
+size_t workspaceBytes(uint32_t maxEvents, uint32_t wordCap, const Caps& cap) {
   Workspace ws;
   Carver c{nullptr};
-  layout(ws, c, maxEvents, wordCap);
+  layout(ws, c, maxEvents, wordCap, cap);
   return c.off + 256;
 }
 
-void workspaceCarve(Workspace& ws, void* base, uint32_t maxEvents, uint32_t wordCap) {
+void workspaceCarve(Workspace& ws, void* base, uint32_t maxEvents, uint32_t wordCap, const Caps& cap) {
   Carver c{static_cast<char*>(base)};
-  layout(ws, c, maxEvents, wordCap);
+  layout(ws, c, maxEvents, wordCap, cap);
 }
 
 cudaError_t runChain(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream, bool riemann,

@@ -47,6 +47,9 @@ constexpr float kHardCurvCut = 0.0328407224959f;
 constexpr float kDcaCutInner = 0.15000000596f;
 constexpr float kDcaCutOuter = 0.25f;
 constexpr uint8_t kBad = 0, kDup = 1, kLoose = 2;
+// "no tuple" in the duplicate removers (the reference's 60000 lies above every
+// index of its 32768 bins; with 32-bit tuple indices a larger one is needed)
+constexpr uint32_t kNoTuple = 0xffffffffu;
 
 __device__ __forceinline__ uint32_t phiBin(int16_t t) { return uint32_t((int(t) >> 9) & 127); }
 
@@ -55,10 +58,10 @@ struct HitsView {
   const int16_t *iphi, *ysize;
   const uint16_t* detInd;
   const uint32_t* phiOff;
-  const uint16_t* phiBins;
+  const uint32_t* phiBins;
 };
 __device__ __forceinline__ HitsView hitsOf(const Workspace& ws, uint32_t e) {
-  size_t hb = size_t(e) * kHitCap;
+  size_t hb = size_t(e) * ws.cap.hits;
   return {ws.xg + hb, ws.yg + hb, ws.zg + hb, ws.rg + hb, ws.iphi + hb, ws.ysize + hb, ws.detInd + hb,
           ws.phiOff + size_t(e) * kPhiStride, ws.phiBins + hb};
 }
@@ -80,9 +83,9 @@ __global__ void kDoubletSetup(Workspace ws, uint32_t nEvents) {
     if (p < ws.ca.nPairs) cum += c->layerStart[li + 1] - c->layerStart[li];
     c->pairCum[p] = cum;  // pairs beyond nPairs own no slots
   }
-  if (cum > kJCap) {
+  if (cum > ws.cap.jCap) {
     c->flags |= kFlagJOverflow;
-    cum = kJCap;
+    cum = ws.cap.jCap;
   }
   c->ntot = cum;
 }
@@ -167,7 +170,7 @@ __device__ __forceinline__ bool doubletAccept(const DoubletSeed& d, const uint4 
   constexpr float minRadius2T4 = 4.f * minRadius * minRadius;
   constexpr float dzdrFact = 8 * 0.0285 / 0.015;
   constexpr float i2p = 3.14159265358979323846 / 32768;
-  if ((rec.w & 0xffffu) > 2000) return false;
+  if ((rec.w & 0x7ffu) > 2000) return false;
   const float zo = __uint_as_float(rec.x), ro = __uint_as_float(rec.y);
   const float dr = ro - d.mer;
   if ((d.cuts & 1u) && (dr > d.maxr || dr < 0 || fabsf((d.mez * ro - d.mer * zo)) > z0cut * dr)) return false;
@@ -195,11 +198,11 @@ __device__ __forceinline__ uint32_t warpDoublets(const DoubletSeed& d, const uin
     const uint32_t b = r ? d.b1 : d.b0, en = r ? d.e1 : d.e0;
     for (uint32_t p0 = b; p0 < en; p0 += 32) {
       const uint32_t p = p0 + lane;
-      uint16_t oi = 0;
+      uint32_t oi = 0;
       bool ok = false;
       if (p < en) {
         const uint4 h = rec[p];
-        oi = uint16_t(h.w >> 16);
+        oi = h.w >> 11;
         ok = doubletAccept(d, h);
       }
       const uint32_t m = __ballot_sync(0xffffffffu, ok);
@@ -252,8 +255,8 @@ __device__ __forceinline__ void forSeedSlots(const PairTable& pt, const HitsView
 constexpr uint32_t kNoTemp = 0xffffffffu;  // the slot's doublets did not fit its warp's staging region
 
 // Pass 1: count each slot's doublets and stage their outer hits, in serial
-// order, in the staging region of the warp that found them (scratchA as
-// 16-bit entries, an equal share per warp: no atomics); the slot's staging
+// order, in the staging region of the warp that found them (scratchA, an
+// equal share per warp: no atomics); the slot's staging
 // offset goes to scratchB.  A slot whose window could overflow the region is
 // only counted, and pass 2 tests its candidates again.
 __global__ void kDoubletCount(Workspace ws) {
@@ -263,13 +266,13 @@ __global__ void kDoubletCount(Workspace ws) {
   const uint32_t ntot = c->ntot;
   loadPairTable(c, pt, ws.ca);
   const HitsView hh = hitsOf(ws, e);
-  const uint4* rec = ws.phiRec + size_t(e) * kHitCap;
-  uint32_t* cnt = ws.jCount + size_t(e) * (kJCap + 1);
-  uint16_t* stage = reinterpret_cast<uint16_t*>(ws.scratchA + size_t(e) * kEdgeCap);
-  uint32_t* slotStage = ws.scratchB + size_t(e) * kEdgeCap;
+  const uint4* rec = ws.phiRec + size_t(e) * ws.cap.hits;
+  uint32_t* cnt = ws.jCount + size_t(e) * (ws.cap.jCap + 1);
+  uint32_t* stage = ws.scratchA + size_t(e) * ws.cap.scratch;
+  uint32_t* slotStage = ws.scratchB + size_t(e) * ws.cap.scratch;
   const uint32_t wpb = blockDim.x >> 5;
   const uint32_t S = gridDim.x * wpb, w = blockIdx.x * wpb + (threadIdx.x >> 5);
-  const uint32_t R = 2 * kEdgeCap / S;  // staging entries per warp
+  const uint32_t R = ws.cap.scratch / S;  // staging entries per warp
   uint32_t used = 0;                     // warp-uniform
   forSeedSlots(pt, hh, ntot, [&](uint32_t j, bool live, const DoubletSeed& d, uint32_t phase) {
     if (phase == 0) {
@@ -278,7 +281,7 @@ __global__ void kDoubletCount(Workspace ws) {
     }
     const uint32_t window = (d.e0 - d.b0) + (d.e1 - d.b1);
     const uint32_t at = used + window <= R ? w * R + used : kNoTemp;
-    const uint32_t n = warpDoublets(d, rec, [&](uint32_t k, uint16_t oi) {
+    const uint32_t n = warpDoublets(d, rec, [&](uint32_t k, uint32_t oi) {
       if (at != kNoTemp) stage[at + k] = oi;
     });
     if (at != kNoTemp) used += n;
@@ -299,12 +302,12 @@ __global__ void __launch_bounds__(256, 5) kDoubletWrite(Workspace ws) {
   const uint32_t ntot = c->ntot;
   loadPairTable(c, pt, ws.ca);
   const HitsView hh = hitsOf(ws, e);
-  const uint4* rec = ws.phiRec + size_t(e) * kHitCap;
-  const uint32_t* off = ws.jOffset + size_t(e) * (kJCap + 1);
-  const size_t cb = size_t(e) * kCellCap;
-  uint32_t* ohc = ws.ohCount + size_t(e) * (kHitCap + 1);
-  const uint16_t* stage = reinterpret_cast<const uint16_t*>(ws.scratchA + size_t(e) * kEdgeCap);
-  const uint32_t* slotStage = ws.scratchB + size_t(e) * kEdgeCap;
+  const uint4* rec = ws.phiRec + size_t(e) * ws.cap.hits;
+  const uint32_t* off = ws.jOffset + size_t(e) * (ws.cap.jCap + 1);
+  const size_t cb = size_t(e) * ws.cap.cells;
+  uint32_t* ohc = ws.ohCount + size_t(e) * (ws.cap.hits + 1);
+  const uint32_t* stage = ws.scratchA + size_t(e) * ws.cap.scratch;
+  const uint32_t* slotStage = ws.scratchB + size_t(e) * ws.cap.scratch;
   const uint32_t lane = laneId(), wpb = blockDim.x >> 5;
   const uint32_t S = gridDim.x * wpb, w = blockIdx.x * wpb + (threadIdx.x >> 5);
   for (uint32_t r0 = 0; w + r0 * S < ntot; r0 += 32) {
@@ -312,7 +315,7 @@ __global__ void __launch_bounds__(256, 5) kDoubletWrite(Workspace ws) {
     uint32_t myBase = 0, myN = 0;
     if (jl < ntot) {
       myBase = off[jl];
-      myN = myBase < kCellCap ? min(off[jl + 1], kCellCap) - myBase : 0u;
+      myN = myBase < ws.cap.cells ? min(off[jl + 1], ws.cap.cells) - myBase : 0u;
     }
     uint32_t live = __ballot_sync(0xffffffffu, myN > 0);
     while (live) {
@@ -324,9 +327,9 @@ __global__ void __launch_bounds__(256, 5) kDoubletWrite(Workspace ws) {
       while (j >= pt.pairCum[pair]) ++pair;
       const uint32_t i = (0 == pair ? j : j - pt.pairCum[pair - 1]) + pt.layerStart[cLayerPairs[2 * pair]];
       const float zi = hh.zg[i], ri = hh.rg[i];
-      auto put = [&](uint32_t k, uint16_t oi) {
+      auto put = [&](uint32_t k, uint32_t oi) {
         const uint32_t idx = base + k;
-        ws.cellInner[cb + idx] = uint16_t(i);
+        ws.cellInner[cb + idx] = i;
         ws.cellOuter[cb + idx] = oi;
         ws.cellPair[cb + idx] = uint8_t(pair);
         ws.cellDoubletId[cb + idx] = int32_t(idx);
@@ -341,7 +344,7 @@ __global__ void __launch_bounds__(256, 5) kDoubletWrite(Workspace ws) {
       } else {
         DoubletSeed d;
         doubletSeed(pt, hh, j, d);
-        warpDoublets(d, rec, [&](uint32_t k, uint16_t oi) {
+        warpDoublets(d, rec, [&](uint32_t k, uint32_t oi) {
           if (k < n) put(k, oi);
         });
       }
@@ -353,10 +356,10 @@ __global__ void kCellsTotal(Workspace ws, uint32_t nEvents) {
   uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nEvents) return;
   EventCounters* c = ws.ev + e;
-  uint32_t raw = ws.jOffset[size_t(e) * (kJCap + 1) + c->ntot];
+  uint32_t raw = ws.jOffset[size_t(e) * (ws.cap.jCap + 1) + c->ntot];
   c->nCellsRaw = raw;
-  c->nCells = min(raw, kCellCap);
-  if (raw >= kCellCap) c->flags |= kFlagCellOverflow;
+  c->nCells = min(raw, ws.cap.cells);
+  if (raw >= ws.cap.cells) c->flags |= kFlagCellOverflow;
 }
 
 // generic CSR helpers ------------------------------------------------------
@@ -373,11 +376,11 @@ __global__ void kZero(uint32_t* p, size_t stride, uint32_t n, const uint32_t* le
 __global__ void kOuterHitFill(Workspace ws) {
   uint32_t e = blockIdx.y;
   uint32_t n = ws.ev[e].nCells;
-  size_t cb = size_t(e) * kCellCap;
-  const uint32_t* off = ws.ohOff + size_t(e) * (kHitCap + 1);
-  uint32_t* cur = ws.ohCount + size_t(e) * (kHitCap + 1);
+  size_t cb = size_t(e) * ws.cap.cells;
+  const uint32_t* off = ws.ohOff + size_t(e) * (ws.cap.hits + 1);
+  uint32_t* cur = ws.ohCount + size_t(e) * (ws.cap.hits + 1);
   for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-    uint16_t oi = ws.cellOuter[cb + c];
+    uint32_t oi = ws.cellOuter[cb + c];
     uint32_t p = atomicAdd(&cur[oi], 1u);
     ws.ohCells[cb + off[oi] + p] = c;
     // connect and fishbone read the first 128 cells of a hit (ascending):
@@ -438,10 +441,10 @@ __device__ __forceinline__ bool dcaCut(float x1, float y1, float x2, float y2, f
 __global__ void kOhRec(Workspace ws) {
   const uint32_t e = blockIdx.y;
   const uint32_t n = ws.ev[e].nCells;
-  const size_t cb = size_t(e) * kCellCap, hb = size_t(e) * kHitCap;
+  const size_t cb = size_t(e) * ws.cap.cells, hb = size_t(e) * ws.cap.hits;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     const uint32_t oc = ws.ohCells[cb + p];
-    const uint16_t ih = ws.cellInner[cb + oc];
+    const uint32_t ih = ws.cellInner[cb + oc];
     const float r = ws.cellInnerR[cb + oc];
     const uint16_t det = ws.detInd[hb + ih];
     ws.ohRec[cb + p] = make_float4(ws.xg[hb + ih], ws.yg[hb + ih], ws.cellInnerZ[cb + oc], det < 96 ? -r : r);
@@ -464,14 +467,15 @@ __global__ void __launch_bounds__(256, 6) kConnect(Workspace ws, uint32_t* edgeO
   const uint32_t ntot = c->ntot;
   const uint32_t nCells = c->nCells;
   const HitsView hh = hitsOf(ws, e);
-  const size_t cb = size_t(e) * kCellCap;
-  const uint32_t* joff = ws.jOffset + size_t(e) * (kJCap + 1);
-  const uint32_t* ohOff = ws.ohOff + size_t(e) * (kHitCap + 1);
+  const size_t cb = size_t(e) * ws.cap.cells;
+  const uint32_t* joff = ws.jOffset + size_t(e) * (ws.cap.jCap + 1);
+  const uint32_t* ohOff = ws.ohOff + size_t(e) * (ws.cap.hits + 1);
   const uint32_t* ohCells = ws.ohCells + cb;
   const float4* ohRec = ws.ohRec + cb;
-  uint32_t* nbrCnt = ws.nbrCount + size_t(e) * (kCellCap + 1);
-  uint32_t* eOc = edgeOc + size_t(e) * kEdgeCap;
-  uint32_t* eIdx = edgeIdx + size_t(e) * kEdgeCap;
+  uint32_t* nbrCnt = ws.nbrCount + size_t(e) * (ws.cap.cells + 1);
+  uint32_t* eOc = edgeOc + size_t(e) * ws.cap.scratch;
+  uint32_t* eIdx = edgeIdx + size_t(e) * ws.cap.scratch;
+  const uint32_t edgeCap = min(ws.cap.edges, ws.cap.scratch);
   const uint32_t lane = laneId(), wpb = blockDim.x >> 5;
   const uint32_t S = gridDim.x * wpb, w = blockIdx.x * wpb + (threadIdx.x >> 5);
   for (uint32_t r0 = 0; w + r0 * S < ntot; r0 += 32) {
@@ -481,7 +485,7 @@ __global__ void __launch_bounds__(256, 6) kConnect(Workspace ws, uint32_t* edgeO
       myBase = joff[jl];
       myEnd = min(joff[jl + 1], nCells);
       if (myBase < myEnd) {
-        const uint16_t h = ws.cellInner[cb + myBase];
+        const uint32_t h = ws.cellInner[cb + myBase];
         myOb = ohOff[h];
         myM = min(ohOff[h + 1] - myOb, uint32_t(PF_MAX_CELLS_PER_HIT));
       }
@@ -494,7 +498,7 @@ __global__ void __launch_bounds__(256, 6) kConnect(Workspace ws, uint32_t* edgeO
       const uint32_t end = __shfl_sync(0xffffffffu, myEnd, l);
       const uint32_t ob = __shfl_sync(0xffffffffu, myOb, l);
       const uint32_t m = __shfl_sync(0xffffffffu, myM, l);
-      const uint16_t h = ws.cellInner[cb + base];
+      const uint32_t h = ws.cellInner[cb + base];
       const float ri = ws.cellInnerR[cb + base], zi = ws.cellInnerZ[cb + base];
       const float thetaCut = hh.detInd[h] < 1184 ? kThetaCutBarrel : kThetaCutForward;
       const float x2 = hh.xg[h], y2 = hh.yg[h];
@@ -505,7 +509,7 @@ __global__ void __launch_bounds__(256, 6) kConnect(Workspace ws, uint32_t* edgeO
         const uint32_t nc = min(32u, end - c0);
         float sro = 0.f, szo = 0.f, sx3 = 0.f, sy3 = 0.f;
         if (lane < nc) {
-          const uint16_t oh = ws.cellOuter[cb + c0 + lane];
+          const uint32_t oh = ws.cellOuter[cb + c0 + lane];
           sro = hh.rg[oh];
           szo = hh.zg[oh];
           sx3 = hh.xg[oh];
@@ -540,7 +544,7 @@ __global__ void __launch_bounds__(256, 6) kConnect(Workspace ws, uint32_t* edgeO
               ws.cellUsed[cb + idx] = 1;
               atomicAdd(&nbrCnt[oc], 1u);
               const uint32_t slot = at + __popc(mask & lanemaskLt());
-              if (slot < kEdgeCap) {
+              if (slot < edgeCap) {
                 eOc[slot] = oc;
                 eIdx[slot] = idx;
               } else {
@@ -558,13 +562,15 @@ __global__ void __launch_bounds__(256, 6) kConnect(Workspace ws, uint32_t* edgeO
 __global__ void kEdgeScatter(Workspace ws, const uint32_t* edgeOc, const uint32_t* edgeIdx) {
   uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
-  uint32_t n = min(c->nEdges, kEdgeCap);
-  const uint32_t* off = ws.nbrOff + size_t(e) * (kCellCap + 1);
-  uint32_t* cur = ws.nbrCount + size_t(e) * (kCellCap + 1);
+  const uint32_t edgeCap = min(ws.cap.edges, ws.cap.scratch);
+  uint32_t n = min(c->nEdges, edgeCap);
+  const uint32_t* off = ws.nbrOff + size_t(e) * (ws.cap.cells + 1);
+  uint32_t* cur = ws.nbrCount + size_t(e) * (ws.cap.cells + 1);
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    uint32_t oc = edgeOc[size_t(e) * kEdgeCap + k];
+    uint32_t oc = edgeOc[size_t(e) * ws.cap.scratch + k];
     uint32_t p = atomicAdd(&cur[oc], 1u);
-    if (off[oc] + p < kEdgeCap) ws.nbr[size_t(e) * kEdgeCap + off[oc] + p] = edgeIdx[size_t(e) * kEdgeCap + k];
+    if (off[oc] + p < edgeCap)
+      ws.nbr[size_t(e) * ws.cap.edges + off[oc] + p] = edgeIdx[size_t(e) * ws.cap.scratch + k];
     if (p == 1) noteSegment(ws, e, 1, oc);
   }
 }
@@ -574,7 +580,7 @@ __global__ void kNbrPool(Workspace ws) {
   uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   uint32_t n = c->nCells;
-  const uint32_t* off = ws.nbrOff + size_t(e) * (kCellCap + 1);
+  const uint32_t* off = ws.nbrOff + size_t(e) * (ws.cap.cells + 1);
   uint32_t local = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     local += (off[i + 1] > off[i]) ? 1u : 0u;
@@ -604,12 +610,12 @@ __global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws, bool 
   const uint32_t nHits = c->nHits;
   if (nHits < 2) return;
   const HitsView hh = hitsOf(ws, e);
-  const size_t cb = size_t(e) * kCellCap;
-  const uint32_t* ohOff = ws.ohOff + size_t(e) * (kHitCap + 1);
+  const size_t cb = size_t(e) * ws.cap.cells;
+  const uint32_t* ohOff = ws.ohOff + size_t(e) * (ws.cap.hits + 1);
   const uint32_t* ohCells = ws.ohCells + cb;
   const float4* ohRec = ws.ohRec + cb;
   const uint16_t* ohDet = ws.ohDet + cb;
-  const uint32_t* trkOff = ws.trkOff + size_t(e) * (kCellCap + 1);
+  const uint32_t* trkOff = ws.trkOff + size_t(e) * (ws.cap.cells + 1);
   const uint32_t w = threadIdx.x >> 5, lane = laneId();
   float* sx = sxA[w];
   float* sy = syA[w];
@@ -717,11 +723,11 @@ __global__ void kNtupletCount(Workspace ws) {
   uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   uint32_t n = c->nCells;
-  size_t cb = size_t(e) * kCellCap;
-  const uint32_t* nbrOff = ws.nbrOff + size_t(e) * (kCellCap + 1);
-  const uint32_t* nbr = ws.nbr + size_t(e) * kEdgeCap;
-  uint32_t* tc = ws.startTupleCount + size_t(e) * (kCellCap + 1);
-  uint32_t* hc = ws.startHitCount + size_t(e) * (kCellCap + 1);
+  size_t cb = size_t(e) * ws.cap.cells;
+  const uint32_t* nbrOff = ws.nbrOff + size_t(e) * (ws.cap.cells + 1);
+  const uint32_t* nbr = ws.nbr + size_t(e) * ws.cap.edges;
+  uint32_t* tc = ws.startTupleCount + size_t(e) * (ws.cap.cells + 1);
+  uint32_t* hc = ws.startHitCount + size_t(e) * (ws.cap.cells + 1);
   for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
     uint32_t nt = 0, nh = 0;
     if (isStartCell(ws, cb, idx)) {
@@ -740,21 +746,21 @@ __global__ void kNtupletWrite(Workspace ws) {
   uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   uint32_t n = c->nCells;
-  size_t cb = size_t(e) * kCellCap;
-  const uint32_t* nbrOff = ws.nbrOff + size_t(e) * (kCellCap + 1);
-  const uint32_t* nbr = ws.nbr + size_t(e) * kEdgeCap;
-  const uint32_t* to = ws.startTupleOff + size_t(e) * (kCellCap + 1);
-  const uint32_t* ho = ws.startHitOff + size_t(e) * (kCellCap + 1);
-  uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
-  uint16_t* th = ws.tupleHits + size_t(e) * kTupleHitCap;
-  uint32_t* tcell = ws.tupleCells + size_t(e) * kTupleCellCap;
-  uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  size_t cb = size_t(e) * ws.cap.cells;
+  const uint32_t* nbrOff = ws.nbrOff + size_t(e) * (ws.cap.cells + 1);
+  const uint32_t* nbr = ws.nbr + size_t(e) * ws.cap.edges;
+  const uint32_t* to = ws.startTupleOff + size_t(e) * (ws.cap.cells + 1);
+  const uint32_t* ho = ws.startHitOff + size_t(e) * (ws.cap.cells + 1);
+  uint32_t* toff = ws.tupleOff + size_t(e) * (ws.cap.tuples + 1);
+  uint32_t* th = ws.tupleHits + size_t(e) * ws.cap.tupleHits();
+  uint32_t* tcell = ws.tupleCells + size_t(e) * ws.cap.tupleCells();
+  uint8_t* q = ws.quality + size_t(e) * ws.cap.tuples;
   for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
     if (!isStartCell(ws, cb, idx)) continue;
     uint32_t m = to[idx], off = ho[idx];
-    if (m >= kTupleBins) continue;
+    if (m >= ws.cap.tuples) continue;
     dfsNtuplets(idx, ws.cellDoubletId + cb, nbrOff, nbr, ws.ca.minHits, [&](int ncells, const uint32_t* cells) {
-      if (m < kTupleBins) {
+      if (m < ws.cap.tuples) {
         toff[m] = off;
         for (int k = 0; k < ncells; ++k) {
           th[off + k] = ws.cellInner[cb + cells[k]];
@@ -775,17 +781,18 @@ __global__ void kTupleFinalize(Workspace ws) {
   uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   uint32_t m = c->apcM, nh = c->apcN;
-  uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
-  if (m >= kTupleBins) {
+  uint32_t* toff = ws.tupleOff + size_t(e) * (ws.cap.tuples + 1);
+  const uint32_t bins = ws.cap.tuples;
+  if (m >= bins) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-      toff[kTupleBins] = toff[kTupleBins - 1];
+      toff[bins] = toff[bins - 1];
       c->flags |= kFlagTupleOverflow;
     }
   } else {
-    for (uint32_t i = m + blockIdx.x * blockDim.x + threadIdx.x; i <= kTupleBins; i += gridDim.x * blockDim.x)
+    for (uint32_t i = m + blockIdx.x * blockDim.x + threadIdx.x; i <= bins; i += gridDim.x * blockDim.x)
       toff[i] = nh;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) c->nTuples = min(m, kTupleBins);
+  if (blockIdx.x == 0 && threadIdx.x == 0) c->nTuples = min(m, bins);
 }
 
 __device__ __forceinline__ uint32_t tupleSize(const uint32_t* toff, uint32_t t) { return toff[t + 1] - toff[t]; }
@@ -804,8 +811,8 @@ __global__ void kTrackCount(Workspace ws) {
   uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   uint32_t nt = c->nTuples;
-  const uint32_t* tcell = ws.tupleCells + size_t(e) * kTupleCellCap;
-  uint32_t* cnt = ws.trkCount + size_t(e) * (kCellCap + 1);
+  const uint32_t* tcell = ws.tupleCells + size_t(e) * ws.cap.tupleCells();
+  uint32_t* cnt = ws.trkCount + size_t(e) * (ws.cap.cells + 1);
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
     const uint32_t ncell = tupleCellCount(tcell, t);
     for (uint32_t k = 0; k < ncell; ++k) atomicAdd(&cnt[tcell[4 * t + k]], 1u);
@@ -816,16 +823,16 @@ __global__ void kTrackFill(Workspace ws) {
   uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   uint32_t nt = c->nTuples;
-  const uint32_t* tcell = ws.tupleCells + size_t(e) * kTupleCellCap;
-  const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
-  uint32_t* cur = ws.trkCount + size_t(e) * (kCellCap + 1);
-  uint16_t* trk = ws.trk + size_t(e) * kTupleCellCap;
+  const uint32_t* tcell = ws.tupleCells + size_t(e) * ws.cap.tupleCells();
+  const uint32_t* off = ws.trkOff + size_t(e) * (ws.cap.cells + 1);
+  uint32_t* cur = ws.trkCount + size_t(e) * (ws.cap.cells + 1);
+  uint32_t* trk = ws.trk + size_t(e) * ws.cap.tupleCells();
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
     const uint32_t ncell = tupleCellCount(tcell, t);
     for (uint32_t k = 0; k < ncell; ++k) {
       uint32_t cc = tcell[4 * t + k];
       uint32_t p = atomicAdd(&cur[cc], 1u);
-      trk[off[cc] + p] = uint16_t(t);
+      trk[off[cc] + p] = t;
       if (p == 1) noteSegment(ws, e, 2, cc);
     }
   }
@@ -840,8 +847,8 @@ __global__ void kTrackPool(Workspace ws, uint32_t* candFlag) {
   uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   uint32_t n = c->nCells;
-  const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
-  uint32_t* flag = candFlag + size_t(e) * (kCellCap + 1);
+  const uint32_t* off = ws.trkOff + size_t(e) * (ws.cap.cells + 1);
+  uint32_t* flag = candFlag + size_t(e) * (ws.cap.cells + 1);
   uint32_t local = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     uint32_t s = off[i + 1] - off[i];
@@ -855,9 +862,9 @@ __global__ void kTrackPool(Workspace ws, uint32_t* candFlag) {
 __global__ void kCandidateScatter(Workspace ws, const uint32_t* candFlag, const uint32_t* candOff) {
   uint32_t e = blockIdx.y;
   uint32_t n = ws.ev[e].nCells;
-  const uint32_t* f = candFlag + size_t(e) * (kCellCap + 1);
-  const uint32_t* o = candOff + size_t(e) * (kCellCap + 1);
-  uint32_t* cand = ws.candidates + size_t(e) * kCellCap;
+  const uint32_t* f = candFlag + size_t(e) * (ws.cap.cells + 1);
+  const uint32_t* o = candOff + size_t(e) * (ws.cap.cells + 1);
+  uint32_t* cand = ws.candidates + size_t(e) * ws.cap.cells;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     if (f[i]) cand[o[i]] = i;
 }
@@ -867,11 +874,11 @@ __global__ void kEarlyDup(Workspace ws) {
   uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   uint32_t nc = c->nCandidates;
-  const uint32_t* cand = ws.candidates + size_t(e) * kCellCap;
-  const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
-  const uint16_t* trk = ws.trk + size_t(e) * kTupleCellCap;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
-  uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  const uint32_t* cand = ws.candidates + size_t(e) * ws.cap.cells;
+  const uint32_t* off = ws.trkOff + size_t(e) * (ws.cap.cells + 1);
+  const uint32_t* trk = ws.trk + size_t(e) * ws.cap.tupleCells();
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (ws.cap.tuples + 1);
+  uint8_t* q = ws.quality + size_t(e) * ws.cap.tuples;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x) {
     uint32_t cell = cand[k];
     uint32_t b = off[cell], s = trkListSize(off, cell);
@@ -885,11 +892,11 @@ __global__ void kEarlyDup(Workspace ws) {
 // tuple hits -> detector indices (kernel_fillHitDetIndices)
 __global__ void kTupleDet(Workspace ws) {
   uint32_t e = blockIdx.y;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
-  uint32_t n = toff[kTupleBins];
-  const uint16_t* th = ws.tupleHits + size_t(e) * kTupleHitCap;
-  uint16_t* td = ws.tupleDet + size_t(e) * kTupleHitCap;
-  const uint16_t* det = ws.detInd + size_t(e) * kHitCap;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (ws.cap.tuples + 1);
+  uint32_t n = toff[ws.cap.tuples];
+  const uint32_t* th = ws.tupleHits + size_t(e) * ws.cap.tupleHits();
+  uint16_t* td = ws.tupleDet + size_t(e) * ws.cap.tupleHits();
+  const uint16_t* det = ws.detInd + size_t(e) * ws.cap.hits;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) td[k] = det[th[k]];
 }
 
@@ -905,10 +912,10 @@ __global__ void __launch_bounds__(1024) kMultiplicity(Workspace ws) {
   const uint32_t e = blockIdx.x;
   EventCounters* c = ws.ev + e;
   const uint32_t nt = c->nTuples;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
-  const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (ws.cap.tuples + 1);
+  const uint8_t* q = ws.quality + size_t(e) * ws.cap.tuples;
   uint32_t* tm = ws.tmOff + size_t(e) * 16;
-  uint16_t* bins = ws.tmBins + size_t(e) * kTupleBins;
+  uint32_t* bins = ws.tmBins + size_t(e) * ws.cap.tuples;
   auto binOf = [&](uint32_t t) -> uint32_t {  // 0: not binned
     const uint32_t nh = tupleSize(toff, t);
     return (nh < 3 || nh > 5 || q[t] == kDup) ? 0u : nh;
@@ -926,10 +933,15 @@ __global__ void __launch_bounds__(1024) kMultiplicity(Workspace ws) {
       start[b] = acc;
       tm[8 + b] = acc;  // start of bin b
       tm[b] = cnt[b];
-      if (cnt[b] > PF_MAX_TUPLES) c->flags |= kFlagFitBinOverflow;
+      if (cnt[b] > ws.cap.multiplicity) c->flags |= kFlagFitBinOverflow;
       acc += cnt[b];
     }
-    if (acc > PF_MAX_TUPLES) c->flags |= kFlagTmOverflow;
+    if (acc > ws.cap.multiplicity) c->flags |= kFlagTmOverflow;
+    // the neighbour and track list pools of the reference (CellNeighborsVector,
+    // CellTracksVector: cap.lists lists including the reserved empty one);
+    // beyond them its lists depend on the order the cells are visited
+    if (c->nNbrLists > ws.cap.lists) c->flags |= kFlagNbrPoolOverflow;
+    if (c->nTrkLists > ws.cap.lists) c->flags |= kFlagTrkPoolOverflow;
   }
   __syncthreads();
   uint64_t carry = 0;
@@ -941,7 +953,7 @@ __global__ void __launch_bounds__(1024) kMultiplicity(Workspace ws) {
     const uint64_t pre = blockExclusiveScan64(key, scanSh, &tot) + carry;
     if (b) {
       const uint32_t pos = start[b] + uint32_t((pre >> (20 * (b - 3))) & 0xfffffu);
-      if (pos < kTupleBins) bins[pos] = uint16_t(t);
+      if (pos < ws.cap.tuples) bins[pos] = t;
     }
     carry += tot;
   }
@@ -953,11 +965,11 @@ __global__ void __launch_bounds__(1024) kMultiplicity(Workspace ws) {
 __global__ void kClassify(Workspace ws) {
   uint32_t e = blockIdx.y;
   uint32_t nt = ws.ev[e].nTuples;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
-  uint8_t* q = ws.quality + size_t(e) * kTupleBins;
-  const float* st = ws.state + size_t(e) * kTupleBins * 5;
-  const float* pt = ws.pt + size_t(e) * kTupleBins;
-  const float* chi2 = ws.chi2 + size_t(e) * kTupleBins;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (ws.cap.tuples + 1);
+  uint8_t* q = ws.quality + size_t(e) * ws.cap.tuples;
+  const float* st = ws.state + size_t(e) * ws.cap.tuples * 5;
+  const float* pt = ws.pt + size_t(e) * ws.cap.tuples;
+  const float* chi2 = ws.chi2 + size_t(e) * ws.cap.tuples;
   const float c0 = float(0.68177776), c1 = float(0.74609577), c2 = float(-0.08035491), c3 = float(0.00315399);
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
     uint32_t nh = tupleSize(toff, t);
@@ -976,7 +988,7 @@ __global__ void kClassify(Workspace ws) {
   }
 }
 
-__device__ __forceinline__ bool inTrkList(const uint32_t* off, const uint16_t* trk, uint32_t cell, uint16_t t) {
+__device__ __forceinline__ bool inTrkList(const uint32_t* off, const uint32_t* trk, uint32_t cell, uint32_t t) {
   uint32_t b = off[cell], s = off[cell + 1] - b;
   if (s <= uint32_t(PF_MAX_CELL_TRACKS)) return true;  // t is known to be in the full list
   return t <= trk[b + PF_MAX_CELL_TRACKS - 1];
@@ -989,18 +1001,18 @@ __device__ __forceinline__ bool inTrkList(const uint32_t* off, const uint16_t* t
 __global__ void kFastDupInDegree(Workspace ws, uint32_t* indeg, const uint32_t* candFlag) {
   uint32_t e = blockIdx.y;
   uint32_t nc = ws.ev[e].nCandidates;
-  const uint32_t* cand = ws.candidates + size_t(e) * kCellCap;
-  const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
-  const uint16_t* trk = ws.trk + size_t(e) * kTupleCellCap;
-  const uint32_t* tcell = ws.tupleCells + size_t(e) * kTupleCellCap;
-  const uint32_t* flag = candFlag + size_t(e) * (kCellCap + 1);
-  uint32_t* deg = indeg + size_t(e) * kCellCap;
+  const uint32_t* cand = ws.candidates + size_t(e) * ws.cap.cells;
+  const uint32_t* off = ws.trkOff + size_t(e) * (ws.cap.cells + 1);
+  const uint32_t* trk = ws.trk + size_t(e) * ws.cap.tupleCells();
+  const uint32_t* tcell = ws.tupleCells + size_t(e) * ws.cap.tupleCells();
+  const uint32_t* flag = candFlag + size_t(e) * (ws.cap.cells + 1);
+  uint32_t* deg = indeg + size_t(e) * ws.cap.cells;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x) {
     uint32_t cell = cand[k];
     uint32_t b = off[cell], s = trkListSize(off, cell);
     uint32_t d = 0;
     for (uint32_t j = 0; j < s; ++j) {
-      uint16_t t = trk[b + j];
+      uint32_t t = trk[b + j];
       uint32_t ncell = tupleCellCount(tcell, t);
       for (uint32_t q = 0; q < ncell; ++q) {
         uint32_t o = tcell[4 * t + q];
@@ -1029,16 +1041,16 @@ __global__ void __launch_bounds__(kFastDupThreads)
   uint32_t* N = cl.map_shared_rank(sN, 0);
   const uint32_t e = blockIdx.y;
   const uint32_t nc = ws.ev[e].nCandidates;
-  const uint32_t* cand = ws.candidates + size_t(e) * kCellCap;
-  const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
-  const uint16_t* trk = ws.trk + size_t(e) * kTupleCellCap;
-  const uint32_t* tcell = ws.tupleCells + size_t(e) * kTupleCellCap;
-  const uint32_t* flag = candFlag + size_t(e) * (kCellCap + 1);
-  const uint32_t* cidx = candOff + size_t(e) * (kCellCap + 1);
-  uint32_t* deg = indeg + size_t(e) * kCellCap;
-  uint32_t* L[2] = {lists + size_t(e) * kEdgeCap, lists + size_t(e) * kEdgeCap + kCellCap};
-  uint8_t* q = ws.quality + size_t(e) * kTupleBins;
-  const float* tip = ws.state + size_t(e) * kTupleBins * 5 + 1;
+  const uint32_t* cand = ws.candidates + size_t(e) * ws.cap.cells;
+  const uint32_t* off = ws.trkOff + size_t(e) * (ws.cap.cells + 1);
+  const uint32_t* trk = ws.trk + size_t(e) * ws.cap.tupleCells();
+  const uint32_t* tcell = ws.tupleCells + size_t(e) * ws.cap.tupleCells();
+  const uint32_t* flag = candFlag + size_t(e) * (ws.cap.cells + 1);
+  const uint32_t* cidx = candOff + size_t(e) * (ws.cap.cells + 1);
+  uint32_t* deg = indeg + size_t(e) * ws.cap.cells;
+  uint32_t* L[2] = {lists + size_t(e) * ws.cap.scratch, lists + size_t(e) * ws.cap.scratch + ws.cap.cells};
+  uint8_t* q = ws.quality + size_t(e) * ws.cap.tuples;
+  const float* tip = ws.state + size_t(e) * ws.cap.tuples * 5 + 1;
   const uint32_t gtid = r * blockDim.x + threadIdx.x, gstride = P * blockDim.x;
   if (r == 0 && threadIdx.x < 2) sN[threadIdx.x] = 0;
   cl.sync();
@@ -1059,9 +1071,9 @@ __global__ void __launch_bounds__(kFastDupThreads)
       const uint32_t cell = cand[Lc[i]];
       const uint32_t b = off[cell], s = trkListSize(off, cell);
       float mc = 10000.f;
-      uint16_t im = 60000;
+      uint32_t im = kNoTuple;
       for (uint32_t j = 0; j < s; ++j) {
-        const uint16_t t = trk[b + j];
+        const uint32_t t = trk[b + j];
         const float score = fabsf(tip[size_t(t) * 5]);
         if (q[t] == kLoose && score < mc) {
           mc = score;
@@ -1069,12 +1081,12 @@ __global__ void __launch_bounds__(kFastDupThreads)
         }
       }
       for (uint32_t j = 0; j < s; ++j) {
-        const uint16_t t = trk[b + j];
+        const uint32_t t = trk[b + j];
         if (q[t] != kBad && t != im) q[t] = kDup;
       }
       // release later candidates sharing a track
       for (uint32_t j = 0; j < s; ++j) {
-        const uint16_t t = trk[b + j];
+        const uint32_t t = trk[b + j];
         const uint32_t ncell = tupleCellCount(tcell, t);
         for (uint32_t qq = 0; qq < ncell; ++qq) {
           const uint32_t o = tcell[4 * t + qq];
@@ -1095,10 +1107,10 @@ __global__ void __launch_bounds__(kFastDupThreads)
 __global__ void kHitToTupleCount(Workspace ws) {
   uint32_t e = blockIdx.y;
   uint32_t nt = ws.ev[e].nTuples;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
-  const uint16_t* th = ws.tupleHits + size_t(e) * kTupleHitCap;
-  const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
-  uint32_t* cnt = ws.h2tCount + size_t(e) * (kHitCap + 1);
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (ws.cap.tuples + 1);
+  const uint32_t* th = ws.tupleHits + size_t(e) * ws.cap.tupleHits();
+  const uint8_t* q = ws.quality + size_t(e) * ws.cap.tuples;
+  uint32_t* cnt = ws.h2tCount + size_t(e) * (ws.cap.hits + 1);
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
     if (tupleSize(toff, t) == 0 || q[t] != kLoose) continue;
     for (uint32_t k = toff[t]; k < toff[t + 1]; ++k) atomicAdd(&cnt[th[k]], 1u);
@@ -1108,21 +1120,21 @@ __global__ void kHitToTupleFill(Workspace ws) {
   uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   uint32_t nt = c->nTuples;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
-  const uint16_t* th = ws.tupleHits + size_t(e) * kTupleHitCap;
-  const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
-  const uint32_t* off = ws.h2tOff + size_t(e) * (kHitCap + 1);
-  uint32_t* cur = ws.h2tCount + size_t(e) * (kHitCap + 1);
-  uint16_t* h2t = ws.h2t + size_t(e) * kH2TCap;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (ws.cap.tuples + 1);
+  const uint32_t* th = ws.tupleHits + size_t(e) * ws.cap.tupleHits();
+  const uint8_t* q = ws.quality + size_t(e) * ws.cap.tuples;
+  const uint32_t* off = ws.h2tOff + size_t(e) * (ws.cap.hits + 1);
+  uint32_t* cur = ws.h2tCount + size_t(e) * (ws.cap.hits + 1);
+  uint32_t* h2t = ws.h2t + size_t(e) * ws.cap.h2t;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
     if (tupleSize(toff, t) == 0 || q[t] != kLoose) continue;
     for (uint32_t k = toff[t]; k < toff[t + 1]; ++k) {
-      uint16_t h = th[k];
+      uint32_t h = th[k];
       uint32_t p = atomicAdd(&cur[h], 1u);
       uint32_t pos = off[h] + p;
       if (p == 1) noteSegment(ws, e, 3, h);
-      if (pos < kH2TCap)
-        h2t[pos] = uint16_t(t);
+      if (pos < ws.cap.h2t)
+        h2t[pos] = t;
       else
         atomicOr(&c->flags, kFlagH2TOverflow);
     }
@@ -1132,13 +1144,13 @@ __global__ void kHitToTupleFill(Workspace ws) {
 // kernel_tripletCleaner: one thread per hit with >= 2 loose tuples
 __global__ void kTripletCleaner(Workspace ws) {
   uint32_t e = blockIdx.y;
-  const uint32_t* off = ws.h2tOff + size_t(e) * (kHitCap + 1);
-  const uint16_t* h2t = ws.h2t + size_t(e) * kH2TCap;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
-  uint8_t* q = ws.quality + size_t(e) * kTupleBins;
-  const float* tip = ws.state + size_t(e) * kTupleBins * 5 + 1;
-  for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < kHitCap; h += gridDim.x * blockDim.x) {
-    uint32_t b = off[h], en = min(off[h + 1], kH2TCap);
+  const uint32_t* off = ws.h2tOff + size_t(e) * (ws.cap.hits + 1);
+  const uint32_t* h2t = ws.h2t + size_t(e) * ws.cap.h2t;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (ws.cap.tuples + 1);
+  uint8_t* q = ws.quality + size_t(e) * ws.cap.tuples;
+  const float* tip = ws.state + size_t(e) * ws.cap.tuples * 5 + 1;
+  for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < ws.cap.hits; h += gridDim.x * blockDim.x) {
+    uint32_t b = off[h], en = min(off[h + 1], ws.cap.h2t);
     if (en <= b || en - b < 2) continue;
     uint32_t maxNh = 0;
     for (uint32_t p = b; p < en; ++p) maxNh = max(maxNh, tupleSize(toff, h2t[p]));
@@ -1146,9 +1158,9 @@ __global__ void kTripletCleaner(Workspace ws) {
       if (tupleSize(toff, h2t[p]) != maxNh) q[h2t[p]] = kDup;
     if (maxNh > 3) continue;
     float mc = 10000.f;
-    uint16_t im = 60000;
+    uint32_t im = kNoTuple;
     for (uint32_t p = b; p < en; ++p) {
-      uint16_t t = h2t[p];
+      uint32_t t = h2t[p];
       float s = fabsf(tip[size_t(t) * 5]);
       if (q[t] != kBad && s < mc) {
         mc = s;
@@ -1156,7 +1168,7 @@ __global__ void kTripletCleaner(Workspace ws) {
       }
     }
     for (uint32_t p = b; p < en; ++p) {
-      uint16_t t = h2t[p];
+      uint32_t t = h2t[p];
       if (q[t] != kBad && t != im) q[t] = kDup;
     }
   }
@@ -1167,10 +1179,10 @@ __global__ void kTripletCleaner(Workspace ws) {
 __global__ void kFishboneCleaner(Workspace ws) {
   const uint32_t e = blockIdx.y;
   const uint32_t n = ws.ev[e].nCells;
-  const size_t cb = size_t(e) * kCellCap;
-  const uint32_t* off = ws.trkOff + size_t(e) * (kCellCap + 1);
-  const uint16_t* trk = ws.trk + size_t(e) * kTupleCellCap;
-  uint8_t* q = ws.quality + size_t(e) * kTupleBins;
+  const size_t cb = size_t(e) * ws.cap.cells;
+  const uint32_t* off = ws.trkOff + size_t(e) * (ws.cap.cells + 1);
+  const uint32_t* trk = ws.trk + size_t(e) * ws.cap.tupleCells();
+  uint8_t* q = ws.quality + size_t(e) * ws.cap.tuples;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     if (ws.cellDoubletId[cb + i] >= 0) continue;
     const uint32_t b = off[i], s = trkListSize(off, i);
@@ -1184,6 +1196,8 @@ __global__ void kFishboneCleaner(Workspace ws) {
 
 cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   (void)es;
+  const uint32_t kHitCap = ws.cap.hits, kCellCap = ws.cap.cells, kJCap = ws.cap.jCap;
+  const uint32_t kTupleCellCap = ws.cap.tupleCells();
   const uint32_t gx = nEvents >= 32 ? 16 : (nEvents >= 8 ? 64 : 296);  // blocks per event for flat loops
   dim3 g(gx, nEvents);
   // ---- doublets: count per inner-hit slot, scan, write in serial order
@@ -1203,7 +1217,8 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   PG_PROBED("kConnect", stream, kConnect<<<dim3(tunedGrid(ws, kTuneConnect, gx * 4), nEvents), 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
   segScan(ws.nbrCount, ws.nbrOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanSums, nEvents, stream, true);
   PG_PROBED("kEdgeScatter", stream, kEdgeScatter<<<dim3(tunedGrid(ws, kTuneEdgeScatter, gx), nEvents), 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
-  sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.nbr, kEdgeCap, ws.nbrOff, kCellCap + 1, EVF(nCells), 0, false, kEdgeCap, 1);
+  sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.nbr, ws.cap.edges, ws.nbrOff, kCellCap + 1, EVF(nCells), 0, false,
+                         min(ws.cap.edges, ws.cap.scratch), 1);
   PG_PROBED("kNbrPool", stream, kNbrPool<<<dim3(tunedGrid(ws, kTuneNbrPool, gx), nEvents), 256, 0, stream>>>(ws));
   // ---- early fishbone
   if (ws.ca.earlyFishbone)
@@ -1219,7 +1234,7 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   PG_PROBED("kTrackCount", stream, kTrackCount<<<dim3(tunedGrid(ws, kTuneTrackCount, gx), nEvents), 256, 0, stream>>>(ws));
   segScan(ws.trkCount, ws.trkOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanSums, nEvents, stream, true);
   PG_PROBED("kTrackFill", stream, kTrackFill<<<dim3(tunedGrid(ws, kTuneTrackFill, gx), nEvents), 256, 0, stream>>>(ws));
-  sortSegments<uint16_t>(ws, nEvents, stream, gx * 2, ws.trk, kTupleCellCap, ws.trkOff, kCellCap + 1, EVF(nCells), 0, false, kTupleCellCap, 2);
+  sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.trk, kTupleCellCap, ws.trkOff, kCellCap + 1, EVF(nCells), 0, false, kTupleCellCap, 2);
   uint32_t* candFlag = ws.startTupleCount;  // scratch
   uint32_t* candOff = ws.startHitCount;
   PG_PROBED("kTrackPool", stream, kTrackPool<<<dim3(tunedGrid(ws, kTuneTrackPool, gx), nEvents), 256, 0, stream>>>(ws, candFlag));
@@ -1236,6 +1251,7 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
 }
 
 cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
+  const uint32_t kHitCap = ws.cap.hits;
   const uint32_t gx = nEvents >= 32 ? 16 : (nEvents >= 8 ? 64 : 296);
   dim3 g(gx, nEvents);
   PG_PROBED("kClassify", stream, kClassify<<<dim3(tunedGrid(ws, kTuneClassify, gx), nEvents), 256, 0, stream>>>(ws));
@@ -1244,8 +1260,8 @@ cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   // fastDuplicateRemover (candFlag survives in startTupleCount from runCA)
   uint32_t* candFlag = ws.startTupleCount;
   uint32_t* candOff = ws.startHitCount;  // candidate index of each cell, from runCA
-  uint32_t* indeg = ws.scratchA;        // [maxEvents][kEdgeCap] >= kCellCap
-  uint32_t* lists = ws.scratchB;        // two worklists of kCellCap per event
+  uint32_t* indeg = ws.scratchA;        // [maxEvents][cap.scratch], cap.cells per event used
+  uint32_t* lists = ws.scratchB;        // two worklists of cap.cells per event (cap.scratch >= 2 cap.cells)
   PG_PROBED("kFastDupInDegree", stream, kFastDupInDegree<<<dim3(tunedGrid(ws, kTuneFastDupInDegree, gx), nEvents), 256, 0, stream>>>(ws, indeg, candFlag));
   const uint32_t P = nEvents <= kClusterMaxEvents ? kFastDupCtas : 2;
   cudaError_t le = cudaSuccess;
@@ -1258,7 +1274,8 @@ cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   PG_PROBED("kHitToTupleCount", stream, kHitToTupleCount<<<dim3(tunedGrid(ws, kTuneHitToTupleCount, gx), nEvents), 256, 0, stream>>>(ws));
   segScan(ws.h2tCount, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, nullptr, 0, ws.scanSums, nEvents, stream, true);
   PG_PROBED("kHitToTupleFill", stream, kHitToTupleFill<<<dim3(tunedGrid(ws, kTuneHitToTupleFill, gx), nEvents), 256, 0, stream>>>(ws));
-  sortSegments<uint16_t>(ws, nEvents, stream, gx * 2, ws.h2t, kH2TCap, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, true, kH2TCap, 3);
+  sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.h2t, ws.cap.h2t, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, true,
+                         ws.cap.h2t, 3);
   PG_PROBED("kTripletCleaner", stream, kTripletCleaner<<<dim3(tunedGrid(ws, kTuneTripletCleaner, gx * 2), nEvents), 256, 0, stream>>>(ws));
   return cudaGetLastError();
 }

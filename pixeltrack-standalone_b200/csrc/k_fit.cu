@@ -354,9 +354,9 @@ __global__ void kFitZero(Workspace ws) {
   const uint32_t e = blockIdx.y;
   const uint32_t nt = ws.ev[e].nTuples;
   const bool all = (ws.ev[e].flags & (kFlagFitBinOverflow | kFlagTmOverflow)) != 0;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
-  const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
-  const size_t tb = size_t(e) * kTupleBins;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (ws.cap.tuples + 1);
+  const uint8_t* q = ws.quality + size_t(e) * ws.cap.tuples;
+  const size_t tb = size_t(e) * ws.cap.tuples;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
     if (!all && toff[t + 1] - toff[t] >= 3 && q[t] != 1) continue;  // 1: duplicate
     for (int k = 0; k < 5; ++k) ws.state[tb * 5 + size_t(t) * 5 + k] = 0.f;
@@ -372,17 +372,17 @@ template <int N, bool kRiemann = false>
 __device__ __forceinline__ void blFitBin(const DeviceES& es, const Workspace& ws, uint32_t nh) {
   uint32_t e = blockIdx.y;
   const uint32_t* tm = ws.tmOff + size_t(e) * 16;
-  uint32_t size = min(tm[nh], uint32_t(PF_MAX_TUPLES));
+  uint32_t size = min(tm[nh], ws.cap.multiplicity);
   uint32_t start = tm[8 + nh];
-  const uint16_t* bins = ws.tmBins + size_t(e) * kTupleBins;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
-  const uint16_t* th = ws.tupleHits + size_t(e) * kTupleHitCap;
-  size_t hb = size_t(e) * kHitCap;
-  size_t tb = size_t(e) * kTupleBins;
+  const uint32_t* bins = ws.tmBins + size_t(e) * ws.cap.tuples;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (ws.cap.tuples + 1);
+  const uint32_t* th = ws.tupleHits + size_t(e) * ws.cap.tupleHits();
+  size_t hb = size_t(e) * ws.cap.hits;
+  size_t tb = size_t(e) * ws.cap.tuples;
   const double B = double(float(0.0114256972711507));
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < size; k += gridDim.x * blockDim.x) {
     uint32_t tkid = bins[start + k];
-    const uint16_t* hid = th + toff[tkid];
+    const uint32_t* hid = th + toff[tkid];
     double H[3 * N];
     float ge[6 * N];
 #pragma unroll

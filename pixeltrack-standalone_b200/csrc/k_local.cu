@@ -184,7 +184,7 @@ __global__ void kInitEvents(Workspace ws, uint32_t nEvents) {
     c->nBigMod = 0;
     c->nSegList[0] = c->nSegList[1] = c->nSegList[2] = c->nSegList[3] = 0;
     c->nBigHitMod = 0;
-    c->flags = c->nWords > kMaxFedWords ? kFlagTooManyWords : 0u;
+    c->flags = c->nWords > ws.cap.fedWords ? kFlagTooManyWords : 0u;
   }
   uint32_t* cim = ws.clusInModule + size_t(e) * kModStride;
   for (uint32_t i = threadIdx.x; i < kModStride; i += blockDim.x) {
@@ -805,7 +805,7 @@ __global__ void kHitsModuleStart(DeviceES es, Workspace ws) {
     uint32_t v = i < kMaxModules ? min(uint32_t(PF_MAX_CLUS_PER_MODULE), cim[i]) : 0u;
     uint32_t tot;
     uint32_t inc = blockExclusiveScan(v, scanSh, &tot) + v;
-    if (i < kMaxModules) cms[i + 1] = min(carry + inc, uint32_t(PF_MAX_HITS));
+    if (i < kMaxModules) cms[i + 1] = min(carry + inc, ws.cap.hits);
     carry += tot;
   }
   if (threadIdx.x == 0) cms[0] = 0;
@@ -813,7 +813,7 @@ __global__ void kHitsModuleStart(DeviceES es, Workspace ws) {
   EventCounters* c = ws.ev + e;
   if (threadIdx.x == 0) {
     c->nHits = cms[kMaxModules];
-    if (carry > PF_MAX_HITS) c->flags |= kFlagHitOverflow;
+    if (carry > ws.cap.hits) c->flags |= kFlagHitOverflow;
   }
   if (threadIdx.x < 11) c->layerStart[threadIdx.x] = cms[es.lg->layerStart[threadIdx.x]];
   PfAverageGeometry* agc = ws.agc + e;
@@ -929,7 +929,7 @@ __device__ void hitsModuleBlock(const DeviceES& es, const Workspace& ws, uint32_
   const PfDetParams& dp = es.det[me];
   const PfCommonParams& cp = *es.common;
   const PfBeamSpot& bs = *es.bs;
-  const size_t hb = size_t(e) * kHitCap;
+  const size_t hb = size_t(e) * ws.cap.hits;
   const uint32_t cmsMe = ws.clusModuleStart[size_t(e) * kModStride + me];
   for (int startClus = 0; startClus < nclus; startClus += kHitBatch) {
     int nIn = min(kHitBatch, nclus - startClus);
@@ -970,7 +970,7 @@ __device__ void hitsModuleBlock(const DeviceES& es, const Workspace& ws, uint32_
     __syncthreads();
     for (int ic = threadIdx.x; ic < nIn; ic += blockDim.x) {
       uint32_t h = cmsMe + startClus + ic;
-      if (h >= uint32_t(PF_MAX_HITS)) continue;
+      if (h >= ws.cap.hits) continue;
       writeHit(ws, hb, h, me, dp, cp, bs, minRow[ic], maxRow[ic], minCol[ic], maxCol[ic], Qfx[ic], Qlx[ic], Qfy[ic],
                Qly[ic], chg[ic]);
     }
@@ -1057,8 +1057,8 @@ __global__ void __launch_bounds__(kHitWarps * 32) kGetHitsSmall(DeviceES es, Wor
   __syncwarp();
   if (lane < nclus) {
     const uint32_t h = ws.clusModuleStart[size_t(e) * kModStride + me] + lane;
-    if (h < uint32_t(PF_MAX_HITS))
-      writeHit(ws, size_t(e) * kHitCap, h, me, es.det[me], *es.common, *es.bs, minRow[lane], maxRow[lane],
+    if (h < ws.cap.hits)
+      writeHit(ws, size_t(e) * ws.cap.hits, h, me, es.det[me], *es.common, *es.bs, minRow[lane], maxRow[lane],
                minCol[lane], maxCol[lane], Qfx[lane], Qlx[lane], Qfy[lane], Qly[lane], chg[lane]);
   }
 }
@@ -1077,7 +1077,7 @@ __global__ void kPhiCount(Workspace ws) {
   const EventCounters* c = ws.ev + e;
   uint32_t nt = c->layerStart[10];
   uint32_t* off = ws.phiOff + size_t(e) * kPhiStride;
-  const int16_t* iphi = ws.iphi + size_t(e) * kHitCap;
+  const int16_t* iphi = ws.iphi + size_t(e) * ws.cap.hits;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
     uint32_t b = phiBinOf(iphi[i]) + 128 * layerOfHit(c->layerStart, i);
     atomicAdd(&off[b], 1u);
@@ -1091,12 +1091,12 @@ __global__ void kPhiFill(Workspace ws, uint32_t* cursor) {
   uint32_t nt = c->layerStart[10];
   const uint32_t* off = ws.phiOff + size_t(e) * kPhiStride;
   uint32_t* cur = cursor + size_t(e) * kPhiStride;
-  const int16_t* iphi = ws.iphi + size_t(e) * kHitCap;
-  uint16_t* bins = ws.phiBins + size_t(e) * kHitCap;
+  const int16_t* iphi = ws.iphi + size_t(e) * ws.cap.hits;
+  uint32_t* bins = ws.phiBins + size_t(e) * ws.cap.hits;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
     uint32_t b = phiBinOf(iphi[i]) + 128 * layerOfHit(c->layerStart, i);
     uint32_t p = atomicAdd(&cur[b], 1u);
-    bins[off[b] + p] = uint16_t(i);
+    bins[off[b] + p] = i;
   }
 }
 
@@ -1107,7 +1107,7 @@ __global__ void kPhiSort(Workspace ws) {
   if (b >= kPhiTot - 1) return;
   if (ws.ev[e].nHits == 0) return;
   const uint32_t* off = ws.phiOff + size_t(e) * kPhiStride;
-  uint16_t* bins = ws.phiBins + size_t(e) * kHitCap;
+  uint32_t* bins = ws.phiBins + size_t(e) * ws.cap.hits;
   warpSortSegment(bins + off[b], off[b + 1] - off[b], true);
 }
 
@@ -1116,15 +1116,17 @@ __global__ void kPhiSort(Workspace ws) {
 __global__ void kPhiRec(Workspace ws) {
   const uint32_t e = blockIdx.y;
   const uint32_t n = ws.phiOff[size_t(e) * kPhiStride + kPhiTot - 1];
-  const size_t hb = size_t(e) * kHitCap;
-  const uint16_t* bins = ws.phiBins + hb;
+  const size_t hb = size_t(e) * ws.cap.hits;
+  const uint32_t* bins = ws.phiBins + hb;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     const uint32_t h = bins[p];
     uint4 r;
     r.x = __float_as_uint(ws.zg[hb + h]);
     r.y = __float_as_uint(ws.rg[hb + h]);
     r.z = uint32_t(uint16_t(ws.iphi[hb + h])) | (uint32_t(uint16_t(ws.ysize[hb + h])) << 16);
-    r.w = uint32_t(ws.detInd[hb + h]) | (h << 16);
+    // the module index saturates at 2047, which the doublet search rejects
+    // like any index above 2000; the hit index takes the upper 21 bits
+    r.w = min(uint32_t(ws.detInd[hb + h]), 2047u) | (h << 11);
     ws.phiRec[hb + p] = r;
   }
 }

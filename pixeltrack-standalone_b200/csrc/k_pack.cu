@@ -6,6 +6,8 @@
 // loose, in tuple order) with their fit state, covariance, hits and vertex
 // assignment, and the vertices.  The destination is mapped pinned host memory,
 // so the transfer is exact-sized and needs no host synchronisation.
+#include <atomic>
+
 #include <cooperative_groups.h>
 
 #include "device_utils.cuh"
@@ -51,23 +53,28 @@ __device__ __forceinline__ uint32_t packHalves(uint32_t w, uint32_t n, F&& get) 
 // at once; the gathers come from device memory.
 constexpr uint32_t kPackCtas = 8;  // CTAs per event in a small batch
 
+// dynamic shared memory: the slice's loose tuple indices and the whole list
+constexpr size_t kPackSmemBytes = 2 * size_t(kResultTracks) * sizeof(uint32_t);
+
 __global__ void __launch_bounds__(512) kPackResults(Workspace ws, uint8_t* out) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   const uint32_t r = cl.block_rank(), P = cl.num_blocks();
+  extern __shared__ __align__(16) uint32_t packSm[];
+  uint32_t* sLocal = packSm;
+  uint32_t* sIdx = packSm + kResultTracks;
   __shared__ uint32_t scanSh[33];
-  __shared__ uint16_t sLocal[kResultTracks];
-  __shared__ uint16_t sIdx[kResultTracks];
   __shared__ uint32_t sCount;
   __shared__ uint32_t sOff[kPackCtas + 1];  // P <= kPackCtas
   const uint32_t e = blockIdx.y;
   const EventCounters* c = ws.ev + e;
   uint8_t* base = out + size_t(e) * kResultStride;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
-  const uint16_t* th = ws.tupleHits + size_t(e) * kTupleHitCap;
-  const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
-  const size_t tb = size_t(e) * kTupleBins;
-  const uint32_t guard = c->apcM >= kTupleBins ? kTupleBins - 1 : c->nTuples;
+  const uint32_t bins = ws.cap.tuples;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (bins + 1);
+  const uint32_t* th = ws.tupleHits + size_t(e) * ws.cap.tupleHits();
+  const uint8_t* q = ws.quality + size_t(e) * bins;
+  const size_t tb = size_t(e) * bins;
+  const uint32_t guard = c->apcM >= bins ? bins - 1 : c->nTuples;
   // ---- this CTA's slice of the tuples: loose ones in tuple order
   const uint32_t chunk = (guard + P - 1) / P;
   const uint32_t lo = min(guard, r * chunk), hi = min(guard, lo + chunk);
@@ -77,7 +84,7 @@ __global__ void __launch_bounds__(512) kPackResults(Workspace ws, uint8_t* out) 
     const uint32_t loose = (t < hi && q[t] >= 2) ? 1u : 0u;
     uint32_t tot;
     const uint32_t p = carry + blockExclusiveScan(loose, scanSh, &tot);
-    if (loose && p < kResultTracks) sLocal[p] = uint16_t(t);
+    if (loose && p < kResultTracks) sLocal[p] = t;
     carry += tot;
   }
   if (threadIdx.x == 0) sCount = carry;
@@ -95,7 +102,7 @@ __global__ void __launch_bounds__(512) kPackResults(Workspace ws, uint8_t* out) 
   const uint32_t n = min(nLoose, kResultTracks);
   // ---- the whole list, gathered from the cluster's shared memories
   for (uint32_t k = 0; k < P; ++k) {
-    const uint16_t* src = cl.map_shared_rank(sLocal, k);
+    const uint32_t* src = cl.map_shared_rank(sLocal, k);
     const uint32_t o = sOff[k], m = min(sOff[k + 1], n) > o ? min(sOff[k + 1], n) - o : 0u;
     for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) sIdx[o + j] = src[j];
   }
@@ -131,12 +138,11 @@ __global__ void __launch_bounds__(512) kPackResults(Workspace ws, uint8_t* out) 
   f = reinterpret_cast<float*>(base + kResOffChi2);
   for (uint32_t j = a + threadIdx.x; j < b; j += T) f[j] = ws.chi2[tb + sIdx[j]];
   w32 = reinterpret_cast<uint32_t*>(base + kResOffHits);
-  sl((5 * n + 1) / 2, a, b);
-  for (uint32_t w = a + threadIdx.x; w < b; w += T)
-    w32[w] = packHalves(w, 5 * n, [&](uint32_t i) {
-      const uint32_t t = sIdx[i / 5], k = i % 5;
-      return k < toff[t + 1] - toff[t] ? uint32_t(th[toff[t] + k]) : 0xffffu;
-    });
+  sl(5 * n, a, b);
+  for (uint32_t i = a + threadIdx.x; i < b; i += T) {
+    const uint32_t t = sIdx[i / 5], k = i % 5;
+    w32[i] = k < toff[t + 1] - toff[t] ? th[toff[t] + k] : 0xffffffffu;
+  }
   const bool hasVtx = c->nVertices > 0;
   w32 = reinterpret_cast<uint32_t*>(base + kResOffVertex);
   sl((n + 1) / 2, a, b);
@@ -171,6 +177,9 @@ __global__ void __launch_bounds__(512) kPackResults(Workspace ws, uint8_t* out) 
     h.nTupleHits = toff[guard];
     h.nModules = c->nModules;
     *reinterpret_cast<ResultHeader*>(base) = h;
+    // the loose-track count of pg_event_counts (the last writer of the
+    // quality codes, the triplet cleaner, has finished)
+    ws.ev[e].nLoose = nLoose;
   }
 }
 
@@ -181,9 +190,19 @@ void launchSetInput(Workspace& ws, const uint32_t* words, const uint8_t* fedIds,
 }
 
 void launchPack(Workspace& ws, uint32_t nEvents, uint8_t* out, cudaStream_t s) {
+  // opt in to more than 48 KB of dynamic shared memory, once per device
+  static std::atomic<uint64_t> ready{0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const uint64_t bit = uint64_t(1) << (dev & 63);
+  if (!(ready.load() & bit)) {
+    if (cudaFuncSetAttribute(kPackResults, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPackSmemBytes)) ==
+        cudaSuccess)
+      ready.fetch_or(bit);
+  }
   const uint32_t P = nEvents <= kClusterMaxEvents ? kPackCtas : 1;
   // a failed launch is reported by the stream's next error check
-  PG_PROBED("kPackResults", s, (void)launchClustered(kPackResults, P, nEvents, 512, 0, s, ws, out));
+  PG_PROBED("kPackResults", s, (void)launchClustered(kPackResults, P, nEvents, 512, kPackSmemBytes, s, ws, out));
 }
 
 }  // namespace pixgpu

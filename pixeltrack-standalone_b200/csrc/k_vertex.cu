@@ -22,19 +22,22 @@ namespace pixgpu {
 
 namespace {
 
-static_assert(kVtxScratchAWords <= kEdgeCap && kVtxScratchBWords <= kEdgeCap,
+// the per-event scratch stride is at least the reference's 2 x 458752 words
+// (pixgpu_internal.cuh referenceCaps; larger capacities only widen it)
+static_assert(kVtxScratchAWords <= 2 * size_t(PF_MAX_DOUBLETS_PARAM) &&
+                  kVtxScratchBWords <= 2 * size_t(PF_MAX_DOUBLETS_PARAM),
               "vertex scratch exceeds the per-event scratchA/scratchB stride");
 constexpr int kVtxThreads = 1024;
 // events with at most this many vertex tracks keep every per-track array in
-// shared memory (38 bytes per track); larger ones use the global scratch
+// shared memory (40 bytes per track); larger ones use the global scratch
 constexpr uint32_t kSmemTracks = 4096;
-constexpr size_t kTrackBytes = 8 * 4 + 2 * 2 + 2;
+constexpr size_t kTrackBytes = 9 * 4 + 2 + 2;
 constexpr size_t kVtxSmemBytes = kSmemTracks * kTrackBytes;
 constexpr uint32_t kVtxCtas = 4;  // CTAs per event in a small batch
 
 struct VtxScratch {
   float *zt, *ezt2, *ptt2, *zz;
-  uint16_t* itrk;
+  uint32_t* itrk;    // tuple index of each vertex track
   uint8_t *izt, *newV;
   int32_t *iv, *nn, *root;
   uint32_t* list;    // tracks grouped by vertex
@@ -51,18 +54,18 @@ __device__ __forceinline__ VtxScratch carve(char* p, uint32_t cap) {
   s.nn = s.iv + cap;
   s.root = s.nn + cap;
   s.list = reinterpret_cast<uint32_t*>(s.root + cap);
-  s.itrk = reinterpret_cast<uint16_t*>(s.list + cap);
-  s.hbins = s.itrk + cap;
+  s.itrk = s.list + cap;
+  s.hbins = reinterpret_cast<uint16_t*>(s.itrk + cap);
   s.izt = reinterpret_cast<uint8_t*>(s.hbins + cap);
   s.newV = s.izt + cap;
   return s;
 }
 
 __device__ __forceinline__ VtxScratch scratchOf(const Workspace& ws, uint32_t e) {
-  // carve per-event scratch out of scratchA/scratchB (kEdgeCap words each;
+  // carve per-event scratch out of scratchA/scratchB (cap.scratch words each;
   // kVtxScratchAWords and kVtxScratchBWords of them are used)
-  uint32_t* a = ws.scratchA + size_t(e) * kEdgeCap;
-  uint32_t* b = ws.scratchB + size_t(e) * kEdgeCap;
+  uint32_t* a = ws.scratchA + size_t(e) * ws.cap.scratch;
+  uint32_t* b = ws.scratchB + size_t(e) * ws.cap.scratch;
   VtxScratch s;
   s.zt = reinterpret_cast<float*>(a);
   s.ezt2 = reinterpret_cast<float*>(a + kMaxVtxTracks);
@@ -72,12 +75,12 @@ __device__ __forceinline__ VtxScratch scratchOf(const Workspace& ws, uint32_t e)
   s.nn = reinterpret_cast<int32_t*>(a + 5 * kMaxVtxTracks);
   s.root = reinterpret_cast<int32_t*>(a + 6 * kMaxVtxTracks);
   s.list = a + 7 * kMaxVtxTracks;
-  static_assert(8 * size_t(kMaxVtxTracks) == kVtxScratchAWords, "scratch A layout");
-  s.itrk = reinterpret_cast<uint16_t*>(b);
-  s.hbins = reinterpret_cast<uint16_t*>(b) + kMaxVtxTracks;
-  s.izt = reinterpret_cast<uint8_t*>(b + kMaxVtxTracks);
-  s.newV = reinterpret_cast<uint8_t*>(b + kMaxVtxTracks) + kMaxVtxTracks;
-  static_assert(size_t(kMaxVtxTracks) + 2 * size_t(kMaxVtxTracks) / 4 == kVtxScratchBWords, "scratch B layout");
+  s.itrk = a + 8 * kMaxVtxTracks;
+  static_assert(9 * size_t(kMaxVtxTracks) == kVtxScratchAWords, "scratch A layout");
+  s.hbins = reinterpret_cast<uint16_t*>(b);
+  s.izt = reinterpret_cast<uint8_t*>(b + kMaxVtxTracks / 2);
+  s.newV = reinterpret_cast<uint8_t*>(b + kMaxVtxTracks / 2) + kMaxVtxTracks;
+  static_assert(size_t(kMaxVtxTracks) / 2 + 2 * size_t(kMaxVtxTracks) / 4 == kVtxScratchBWords, "scratch B layout");
   return s;
 }
 
@@ -359,12 +362,12 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
   const uint32_t lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   EventCounters* c = ws.ev + e;
   const uint32_t nTuples = c->nTuples;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (kTupleBins + 1);
-  const uint8_t* q = ws.quality + size_t(e) * kTupleBins;
-  const float* pt = ws.pt + size_t(e) * kTupleBins;
-  const float* st = ws.state + size_t(e) * kTupleBins * 5;
-  const float* cov = ws.cov + size_t(e) * kTupleBins * 15;
-  int16_t* idv = ws.idv + size_t(e) * kTupleBins;
+  const uint32_t* toff = ws.tupleOff + size_t(e) * (ws.cap.tuples + 1);
+  const uint8_t* q = ws.quality + size_t(e) * ws.cap.tuples;
+  const float* pt = ws.pt + size_t(e) * ws.cap.tuples;
+  const float* st = ws.state + size_t(e) * ws.cap.tuples * 5;
+  const float* cov = ws.cov + size_t(e) * ws.cap.tuples * 15;
+  int16_t* idv = ws.idv + size_t(e) * ws.cap.tuples;
   float* zv = ws.zv + size_t(e) * kMaxVtx;
   float* wv = ws.wv + size_t(e) * kMaxVtx;
   float* vchi2 = ws.vchi2 + size_t(e) * kMaxVtx;
@@ -375,7 +378,8 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
   // ---- loadTracks: the serial loop stops at the first empty tuple
   if (threadIdx.x == 0) {
     uint32_t g = nTuples;
-    if (nTuples == kTupleBins && toff[kTupleBins] == toff[kTupleBins - 1]) g = kTupleBins - 1;
+    const uint32_t bins = ws.cap.tuples;
+    if (nTuples == bins && toff[bins] == toff[bins - 1]) g = bins - 1;
     sGuard = g;
   }
   __syncthreads();
@@ -396,7 +400,11 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
   }
   uint32_t total;
   const uint32_t first = blockExclusiveScan(mine, scanSh, &total);
-  if (threadIdx.x == 0) sNt = min(total, kMaxVtxTracks);
+  if (threadIdx.x == 0) {
+    sNt = min(total, kMaxVtxTracks);
+    // beyond ZVertexSoA::MAXTRACKS the reference writes past its arrays
+    if (total > kMaxVtxTracks && rank == 0) atomicOr(&c->flags, kFlagVtxOverflow);
+  }
   __syncthreads();
   // the count decides where the per-track arrays live; the neighbour
   // searches are split among the cluster's CTAs when they are in shared memory
@@ -408,7 +416,7 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
     uint32_t it = first;
     for (uint32_t t = t0; t < t1 && it < kMaxVtxTracks; ++t) {
       if (!selected(t)) continue;
-      s.itrk[it] = uint16_t(t);
+      s.itrk[it] = t;
       s.zt[it] = st[size_t(t) * 5 + 4];
       s.ezt2[it] = cov[size_t(t) * 15 + 14];
       s.ptt2[it] = pt[t] * pt[t];
@@ -458,7 +466,11 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
       pos += __popc(m);
     }
   }
-  __syncthreads();
+  }
+  // every CTA of the cluster has started and cleared its own neighbour counts
+  // before any CTA writes counts into the others' shared memory
+  cl.sync();
+  if (active) {
   // neighbour counts: one warp per track, the lanes take 32 consecutive
   // entries of the track's three bins at a time
   for (uint32_t i = wFirst + (threadIdx.x >> 5); i < nt; i += wStride) {

@@ -25,11 +25,13 @@ namespace {
 constexpr size_t kCountersBytes = 256;
 constexpr size_t kScratchABytes = kVtxScratchAWords * 4;
 constexpr size_t kScratchBBytes = kVtxScratchBWords * 4;
-constexpr size_t kNoAllocBytes = kCountersBytes + kScratchABytes + kScratchBBytes;  // 1.25 MB
+constexpr size_t kNoAllocBytes = kCountersBytes + kScratchABytes + kScratchBBytes;  // 1.31 MB
 static_assert(sizeof(EventCounters) <= kCountersBytes, "counters do not fit their scratch slot");
-static_assert(kNoAllocBytes <= 1280 * 1024, "the documented 1.25 MB bound of the static scratch");
-// the tuple limit the entry point checks stays within the kernel's track cap
-static_assert(kTupleBins <= kMaxVtxTracks, "n_tuples limit above the vertex scratch");
+static_assert(kNoAllocBytes <= 1310720 + 256, "the documented 1.3 MB bound of the static scratch");
+// the tuple limit (n_tuples < kNoAllocMaxTuples + 1) and the reference's
+// TrackSoA stride the one-event workspace uses
+constexpr uint32_t kNoAllocMaxTuples = PF_TRACK_STRIDE - 1;  // 32767
+static_assert(PF_TRACK_STRIDE <= kMaxVtxTracks, "n_tuples limit above the vertex scratch");
 
 static __device__ __align__(256) unsigned char gVtxScratch[kNoAllocBytes];
 
@@ -80,7 +82,7 @@ extern "C" int pg_vertices_noalloc(const uint32_t* tuple_off, const uint8_t* qua
     setMessage(msg, msg_cap, "pg_vertices_noalloc: null pointer argument");
     return PG_ERR_ARG;
   }
-  if (n_tuples >= kTupleBins) {
+  if (n_tuples > kNoAllocMaxTuples) {
     setMessage(msg, msg_cap, "pg_vertices_noalloc: n_tuples above 32767, the static scratch limit");
     return PG_ERR_CAPACITY;
   }
@@ -94,6 +96,8 @@ extern "C" int pg_vertices_noalloc(const uint32_t* tuple_off, const uint8_t* qua
   // a one-event workspace: the caller's arrays plus the static scratch
   Workspace ws{};
   ws.maxEvents = 1;
+  // the reference's capacities: a TrackSoA stride of 32768 tuples
+  ws.cap = referenceCaps();
   ws.ev = reinterpret_cast<EventCounters*>(base);
   ws.tupleOff = const_cast<uint32_t*>(tuple_off);
   ws.quality = const_cast<uint8_t*>(quality);

@@ -14,47 +14,78 @@ namespace pixgpu {
 // ---------------------------------------------------------------- capacities
 constexpr uint32_t kMaxModules = PF_MAX_MODULES;         // 2000
 constexpr uint32_t kModStride = 2048;                    // per-event stride of module arrays
-constexpr uint32_t kHitCap = PF_MAX_HITS;                // 49152 hits per event
 constexpr uint32_t kPhiTot = 10 * PF_PHI_BINS + 1;       // 1281
 constexpr uint32_t kPhiStride = 1288;
-constexpr uint32_t kJCap = 6 * kHitCap;                  // doublet inner-hit slots (sum of inner layer sizes)
-constexpr uint32_t kCellCap = PF_MAX_DOUBLETS_PARAM;     // 458752 doublets per event
-constexpr uint32_t kEdgeCap = 2 * kCellCap;              // CA neighbour links kept per event
-constexpr uint32_t kTupleBins = PF_TRACK_STRIDE;         // 32768 tuples (HitContainer bins)
-constexpr uint32_t kTupleHitCap = 5 * kTupleBins;        // 163840
-constexpr uint32_t kTupleCellCap = 4 * kTupleBins;       // cells per tuple <= 4
-constexpr uint32_t kH2TCap = 4 * PF_MAX_TUPLES;          // HitToTuple capacity (98304)
 constexpr uint32_t kMaxVtx = PF_MAX_VTX;
 constexpr uint32_t kErrCap = 4096;                       // digi errors kept per event
-constexpr uint32_t kMaxFedWords = PF_MAX_FED_WORDS;      // 300000 words per event
 constexpr uint32_t kBigSegCap = 8192;                    // long list segments queued per event and sort
+// hit indices are packed with a module index into one 32-bit word of the
+// doublet search's hit records (11 + 21 bits)
+constexpr uint32_t kMaxHitCapLimit = 1u << 21;
+
+// Per-event container capacities (a context's pg_config caps).  The
+// defaults are the reference's compile-time constants and module parameters,
+// whose truncation order parity covers; larger values run the same algorithm
+// on events whose containers would overflow (indices are 32-bit throughout).
+// Every per-event array is strided by these.
+struct Caps {
+  uint32_t fedWords;      // FED words per event (MAX_FED_WORDS)
+  uint32_t hits;          // clusters kept per event (maxNumberOfHits)
+  uint32_t cells;         // doublets (maxNumberOfDoublets, the module parameter)
+  uint32_t edges;         // CA links kept (the neighbour lists' content)
+  uint32_t lists;         // cells with a neighbour / a track list (maxNumOfActiveDoublets)
+  uint32_t tuples;        // HitContainer bins = TrackSoA stride
+  uint32_t multiplicity;  // TupleMultiplicity content = concurrent fits per multiplicity (maxNumberOfTuples)
+  uint32_t h2t;           // HitToTuple content
+  uint32_t jCap;          // doublet inner-hit slots (6 x hits covers every inner layer of the 19 pairs)
+  uint32_t scratch;       // 32-bit words of scratchA/scratchB per event
+  __host__ __device__ uint32_t tupleHits() const { return 5 * tuples; }
+  __host__ __device__ uint32_t tupleCells() const { return 4 * tuples; }
+};
+
+// the reference's capacities
+inline Caps referenceCaps() {
+  Caps c;
+  c.fedWords = PF_MAX_FED_WORDS;         // 300000
+  c.hits = PF_MAX_HITS;                  // 49152
+  c.cells = PF_MAX_DOUBLETS_PARAM;       // 458752
+  c.edges = 2 * PF_MAX_DOUBLETS_PARAM;   // 917504
+  c.lists = PF_MAX_ACTIVE_DOUBLETS;      // 65536
+  c.tuples = PF_TRACK_STRIDE;            // 32768
+  c.multiplicity = PF_MAX_TUPLES;        // 24576
+  c.h2t = 4 * PF_MAX_TUPLES;             // 98304
+  c.jCap = 6 * c.hits;
+  c.scratch = c.edges;
+  return c;
+}
+
 // The vertex finder's track cap (ZVertexSoA MAXTRACKS) and the per-event
 // scratch it carves out of scratchA/scratchB for events above its
-// shared-memory size (k_vertex.cu scratchOf): eight 32-bit arrays in A; two
-// 16-bit and two 8-bit arrays in B.  noalloc.cu sizes its static array from
-// the same numbers.
+// shared-memory size (k_vertex.cu scratchOf): nine 32-bit arrays in A (the
+// ninth the tracks' tuple indices); one 16-bit and two 8-bit arrays in B.
+// noalloc.cu sizes its static array from the same numbers.
 constexpr uint32_t kMaxVtxTracks = 32 * 1024;
-constexpr size_t kVtxScratchAWords = size_t(8) * kMaxVtxTracks;
-constexpr size_t kVtxScratchBWords = size_t(kMaxVtxTracks) + kMaxVtxTracks / 2;
+constexpr size_t kVtxScratchAWords = size_t(9) * kMaxVtxTracks;
+constexpr size_t kVtxScratchBWords = size_t(kMaxVtxTracks);
 
 // flag bits in EventCounters::flags (capacity conditions where the result no
 // longer follows the reference's truncation order exactly)
 enum : uint32_t {
   kFlagModuleTooBig = 1u << 0,      // > 4000 pixels in a module (reference behaviour undefined)
-  kFlagEdgeOverflow = 1u << 1,      // more CA links than kEdgeCap
+  kFlagEdgeOverflow = 1u << 1,      // more CA links than cap.edges
   kFlagNbrPoolOverflow = 1u << 2,   // more cells with neighbours than the 65535-list pool
   kFlagTrkPoolOverflow = 1u << 3,   // more cells with tracks than the 65535-list pool
-  kFlagFitBinOverflow = 1u << 4,    // > 24576 tuples of one multiplicity (fit order dependent)
-  kFlagTupleOverflow = 1u << 5,     // > 32768 tuples (reference drops the tail)
+  kFlagFitBinOverflow = 1u << 4,    // more tuples of one multiplicity than concurrent fits
+  kFlagTupleOverflow = 1u << 5,     // more tuples than HitContainer bins (reference drops the tail)
   kFlagCellOverflow = 1u << 6,      // doublet capacity reached (reference truncates; reproduced)
-  kFlagHitOverflow = 1u << 7,       // > 49152 clusters (reference truncates; reproduced)
+  kFlagHitOverflow = 1u << 7,       // more clusters than the hit capacity (reference truncates; reproduced)
   kFlagErrOverflow = 1u << 8,       // more digi errors than kErrCap
-  kFlagTooManyWords = 1u << 9,      // event larger than kMaxFedWords
+  kFlagTooManyWords = 1u << 9,      // event larger than cap.fedWords
   kFlagH2TOverflow = 1u << 10,      // hit-to-tuple capacity exceeded
   kFlagTmOverflow = 1u << 11,       // tuple multiplicity capacity exceeded
   kFlagVtxOverflow = 1u << 12,      // split vertex with >= 512 tracks or > 1024 vertices
   kFlagDeepTuple = 1u << 13,        // a CA path longer than 5 hits (reference aborts)
-  kFlagJOverflow = 1u << 14,        // more doublet inner-hit slots than kJCap
+  kFlagJOverflow = 1u << 14,        // more doublet inner-hit slots than cap.jCap
   kFlagBadInput = 1u << 15,         // words/cabling entries outside the tables (ignored)
   kFlagSplitModule = 1u << 17,      // a module's digis in several runs (later runs read as padding)
   kFlagTooManyRuns = 1u << 18       // more than 2000 module runs (the reference's counter wraps)
@@ -169,6 +200,7 @@ struct LaunchTuning {
 struct Workspace {
   uint32_t maxEvents;
   uint32_t wordCap;          // words over the whole batch
+  Caps cap;                  // per-event capacities (the strides of every per-event array)
   CAConfig ca;               // the context's CA configuration
   FedScanBuffers scan;       // device FED scan (scan.on == 0: not used)
   LaunchTuning tune;         // grid scales of the tunable launches (host side)
@@ -186,68 +218,69 @@ struct Workspace {
   uint32_t* errWordIdx;      // [maxEvents][kErrCap]
   // clusters [maxEvents][kModStride]
   uint32_t *moduleStart, *clusInModule, *moduleId, *clusModuleStart;
-  // hits [maxEvents][kHitCap]
+  // hits [maxEvents][cap.hits]
   float *xl, *yl, *xerr, *yerr, *xg, *yg, *zg, *rg;
   int32_t* charge;
   int16_t *iphi, *xsize, *ysize;
   uint16_t* detInd;
   uint32_t* phiOff;          // [maxEvents][kPhiStride]
-  uint16_t* phiBins;         // [maxEvents][kHitCap]
-  uint4* phiRec;             // [maxEvents][kHitCap] hit records in phiBins order: z, r, iphi|ysize<<16, detInd|hit<<16
+  uint32_t* phiBins;         // [maxEvents][cap.hits]
+  uint4* phiRec;             // [maxEvents][cap.hits] hit records in phiBins order: z, r, iphi|ysize<<16,
+                             // min(detInd, 2047)|hit<<11
   PfAverageGeometry* agc;    // [maxEvents]
   // doublets
-  uint32_t* jCount;          // [maxEvents][kJCap + 1]
-  uint32_t* jOffset;         // [maxEvents][kJCap + 1]
-  uint16_t *cellInner, *cellOuter;   // [maxEvents][kCellCap]
+  uint32_t* jCount;          // [maxEvents][cap.jCap + 1]
+  uint32_t* jOffset;         // [maxEvents][cap.jCap + 1]
+  uint32_t *cellInner, *cellOuter;   // [maxEvents][cap.cells]
   uint8_t* cellPair;
   int32_t* cellDoubletId;
   uint8_t* cellUsed;
   float *cellInnerZ, *cellInnerR;
   // cells by outer hit (isOuterHitOfCell), CSR sorted ascending
-  uint32_t* ohCount;         // [maxEvents][kHitCap + 1]
-  uint32_t* ohOff;           // [maxEvents][kHitCap + 1]
-  uint32_t* ohCells;         // [maxEvents][kCellCap]
-  float4* ohRec;             // [maxEvents][kCellCap] inner hit of each ohCells entry: x, y, z, +-r (- : dca region inner)
-  uint16_t* ohDet;           // [maxEvents][kCellCap] module index of that inner hit
+  uint32_t* ohCount;         // [maxEvents][cap.hits + 1]
+  uint32_t* ohOff;           // [maxEvents][cap.hits + 1]
+  uint32_t* ohCells;         // [maxEvents][cap.cells]
+  float4* ohRec;             // [maxEvents][cap.cells] inner hit of each ohCells entry: x, y, z, +-r (- : dca region inner)
+  uint16_t* ohDet;           // [maxEvents][cap.cells] module index of that inner hit
   // CA neighbour links (outerNeighbors), CSR sorted ascending
-  uint32_t* nbrCount;        // [maxEvents][kCellCap + 1]
-  uint32_t* nbrOff;          // [maxEvents][kCellCap + 1]
-  uint32_t* nbr;             // [maxEvents][kEdgeCap]
+  uint32_t* nbrCount;        // [maxEvents][cap.cells + 1]
+  uint32_t* nbrOff;          // [maxEvents][cap.cells + 1]
+  uint32_t* nbr;             // [maxEvents][cap.edges]
   // tuples
-  uint32_t* startTupleCount; // [maxEvents][kCellCap + 1]
-  uint32_t* startTupleOff;   // [maxEvents][kCellCap + 1]
-  uint32_t* startHitCount;   // [maxEvents][kCellCap + 1]
-  uint32_t* startHitOff;     // [maxEvents][kCellCap + 1]
-  uint32_t* tupleOff;        // [maxEvents][kTupleBins + 1]
-  uint16_t* tupleHits;       // [maxEvents][kTupleHitCap]
-  uint16_t* tupleDet;        // [maxEvents][kTupleHitCap]
-  uint32_t* tupleCells;      // [maxEvents][kTupleCellCap]  (4 slots per tuple)
-  uint8_t* quality;          // [maxEvents][kTupleBins]
+  uint32_t* startTupleCount; // [maxEvents][cap.cells + 1]
+  uint32_t* startTupleOff;   // [maxEvents][cap.cells + 1]
+  uint32_t* startHitCount;   // [maxEvents][cap.cells + 1]
+  uint32_t* startHitOff;     // [maxEvents][cap.cells + 1]
+  uint32_t* tupleOff;        // [maxEvents][cap.tuples + 1]
+  uint32_t* tupleHits;       // [maxEvents][cap.tupleHits()]
+  uint16_t* tupleDet;        // [maxEvents][cap.tupleHits()]
+  uint32_t* tupleCells;      // [maxEvents][cap.tupleCells()]  (4 slots per tuple)
+  uint8_t* quality;          // [maxEvents][cap.tuples]
   // cell -> tracks, CSR sorted ascending
-  uint32_t* trkCount;        // [maxEvents][kCellCap + 1]
-  uint32_t* trkOff;          // [maxEvents][kCellCap + 1]
-  uint16_t* trk;             // [maxEvents][kTupleCellCap]
-  uint32_t* candidates;      // [maxEvents][kCellCap] cells with >= 2 tracks, ascending
+  uint32_t* trkCount;        // [maxEvents][cap.cells + 1]
+  uint32_t* trkOff;          // [maxEvents][cap.cells + 1]
+  uint32_t* trk;             // [maxEvents][cap.tupleCells()]
+  uint32_t* candidates;      // [maxEvents][cap.cells] cells with >= 2 tracks, ascending
   // tuple multiplicity
   uint32_t* tmOff;           // [maxEvents][16]
-  uint16_t* tmBins;          // [maxEvents][kTupleBins]
-  // fit results [maxEvents][kTupleBins * k]
+  uint32_t* tmBins;          // [maxEvents][cap.tuples]
+  // fit results [maxEvents][cap.tuples * k]
   float *state, *cov, *pt, *eta, *chi2;
   // hit -> tuple
-  uint32_t* h2tCount;        // [maxEvents][kHitCap + 1]
-  uint32_t* h2tOff;          // [maxEvents][kHitCap + 1]
-  uint16_t* h2t;             // [maxEvents][kH2TCap]
+  uint32_t* h2tCount;        // [maxEvents][cap.hits + 1]
+  uint32_t* h2tOff;          // [maxEvents][cap.hits + 1]
+  uint32_t* h2t;             // [maxEvents][cap.h2t]
   // vertices
   float *zv, *wv, *vchi2, *ptv2;  // [maxEvents][kMaxVtx]
   int32_t* ndof;             // [maxEvents][kMaxVtx]
   uint16_t* sortInd;         // [maxEvents][kMaxVtx]
-  int16_t* idv;              // [maxEvents][kTupleBins]
+  int16_t* idv;              // [maxEvents][cap.tuples]
   // scratch: CA link lists before ordering, cleaner state
-  uint32_t* scratchA;        // [maxEvents][kEdgeCap]
-  uint32_t* scratchB;        // [maxEvents][kEdgeCap]
+  uint32_t* scratchA;        // [maxEvents][cap.scratch]
+  uint32_t* scratchB;        // [maxEvents][cap.scratch]
   uint32_t* scanSums;        // [maxEvents][kScanMaxSlices] slice totals of the segmented scans
   uint32_t* bigSeg;          // [maxEvents][kBigSegCap] long segments awaiting the block sort
-  uint32_t* segList;         // [maxEvents][kCellCap] segments with >= 2 entries (the ones to order)
+  uint32_t* segList;         // [maxEvents][cap.cells] segments with >= 2 entries (the ones to order)
 };
 
 // A CSR fill notes segment s when it places s's second entry: only those
@@ -257,7 +290,7 @@ struct Workspace {
 // the next fill.
 __device__ __forceinline__ void noteSegment(const Workspace& ws, uint32_t e, int list, uint32_t s) {
   const uint32_t k = atomicAdd(&ws.ev[e].nSegList[list], 1u);
-  ws.segList[size_t(e) * kCellCap + k] = s;
+  ws.segList[size_t(e) * ws.cap.cells + k] = s;
 }
 
 // ---------------------------------------------------------------- kernel timing probe
@@ -284,8 +317,8 @@ void probeEnd(cudaStream_t s);
   } while (0)
 
 // ---------------------------------------------------------------- launch API (host)
-size_t workspaceBytes(uint32_t maxEvents, uint32_t wordCap);
-void workspaceCarve(Workspace& ws, void* base, uint32_t maxEvents, uint32_t wordCap);
+size_t workspaceBytes(uint32_t maxEvents, uint32_t wordCap, const Caps& cap);
+void workspaceCarve(Workspace& ws, void* base, uint32_t maxEvents, uint32_t wordCap, const Caps& cap);
 
 // Batches up to this many events run the per-event cooperative kernels
 // (result packing, duplicate rounds, vertexing) as clusters of several CTAs

@@ -16,7 +16,7 @@ struct ResultHeader {
   uint32_t nEdges, nTupleHits, nModules;
   uint32_t pad[5];
 };
-constexpr size_t kResultTrackBytes = 4 + 1 + 1 + 20 + 60 + 4 + 4 + 4 + 10 + 2;  // per stored track
+constexpr size_t kResultTrackBytes = 4 + 1 + 1 + 20 + 60 + 4 + 4 + 4 + 20 + 2;  // per stored track
 constexpr size_t kResultVertexBytes = 4 + 4 + 4 + 4 + 4 + 2;                   // per stored vertex
 
 struct ResultTracks {
@@ -26,7 +26,7 @@ struct ResultTracks {
   float* state;   // [n][5]
   float* cov;     // [n][15]
   float *pt, *eta, *chi2;
-  uint16_t* hits;  // [n][5]
+  uint32_t* hits;  // [n][5]
   int16_t* vertex;
 };
 
@@ -45,7 +45,7 @@ constexpr size_t kResOffPt = kResOffCov + 4 * 15 * size_t(kResultTracks);
 constexpr size_t kResOffEta = kResOffPt + 4 * size_t(kResultTracks);
 constexpr size_t kResOffChi2 = kResOffEta + 4 * size_t(kResultTracks);
 constexpr size_t kResOffHits = kResOffChi2 + 4 * size_t(kResultTracks);
-constexpr size_t kResOffVertex = kResOffHits + 2 * 5 * size_t(kResultTracks);
+constexpr size_t kResOffVertex = kResOffHits + 4 * 5 * size_t(kResultTracks);
 constexpr size_t kResOffZv = kResOffVertex + 2 * size_t(kResultTracks);
 constexpr size_t kResOffWv = kResOffZv + 4 * size_t(kResultVertices);
 constexpr size_t kResOffVchi2 = kResOffWv + 4 * size_t(kResultVertices);
@@ -70,7 +70,7 @@ PG_HD inline ResultTracks resultTracks(uint8_t* base) {
   t.pt = reinterpret_cast<float*>(base + kResOffPt);
   t.eta = reinterpret_cast<float*>(base + kResOffEta);
   t.chi2 = reinterpret_cast<float*>(base + kResOffChi2);
-  t.hits = reinterpret_cast<uint16_t*>(base + kResOffHits);
+  t.hits = reinterpret_cast<uint32_t*>(base + kResOffHits);
   t.vertex = reinterpret_cast<int16_t*>(base + kResOffVertex);
   return t;
 }

@@ -90,7 +90,8 @@ void launchGather(Workspace& ws, const uint32_t* poolWords, const uint8_t* poolF
 
 int poolCreate(pg_ctx* c, uint64_t words) {
   Pool& p = c->pool;
-  if (words < kMaxFedWords || words > (uint64_t(1) << 31)) return fail(c, PG_ERR_ARG, "pool size");
+  const uint32_t maxWords = c->caps.fedWords;
+  if (words < maxWords || words > (uint64_t(1) << 31)) return fail(c, PG_ERR_ARG, "pool size");
   p.capWords = uint32_t(words) & ~(kExtentAlign - 1);
   if (cudaMalloc(&p.dWords, size_t(p.capWords) * 4) != cudaSuccess ||
       cudaMalloc(&p.dFed, size_t(p.capWords) / 2 + 16) != cudaSuccess)
@@ -102,8 +103,8 @@ int poolCreate(pg_ctx* c, uint64_t words) {
   p.freeWords = p.capWords;
   p.stagers.resize(kStagers);
   for (auto& st : p.stagers) {
-    if (cudaMallocHost(&st.hWords, size_t(kMaxFedWords) * 4) != cudaSuccess ||
-        cudaMallocHost(&st.hFed, size_t(kMaxFedWords) / 2 + 16) != cudaSuccess ||
+    if (cudaMallocHost(&st.hWords, size_t(maxWords) * 4) != cudaSuccess ||
+        cudaMallocHost(&st.hFed, size_t(maxWords) / 2 + 16) != cudaSuccess ||
         cudaEventCreateWithFlags(&st.copied, cudaEventDisableTiming) != cudaSuccess)
       return fail(c, PG_ERR_NOMEM, "pool staging buffers");
   }
@@ -154,7 +155,7 @@ int poolStage(pg_ctx* c, const uint8_t* raw, size_t size, uint32_t* stager, uint
     p.nextStager = (uint32_t(k) + 1) % kStagers;
   }
   Stager& st = p.stagers[k];
-  int rc = unpackRaw(c->hes.fedIds, raw, size, st.hWords, st.hFed, kMaxFedWords, nWords);
+  int rc = unpackRaw(c->hes.fedIds, raw, size, st.hWords, st.hFed, c->caps.fedWords, nWords);
   if (rc != PG_OK) {
     std::lock_guard<std::mutex> lk(p.mu);
     st.used = false;

@@ -99,6 +99,7 @@ struct HostES {
 struct pg_ctx {
   int device = 0;
   pg_config cfg{};
+  pixgpu::Caps caps{};  // per-event capacities resolved from cfg
   HostES hes;
   void* esMem = nullptr;
   pixgpu::DeviceES des{};
@@ -114,6 +115,9 @@ struct pg_ctx {
 namespace pixgpu {
 
 int fail(pg_ctx* c, int code, const std::string& msg);
+// the capacities a configuration asks for (0 fields: the reference's); false
+// when a field is below the reference's value or beyond the index widths
+bool resolveCaps(const pg_config& cfg, Caps* out);
 // the context's last error message (a copy taken under errMu)
 std::string lastError(pg_ctx* c);
 // the launch tuning for batches of n events: n's table, else the largest tuned size below n, else defaults

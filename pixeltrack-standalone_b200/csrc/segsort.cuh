@@ -64,12 +64,12 @@ __device__ void serialSort(T* seg, uint32_t n, bool desc) {
 
 template <typename T>
 __global__ void kSortListed(T* data, size_t dataStride, const uint32_t* off, size_t offStride, const uint32_t* list,
-                            const uint32_t* nList, uint32_t nListStride, bool desc, uint32_t dataCap, uint32_t* big,
-                            uint32_t* nBig, uint32_t nBigStride) {
+                            size_t listStride, const uint32_t* nList, uint32_t nListStride, bool desc,
+                            uint32_t dataCap, uint32_t* big, uint32_t* nBig, uint32_t nBigStride) {
   const uint32_t e = blockIdx.y;
   const uint32_t nseg = nList[size_t(e) * nListStride];
   const uint32_t* o = off + size_t(e) * offStride;
-  const uint32_t* L = list + size_t(e) * kCellCap;
+  const uint32_t* L = list + size_t(e) * listStride;
   T* d = data + size_t(e) * dataStride;
   for (uint32_t s0 = blockIdx.x * blockDim.x; s0 < nseg; s0 += gridDim.x * blockDim.x) {
     const uint32_t k = s0 + threadIdx.x;
@@ -142,8 +142,8 @@ void sortSegments(Workspace& ws, uint32_t nEvents, cudaStream_t stream, uint32_t
   (void)fixedLen;
   PG_PROBED("kSortSegments", stream,
             kSortListed<T><<<dim3(gx, nEvents), 256, 0, stream>>>(data, dataStride, off, offStride, ws.segList,
-                                                                  &ws.ev[0].nSegList[slot], stride, desc, dataCap,
-                                                                  ws.bigSeg, nBig, stride));
+                                                                  ws.cap.cells, &ws.ev[0].nSegList[slot], stride,
+                                                                  desc, dataCap, ws.bigSeg, nBig, stride));
   PG_PROBED("kSortBig", stream,
             kSortBig<T><<<dim3(8, nEvents), 256, 0, stream>>>(data, dataStride, off, offStride, desc, dataCap,
                                                               ws.bigSeg, nBig, stride));

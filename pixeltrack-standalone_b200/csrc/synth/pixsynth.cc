@@ -560,6 +560,19 @@ void ps_default_event_config(ps_event_config* cfg) {
   cfg->noise_frac = 0.001;
   cfg->inject_errors = 0;
   cfg->fixed_pu = 1;
+  cfg->soft_per_vertex = 0.0;
+  cfg->soft_pt_min = 0.05;
+  cfg->soft_pt_mean = 0.25;
+  cfg->secondary_frac = 0.0;
+}
+
+void ps_calibrated_event_config(ps_event_config* cfg) {
+  ps_default_event_config(cfg);
+  cfg->tracks_per_vertex = 28.0;
+  cfg->pt_index = 3.5;
+  cfg->soft_per_vertex = 50.0;
+  cfg->soft_pt_mean = 0.25;
+  cfg->secondary_frac = 0.8;
 }
 
 int ps_detector_create(const ps_detector_config* cfg, ps_detector** out) {
@@ -629,6 +642,165 @@ int ps_event_generate(const ps_detector* det, uint64_t seed, double pu, const ps
   std::vector<Deposit> deposits;
   deposits.reserve(size_t(nvtx * cfg.tracks_per_vertex * 5 * 4) + 16);
 
+  // One charged track from (vx, vy, vz): helix steps from surface to
+  // surface, charge deposits on every module crossed, multiple scattering at
+  // each layer.  `start` > 0 moves the origin that far along the initial
+  // direction in the transverse plane (a displaced secondary).
+  auto propagate = [&](double vx, double vy, double vz, double pt, double eta, double phi, int q, int iv,
+                       double start) {
+    double cot = std::sinh(eta);
+    double R = pt / kBField;
+    Helix hx{vx, vy, vz, phi, cot, q / R};
+    if (start > 0) {
+      double P0[3];
+      hx.at(start, P0);
+      double T0[3];
+      hx.tangent(start, T0);
+      hx.x = P0[0];
+      hx.y = P0[1];
+      hx.z = P0[2];
+      hx.psi = std::atan2(T0[1], T0[0]);
+    }
+    double p = pt * std::sqrt(1 + cot * cot);
+    uint8_t nh = 0;
+    bool crossedB[4] = {false, false, false, false};
+    bool crossedD[6][4] = {};
+    for (int step = 0; step < 30; ++step) {
+      // next surface
+      double bestS = -1;
+      int bestKind = -1, bestA = 0, bestB = 0;
+      for (int L = 0; L < 4; ++L) {
+        if (crossedB[L]) continue;
+        double s = hx.cylinder(kBarrelR[L]);
+        if (s > 0 && (bestS < 0 || s < bestS)) {
+          bestS = s; bestKind = 0; bestA = L;
+        }
+      }
+      if (hx.cot != 0) {
+        for (int e = 0; e < 6; ++e)
+          for (int pl = 0; pl < 4; ++pl) {
+            if (crossedD[e][pl]) continue;
+            int disk = e % 3;
+            int g = pl / 2, pan = 1 + pl % 2;
+            double az = kDiskZ[disk] + (pan == 1 ? -0.25 : 0.25) + (g == 1 ? 0.8 : 0.0);
+            double zp = e < 3 ? az : -az;
+            double s = (zp - hx.z) / hx.cot;
+            if (s > 1e-6 && (bestS < 0 || s < bestS)) {
+              bestS = s; bestKind = 1; bestA = e; bestB = pl;
+            }
+          }
+      }
+      if (bestS < 0) break;
+      double Pc[3];
+      hx.at(bestS, Pc);
+      if (std::fabs(Pc[2]) > 55.0 || std::hypot(Pc[0], Pc[1]) > 17.5) break;
+      std::vector<SimHit> hits;
+      if (bestKind == 0) {
+        int L = bestA;
+        crossedB[L] = true;
+        int nl = kLadders[L];
+        double phic = std::atan2(Pc[1], Pc[0]);
+        if (phic < 0) phic += 2 * kPi;
+        int l0 = int(std::floor(phic * nl / (2 * kPi)));
+        for (int dlad = -1; dlad <= 1; ++dlad) {
+          int l = ((l0 + dlad) % nl + nl) % nl;
+          const Module& ref = d.modules[kLayerStart[L] + 8 * l];
+          double lp[3] = {ref.p[0], ref.p[1], 0.0};
+          double s;
+          if (!hx.plane(ref.ez, lp, bestS, s)) continue;
+          double P[3];
+          hx.at(s, P);
+          double rel[3] = {P[0] - lp[0], P[1] - lp[1], P[2]};
+          double lx = dot3(ref.ex, rel);
+          if (std::fabs(lx) >= kHalfX) continue;
+          int k = int(std::floor((P[2] + 26.8) / 6.7));
+          if (k < 0 || k > 7) continue;
+          double ly = P[2] - (k - 3.5) * 6.7;
+          if (std::fabs(ly) >= kHalfY) continue;
+          SimHit h;
+          h.module = kLayerStart[L] + 8 * l + k;
+          h.s = s;
+          std::memcpy(h.P, P, sizeof(P));
+          hx.tangent(s, h.T);
+          hits.push_back(h);
+        }
+      } else {
+        int e = bestA, pl = bestB;
+        crossedD[e][pl] = true;
+        int g = pl / 2, pan = 1 + pl % 2;
+        double r = std::hypot(Pc[0], Pc[1]);
+        if (std::fabs(r - kRingR[g]) < kHalfY + 0.01) {
+          int n = kRingN[g];
+          double phic = std::atan2(Pc[1], Pc[0]);
+          if (phic < 0) phic += 2 * kPi;
+          int j0 = int(std::floor(phic * n / (2 * kPi)));
+          int base = kLayerStart[4 + e] + (g == 1 ? kRingN[0] : 0);
+          for (int dj = -2; dj <= 2; ++dj) {
+            int j = ((j0 + dj) % n + n) % n;
+            if (1 + j % 2 != pan) continue;
+            const Module& m = d.modules[base + j];
+            double rel[3] = {Pc[0] - m.p[0], Pc[1] - m.p[1], Pc[2] - m.p[2]};
+            double lx = dot3(m.ex, rel), ly = dot3(m.ey, rel);
+            if (std::fabs(lx) >= kHalfX || std::fabs(ly) >= kHalfY) continue;
+            SimHit h;
+            h.module = base + j;
+            h.s = bestS;
+            std::memcpy(h.P, Pc, sizeof(Pc));
+            hx.tangent(bestS, h.T);
+            hits.push_back(h);
+          }
+        }
+      }
+      if (hits.empty()) continue;
+      std::sort(hits.begin(), hits.end(), [](const SimHit& a, const SimHit& b) { return a.s < b.s; });
+      for (auto& h : hits) {
+        double path = 1.0;
+        {
+          const Module& m = d.modules[h.module];
+          double tn = std::sqrt(dot3(h.T, h.T));
+          double cz = std::fabs(dot3(m.ez, h.T)) / tn;
+          path = 1.0 / std::max(cz, 0.05);
+        }
+        double qtot = (21000.0 + 1400.0 * moyal(rng)) * std::min(path, 8.0);
+        depositHit(d, h, qtot, rng, deposits);
+        ++nh;
+        ++ev->nSimHits;
+      }
+      // multiple scattering at the last hit, restart the helix there
+      const SimHit& last = hits.back();
+      double tn = std::sqrt(dot3(last.T, last.T));
+      double dir[3] = {last.T[0] / tn, last.T[1] / tn, last.T[2] / tn};
+      double x0 = (bestKind == 0 ? 0.025 : 0.03) * hits.size();
+      double th0 = 0.0136 / p * std::sqrt(x0) * (1 + 0.038 * std::log(x0));
+      double u1[3] = {-dir[1], dir[0], 0};
+      double nu = std::sqrt(u1[0] * u1[0] + u1[1] * u1[1]);
+      if (nu < 1e-9) {
+        u1[0] = 1; u1[1] = 0; nu = 1;
+      }
+      u1[0] /= nu; u1[1] /= nu;
+      double u2[3] = {dir[1] * u1[2] - dir[2] * u1[1], dir[2] * u1[0] - dir[0] * u1[2], dir[0] * u1[1] - dir[1] * u1[0]};
+      double a1 = th0 * N(rng), a2 = th0 * N(rng);
+      double nd[3];
+      for (int k = 0; k < 3; ++k) nd[k] = dir[k] + a1 * u1[k] + a2 * u2[k];
+      double nn = std::sqrt(dot3(nd, nd));
+      for (int k = 0; k < 3; ++k) nd[k] /= nn;
+      double ptn = p * std::sqrt(nd[0] * nd[0] + nd[1] * nd[1]);
+      if (ptn < 1e-3) break;
+      hx.x = last.P[0];
+      hx.y = last.P[1];
+      hx.z = last.P[2];
+      hx.psi = std::atan2(nd[1], nd[0]);
+      hx.cot = nd[2] / std::sqrt(nd[0] * nd[0] + nd[1] * nd[1]);
+      hx.kappa = q * kBField / ptn;
+    }
+    ev->tpt.push_back(float(pt));
+    ev->teta.push_back(float(eta));
+    ev->tphi.push_back(float(phi));
+    ev->tq.push_back(q);
+    ev->tv.push_back(iv);
+    ev->tnh.push_back(nh);
+  };
+
   for (int iv = 0; iv < nvtx; ++iv) {
     double vz = d.bs.z + 3.5 * N(rng);
     double vx = d.bs.x + 0.0015 * N(rng), vy = d.bs.y + 0.0015 * N(rng);
@@ -641,147 +813,24 @@ int ps_event_generate(const ps_detector* det, uint64_t seed, double pu, const ps
       double eta = (2 * U(rng) - 1) * cfg.eta_max;
       double phi = (2 * U(rng) - 1) * kPi;
       int q = U(rng) < 0.5 ? -1 : 1;
-      double cot = std::sinh(eta);
-      double R = pt / kBField;
-      Helix hx{vx, vy, vz, phi, cot, q / R};
-      double p = pt * std::sqrt(1 + cot * cot);
-      uint8_t nh = 0;
-      bool crossedB[4] = {false, false, false, false};
-      bool crossedD[6][4] = {};
-      for (int step = 0; step < 30; ++step) {
-        // next surface
-        double bestS = -1;
-        int bestKind = -1, bestA = 0, bestB = 0;
-        for (int L = 0; L < 4; ++L) {
-          if (crossedB[L]) continue;
-          double s = hx.cylinder(kBarrelR[L]);
-          if (s > 0 && (bestS < 0 || s < bestS)) {
-            bestS = s; bestKind = 0; bestA = L;
-          }
-        }
-        if (hx.cot != 0) {
-          for (int e = 0; e < 6; ++e)
-            for (int pl = 0; pl < 4; ++pl) {
-              if (crossedD[e][pl]) continue;
-              int disk = e % 3;
-              int g = pl / 2, pan = 1 + pl % 2;
-              double az = kDiskZ[disk] + (pan == 1 ? -0.25 : 0.25) + (g == 1 ? 0.8 : 0.0);
-              double zp = e < 3 ? az : -az;
-              double s = (zp - hx.z) / hx.cot;
-              if (s > 1e-6 && (bestS < 0 || s < bestS)) {
-                bestS = s; bestKind = 1; bestA = e; bestB = pl;
-              }
-            }
-        }
-        if (bestS < 0) break;
-        double Pc[3];
-        hx.at(bestS, Pc);
-        if (std::fabs(Pc[2]) > 55.0 || std::hypot(Pc[0], Pc[1]) > 17.5) break;
-        std::vector<SimHit> hits;
-        if (bestKind == 0) {
-          int L = bestA;
-          crossedB[L] = true;
-          int nl = kLadders[L];
-          double phic = std::atan2(Pc[1], Pc[0]);
-          if (phic < 0) phic += 2 * kPi;
-          int l0 = int(std::floor(phic * nl / (2 * kPi)));
-          for (int dlad = -1; dlad <= 1; ++dlad) {
-            int l = ((l0 + dlad) % nl + nl) % nl;
-            const Module& ref = d.modules[kLayerStart[L] + 8 * l];
-            double lp[3] = {ref.p[0], ref.p[1], 0.0};
-            double s;
-            if (!hx.plane(ref.ez, lp, bestS, s)) continue;
-            double P[3];
-            hx.at(s, P);
-            double rel[3] = {P[0] - lp[0], P[1] - lp[1], P[2]};
-            double lx = dot3(ref.ex, rel);
-            if (std::fabs(lx) >= kHalfX) continue;
-            int k = int(std::floor((P[2] + 26.8) / 6.7));
-            if (k < 0 || k > 7) continue;
-            double ly = P[2] - (k - 3.5) * 6.7;
-            if (std::fabs(ly) >= kHalfY) continue;
-            SimHit h;
-            h.module = kLayerStart[L] + 8 * l + k;
-            h.s = s;
-            std::memcpy(h.P, P, sizeof(P));
-            hx.tangent(s, h.T);
-            hits.push_back(h);
-          }
-        } else {
-          int e = bestA, pl = bestB;
-          crossedD[e][pl] = true;
-          int g = pl / 2, pan = 1 + pl % 2;
-          double r = std::hypot(Pc[0], Pc[1]);
-          if (std::fabs(r - kRingR[g]) < kHalfY + 0.01) {
-            int n = kRingN[g];
-            double phic = std::atan2(Pc[1], Pc[0]);
-            if (phic < 0) phic += 2 * kPi;
-            int j0 = int(std::floor(phic * n / (2 * kPi)));
-            int base = kLayerStart[4 + e] + (g == 1 ? kRingN[0] : 0);
-            for (int dj = -2; dj <= 2; ++dj) {
-              int j = ((j0 + dj) % n + n) % n;
-              if (1 + j % 2 != pan) continue;
-              const Module& m = d.modules[base + j];
-              double rel[3] = {Pc[0] - m.p[0], Pc[1] - m.p[1], Pc[2] - m.p[2]};
-              double lx = dot3(m.ex, rel), ly = dot3(m.ey, rel);
-              if (std::fabs(lx) >= kHalfX || std::fabs(ly) >= kHalfY) continue;
-              SimHit h;
-              h.module = base + j;
-              h.s = bestS;
-              std::memcpy(h.P, Pc, sizeof(Pc));
-              hx.tangent(bestS, h.T);
-              hits.push_back(h);
-            }
-          }
-        }
-        if (hits.empty()) continue;
-        std::sort(hits.begin(), hits.end(), [](const SimHit& a, const SimHit& b) { return a.s < b.s; });
-        for (auto& h : hits) {
-          double path = 1.0;
-          {
-            const Module& m = d.modules[h.module];
-            double tn = std::sqrt(dot3(h.T, h.T));
-            double cz = std::fabs(dot3(m.ez, h.T)) / tn;
-            path = 1.0 / std::max(cz, 0.05);
-          }
-          double qtot = (21000.0 + 1400.0 * moyal(rng)) * std::min(path, 8.0);
-          depositHit(d, h, qtot, rng, deposits);
-          ++nh;
-          ++ev->nSimHits;
-        }
-        // multiple scattering at the last hit, restart the helix there
-        const SimHit& last = hits.back();
-        double tn = std::sqrt(dot3(last.T, last.T));
-        double dir[3] = {last.T[0] / tn, last.T[1] / tn, last.T[2] / tn};
-        double x0 = (bestKind == 0 ? 0.025 : 0.03) * hits.size();
-        double th0 = 0.0136 / p * std::sqrt(x0) * (1 + 0.038 * std::log(x0));
-        double u1[3] = {-dir[1], dir[0], 0};
-        double nu = std::sqrt(u1[0] * u1[0] + u1[1] * u1[1]);
-        if (nu < 1e-9) {
-          u1[0] = 1; u1[1] = 0; nu = 1;
-        }
-        u1[0] /= nu; u1[1] /= nu;
-        double u2[3] = {dir[1] * u1[2] - dir[2] * u1[1], dir[2] * u1[0] - dir[0] * u1[2], dir[0] * u1[1] - dir[1] * u1[0]};
-        double a1 = th0 * N(rng), a2 = th0 * N(rng);
-        double nd[3];
-        for (int k = 0; k < 3; ++k) nd[k] = dir[k] + a1 * u1[k] + a2 * u2[k];
-        double nn = std::sqrt(dot3(nd, nd));
-        for (int k = 0; k < 3; ++k) nd[k] /= nn;
-        double ptn = p * std::sqrt(nd[0] * nd[0] + nd[1] * nd[1]);
-        if (ptn < 1e-3) break;
-        hx.x = last.P[0];
-        hx.y = last.P[1];
-        hx.z = last.P[2];
-        hx.psi = std::atan2(nd[1], nd[0]);
-        hx.cot = nd[2] / std::sqrt(nd[0] * nd[0] + nd[1] * nd[1]);
-        hx.kappa = q * kBField / ptn;
+      propagate(vx, vy, vz, pt, eta, phi, q, iv, 0.0);
+    }
+    // soft component: exponential pT above soft_pt_min (loopers below
+    // ~0.3 GeV curl inside the pixel volume), a share of it produced
+    // displaced (conversions and decays: outside the CA's z0/dca cuts).
+    // No random numbers are drawn when it is off, so events without it are
+    // those of earlier versions of this generator.
+    if (cfg.soft_per_vertex > 0) {
+      int nsoft = std::poisson_distribution<int>(cfg.soft_per_vertex)(rng);
+      std::exponential_distribution<double> Ex(1.0 / std::max(cfg.soft_pt_mean, 1e-3));
+      for (int it = 0; it < nsoft; ++it) {
+        double pt = cfg.soft_pt_min + Ex(rng);
+        double eta = (2 * U(rng) - 1) * cfg.eta_max;
+        double phi = (2 * U(rng) - 1) * kPi;
+        int q = U(rng) < 0.5 ? -1 : 1;
+        double start = U(rng) < cfg.secondary_frac ? 2.0 + 10.0 * U(rng) : 0.0;
+        propagate(vx, vy, vz, pt, eta, phi, q, iv, start);
       }
-      ev->tpt.push_back(float(pt));
-      ev->teta.push_back(float(eta));
-      ev->tphi.push_back(float(phi));
-      ev->tq.push_back(q);
-      ev->tv.push_back(iv);
-      ev->tnh.push_back(nh);
     }
   }
   // merge deposits per pixel

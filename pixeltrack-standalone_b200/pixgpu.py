@@ -27,16 +27,16 @@ _TYPES = {
     "moduleId": np.uint32, "clusModuleStart": np.uint32, "xl": np.float32, "yl": np.float32,
     "xerr": np.float32, "yerr": np.float32, "xg": np.float32, "yg": np.float32, "zg": np.float32,
     "rg": np.float32, "charge": np.int32, "iphi": np.int16, "xsize": np.int16, "ysize": np.int16,
-    "detInd": np.uint16, "hitsLayerStart": np.uint32, "phiOff": np.uint32, "phiBins": np.uint16,
-    "agcLadderR": np.float32, "cellInner": np.uint16, "cellOuter": np.uint16, "cellLayerPair": np.int16,
+    "detInd": np.uint16, "hitsLayerStart": np.uint32, "phiOff": np.uint32, "phiBins": np.uint32,
+    "agcLadderR": np.float32, "cellInner": np.uint32, "cellOuter": np.uint32, "cellLayerPair": np.int16,
     "cellDoubletId": np.int32, "cellUsed": np.uint16, "cellNbrOff": np.uint32, "cellNbr": np.uint32,
-    "cellTrkOff": np.uint32, "cellTrk": np.uint16, "outerHitOff": np.uint32, "outerHitCells": np.uint32,
-    "tupleOff": np.uint32, "tupleHits": np.uint16, "tupleDet": np.uint16, "quality": np.uint8,
+    "cellTrkOff": np.uint32, "cellTrk": np.uint32, "outerHitOff": np.uint32, "outerHitCells": np.uint32,
+    "tupleOff": np.uint32, "tupleHits": np.uint32, "tupleDet": np.uint16, "quality": np.uint8,
     "state": np.float32, "cov": np.float32, "pt": np.float32, "eta": np.float32, "chi2": np.float32,
     "zv": np.float32, "wv": np.float32, "vchi2": np.float32, "ptv2": np.float32, "ndof": np.int32,
     "sortInd": np.uint16, "idv": np.int16,
     "outerHitOffRaw": np.uint32, "outerHitCellsRaw": np.uint32, "cellNbrOffRaw": np.uint32,
-    "cellNbrRaw": np.uint32, "cellTrkOffRaw": np.uint32, "cellTrkRaw": np.uint16,
+    "cellNbrRaw": np.uint32, "cellTrkOffRaw": np.uint32, "cellTrkRaw": np.uint32,
 }
 SCALARS = ["nDigis", "nModules", "nClusters", "nHits", "nCells", "nTuples", "nVertices", "nNbrLists",
            "nTrkLists"]
@@ -84,6 +84,8 @@ def synth():
                                           ctypes.POINTER(ctypes.c_size_t)]
         _synth.ps_detector_write.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         _synth.ps_detector_destroy.argtypes = [ctypes.c_void_p]
+        _synth.ps_calibrated_event_config.argtypes = [ctypes.c_void_p]
+        _synth.ps_default_event_config.argtypes = [ctypes.c_void_p]
         _synth.ps_fit_tuples.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
                                          ctypes.c_void_p, ctypes.c_void_p]
     return _synth
@@ -96,7 +98,8 @@ class DetectorConfig(ctypes.Structure):
 class EventConfig(ctypes.Structure):
     _fields_ = [("tracks_per_vertex", ctypes.c_double), ("pt_min", ctypes.c_double), ("pt_index", ctypes.c_double),
                 ("eta_max", ctypes.c_double), ("noise_frac", ctypes.c_double), ("inject_errors", ctypes.c_int),
-                ("fixed_pu", ctypes.c_int)]
+                ("fixed_pu", ctypes.c_int), ("soft_per_vertex", ctypes.c_double), ("soft_pt_min", ctypes.c_double),
+                ("soft_pt_mean", ctypes.c_double), ("secondary_frac", ctypes.c_double)]
 
 
 class Truth(ctypes.Structure):
@@ -108,6 +111,10 @@ class Truth(ctypes.Structure):
 
 ES_NAMES = ["cablingMap.bin", "gain.bin", "cpefast.bin", "beamspot.bin", "fedIds.bin"]
 BASE_SEED = 20261203
+# the benchmark's PU50 events: event k is seed BENCH_SEED_BASE + k of the
+# calibrated event model
+BENCH_SEED_BASE = BASE_SEED + 100000
+BENCH_MODEL = "calibrated"
 # pg_flag bits (include/pixgpu.h)
 PG_FLAG_TUPLE_OVERFLOW = 1 << 5
 PG_FLAG_CELL_OVERFLOW = 1 << 6
@@ -138,10 +145,18 @@ class Detector:
             raise RuntimeError("ps_detector_write failed")
 
     def event(self, seed, pu, tracks_per_vertex=None, inject_errors=0, noise_frac=None, fixed_pu=True,
-              with_truth=False):
+              with_truth=False, model="dense"):
+        """One raw.bin record.  model: "dense" (every track prompt and above 0.5 GeV,
+        ps_default_event_config) or "calibrated" (ps_calibrated_event_config: a soft,
+        mostly displaced component; PU50 gives ~57k digis, ~18k hits, ~1.6k loose tracks)."""
         lib = synth()
         cfg = EventConfig()
-        lib.ps_default_event_config(ctypes.byref(cfg))
+        if model == "dense":
+            lib.ps_default_event_config(ctypes.byref(cfg))
+        elif model == "calibrated":
+            lib.ps_calibrated_event_config(ctypes.byref(cfg))
+        else:
+            raise ValueError("model: 'dense' or 'calibrated'")
         if tracks_per_vertex is not None:
             cfg.tracks_per_vertex = tracks_per_vertex
         if noise_frac is not None:
@@ -199,11 +214,20 @@ CA_FIELDS = ("min_hits_per_ntuplet", "include_jumping_forward_doublets", "early_
              "ideal_conditions", "do_cluster_cut", "do_z0_cut", "do_pt_cut")
 
 
+# per-event container capacities (pg_config cap_* fields); 0 keeps the reference's value
+CAPS_FIELDS = ("fed_words", "hits", "doublets", "lists", "tuples", "multiplicity", "hit_to_tuple")
+# capacities for events up to pileup 250 of the calibrated generator (PU250:
+# ~86k hits, ~4.3M doublets, ~0.93M cells with tracks, ~0.61M tuples)
+WIDE_CAPS = {"fed_words": 400000, "hits": 131072, "doublets": 6 << 20, "lists": 2 << 20, "tuples": (1 << 20) - 1,
+             "multiplicity": (1 << 20) - 1, "hit_to_tuple": 1 << 20}
+
+
 class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("max_events", ctypes.c_uint32), ("max_words_per_batch", ctypes.c_uint32),
                 ("slots", ctypes.c_uint32), ("use_graphs", ctypes.c_uint32), ("pool_words", ctypes.c_uint64),
                 ("hbm_fraction", ctypes.c_double), ("riemann_fit", ctypes.c_uint32), ("vertex_algo", ctypes.c_uint32)] + \
-        [(n, ctypes.c_uint32) for n in CA_FIELDS] + [("formatter_errors", ctypes.c_uint32), ("fed_scan", ctypes.c_uint32)]
+        [(n, ctypes.c_uint32) for n in CA_FIELDS] + [("formatter_errors", ctypes.c_uint32), ("fed_scan", ctypes.c_uint32)] + \
+        [("cap_" + n, ctypes.c_uint32) for n in CAPS_FIELDS]
 
 
 def tune_kernel_names():
@@ -257,7 +281,7 @@ RESULT_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_ui
 # (field, dtype, elements per track / vertex)
 _TRACK_FIELDS = [("tuple_index", np.uint32, 1), ("track_n_hits", np.uint8, 1), ("quality", np.uint8, 1),
                  ("state", np.float32, 5), ("cov", np.float32, 15), ("pt", np.float32, 1), ("eta", np.float32, 1),
-                 ("chi2", np.float32, 1), ("hits", np.uint16, 5), ("vertex", np.int16, 1)]
+                 ("chi2", np.float32, 1), ("hits", np.uint32, 5), ("vertex", np.int16, 1)]
 _VERTEX_FIELDS = [("zv", np.float32), ("wv", np.float32), ("vchi2", np.float32), ("ptv2", np.float32),
                   ("ndof", np.int32), ("sort_ind", np.uint16)]
 
@@ -414,12 +438,13 @@ class Chain:
 
     def __init__(self, es_images, max_events=64, max_words_per_batch=None, slots=1, device=0, use_graphs=True,
                  pool_words=0, hbm_fraction=0.5, riemann_fit=False, vertex_algo=0, ca=None, formatter_errors=False,
-                 fed_scan="host"):
+                 fed_scan="host", caps=None):
         """ca: CAHitNtupletGeneratorOnGPU parameters overriding the reference's (pg_config field
         names: min_hits_per_ntuplet, include_jumping_forward_doublets, early_fishbone, late_fishbone,
         ideal_conditions, do_cluster_cut, do_z0_cut, do_pt_cut).  formatter_errors: record the FED
         loop's framing errors ("formatterErrors").  fed_scan: "host", or "device" for the header and
-        trailer checks and the word concatenation on the GPU."""
+        trailer checks and the word concatenation on the GPU.  caps: per-event container capacities
+        (CAPS_FIELDS names, e.g. WIDE_CAPS) above the reference's."""
         lib = gpu_lib()
         self._keep = list(es_images)
         img = ESImages(*[x for b in self._keep for x in (b, len(b))])
@@ -438,6 +463,10 @@ class Chain:
             if k not in CA_FIELDS:
                 raise ValueError("unknown CA parameter %s" % k)
             setattr(cfg, k, int(v))
+        for k, v in (caps or {}).items():
+            if k not in CAPS_FIELDS:
+                raise ValueError("unknown capacity %s" % k)
+            setattr(cfg, "cap_" + k, int(v))
         self._h = ctypes.c_void_p()
         rc = lib.pg_create(ctypes.byref(img), ctypes.byref(cfg), ctypes.byref(self._h))
         if rc != 0:
@@ -506,9 +535,10 @@ class Chain:
         def capped(off, val, cap):
             off = off.astype(np.int64)
             sizes = np.minimum(np.diff(off), cap)
-            newoff = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint32)
-            parts = [val[off[i]:off[i] + sizes[i]] for i in range(len(sizes))]
-            return newoff, (np.concatenate(parts) if parts else val[:0]).astype(val.dtype)
+            newoff = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+            # source position of every kept entry: its segment's start plus its rank
+            pos = np.arange(newoff[-1]) - np.repeat(newoff[:-1] - off[:-1], sizes)
+            return newoff.astype(np.uint32), val[pos].astype(val.dtype)
         out["outerHitOff"], out["outerHitCells"] = capped(self.product(k, "outerHitOffRaw"),
                                                           self.product(k, "outerHitCellsRaw"), 128)
         if out["nHits"] == 0:

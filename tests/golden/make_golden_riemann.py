@@ -1,6 +1,6 @@
 """Writes tests/golden/riemann_fits.npz: the reference's own Riemann fit
 (plugin-PixelTriplets/RiemannFit.h, compiled from its sources by
-oracle/ref/Makefile with the linear-algebra shim of oracle/ref/eigen_shim) on
+oracle/ref/Makefile with the linear-algebra subset of pixeltrack-standalone_b200/framework/compat/eigen) on
 seeded synthetic 3-, 4- and 5-hit tuples (5-hit tuples are fitted on their
 first 4 hits, as fit5as4 does).  Needs the reference tree; run from the
 repository root:

@@ -9,9 +9,17 @@ One JSON line (rank 0):
              records: FED scan on the host, H2D of the words, chain, results
              written to host memory, every step inside the timed region;
   per_event  the plain one-event-per-launch chain (no graph), for the
-             batched-vs-per-event ratio;
+             batched-vs-per-event ratio, with its per-event latency p50/p99;
   serving    the continuous-batching serving loop (pg_serve): Poisson
-             arrivals, p50/p99 latency from arrival to completion;
+             arrivals swept over the offered load, p50/p99 latency from
+             arrival to completion, and the highest sustained rate whose p99
+             stays under 5 ms against the best per-event rate;
+  batched_mixed_pu, serving_mixed_pu
+             the uneven-pileup configurations (PU uniform 20-200 per 64-event
+             batch; PU log-uniform 30-250 served at 10-100 kHz) with the
+             container capacities widened for them, and their capacity flags;
+  dense_pu50 the batched rate on the denser event model (every track prompt
+             and above 0.5 GeV: ~3x the doublets of the calibrated one);
   roofline   the dominant kernel (largest share of device time, found by a
              timed census of every kernel) against the measured HBM copy
              bandwidth, its duration measured with timing events captured
@@ -48,8 +56,10 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import replicas  # noqa: E402
 
 METRIC = "events/s and p50/p99 latency at PU50: batched serving vs per-event chain, one B200"
-DATA = ("synthetic: seeded Phase-1 pixel events (1856 modules, 108 FEDs, helices in 3.8 T, Landau charge), "
-        "PU50 ~61k digis/event, packed into FED words through the generated cabling map")
+DATA = ("synthetic: seeded Phase-1 pixel events (1856 modules, 108 FEDs, helices in 3.8 T, Landau charge; "
+        "calibrated event model: prompt power-law tracks above 0.5 GeV plus a soft, mostly displaced component), "
+        "PU50 ~57k digis, ~18k hits, ~1.6k loose tracks per event, packed into FED words through the generated "
+        "cabling map")
 PU = 50
 SEED0 = 20261203
 
@@ -92,13 +102,14 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--batch", type=int, default=64, help="events per launch sequence")
-    p.add_argument("--events", type=int, default=576, help="distinct PU50 events (inputs > L2)")
+    p.add_argument("--events", type=int, default=1000, help="distinct PU50 events (inputs > L2)")
     p.add_argument("--slots", type=int, default=3, help="batches in flight")
     p.add_argument("--per-event", type=int, default=256, help="events for the one-event-per-launch leg")
     p.add_argument("--serve", type=int, default=4000, help="requests for the serving leg (0: skip)")
     p.add_argument("--serve-batch", type=int, default=32, help="max events per serving batch")
     p.add_argument("--serve-slots", type=int, default=6, help="batches in flight in the serving loop")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
+    p.add_argument("--serve-mixed", type=int, default=2000, help="requests per uneven-pileup serving point (0: skip)")
     p.add_argument("--mixed-batches", type=int, default=3,
                    help="distinct 64-event batches with PU uniform in [20, 200] (0: skip that leg)")
     p.add_argument("--tune-out", default="", help="where to write the table --autotune finds")
@@ -115,10 +126,10 @@ def dist_env():
     return rank, world, local
 
 
-def make_events(det, n, pu=PU, base=SEED0 + 100000):
+def make_events(det, n, pu=PU, base=SEED0 + 100000, model="calibrated"):
     """n distinct seeded events, generated on all host cores."""
     with cf.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
-        return list(ex.map(lambda k: det.event(base + k, pu), range(n)))
+        return list(ex.map(lambda k: det.event(base + k, pu, model=model), range(n)))
 
 
 class Clocks:
@@ -175,6 +186,22 @@ class Clocks:
         if not sm:
             return None
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+# capacities for the 64-event batches of PU uniform in [20, 200] (calibrated
+# model, PU200: ~68k hits, ~2.8M doublets, ~0.5M cells with tracks, ~0.33M tuples)
+PU200_CAPS = {"fed_words": 300000, "hits": 98304, "doublets": 4 << 20, "lists": 1 << 20, "tuples": 512 * 1024,
+              "multiplicity": 512 * 1024, "hit_to_tuple": 1 << 19}
 
 
 def peaks():
@@ -396,11 +423,14 @@ def run_ours(a):
     units = collections.Counter()
     result_bytes = [0]
 
+    margins = collections.Counter()
+
     def done(slot):
         probe_ms.extend(ms for _, ms in chain.probe_read(slot))
         sm = chain.summary(slot)
         units.update(units_of(sm))
         result_bytes[0] += sm["result_bytes"]
+        margins.update({"cut_decisions_on_boundary": sm["n_cut_margin"], "flagged_events": sm["n_flagged_events"]})
 
     sub = lambda i: chain.submit_pooled(batches[i % len(batches)], keep=True)  # noqa: E731
     pipeline(chain, torch, a.warmup, sub, lambda s: None)
@@ -447,22 +477,28 @@ def run_ours(a):
            "chain_roofline": {"achieved": chain_ach, "peak": hbm, "unit": "GB/s", "frac": chain_ach / hbm,
                               "bytes_per_event": chain_bytes(u_evt)},
            "units_per_event": u_evt,
+           "cut_margin": {"decisions_within_4_ulp_per_event": margins["cut_decisions_on_boundary"] / events,
+                          "events_with_capacity_flags": margins["flagged_events"], "events": events},
            "kernel_shares": {k: round(v / total_ms, 4) for k, v in
                              sorted(census.items(), key=lambda x: -x[1])[:12]},
            "result_bytes_per_step": result_bytes[0] / max(1, a.steps)}
 
     # ------------------------------------------------------------ batched, uneven pileup
     # 64 events per launch with PU uniform in [20, 200] (the batched-chain
-    # configuration), device-resident inputs, the same tuning
+    # configuration), device-resident inputs, the same tuning, and the
+    # container capacities widened for PU 200 (at the reference's, most of
+    # these events would be truncated: no tuples above PU ~80)
     if rank == 0 and world == 1 and a.mixed_batches:
         rng = np.random.default_rng(3)
         mpus = rng.uniform(20.0, 200.0, B * a.mixed_batches)
         with cf.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
-            mraws = list(ex.map(lambda k: det.event(SEED0 + 200000 + k, float(mpus[k])), range(len(mpus))))
+            mraws = list(ex.map(lambda k: det.event(SEED0 + 200000 + k, float(mpus[k]), model="calibrated"),
+                                range(len(mpus))))
         mnw = [len(r) // 4 for r in mraws]
         mb = [mnw[i * B:(i + 1) * B] for i in range(a.mixed_batches)]
         mchain = pixgpu.Chain(det.es, max_events=B, max_words_per_batch=max(sum(x) for x in mb) + 1024,
-                              slots=a.slots, device=dev, pool_words=sum(mnw) + 64 * len(mnw) + 4096)
+                              slots=2, device=dev, pool_words=sum(mnw) + 64 * len(mnw) + 4096,
+                              caps=PU200_CAPS)
         load_tuning(mchain)
         mh = []
         for r in mraws:
@@ -473,14 +509,21 @@ def run_ours(a):
             mh.append(h)
         mbatches = [mh[i * B:(i + 1) * B] for i in range(a.mixed_batches)]
         mchain.prepare(B)
+        mflags = [0]
+
+        def mdone(slot):
+            mflags[0] += mchain.summary(slot)["n_flagged_events"]
         msub = lambda i: mchain.submit_pooled(mbatches[i % len(mbatches)], keep=True)  # noqa: E731
         pipeline(mchain, torch, a.warmup, msub, lambda s: None)
-        msteps = max(8, a.steps // 2)
-        mms = pipeline(mchain, torch, msteps, msub, lambda s: None)
+        msteps = max(8, a.steps // 4)
+        mms = pipeline(mchain, torch, msteps, msub, mdone)
+        slot_gb = mchain.slot_bytes() / 1e9
         mchain.close()
         out["batched_mixed_pu"] = {"pu": "uniform 20-200", "events_per_batch": B, "distinct_events": len(mraws),
                                    "mean_words_per_event": float(np.mean(mnw)), "steps": msteps,
-                                   "events_per_s": msteps * B / (mms / 1e3), "ms_per_step": mms / msteps}
+                                   "events_per_s": msteps * B / (mms / 1e3), "ms_per_step": mms / msteps,
+                                   "caps": PU200_CAPS, "slot_gb": slot_gb,
+                                   "events_with_capacity_flags": mflags[0], "events_timed": msteps * B}
 
     # ------------------------------------------------------------ end to end through pg_submit
     nbh = len(raws) // B
@@ -532,53 +575,103 @@ def run_ours(a):
             c1 = pixgpu.Chain(det.es, max_events=1, max_words_per_batch=int(max(nw)) + 1024, slots=slots,
                               device=dev, use_graphs=graphs, pool_words=sum(nw) + 64 * len(nw) + 4096)
             load_tuning(c1)
-            hs = [c1.pool_put(r) for r in raws[:64]]
+            hs = [c1.pool_put(r) for r in raws]
             sub1 = lambda i: c1.submit_pooled([hs[i % len(hs)]], keep=True)  # noqa: E731
             pipeline(c1, torch, 8, sub1, lambda s: None)
             pms = pipeline(c1, torch, a.per_event, sub1, lambda s: None)
-            c1.close()
             pe[label] = a.per_event / (pms / 1e3)
+            if slots == 1:
+                # latency of one event alone: submit, wait, on the host clock
+                lat = []
+                for i in range(min(a.per_event, 256)):
+                    t0 = time.perf_counter()
+                    s1 = c1.submit_pooled([hs[i % len(hs)]], keep=True)
+                    c1.wait(s1)
+                    lat.append(time.perf_counter() - t0)
+                    c1.release(s1)
+                pe_lat = {"p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                          "events": len(lat)}
+            c1.close()
         best = max(pe.values())
-        out["per_event"] = {"events_per_s": pe, "mode": "one event per launch sequence, plain launches (no graph), "
-                                                          "device-resident inputs"}
+        out["per_event"] = {"events_per_s": pe, "latency_1_stream": pe_lat,
+                            "mode": "one event per launch sequence, plain launches (no graph), device-resident inputs"}
         out["batched_vs_per_event"] = value / best
 
-        # ------------------------------------------------------------ serving loop
+        # ------------------------------------------------------------ serving loop: load sweep
         if a.serve:
             sv = {}
             sc = pixgpu.Chain(det.es, max_events=a.serve_batch, max_words_per_batch=int(max(nw)) * a.serve_batch,
                               slots=a.serve_slots, device=dev, pool_words=64 * 1000 * 1000)
             load_tuning(sc)
             sc.prepare(a.serve_batch)
-            for frac in (0.5, 0.8):
+            best_ok = None
+            for frac in (0.2, 0.35, 0.5, 0.65, 0.8, 0.9):
                 rate = frac * value
                 st, lat = sc.serve(raws, a.serve, rate_hz=rate, max_batch=a.serve_batch, seed=11, upload_threads=4)
-                sv["%.0f%% of batched throughput" % (100 * frac)] = {
-                    "offered_hz": st["offered_hz"], "events_per_s": st["events_per_s"], "p50_ms": st["p50_ms"],
-                    "p99_ms": st["p99_ms"], "mean_batch": st["mean_batch"], "batches": st["batches"],
-                    "admission_waits": st["admission_waits"]}
+                pt = {"offered_hz": st["offered_hz"], "events_per_s": st["events_per_s"], "p50_ms": st["p50_ms"],
+                      "p99_ms": st["p99_ms"], "mean_batch": st["mean_batch"], "batches": st["batches"],
+                      "admission_waits": st["admission_waits"]}
+                sv["%.0f%% of batched throughput" % (100 * frac)] = pt
+                if st["p99_ms"] < 5.0 and (best_ok is None or st["events_per_s"] > best_ok["events_per_s"]):
+                    best_ok = dict(pt, load=frac)
             sc.close()
             out["serving"] = {"pu": PU, "requests": a.serve, "max_batch": a.serve_batch, "slots": a.serve_slots,
-                              "points": sv}
-            # uneven pileup: PU log-uniform in [30, 250], Poisson arrivals
+                              "points": sv,
+                              "best_under_5ms_p99": best_ok,
+                              "best_under_5ms_p99_vs_per_event": (best_ok["events_per_s"] / best) if best_ok else None}
+
+        # ------------------------------------------------------------ serving, uneven pileup (10-100 kHz)
+        if a.serve_mixed:
             rng = np.random.default_rng(7)
-            pus = np.exp(rng.uniform(np.log(30), np.log(250), 96))
+            pus = np.exp(rng.uniform(np.log(30), np.log(250), 128))
             with cf.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
-                mraws = list(ex.map(lambda k: det.event(SEED0 + 300000 + k, float(pus[k])), range(len(pus))))
-            mc = pixgpu.Chain(det.es, max_events=a.serve_batch, max_words_per_batch=a.serve_batch * 300000,
-                              slots=a.serve_slots,
-                              device=dev, pool_words=128 * 1000 * 1000)
+                mraws = list(ex.map(lambda k: det.event(SEED0 + 300000 + k, float(pus[k]), model="calibrated"),
+                                    range(len(pus))))
+            mb_serve = 16
+            mc = pixgpu.Chain(det.es, max_events=mb_serve, max_words_per_batch=mb_serve * 300000, slots=3,
+                              device=dev, pool_words=96 * 1000 * 1000, caps=pixgpu.WIDE_CAPS)
             load_tuning(mc)
-            mc.prepare(a.serve_batch)
+            mc.prepare(mb_serve)
             mv = {}
-            for rate in (1000.0, 2000.0):
-                st, _ = mc.serve(mraws, a.serve // 2, rate_hz=rate, max_batch=a.serve_batch, seed=13, upload_threads=4)
-                mv["%.0f Hz" % rate] = {"offered_hz": st["offered_hz"], "events_per_s": st["events_per_s"],
-                                        "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_batch": st["mean_batch"],
-                                        "admission_waits": st["admission_waits"]}
+            flagged = [0]
+
+            def on_result(req, ev, res):
+                if res["flags"] & ~(1 << 16):  # bit 16: compact result truncated, not a chain capacity
+                    flagged[0] += 1
+            for rate in (10000.0, 30000.0, 100000.0):
+                st, _ = mc.serve(mraws, a.serve_mixed, rate_hz=rate, max_batch=mb_serve, seed=13, upload_threads=4,
+                                 on_result=on_result)
+                mv["%.0f kHz" % (rate / 1e3)] = {"offered_hz": st["offered_hz"], "events_per_s": st["events_per_s"],
+                                                 "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                                                 "mean_batch": st["mean_batch"],
+                                                 "admission_waits": st["admission_waits"]}
+            slot_gb = mc.slot_bytes() / 1e9
             mc.close()
             out["serving_mixed_pu"] = {"pu": "log-uniform 30-250", "distinct_events": len(mraws),
-                                       "requests": a.serve // 2, "points": mv}
+                                       "requests_per_point": a.serve_mixed, "max_batch": mb_serve, "slots": 3,
+                                       "caps": pixgpu.WIDE_CAPS, "slot_gb": slot_gb,
+                                       "results_with_capacity_flags": flagged[0], "points": mv,
+                                       "note": "offered rates above the sustained rate are admission-limited: "
+                                               "arrivals wait for pool space and free slots"}
+
+        # ------------------------------------------------------------ dense event model, batched
+        draws = make_events(det, 2 * B, base=SEED0 + 400000, model="dense")
+        dnw = [len(r) // 4 for r in draws]
+        dchain = pixgpu.Chain(det.es, max_events=B, max_words_per_batch=int(max(dnw)) * B + 1024, slots=a.slots,
+                              device=dev, pool_words=sum(dnw) + 64 * len(dnw) + 4096)
+        load_tuning(dchain)
+        dh = [dchain.pool_put(r) for r in draws]
+        dbatches = [dh[:B], dh[B:2 * B]]
+        dchain.prepare(B)
+        dunits = collections.Counter()
+        dsub = lambda i: dchain.submit_pooled(dbatches[i % 2], keep=True)  # noqa: E731
+        pipeline(dchain, torch, a.warmup, dsub, lambda s: None)
+        dsteps = max(8, a.steps // 4)
+        dms = pipeline(dchain, torch, dsteps, dsub, lambda s: dunits.update(units_of(dchain.summary(s))))
+        dchain.close()
+        out["dense_pu50"] = {"events_per_s": dsteps * B / (dms / 1e3), "steps": dsteps,
+                             "units_per_event": {k: v / (dsteps * B) for k, v in dunits.items()},
+                             "model": "every track prompt and above 0.5 GeV (ps_default_event_config)"}
 
         # ------------------------------------------------------------ fits: FP64 and mixed precision
         out["fits"] = fit_leg(det, dev, torch)
@@ -591,13 +684,27 @@ def run_ours(a):
         if oracle.ref_available():
             d = tempfile.mkdtemp()
             det.write(d)
-            wall_c, _ = oracle.ref_time_events(d, sample, cores)
+            wall_c, lat_c = oracle.ref_time_events(d, sample, cores)
             kind = "reference"
         else:
-            wall_c, _ = oracle.Oracle(det.es).time_events(sample, cores)
+            d = None
+            wall_c, lat_c = oracle.Oracle(det.es).time_events(sample, cores)
             kind = "port"
         out["cpu_baseline"] = {"value": len(sample) / wall_c, "unit": "events/s", "cores": cores, "kind": kind,
-                               "sample": "%d distinct PU50 events, one chain instance per thread" % len(sample)}
+                               "sample": "%d distinct PU50 events, one chain instance per thread" % len(sample),
+                               "cpu_model": cpu_model(),
+                               "latency_p50_ms": 1e3 * float(np.percentile(lat_c, 50)),
+                               "latency_p99_ms": 1e3 * float(np.percentile(lat_c, 99))}
+        # the reference's plain chain on 100 PU20 events, one thread (config 1)
+        c1raws = make_events(det, 100, pu=20, base=SEED0, model="dense")
+        if oracle.ref_available():
+            wall_1, lat_1 = oracle.ref_time_events(d, c1raws, 1)
+        else:
+            wall_1, lat_1 = oracle.Oracle(det.es).time_events(c1raws, 1)
+        out["cpu_pu20_one_thread"] = {"events_per_s": 100 / wall_1, "events": 100, "threads": 1, "kind": kind,
+                                      "latency_p50_ms": 1e3 * float(np.percentile(lat_1, 50)),
+                                      "latency_p99_ms": 1e3 * float(np.percentile(lat_1, 99)),
+                                      "model": "power-law tracks above 0.5 GeV (the dense model), ~25k digis"}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:

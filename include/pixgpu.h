@@ -139,6 +139,14 @@ typedef struct pg_event_counts {
   uint32_t n_words, n_modules, n_digi_errors, n_hits;
   uint32_t n_cells, n_tuples, n_loose, n_vertices;
   uint32_t flags;               /* capacity flags (PG_FLAG_*) */
+  /* cut decisions whose two sides lie within four single-precision ulps
+     (2^-22 relative) of each other, counted over every decision the chain
+     evaluates: the doublet cuts (gpuPixelDoubletsAlgos.h:146-170: z window,
+     dr, z0, pt), the CA cuts (GPUCACell.h:175-206: RZ alignment, curvature,
+     dca) and the classification cuts (CAHitNtupletGeneratorKernelsImpl.h:
+     340-406: chi2, tip, pt, zip).  These are the decisions that can flip when
+     the operands come from another precision (an FP32 fit, FMA contraction). */
+  uint32_t n_cut_margin_doublets, n_cut_margin_ca, n_cut_margin_quality;
 } pg_event_counts;
 
 /* the reference's configuration; start every pg_config from it */
@@ -196,7 +204,7 @@ void* pg_slot_stream(pg_ctx* ctx, uint32_t slot);
  * PixelVertexSoAFromCUDA.cc).  Written by the device into mapped pinned host memory;
  * the pointers stay valid until pg_release of the slot. */
 typedef struct pg_result_view {
-  uint32_t n_tracks;       /* loose tracks stored (at most 8192) */
+  uint32_t n_tracks;       /* loose tracks stored (at most 16384) */
   uint32_t n_loose_all;    /* loose tracks found */
   uint32_t n_vertices, n_hits, n_tuples, n_digis, n_cells;
   uint32_t flags;          /* capacity flags; bit 16: more loose tracks than stored */
@@ -235,6 +243,8 @@ typedef struct pg_batch_summary {
   uint32_t n_events, flags;          /* flags: OR over the events */
   uint64_t n_tracks, n_vertices, result_bytes;
   uint64_t n_digis, n_modules, n_hits, n_cells, n_edges, n_tuples, n_tuple_hits;
+  uint64_t n_cut_margin;             /* cut decisions on their float boundary (pg_event_counts) */
+  uint64_t n_flagged_events;         /* events with any capacity flag (PG_FLAG_*; not bit 16) */
 } pg_batch_summary;
 int pg_batch_summary_get(pg_ctx* ctx, uint32_t slot, pg_batch_summary* out);
 

@@ -118,6 +118,11 @@ struct CA {
   std::vector<uint32_t> tmBins;
   // fit results
   std::vector<float> state, cov, pt, eta, chi2;      // state[i*5+k], cov[i*15+k]
+  // cut decisions whose two sides lie within kCutMarginRel of each other
+  // (cutNear): doublet cuts, CA cuts (RZ alignment, curvature, dca),
+  // classification cuts; the decisions that can flip when the operands are
+  // computed in another precision
+  uint32_t nearDoublet = 0, nearCA = 0, nearQuality = 0;
   uint32_t size(uint32_t t) const { return tupleOff[t + 1] - tupleOff[t]; }
 };
 
@@ -174,6 +179,17 @@ void brokenLineFit(int N, const double* hits /*3xN col-major*/, const float* hit
 // Riemann fit of one tuple of N (3 or 4) hits; same I/O as brokenLineFit
 void riemannFit(int N, const double* hits /*3xN col-major*/, const float* hits_ge /*6xN*/, double B, float* state5,
                 float* cov15, float* pt, float* eta, float* chi2);
+
+// Relative margin below which a cut decision counts as on its boundary: four
+// single-precision ulps (2^-22) of the larger side.  Evaluated in double from
+// the operands the cut compares, so that every implementation of the chain
+// that computes those operands bit for bit counts the same decisions.
+constexpr double kCutMarginRel = 1.0 / 4194304.0;
+inline bool cutNear(double a, double b) {
+  const double d = a > b ? a - b : b - a;
+  const double m = (a < 0 ? -a : a) > (b < 0 ? -b : b) ? (a < 0 ? -a : a) : (b < 0 ? -b : b);
+  return d <= kCutMarginRel * m;
+}
 
 // whole chain for one raw.bin event record
 struct Options {

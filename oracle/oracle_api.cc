@@ -132,6 +132,9 @@ void record(Handle& h) {
   h.put("pt", ca.pt.data(), nt);
   h.put("eta", ca.eta.data(), nt);
   h.put("chi2", ca.chi2.data(), nt);
+  h.put1<uint32_t>("nCutMarginDoublets", ca.nearDoublet);
+  h.put1<uint32_t>("nCutMarginCA", ca.nearCA);
+  h.put1<uint32_t>("nCutMarginQuality", ca.nearQuality);
   h.put1<uint32_t>("nVertices", v.nvFinal);
   h.put("zv", v.zv.data(), v.nvFinal);
   h.put("wv", v.wv.data(), v.nvFinal);

@@ -49,12 +49,16 @@ inline float short2phi(short x) {
 inline uint32_t phiBin(int16_t t) { return uint32_t((int(t) >> 9) & 127); }
 
 // GPUCACell.h:175-185; fabs(float) resolves to the double overload in the serial build
-bool areAlignedRZ(float r1, float z1, float ri, float zi, float ro, float zo, float ptmin, float thetaCut) {
+bool areAlignedRZ(float r1, float z1, float ri, float zi, float ro, float zo, float ptmin, float thetaCut,
+                  uint32_t* near) {
   float radius_diff = std::abs(r1 - ro);
   float distance_13_squared = radius_diff * radius_diff + (z1 - zo) * (z1 - zo);
   float pMin = ptmin * std::sqrt(distance_13_squared);
   double tan_12_13_half_mul_distance_13_squared = ::fabs(double(z1 * (ri - ro) + zi * (ro - r1) + zo * (r1 - ri)));
-  return tan_12_13_half_mul_distance_13_squared * pMin <= double(thetaCut * distance_13_squared * radius_diff);
+  const double lhs = tan_12_13_half_mul_distance_13_squared * pMin;
+  const double rhs = double(thetaCut * distance_13_squared * radius_diff);
+  *near += cutNear(lhs, rhs);
+  return lhs <= rhs;
 }
 
 // CircleEq.h:23-107 (float), dca0 and curvature
@@ -117,6 +121,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
   ca.nbrPool = 1;
   ca.trkPool = 1;
   ca.apcM = ca.apcN = 0;
+  ca.nearDoublet = ca.nearCA = ca.nearQuality = 0;
   ca.tupleBins = kTupleBins;
   ca.tupleOff.assign(kTupleBins + 1, 0);
   ca.tupleHits.assign(5 * kTupleBins, 0);
@@ -155,6 +160,7 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
       uint16_t mi = hh.detInd[i];
       if (mi > 2000) continue;
       float mez = hh.zg[i];
+      ca.nearDoublet += cutNear(mez, kMinZ[pairLayerId]) + cutNear(mez, kMaxZ[pairLayerId]);
       if (mez < kMinZ[pairLayerId] || mez > kMaxZ[pairLayerId]) continue;
       int16_t mes = -1;
       if (prm.doClusterCut) {
@@ -182,7 +188,10 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
           if (prm.doZ0Cut) {
             float zo = hh.zg[oi], ro = hh.rg[oi];
             float dr = ro - mer;
-            if (dr > kMaxR[pairLayerId] || dr < 0 || std::abs((mez * ro - mer * zo)) > z0cut * dr) continue;
+            ca.nearDoublet += cutNear(dr, kMaxR[pairLayerId]);
+            if (dr > kMaxR[pairLayerId] || dr < 0) continue;
+            ca.nearDoublet += cutNear(std::abs((mez * ro - mer * zo)), z0cut * dr);
+            if (std::abs((mez * ro - mer * zo)) > z0cut * dr) continue;
           }
           int16_t mop = hh.iphi[oi];
           uint16_t idphi = uint16_t(std::min(std::abs(int16_t(mop - mep)), std::abs(int16_t(mep - mop))));
@@ -202,10 +211,15 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
           if (prm.doPtCut) {
             float ri = mer, ro = hh.rg[oi];
             float dphi = short2phi(short(idphi));
+            ca.nearDoublet += cutNear(dphi * dphi * (minRadius2T4 - ri * ro), (ro - ri) * (ro - ri));
             if (dphi * dphi * (minRadius2T4 - ri * ro) > (ro - ri) * (ro - ri)) continue;
           }
           uint32_t ind = ca.nCells;
-          if (ind >= caps.doublets) break;
+          // full container: the reference leaves the bin (break), storing
+          // nothing more; the candidates are still tested here so that the
+          // cut-margin count covers every candidate of the windows (the
+          // stored doublets are the same)
+          if (ind >= caps.doublets) continue;
           ca.nCells++;
           ca.inner.push_back(i);
           ca.outer.push_back(oi);
@@ -233,7 +247,8 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
     bool isBarrel = float(hh.detInd[innerHit]) < 1184;
     for (uint32_t oc : vi) {
       float r1 = ca.innerR[oc], z1 = ca.innerZ[oc];
-      bool aligned = areAlignedRZ(r1, z1, ri, zi, ro, zo, kPtMin, isBarrel ? kThetaCutBarrel : kThetaCutForward);
+      bool aligned =
+          areAlignedRZ(r1, z1, ri, zi, ro, zo, kPtMin, isBarrel ? kThetaCutBarrel : kThetaCutForward, &ca.nearCA);
       if (!aligned) continue;
       // GPUCACell::dcaCut (GPUCACell.h:187-206)
       float x1 = hh.xg[ca.inner[oc]], y1 = hh.yg[ca.inner[oc]];
@@ -241,7 +256,9 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
       float x3 = hh.xg[ca.outer[idx]], y3 = hh.yg[ca.outer[idx]];
       float region = float(hh.detInd[ca.inner[oc]]) < 96 ? kDcaCutInner : kDcaCutOuter;
       Circle eq = circleEq(x1, y1, x2, y2, x3, y3);
+      ca.nearCA += cutNear(eq.c, kHardCurvCut);
       if (eq.c > kHardCurvCut) continue;
+      ca.nearCA += cutNear(std::abs(dca0(eq)), region * std::abs(eq.c));
       if (!(std::abs(dca0(eq)) < region * std::abs(eq.c))) continue;
       // GPUCACell::addOuterNeighbor (GPUCACell.h:67-86): pool of maxNumOfActiveDoublets lists
       if (ca.nbr[oc].empty() && !hasNbrList[oc]) {
@@ -445,9 +462,12 @@ void makeTuples(const ES& es, const Hits& hh, CA& ca, const CAParams& prm) {
     if (isNaN) continue;
     float pt = std::min<float>(ca.pt[it], chi2MaxPt);
     float chi2Cut = chi2Scale * (chi2Coeff[0] + pt * (chi2Coeff[1] + pt * (chi2Coeff[2] + pt * chi2Coeff[3])));
+    ca.nearQuality += cutNear(3.f * ca.chi2[it], chi2Cut);
     if (3.f * ca.chi2[it] >= chi2Cut) continue;
     float maxTip = nh > 3 ? 0.5f : 0.3f, minPt = nh > 3 ? 0.3f : 0.5f, maxZip = 12.f;
     float tip = ca.state[size_t(it) * 5 + 1], zip = ca.state[size_t(it) * 5 + 4];
+    // the three region cuts are all evaluated (their margins counted), then combined
+    ca.nearQuality += cutNear(std::abs(tip), maxTip) + cutNear(ca.pt[it], minPt) + cutNear(std::abs(zip), maxZip);
     bool isOk = (std::abs(tip) < maxTip) and (ca.pt[it] > minPt) and (std::abs(zip) < maxZip);
     if (isOk) ca.quality[it] = kLoose;
   }

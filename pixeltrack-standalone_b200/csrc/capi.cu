@@ -667,6 +667,9 @@ int pg_event_counts_get(pg_ctx* c, uint32_t k, pg_event_counts* out) {
   out->n_tuples = ec.nTuples;
   out->n_loose = ec.nLoose;
   out->n_vertices = ec.nVertices;
+  out->n_cut_margin_doublets = ec.nearDoublet;
+  out->n_cut_margin_ca = ec.nearCA;
+  out->n_cut_margin_quality = ec.nearQuality;
   out->flags = ec.flags;
   return PG_OK;
 }
@@ -705,8 +708,12 @@ int slotProduct(pg_ctx* c, Slot& s, uint32_t k, const char* name, void* dst, siz
                tb = size_t(k) * kTupleBins, vb = size_t(k) * kMaxVtx;
   const uint32_t nh = ec.nHits, nc = ec.nCells;
   if (n == "nDigis" || n == "nModules" || n == "nClusters" || n == "nHits" || n == "nCells" || n == "nTuples" ||
-      n == "nVertices" || n == "nNbrLists" || n == "nTrkLists") {
-    uint32_t v = n == "nDigis" ? ec.nWords
+      n == "nVertices" || n == "nNbrLists" || n == "nTrkLists" || n == "nCutMarginDoublets" || n == "nCutMarginCA" ||
+      n == "nCutMarginQuality") {
+    uint32_t v = n == "nCutMarginDoublets" ? ec.nearDoublet
+                 : n == "nCutMarginCA" ? ec.nearCA
+                 : n == "nCutMarginQuality" ? ec.nearQuality
+                 : n == "nDigis" ? ec.nWords
                  : n == "nModules" ? ec.nModules
                  : (n == "nClusters" || n == "nHits") ? ec.nHits
                  : n == "nCells" ? ec.nCells
@@ -919,6 +926,8 @@ int pg_batch_summary_get(pg_ctx* c, uint32_t slot, pg_batch_summary* out) {
     out->n_edges += h->nEdges;
     out->n_tuples += h->nTuples;
     out->n_tuple_hits += h->nTupleHits;
+    out->n_cut_margin += uint64_t(h->nearDoublet) + h->nearCA + h->nearQuality;
+    out->n_flagged_events += (h->flags & ~kFlagResultOverflow) ? 1 : 0;
   }
   return PG_OK;
 }

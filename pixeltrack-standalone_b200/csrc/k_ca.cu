@@ -119,7 +119,8 @@ __device__ __forceinline__ void loadPairTable(const EventCounters* c, PairTable&
   __syncthreads();
 }
 
-__device__ __forceinline__ bool doubletSeed(const PairTable& c, const HitsView& hh, uint32_t j, DoubletSeed& d) {
+__device__ __forceinline__ bool doubletSeed(const PairTable& c, const HitsView& hh, uint32_t j, DoubletSeed& d,
+                                            uint32_t* near = nullptr) {
   uint32_t pair = 0;
   while (j >= c.pairCum[pair]) ++pair;
   const uint8_t inner = cLayerPairs[2 * pair], outer = cLayerPairs[2 * pair + 1];
@@ -132,6 +133,7 @@ __device__ __forceinline__ bool doubletSeed(const PairTable& c, const HitsView& 
   d.i = i;
   if (hh.detInd[i] > 2000) return false;
   d.mez = hh.zg[i];
+  if (near) *near += cutNear(d.mez, cMinZ[pair]) + cutNear(d.mez, cMaxZ[pair]);
   if (d.mez < cMinZ[pair] || d.mez > cMaxZ[pair]) return false;
   d.mes = -1;
   if (c.ca.doClusterCut) {
@@ -163,8 +165,10 @@ __device__ __forceinline__ bool doubletSeed(const PairTable& c, const HitsView& 
   return true;
 }
 
-// candidate test on a packed hit record (kPhiRec layout)
-__device__ __forceinline__ bool doubletAccept(const DoubletSeed& d, const uint4 rec) {
+// candidate test on a packed hit record (kPhiRec layout); with `near`, the
+// float cuts evaluated that lie on their boundary are counted
+template <bool kNear = false>
+__device__ __forceinline__ bool doubletAccept(const DoubletSeed& d, const uint4 rec, uint32_t& near) {
   constexpr float z0cut = 12.f;
   constexpr float minRadius = 0.5f * 87.78f;
   constexpr float minRadius2T4 = 4.f * minRadius * minRadius;
@@ -173,7 +177,12 @@ __device__ __forceinline__ bool doubletAccept(const DoubletSeed& d, const uint4 
   if ((rec.w & 0x7ffu) > 2000) return false;
   const float zo = __uint_as_float(rec.x), ro = __uint_as_float(rec.y);
   const float dr = ro - d.mer;
-  if ((d.cuts & 1u) && (dr > d.maxr || dr < 0 || fabsf((d.mez * ro - d.mer * zo)) > z0cut * dr)) return false;
+  if (d.cuts & 1u) {
+    if (kNear) near += cutNear(dr, d.maxr);
+    if (dr > d.maxr || dr < 0) return false;
+    if (kNear) near += cutNear(fabsf((d.mez * ro - d.mer * zo)), z0cut * dr);
+    if (fabsf((d.mez * ro - d.mer * zo)) > z0cut * dr) return false;
+  }
   const int16_t mop = int16_t(rec.z & 0xffffu);
   const uint16_t idphi = uint16_t(min(abs(int(int16_t(mop - d.mep))), abs(int(int16_t(d.mep - mop)))));
   if (idphi > d.iphicut) return false;
@@ -183,15 +192,19 @@ __device__ __forceinline__ bool doubletAccept(const DoubletSeed& d, const uint4 
                                     abs(d.mes - int(fabsf((d.mez - zo) / (d.mer - ro)) * dzdrFact + 0.5f)) > 20);
   if ((d.cuts & 2u) && cut) return false;
   const float dphi = float(short(idphi)) * i2p;
-  if ((d.cuts & 4u) && dphi * dphi * (minRadius2T4 - d.mer * ro) > (ro - d.mer) * (ro - d.mer)) return false;
+  if (d.cuts & 4u) {
+    if (kNear) near += cutNear(dphi * dphi * (minRadius2T4 - d.mer * ro), (ro - d.mer) * (ro - d.mer));
+    if (dphi * dphi * (minRadius2T4 - d.mer * ro) > (ro - d.mer) * (ro - d.mer)) return false;
+  }
   return true;
 }
 
 // One warp per inner-hit slot: lanes test consecutive candidates of the
 // window; the ballots give the count (pass 1) and the serial positions
 // (pass 2).  F(position among the slot's doublets, outer hit).
-template <typename F>
-__device__ __forceinline__ uint32_t warpDoublets(const DoubletSeed& d, const uint4* rec, F&& f) {
+template <bool kNear = false, typename F>
+__device__ __forceinline__ uint32_t warpDoublets(const DoubletSeed& d, const uint4* rec, F&& f, uint32_t* near = nullptr) {
+  uint32_t nearLane = 0;
   const uint32_t lane = laneId();
   uint32_t n = 0;
   for (int r = 0; r < 2; ++r) {
@@ -203,13 +216,14 @@ __device__ __forceinline__ uint32_t warpDoublets(const DoubletSeed& d, const uin
       if (p < en) {
         const uint4 h = rec[p];
         oi = h.w >> 11;
-        ok = doubletAccept(d, h);
+        ok = doubletAccept<kNear>(d, h, nearLane);
       }
       const uint32_t m = __ballot_sync(0xffffffffu, ok);
       if (ok) f(n + __popc(m & lanemaskLt()), oi);
       n += __popc(m);
     }
   }
+  if (kNear) *near += nearLane;
   return n;
 }
 
@@ -219,13 +233,13 @@ __device__ __forceinline__ uint32_t warpDoublets(const DoubletSeed& d, const uin
 // event), so that dense runs of consecutive slots spread over the warps.
 template <typename PerSlot>
 __device__ __forceinline__ void forSeedSlots(const PairTable& pt, const HitsView& hh, uint32_t ntot,
-                                             PerSlot&& perSlot) {
+                                             PerSlot&& perSlot, uint32_t* near) {
   const uint32_t lane = laneId(), wpb = blockDim.x >> 5;
   const uint32_t S = gridDim.x * wpb, w = blockIdx.x * wpb + (threadIdx.x >> 5);
   for (uint32_t r0 = 0; w + r0 * S < ntot; r0 += 32) {
     const uint32_t j = w + (r0 + lane) * S;
     DoubletSeed d;
-    const bool live = j < ntot && doubletSeed(pt, hh, j, d) && (d.e0 > d.b0 || d.e1 > d.b1);
+    const bool live = j < ntot && doubletSeed(pt, hh, j, d, near) && (d.e0 > d.b0 || d.e1 > d.b1);
     uint32_t m = __ballot_sync(0xffffffffu, live);
     perSlot(j, live, d, 0u);  // every lane sees its own slot first
     while (m) {
@@ -274,6 +288,7 @@ __global__ void kDoubletCount(Workspace ws) {
   const uint32_t S = gridDim.x * wpb, w = blockIdx.x * wpb + (threadIdx.x >> 5);
   const uint32_t R = ws.cap.scratch / S;  // staging entries per warp
   uint32_t used = 0;                     // warp-uniform
+  uint32_t near = 0;                     // per lane: cut decisions on their boundary
   forSeedSlots(pt, hh, ntot, [&](uint32_t j, bool live, const DoubletSeed& d, uint32_t phase) {
     if (phase == 0) {
       if (j < ntot && !live) cnt[j] = 0;
@@ -281,15 +296,17 @@ __global__ void kDoubletCount(Workspace ws) {
     }
     const uint32_t window = (d.e0 - d.b0) + (d.e1 - d.b1);
     const uint32_t at = used + window <= R ? w * R + used : kNoTemp;
-    const uint32_t n = warpDoublets(d, rec, [&](uint32_t k, uint32_t oi) {
+    const uint32_t n = warpDoublets<true>(d, rec, [&](uint32_t k, uint32_t oi) {
       if (at != kNoTemp) stage[at + k] = oi;
-    });
+    }, &near);
     if (at != kNoTemp) used += n;
     if (laneId() == phase - 1) {
       cnt[j] = n;
       slotStage[j] = at;
     }
-  });
+  }, &near);
+  near = __reduce_add_sync(0xffffffffu, near);
+  if (laneId() == 0 && near) atomicAdd(&ws.ev[e].nearDoublet, near);
 }
 
 // Pass 2: each slot's doublets from its staging entries to their serial
@@ -393,7 +410,8 @@ __global__ void kOuterHitFill(Workspace ws) {
 
 // GPUCACell::areAlignedRZ: fabs(float) binds to the double overload in the
 // serial build, so the left-hand product is formed in double precision
-__device__ __forceinline__ bool alignedRZ(float r1, float z1, float ri, float zi, float ro, float zo, float thetaCut) {
+__device__ __forceinline__ bool alignedRZ(float r1, float z1, float ri, float zi, float ro, float zo, float thetaCut,
+                                          uint32_t& near) {
   float radius_diff = fabsf(r1 - ro);
   float distance_13_squared = radius_diff * radius_diff + (z1 - zo) * (z1 - zo);
   const float area = z1 * (ri - ro) + zi * (ro - r1) + zo * (r1 - ri);
@@ -405,10 +423,13 @@ __device__ __forceinline__ bool alignedRZ(float r1, float z1, float ri, float zi
   if (rhs > 1e-15f && area * area * (kPtMin * kPtMin) * distance_13_squared > 1.0001f * rhs * rhs) return false;
   float pMin = kPtMin * sqrtf(distance_13_squared);
   double lhs = fabs(double(area));
+  // pairs the rejection above dropped lie far from the boundary
+  near += cutNear(lhs * double(pMin), double(rhs));
   return lhs * double(pMin) <= double(rhs);
 }
 
-__device__ __forceinline__ bool dcaCut(float x1, float y1, float x2, float y2, float x3, float y3, float region) {
+__device__ __forceinline__ bool dcaCut(float x1, float y1, float x2, float y2, float x3, float y3, float region,
+                                       uint32_t& near) {
   bool noflip = fabsf(x3 - x1) < fabsf(y3 - y1);
   float x1p = noflip ? x1 - x2 : y1 - y2;
   float y1p = noflip ? y1 - y2 : x1 - x2;
@@ -427,10 +448,12 @@ __device__ __forceinline__ bool dcaCut(float x1, float y1, float x2, float y2, f
   float cc = noflip ? ct : -ct;
   float alpha = noflip ? al2 : -be2;
   float beta = noflip ? be2 : -al2;
+  near += cutNear(cc, kHardCurvCut);
   if (cc > kHardCurvCut) return false;
   float xx = cc * x2 + alpha;
   float yy = cc * y2 + beta;
   float dca0 = sqrtf(xx * xx + yy * yy) - 1.f;
+  near += cutNear(fabsf(dca0), region * fabsf(cc));
   return fabsf(dca0) < region * fabsf(cc);
 }
 
@@ -478,6 +501,7 @@ __global__ void __launch_bounds__(256, 6) kConnect(Workspace ws, uint32_t* edgeO
   const uint32_t edgeCap = min(ws.cap.edges, ws.cap.scratch);
   const uint32_t lane = laneId(), wpb = blockDim.x >> 5;
   const uint32_t S = gridDim.x * wpb, w = blockIdx.x * wpb + (threadIdx.x >> 5);
+  uint32_t near = 0;  // per lane: cut decisions on their boundary
   for (uint32_t r0 = 0; w + r0 * S < ntot; r0 += 32) {
     const uint32_t jl = w + (r0 + lane) * S;
     uint32_t myBase = 0, myEnd = 0, myOb = 0, myM = 0;
@@ -531,8 +555,8 @@ __global__ void __launch_bounds__(256, 6) kConnect(Workspace ws, uint32_t* edgeO
             const uint32_t src = t < nc ? t : 0u;
             const float ro = __shfl_sync(0xffffffffu, sro, src), zo = __shfl_sync(0xffffffffu, szo, src);
             const float x3 = __shfl_sync(0xffffffffu, sx3, src), y3 = __shfl_sync(0xffffffffu, sy3, src);
-            const bool ok = t < nc && k < m && alignedRZ(rr1, r1.z, ri, zi, ro, zo, thetaCut) &&
-                            dcaCut(r1.x, r1.y, x2, y2, x3, y3, region);
+            const bool ok = t < nc && k < m && alignedRZ(rr1, r1.z, ri, zi, ro, zo, thetaCut, near) &&
+                            dcaCut(r1.x, r1.y, x2, y2, x3, y3, region, near);
             const uint32_t mask = __ballot_sync(0xffffffffu, ok);
             if (mask == 0) continue;
             uint32_t at = 0;
@@ -557,6 +581,8 @@ __global__ void __launch_bounds__(256, 6) kConnect(Workspace ws, uint32_t* edgeO
       }
     }
   }
+  near = __reduce_add_sync(0xffffffffu, near);
+  if (lane == 0 && near) atomicAdd(&c->nearCA, near);
 }
 
 __global__ void kEdgeScatter(Workspace ws, const uint32_t* edgeOc, const uint32_t* edgeIdx) {
@@ -971,6 +997,7 @@ __global__ void kClassify(Workspace ws) {
   const float* pt = ws.pt + size_t(e) * ws.cap.tuples;
   const float* chi2 = ws.chi2 + size_t(e) * ws.cap.tuples;
   const float c0 = float(0.68177776), c1 = float(0.74609577), c2 = float(-0.08035491), c3 = float(0.00315399);
+  uint32_t near = 0;  // per thread: cut decisions on their boundary
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
     uint32_t nh = tupleSize(toff, t);
     if (nh == 0) continue;  // beyond the serial loop's guard (only the overflow tail)
@@ -981,11 +1008,16 @@ __global__ void kClassify(Workspace ws) {
     if (isNaN) continue;
     float p = fminf(pt[t], 10.f);
     float chi2Cut = 30.f * (c0 + p * (c1 + p * (c2 + p * c3)));
+    near += cutNear(3.f * chi2[t], chi2Cut);
     if (3.f * chi2[t] >= chi2Cut) continue;
     float maxTip = nh > 3 ? 0.5f : 0.3f, minPt = nh > 3 ? 0.3f : 0.5f;
+    near += cutNear(fabsf(st[size_t(t) * 5 + 1]), maxTip) + cutNear(pt[t], minPt) +
+            cutNear(fabsf(st[size_t(t) * 5 + 4]), 12.f);
     bool isOk = (fabsf(st[size_t(t) * 5 + 1]) < maxTip) && (pt[t] > minPt) && (fabsf(st[size_t(t) * 5 + 4]) < 12.f);
     if (isOk) q[t] = kLoose;
   }
+  near = __reduce_add_sync(0xffffffffu, near);
+  if ((threadIdx.x & 31) == 0 && near) atomicAdd(&ws.ev[e].nearQuality, near);
 }
 
 __device__ __forceinline__ bool inTrkList(const uint32_t* off, const uint32_t* trk, uint32_t cell, uint32_t t) {

@@ -184,6 +184,7 @@ __global__ void kInitEvents(Workspace ws, uint32_t nEvents) {
     c->nBigMod = 0;
     c->nSegList[0] = c->nSegList[1] = c->nSegList[2] = c->nSegList[3] = 0;
     c->nBigHitMod = 0;
+    c->nearDoublet = c->nearCA = c->nearQuality = 0;
     c->flags = c->nWords > ws.cap.fedWords ? kFlagTooManyWords : 0u;
   }
   uint32_t* cim = ws.clusInModule + size_t(e) * kModStride;

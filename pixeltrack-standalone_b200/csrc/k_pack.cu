@@ -176,6 +176,9 @@ __global__ void __launch_bounds__(512) kPackResults(Workspace ws, uint8_t* out) 
     h.nEdges = c->nEdges;
     h.nTupleHits = toff[guard];
     h.nModules = c->nModules;
+    h.nearDoublet = c->nearDoublet;
+    h.nearCA = c->nearCA;
+    h.nearQuality = c->nearQuality;
     *reinterpret_cast<ResultHeader*>(base) = h;
     // the loose-track count of pg_event_counts (the last writer of the
     // quality codes, the triplet cleaner, has finished)

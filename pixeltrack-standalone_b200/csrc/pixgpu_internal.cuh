@@ -123,7 +123,19 @@ struct EventCounters {
   uint32_t nBigMod;             // modules queued for the block clusterizer
   uint32_t nSegList[4];         // list segments that received a second entry, per list ordering
   uint32_t nBigHitMod;          // modules queued for the block rechit kernel
+  // cut decisions on their float boundary (cutNear): doublet, CA and quality cuts
+  uint32_t nearDoublet, nearCA, nearQuality;
 };
+
+// A cut decision counts as on its boundary when its two sides lie within
+// four single-precision ulps (2^-22, relative) of the larger one, evaluated
+// in double from the operands the cut compares: the decisions that can flip
+// when those operands come from another precision.  The oracle counts the
+// same decisions with the same test.
+__device__ __forceinline__ uint32_t cutNear(double a, double b) {
+  const double d = fabs(a - b);
+  return d <= (1.0 / 4194304.0) * fmax(fabs(a), fabs(b)) ? 1u : 0u;
+}
 
 // ---------------------------------------------------------------- ES on device
 struct DeviceES {

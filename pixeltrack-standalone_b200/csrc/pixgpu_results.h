@@ -7,14 +7,15 @@
 
 namespace pixgpu {
 
-constexpr uint32_t kResultTracks = 8192;  // loose tracks kept per event
+constexpr uint32_t kResultTracks = 16384;  // loose tracks kept per event (PU 250: ~11k)
 constexpr uint32_t kResultVertices = 1024;
 constexpr uint32_t kFlagResultOverflow = 1u << 16;
 
 struct ResultHeader {
   uint32_t nTracks, nLooseAll, nVertices, nHits, nTuples, nDigis, nCells, flags;
   uint32_t nEdges, nTupleHits, nModules;
-  uint32_t pad[5];
+  uint32_t nearDoublet, nearCA, nearQuality;  // cut decisions on their float boundary
+  uint32_t pad[2];
 };
 constexpr size_t kResultTrackBytes = 4 + 1 + 1 + 20 + 60 + 4 + 4 + 4 + 20 + 2;  // per stored track
 constexpr size_t kResultVertexBytes = 4 + 4 + 4 + 4 + 4 + 2;                   // per stored vertex

@@ -39,7 +39,7 @@ _TYPES = {
     "cellNbrRaw": np.uint32, "cellTrkOffRaw": np.uint32, "cellTrkRaw": np.uint32,
 }
 SCALARS = ["nDigis", "nModules", "nClusters", "nHits", "nCells", "nTuples", "nVertices", "nNbrLists",
-           "nTrkLists"]
+           "nTrkLists", "nCutMarginDoublets", "nCutMarginCA", "nCutMarginQuality"]
 ERROR_DTYPE = np.dtype([("rawId", "<u4"), ("word", "<u4"), ("errorType", "u1"), ("fedId", "u1"),
                         ("pad", "u1", 2)])
 # PfFormatterError: the 64-bit header/trailer word, the error type, the full FED id
@@ -269,7 +269,8 @@ class ServeStats(ctypes.Structure):
 class BatchSummary(ctypes.Structure):
     _fields_ = [("n_events", ctypes.c_uint32), ("flags", ctypes.c_uint32)] + \
         [(n, ctypes.c_uint64) for n in ("n_tracks", "n_vertices", "result_bytes", "n_digis", "n_modules", "n_hits",
-                                        "n_cells", "n_edges", "n_tuples", "n_tuple_hits")]
+                                        "n_cells", "n_edges", "n_tuples", "n_tuple_hits", "n_cut_margin",
+                                        "n_flagged_events")]
 
 
 class ProbeEntry(ctypes.Structure):
@@ -303,7 +304,8 @@ def result_from_view(v):
 
 class EventCounts(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in ("n_words", "n_modules", "n_digi_errors", "n_hits", "n_cells",
-                                                "n_tuples", "n_loose", "n_vertices", "flags")]
+                                                "n_tuples", "n_loose", "n_vertices", "flags", "n_cut_margin_doublets",
+                                                "n_cut_margin_ca", "n_cut_margin_quality")]
 
 
 def gpu_lib():
@@ -716,6 +718,10 @@ class Chain:
         torch.cuda.synchronize()
         return {"state": st.cpu().numpy(), "cov": cv.cpu().numpy(), "pt": pt.cpu().numpy(), "eta": eta.cpu().numpy(),
                 "chi2": chi2.cpu().numpy()}
+
+    def slot_bytes(self):
+        """Device bytes of one batch slot (pg_slot_bytes)."""
+        return int(gpu_lib().pg_slot_bytes(self._h))
 
     def close(self):
         if self._h:

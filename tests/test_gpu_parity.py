@@ -103,3 +103,28 @@ def test_broken_line_fit_matches_oracle(chain, nhits, N):
         den = np.maximum(np.maximum(np.abs(a), np.abs(b)), 1e-30)
         rel = np.abs(a - b) / den
         assert rel.max() <= RTOL, (k, float(rel.max()))
+
+
+def test_cut_margin_counts_match_oracle(default_detector):
+    """Cut decisions on their float boundary (within four single-precision
+    ulps), counted per event by the GPU chain and by the oracle over the same
+    decisions: doublet cuts, CA cuts and classification cuts.  40 dense PU50
+    events, one batch; the oracle finds 21 such decisions in them."""
+    import oracle
+    import pixgpu
+    raws = [default_detector.event(pixgpu.BASE_SEED + 5000 + k, 50) for k in range(40)]
+    c = pixgpu.Chain(default_detector.es, max_events=40, max_words_per_batch=sum(len(r) // 4 for r in raws) + 1024)
+    try:
+        c.process(raws)
+        got = [c.counts(k) for k in range(len(raws))]
+    finally:
+        c.close()
+    orc = oracle.Oracle(default_detector.es)
+    total = 0
+    for k, r in enumerate(raws):
+        w = orc.process(r, list(oracle.CUT_MARGIN_COUNTS))
+        want = (w["nCutMarginDoublets"], w["nCutMarginCA"], w["nCutMarginQuality"])
+        have = (got[k]["n_cut_margin_doublets"], got[k]["n_cut_margin_ca"], got[k]["n_cut_margin_quality"])
+        assert have == want, (k, have, want)
+        total += sum(want)
+    assert total > 0

@@ -117,6 +117,10 @@ typedef struct pg_config {
                                     ErrorChecker records none (ErrorChecker.cc:36) */
   uint32_t fed_scan;             /* 0: the FED header/trailer checks and word concatenation on the host
                                     (default); 1: on the device, from the whole FED buffers */
+  uint32_t mixed_fit;            /* 1: the chain fits with the mixed-precision variant of its fit
+                                    (pg_fit_broken_line_mixed, pg_fit_riemann_mixed) in place of FP64
+                                    (the reference's precision, default 0); see pg_event_counts for the
+                                    cut decisions whose outcome precision can change */
   /* Per-event container capacities.  0 keeps the reference's value (given
      beside each), whose truncation order the results reproduce.  Larger
      values run the same algorithm on events whose containers would overflow
@@ -163,6 +167,19 @@ size_t pg_slot_bytes(const pg_ctx* ctx);
  * FED index, as SiPixelRawToClusterCUDA::produce does on the host. */
 int pg_unpack_raw(const pg_ctx* ctx, const uint8_t* raw, size_t raw_size, uint32_t* words, uint8_t* fed_ids,
                   uint32_t cap_words, uint32_t* n_words);
+
+/* Clustering of given digis on slot 0 (synchronous): countModules, findClus
+ * and clusterChargeCut (plugin-SiPixelClusterizer/gpuClustering.h:19-273,
+ * gpuClusterChargeCut.h:14-114) on n digis in host memory -- module index
+ * (9999 for an invalid digi), row, column and calibrated charge, the
+ * input of the reference's clustering kernels and of its clustering test
+ * (test/gpuClustering_t.h).  Out: the module index after the charge cut
+ * (9999 for removed pixels), the cluster index per digi, and per module the
+ * cluster count, module id and the module-run starts (module_start[0] = the
+ * run count, as countModules leaves it; 2000 / 2001 entries). */
+int pg_cluster_digis(pg_ctx* ctx, uint32_t n, const uint16_t* module_ind, const uint16_t* xx, const uint16_t* yy,
+                     const uint16_t* adc, uint16_t* module_ind_out, int32_t* clus, uint32_t* clus_in_module,
+                     uint32_t* module_id, uint32_t* module_start, uint32_t* n_modules, uint32_t* flags);
 
 /* Synchronous: unpack, copy to the device, run the chain on slot 0 and wait. */
 int pg_process_batch(pg_ctx* ctx, uint32_t n_events, const uint8_t* const* raws, const size_t* raw_sizes);

@@ -438,6 +438,7 @@ void pg_default_config(pg_config* cfg) {
   cfg->do_pt_cut = 1;
   cfg->formatter_errors = 0;
   cfg->fed_scan = 0;
+  cfg->mixed_fit = 0;
   // the reference's container capacities
   cfg->cap_fed_words = cfg->cap_hits = cfg->cap_doublets = cfg->cap_lists = 0;
   cfg->cap_tuples = cfg->cap_multiplicity = cfg->cap_hit_to_tuple = 0;
@@ -458,6 +459,7 @@ int createSlot(pg_ctx* c, Slot& s, size_t bytes) {
   s.ws.ca.doPtCut = c->cfg.do_pt_cut != 0;
   s.ws.ca.earlyFishbone = c->cfg.early_fishbone != 0;
   s.ws.ca.lateFishbone = c->cfg.late_fishbone != 0;
+  s.ws.ca.mixedFit = c->cfg.mixed_fit != 0;
   if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&s.gathered, cudaEventDisableTiming) != cudaSuccess ||
@@ -550,7 +552,8 @@ int pg_create(const pg_es_images* es, const pg_config* cfgIn, pg_ctx** out) {
     pg_default_config(&c->cfg);
   if (c->cfg.max_events == 0 || c->cfg.max_words_per_batch == 0 || c->cfg.max_words_per_batch > (1u << 30) ||
       c->cfg.vertex_algo > 2 || c->cfg.min_hits_per_ntuplet < 3 || c->cfg.min_hits_per_ntuplet > 4 ||
-      c->cfg.fed_scan > 1 || (c->cfg.fed_scan && c->cfg.pool_words))  // the pool stages on the host
+      c->cfg.fed_scan > 1 || (c->cfg.fed_scan && c->cfg.pool_words) ||  // the pool stages on the host
+      c->cfg.mixed_fit > 1)
     return PG_ERR_ARG;
   if (!resolveCaps(c->cfg, &c->caps)) return PG_ERR_ARG;
   c->device = c->cfg.device;
@@ -619,6 +622,50 @@ int pg_unpack_raw(const pg_ctx* c, const uint8_t* raw, size_t n, uint32_t* words
                   uint32_t* nWords) {
   if (!c || !raw || !words || !fedIds || !nWords) return PG_ERR_ARG;
   return unpackRaw(c->hes.fedIds, raw, n, words, fedIds, cap, nWords);
+}
+
+int pg_cluster_digis(pg_ctx* c, uint32_t n, const uint16_t* moduleInd, const uint16_t* xx, const uint16_t* yy,
+                     const uint16_t* adc, uint16_t* moduleIndOut, int32_t* clus, uint32_t* clusInModule,
+                     uint32_t* moduleId, uint32_t* moduleStart, uint32_t* nModules, uint32_t* flags) {
+  if (!c || !moduleInd || !xx || !yy || !adc || !moduleIndOut || !clus || !clusInModule || !moduleId ||
+      !moduleStart || !nModules)
+    return PG_ERR_ARG;
+  Slot& s = c->slots[0];
+  if (s.state != SlotState::kFree) return fail(c, PG_ERR_BUSY, "slot 0 holds an asynchronous batch");
+  if (n > c->cfg.max_words_per_batch || n > c->caps.fedWords)
+    return fail(c, PG_ERR_CAPACITY, "more digis than a batch or an event holds");
+  cudaSetDevice(c->cfg.device);
+  Workspace& ws = s.ws;
+  std::vector<int32_t> iota(n);
+  for (uint32_t i = 0; i < n; ++i) iota[i] = int32_t(i);
+  const uint32_t off[2] = {0, n};
+  cudaError_t e = cudaSuccess;
+  auto h2d = [&](void* dst, const void* src, size_t bytes) {
+    if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s.stream);
+  };
+  h2d(ws.moduleInd, moduleInd, size_t(n) * 2);
+  h2d(ws.xx, xx, size_t(n) * 2);
+  h2d(ws.yy, yy, size_t(n) * 2);
+  h2d(ws.adc, adc, size_t(n) * 2);
+  h2d(ws.clus, iota.data(), size_t(n) * 4);
+  h2d(ws.wordOffsets, off, sizeof(off));
+  if (e == cudaSuccess) e = runClusters(ws, 1, s.stream);
+  EventCounters ec{};
+  auto d2h = [&](void* dst, const void* src, size_t bytes) {
+    if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s.stream);
+  };
+  d2h(moduleIndOut, ws.moduleInd, size_t(n) * 2);
+  d2h(clus, ws.clus, size_t(n) * 4);
+  d2h(clusInModule, ws.clusInModule, size_t(kMaxModules) * 4);
+  d2h(moduleId, ws.moduleId, size_t(kMaxModules) * 4);
+  d2h(moduleStart, ws.moduleStart, size_t(kMaxModules + 1) * 4);
+  d2h(&ec, ws.ev, sizeof(ec));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);
+  if (e != cudaSuccess) return cudaFail(c, e, "clustering");
+  s.nEvents = 0;  // the slot's products no longer describe a batch
+  *nModules = std::min(ec.nModules, kMaxModules);
+  if (flags) *flags = ec.flags;
+  return PG_OK;
 }
 
 int pg_stage_batch(pg_ctx* c, uint32_t slot, uint32_t nEvents, const uint8_t* const* raws, const size_t* sizes) {

@@ -346,6 +346,8 @@ __device__ void blFit(const double* H3, const float* ge, double B, FitOut& out) 
   out.chi2 = float((double(cchi2) + lchi2) / (2 * N - 5));
 }
 
+#include "k_fit_mixed.cuh"
+
 // zero the fit results of every stored tuple (the reference's TrackSoA is value-initialised)
 // Tuples that no fit writes get zero fit results: those kept out of the
 // multiplicity bins (duplicates), and every tuple of an event whose bins
@@ -367,8 +369,11 @@ __global__ void kFitZero(Workspace ws) {
   }
 }
 
+// the fits a chain can run (pg_config riemann_fit, mixed_fit)
+enum FitMode { kFitBrokenLine, kFitRiemann, kFitBrokenLineMixed, kFitRiemannMixed };
+
 // one thread per (tuple of the multiplicity bin nh); fits the first N hits
-template <int N, bool kRiemann = false>
+template <int N, int kMode = kFitBrokenLine>
 __device__ __forceinline__ void blFitBin(const DeviceES& es, const Workspace& ws, uint32_t nh) {
   uint32_t e = blockIdx.y;
   const uint32_t* tm = ws.tmOff + size_t(e) * 16;
@@ -402,10 +407,24 @@ __device__ __forceinline__ void blFitBin(const DeviceES& es, const Workspace& ws
       H[3 * i + 2] = ws.zg[hb + hit];
     }
     FitOut o;
-    if constexpr (kRiemann)
+    if constexpr (kMode == kFitRiemann) {
       rfFit<N, double>(H, ge, B, o);
-    else
+    } else if constexpr (kMode == kFitRiemannMixed) {
+      rfFit<N, float>(H, ge, B, o);
+    } else if constexpr (kMode == kFitBrokenLineMixed) {
+      // the mixed fit takes single-precision hits relative to the first one
+      // and the first hit in double precision (k_fit_mixed.cuh)
+      float Hf[3 * N];
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        Hf[3 * i + 0] = float(H[3 * i + 0] - H[0]);
+        Hf[3 * i + 1] = float(H[3 * i + 1] - H[1]);
+        Hf[3 * i + 2] = float(H[3 * i + 2]);
+      }
+      blFitMixed<N>(Hf, ge, H[0], H[1], float(B), B, o);
+    } else {
       blFit<N>(H, ge, B, o);
+    }
 #pragma unroll
     for (int j = 0; j < 5; ++j) ws.state[tb * 5 + size_t(tkid) * 5 + j] = o.state[j];
 #pragma unroll
@@ -429,9 +448,25 @@ __global__ void __launch_bounds__(128, 4) kBLFit(DeviceES es, Workspace ws) {
 // CAHitNtupletGeneratorOnGPU.cc:116-120; RiemannFitOnGPU.cc:3-110)
 __global__ void __launch_bounds__(128) kRiemannFit(DeviceES es, Workspace ws) {
   if (blockIdx.z == 0)
-    blFitBin<3, true>(es, ws, 3);
+    blFitBin<3, kFitRiemann>(es, ws, 3);
   else
-    blFitBin<4, true>(es, ws, 3 + blockIdx.z);
+    blFitBin<4, kFitRiemann>(es, ws, 3 + blockIdx.z);
+}
+
+// the mixed-precision variants of both fits inside the chain (pg_config
+// mixed_fit): a precision choice beside the reference's FP64 fits, whose
+// effect on the chain's quality codes and vertices is measured against them
+__global__ void __launch_bounds__(128, 4) kBLFitMixed(DeviceES es, Workspace ws) {
+  if (blockIdx.z == 0)
+    blFitBin<3, kFitBrokenLineMixed>(es, ws, 3);
+  else
+    blFitBin<4, kFitBrokenLineMixed>(es, ws, 3 + blockIdx.z);
+}
+__global__ void __launch_bounds__(128) kRiemannFitMixed(DeviceES es, Workspace ws) {
+  if (blockIdx.z == 0)
+    blFitBin<3, kFitRiemannMixed>(es, ws, 3);
+  else
+    blFitBin<4, kFitRiemannMixed>(es, ws, 3 + blockIdx.z);
 }
 
 // standalone fit of externally supplied tuples (fit workload and tests)
@@ -457,7 +492,6 @@ __global__ void kBLFitDirect(uint32_t n, const double* hits, const float* hge, d
   }
 }
 
-#include "k_fit_mixed.cuh"
 
 }  // namespace
 
@@ -467,10 +501,15 @@ cudaError_t runFits(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStr
   PG_PROBED("kFitZero", stream, kFitZero<<<dim3(tunedGrid(ws, kTuneFitZero, g.x), nEvents), 256, 0, stream>>>(ws));
   // FP64-bound: enough warps per SM to cover the double-precision latency
   const uint32_t fx = nEvents >= 32 ? 16 : (nEvents >= 8 ? 64 : 296);
-  if (riemann)
-    PG_PROBED("kRiemannFit", stream, kRiemannFit<<<dim3(tunedGrid(ws, kTuneFit, fx), nEvents, 3), 128, 0, stream>>>(es, ws));
+  const dim3 fg(tunedGrid(ws, kTuneFit, fx), nEvents, 3);
+  if (riemann && ws.ca.mixedFit)
+    PG_PROBED("kRiemannFitMixed", stream, kRiemannFitMixed<<<fg, 128, 0, stream>>>(es, ws));
+  else if (riemann)
+    PG_PROBED("kRiemannFit", stream, kRiemannFit<<<fg, 128, 0, stream>>>(es, ws));
+  else if (ws.ca.mixedFit)
+    PG_PROBED("kBLFitMixed", stream, kBLFitMixed<<<fg, 128, 0, stream>>>(es, ws));
   else
-    PG_PROBED("kBLFit", stream, kBLFit<<<dim3(tunedGrid(ws, kTuneFit, fx), nEvents, 3), 128, 0, stream>>>(es, ws));
+    PG_PROBED("kBLFit", stream, kBLFit<<<fg, 128, 0, stream>>>(es, ws));
   return cudaGetLastError();
 }
 

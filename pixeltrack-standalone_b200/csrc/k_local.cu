@@ -1163,6 +1163,20 @@ __global__ void kSortErrors(Workspace ws) {
 
 }  // namespace
 
+// countModules, findClus and clusterChargeCut alone, on digis already in ws
+// (xx, yy, calibrated adc, moduleInd, clus = index) with their word offsets
+cudaError_t runClusters(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
+  PG_PROBED("kInitEvents", stream, kInitEvents<<<nEvents, 256, 0, stream>>>(ws, nEvents));
+  const int flatBlocks = 148 * 8;
+  PG_PROBED("kModuleBoundaries", stream, kModuleBoundaries<<<tunedGrid(ws, kTuneModuleBoundaries, flatBlocks), 256, 0, stream>>>(ws, nEvents));
+  PG_PROBED("kSortModules", stream, kSortModules<<<nEvents, 1024, 0, stream>>>(ws, nEvents));
+  PG_PROBED("kFindClusters", stream,
+            kFindClustersSmall<<<dim3((kMaxModules + kSmallWarps - 1) / kSmallWarps, nEvents), kSmallWarps * 32, 0,
+                                 stream>>>(ws));
+  PG_PROBED("kFindClustersBig", stream, kFindClustersBig<<<dim3(tunedGrid(ws, kTuneFindClustersBig, 64), nEvents), kClusThreads, 0, stream>>>(ws));
+  return cudaGetLastError();
+}
+
 cudaError_t runLocal(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   PG_PROBED("kInitEvents", stream, kInitEvents<<<nEvents, 256, 0, stream>>>(ws, nEvents));
   const int flatBlocks = 148 * 8;

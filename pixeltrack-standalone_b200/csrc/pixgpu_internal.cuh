@@ -171,6 +171,7 @@ struct CAConfig {
   uint32_t idealConditions;  // every ladder treated as outer in the cluster-size cut
   uint32_t doClusterCut, doZ0Cut, doPtCut;
   uint32_t earlyFishbone, lateFishbone;
+  uint32_t mixedFit;         // the fits' mixed-precision variants (pg_config mixed_fit)
 };
 
 // FED scan on the device (fedscan.cu): the batch's whole FED blocks and the
@@ -366,6 +367,8 @@ cudaError_t runChain(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaSt
                      int vertexAlgo = 0);
 // Individual stages (used by runChain and by the stage-level tests)
 cudaError_t runLocal(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream);
+// countModules + findClus + clusterChargeCut on digis already in ws
+cudaError_t runClusters(Workspace& ws, uint32_t nEvents, cudaStream_t stream);
 cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream);
 cudaError_t runFits(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStream_t stream, bool riemann = false);
 // algo: 0 clusterTracksByDensity (default), 1 clusterTracksDBSCAN, 2 clusterTracksIterative

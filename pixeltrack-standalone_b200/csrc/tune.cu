@@ -32,13 +32,16 @@ int tuneIndex(const char* name) {
   if (!name) return -1;
   for (uint32_t i = 0; i < kNumTune; ++i)
     if (std::strcmp(name, kTuneNames[i]) == 0) return int(i);
-  if (std::strcmp(name, "kRiemannFit") == 0) return int(kTuneFit);
+  if (std::strcmp(name, "kRiemannFit") == 0 || std::strcmp(name, "kBLFitMixed") == 0 ||
+      std::strcmp(name, "kRiemannFitMixed") == 0)
+    return int(kTuneFit);
   return -1;
 }
 
 // the name the probe sees for a tunable launch
 const char* launchedName(const pg_ctx* c, uint32_t id) {
-  if (id == kTuneFit && c->cfg.riemann_fit) return "kRiemannFit";
+  if (id == kTuneFit && c->cfg.riemann_fit) return c->cfg.mixed_fit ? "kRiemannFitMixed" : "kRiemannFit";
+  if (id == kTuneFit && c->cfg.mixed_fit) return "kBLFitMixed";
   return kTuneNames[id];
 }
 

@@ -226,7 +226,8 @@ class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("max_events", ctypes.c_uint32), ("max_words_per_batch", ctypes.c_uint32),
                 ("slots", ctypes.c_uint32), ("use_graphs", ctypes.c_uint32), ("pool_words", ctypes.c_uint64),
                 ("hbm_fraction", ctypes.c_double), ("riemann_fit", ctypes.c_uint32), ("vertex_algo", ctypes.c_uint32)] + \
-        [(n, ctypes.c_uint32) for n in CA_FIELDS] + [("formatter_errors", ctypes.c_uint32), ("fed_scan", ctypes.c_uint32)] + \
+        [(n, ctypes.c_uint32) for n in CA_FIELDS] + [("formatter_errors", ctypes.c_uint32), ("fed_scan", ctypes.c_uint32),
+                                                      ("mixed_fit", ctypes.c_uint32)] + \
         [("cap_" + n, ctypes.c_uint32) for n in CAPS_FIELDS]
 
 
@@ -440,13 +441,14 @@ class Chain:
 
     def __init__(self, es_images, max_events=64, max_words_per_batch=None, slots=1, device=0, use_graphs=True,
                  pool_words=0, hbm_fraction=0.5, riemann_fit=False, vertex_algo=0, ca=None, formatter_errors=False,
-                 fed_scan="host", caps=None):
+                 fed_scan="host", caps=None, mixed_fit=False):
         """ca: CAHitNtupletGeneratorOnGPU parameters overriding the reference's (pg_config field
         names: min_hits_per_ntuplet, include_jumping_forward_doublets, early_fishbone, late_fishbone,
         ideal_conditions, do_cluster_cut, do_z0_cut, do_pt_cut).  formatter_errors: record the FED
         loop's framing errors ("formatterErrors").  fed_scan: "host", or "device" for the header and
         trailer checks and the word concatenation on the GPU.  caps: per-event container capacities
-        (CAPS_FIELDS names, e.g. WIDE_CAPS) above the reference's."""
+        (CAPS_FIELDS names, e.g. WIDE_CAPS) above the reference's.  mixed_fit: the chain's fit in its
+        mixed-precision variant (FP32 with FP64 Cholesky solves and covariance) instead of FP64."""
         lib = gpu_lib()
         self._keep = list(es_images)
         img = ESImages(*[x for b in self._keep for x in (b, len(b))])
@@ -458,6 +460,7 @@ class Chain:
         cfg.use_graphs, cfg.pool_words, cfg.hbm_fraction = 1 if use_graphs else 0, pool_words, hbm_fraction
         cfg.riemann_fit, cfg.vertex_algo = 1 if riemann_fit else 0, int(vertex_algo)
         cfg.formatter_errors = 1 if formatter_errors else 0
+        cfg.mixed_fit = 1 if mixed_fit else 0
         if fed_scan not in ("host", "device"):
             raise ValueError("fed_scan: 'host' or 'device'")
         cfg.fed_scan = 1 if fed_scan == "device" else 0

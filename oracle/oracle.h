@@ -149,6 +149,11 @@ void fedLoop(const ES& es, const uint8_t* raw, size_t n, Words& w, bool formatte
              const Caps& caps = Caps());
 // SiPixelRawToClusterGPUKernel::makeClusters (SiPixelRawToClusterGPUKernel.cc:509-600)
 void makeClusters(const ES& es, const Words& w, Digis& d, Clusters& c, const Caps& caps = Caps());
+// countModules, findClus, clusterChargeCut and fillHitsModuleStart on the
+// digis d (xx, yy, calibrated adc, moduleInd; nDigis) -- the second half of
+// makeClusters (gpuClustering.h:19-273, gpuClusterChargeCut.h:14-114,
+// SiPixelRawToClusterGPUKernel.cc:464-506); sets d.clus and d.nModules
+void clusterDigis(Digis& d, Clusters& c, const Caps& caps = Caps());
 // PixelRecHitGPUKernel::makeHits (plugin-SiPixelRecHits/PixelRecHits.cc:33-53)
 void makeHits(const ES& es, const Digis& d, const Clusters& c, Hits& h, const Caps& caps = Caps());
 // the CA module's configurable switches (CAHitNtupletGeneratorOnGPU.cc:46-58,

@@ -158,6 +158,10 @@ class Oracle(_Named):
             raise RuntimeError("oracle fit failed")
         return out
 
+    def cluster_digis(self, module_ind, xx, yy, adc):
+        """countModules, findClus and clusterChargeCut on given digis (calibrated charges)."""
+        return _cluster_digis(self.lib.or_cluster_digis, module_ind, xx, yy, adc)
+
     def vertices(self, tupleOff, quality, pt, state, cov):
         """The serial vertex finder on a given track SoA (n tuples)."""
         n = len(quality)
@@ -186,6 +190,24 @@ class Oracle(_Named):
 
 
 REF_LIB = os.path.join(HERE, "_ref", "libpixref.so")
+
+
+def _cluster_digis(fn, module_ind, xx, yy, adc):
+    """or_cluster_digis on host arrays; returns a dict of arrays."""
+    n = len(module_ind)
+    arrs = [np.ascontiguousarray(a, dtype=np.uint16) for a in (module_ind, xx, yy, adc)]
+    out = {"moduleInd": np.zeros(n, np.uint16), "clus": np.zeros(n, np.int32),
+           "clusInModule": np.zeros(2000, np.uint32), "moduleId": np.zeros(2000, np.uint32),
+           "moduleStart": np.zeros(2001, np.uint32)}
+    nm = ctypes.c_uint32()
+    fn.argtypes = [ctypes.c_uint32] + [ctypes.c_void_p] * 10
+    rc = fn(n, *[a.ctypes.data for a in arrs],
+            *[out[k].ctypes.data for k in ("moduleInd", "clus", "clusInModule", "moduleId", "moduleStart")],
+            ctypes.byref(nm))
+    if rc != 0:
+        raise RuntimeError("oracle: clustering undefined for these digis")
+    out["nModules"] = nm.value
+    return out
 
 
 def ref_available():

@@ -310,6 +310,35 @@ int or_fit_riemann(int N, uint32_t n, const double* hits, const float* ge, doubl
   return 0;
 }
 
+// Clustering of given digis (module index, row, column, calibrated charge):
+// moduleIndOut/clus per digi, clusInModule/moduleId per module (2000),
+// moduleStart (2001), the module-run count; -1 where the reference's result
+// is undefined (a module's digis in two runs).
+int or_cluster_digis(uint32_t n, const uint16_t* moduleInd, const uint16_t* xx, const uint16_t* yy,
+                     const uint16_t* adc, uint16_t* moduleIndOut, int32_t* clus, uint32_t* clusInModule,
+                     uint32_t* moduleId, uint32_t* moduleStart, uint32_t* nModules) {
+  oracle::Digis d;
+  oracle::Clusters c;
+  d.nDigis = n;
+  d.xx.assign(xx, xx + n);
+  d.yy.assign(yy, yy + n);
+  d.adc.assign(adc, adc + n);
+  d.moduleInd.assign(moduleInd, moduleInd + n);
+  d.clus.assign(n, 0);
+  try {
+    oracle::clusterDigis(d, c);
+  } catch (std::exception&) {
+    return -1;
+  }
+  std::copy(d.moduleInd.begin(), d.moduleInd.end(), moduleIndOut);
+  std::copy(d.clus.begin(), d.clus.end(), clus);
+  std::copy(c.clusInModule.begin(), c.clusInModule.end(), clusInModule);
+  std::copy(c.moduleId.begin(), c.moduleId.end(), moduleId);
+  std::copy(c.moduleStart.begin(), c.moduleStart.end(), moduleStart);
+  *nModules = d.nModules;
+  return 0;
+}
+
 // Vertexing of a given track SoA (n tuples): tuple_off[n+1], quality[n],
 // pt[n], state[n*5], cov[n*15]; outputs idv[n], zv/wv/chi2/ptv2/ndof/sortInd
 // (1024 each) and the vertex count.  Test infrastructure for the vertex

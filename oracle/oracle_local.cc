@@ -375,10 +375,7 @@ void makeClusters(const ES& es, const Words& w, Digis& d, Clusters& c, const Cap
   d.pdigi.assign(nW, 0);
   d.rawIdArr.assign(nW, 0);
   d.errors.clear();
-  c.moduleStart.assign(PF_MAX_MODULES + 1, 0);
-  c.clusInModule.assign(PF_MAX_MODULES, 0);
-  c.moduleId.assign(PF_MAX_MODULES, 0);
-  c.clusModuleStart.assign(PF_MAX_MODULES + 1, 0);
+
 
   // ---- RawToDigi_kernel (:342-462), useQualityInfo = includeErrors = true
   for (uint32_t i = 0; i < nW; ++i) {
@@ -470,6 +467,15 @@ void makeClusters(const ES& es, const Words& w, Digis& d, Clusters& c, const Cap
     }
   }
 
+  clusterDigis(d, c, caps);
+}
+
+void clusterDigis(Digis& d, Clusters& c, const Caps& caps) {
+  const uint32_t nW = d.nDigis;
+  c.moduleStart.assign(PF_MAX_MODULES + 1, 0);
+  c.clusInModule.assign(PF_MAX_MODULES, 0);
+  c.moduleId.assign(PF_MAX_MODULES, 0);
+  c.clusModuleStart.assign(PF_MAX_MODULES + 1, 0);
   // ---- countModules (gpuClustering.h:19-37)
   std::vector<uint32_t>& ms = c.moduleStart;
   for (uint32_t i = 0; i < nW; ++i) {

@@ -116,6 +116,7 @@ BASE_SEED = 20261203
 BENCH_SEED_BASE = BASE_SEED + 100000
 BENCH_MODEL = "calibrated"
 # pg_flag bits (include/pixgpu.h)
+PG_FLAG_MODULE_TOO_BIG = 1 << 0
 PG_FLAG_TUPLE_OVERFLOW = 1 << 5
 PG_FLAG_CELL_OVERFLOW = 1 << 6
 PG_FLAG_TOO_MANY_WORDS = 1 << 9
@@ -721,6 +722,24 @@ class Chain:
         torch.cuda.synchronize()
         return {"state": st.cpu().numpy(), "cov": cv.cpu().numpy(), "pt": pt.cpu().numpy(), "eta": eta.cpu().numpy(),
                 "chi2": chi2.cpu().numpy()}
+
+    def cluster_digis(self, module_ind, xx, yy, adc):
+        """pg_cluster_digis: countModules, findClus and clusterChargeCut on given digis
+        (module index, row, column, calibrated charge); returns a dict of arrays."""
+        lib = gpu_lib()
+        n = len(module_ind)
+        arrs = [np.ascontiguousarray(a, dtype=np.uint16) for a in (module_ind, xx, yy, adc)]
+        out = {"moduleInd": np.zeros(n, np.uint16), "clus": np.zeros(n, np.int32),
+               "clusInModule": np.zeros(2000, np.uint32), "moduleId": np.zeros(2000, np.uint32),
+               "moduleStart": np.zeros(2001, np.uint32)}
+        nm, fl = ctypes.c_uint32(), ctypes.c_uint32()
+        lib.pg_cluster_digis.argtypes = [ctypes.c_void_p, ctypes.c_uint32] + [ctypes.c_void_p] * 11
+        self._check(lib.pg_cluster_digis(self._h, n, *[a.ctypes.data for a in arrs],
+                                         *[out[k].ctypes.data for k in ("moduleInd", "clus", "clusInModule",
+                                                                        "moduleId", "moduleStart")],
+                                         ctypes.byref(nm), ctypes.byref(fl)), "pg_cluster_digis")
+        out["nModules"], out["flags"] = nm.value, fl.value
+        return out
 
     def slot_bytes(self):
         """Device bytes of one batch slot (pg_slot_bytes)."""

@@ -29,6 +29,8 @@ def main():
     p.add_argument("--repeat", type=int, default=3)
     p.add_argument("--slots", type=int, default=1)
     p.add_argument("--seed", type=int, default=pixgpu.BASE_SEED + 1000)
+    p.add_argument("--model", choices=["calibrated", "dense"], default="calibrated",
+                   help="event model of the generator (pixgpu.Detector.event)")
     p.add_argument("--no-graphs", action="store_true")
     p.add_argument("--probe", action="store_true", help="per-kernel device times of a batch")
     p.add_argument("--fed-scan", choices=["host", "device"], default="host",
@@ -40,7 +42,7 @@ def main():
     a = p.parse_args()
     det = pixgpu.Detector()
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
-        raws = list(ex.map(lambda k: det.event(a.seed + k, a.pu), range(a.events)))
+        raws = list(ex.map(lambda k: det.event(a.seed + k, a.pu, model=a.model), range(a.events)))
     words = [len(r) // 4 for r in raws]
     device_scan = a.fed_scan == "device"
     chain = pixgpu.Chain(det.es, max_events=a.batch, max_words_per_batch=max(words) * a.batch + 1024, slots=a.slots,

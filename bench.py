@@ -605,7 +605,7 @@ def run_ours(a):
             load_tuning(sc)
             sc.prepare(a.serve_batch)
             best_ok = None
-            for frac in (0.2, 0.35, 0.5, 0.65, 0.8, 0.9):
+            for frac in (0.2, 0.35, 0.5, 0.6, 0.65, 0.7, 0.75, 0.8, 0.9):
                 rate = frac * value
                 st, lat = sc.serve(raws, a.serve, rate_hz=rate, max_batch=a.serve_batch, seed=11, upload_threads=4)
                 pt = {"offered_hz": st["offered_hz"], "events_per_s": st["events_per_s"], "p50_ms": st["p50_ms"],

@@ -57,7 +57,9 @@ enum pg_status {
    where the reference's behaviour is undefined or its truncation order is not
    reproduced exactly */
 enum pg_flag {
-  PG_FLAG_MODULE_TOO_BIG = 1u << 0,    /* > 4000 pixels in a module */
+  PG_FLAG_MODULE_TOO_BIG = 1u << 0,    /* a module of > 4000 pixels or > 1024 clusters (clustered on its
+                                          first 4000 pixels / its first 1024 clusters kept, as the
+                                          reference's serial build does) */
   PG_FLAG_EDGE_OVERFLOW = 1u << 1,     /* more CA links than the edge capacity */
   PG_FLAG_NBR_POOL_OVERFLOW = 1u << 2, /* more cells with neighbours than the list pool */
   PG_FLAG_TRK_POOL_OVERFLOW = 1u << 3, /* more cells with tracks than the list pool */

@@ -600,6 +600,10 @@ void clusterDigis(Digis& d, Clusters& c, const Caps& caps) {
     for (uint32_t i = firstPixel; i < nW; ++i) {
       if (d.moduleInd[i] == kInvId) continue;
       if (d.moduleInd[i] != thisModuleId) break;
+      // a pixel past the 4000-pixel cap of a module of at most 1024 clusters
+      // still holds its initial index: the reference sums past its array
+      if (uint32_t(d.clus[i]) >= nclus)
+        throw std::runtime_error("undefined in the reference: a pixel beyond a module's 4000-pixel cap");
       charge[d.clus[i]] += d.adc[i];
     }
     int chargeCut = thisModuleId < 96 ? 2000 : 4000;

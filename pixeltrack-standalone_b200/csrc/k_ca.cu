@@ -1064,6 +1064,34 @@ __global__ void kFastDupInDegree(Workspace ws, uint32_t* indeg, const uint32_t* 
 // barriers; the two worklist counters live in the shared memory of rank 0.
 constexpr int kFastDupThreads = 1024;
 constexpr uint32_t kFastDupCtas = 8;
+constexpr uint32_t kFastDupStage = 4096;  // worklist entries a CTA stages per round in shared memory
+
+// Appends of one round to the next worklist: each CTA stages its entries in
+// its own shared memory (local atomics), then reserves their place in the
+// worklist with one atomic on rank 0's counter (distributed shared memory)
+// and copies them.  Entries beyond the staging capacity are appended directly.
+struct WorklistStage {
+  uint32_t n;
+  uint32_t base;
+  uint32_t item[kFastDupStage];
+};
+__device__ __forceinline__ void stagePush(WorklistStage& st, uint32_t* remoteCount, uint32_t* list, uint32_t v) {
+  const uint32_t p = atomicAdd(&st.n, 1u);
+  if (p < kFastDupStage)
+    st.item[p] = v;
+  else
+    list[atomicAdd(remoteCount, 1u)] = v;
+}
+// called by every thread of the CTA; leaves st.n at zero
+__device__ __forceinline__ void stageFlush(WorklistStage& st, uint32_t* remoteCount, uint32_t* list) {
+  __syncthreads();
+  const uint32_t m = min(st.n, kFastDupStage);
+  if (threadIdx.x == 0) st.base = m ? atomicAdd(remoteCount, m) : 0u;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) list[st.base + i] = st.item[i];
+  __syncthreads();
+  if (threadIdx.x == 0) st.n = 0;
+}
 __global__ void __launch_bounds__(kFastDupThreads)
     kFastDupRounds(Workspace ws, uint32_t* indeg, uint32_t* lists, const uint32_t* candFlag, const uint32_t* candOff) {
   namespace cg = cooperative_groups;
@@ -1084,10 +1112,13 @@ __global__ void __launch_bounds__(kFastDupThreads)
   uint8_t* q = ws.quality + size_t(e) * ws.cap.tuples;
   const float* tip = ws.state + size_t(e) * ws.cap.tuples * 5 + 1;
   const uint32_t gtid = r * blockDim.x + threadIdx.x, gstride = P * blockDim.x;
+  __shared__ WorklistStage st;
   if (r == 0 && threadIdx.x < 2) sN[threadIdx.x] = 0;
+  if (threadIdx.x == 0) st.n = 0;
   cl.sync();
   for (uint32_t k = gtid; k < nc; k += gstride)
-    if (deg[k] == 0) L[0][atomicAdd(&N[0], 1u)] = k;
+    if (deg[k] == 0) stagePush(st, &N[0], L[0], k);
+  stageFlush(st, &N[0], L[0]);
   cl.sync();
   int cur = 0;
   for (;;) {
@@ -1124,11 +1155,12 @@ __global__ void __launch_bounds__(kFastDupThreads)
           const uint32_t o = tcell[4 * t + qq];
           if (o > cell && flag[o] && inTrkList(off, trk, o, t)) {
             const uint32_t ko = cidx[o];
-            if (atomicSub(&deg[ko], 1u) == 1u) Ln[atomicAdd(&N[cur ^ 1], 1u)] = ko;
+            if (atomicSub(&deg[ko], 1u) == 1u) stagePush(st, &N[cur ^ 1], Ln, ko);
           }
         }
       }
     }
+    stageFlush(st, &N[cur ^ 1], Ln);
     cur ^= 1;
     // the round's quality writes and the next worklist are complete
     cl.sync();

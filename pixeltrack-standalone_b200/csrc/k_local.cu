@@ -187,6 +187,10 @@ __global__ void kInitEvents(Workspace ws, uint32_t nEvents) {
     c->nearDoublet = c->nearCA = c->nearQuality = 0;
     c->flags = c->nWords > ws.cap.fedWords ? kFlagTooManyWords : 0u;
   }
+  // the module-run start bitmap of kModuleBoundaries (in scratchA, free until the doublets)
+  uint32_t* bm = ws.scratchA + size_t(e) * ws.cap.scratch;
+  const uint32_t nbw = (min(ws.wordOffsets[e + 1] - ws.wordOffsets[e], ws.cap.fedWords) + 31) / 32;
+  for (uint32_t i = threadIdx.x; i < nbw; i += blockDim.x) bm[i] = 0;
   uint32_t* cim = ws.clusInModule + size_t(e) * kModStride;
   for (uint32_t i = threadIdx.x; i < kModStride; i += blockDim.x) {
     cim[i] = 0;
@@ -333,7 +337,8 @@ __global__ void kRawToDigi(DeviceES es, Workspace ws, uint32_t nEvents) {
   }
 }
 
-// module-run boundaries (countModules), appended unordered then sorted per event
+// module-run boundaries (countModules): each run start is marked in a bitmap
+// of the event's digis, which kSortModules reads in order
 __global__ void kModuleBoundaries(Workspace ws, uint32_t nEvents) {
   const uint32_t total = ws.wordOffsets[nEvents];
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
@@ -344,40 +349,48 @@ __global__ void kModuleBoundaries(Workspace ws, uint32_t nEvents) {
     int j = int(g) - 1;
     while (j >= int(start) && ws.moduleInd[j] == kInvId) --j;
     if (j < int(start) || ws.moduleInd[j] != id) {
-      uint32_t loc = atomicAdd(&ws.ev[e].nModules, 1u);
-      if (loc < kMaxModules) ws.moduleStart[size_t(e) * kModStride + 1 + loc] = g - start;
+      const uint32_t i = g - start;
+      if (i < ws.cap.fedWords) atomicOr(&ws.scratchA[size_t(e) * ws.cap.scratch + (i >> 5)], 1u << (i & 31));
     }
   }
 }
 
-// sort the module-run starts of each event (<= 2000) ascending, bitonic in shared memory
+// the module-run starts of each event (<= 2000) in ascending order, from the boundary bitmap
 __global__ void kSortModules(Workspace ws, uint32_t nEvents) {
   __shared__ uint32_t s[2048];
+  __shared__ uint32_t scanShMod[33];
+  __shared__ uint32_t sTmp[2048];
+  __shared__ uint32_t sRuns;
   uint32_t e = blockIdx.x;
   EventCounters* c = ws.ev + e;
-  uint32_t n = c->nModules;
-  if (n > kMaxModules) {
-    n = kMaxModules;
-  }
   uint32_t* ms = ws.moduleStart + size_t(e) * kModStride;
-  for (uint32_t i = threadIdx.x; i < 2048; i += blockDim.x) s[i] = i < n ? ms[1 + i] : 0xffffffffu;
-  __syncthreads();
-  for (uint32_t k = 2; k <= 2048; k <<= 1) {
-    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-      for (uint32_t i = threadIdx.x; i < 2048; i += blockDim.x) {
-        uint32_t ixj = i ^ j;
-        if (ixj > i) {
-          bool up = (i & k) == 0;
-          uint32_t a = s[i], b = s[ixj];
-          if ((a > b) == up) {
-            s[i] = b;
-            s[ixj] = a;
-          }
-        }
+  // the run starts in position order: each thread takes a contiguous chunk
+  // of the bitmap, a block scan of the chunks' bit counts places them
+  {
+    const uint32_t* bm = ws.scratchA + size_t(e) * ws.cap.scratch;
+    const uint32_t nbw = (min(c->nWords, ws.cap.fedWords) + 31) / 32;
+    const uint32_t chunk = (nbw + blockDim.x - 1) / blockDim.x;
+    const uint32_t w0 = min(nbw, threadIdx.x * chunk), w1 = min(nbw, w0 + chunk);
+    uint32_t mine = 0;
+    for (uint32_t w = w0; w < w1; ++w) mine += __popc(bm[w]);
+    uint32_t tot;
+    uint32_t at = blockExclusiveScan(mine, scanShMod, &tot);
+    for (uint32_t w = w0; w < w1; ++w) {
+      uint32_t bits = bm[w];
+      while (bits) {
+        const uint32_t b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        if (at < kMaxModules) s[at] = 32 * w + b;
+        ++at;
       }
-      __syncthreads();
     }
+    if (threadIdx.x == 0) sRuns = tot;
+    __syncthreads();
   }
+  // more than 2000 runs: the reference's counter stops at its capacity
+  // (gpuClustering.h:33); the first 2000 in position order are kept, flagged
+  if (threadIdx.x == 0) c->nModules = sRuns;
+  uint32_t n = min(sRuns, kMaxModules);
   // A module whose digis come in more than one run (only in corrupted data:
   // a module is read out in one block per link) is clustered run by run by the
   // reference, whose serial build then overwrites the module's cluster count
@@ -420,25 +433,20 @@ __global__ void kSortModules(Workspace ws, uint32_t nEvents) {
       }
     }
     __syncthreads();
-    // drop the later runs from the list (their starts sort past the kept ones)
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
-      if (sDrop[i]) s[i] = 0xffffffffu;
-    __syncthreads();
-    for (uint32_t k = 2; k <= 2048; k <<= 1) {
-      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-        for (uint32_t i = threadIdx.x; i < 2048; i += blockDim.x) {
-          uint32_t ixj = i ^ j;
-          if (ixj > i) {
-            bool up = (i & k) == 0;
-            uint32_t a = s[i], b = s[ixj];
-            if ((a > b) == up) {
-              s[i] = b;
-              s[ixj] = a;
-            }
-          }
-        }
-        __syncthreads();
+    // drop the later runs from the list, keeping the others in order
+    {
+      uint32_t carry = 0;
+      for (uint32_t i0 = 0; i0 < n; i0 += blockDim.x) {
+        const uint32_t i = i0 + threadIdx.x;
+        const uint32_t keep = (i < n && !sDrop[i]) ? 1u : 0u;
+        uint32_t tot;
+        const uint32_t pre = blockExclusiveScan(keep, scanShMod, &tot);
+        if (keep) sTmp[carry + pre] = s[i];
+        carry += tot;
       }
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < carry; i += blockDim.x) s[i] = sTmp[i];
+      __syncthreads();
     }
   }
   const uint32_t kept = n - sNDrop;
@@ -480,6 +488,7 @@ __device__ void clusterModuleBlock(const Workspace& ws, uint32_t e, uint32_t mod
     if (threadIdx.x == 0) ws.moduleId[size_t(e) * kModStride + module] = 0xffffffffu;
     return;
   }
+  const uint32_t moduleEnd = msize;  // the run's end before the 4000-pixel cap
   if (msize - firstPixel > PF_MAX_PIX_IN_MODULE) {
     if (threadIdx.x == 0) atomicOr(&ws.ev[e].flags, kFlagModuleTooBig);
     msize = firstPixel + PF_MAX_PIX_IN_MODULE;
@@ -642,6 +651,17 @@ __device__ void clusterModuleBlock(const Workspace& ws, uint32_t e, uint32_t mod
       }
     }
   }
+  // pixels past the 4000-pixel cap kept their initial index (countModules);
+  // the cluster-count cap then invalidates them, as it does every index of
+  // 1024 and above (gpuClusterChargeCut.h:46-59).  (With at most 1024
+  // clusters the reference's charge sums index past their array: undefined,
+  // flagged, left as is.)
+  if (found > uint32_t(PF_MAX_CLUS_PER_MODULE))
+    for (uint32_t g = firstPixel + np + threadIdx.x; g < moduleEnd; g += blockDim.x)
+      if (ws.moduleInd[start + g] == thisModuleId) {
+        ws.moduleInd[start + g] = kInvId;
+        ws.clus[start + g] = kInvId;
+      }
   if (threadIdx.x == 0) {
     ws.clusInModule[size_t(e) * kModStride + thisModuleId] = (found == 0 || allGood) ? found : newTotal;
     ws.moduleId[size_t(e) * kModStride + module] = thisModuleId;

@@ -71,7 +71,7 @@ constexpr size_t kVtxScratchBWords = size_t(kMaxVtxTracks);
 // flag bits in EventCounters::flags (capacity conditions where the result no
 // longer follows the reference's truncation order exactly)
 enum : uint32_t {
-  kFlagModuleTooBig = 1u << 0,      // > 4000 pixels in a module (reference behaviour undefined)
+  kFlagModuleTooBig = 1u << 0,      // > 4000 pixels or > 1024 clusters in a module (truncated as the serial build)
   kFlagEdgeOverflow = 1u << 1,      // more CA links than cap.edges
   kFlagNbrPoolOverflow = 1u << 2,   // more cells with neighbours than the 65535-list pool
   kFlagTrkPoolOverflow = 1u << 3,   // more cells with tracks than the 65535-list pool

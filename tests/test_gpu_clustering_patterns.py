@@ -65,4 +65,4 @@ def test_module_capacity_edges(chain, default_detector, n):
     assert len(set(got["clus"][kept].tolist())) == 1024
     assert got["clusInModule"][300] == min(n, 4000)
     assert got["clusInModule"][120] == 30 and got["clusInModule"][500] == 40
-    assert bool(got["flags"] & pixgpu.PG_FLAG_MODULE_TOO_BIG) == (n > 4000)
+    assert got["flags"] & pixgpu.PG_FLAG_MODULE_TOO_BIG  # both caps are reported

@@ -832,6 +832,12 @@ __device__ __forceinline__ uint32_t tupleCellCount(const uint32_t* tcell, uint32
   return n;
 }
 
+// the four cell slots of tuple t in one load (the slots of a tuple are 16
+// bytes, 16-byte aligned); the cells are the slots before the first 0xffffffff
+__device__ __forceinline__ uint4 tupleCellSlots(const uint32_t* tcell, uint32_t t) {
+  return *reinterpret_cast<const uint4*>(tcell + 4 * size_t(t));
+}
+
 // cell -> track lists: count, (scan), fill, order
 __global__ void kTrackCount(Workspace ws) {
   uint32_t e = blockIdx.y;
@@ -1038,20 +1044,23 @@ __global__ void kFastDupInDegree(Workspace ws, uint32_t* indeg, const uint32_t* 
   const uint32_t* trk = ws.trk + size_t(e) * ws.cap.tupleCells();
   const uint32_t* tcell = ws.tupleCells + size_t(e) * ws.cap.tupleCells();
   const uint32_t* flag = candFlag + size_t(e) * (ws.cap.cells + 1);
-  uint32_t* deg = indeg + size_t(e) * ws.cap.cells;
+  uint32_t* deg = indeg + size_t(e) * ws.cap.cells;  // by cell
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x) {
     uint32_t cell = cand[k];
     uint32_t b = off[cell], s = trkListSize(off, cell);
     uint32_t d = 0;
     for (uint32_t j = 0; j < s; ++j) {
-      uint32_t t = trk[b + j];
-      uint32_t ncell = tupleCellCount(tcell, t);
-      for (uint32_t q = 0; q < ncell; ++q) {
-        uint32_t o = tcell[4 * t + q];
+      const uint32_t t = trk[b + j];
+      const uint4 tc = tupleCellSlots(tcell, t);
+      const uint32_t cs[4] = {tc.x, tc.y, tc.z, tc.w};
+#pragma unroll
+      for (uint32_t q = 0; q < 4; ++q) {
+        const uint32_t o = cs[q];
+        if (o == 0xffffffffu) break;
         if (o < cell && flag[o] && inTrkList(off, trk, o, t)) ++d;
       }
     }
-    deg[k] = d;
+    deg[cell] = d;
   }
 }
 
@@ -1065,6 +1074,8 @@ __global__ void kFastDupInDegree(Workspace ws, uint32_t* indeg, const uint32_t* 
 constexpr int kFastDupThreads = 1024;
 constexpr uint32_t kFastDupCtas = 8;
 constexpr uint32_t kFastDupStage = 4096;  // worklist entries a CTA stages per round in shared memory
+constexpr uint32_t kDupGroup = 4;         // lanes per candidate in a round
+constexpr uint32_t kDupGroupsPerWarp = 32 / kDupGroup;
 
 // Appends of one round to the next worklist: each CTA stages its entries in
 // its own shared memory (local atomics), then reserves their place in the
@@ -1093,7 +1104,7 @@ __device__ __forceinline__ void stageFlush(WorklistStage& st, uint32_t* remoteCo
   if (threadIdx.x == 0) st.n = 0;
 }
 __global__ void __launch_bounds__(kFastDupThreads)
-    kFastDupRounds(Workspace ws, uint32_t* indeg, uint32_t* lists, const uint32_t* candFlag, const uint32_t* candOff) {
+    kFastDupRounds(Workspace ws, uint32_t* indeg, uint32_t* lists, const uint32_t* candFlag) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   const uint32_t r = cl.block_rank(), P = cl.num_blocks();
@@ -1106,19 +1117,23 @@ __global__ void __launch_bounds__(kFastDupThreads)
   const uint32_t* trk = ws.trk + size_t(e) * ws.cap.tupleCells();
   const uint32_t* tcell = ws.tupleCells + size_t(e) * ws.cap.tupleCells();
   const uint32_t* flag = candFlag + size_t(e) * (ws.cap.cells + 1);
-  const uint32_t* cidx = candOff + size_t(e) * (ws.cap.cells + 1);
-  uint32_t* deg = indeg + size_t(e) * ws.cap.cells;
-  uint32_t* L[2] = {lists + size_t(e) * ws.cap.scratch, lists + size_t(e) * ws.cap.scratch + ws.cap.cells};
+  uint32_t* deg = indeg + size_t(e) * ws.cap.cells;  // by cell
+  uint32_t* const L0 = lists + size_t(e) * ws.cap.scratch;  // worklists: L0 and L0 + cap.cells
+  auto L = [&](int w) { return L0 + (w ? ws.cap.cells : 0u); };
   uint8_t* q = ws.quality + size_t(e) * ws.cap.tuples;
   const float* tip = ws.state + size_t(e) * ws.cap.tuples * 5 + 1;
   const uint32_t gtid = r * blockDim.x + threadIdx.x, gstride = P * blockDim.x;
+  const uint32_t gwarp = gtid >> 5, nwarps = gstride >> 5;
+  const uint32_t sub = (threadIdx.x & 31) / kDupGroup, gl = threadIdx.x % kDupGroup;
   __shared__ WorklistStage st;
   if (r == 0 && threadIdx.x < 2) sN[threadIdx.x] = 0;
   if (threadIdx.x == 0) st.n = 0;
   cl.sync();
-  for (uint32_t k = gtid; k < nc; k += gstride)
-    if (deg[k] == 0) stagePush(st, &N[0], L[0], k);
-  stageFlush(st, &N[0], L[0]);
+  for (uint32_t k = gtid; k < nc; k += gstride) {
+    const uint32_t cell = cand[k];
+    if (deg[cell] == 0) stagePush(st, &N[0], L(0), cell);
+  }
+  stageFlush(st, &N[0], L(0));
   cl.sync();
   int cur = 0;
   for (;;) {
@@ -1128,35 +1143,54 @@ __global__ void __launch_bounds__(kFastDupThreads)
     cl.sync();
     if (n == 0) break;
     if (r == 0 && threadIdx.x == 0) N[cur] = 0;
-    const uint32_t* Lc = L[cur];
-    uint32_t* Ln = L[cur ^ 1];
-    for (uint32_t i = gtid; i < n; i += gstride) {
-      const uint32_t cell = cand[Lc[i]];
-      const uint32_t b = off[cell], s = trkListSize(off, cell);
-      float mc = 10000.f;
-      uint32_t im = kNoTuple;
-      for (uint32_t j = 0; j < s; ++j) {
-        const uint32_t t = trk[b + j];
-        const float score = fabsf(tip[size_t(t) * 5]);
-        if (q[t] == kLoose && score < mc) {
-          mc = score;
-          im = t;
+    const uint32_t* Lc = L(cur);
+    uint32_t* Ln = L(cur ^ 1);
+    // kDupGroup lanes per candidate: the lanes of a group split the cell's
+    // track list, so an item costs a few dependent loads whatever its size;
+    // the warp's trip counts are uniform for the shuffles
+    for (uint32_t i0 = gwarp * kDupGroupsPerWarp; i0 < n; i0 += nwarps * kDupGroupsPerWarp) {
+      const uint32_t i = i0 + sub;
+      uint32_t cell = 0, b = 0, s = 0;
+      if (i < n) {
+        cell = Lc[i];
+        b = off[cell];
+        s = trkListSize(off, cell);
+      }
+      const uint32_t sMax = __reduce_max_sync(0xffffffffu, s);
+      // the serial loop's choice: the first loose track of minimal |tip|
+      // below 10000 (key: score bits, then list position)
+      unsigned long long best = ~0ull;
+      for (uint32_t j0 = 0; j0 < sMax; j0 += kDupGroup) {
+        const uint32_t j = j0 + gl;
+        if (j < s) {
+          const uint32_t t = trk[b + j];
+          const float score = fabsf(tip[size_t(t) * 5]);
+          if (q[t] == kLoose && score < 10000.f) {
+            const unsigned long long key = (uint64_t(__float_as_uint(score)) << 32) | j;
+            best = key < best ? key : best;
+          }
         }
       }
-      for (uint32_t j = 0; j < s; ++j) {
+#pragma unroll
+      for (uint32_t o = 1; o < kDupGroup; o <<= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
+        best = other < best ? other : best;
+      }
+      const uint32_t im = (i < n && best != ~0ull) ? trk[b + uint32_t(best & 0xffffffffu)] : kNoTuple;
+      for (uint32_t j0 = 0; j0 < sMax; j0 += kDupGroup) {
+        const uint32_t j = j0 + gl;
+        if (j >= s) continue;
         const uint32_t t = trk[b + j];
         if (q[t] != kBad && t != im) q[t] = kDup;
-      }
-      // release later candidates sharing a track
-      for (uint32_t j = 0; j < s; ++j) {
-        const uint32_t t = trk[b + j];
-        const uint32_t ncell = tupleCellCount(tcell, t);
-        for (uint32_t qq = 0; qq < ncell; ++qq) {
-          const uint32_t o = tcell[4 * t + qq];
-          if (o > cell && flag[o] && inTrkList(off, trk, o, t)) {
-            const uint32_t ko = cidx[o];
-            if (atomicSub(&deg[ko], 1u) == 1u) stagePush(st, &N[cur ^ 1], Ln, ko);
-          }
+        // release later candidates sharing the track
+        const uint4 tc = tupleCellSlots(tcell, t);
+        const uint32_t cs[4] = {tc.x, tc.y, tc.z, tc.w};
+#pragma unroll
+        for (uint32_t qq = 0; qq < 4; ++qq) {
+          const uint32_t o = cs[qq];
+          if (o == 0xffffffffu) break;
+          if (o > cell && flag[o] && inTrkList(off, trk, o, t) && atomicSub(&deg[o], 1u) == 1u)
+            stagePush(st, &N[cur ^ 1], Ln, o);
         }
       }
     }
@@ -1323,15 +1357,13 @@ cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   if (ws.ca.lateFishbone) PG_PROBED("kFishboneCleaner", stream, kFishboneCleaner<<<g, 256, 0, stream>>>(ws));
   // fastDuplicateRemover (candFlag survives in startTupleCount from runCA)
   uint32_t* candFlag = ws.startTupleCount;
-  uint32_t* candOff = ws.startHitCount;  // candidate index of each cell, from runCA
   uint32_t* indeg = ws.scratchA;        // [maxEvents][cap.scratch], cap.cells per event used
   uint32_t* lists = ws.scratchB;        // two worklists of cap.cells per event (cap.scratch >= 2 cap.cells)
   PG_PROBED("kFastDupInDegree", stream, kFastDupInDegree<<<dim3(tunedGrid(ws, kTuneFastDupInDegree, gx), nEvents), 256, 0, stream>>>(ws, indeg, candFlag));
   const uint32_t P = nEvents <= kClusterMaxEvents ? kFastDupCtas : 2;
   cudaError_t le = cudaSuccess;
   PG_PROBED("kFastDupRounds", stream,
-            le = launchClustered(kFastDupRounds, P, nEvents, kFastDupThreads, 0, stream, ws, indeg, lists, candFlag,
-                                 candOff));
+            le = launchClustered(kFastDupRounds, P, nEvents, kFastDupThreads, 0, stream, ws, indeg, lists, candFlag));
   if (le != cudaSuccess) return le;
   // hit -> tuple map and triplet cleaner
   PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, nullptr, 0));

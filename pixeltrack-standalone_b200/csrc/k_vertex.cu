@@ -112,12 +112,19 @@ __device__ void groupByVertex(const VtxScratch& s, uint32_t nt, uint32_t nv, uin
   for (uint32_t v = threadIdx.x >> 5; v < nv; v += nw) {
     uint32_t pos = vOff[v];
     const uint32_t end = vOff[v + 1];
-    for (uint32_t i0 = 0; i0 < nt && pos < end; i0 += 32) {
-      const uint32_t i = i0 + lane;
-      const bool in = i < nt && s.iv[i] == int32_t(v);
-      const uint32_t m = __ballot_sync(0xffffffffu, in);
-      if (in) s.list[pos + __popc(m & lanemaskLt())] = i;
-      pos += __popc(m);
+    for (uint32_t i0 = 0; i0 < nt && pos < end; i0 += 128) {
+      bool in[4];
+#pragma unroll
+      for (uint32_t u = 0; u < 4; ++u) {
+        const uint32_t i = i0 + u * 32 + lane;
+        in[u] = i < nt && s.iv[i] == int32_t(v);
+      }
+#pragma unroll
+      for (uint32_t u = 0; u < 4; ++u) {
+        const uint32_t m = __ballot_sync(0xffffffffu, in[u]);
+        if (in[u]) s.list[pos + __popc(m & lanemaskLt())] = i0 + u * 32 + lane;
+        pos += __popc(m);
+      }
     }
   }
   __syncthreads();
@@ -128,6 +135,16 @@ __device__ void groupByVertex(const VtxScratch& s, uint32_t nt, uint32_t nv, uin
 // once and every lane adds them in order from the shuffles.  Terms of tracks
 // that the serial loop skips are +0.0, which leaves a sum unchanged (a sum
 // that starts at +0.0 never becomes -0.0 under round-to-nearest).
+
+// sum + the 32 lanes' terms, added in lane order (every lane gets the sum).
+// All 32 terms are added: the lanes past the vertex's tracks hold +0.0, which
+// leaves the sum unchanged.  Unrolled, the shuffles issue back to back and
+// only the additions form the dependent chain.
+__device__ __forceinline__ float laneOrderSum(float sum, float t) {
+#pragma unroll
+  for (int l = 0; l < 32; ++l) sum += __shfl_sync(0xffffffffu, t, l);
+  return sum;
+}
 
 // fitVertices: weighted z, chi2 outlier rejection (iv = 9999), ndof and weight;
 // one warp per vertex
@@ -147,11 +164,8 @@ __device__ void fitVertices(const VtxScratch& s, uint32_t nt, uint32_t nv, float
         tz = s.zt[i] * wi;
         tw = wi;
       }
-      const uint32_t cnt = min(32u, n - k0);
-      for (uint32_t l = 0; l < cnt; ++l) {
-        z += __shfl_sync(0xffffffffu, tz, l);
-        w += __shfl_sync(0xffffffffu, tw, l);
-      }
+      z = laneOrderSum(z, tz);
+      w = laneOrderSum(w, tw);
     }
     z /= w;
     int32_t nd = -1;
@@ -172,8 +186,7 @@ __device__ void fitVertices(const VtxScratch& s, uint32_t nt, uint32_t nv, float
         }
       }
       nd += __popc(__ballot_sync(0xffffffffu, acc));
-      const uint32_t cnt = min(32u, n - k0);
-      for (uint32_t l = 0; l < cnt; ++l) c2s += __shfl_sync(0xffffffffu, t, l);
+      c2s = laneOrderSum(c2s, t);
     }
     if (nd > 0) w *= float(nd) / c2s;
     if (lane == 0) {
@@ -388,18 +401,28 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
     const uint32_t nh = toff[t + 1] - toff[t];
     return nh >= 4 && q[t] == 2 && !(pt[t] < 0.5f);
   };
-  // each thread takes a contiguous chunk of tuples: its selected tracks keep
-  // ascending order, one block scan places them, and the loads of a chunk
-  // are independent of each other
-  const uint32_t chunk = (guard + blockDim.x - 1) / blockDim.x;
-  const uint32_t t0 = min(guard, threadIdx.x * chunk), t1 = min(guard, t0 + chunk);
-  uint32_t mine = 0;
-  for (uint32_t t = t0; t < t1; ++t) {
-    if (rank == 0) idv[t] = -1;
-    mine += selected(t) ? 1u : 0u;
+  // each warp takes a contiguous range of tuples, 32 consecutive ones per
+  // step (coalesced loads); one block scan over the warps' counts places each
+  // warp's run, and a second walk writes its selected tracks in ascending
+  // order.  The selection of each step is kept as a bit when the range has at
+  // most 32 steps (up to 32768 tuples), else evaluated again.
+  const uint32_t warp = threadIdx.x >> 5;
+  const uint32_t R = (guard + nw * 32 - 1) / (nw * 32) * 32;
+  const uint32_t w0 = min(guard, warp * R), w1 = min(guard, w0 + R);
+  const bool keepBits = R <= 32 * 32;
+  uint32_t cnt = 0, bits = 0;
+  for (uint32_t k = 0; w0 + k * 32 < w1; ++k) {
+    const uint32_t t = w0 + k * 32 + lane;
+    bool sel = false;
+    if (t < w1) {
+      if (rank == 0) idv[t] = -1;
+      sel = selected(t);
+    }
+    if (sel && keepBits) bits |= 1u << k;
+    cnt += __popc(__ballot_sync(0xffffffffu, sel));
   }
   uint32_t total;
-  const uint32_t first = blockExclusiveScan(mine, scanSh, &total);
+  const uint32_t first = __shfl_sync(0xffffffffu, blockExclusiveScan(lane == 0 ? cnt : 0u, scanSh, &total), 0);
   if (threadIdx.x == 0) {
     sNt = min(total, kMaxVtxTracks);
     // beyond ZVertexSoA::MAXTRACKS the reference writes past its arrays
@@ -413,14 +436,19 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
   const bool active = split || rank == 0;
   const uint32_t wFirst = split ? rank * nw : 0, wStride = split ? P * nw : nw;
   if (active) {
-    uint32_t it = first;
-    for (uint32_t t = t0; t < t1 && it < kMaxVtxTracks; ++t) {
-      if (!selected(t)) continue;
-      s.itrk[it] = t;
-      s.zt[it] = st[size_t(t) * 5 + 4];
-      s.ezt2[it] = cov[size_t(t) * 15 + 14];
-      s.ptt2[it] = pt[t] * pt[t];
-      ++it;
+    uint32_t pos = first;
+    for (uint32_t k = 0; w0 + k * 32 < w1; ++k) {
+      const uint32_t t = w0 + k * 32 + lane;
+      const bool sel = keepBits ? ((bits >> k) & 1u) != 0 : (t < w1 && selected(t));
+      const uint32_t m = __ballot_sync(0xffffffffu, sel);
+      const uint32_t it = pos + __popc(m & lanemaskLt());
+      if (sel && it < kMaxVtxTracks) {
+        s.itrk[it] = t;
+        s.zt[it] = st[size_t(t) * 5 + 4];
+        s.ezt2[it] = cov[size_t(t) * 15 + 14];
+        s.ptt2[it] = pt[t] * pt[t];
+      }
+      pos += __popc(m);
     }
   }
   __syncthreads();
@@ -458,12 +486,20 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
   for (uint32_t b = threadIdx.x >> 5; b < 256; b += nw) {
     uint32_t pos = hoff[b];
     const uint32_t end = hoff[b + 1];
-    for (uint32_t r0 = 0; r0 < nt && pos < end; r0 += 32) {
-      const uint32_t r = r0 + lane;
-      const bool in = r < nt && s.izt[nt - 1 - r] == b;
-      const uint32_t m = __ballot_sync(0xffffffffu, in);
-      if (in) s.hbins[pos + __popc(m & lanemaskLt())] = uint16_t(nt - 1 - r);
-      pos += __popc(m);
+    // 128 tracks per step: the four loads issue together
+    for (uint32_t r0 = 0; r0 < nt && pos < end; r0 += 128) {
+      bool in[4];
+#pragma unroll
+      for (uint32_t u = 0; u < 4; ++u) {
+        const uint32_t r = r0 + u * 32 + lane;
+        in[u] = r < nt && s.izt[nt - 1 - r] == b;
+      }
+#pragma unroll
+      for (uint32_t u = 0; u < 4; ++u) {
+        const uint32_t m = __ballot_sync(0xffffffffu, in[u]);
+        if (in[u]) s.hbins[pos + __popc(m & lanemaskLt())] = uint16_t(nt - 1 - (r0 + u * 32 + lane));
+        pos += __popc(m);
+      }
     }
   }
   }
@@ -631,13 +667,10 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
             }
           }
         }
-        const uint32_t cnt = min(32u, n - k0);
-        for (uint32_t l = 0; l < cnt; ++l) {
-          znew[0] += __shfl_sync(0xffffffffu, z0, l);
-          wnew[0] += __shfl_sync(0xffffffffu, w0, l);
-          znew[1] += __shfl_sync(0xffffffffu, z1, l);
-          wnew[1] += __shfl_sync(0xffffffffu, w1, l);
-        }
+        znew[0] = laneOrderSum(znew[0], z0);
+        wnew[0] = laneOrderSum(wnew[0], w0);
+        znew[1] = laneOrderSum(znew[1], z1);
+        wnew[1] = laneOrderSum(wnew[1], w1);
       }
       znew[0] /= wnew[0];
       znew[1] /= wnew[1];
@@ -711,8 +744,7 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
         const uint32_t i = s.list[b + k];
         if (s.iv[i] <= 9990) t = s.ptt2[i];
       }
-      const uint32_t cnt = min(32u, n - k0);
-      for (uint32_t l = 0; l < cnt; ++l) p2 += __shfl_sync(0xffffffffu, t, l);
+      p2 = laneOrderSum(p2, t);
     }
     if (lane == 0) ptv2[v] = p2;
   }

@@ -273,7 +273,9 @@ constexpr uint32_t kNoTemp = 0xffffffffu;  // the slot's doublets did not fit it
 // equal share per warp: no atomics); the slot's staging
 // offset goes to scratchB.  A slot whose window could overflow the region is
 // only counted, and pass 2 tests its candidates again.
-__global__ void kDoubletCount(Workspace ws) {
+// (256, 4): 76 -> 64 registers, four blocks per SM instead of three; measured
+// A/B at 64 PU50 events per batch, three in flight: 671 -> 598 us, +1.5 % events/s
+__global__ void __launch_bounds__(256, 4) kDoubletCount(Workspace ws) {
   __shared__ PairTable pt;
   const uint32_t e = blockIdx.y;
   const EventCounters* c = ws.ev + e;

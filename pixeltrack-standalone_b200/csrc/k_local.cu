@@ -463,6 +463,7 @@ __global__ void kSortModules(Workspace ws, uint32_t nEvents) {
 constexpr int kClusThreads = 256;
 constexpr uint32_t kSmallPix = 128;  // modules up to this many pixels are clustered by one warp
 constexpr int kSmallWarps = 8;
+constexpr uint32_t kModCols = 416;  // pixel columns (y) of a module
 
 // findClus + clusterChargeCut of one module run by the whole block (modules
 // with more than kSmallPix pixels): column histogram, union-find with roots
@@ -678,13 +679,17 @@ __global__ void __launch_bounds__(kClusThreads) kFindClustersBig(Workspace ws) {
 }
 
 // One warp per module run.  Runs of at most kSmallPix pixels are clustered
-// here: neighbours (|dx| <= 1, |dy| <= 1) found by a direct pair scan,
-// union-find in shared memory, roots ranked by ascending pixel index, then
-// the charge cut with renumbering -- the same numbering as the block path.
-// Larger runs are queued for kFindClustersBig.
-__global__ void __launch_bounds__(kSmallWarps * 32) kFindClustersSmall(Workspace ws) {
+// here: the pixels binned by column (a counting sort in shared memory), each
+// pixel's neighbours (|dx| <= 1, |dy| <= 1) looked up in its own column and
+// the next, union-find in shared memory, roots ranked by ascending pixel
+// index, then the charge cut with renumbering -- the same numbering as the
+// block path.  Larger runs are queued for kFindClustersBig.
+// (256, 6): at most 40 registers, six blocks per SM beside their 28 KB of shared memory
+__global__ void __launch_bounds__(kSmallWarps * 32, 6) kFindClustersSmall(Workspace ws) {
   __shared__ uint16_t sxA[kSmallWarps][kSmallPix], syA[kSmallWarps][kSmallPix], rkA[kSmallWarps][kSmallPix];
   __shared__ int32_t labA[kSmallWarps][kSmallPix], chgA[kSmallWarps][kSmallPix];
+  __shared__ uint32_t colA[kSmallWarps][kModCols];  // column bins: counts, then bin ends
+  __shared__ uint8_t ordA[kSmallWarps][kSmallPix];  // pixels ordered by column
   const uint32_t e = blockIdx.y, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t module = blockIdx.x * kSmallWarps + w;
   EventCounters* c = ws.ev + e;
@@ -714,12 +719,24 @@ __global__ void __launch_bounds__(kSmallWarps * 32) kFindClustersSmall(Workspace
   int32_t* chg = chgA[w];
   uint16_t* gmid = ws.moduleInd + start + firstPixel;
   int32_t* gclus = ws.clus + start + firstPixel;
-  for (uint32_t k = lane; k < np; k += 32) {
-    const bool valid = gmid[k] != kInvId;
-    sx[k] = ws.xx[start + firstPixel + k];
-    sy[k] = valid ? ws.yy[start + firstPixel + k] : uint16_t(0xffff);
-    lab[k] = int32_t(k);
+  // a lane holds at most kSmallPix / 32 pixels: their charges stay in registers
+  int32_t adcR[kSmallPix / 32];
+  bool colOk = true;  // every valid pixel inside the module's columns
+#pragma unroll
+  for (uint32_t u = 0; u < kSmallPix / 32; ++u) {
+    const uint32_t k = lane + 32 * u;
+    adcR[u] = 0;
+    if (k < np) {
+      const bool valid = gmid[k] != kInvId;
+      const uint16_t y = ws.yy[start + firstPixel + k];
+      sx[k] = ws.xx[start + firstPixel + k];
+      sy[k] = valid ? y : uint16_t(0xffff);
+      adcR[u] = int32_t(ws.adc[start + firstPixel + k]);
+      lab[k] = int32_t(k);
+      colOk &= !valid || y < kModCols;
+    }
   }
+  colOk = __all_sync(0xffffffffu, colOk);
   __syncwarp();
   auto find = [&](int32_t a) {
     while (true) {
@@ -730,26 +747,72 @@ __global__ void __launch_bounds__(kSmallWarps * 32) kFindClustersSmall(Workspace
       a = p;
     }
   };
-  for (uint32_t k = lane; k < np; k += 32) {
-    const uint16_t yk = sy[k];
-    if (yk == 0xffff) continue;
-    const int xk = sx[k];
-    for (uint32_t m = k + 1; m < np; ++m) {
-      const uint16_t ym = sy[m];
-      if (ym == 0xffff || abs(int(ym) - int(yk)) > 1 || abs(int(sx[m]) - xk) > 1) continue;
-      int32_t a = int32_t(k), bb = int32_t(m);
-      while (true) {
-        a = find(a);
-        bb = find(bb);
-        if (a == bb) break;
-        if (a > bb) {
-          const int32_t t = a;
-          a = bb;
-          bb = t;
-        }
-        const int32_t old = atomicCAS(&lab[bb], bb, a);
-        if (old == bb) break;
-        bb = old;
+  // union of neighbours (|dx| <= 1, |dy| <= 1).  The components, and with
+  // them the roots (the smallest pixel index of each), do not depend on the
+  // order the neighbour pairs are found in.
+  auto unite = [&](int32_t a, int32_t bb) {
+    while (true) {
+      a = find(a);
+      bb = find(bb);
+      if (a == bb) break;
+      if (a > bb) {
+        const int32_t t = a;
+        a = bb;
+        bb = t;
+      }
+      const int32_t old = atomicCAS(&lab[bb], bb, a);
+      if (old == bb) break;
+      bb = old;
+    }
+  };
+  if (colOk) {
+    // pixels binned by column (counting sort): a pixel's neighbours lie in
+    // its own column and the next one
+    uint32_t* col = colA[w];
+    uint8_t* ord = ordA[w];
+    for (uint32_t b = lane; b < kModCols; b += 32) col[b] = 0;
+    __syncwarp();
+    for (uint32_t k = lane; k < np; k += 32)
+      if (sy[k] != 0xffff) atomicAdd(&col[sy[k]], 1u);
+    __syncwarp();
+    {
+      constexpr uint32_t per = kModCols / 32;  // consecutive bins per lane
+      static_assert(kModCols % 32 == 0, "column bins per lane");
+      uint32_t v[per], run = 0;
+#pragma unroll
+      for (uint32_t j = 0; j < per; ++j) {
+        v[j] = run;
+        run += col[lane * per + j];
+      }
+      const uint32_t base = warpInclusiveScan(run) - run;
+#pragma unroll
+      for (uint32_t j = 0; j < per; ++j) col[lane * per + j] = base + v[j];
+    }
+    __syncwarp();
+    for (uint32_t k = lane; k < np; k += 32)
+      if (sy[k] != 0xffff) ord[atomicAdd(&col[sy[k]], 1u)] = uint8_t(k);
+    __syncwarp();
+    // col[b] is now the end of bin b and the start of bin b + 1
+    for (uint32_t k = lane; k < np; k += 32) {
+      const uint16_t yk = sy[k];
+      if (yk == 0xffff) continue;
+      const int xk = sx[k];
+      const uint32_t p0 = yk > 0 ? col[yk - 1] : 0u;
+      const uint32_t p1 = col[min(uint32_t(yk) + 1u, kModCols - 1u)];
+      for (uint32_t p = p0; p < p1; ++p) {
+        const uint32_t m = ord[p];
+        if (m != k && abs(int(sx[m]) - xk) <= 1) unite(int32_t(k), int32_t(m));
+      }
+    }
+  } else {
+    for (uint32_t k = lane; k < np; k += 32) {
+      const uint16_t yk = sy[k];
+      if (yk == 0xffff) continue;
+      const int xk = sx[k];
+      for (uint32_t m = k + 1; m < np; ++m) {
+        const uint16_t ym = sy[m];
+        if (ym == 0xffff || abs(int(ym) - int(yk)) > 1 || abs(int(sx[m]) - xk) > 1) continue;
+        unite(int32_t(k), int32_t(m));
       }
     }
   }
@@ -774,11 +837,13 @@ __global__ void __launch_bounds__(kSmallWarps * 32) kFindClustersSmall(Workspace
   }
   for (uint32_t k = lane; k < found; k += 32) chg[k] = 0;
   __syncwarp();
-  for (uint32_t k = lane; k < np; k += 32) {
-    if (sy[k] == 0xffff) continue;
+#pragma unroll
+  for (uint32_t u = 0; u < kSmallPix / 32; ++u) {
+    const uint32_t k = lane + 32 * u;
+    if (k >= np || sy[k] == 0xffff) continue;
     const int32_t id = rk[lab[k]];
     lab[k] = id;
-    atomicAdd(&chg[id], int32_t(ws.adc[start + firstPixel + k]));
+    atomicAdd(&chg[id], adcR[u]);
   }
   __syncwarp();
   // charge cut: new ids (stored as id + 1, 0 = removed)

@@ -136,6 +136,15 @@ __device__ __forceinline__ uint32_t cutNear(double a, double b) {
   const double d = fabs(a - b);
   return d <= (1.0 / 4194304.0) * fmax(fabs(a), fabs(b)) ? 1u : 0u;
 }
+// The same test on single-precision operands, with a single-precision
+// exclusion first: the rounded |a - b| is within 2^-24 of the exact one
+// (exact for subnormal results), so a rounded difference above 2^-21 of the
+// larger magnitude (a power-of-two scaling, exact for normal results) means
+// the exact test fails.  NaN operands reach the exact test, which fails.
+__device__ __forceinline__ uint32_t cutNear(float a, float b) {
+  if (fabsf(a - b) > 4.76837158203125e-7f * fmaxf(fabsf(a), fabsf(b))) return 0u;
+  return cutNear(double(a), double(b));
+}
 
 // ---------------------------------------------------------------- ES on device
 struct DeviceES {

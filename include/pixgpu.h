@@ -78,8 +78,10 @@ enum pg_flag {
   /* bit 16 is the results' "more loose tracks than stored" */
   PG_FLAG_SPLIT_MODULE = 1u << 17,     /* a module's digis in several runs: the later runs are read as
                                           padding (the reference's result is loop-order dependent) */
-  PG_FLAG_TOO_MANY_RUNS = 1u << 18     /* more than 2000 module runs: the first 2000 found are kept (the
+  PG_FLAG_TOO_MANY_RUNS = 1u << 18,    /* more than 2000 module runs: the first 2000 found are kept (the
                                           reference's countModules counter wraps, gpuClustering.h:33) */
+  PG_FLAG_SCAN_STALL = 1u << 19        /* a prefix-scan tile waited past its bound for the tile before it:
+                                          the event's offsets are invalid (not expected to occur) */
 };
 
 typedef struct pg_ctx pg_ctx;

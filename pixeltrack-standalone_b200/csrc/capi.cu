@@ -450,6 +450,10 @@ int createSlot(pg_ctx* c, Slot& s, size_t bytes) {
   const uint32_t E = c->cfg.max_events;
   if (cudaMalloc(&s.dmem, bytes) != cudaSuccess) return fail(c, PG_ERR_NOMEM, "slot workspace");
   workspaceCarve(s.ws, s.dmem, E, c->cfg.max_words_per_batch, c->caps);
+  // scan state words and batch epochs start at zero (no tile published)
+  if (cudaMemset(s.ws.scanState, 0, size_t(E) * kScanCalls * s.ws.scanTiles * sizeof(uint64_t)) != cudaSuccess ||
+      cudaMemset(s.ws.scanEpoch, 0, size_t(E) * sizeof(uint32_t)) != cudaSuccess)
+    return fail(c, PG_ERR_CUDA, "slot scan state");
   // layer pairs of CAHitNtupletGeneratorKernels.cc:52-57
   s.ws.ca.nPairs = c->cfg.min_hits_per_ntuplet > 3 ? 13u : (c->cfg.include_jumping_forward_doublets ? 19u : 15u);
   s.ws.ca.minHits = c->cfg.min_hits_per_ntuplet;

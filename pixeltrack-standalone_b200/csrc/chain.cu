@@ -1,4 +1,5 @@
 // Batch workspace layout and the launch sequence of the whole chain.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -113,7 +114,13 @@ void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W, const Caps& cap) {
   c.take(ws.idv, T);
   c.take(ws.scratchA, size_t(E) * cap.scratch);
   c.take(ws.scratchB, size_t(E) * cap.scratch);
-  c.take(ws.scanSums, size_t(E) * kScanMaxSlices);
+  {
+    const uint32_t longest = std::max(std::max(cap.jCap, cap.cells), std::max(cap.hits, kPhiTot));
+    ws.scanTiles = (longest + kScanTile - 1) / kScanTile + 1;
+  }
+  c.take(ws.scanState, size_t(E) * kScanCalls * ws.scanTiles);
+  c.take(ws.scanTicket, size_t(E) * kScanCalls);
+  c.take(ws.scanEpoch, E);
   c.take(ws.bigSeg, size_t(E) * kBigSegCap);
   c.take(ws.segList, size_t(E) * cap.cells);
 }

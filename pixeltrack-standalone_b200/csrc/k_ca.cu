@@ -883,24 +883,25 @@ __global__ void kTrackPool(Workspace ws, uint32_t* candFlag) {
   uint32_t n = c->nCells;
   const uint32_t* off = ws.trkOff + size_t(e) * (ws.cap.cells + 1);
   uint32_t* flag = candFlag + size_t(e) * (ws.cap.cells + 1);
+  uint32_t* cand = ws.candidates + size_t(e) * ws.cap.cells;
   uint32_t local = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     uint32_t s = off[i + 1] - off[i];
     local += s > 0 ? 1u : 0u;
-    flag[i] = min(s, uint32_t(PF_MAX_CELL_TRACKS)) >= 2 ? 1u : 0u;
+    const bool isCand = min(s, uint32_t(PF_MAX_CELL_TRACKS)) >= 2;
+    flag[i] = isCand ? 1u : 0u;
+    // the candidate list in no particular order: the duplicate removers that
+    // read it do not depend on it
+    const uint32_t am = __activemask();
+    const uint32_t m = __ballot_sync(am, isCand);
+    const uint32_t leader = uint32_t(__ffs(am) - 1);
+    uint32_t at = 0;
+    if (laneId() == leader && m) at = atomicAdd(&c->nCandidates, uint32_t(__popc(m)));
+    at = __shfl_sync(am, at, leader);
+    if (isCand) cand[at + __popc(m & lanemaskLt())] = i;
   }
   local = __reduce_add_sync(0xffffffffu, local);
   if ((threadIdx.x & 31) == 0 && local) atomicAdd(&c->nTrkLists, local);
-}
-
-__global__ void kCandidateScatter(Workspace ws, const uint32_t* candFlag, const uint32_t* candOff) {
-  uint32_t e = blockIdx.y;
-  uint32_t n = ws.ev[e].nCells;
-  const uint32_t* f = candFlag + size_t(e) * (ws.cap.cells + 1);
-  const uint32_t* o = candOff + size_t(e) * (ws.cap.cells + 1);
-  uint32_t* cand = ws.candidates + size_t(e) * ws.cap.cells;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    if (f[i]) cand[o[i]] = i;
 }
 
 // kernel_earlyDuplicateRemover: per cell with >= 2 tracks
@@ -1304,18 +1305,19 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   PG_PROBED("kDoubletSetup", stream, kDoubletSetup<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents));
   PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.ohCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
   PG_PROBED("kDoubletCount", stream, kDoubletCount<<<dim3(tunedGrid(ws, kTuneDoubletCount, gx * 4), nEvents), 256, 0, stream>>>(ws));
-  segScan(ws.jCount, ws.jOffset, kJCap + 1, EVF(ntot), kJCap, nullptr, 0, ws.scanSums, nEvents, stream);
+  segScan(ws, kScanDoubletSlots, ws.jCount, ws.jOffset, kJCap + 1, EVF(ntot), kJCap, nullptr, 0, nEvents, stream);
   PG_PROBED("kDoubletWrite", stream, kDoubletWrite<<<dim3(tunedGrid(ws, kTuneDoubletWrite, gx * 4), nEvents), 256, 0, stream>>>(ws));
   PG_PROBED("kCellsTotal", stream, kCellsTotal<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents));
   // ---- isOuterHitOfCell: scan of the per-hit counts, unordered fill, order per hit
-  segScan(ws.ohCount, ws.ohOff, kHitCap + 1, EVF(nHits), kHitCap, nullptr, 0, ws.scanSums, nEvents, stream, true);
+  segScan(ws, kScanOuterHits, ws.ohCount, ws.ohOff, kHitCap + 1, EVF(nHits), kHitCap, nullptr, 0, nEvents, stream, true);
   PG_PROBED("kOuterHitFill", stream, kOuterHitFill<<<dim3(tunedGrid(ws, kTuneOuterHitFill, gx), nEvents), 256, 0, stream>>>(ws));
   sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.ohCells, kCellCap, ws.ohOff, kHitCap + 1, EVF(nHits), 0, false, kCellCap, 0);
   PG_PROBED("kOhRec", stream, kOhRec<<<dim3(tunedGrid(ws, kTuneOhRec, gx), nEvents), 256, 0, stream>>>(ws));
   // ---- CA links: edges appended unordered, then CSR by inner cell, ordered ascending
   PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbrCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
   PG_PROBED("kConnect", stream, kConnect<<<dim3(tunedGrid(ws, kTuneConnect, gx * 4), nEvents), 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
-  segScan(ws.nbrCount, ws.nbrOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanSums, nEvents, stream, true);
+  segScan(ws, kScanNeighbours, ws.nbrCount, ws.nbrOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, nEvents, stream,
+          true);
   PG_PROBED("kEdgeScatter", stream, kEdgeScatter<<<dim3(tunedGrid(ws, kTuneEdgeScatter, gx), nEvents), 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
   sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.nbr, ws.cap.edges, ws.nbrOff, kCellCap + 1, EVF(nCells), 0, false,
                          min(ws.cap.edges, ws.cap.scratch), 1);
@@ -1325,21 +1327,21 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
     PG_PROBED("kFishbone", stream, kFishbone<<<dim3(tunedGrid(ws, kTuneFishbone, gx * 2), nEvents), 256, 0, stream>>>(ws, false));
   // ---- n-tuplets: DFS count, scans, DFS write, finalize
   PG_PROBED("kNtupletCount", stream, kNtupletCount<<<dim3(tunedGrid(ws, kTuneNtupletCount, gx * 8), nEvents), 128, 0, stream>>>(ws));
-  segScan(ws.startTupleCount, ws.startTupleOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcM), ws.scanSums, nEvents, stream);
-  segScan(ws.startHitCount, ws.startHitOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcN), ws.scanSums, nEvents, stream);
+  segScan(ws, kScanStartTuples, ws.startTupleCount, ws.startTupleOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcM),
+          nEvents, stream);
+  segScan(ws, kScanStartHits, ws.startHitCount, ws.startHitOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcN), nEvents,
+          stream);
   PG_PROBED("kNtupletWrite", stream, kNtupletWrite<<<dim3(tunedGrid(ws, kTuneNtupletWrite, gx * 8), nEvents), 128, 0, stream>>>(ws));
   PG_PROBED("kTupleFinalize", stream, kTupleFinalize<<<dim3(32, nEvents), 1024, 0, stream>>>(ws));
   // ---- cell -> track lists
   PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.trkCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
   PG_PROBED("kTrackCount", stream, kTrackCount<<<dim3(tunedGrid(ws, kTuneTrackCount, gx), nEvents), 256, 0, stream>>>(ws));
-  segScan(ws.trkCount, ws.trkOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, ws.scanSums, nEvents, stream, true);
+  segScan(ws, kScanCellTracks, ws.trkCount, ws.trkOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, nEvents, stream,
+          true);
   PG_PROBED("kTrackFill", stream, kTrackFill<<<dim3(tunedGrid(ws, kTuneTrackFill, gx), nEvents), 256, 0, stream>>>(ws));
   sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.trk, kTupleCellCap, ws.trkOff, kCellCap + 1, EVF(nCells), 0, false, kTupleCellCap, 2);
   uint32_t* candFlag = ws.startTupleCount;  // scratch
-  uint32_t* candOff = ws.startHitCount;
   PG_PROBED("kTrackPool", stream, kTrackPool<<<dim3(tunedGrid(ws, kTuneTrackPool, gx), nEvents), 256, 0, stream>>>(ws, candFlag));
-  segScan(candFlag, candOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(nCandidates), ws.scanSums, nEvents, stream);
-  PG_PROBED("kCandidateScatter", stream, kCandidateScatter<<<dim3(tunedGrid(ws, kTuneCandidateScatter, gx), nEvents), 256, 0, stream>>>(ws, candFlag, candOff));
   PG_PROBED("kEarlyDup", stream, kEarlyDup<<<dim3(tunedGrid(ws, kTuneEarlyDup, gx), nEvents), 256, 0, stream>>>(ws));
   PG_PROBED("kTupleDet", stream, kTupleDet<<<dim3(tunedGrid(ws, kTuneTupleDet, gx), nEvents), 256, 0, stream>>>(ws));
   // ---- tuple multiplicity for the fits
@@ -1370,7 +1372,7 @@ cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
   // hit -> tuple map and triplet cleaner
   PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
   PG_PROBED("kHitToTupleCount", stream, kHitToTupleCount<<<dim3(tunedGrid(ws, kTuneHitToTupleCount, gx), nEvents), 256, 0, stream>>>(ws));
-  segScan(ws.h2tCount, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, nullptr, 0, ws.scanSums, nEvents, stream, true);
+  segScan(ws, kScanHitTuples, ws.h2tCount, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, nullptr, 0, nEvents, stream, true);
   PG_PROBED("kHitToTupleFill", stream, kHitToTupleFill<<<dim3(tunedGrid(ws, kTuneHitToTupleFill, gx), nEvents), 256, 0, stream>>>(ws));
   sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.h2t, ws.cap.h2t, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, true,
                          ws.cap.h2t, 3);

@@ -186,7 +186,9 @@ __global__ void kInitEvents(Workspace ws, uint32_t nEvents) {
     c->nBigHitMod = 0;
     c->nearDoublet = c->nearCA = c->nearQuality = 0;
     c->flags = c->nWords > ws.cap.fedWords ? kFlagTooManyWords : 0u;
+    ws.scanEpoch[e] += 1;  // tags this batch's scan state words
   }
+  if (threadIdx.x < kScanCalls) ws.scanTicket[size_t(e) * kScanCalls + threadIdx.x] = 0;
   // the module-run start bitmap of kModuleBoundaries (in scratchA, free until the doublets)
   uint32_t* bm = ws.scratchA + size_t(e) * ws.cap.scratch;
   const uint32_t nbw = (min(ws.wordOffsets[e + 1] - ws.wordOffsets[e], ws.cap.fedWords) + 31) / 32;
@@ -1284,7 +1286,7 @@ cudaError_t runLocal(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaSt
   PG_PROBED("kZeroU32", stream, kZeroU32<<<dim3(2, nEvents), 1024, 0, stream>>>(cursor, kPhiStride, kPhiStride, nEvents));
   PG_PROBED("kPhiCount", stream, kPhiCount<<<dim3(tunedGrid(ws, kTunePhiCount, 16), nEvents), 256, 0, stream>>>(ws));
   // in place exclusive scan of the 1280 counters; the total lands in the extra bin
-  segScan(ws.phiOff, ws.phiOff, kPhiStride, nullptr, 0, kPhiTot - 1, nullptr, 0, ws.scanSums, nEvents, stream);
+  segScan(ws, kScanPhi, ws.phiOff, ws.phiOff, kPhiStride, nullptr, 0, kPhiTot - 1, nullptr, 0, nEvents, stream);
   PG_PROBED("kPhiFill", stream, kPhiFill<<<dim3(tunedGrid(ws, kTunePhiFill, 16), nEvents), 256, 0, stream>>>(ws, cursor));
   PG_PROBED("kPhiSort", stream, kPhiSort<<<dim3((kPhiTot - 1 + 7) / 8, nEvents), 256, 0, stream>>>(ws));
   PG_PROBED("kPhiRec", stream, kPhiRec<<<dim3(tunedGrid(ws, kTunePhiRec, 16), nEvents), 256, 0, stream>>>(ws));

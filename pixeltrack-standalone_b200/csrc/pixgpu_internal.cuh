@@ -88,7 +88,8 @@ enum : uint32_t {
   kFlagJOverflow = 1u << 14,        // more doublet inner-hit slots than cap.jCap
   kFlagBadInput = 1u << 15,         // words/cabling entries outside the tables (ignored)
   kFlagSplitModule = 1u << 17,      // a module's digis in several runs (later runs read as padding)
-  kFlagTooManyRuns = 1u << 18       // more than 2000 module runs (the reference's counter wraps)
+  kFlagTooManyRuns = 1u << 18,      // more than 2000 module runs (the reference's counter wraps)
+  kFlagScanStall = 1u << 19         // a scan tile waited past its bound for its predecessor (offsets invalid)
 };
 
 static_assert(uint32_t(kFlagBadInput) == uint32_t(PG_FLAG_BAD_INPUT) &&
@@ -170,7 +171,19 @@ struct BatchInput {
   const uint8_t* fedIds;
 };
 
-constexpr uint32_t kScanMaxSlices = 64;  // slices of one event's array in the segmented scan
+// segmented scans of the chain: one state region each per event (scan.cu)
+enum ScanCall : uint32_t {
+  kScanPhi = 0,
+  kScanDoubletSlots,
+  kScanOuterHits,
+  kScanNeighbours,
+  kScanStartTuples,
+  kScanStartHits,
+  kScanCellTracks,
+  kScanHitTuples,
+  kScanCalls
+};
+constexpr uint32_t kScanTile = 4096;  // elements per tile of the single-pass scan
 
 // CAHitNtupletGeneratorOnGPU parameters that select among the algorithm's
 // variants (CAHitNtupletGeneratorOnGPU.cc:45-66; CAHitNtupletGeneratorKernels.cc:52-70)
@@ -210,7 +223,7 @@ enum TuneId : uint32_t {
   kTuneRawToDigi, kTuneModuleBoundaries, kTuneFindClustersBig, kTuneGetHitsBig, kTunePhiCount, kTunePhiFill,
   kTunePhiRec, kTuneDoubletCount, kTuneDoubletWrite, kTuneOuterHitFill, kTuneOhRec, kTuneConnect, kTuneEdgeScatter,
   kTuneNbrPool, kTuneFishbone, kTuneNtupletCount, kTuneNtupletWrite, kTuneTrackCount, kTuneTrackFill,
-  kTuneTrackPool, kTuneCandidateScatter, kTuneEarlyDup, kTuneTupleDet, kTuneClassify, kTuneFastDupInDegree,
+  kTuneTrackPool, kTuneEarlyDup, kTuneTupleDet, kTuneClassify, kTuneFastDupInDegree,
   kTuneHitToTupleCount, kTuneHitToTupleFill, kTuneTripletCleaner, kTuneFitZero, kTuneFit, kTuneFedCopy, kNumTune
 };
 extern const char* const kTuneNames[kNumTune];
@@ -282,7 +295,7 @@ struct Workspace {
   uint32_t* trkCount;        // [maxEvents][cap.cells + 1]
   uint32_t* trkOff;          // [maxEvents][cap.cells + 1]
   uint32_t* trk;             // [maxEvents][cap.tupleCells()]
-  uint32_t* candidates;      // [maxEvents][cap.cells] cells with >= 2 tracks, ascending
+  uint32_t* candidates;      // [maxEvents][cap.cells] cells with >= 2 tracks, in no particular order
   // tuple multiplicity
   uint32_t* tmOff;           // [maxEvents][16]
   uint32_t* tmBins;          // [maxEvents][cap.tuples]
@@ -300,7 +313,12 @@ struct Workspace {
   // scratch: CA link lists before ordering, cleaner state
   uint32_t* scratchA;        // [maxEvents][cap.scratch]
   uint32_t* scratchB;        // [maxEvents][cap.scratch]
-  uint32_t* scanSums;        // [maxEvents][kScanMaxSlices] slice totals of the segmented scans
+  // single-pass scans (scan.cu): per event and scan, a tile ticket and one
+  // state word per tile; scanEpoch tags the words of the current batch
+  uint64_t* scanState;       // [maxEvents][kScanCalls][scanTiles]
+  uint32_t* scanTicket;      // [maxEvents][kScanCalls], cleared by kInitEvents
+  uint32_t* scanEpoch;       // [maxEvents], advanced by kInitEvents
+  uint32_t scanTiles;        // tiles of the longest scanned array
   uint32_t* bigSeg;          // [maxEvents][kBigSegCap] long segments awaiting the block sort
   uint32_t* segList;         // [maxEvents][cap.cells] segments with >= 2 entries (the ones to order)
 };
@@ -401,10 +419,10 @@ void launchPack(Workspace& ws, uint32_t nEvents, uint8_t* out, cudaStream_t s);
 // for i <= n_e, where n_e = lenPtr[e*lenStride] (device) or maxLen when lenPtr is
 // null; n_e <= maxLen.  The total lands at out[e*stride + n_e] and, if totalPtr,
 // at totalPtr[e*totalStride].  in may equal out unless zeroIn, which leaves
-// in[0..n_e) zero (the count arrays are reused as fill cursors).
-// sums: [nEvents][kScanMaxSlices] scratch for the slice totals.
-void segScan(uint32_t* in, uint32_t* out, uint32_t stride, const uint32_t* lenPtr, uint32_t lenStride,
-             uint32_t maxLen, uint32_t* totalPtr, uint32_t totalStride, uint32_t* sums, uint32_t nEvents,
-             cudaStream_t stream, bool zeroIn = false);
+// in[0..n_e) zero (the count arrays are reused as fill cursors).  `call`
+// selects the scan's state region (one per scan of a batch).
+void segScan(const Workspace& ws, ScanCall call, uint32_t* in, uint32_t* out, uint32_t stride,
+             const uint32_t* lenPtr, uint32_t lenStride, uint32_t maxLen, uint32_t* totalPtr, uint32_t totalStride,
+             uint32_t nEvents, cudaStream_t stream, bool zeroIn = false);
 
 }  // namespace pixgpu

@@ -1,12 +1,17 @@
 // Batched segmented exclusive scan over per-event arrays with fixed stride
-// and device-resident lengths (no host synchronisation), in two launches:
-// each event's array is cut into S slices of whole tiles; the first kernel
-// sums every slice, the second rescans every slice (from L2) starting at the
-// sum of the slices before it, which each CTA adds up itself.  S grows as the
-// batch shrinks, so that a small batch still spreads over the SMs.
+// and device-resident lengths (no host synchronisation), in one pass with
+// decoupled look-back: the CTAs of an event take the tiles of its array in
+// ticket order; a tile publishes its sum at once, then adds up the sums of
+// the tiles before it (32 at a time, stopping at the first tile that has
+// published its full prefix), publishes its own prefix and writes its
+// outputs.  Each element is read once and written once.
 // out[i] = in[0] + ... + in[i-1] for i <= n (out[n] the total).  The
 // reference's counterpart is the prefix scan of its OneToManyAssoc fills
 // (HistoContainer.h / prefixScan.h, one event at a time).
+//
+// A tile waits only on tiles with smaller tickets, which were taken by CTAs
+// already running, so every wait ends; the wait is bounded all the same and
+// sets kFlagScanStall if the bound is reached.
 #include "device_utils.cuh"
 #include "pixgpu_internal.cuh"
 
@@ -15,111 +20,134 @@ namespace pixgpu {
 namespace {
 
 constexpr uint32_t kScanThreads = 512;
-constexpr uint32_t kScanPer = 8;                           // elements per thread in a tile
-constexpr uint32_t kScanTile = kScanThreads * kScanPer;  // 4096
+constexpr uint32_t kScanPer = kScanTile / kScanThreads;  // 8 elements per thread in a tile
 // A warp owns 32 * kScanPer consecutive elements of a tile; lane l holds
 // element j * 32 + l of that run in v[j] (coalesced loads and stores).
 
-struct Slice {
-  uint32_t n, lo, hi;
-};
-
-__device__ __forceinline__ Slice sliceOf(const uint32_t* lenPtr, uint32_t lenStride, uint32_t fixedLen, uint32_t e,
-                                         uint32_t r, uint32_t S) {
-  Slice s;
-  s.n = lenPtr ? min(lenPtr[size_t(e) * lenStride], fixedLen) : fixedLen;  // fixedLen: the capacity
-  const uint32_t tiles = (s.n + kScanTile - 1) / kScanTile;
-  s.lo = min(s.n, tiles * r / S * kScanTile);
-  s.hi = min(s.n, tiles * (r + 1) / S * kScanTile);
-  return s;
+// state word of a tile: tag (30 bits) | status (2 bits) | value (32 bits).
+// The tag names the batch and the scan, so words left by earlier batches
+// read as "not yet published".
+constexpr uint64_t kStatusSum = 1, kStatusPrefix = 2;
+__device__ __forceinline__ uint64_t stateWord(uint32_t tag, uint64_t status, uint32_t v) {
+  return (uint64_t(tag) << 34) | (status << 32) | v;
+}
+__device__ __forceinline__ void publish(uint64_t* p, uint64_t w) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
+}
+__device__ __forceinline__ uint64_t peek(const uint64_t* p) {
+  uint64_t w;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
+  return w;
 }
 
-__global__ void __launch_bounds__(kScanThreads)
-    kScanSums(const uint32_t* in, uint32_t stride, const uint32_t* lenPtr, uint32_t lenStride, uint32_t fixedLen,
-              uint32_t* sums) {
-  __shared__ uint32_t sh[33];
-  const uint32_t e = blockIdx.y, r = blockIdx.x, S = gridDim.x;
-  const Slice sl = sliceOf(lenPtr, lenStride, fixedLen, e, r, S);
-  const uint32_t* src = in + size_t(e) * stride;
-  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t s = 0;
-  for (uint32_t b = sl.lo; b < sl.hi; b += kScanTile) {
-    const uint32_t w0 = b + warp * 32 * kScanPer + lane;
-#pragma unroll
-    for (uint32_t j = 0; j < kScanPer; ++j) {
-      const uint32_t i = w0 + j * 32;
-      s += i < sl.hi ? src[i] : 0u;
-    }
-  }
-  uint32_t tot;
-  blockExclusiveScan(s, sh, &tot);
-  if (threadIdx.x == 0) sums[size_t(e) * kScanMaxSlices + r] = tot;
-}
+constexpr uint32_t kLookBackPolls = 1u << 22;  // bound on the polls of one look-back (~0.3 s)
 
 __global__ void __launch_bounds__(kScanThreads, 3)
-    kScanSlices(uint32_t* in, uint32_t* out, uint32_t stride, const uint32_t* lenPtr, uint32_t lenStride,
-                uint32_t fixedLen, const uint32_t* sums, uint32_t* totalPtr, uint32_t totalStride, bool zeroIn) {
+    kScanOnePass(uint32_t* in, uint32_t* out, uint32_t stride, const uint32_t* lenPtr, uint32_t lenStride,
+                 uint32_t fixedLen, uint32_t* totalPtr, uint32_t totalStride, bool zeroIn, Workspace ws,
+                 uint32_t call) {
   __shared__ uint32_t sh[33];
-  __shared__ uint32_t sOff;
-  const uint32_t e = blockIdx.y, r = blockIdx.x, S = gridDim.x;
-  const Slice sl = sliceOf(lenPtr, lenStride, fixedLen, e, r, S);
+  __shared__ uint32_t sTile, sPrefix;
+  const uint32_t e = blockIdx.y;
+  const uint32_t n = lenPtr ? min(lenPtr[size_t(e) * lenStride], fixedLen) : fixedLen;  // fixedLen: the capacity
+  const uint32_t tiles = max(1u, (n + kScanTile - 1) / kScanTile);
   uint32_t* src = in + size_t(e) * stride;
   uint32_t* dst = out + size_t(e) * stride;
+  uint64_t* state = ws.scanState + (size_t(e) * kScanCalls + call) * ws.scanTiles;
+  uint32_t* ticket = ws.scanTicket + size_t(e) * kScanCalls + call;
+  const uint32_t tag = (ws.scanEpoch[e] * kScanCalls + call) & 0x3fffffffu;
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (warp == 0) {
-    uint32_t o = 0;
-    for (uint32_t k = lane; k < r; k += 32) o += sums[size_t(e) * kScanMaxSlices + k];
-    o = __reduce_add_sync(0xffffffffu, o);
-    if (lane == 0) sOff = o;
-  }
-  __syncthreads();
-  uint32_t carry = sOff;
-  for (uint32_t b = sl.lo; b < sl.hi; b += kScanTile) {
-    const uint32_t w0 = b + warp * 32 * kScanPer + lane;
+  for (;;) {
+    if (threadIdx.x == 0) sTile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint32_t t = sTile;
+    if (t >= tiles) return;
+    const uint32_t lo = t * kScanTile, hi = min(n, lo + kScanTile);
+    const uint32_t w0 = lo + warp * 32 * kScanPer + lane;
     uint32_t v[kScanPer];
     uint32_t run = 0;  // exclusive prefix of the warp's run so far
 #pragma unroll
     for (uint32_t j = 0; j < kScanPer; ++j) {
       const uint32_t i = w0 + j * 32;
-      const uint32_t x = i < sl.hi ? src[i] : 0u;
+      v[j] = i < hi ? src[i] : 0u;
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < kScanPer; ++j) {
+      const uint32_t x = v[j];
       const uint32_t inc = warpInclusiveScan(x);
       v[j] = run + inc - x;
       run += __shfl_sync(0xffffffffu, inc, 31);
     }
     uint32_t tileTot;
     const uint32_t wpre = blockExclusiveScan(lane == 31 ? run : 0u, sh, &tileTot);
-    const uint32_t base = carry + __shfl_sync(0xffffffffu, wpre, 31);
+    const uint32_t base = __shfl_sync(0xffffffffu, wpre, 31);
+    // publish this tile's sum, then look back (warp 0)
+    if (warp == 0) {
+      uint32_t prefix = 0;
+      if (t == 0) {
+        if (lane == 0) publish(state, stateWord(tag, kStatusPrefix, tileTot));
+      } else {
+        if (lane == 0) publish(state + t, stateWord(tag, kStatusSum, tileTot));
+        int32_t k = int32_t(t) - 1;  // the window covers tiles k - 31 .. k
+        uint32_t polls = 0;
+        bool stalled = false;
+        while (k >= 0) {
+          const int32_t idx = k - int32_t(lane);
+          uint64_t w = idx >= 0 ? peek(state + idx) : stateWord(tag, kStatusPrefix, 0u);
+          const bool ready = uint32_t(w >> 34) == tag && ((w >> 32) & 3u) != 0;
+          if (__all_sync(0xffffffffu, ready)) {
+            // the nearest tile with its full prefix ends the walk
+            const uint32_t pm = __ballot_sync(0xffffffffu, ((w >> 32) & 3u) == kStatusPrefix);
+            const uint32_t stop = pm ? uint32_t(__ffs(pm) - 1) : 32u;
+            const uint32_t val = lane <= stop ? uint32_t(w) : 0u;
+            prefix += __reduce_add_sync(0xffffffffu, val);
+            if (pm) break;
+            k -= 32;
+          } else if (++polls > kLookBackPolls) {
+            stalled = true;
+            break;
+          } else {
+            __nanosleep(64);
+          }
+        }
+        if (lane == 0) {
+          if (stalled) atomicOr(&ws.ev[e].flags, kFlagScanStall);
+          publish(state + t, stateWord(tag, kStatusPrefix, prefix + tileTot));
+        }
+      }
+      if (lane == 0) sPrefix = prefix;
+    }
+    __syncthreads();
+    const uint32_t carry = sPrefix + base;
 #pragma unroll
     for (uint32_t j = 0; j < kScanPer; ++j) {
       const uint32_t i = w0 + j * 32;
-      if (i < sl.hi) {
+      if (i < hi) {
         if (zeroIn) src[i] = 0u;
-        dst[i] = base + v[j];
+        dst[i] = carry + v[j];
       }
     }
-    carry += tileTot;
-  }
-  if (r == S - 1 && threadIdx.x == 0) {
-    dst[sl.n] = carry;
-    if (totalPtr) totalPtr[size_t(e) * totalStride] = carry;
+    if (t == tiles - 1 && threadIdx.x == 0) {
+      dst[n] = sPrefix + tileTot;
+      if (totalPtr) totalPtr[size_t(e) * totalStride] = sPrefix + tileTot;
+    }
+    __syncthreads();  // sTile and sPrefix are rewritten by the next tile
   }
 }
 
 }  // namespace
 
-void segScan(uint32_t* in, uint32_t* out, uint32_t stride, const uint32_t* lenPtr, uint32_t lenStride,
-             uint32_t maxLen, uint32_t* totalPtr, uint32_t totalStride, uint32_t* sums, uint32_t nEvents,
-             cudaStream_t stream, bool zeroIn) {
-  // slices per event: enough CTAs for a few waves, no slice shorter than a tile
-  const uint32_t tiles = (maxLen + kScanTile - 1) / kScanTile;
-  uint32_t S = min(kScanMaxSlices, max(16u, 1024u / max(nEvents, 1u)));
-  S = max(1u, min(S, tiles));
+void segScan(const Workspace& ws, ScanCall call, uint32_t* in, uint32_t* out, uint32_t stride,
+             const uint32_t* lenPtr, uint32_t lenStride, uint32_t maxLen, uint32_t* totalPtr, uint32_t totalStride,
+             uint32_t nEvents, cudaStream_t stream, bool zeroIn) {
+  // CTAs per event: every tile of the longest array at once for small
+  // batches; a CTA takes further tiles while there are any
+  const uint32_t tiles = max(1u, (maxLen + kScanTile - 1) / kScanTile);
+  const uint32_t S = max(1u, min(tiles, max(8u, 1024u / max(nEvents, 1u))));
   const dim3 g(S, nEvents);
-  PG_PROBED("kScanSums", stream,
-            kScanSums<<<g, kScanThreads, 0, stream>>>(in, stride, lenPtr, lenStride, maxLen, sums));
-  PG_PROBED("kScanSlices", stream,
-            kScanSlices<<<g, kScanThreads, 0, stream>>>(in, out, stride, lenPtr, lenStride, maxLen, sums, totalPtr,
-                                                        totalStride, zeroIn));
+  PG_PROBED("kScanOnePass", stream,
+            kScanOnePass<<<g, kScanThreads, 0, stream>>>(in, out, stride, lenPtr, lenStride, maxLen, totalPtr,
+                                                         totalStride, zeroIn, ws, uint32_t(call)));
 }
 
 }  // namespace pixgpu

@@ -22,7 +22,7 @@ const char* const kTuneNames[kNumTune] = {
     "kPhiFill",        "kPhiRec",           "kDoubletCount",    "kDoubletWrite",     "kOuterHitFill",
     "kOhRec",          "kConnect",          "kEdgeScatter",     "kNbrPool",          "kFishbone",
     "kNtupletCount",   "kNtupletWrite",     "kTrackCount",      "kTrackFill",        "kTrackPool",
-    "kCandidateScatter", "kEarlyDup",       "kTupleDet",        "kClassify",         "kFastDupInDegree",
+    "kEarlyDup",       "kTupleDet",         "kClassify",        "kFastDupInDegree",
     "kHitToTupleCount", "kHitToTupleFill",  "kTripletCleaner",  "kFitZero",          "kBLFit",
     "kFedCopy"};
 

@@ -96,7 +96,7 @@ typedef struct pg_es_images {
 
 typedef struct pg_config {
   int device;                    /* CUDA device ordinal */
-  uint32_t max_events;           /* events per batch */
+  uint32_t max_events;           /* events per batch (1..1024) */
   uint32_t max_words_per_batch;  /* FED payload words over a whole batch */
   uint32_t slots;                /* independent batch slots (streams + workspaces); 0: as many as fit in
                                     hbm_fraction of the free device memory, at most 16 */

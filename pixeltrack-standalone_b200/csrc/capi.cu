@@ -554,7 +554,7 @@ int pg_create(const pg_es_images* es, const pg_config* cfgIn, pg_ctx** out) {
     c->cfg = *cfgIn;
   else
     pg_default_config(&c->cfg);
-  if (c->cfg.max_events == 0 || c->cfg.max_words_per_batch == 0 || c->cfg.max_words_per_batch > (1u << 30) ||
+  if (c->cfg.max_events == 0 || c->cfg.max_events > kFlatMaxEvents || c->cfg.max_words_per_batch == 0 || c->cfg.max_words_per_batch > (1u << 30) ||
       c->cfg.vertex_algo > 2 || c->cfg.min_hits_per_ntuplet < 3 || c->cfg.min_hits_per_ntuplet > 4 ||
       c->cfg.fed_scan > 1 || (c->cfg.fed_scan && c->cfg.pool_words) ||  // the pool stages on the host
       c->cfg.mixed_fit > 1)

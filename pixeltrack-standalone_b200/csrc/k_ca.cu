@@ -955,14 +955,46 @@ __global__ void __launch_bounds__(1024) kMultiplicity(Workspace ws) {
     const uint32_t nh = tupleSize(toff, t);
     return (nh < 3 || nh > 5 || q[t] == kDup) ? 0u : nh;
   };
-  if (threadIdx.x < 8) cnt[threadIdx.x] = 0;
-  __syncthreads();
-  for (uint32_t t = threadIdx.x; t < nt; t += blockDim.x) {
-    const uint32_t b = binOf(t);
-    if (b) atomicAdd(&cnt[b], 1u);
+  // Each warp takes a contiguous range of tuples, 32 consecutive ones per
+  // step (coalesced loads, four steps in flight).  A lane keeps the bin of
+  // each of its tuples as a 2-bit code (up to 128 steps), so the second walk,
+  // which places the tuples, needs no loads.
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint32_t R = (nt + nw * 32 - 1) / (nw * 32) * 32;
+  const uint32_t w0 = min(nt, warp * R), w1 = min(nt, w0 + R);
+  const uint32_t steps = (w1 - w0 + 31) / 32;
+  constexpr uint32_t kKeptSteps = 128;
+  const bool kept = steps <= kKeptSteps;
+  uint64_t code[kKeptSteps / 32] = {0, 0, 0, 0};
+  uint32_t n3 = 0, n4 = 0, n5 = 0;
+#pragma unroll
+  for (uint32_t g = 0; g < kKeptSteps / 32 + 1; ++g) {
+    // steps [32 g, 32 g + 32); the last group takes every step beyond 128
+    const uint32_t kEnd = g < kKeptSteps / 32 ? min(steps, 32 * g + 32) : steps;
+    for (uint32_t k = 32 * g; k < kEnd; k += 4) {
+      uint32_t bb[4];
+#pragma unroll
+      for (uint32_t u = 0; u < 4; ++u) {
+        const uint32_t t = w0 + (k + u) * 32 + lane;
+        bb[u] = (k + u < kEnd && t < w1) ? binOf(t) : 0u;
+      }
+#pragma unroll
+      for (uint32_t u = 0; u < 4; ++u) {
+        n3 += bb[u] == 3 ? 1u : 0u;
+        n4 += bb[u] == 4 ? 1u : 0u;
+        n5 += bb[u] == 5 ? 1u : 0u;
+        if (g < kKeptSteps / 32 && bb[u]) code[g < kKeptSteps / 32 ? g : 0] |= uint64_t(bb[u] - 2) << (2 * (k + u - 32 * g));
+      }
+    }
   }
-  __syncthreads();
+  n3 = __reduce_add_sync(0xffffffffu, n3);
+  n4 = __reduce_add_sync(0xffffffffu, n4);
+  n5 = __reduce_add_sync(0xffffffffu, n5);
+  uint64_t tot;
+  const uint64_t mine = uint64_t(n3) | (uint64_t(n4) << 20) | (uint64_t(n5) << 40);
+  const uint64_t warpPre = __shfl_sync(0xffffffffu, blockExclusiveScan64(lane == 0 ? mine : 0ull, scanSh, &tot), 0);
   if (threadIdx.x == 0) {
+    for (int b = 0; b < 8; ++b) cnt[b] = (b >= 3 && b <= 5) ? uint32_t((tot >> (20 * (b - 3))) & 0xfffffu) : 0u;
     uint32_t acc = 0;
     for (int b = 0; b < 8; ++b) {
       start[b] = acc;
@@ -979,18 +1011,32 @@ __global__ void __launch_bounds__(1024) kMultiplicity(Workspace ws) {
     if (c->nTrkLists > ws.cap.lists) c->flags |= kFlagTrkPoolOverflow;
   }
   __syncthreads();
-  uint64_t carry = 0;
-  for (uint32_t t0 = 0; t0 < nt; t0 += blockDim.x) {
-    const uint32_t t = t0 + threadIdx.x;
-    const uint32_t b = t < nt ? binOf(t) : 0u;
-    const uint64_t key = b ? (uint64_t(1) << (20 * (b - 3))) : 0ull;
-    uint64_t tot;
-    const uint64_t pre = blockExclusiveScan64(key, scanSh, &tot) + carry;
-    if (b) {
-      const uint32_t pos = start[b] + uint32_t((pre >> (20 * (b - 3))) & 0xfffffu);
-      if (pos < ws.cap.tuples) bins[pos] = t;
+  // the serial fill order: ascending tuple index (warps in range order, then
+  // steps, then lanes)
+  uint32_t run[3] = {uint32_t(warpPre & 0xfffffu), uint32_t((warpPre >> 20) & 0xfffffu),
+                     uint32_t((warpPre >> 40) & 0xfffffu)};
+#pragma unroll
+  for (uint32_t g = 0; g < kKeptSteps / 32 + 1; ++g) {
+    const uint32_t kEnd = g < kKeptSteps / 32 ? min(steps, 32 * g + 32) : steps;
+    for (uint32_t k = 32 * g; k < kEnd; ++k) {
+      const uint32_t t = w0 + k * 32 + lane;
+      uint32_t b = 0;
+      if (kept && g < kKeptSteps / 32)
+        b = t < w1 ? uint32_t((code[g < kKeptSteps / 32 ? g : 0] >> (2 * (k - 32 * g))) & 3u) : 0u;
+      else
+        b = t < w1 ? binOf(t) : 0u;
+      if (kept && b) b += 2;  // codes 1, 2, 3 are the bins 3, 4, 5
+#pragma unroll
+      for (uint32_t bi = 0; bi < 3; ++bi) {
+        const bool in = b == bi + 3;
+        const uint32_t m = __ballot_sync(0xffffffffu, in);
+        if (in) {
+          const uint32_t pos = start[bi + 3] + run[bi] + __popc(m & lanemaskLt());
+          if (pos < ws.cap.tuples) bins[pos] = t;
+        }
+        run[bi] += __popc(m);
+      }
     }
-    carry += tot;
   }
 }
 
@@ -1250,7 +1296,8 @@ __global__ void kTripletCleaner(Workspace ws) {
   const uint32_t* toff = ws.tupleOff + size_t(e) * (ws.cap.tuples + 1);
   uint8_t* q = ws.quality + size_t(e) * ws.cap.tuples;
   const float* tip = ws.state + size_t(e) * ws.cap.tuples * 5 + 1;
-  for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < ws.cap.hits; h += gridDim.x * blockDim.x) {
+  const uint32_t nHits = min(ws.ev[e].nHits, ws.cap.hits);  // the offsets are scanned up to nHits
+  for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < nHits; h += gridDim.x * blockDim.x) {
     uint32_t b = off[h], en = min(off[h + 1], ws.cap.h2t);
     if (en <= b || en - b < 2) continue;
     uint32_t maxNh = 0;
@@ -1303,7 +1350,7 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   dim3 g(gx, nEvents);
   // ---- doublets: count per inner-hit slot, scan, write in serial order
   PG_PROBED("kDoubletSetup", stream, kDoubletSetup<<<(nEvents + 63) / 64, 64, 0, stream>>>(ws, nEvents));
-  PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.ohCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
+  PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.ohCount, kHitCap + 1, kHitCap + 1, EVF(nHits)));
   PG_PROBED("kDoubletCount", stream, kDoubletCount<<<dim3(tunedGrid(ws, kTuneDoubletCount, gx * 4), nEvents), 256, 0, stream>>>(ws));
   segScan(ws, kScanDoubletSlots, ws.jCount, ws.jOffset, kJCap + 1, EVF(ntot), kJCap, nullptr, 0, nEvents, stream);
   PG_PROBED("kDoubletWrite", stream, kDoubletWrite<<<dim3(tunedGrid(ws, kTuneDoubletWrite, gx * 4), nEvents), 256, 0, stream>>>(ws));
@@ -1370,9 +1417,9 @@ cudaError_t runCleaners(Workspace& ws, uint32_t nEvents, cudaStream_t stream) {
             le = launchClustered(kFastDupRounds, P, nEvents, kFastDupThreads, 0, stream, ws, indeg, lists, candFlag));
   if (le != cudaSuccess) return le;
   // hit -> tuple map and triplet cleaner
-  PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, nullptr, 0));
+  PG_PROBED("kZero", stream, kZero<<<dim3(48, nEvents), 256, 0, stream>>>(ws.h2tCount, kHitCap + 1, kHitCap + 1, EVF(nHits)));
   PG_PROBED("kHitToTupleCount", stream, kHitToTupleCount<<<dim3(tunedGrid(ws, kTuneHitToTupleCount, gx), nEvents), 256, 0, stream>>>(ws));
-  segScan(ws, kScanHitTuples, ws.h2tCount, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, nullptr, 0, nEvents, stream, true);
+  segScan(ws, kScanHitTuples, ws.h2tCount, ws.h2tOff, kHitCap + 1, EVF(nHits), kHitCap, nullptr, 0, nEvents, stream, true);
   PG_PROBED("kHitToTupleFill", stream, kHitToTupleFill<<<dim3(tunedGrid(ws, kTuneHitToTupleFill, gx), nEvents), 256, 0, stream>>>(ws));
   sortSegments<uint32_t>(ws, nEvents, stream, gx * 2, ws.h2t, ws.cap.h2t, ws.h2tOff, kHitCap + 1, nullptr, 0, kHitCap, true,
                          ws.cap.h2t, 3);

@@ -372,20 +372,48 @@ __global__ void kFitZero(Workspace ws) {
 // the fits a chain can run (pg_config riemann_fit, mixed_fit)
 enum FitMode { kFitBrokenLine, kFitRiemann, kFitBrokenLineMixed, kFitRiemannMixed };
 
+// the tuples of multiplicity bin nh of every event of the batch, as one flat
+// range over the events (uneven events share the whole grid): pre[e] is the
+// exclusive prefix of the per-event bin sizes, built by each block
+__device__ __forceinline__ uint32_t fitBinPrefix(const Workspace& ws, uint32_t nh, uint32_t nEvents, uint32_t* pre,
+                                                 uint32_t* scanSh) {
+  uint32_t carry = 0;
+  for (uint32_t e0 = 0; e0 < nEvents; e0 += blockDim.x) {
+    const uint32_t e = e0 + threadIdx.x;
+    const uint32_t v = e < nEvents ? min(ws.tmOff[size_t(e) * 16 + nh], ws.cap.multiplicity) : 0u;
+    uint32_t tot;
+    const uint32_t x = blockExclusiveScan(v, scanSh, &tot);
+    if (e < nEvents) pre[e] = carry + x;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) pre[nEvents] = carry;
+  __syncthreads();
+  return pre[nEvents];
+}
+
 // one thread per (tuple of the multiplicity bin nh); fits the first N hits
 template <int N, int kMode = kFitBrokenLine>
-__device__ __forceinline__ void blFitBin(const DeviceES& es, const Workspace& ws, uint32_t nh) {
-  uint32_t e = blockIdx.y;
-  const uint32_t* tm = ws.tmOff + size_t(e) * 16;
-  uint32_t size = min(tm[nh], ws.cap.multiplicity);
-  uint32_t start = tm[8 + nh];
-  const uint32_t* bins = ws.tmBins + size_t(e) * ws.cap.tuples;
-  const uint32_t* toff = ws.tupleOff + size_t(e) * (ws.cap.tuples + 1);
-  const uint32_t* th = ws.tupleHits + size_t(e) * ws.cap.tupleHits();
-  size_t hb = size_t(e) * ws.cap.hits;
-  size_t tb = size_t(e) * ws.cap.tuples;
+__device__ __forceinline__ void blFitBin(const DeviceES& es, const Workspace& ws, uint32_t nh, uint32_t nEvents,
+                                         uint32_t* pre, uint32_t* scanSh) {
+  const uint32_t total = fitBinPrefix(ws, nh, nEvents, pre, scanSh);
   const double B = double(float(0.0114256972711507));
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < size; k += gridDim.x * blockDim.x) {
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    // the event of flat item g: the last e with pre[e] <= g (empty events skipped)
+    uint32_t lo = 0, hi = nEvents;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (pre[mid] <= g)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const uint32_t e = lo, k = g - pre[lo];
+    const uint32_t start = ws.tmOff[size_t(e) * 16 + 8 + nh];
+    const uint32_t* bins = ws.tmBins + size_t(e) * ws.cap.tuples;
+    const uint32_t* toff = ws.tupleOff + size_t(e) * (ws.cap.tuples + 1);
+    const uint32_t* th = ws.tupleHits + size_t(e) * ws.cap.tupleHits();
+    const size_t hb = size_t(e) * ws.cap.hits;
+    const size_t tb = size_t(e) * ws.cap.tuples;
     uint32_t tkid = bins[start + k];
     const uint32_t* hid = th + toff[tkid];
     double H[3 * N];
@@ -437,36 +465,40 @@ __device__ __forceinline__ void blFitBin(const DeviceES& es, const Workspace& ws
 
 // the three multiplicity bins in one launch: blockIdx.z = 0, 1, 2 fits the
 // 3-hit tuples, the 4-hit tuples and the first 4 hits of the 5-hit tuples
-__global__ void __launch_bounds__(128, 4) kBLFit(DeviceES es, Workspace ws) {
+__global__ void __launch_bounds__(128, 4) kBLFit(DeviceES es, Workspace ws, uint32_t nEvents) {
+  __shared__ uint32_t pre[kFlatMaxEvents + 1], scanSh[33];
   if (blockIdx.z == 0)
-    blFitBin<3>(es, ws, 3);
+    blFitBin<3>(es, ws, 3, nEvents, pre, scanSh);
   else
-    blFitBin<4>(es, ws, 3 + blockIdx.z);
+    blFitBin<4>(es, ws, 3 + blockIdx.z, nEvents, pre, scanSh);
 }
 
 // the same bins through the Riemann fit (useRiemannFit,
 // CAHitNtupletGeneratorOnGPU.cc:116-120; RiemannFitOnGPU.cc:3-110)
-__global__ void __launch_bounds__(128) kRiemannFit(DeviceES es, Workspace ws) {
+__global__ void __launch_bounds__(128) kRiemannFit(DeviceES es, Workspace ws, uint32_t nEvents) {
+  __shared__ uint32_t pre[kFlatMaxEvents + 1], scanSh[33];
   if (blockIdx.z == 0)
-    blFitBin<3, kFitRiemann>(es, ws, 3);
+    blFitBin<3, kFitRiemann>(es, ws, 3, nEvents, pre, scanSh);
   else
-    blFitBin<4, kFitRiemann>(es, ws, 3 + blockIdx.z);
+    blFitBin<4, kFitRiemann>(es, ws, 3 + blockIdx.z, nEvents, pre, scanSh);
 }
 
 // the mixed-precision variants of both fits inside the chain (pg_config
 // mixed_fit): a precision choice beside the reference's FP64 fits, whose
 // effect on the chain's quality codes and vertices is measured against them
-__global__ void __launch_bounds__(128, 4) kBLFitMixed(DeviceES es, Workspace ws) {
+__global__ void __launch_bounds__(128, 4) kBLFitMixed(DeviceES es, Workspace ws, uint32_t nEvents) {
+  __shared__ uint32_t pre[kFlatMaxEvents + 1], scanSh[33];
   if (blockIdx.z == 0)
-    blFitBin<3, kFitBrokenLineMixed>(es, ws, 3);
+    blFitBin<3, kFitBrokenLineMixed>(es, ws, 3, nEvents, pre, scanSh);
   else
-    blFitBin<4, kFitBrokenLineMixed>(es, ws, 3 + blockIdx.z);
+    blFitBin<4, kFitBrokenLineMixed>(es, ws, 3 + blockIdx.z, nEvents, pre, scanSh);
 }
-__global__ void __launch_bounds__(128) kRiemannFitMixed(DeviceES es, Workspace ws) {
+__global__ void __launch_bounds__(128) kRiemannFitMixed(DeviceES es, Workspace ws, uint32_t nEvents) {
+  __shared__ uint32_t pre[kFlatMaxEvents + 1], scanSh[33];
   if (blockIdx.z == 0)
-    blFitBin<3, kFitRiemannMixed>(es, ws, 3);
+    blFitBin<3, kFitRiemannMixed>(es, ws, 3, nEvents, pre, scanSh);
   else
-    blFitBin<4, kFitRiemannMixed>(es, ws, 3 + blockIdx.z);
+    blFitBin<4, kFitRiemannMixed>(es, ws, 3 + blockIdx.z, nEvents, pre, scanSh);
 }
 
 // standalone fit of externally supplied tuples (fit workload and tests)
@@ -501,15 +533,17 @@ cudaError_t runFits(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStr
   PG_PROBED("kFitZero", stream, kFitZero<<<dim3(tunedGrid(ws, kTuneFitZero, g.x), nEvents), 256, 0, stream>>>(ws));
   // FP64-bound: enough warps per SM to cover the double-precision latency
   const uint32_t fx = nEvents >= 32 ? 16 : (nEvents >= 8 ? 64 : 296);
-  const dim3 fg(tunedGrid(ws, kTuneFit, fx), nEvents, 3);
+  // one flat grid over the batch's tuples (z: the multiplicity bin), as many
+  // blocks as a grid row per event would have
+  const dim3 fg(tunedGrid(ws, kTuneFit, fx) * nEvents, 1, 3);
   if (riemann && ws.ca.mixedFit)
-    PG_PROBED("kRiemannFitMixed", stream, kRiemannFitMixed<<<fg, 128, 0, stream>>>(es, ws));
+    PG_PROBED("kRiemannFitMixed", stream, kRiemannFitMixed<<<fg, 128, 0, stream>>>(es, ws, nEvents));
   else if (riemann)
-    PG_PROBED("kRiemannFit", stream, kRiemannFit<<<fg, 128, 0, stream>>>(es, ws));
+    PG_PROBED("kRiemannFit", stream, kRiemannFit<<<fg, 128, 0, stream>>>(es, ws, nEvents));
   else if (ws.ca.mixedFit)
-    PG_PROBED("kBLFitMixed", stream, kBLFitMixed<<<fg, 128, 0, stream>>>(es, ws));
+    PG_PROBED("kBLFitMixed", stream, kBLFitMixed<<<fg, 128, 0, stream>>>(es, ws, nEvents));
   else
-    PG_PROBED("kBLFit", stream, kBLFit<<<fg, 128, 0, stream>>>(es, ws));
+    PG_PROBED("kBLFit", stream, kBLFit<<<fg, 128, 0, stream>>>(es, ws, nEvents));
   return cudaGetLastError();
 }
 

@@ -29,10 +29,13 @@ static_assert(kVtxScratchAWords <= 2 * size_t(PF_MAX_DOUBLETS_PARAM) &&
               "vertex scratch exceeds the per-event scratchA/scratchB stride");
 constexpr int kVtxThreads = 1024;
 // events with at most this many vertex tracks keep every per-track array in
-// shared memory (40 bytes per track); larger ones use the global scratch
-constexpr uint32_t kSmemTracks = 4096;
+// shared memory (40 bytes per track: 220 KB, about the vertex tracks of a
+// PU 250 event); larger ones use the global scratch
+constexpr uint32_t kSmemTracks = 5500;
 constexpr size_t kTrackBytes = 9 * 4 + 2 + 2;
 constexpr size_t kVtxSmemBytes = kSmemTracks * kTrackBytes;
+// with the kernel's static shared memory (about 9.4 KB) within the 227 KB of a block
+static_assert(kVtxSmemBytes + 10 * 1024 <= 227 * 1024, "vertex shared memory");
 constexpr uint32_t kVtxCtas = 4;  // CTAs per event in a small batch
 
 struct VtxScratch {
@@ -370,6 +373,7 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
   __shared__ uint32_t hoff[257];
   __shared__ uint32_t vOff[kMaxVtx + 1], vCur[kMaxVtx + 1];
   __shared__ uint32_t sNt, sFound, sGuard, sNv;
+  __shared__ uint32_t sCtaCnt;  // tracks this CTA selected
   __shared__ int sFlag;
   const uint32_t e = blockIdx.y;
   const uint32_t lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -397,61 +401,104 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
   }
   __syncthreads();
   const uint32_t guard = sGuard;
+  // the selection of tuple t, its four loads issued together
   auto selected = [&](uint32_t t) {
     const uint32_t nh = toff[t + 1] - toff[t];
-    return nh >= 4 && q[t] == 2 && !(pt[t] < 0.5f);
+    const uint8_t qt = q[t];
+    const float ptt = pt[t];
+    return (nh >= 4) & (qt == 2) & !(ptt < 0.5f);
   };
-  // each warp takes a contiguous range of tuples, 32 consecutive ones per
-  // step (coalesced loads); one block scan over the warps' counts places each
-  // warp's run, and a second walk writes its selected tracks in ascending
-  // order.  The selection of each step is kept as a bit when the range has at
-  // most 32 steps (up to 32768 tuples), else evaluated again.
+  // The cluster's CTAs split the tuples: CTA r takes [g0, g1).  Inside it each
+  // warp takes a contiguous range, 32 consecutive tuples per step (coalesced
+  // loads, four steps in flight).  Block scans over the warps' counts and the
+  // CTAs' counts place every run, and a second walk writes the selected tracks
+  // in ascending order (into every CTA's shared memory, or the global
+  // scratch).  The selection of each step is kept as a bit when the range has
+  // at most 32 steps, else evaluated again.
+  const uint32_t g0 = uint32_t(uint64_t(guard) * rank / P), g1 = uint32_t(uint64_t(guard) * (rank + 1) / P);
+  for (uint32_t t = g0 + threadIdx.x; t < g1; t += blockDim.x) idv[t] = -1;
   const uint32_t warp = threadIdx.x >> 5;
-  const uint32_t R = (guard + nw * 32 - 1) / (nw * 32) * 32;
-  const uint32_t w0 = min(guard, warp * R), w1 = min(guard, w0 + R);
-  const bool keepBits = R <= 32 * 32;
+  const uint32_t R = (g1 - g0 + nw * 32 - 1) / (nw * 32) * 32;
+  const uint32_t w0 = min(g1, g0 + warp * R), w1 = min(g1, w0 + R);
+  const uint32_t steps = (w1 - w0 + 31) / 32;
+  const bool keepBits = steps <= 32;
   uint32_t cnt = 0, bits = 0;
-  for (uint32_t k = 0; w0 + k * 32 < w1; ++k) {
-    const uint32_t t = w0 + k * 32 + lane;
-    bool sel = false;
-    if (t < w1) {
-      if (rank == 0) idv[t] = -1;
-      sel = selected(t);
+  for (uint32_t k = 0; k < steps; k += 4) {
+    bool sel[4];
+#pragma unroll
+    for (uint32_t u = 0; u < 4; ++u) {
+      const uint32_t t = w0 + (k + u) * 32 + lane;
+      sel[u] = k + u < steps && t < w1 && selected(t);
     }
-    if (sel && keepBits) bits |= 1u << k;
-    cnt += __popc(__ballot_sync(0xffffffffu, sel));
+#pragma unroll
+    for (uint32_t u = 0; u < 4; ++u) {
+      if (sel[u] && keepBits) bits |= 1u << (k + u);
+      cnt += __popc(__ballot_sync(0xffffffffu, sel[u]));
+    }
   }
-  uint32_t total;
-  const uint32_t first = __shfl_sync(0xffffffffu, blockExclusiveScan(lane == 0 ? cnt : 0u, scanSh, &total), 0);
+  uint32_t ctaTotal;
+  const uint32_t first = __shfl_sync(0xffffffffu, blockExclusiveScan(lane == 0 ? cnt : 0u, scanSh, &ctaTotal), 0);
+  if (threadIdx.x == 0) sCtaCnt = ctaTotal;
+  // every CTA has started and holds its count (and every tuple's idv is
+  // cleared): the counts are read across the cluster
+  cl.sync();
+  uint32_t base = 0, total = 0;
+  for (uint32_t r = 0; r < P; ++r) {
+    const uint32_t n = *cl.map_shared_rank(&sCtaCnt, r);
+    base += r < rank ? n : 0u;
+    total += n;
+  }
   if (threadIdx.x == 0) {
     sNt = min(total, kMaxVtxTracks);
     // beyond ZVertexSoA::MAXTRACKS the reference writes past its arrays
     if (total > kMaxVtxTracks && rank == 0) atomicOr(&c->flags, kFlagVtxOverflow);
   }
   __syncthreads();
-  // the count decides where the per-track arrays live; the neighbour
-  // searches are split among the cluster's CTAs when they are in shared memory
-  const VtxScratch s = sNt <= kSmemTracks ? carve(vsm, kSmemTracks) : scratchOf(ws, e);
-  const bool split = P > 1 && sNt <= kSmemTracks && algo == 0;
-  const bool active = split || rank == 0;
+  // The count decides where the per-track arrays live: in the shared memory
+  // of every CTA, or once in the global scratch.  The neighbour searches are
+  // split among the cluster's CTAs (the density clusterer); their results go
+  // to every CTA's shared memory, or once to the global scratch.
+  const bool smemPath = sNt <= kSmemTracks;
+  const VtxScratch s = smemPath ? carve(vsm, kSmemTracks) : scratchOf(ws, e);
+  const bool split = P > 1 && algo == 0;
+  const bool remote = split && smemPath;       // results written into every CTA
+  const bool active = split || rank == 0;      // CTAs that take part in the searches
+  const bool writer = smemPath || rank == 0;   // CTAs that build their own track arrays
   const uint32_t wFirst = split ? rank * nw : 0, wStride = split ? P * nw : nw;
-  if (active) {
-    uint32_t pos = first;
-    for (uint32_t k = 0; w0 + k * 32 < w1; ++k) {
-      const uint32_t t = w0 + k * 32 + lane;
-      const bool sel = keepBits ? ((bits >> k) & 1u) != 0 : (t < w1 && selected(t));
-      const uint32_t m = __ballot_sync(0xffffffffu, sel);
-      const uint32_t it = pos + __popc(m & lanemaskLt());
-      if (sel && it < kMaxVtxTracks) {
-        s.itrk[it] = t;
-        s.zt[it] = st[size_t(t) * 5 + 4];
-        s.ezt2[it] = cov[size_t(t) * 15 + 14];
-        s.ptt2[it] = pt[t] * pt[t];
+  // every CTA places its selected tracks; in the shared-memory path each
+  // track goes to every CTA that works on it (all with the split, else rank 0)
+  const uint32_t nDst = smemPath ? (split ? P : 1u) : 1u;
+  {
+    uint32_t pos = base + first;
+    for (uint32_t k = 0; k < steps; k += 4) {
+      bool sel[4];
+#pragma unroll
+      for (uint32_t u = 0; u < 4; ++u) {
+        const uint32_t t = w0 + (k + u) * 32 + lane;
+        sel[u] = keepBits ? ((bits >> (k + u)) & 1u) != 0 : (k + u < steps && t < w1 && selected(t));
       }
-      pos += __popc(m);
+#pragma unroll
+      for (uint32_t u = 0; u < 4; ++u) {
+        const uint32_t t = w0 + (k + u) * 32 + lane;
+        const uint32_t m = __ballot_sync(0xffffffffu, sel[u]);
+        const uint32_t it = pos + __popc(m & lanemaskLt());
+        if (sel[u] && it < kMaxVtxTracks) {
+          const float z = st[size_t(t) * 5 + 4], ez = cov[size_t(t) * 15 + 14], p2 = pt[t] * pt[t];
+          for (uint32_t d = 0; d < nDst; ++d) {
+            VtxScratch sd = s;
+            if (smemPath) sd = carve(reinterpret_cast<char*>(cl.map_shared_rank(vsm, split ? d : 0u)), kSmemTracks);
+            sd.itrk[it] = t;
+            sd.zt[it] = z;
+            sd.ezt2[it] = ez;
+            sd.ptt2[it] = p2;
+          }
+        }
+        pos += __popc(m);
+      }
     }
   }
-  __syncthreads();
+  // every track array is complete
+  cl.sync();
   const uint32_t nt = sNt;
   const float eps = 0.07f, errmax = 0.01f, chi2max = 9.f;
   const float er2mx = errmax * errmax;
@@ -463,10 +510,12 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
   for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
     int iz = int(double(s.zt[i]) * 10.);
     iz = min(max(iz, -128), 127);
-    s.izt[i] = uint8_t(iz + 128);
-    atomicAdd(&hoff[s.izt[i]], 1u);
-    s.iv[i] = int32_t(i);
-    s.nn[i] = 0;
+    atomicAdd(&hoff[iz + 128], 1u);
+    if (writer) {
+      s.izt[i] = uint8_t(iz + 128);
+      s.iv[i] = int32_t(i);
+      s.nn[i] = 0;
+    }
   }
   __syncthreads();
   {
@@ -483,7 +532,7 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
   __syncthreads();
   // the serial fill stores each bin in descending track order: one warp per
   // bin walks the tracks from the last one down
-  for (uint32_t b = threadIdx.x >> 5; b < 256; b += nw) {
+  for (uint32_t b = threadIdx.x >> 5; writer && b < 256; b += nw) {
     uint32_t pos = hoff[b];
     const uint32_t end = hoff[b + 1];
     // 128 tracks per step: the four loads issue together
@@ -503,15 +552,16 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
     }
   }
   }
-  // every CTA of the cluster has started and cleared its own neighbour counts
-  // before any CTA writes counts into the others' shared memory
+  // every CTA of the cluster has cleared its own neighbour counts before any
+  // CTA writes counts into the others' shared memory; the global scratch's
+  // histogram is complete
   cl.sync();
   if (active) {
   // neighbour counts: one warp per track, the lanes take 32 consecutive
   // entries of the track's three bins at a time
   for (uint32_t i = wFirst + (threadIdx.x >> 5); i < nt; i += wStride) {
     if (s.ezt2[i] > er2mx) {
-      if (split ? lane < P : lane == 0) *(split ? cl.map_shared_rank(s.nn, lane) + i : s.nn + i) = 0;
+      if (remote ? lane < P : lane == 0) *(remote ? cl.map_shared_rank(s.nn, lane) + i : s.nn + i) = 0;
       continue;
     }
     const int b0 = max(0, int(s.izt[i]) - 1), b1 = min(255, int(s.izt[i]) + 1);
@@ -524,7 +574,7 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
       cnt += (i != j && !(dist > eps) && (algo == 1 || !(dist * dist > chi2max * (ei + s.ezt2[j])))) ? 1u : 0u;
     }
     cnt = __reduce_add_sync(0xffffffffu, cnt);
-    if (split ? lane < P : lane == 0) *(split ? cl.map_shared_rank(s.nn, lane) + i : s.nn + i) = int32_t(cnt);
+    if (remote ? lane < P : lane == 0) *(remote ? cl.map_shared_rank(s.nn, lane) + i : s.nn + i) = int32_t(cnt);
   }
   }
   // every CTA holds every neighbour count
@@ -575,7 +625,7 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
       best = int32_t(s.hbins[lastOk]);
     else if (bestKey != ~0ull)
       best = int32_t(s.hbins[0xffffffffu - uint32_t(bestKey & 0xffffffffu)]);
-    if (split ? lane < P : lane == 0) *(split ? cl.map_shared_rank(s.iv, lane) + i : s.iv + i) = best;
+    if (remote ? lane < P : lane == 0) *(remote ? cl.map_shared_rank(s.iv, lane) + i : s.iv + i) = best;
   }
   }
   // every CTA holds every closest denser neighbour; only rank 0 goes on,

@@ -184,6 +184,7 @@ enum ScanCall : uint32_t {
   kScanCalls
 };
 constexpr uint32_t kScanTile = 4096;  // elements per tile of the single-pass scan
+constexpr uint32_t kFlatMaxEvents = 1024;  // events per batch (kernels with one flat grid over the batch)
 
 // CAHitNtupletGeneratorOnGPU parameters that select among the algorithm's
 // variants (CAHitNtupletGeneratorOnGPU.cc:45-66; CAHitNtupletGeneratorKernels.cc:52-70)

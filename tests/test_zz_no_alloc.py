@@ -5,7 +5,7 @@ device).
 
 pg_vertices_noalloc, given the chain's own track SoA, must return the
 chain's vertices (pg_process_batch products), and on a track set of more
-than 4096 vertex tracks -- large enough for the vertex kernel to work in the
+than 5500 vertex tracks -- large enough for the vertex kernel to work in the
 static scratch instead of shared memory -- the serial vertex finder's
 result.  Everything runs twice in a row, since every call reuses the same
 static scratch."""
@@ -84,7 +84,7 @@ def test_noalloc_vertices_equal_chain_vertices_twice(chain_products):
 
 def test_noalloc_large_track_set_twice(large_track_set):
     nh = np.diff(large_track_set["tupleOff"].astype(np.int64))
-    assert int((nh >= 4).sum()) > 4096  # beyond the kernel's shared-memory size: the static scratch is used
+    assert int((nh >= 4).sum()) > 5500  # beyond the kernel's shared-memory size: the static scratch is used
     for call in range(2):
         _run(large_track_set)
 

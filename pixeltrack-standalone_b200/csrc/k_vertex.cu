@@ -110,23 +110,48 @@ __device__ void groupByVertex(const VtxScratch& s, uint32_t nt, uint32_t nv, uin
     carry += tot;
   }
   __syncthreads();
-  // ordered fill: one warp per vertex walks the tracks in ascending order
+  // ordered fill (ascending track order inside each vertex).  Few vertices:
+  // one warp per vertex walks the tracks, 128 at a time, until it has found
+  // them all.  Many: warp w owns a range of vertices and walks the tracks
+  // once, 32 at a time; lanes of the same vertex are ranked among themselves
+  // (match) and its cursor (vCur) advances by their number.
   const uint32_t lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (uint32_t v = threadIdx.x >> 5; v < nv; v += nw) {
-    uint32_t pos = vOff[v];
-    const uint32_t end = vOff[v + 1];
-    for (uint32_t i0 = 0; i0 < nt && pos < end; i0 += 128) {
-      bool in[4];
+  if (nv <= 2 * nw) {
+    for (uint32_t v = threadIdx.x >> 5; v < nv; v += nw) {
+      uint32_t pos = vOff[v];
+      const uint32_t end = vOff[v + 1];
+      for (uint32_t i0 = 0; i0 < nt && pos < end; i0 += 128) {
+        bool in[4];
 #pragma unroll
-      for (uint32_t u = 0; u < 4; ++u) {
-        const uint32_t i = i0 + u * 32 + lane;
-        in[u] = i < nt && s.iv[i] == int32_t(v);
+        for (uint32_t u = 0; u < 4; ++u) {
+          const uint32_t i = i0 + u * 32 + lane;
+          in[u] = i < nt && s.iv[i] == int32_t(v);
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < 4; ++u) {
+          const uint32_t m = __ballot_sync(0xffffffffu, in[u]);
+          if (in[u]) s.list[pos + __popc(m & lanemaskLt())] = i0 + u * 32 + lane;
+          pos += __popc(m);
+        }
       }
-#pragma unroll
-      for (uint32_t u = 0; u < 4; ++u) {
-        const uint32_t m = __ballot_sync(0xffffffffu, in[u]);
-        if (in[u]) s.list[pos + __popc(m & lanemaskLt())] = i0 + u * 32 + lane;
-        pos += __popc(m);
+    }
+  } else {
+    for (uint32_t v = threadIdx.x; v < nv; v += blockDim.x) vCur[v] = vOff[v];
+    __syncthreads();
+    const uint32_t vpw = (nv + nw - 1) / nw, vLo = (threadIdx.x >> 5) * vpw, vHi = min(nv, vLo + vpw);
+    for (uint32_t i0 = 0; i0 < nt && vLo < vHi; i0 += 32) {
+      const uint32_t i = i0 + lane;
+      const int32_t v = i < nt ? s.iv[i] : -1;
+      const bool in = v >= int32_t(vLo) && v < int32_t(vHi);
+      const uint32_t m = __ballot_sync(0xffffffffu, in);
+      if (m) {
+        const uint32_t peers = __match_any_sync(0xffffffffu, in ? uint32_t(v) : 0xffffffffu) & m;
+        if (in) {
+          s.list[vCur[v] + __popc(peers & lanemaskLt())] = i;
+          __syncwarp(peers);
+          if ((peers & lanemaskLt()) == 0) vCur[v] += __popc(peers);
+        }
+        __syncwarp();
       }
     }
   }
@@ -530,25 +555,42 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
     }
   }
   __syncthreads();
-  // the serial fill stores each bin in descending track order: one warp per
-  // bin walks the tracks from the last one down
-  for (uint32_t b = threadIdx.x >> 5; writer && b < 256; b += nw) {
-    uint32_t pos = hoff[b];
-    const uint32_t end = hoff[b + 1];
-    // 128 tracks per step: the four loads issue together
-    for (uint32_t r0 = 0; r0 < nt && pos < end; r0 += 128) {
-      bool in[4];
-#pragma unroll
-      for (uint32_t u = 0; u < 4; ++u) {
-        const uint32_t r = r0 + u * 32 + lane;
-        in[u] = r < nt && s.izt[nt - 1 - r] == b;
+  // the serial fill stores each bin in descending track order.  Warp w owns
+  // bins [8 w, 8 w + 8) and walks the tracks once from the last one down,
+  // 32 at a time: lanes holding the same bin are ranked among themselves
+  // (match), and the bin's cursor advances by their number.
+  if (writer) {
+    uint32_t* cur = vCur;  // free until the vertex fit: per-bin fill cursors
+    for (uint32_t b = threadIdx.x; b < 256; b += blockDim.x) cur[b] = hoff[b];
+    __syncthreads();
+    const uint32_t bpw = (256 + nw - 1) / nw, bLo = (threadIdx.x >> 5) * bpw, bHi = min(256u, bLo + bpw);
+    for (uint32_t r0 = 0; r0 < nt && bLo < bHi; r0 += 32) {
+      const uint32_t r = r0 + lane;
+      const uint32_t i = nt - 1 - r;
+      const uint32_t b = r < nt ? s.izt[i] : 0xffffu;
+      const bool in = b >= bLo && b < bHi;
+      const uint32_t m = __ballot_sync(0xffffffffu, in);
+      if (m) {
+        const uint32_t peers = __match_any_sync(0xffffffffu, in ? b : 0xffffffffu) & m;
+        if (in) {
+          const uint32_t pos = cur[b] + __popc(peers & lanemaskLt());
+          s.hbins[pos] = uint16_t(i);
+          __syncwarp(peers);
+          if ((peers & lanemaskLt()) == 0) cur[b] += __popc(peers);
+        }
+        __syncwarp();
       }
-#pragma unroll
-      for (uint32_t u = 0; u < 4; ++u) {
-        const uint32_t m = __ballot_sync(0xffffffffu, in[u]);
-        if (in[u]) s.hbins[pos + __popc(m & lanemaskLt())] = uint16_t(nt - 1 - (r0 + u * 32 + lane));
-        pos += __popc(m);
-      }
+    }
+    __syncthreads();
+    // z and its error of every track in histogram order, so that the
+    // neighbour searches read their candidates contiguously (zz and list are
+    // free until the fits)
+    float* zP = s.zz;
+    float* eP = reinterpret_cast<float*>(s.list);
+    for (uint32_t p = threadIdx.x; p < nt; p += blockDim.x) {
+      const uint32_t j = s.hbins[p];
+      zP[p] = s.zt[j];
+      eP[p] = s.ezt2[j];
     }
   }
   }
@@ -556,25 +598,32 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
   // CTA writes counts into the others' shared memory; the global scratch's
   // histogram is complete
   cl.sync();
+  // candidates in histogram order: z, its error and (below) the neighbour count
+  const float* zP = s.zz;
+  const float* eP = reinterpret_cast<const float*>(s.list);
+  int32_t* nP = s.root;  // free until the percolation
   if (active) {
-  // neighbour counts: one warp per track, the lanes take 32 consecutive
-  // entries of the track's three bins at a time
-  for (uint32_t i = wFirst + (threadIdx.x >> 5); i < nt; i += wStride) {
-    if (s.ezt2[i] > er2mx) {
-      if (remote ? lane < P : lane == 0) *(remote ? cl.map_shared_rank(s.nn, lane) + i : s.nn + i) = 0;
-      continue;
-    }
-    const int b0 = max(0, int(s.izt[i]) - 1), b1 = min(255, int(s.izt[i]) + 1);
-    const uint32_t pb = hoff[b0], pe = hoff[b1 + 1];
-    const float zi = s.zt[i], ei = s.ezt2[i];
+  // neighbour counts: one warp per track (taken in histogram order), the
+  // lanes take 32 consecutive entries of the track's three bins at a time.
+  // Each count is kept by track (nn) and by histogram position (nP).
+  for (uint32_t pi = wFirst + (threadIdx.x >> 5); pi < nt; pi += wStride) {
+    const uint32_t i = s.hbins[pi];
+    const float zi = zP[pi], ei = eP[pi];
     uint32_t cnt = 0;  // per lane, summed once per track
-    for (uint32_t p = pb + lane; p < pe; p += 32) {
-      const uint32_t j = s.hbins[p];
-      const float dist = fabsf(zi - s.zt[j]);
-      cnt += (i != j && !(dist > eps) && (algo == 1 || !(dist * dist > chi2max * (ei + s.ezt2[j])))) ? 1u : 0u;
+    if (!(ei > er2mx)) {
+      const int b0 = max(0, int(s.izt[i]) - 1), b1 = min(255, int(s.izt[i]) + 1);
+      const uint32_t pb = hoff[b0], pe = hoff[b1 + 1];
+      for (uint32_t p = pb + lane; p < pe; p += 32) {
+        const uint32_t j = s.hbins[p];
+        const float dist = fabsf(zi - zP[p]);
+        cnt += (i != j && !(dist > eps) && (algo == 1 || !(dist * dist > chi2max * (ei + eP[p])))) ? 1u : 0u;
+      }
+      cnt = __reduce_add_sync(0xffffffffu, cnt);
     }
-    cnt = __reduce_add_sync(0xffffffffu, cnt);
-    if (remote ? lane < P : lane == 0) *(remote ? cl.map_shared_rank(s.nn, lane) + i : s.nn + i) = int32_t(cnt);
+    if (remote ? lane < P : lane == 0) {
+      *(remote ? cl.map_shared_rank(s.nn, lane) + i : s.nn + i) = int32_t(cnt);
+      *(remote ? cl.map_shared_rank(nP, lane) + pi : nP + pi) = int32_t(cnt);
+    }
   }
   }
   // every CTA holds every neighbour count
@@ -588,22 +637,22 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
   // then on every denser, chi2-compatible candidate is taken, so the result
   // is the last of those.  The warp evaluates both, the first as the minimum
   // of (distance, reversed position).
-  for (uint32_t i = wFirst + (threadIdx.x >> 5); i < nt; i += wStride) {
+  for (uint32_t pi = wFirst + (threadIdx.x >> 5); pi < nt; pi += wStride) {
+    const uint32_t i = s.hbins[pi];
     const int b0 = max(0, int(s.izt[i]) - 1), b1 = min(255, int(s.izt[i]) + 1);
     const uint32_t pb = hoff[b0], pe = hoff[b1 + 1];
-    const float zi = s.zt[i], ei = s.ezt2[i];
-    const int32_t ni = s.nn[i];
+    const float zi = zP[pi], ei = eP[pi];
+    const int32_t ni = nP[pi];
     // per-lane running results, combined once per track
     unsigned long long bestKey = ~0ull;
     bool nanLane = false;
     int32_t lastOk = -1;
     for (uint32_t p = pb + lane; p < pe; p += 32) {
-      const uint32_t j = s.hbins[p];
-      const int32_t nj = s.nn[j];
-      const float zj = s.zt[j];
+      const int32_t nj = nP[p];
+      const float zj = zP[p];
       const float dist = fabsf(zi - zj);
       const bool dens = !(nj < ni) && !(nj == ni && zj >= zi);
-      const bool dc = dens && !(dist * dist > chi2max * (ei + s.ezt2[j]));
+      const bool dc = dens && !(dist * dist > chi2max * (ei + eP[p]));
       nanLane |= dens && isnan(dist);
       if (dc) {
         lastOk = int32_t(p);
@@ -760,12 +809,13 @@ __global__ void __launch_bounds__(kVtxThreads) kVertices(Workspace ws, int algo)
     if (threadIdx.x == 0) sNv = found + carry;
   }
   __syncthreads();
-  for (uint32_t kv = threadIdx.x; kv < found; kv += blockDim.x) {
+  // tracks of the split-off halves to their new vertices (warp per vertex)
+  for (uint32_t kv = threadIdx.x >> 5; kv < found; kv += nw) {
     if (vCur[kv] == 0) continue;
-    uint32_t igv = vCur[kv] - 1;
-    uint32_t b = vOff[kv], n = vOff[kv + 1] - b;
-    for (uint32_t k = 0; k < n; ++k) {
-      uint32_t i = s.list[b + k];
+    const uint32_t igv = vCur[kv] - 1;
+    const uint32_t b = vOff[kv], n = vOff[kv + 1] - b;
+    for (uint32_t k = lane; k < n; k += 32) {
+      const uint32_t i = s.list[b + k];
       if (s.iv[i] == int32_t(kv) && s.newV[i] == 1) s.iv[i] = int32_t(igv);
     }
   }

@@ -604,8 +604,8 @@ def run_ours(a):
             best_ok = None
             # the default number of batches in flight over the whole load
             # range, then fewer in flight (larger batches) over the upper part
-            for slots_n, fracs in ((a.serve_slots, (0.2, 0.35, 0.5, 0.6, 0.65, 0.7, 0.75, 0.8, 0.9)),
-                                   (4, (0.65, 0.7, 0.75, 0.8, 0.85)), (3, (0.65, 0.7, 0.75, 0.8, 0.85))):
+            knee = (0.7, 0.725, 0.75, 0.775, 0.8, 0.825, 0.85)
+            for slots_n, fracs in ((a.serve_slots, (0.2, 0.35, 0.5, 0.6, 0.65) + knee + (0.9,)), (4, knee), (3, knee)):
                 if slots_n in by_slots:
                     continue
                 sc = pixgpu.Chain(det.es, max_events=a.serve_batch, max_words_per_batch=int(max(nw)) * a.serve_batch,

@@ -5,6 +5,7 @@ chain.  Events are generated once, uploaded into the device pool, and the
 chain is launched `--repeat` times over batches of `--batch` events.
 
   python pixeltrack-standalone_b200/run_events.py --events 64 --batch 64 --pu 50 --repeat 3
+  python pixeltrack-standalone_b200/run_events.py --events 64 --batch 64 --pu 20 --pu-max 200 --caps wide
 
 --probe adds, after the timed loop, the median wall latency of one batch
 (submit to results on the host) and the device time of every kernel of a
@@ -17,6 +18,8 @@ import os
 import sys
 import time
 
+import numpy as np
+
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 import pixgpu  # noqa: E402
 
@@ -26,6 +29,10 @@ def main():
     p.add_argument("--events", type=int, default=64)
     p.add_argument("--batch", type=int, default=64)
     p.add_argument("--pu", type=float, default=50)
+    p.add_argument("--pu-max", type=float, default=0,
+                   help="uneven pileup: event k takes a seeded PU uniform in [--pu, --pu-max]")
+    p.add_argument("--caps", choices=["reference", "wide"], default="reference",
+                   help="container capacities: the reference's, or pixgpu.WIDE_CAPS (high pileup)")
     p.add_argument("--repeat", type=int, default=3)
     p.add_argument("--slots", type=int, default=1)
     p.add_argument("--seed", type=int, default=pixgpu.BASE_SEED + 1000)
@@ -41,13 +48,15 @@ def main():
                    help="launch-shape cache to load ('' for the default shapes)")
     a = p.parse_args()
     det = pixgpu.Detector()
+    rng = np.random.default_rng(a.seed)
+    pus = rng.uniform(a.pu, a.pu_max, a.events) if a.pu_max > a.pu else np.full(a.events, a.pu)
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
-        raws = list(ex.map(lambda k: det.event(a.seed + k, a.pu, model=a.model), range(a.events)))
+        raws = list(ex.map(lambda k: det.event(a.seed + k, float(pus[k]), model=a.model), range(a.events)))
     words = [len(r) // 4 for r in raws]
     device_scan = a.fed_scan == "device"
     chain = pixgpu.Chain(det.es, max_events=a.batch, max_words_per_batch=max(words) * a.batch + 1024, slots=a.slots,
-                         use_graphs=not a.no_graphs, pool_words=0 if device_scan else sum(words) + 64 * len(words) + 4096,
-                         fed_scan=a.fed_scan)
+                         use_graphs=not a.no_graphs, pool_words=0 if device_scan else max(sum(words) + 64 * len(words), 400000) + 4096,
+                         fed_scan=a.fed_scan, caps=pixgpu.WIDE_CAPS if a.caps == "wide" else None)
     if a.tuning and os.path.exists(a.tuning):
         chain.tune_load(a.tuning)
     if device_scan:
@@ -68,7 +77,8 @@ def main():
             done += len(b)
             chain.release(s)
     dt = time.perf_counter() - t0
-    print("processed %d events (PU %g, batches of %d) in %.3f s: %.1f events/s" % (done, a.pu, a.batch, dt, done / dt))
+    pu = ("%g-%g" % (a.pu, a.pu_max)) if a.pu_max > a.pu else "%g" % a.pu
+    print("processed %d events (PU %s, batches of %d) in %.3f s: %.1f events/s" % (done, pu, a.batch, dt, done / dt))
     if a.probe:
         lat = []
         for b in batches * 3:

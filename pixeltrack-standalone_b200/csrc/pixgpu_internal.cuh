@@ -142,9 +142,13 @@ __device__ __forceinline__ uint32_t cutNear(double a, double b) {
 // (exact for subnormal results), so a rounded difference above 2^-21 of the
 // larger magnitude (a power-of-two scaling, exact for normal results) means
 // the exact test fails.  NaN operands reach the exact test, which fails.
+// The double-precision test is out of line: it is rarely reached, and
+// inlined it cost the hot candidate loops registers and scheduling (measured:
+// doublet count 601 -> 525 us per 64-event batch).
+static __device__ __noinline__ uint32_t cutNearExact(float a, float b) { return cutNear(double(a), double(b)); }
 __device__ __forceinline__ uint32_t cutNear(float a, float b) {
   if (fabsf(a - b) > 4.76837158203125e-7f * fmaxf(fabsf(a), fabsf(b))) return 0u;
-  return cutNear(double(a), double(b));
+  return cutNearExact(a, b);
 }
 
 // ---------------------------------------------------------------- ES on device

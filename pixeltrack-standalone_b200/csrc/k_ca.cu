@@ -331,42 +331,67 @@ __global__ void __launch_bounds__(256, 5) kDoubletWrite(Workspace ws) {
   const uint32_t S = gridDim.x * wpb, w = blockIdx.x * wpb + (threadIdx.x >> 5);
   for (uint32_t r0 = 0; w + r0 * S < ntot; r0 += 32) {
     const uint32_t jl = w + (r0 + lane) * S;
-    uint32_t myBase = 0, myN = 0;
+    uint32_t myBase = 0, myN = 0, myAt = kNoTemp, myI = 0, myPair = 0;
+    float myZ = 0.f, myR = 0.f;
     if (jl < ntot) {
       myBase = off[jl];
       myN = myBase < ws.cap.cells ? min(off[jl + 1], ws.cap.cells) - myBase : 0u;
     }
-    uint32_t live = __ballot_sync(0xffffffffu, myN > 0);
-    while (live) {
-      const int l = __ffs(live) - 1;
-      live &= live - 1;
+    if (myN) {
+      myAt = slotStage[jl];
+      while (jl >= pt.pairCum[myPair]) ++myPair;
+      myI = (0 == myPair ? jl : jl - pt.pairCum[myPair - 1]) + pt.layerStart[cLayerPairs[2 * myPair]];
+      myZ = hh.zg[myI];
+      myR = hh.rg[myI];
+    }
+    auto put = [&](uint32_t idx, uint32_t i, uint32_t pair, float zi, float ri, uint32_t oi) {
+      ws.cellInner[cb + idx] = i;
+      ws.cellOuter[cb + idx] = oi;
+      ws.cellPair[cb + idx] = uint8_t(pair);
+      ws.cellDoubletId[cb + idx] = int32_t(idx);
+      ws.cellUsed[cb + idx] = 0;
+      ws.cellInnerZ[cb + idx] = zi;
+      ws.cellInnerR[cb + idx] = ri;
+      atomicAdd(&ohc[oi], 1u);
+    };
+    // The staged slots' doublets as one flat range over the warp's 32 slots,
+    // so that all lanes copy (a slot holds a few doublets): the lane of flat
+    // entry f is found by a binary search over the lanes' inclusive ends.
+    const uint32_t cnt = myAt != kNoTemp ? myN : 0u;
+    const uint32_t incl = warpInclusiveScan(cnt), excl = incl - cnt;
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    for (uint32_t f0 = 0; f0 < total; f0 += 32) {
+      const uint32_t f = f0 + lane;
+      uint32_t l = 0;
+#pragma unroll
+      for (uint32_t step = 16; step > 0; step >>= 1) {
+        const uint32_t v = __shfl_sync(0xffffffffu, incl, l + step - 1);
+        if (v <= f) l += step;
+      }
+      l &= 31u;  // lanes past the range (f >= total) land on 32; they only read
+      const uint32_t b = __shfl_sync(0xffffffffu, myBase, l), at = __shfl_sync(0xffffffffu, myAt, l);
+      const uint32_t x = __shfl_sync(0xffffffffu, excl, l), i = __shfl_sync(0xffffffffu, myI, l);
+      const uint32_t pair = __shfl_sync(0xffffffffu, myPair, l);
+      const float zi = __shfl_sync(0xffffffffu, myZ, l), ri = __shfl_sync(0xffffffffu, myR, l);
+      if (f < total) {
+        const uint32_t k = f - x;
+        put(b + k, i, pair, zi, ri, stage[at + k]);
+      }
+    }
+    // slots whose doublets did not fit the count pass's staging: found again
+    uint32_t redo = __ballot_sync(0xffffffffu, myN > 0 && myAt == kNoTemp);
+    while (redo) {
+      const int l = __ffs(redo) - 1;
+      redo &= redo - 1;
       const uint32_t j = w + (r0 + uint32_t(l)) * S;
       const uint32_t base = __shfl_sync(0xffffffffu, myBase, l), n = __shfl_sync(0xffffffffu, myN, l);
-      uint32_t pair = 0;
-      while (j >= pt.pairCum[pair]) ++pair;
-      const uint32_t i = (0 == pair ? j : j - pt.pairCum[pair - 1]) + pt.layerStart[cLayerPairs[2 * pair]];
-      const float zi = hh.zg[i], ri = hh.rg[i];
-      auto put = [&](uint32_t k, uint32_t oi) {
-        const uint32_t idx = base + k;
-        ws.cellInner[cb + idx] = i;
-        ws.cellOuter[cb + idx] = oi;
-        ws.cellPair[cb + idx] = uint8_t(pair);
-        ws.cellDoubletId[cb + idx] = int32_t(idx);
-        ws.cellUsed[cb + idx] = 0;
-        ws.cellInnerZ[cb + idx] = zi;
-        ws.cellInnerR[cb + idx] = ri;
-        atomicAdd(&ohc[oi], 1u);
-      };
-      const uint32_t at = slotStage[j];
-      if (at != kNoTemp) {
-        for (uint32_t k = lane; k < n; k += 32) put(k, stage[at + k]);
-      } else {
-        DoubletSeed d;
-        doubletSeed(pt, hh, j, d);
-        warpDoublets(d, rec, [&](uint32_t k, uint32_t oi) {
-          if (k < n) put(k, oi);
-        });
-      }
+      const uint32_t i = __shfl_sync(0xffffffffu, myI, l), pair = __shfl_sync(0xffffffffu, myPair, l);
+      const float zi = __shfl_sync(0xffffffffu, myZ, l), ri = __shfl_sync(0xffffffffu, myR, l);
+      DoubletSeed d;
+      doubletSeed(pt, hh, j, d);
+      warpDoublets(d, rec, [&](uint32_t k, uint32_t oi) {
+        if (k < n) put(base + k, i, pair, zi, ri, oi);
+      });
     }
   }
 }

@@ -677,52 +677,70 @@ __global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws, bool 
   uint8_t* su = suA[w];
   uint32_t* raw = rawA[w];
   uint32_t* sc = scA[w];
-  for (uint32_t h = blockIdx.x * kFishWarps + w; h < nHits; h += gridDim.x * kFishWarps) {
-    const uint32_t b = ohOff[h], s = min(ohOff[h + 1] - b, uint32_t(PF_MAX_CELLS_PER_HIT));
-    if (s < 2) continue;
-    const float xo = hh.xg[h], yo = hh.yg[h], zo = hh.zg[h];
-    // stage the hit's cells in ascending cell order (the list is filled
-    // unordered; up to 128 entries, at most 4 per lane)
-    for (uint32_t k = lane; k < s; k += 32) raw[k] = ohCells[b + k];
+  // One hit, done by the `width` lanes starting at lane g0 (the whole warp
+  // for up to 128 cells, a half warp for up to 16): stages the hit's cells in
+  // ascending cell order at sx..sc[o..] (the list is filled unordered) and
+  // compares them.
+  auto fishHit = [&](uint32_t h, uint32_t b, uint32_t s, uint32_t o, uint32_t g0, uint32_t width) {
+    const uint32_t gl = lane - g0;
+    const float xo = s ? hh.xg[h] : 0.f, yo = s ? hh.yg[h] : 0.f, zo = s ? hh.zg[h] : 0.f;
+    for (uint32_t k = gl; k < s; k += width) raw[o + k] = ohCells[b + k];
     __syncwarp();
-#pragma unroll
-    for (uint32_t j = 0; j < PF_MAX_CELLS_PER_HIT / 32; ++j) {
-      const uint32_t k = lane + 32 * j;
-      if (k < s) {
-        const uint32_t cell = raw[k];
-        uint32_t r = 0;
-        for (uint32_t m = 0; m < s; ++m) r += raw[m] < cell ? 1u : 0u;
-        const float4 rec = ohRec[b + k];
-        sx[r] = rec.x - xo;
-        sy[r] = rec.y - yo;
-        sz[r] = rec.z - zo;
-        sd[r] = ohDet[b + k];
-        su[r] = ws.cellUsed[cb + cell] && !(checkTrack && trkOff[cell + 1] == trkOff[cell]) ? 1 : 0;
-        sc[r] = cell;
-      }
+    for (uint32_t k = gl; k < s; k += width) {
+      const uint32_t cell = raw[o + k];
+      uint32_t r = 0;
+      for (uint32_t m = 0; m < s; ++m) r += raw[o + m] < cell ? 1u : 0u;
+      const float4 rec = ohRec[b + k];
+      sx[o + r] = rec.x - xo;
+      sy[o + r] = rec.y - yo;
+      sz[o + r] = rec.z - zo;
+      sd[o + r] = ohDet[b + k];
+      su[o + r] = ws.cellUsed[cb + cell] && !(checkTrack && trkOff[cell + 1] == trkOff[cell]) ? 1 : 0;
+      sc[o + r] = cell;
     }
     __syncwarp();
-    for (uint32_t ic = lane; ic < s; ic += 32) {
-      if (0 == su[ic]) continue;
-      const float xi = sx[ic], yi = sy[ic], zi = sz[ic];
-      const uint16_t di = sd[ic];
+    for (uint32_t ic = gl; ic < s; ic += width) {
+      if (0 == su[o + ic]) continue;
+      const float xi = sx[o + ic], yi = sy[o + ic], zi = sz[o + ic];
+      const uint16_t di = sd[o + ic];
       const float ni = xi * xi + yi * yi + zi * zi;
       for (uint32_t jc = ic + 1; jc < s; ++jc) {
-        if (0 == su[jc]) continue;
-        const float xj = sx[jc], yj = sy[jc], zj = sz[jc];
+        if (0 == su[o + jc]) continue;
+        const float xj = sx[o + jc], yj = sy[o + jc], zj = sz[o + jc];
         const float nj = xj * xj + yj * yj + zj * zj;
         const float cos12 = xi * xj + yi * yj + zi * zj;
-        if (di != sd[jc] && cos12 * cos12 >= 0.99999f * ni * nj) {
+        if (di != sd[o + jc] && cos12 * cos12 >= 0.99999f * ni * nj) {
           if (ni > nj) {
-            ws.cellDoubletId[cb + sc[ic]] = -1;
+            ws.cellDoubletId[cb + sc[o + ic]] = -1;
             break;
           } else {
-            ws.cellDoubletId[cb + sc[jc]] = -1;
+            ws.cellDoubletId[cb + sc[o + jc]] = -1;
           }
         }
       }
     }
     __syncwarp();
+  };
+  // Hits are taken two at a time: each half of the warp does one when both
+  // have at most 16 cells (most hits have about ten), else the warp does them
+  // one after the other.  A half with fewer than two cells compares nothing.
+  const uint32_t stride = gridDim.x * kFishWarps;
+  for (uint32_t h = blockIdx.x * kFishWarps + w; h < nHits; h += 2 * stride) {
+    const uint32_t h2 = h + stride;
+    const uint32_t b1 = ohOff[h], s1 = min(ohOff[h + 1] - b1, uint32_t(PF_MAX_CELLS_PER_HIT));
+    uint32_t b2 = 0, s2 = 0;
+    if (h2 < nHits) {
+      b2 = ohOff[h2];
+      s2 = min(ohOff[h2 + 1] - b2, uint32_t(PF_MAX_CELLS_PER_HIT));
+    }
+    if (s1 <= 16 && s2 <= 16) {
+      const bool second = lane >= 16;
+      const uint32_t s = second ? s2 : s1;
+      fishHit(second ? h2 : h, second ? b2 : b1, s < 2 ? 0u : s, second ? 16u : 0u, second ? 16u : 0u, 16u);
+    } else {
+      if (s1 >= 2) fishHit(h, b1, s1, 0u, 0u, 32u);
+      if (s2 >= 2) fishHit(h2, b2, s2, 0u, 0u, 32u);
+    }
   }
 }
 

@@ -790,7 +790,34 @@ __device__ __forceinline__ bool isStartCell(const Workspace& ws, size_t cb, uint
   return ws.ca.minHits > 3 ? pid < 3 : (pid < 8 || pid > 12);
 }
 
+// The count pass stages every tuple it finds, so that the write pass is a
+// flat copy instead of a second search: the tuple's cells padded with ~0
+// (scratchA, 16-byte aligned), and its rank and first-hit offset among the
+// tuples of its start cell (scratchB).  Both regions are free between the CA
+// links and the duplicate rounds.  Records are appended in any order (one
+// atomic per group of lanes that find a tuple together); the write pass puts
+// each at its serial position, the start cell's scanned offsets plus its
+// rank.  An event with more tuples than the staging holds is written by a
+// second search, as before.
+struct TupleStage {
+  uint4* cells;
+  uint32_t* rank;
+  uint32_t* hit;
+  uint32_t cap;
+};
+__device__ __forceinline__ TupleStage tupleStage(const Workspace& ws, uint32_t e) {
+  uint32_t* a = ws.scratchA + size_t(e) * ws.cap.scratch;
+  const uint32_t pad = uint32_t((16u - (reinterpret_cast<uintptr_t>(a) & 15u)) & 15u) / 4u;
+  TupleStage t;
+  t.cap = min(ws.cap.tuples, (ws.cap.scratch - pad) / 4u);
+  t.cells = reinterpret_cast<uint4*>(a + pad);
+  t.rank = ws.scratchB + size_t(e) * ws.cap.scratch;
+  t.hit = t.rank + t.cap;
+  return t;
+}
+
 __global__ void kNtupletCount(Workspace ws) {
+  namespace cg = cooperative_groups;
   uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   uint32_t n = c->nCells;
@@ -799,10 +826,21 @@ __global__ void kNtupletCount(Workspace ws) {
   const uint32_t* nbr = ws.nbr + size_t(e) * ws.cap.edges;
   uint32_t* tc = ws.startTupleCount + size_t(e) * (ws.cap.cells + 1);
   uint32_t* hc = ws.startHitCount + size_t(e) * (ws.cap.cells + 1);
+  const TupleStage st = tupleStage(ws, e);
   for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
     uint32_t nt = 0, nh = 0;
     if (isStartCell(ws, cb, idx)) {
-      bool ok = dfsNtuplets(idx, ws.cellDoubletId + cb, nbrOff, nbr, ws.ca.minHits, [&](int ncells, const uint32_t*) {
+      bool ok = dfsNtuplets(idx, ws.cellDoubletId + cb, nbrOff, nbr, ws.ca.minHits, [&](int ncells, const uint32_t* cells) {
+        const cg::coalesced_group g = cg::coalesced_threads();
+        uint32_t s0 = 0;
+        if (g.thread_rank() == 0) s0 = atomicAdd(&c->nStaged, g.size());
+        const uint32_t s = g.shfl(s0, 0) + g.thread_rank();
+        if (s < st.cap) {
+          st.cells[s] = make_uint4(cells[0], ncells > 1 ? cells[1] : ~0u, ncells > 2 ? cells[2] : ~0u,
+                                   ncells > 3 ? cells[3] : ~0u);
+          st.rank[s] = nt;
+          st.hit[s] = nh;
+        }
         ++nt;
         nh += uint32_t(ncells) + 1;
       });
@@ -826,6 +864,36 @@ __global__ void kNtupletWrite(Workspace ws) {
   uint32_t* th = ws.tupleHits + size_t(e) * ws.cap.tupleHits();
   uint32_t* tcell = ws.tupleCells + size_t(e) * ws.cap.tupleCells();
   uint8_t* q = ws.quality + size_t(e) * ws.cap.tuples;
+  const TupleStage st = tupleStage(ws, e);
+  const uint32_t staged = c->nStaged;
+  if (staged <= st.cap) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < staged; s += gridDim.x * blockDim.x) {
+      const uint4 r = st.cells[s];
+      const uint32_t m = to[r.x] + st.rank[s];
+      if (m >= ws.cap.tuples) continue;
+      const uint32_t off = ho[r.x] + st.hit[s];
+      toff[m] = off;
+      // the cells (at least two) and their hits; the per-event stride of
+      // tcell is 4 * cap.tuples words on a 256-byte aligned base
+      th[off] = ws.cellInner[cb + r.x];
+      th[off + 1] = ws.cellInner[cb + r.y];
+      uint32_t last = r.y, nc = 2;
+      if (r.z != ~0u) {
+        th[off + 2] = ws.cellInner[cb + r.z];
+        last = r.z;
+        nc = 3;
+        if (r.w != ~0u) {
+          th[off + 3] = ws.cellInner[cb + r.w];
+          last = r.w;
+          nc = 4;
+        }
+      }
+      th[off + nc] = ws.cellOuter[cb + last];
+      reinterpret_cast<uint4*>(tcell)[m] = r;
+      q[m] = kBad;
+    }
+    return;
+  }
   for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
     if (!isStartCell(ws, cb, idx)) continue;
     uint32_t m = to[idx], off = ho[idx];

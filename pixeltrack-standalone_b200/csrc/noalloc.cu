@@ -22,12 +22,12 @@ namespace {
 // areas the vertex kernel uses for events above its shared-memory size, with
 // the sizes that kernel carves (pixgpu_internal.cuh: kVtxScratchAWords,
 // kVtxScratchBWords for kMaxVtxTracks tracks).
-constexpr size_t kCountersBytes = 256;
+constexpr size_t kCountersBytes = 512;
 constexpr size_t kScratchABytes = kVtxScratchAWords * 4;
 constexpr size_t kScratchBBytes = kVtxScratchBWords * 4;
-constexpr size_t kNoAllocBytes = kCountersBytes + kScratchABytes + kScratchBBytes;  // 1.31 MB
+constexpr size_t kNoAllocBytes = kCountersBytes + kScratchABytes + kScratchBBytes;  // 1.25 MiB + 512 B
 static_assert(sizeof(EventCounters) <= kCountersBytes, "counters do not fit their scratch slot");
-static_assert(kNoAllocBytes <= 1310720 + 256, "the documented 1.3 MB bound of the static scratch");
+static_assert(kNoAllocBytes <= 1310720 + 512, "the documented 1.25 MB bound of the static scratch");
 // the tuple limit (n_tuples < kNoAllocMaxTuples + 1) and the reference's
 // TrackSoA stride the one-event workspace uses
 constexpr uint32_t kNoAllocMaxTuples = PF_TRACK_STRIDE - 1;  // 32767

@@ -126,6 +126,7 @@ struct EventCounters {
   uint32_t nBigHitMod;          // modules queued for the block rechit kernel
   // cut decisions on their float boundary (cutNear): doublet, CA and quality cuts
   uint32_t nearDoublet, nearCA, nearQuality;
+  uint32_t nStaged;             // tuples staged by the n-tuplet count pass
 };
 
 // A cut decision counts as on its boundary when its two sides lie within

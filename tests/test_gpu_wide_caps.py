@@ -48,3 +48,37 @@ def test_mixed_pileup_batch_with_wide_caps(wide_chain, default_detector):
         diffs = oracle.compare(alone[k], wide_chain.products(k), rtol=0)
         assert diffs == [], (k, diffs[:3])
         assert wide_chain.counts(k)["flags"] == 0
+
+
+def test_tuple_overflow_keeps_the_serial_prefix(default_detector):
+    """An event with more tuples than the reference's 32768: with a tuple
+    capacity that holds them all the chain equals the oracle (the n-tuplet
+    write copies the tuples its count pass staged); at the reference's
+    capacity the event overflows (the write searches a second time instead)
+    and its stored tuples are the oracle's first 32767, as the reference
+    keeps them (HistoContainer.h:193-204, bulkFinalizeFill)."""
+    import oracle
+    import pixgpu
+    caps = {"tuples": 1 << 17, "multiplicity": 1 << 17, "hit_to_tuple": 1 << 20}
+    raw = default_detector.event(20261203 + 7055, 55)  # dense model: ~412k doublets, ~34k tuples
+    want = oracle.Oracle(default_detector.es, caps=caps).process(raw)
+    assert want["nTuples"] > 32768 and want["nCells"] < 458752
+    for ch_caps in (caps, None):
+        ch = pixgpu.Chain(default_detector.es, max_events=1, max_words_per_batch=400000, caps=ch_caps)
+        try:
+            ch.process([raw])
+            flags = ch.counts(0)["flags"]
+            got = ch.products(0)
+        finally:
+            ch.close()
+        if ch_caps:
+            assert flags == 0
+            diffs = oracle.compare(want, got, rtol=RTOL)
+            assert diffs == [], "\n".join("%s: %s" % d for d in diffs)
+        else:
+            assert flags & pixgpu.PG_FLAG_TUPLE_OVERFLOW
+            off = np.asarray(got["tupleOff"], np.int64)
+            assert len(off) == 32768
+            np.testing.assert_array_equal(off, np.asarray(want["tupleOff"], np.int64)[:32768])
+            np.testing.assert_array_equal(np.asarray(got["tupleHits"])[:off[-1]],
+                                          np.asarray(want["tupleHits"])[:off[-1]])

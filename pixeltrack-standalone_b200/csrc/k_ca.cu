@@ -509,9 +509,18 @@ __global__ void kOhRec(Workspace ws) {
 // non-empty ones in turn; for a slot, lane t stages the outer hit of cell t
 // and the lanes form groups of G candidates (G the power of two covering the
 // list, at most 32), each group testing another cell of the slot, so short
-// candidate lists still keep the lanes busy.  Accepted links (oc <- idx) are
-// appended unordered with one atomic per warp and round.
-__global__ void __launch_bounds__(256, 6) kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
+// candidate lists still keep the lanes busy.
+// Only about 2 % of the pairs pass the r-z alignment test, so the pairs that
+// do are queued (per warp, in shared memory) and the dca test runs on 32
+// queued pairs at a time, every lane busy, instead of on every round that
+// has one passing lane.  Accepted links (oc <- idx) are appended unordered
+// with one atomic per warp and round.
+constexpr uint32_t kConnectWarps = 8;   // 256 threads
+constexpr uint32_t kConnectQueue = 64;  // ring of queued pairs per warp (a round adds at most 32)
+__global__ void __launch_bounds__(kConnectWarps * 32, 6) kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
+  // queued pair: ohRec/ohCells position of the candidate, the cell, the
+  // slot's inner hit and the cell's outer hit
+  __shared__ uint4 queueA[kConnectWarps][kConnectQueue];
   const uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   const uint32_t ntot = c->ntot;
@@ -528,7 +537,44 @@ __global__ void __launch_bounds__(256, 6) kConnect(Workspace ws, uint32_t* edgeO
   const uint32_t edgeCap = min(ws.cap.edges, ws.cap.scratch);
   const uint32_t lane = laneId(), wpb = blockDim.x >> 5;
   const uint32_t S = gridDim.x * wpb, w = blockIdx.x * wpb + (threadIdx.x >> 5);
-  uint32_t near = 0;  // per lane: cut decisions on their boundary
+  uint4* queue = queueA[threadIdx.x >> 5];
+  uint32_t qHead = 0, qTail = 0;  // warp-uniform ring positions
+  uint32_t near = 0;              // per lane: cut decisions on their boundary
+  // dca test of the nq (<= 32) oldest queued pairs, one per lane
+  auto drain = [&](uint32_t nq) {
+    __syncwarp();
+    bool ok = false;
+    uint32_t p = 0, idx = 0;
+    if (lane < nq) {
+      const uint4 qe = queue[(qHead + lane) & (kConnectQueue - 1)];
+      p = qe.x;
+      idx = qe.y;
+      const float4 r1 = ohRec[p];
+      const float region = r1.w < 0.f ? kDcaCutInner : kDcaCutOuter;
+      ok = dcaCut(r1.x, r1.y, hh.xg[qe.z], hh.yg[qe.z], hh.xg[qe.w], hh.yg[qe.w], region, near);
+    }
+    qHead += nq;
+    const uint32_t mask = __ballot_sync(0xffffffffu, ok);
+    if (mask) {
+      uint32_t at = 0;
+      if (lane == 0) at = atomicAdd(&c->nEdges, uint32_t(__popc(mask)));
+      at = __shfl_sync(0xffffffffu, at, 0);
+      if (ok) {
+        const uint32_t oc = ohCells[p];
+        ws.cellUsed[cb + idx] = 1;
+        ws.cellUsed[cb + oc] = 1;
+        atomicAdd(&nbrCnt[oc], 1u);
+        const uint32_t slot = at + __popc(mask & lanemaskLt());
+        if (slot < edgeCap) {
+          eOc[slot] = oc;
+          eIdx[slot] = idx;
+        } else {
+          atomicOr(&c->flags, kFlagEdgeOverflow);
+        }
+      }
+    }
+    __syncwarp();  // the entries are read before the next round overwrites them
+  };
   for (uint32_t r0 = 0; w + r0 * S < ntot; r0 += 32) {
     const uint32_t jl = w + (r0 + lane) * S;
     uint32_t myBase = 0, myEnd = 0, myOb = 0, myM = 0;
@@ -552,62 +598,40 @@ __global__ void __launch_bounds__(256, 6) kConnect(Workspace ws, uint32_t* edgeO
       const uint32_t h = ws.cellInner[cb + base];
       const float ri = ws.cellInnerR[cb + base], zi = ws.cellInnerZ[cb + base];
       const float thetaCut = hh.detInd[h] < 1184 ? kThetaCutBarrel : kThetaCutForward;
-      const float x2 = hh.xg[h], y2 = hh.yg[h];
       // lanes form 32/G groups of G >= m candidates; each group tests one cell
       const uint32_t G = m > 16 ? 32u : (m > 8 ? 16u : (m > 4 ? 8u : (m > 2 ? 4u : (m > 1 ? 2u : 1u))));
       const uint32_t R = 32u / G, grp = lane / G, kk = lane % G;
       for (uint32_t c0 = base; c0 < end; c0 += 32) {
         const uint32_t nc = min(32u, end - c0);
-        float sro = 0.f, szo = 0.f, sx3 = 0.f, sy3 = 0.f;
+        float sro = 0.f, szo = 0.f;
+        uint32_t soh = 0;
         if (lane < nc) {
-          const uint32_t oh = ws.cellOuter[cb + c0 + lane];
-          sro = hh.rg[oh];
-          szo = hh.zg[oh];
-          sx3 = hh.xg[oh];
-          sy3 = hh.yg[oh];
+          soh = ws.cellOuter[cb + c0 + lane];
+          sro = hh.rg[soh];
+          szo = hh.zg[soh];
         }
         for (uint32_t k0 = 0; k0 < m; k0 += G) {
           const uint32_t k = k0 + kk;
           float4 r1 = make_float4(0.f, 0.f, 0.f, 0.f);
-          uint32_t oc = 0;
-          if (k < m) {
-            r1 = ohRec[ob + k];
-            oc = ohCells[ob + k];
-          }
-          const float region = r1.w < 0.f ? kDcaCutInner : kDcaCutOuter;
+          if (k < m) r1 = ohRec[ob + k];
           const float rr1 = fabsf(r1.w);
-          bool usedOc = false;
           for (uint32_t t0 = 0; t0 < nc; t0 += R) {
             const uint32_t t = t0 + grp;
             const uint32_t src = t < nc ? t : 0u;
             const float ro = __shfl_sync(0xffffffffu, sro, src), zo = __shfl_sync(0xffffffffu, szo, src);
-            const float x3 = __shfl_sync(0xffffffffu, sx3, src), y3 = __shfl_sync(0xffffffffu, sy3, src);
-            const bool ok = t < nc && k < m && alignedRZ(rr1, r1.z, ri, zi, ro, zo, thetaCut, near) &&
-                            dcaCut(r1.x, r1.y, x2, y2, x3, y3, region, near);
-            const uint32_t mask = __ballot_sync(0xffffffffu, ok);
+            const bool pass = t < nc && k < m && alignedRZ(rr1, r1.z, ri, zi, ro, zo, thetaCut, near);
+            const uint32_t mask = __ballot_sync(0xffffffffu, pass);
             if (mask == 0) continue;
-            uint32_t at = 0;
-            if (lane == 0) at = atomicAdd(&c->nEdges, uint32_t(__popc(mask)));
-            at = __shfl_sync(0xffffffffu, at, 0);
-            if (ok) {
-              const uint32_t idx = c0 + t;
-              usedOc = true;
-              ws.cellUsed[cb + idx] = 1;
-              atomicAdd(&nbrCnt[oc], 1u);
-              const uint32_t slot = at + __popc(mask & lanemaskLt());
-              if (slot < edgeCap) {
-                eOc[slot] = oc;
-                eIdx[slot] = idx;
-              } else {
-                atomicOr(&c->flags, kFlagEdgeOverflow);
-              }
-            }
+            const uint32_t oh = __shfl_sync(0xffffffffu, soh, src);
+            if (pass) queue[(qTail + __popc(mask & lanemaskLt())) & (kConnectQueue - 1)] = make_uint4(ob + k, c0 + t, h, oh);
+            qTail += __popc(mask);
+            if (qTail - qHead >= 32) drain(32);
           }
-          if (usedOc) ws.cellUsed[cb + oc] = 1;
         }
       }
     }
   }
+  while (qTail != qHead) drain(min(32u, qTail - qHead));
   near = __reduce_add_sync(0xffffffffu, near);
   if (lane == 0 && near) atomicAdd(&c->nearCA, near);
 }
@@ -1473,7 +1497,7 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   PG_PROBED("kOhRec", stream, kOhRec<<<dim3(tunedGrid(ws, kTuneOhRec, gx), nEvents), 256, 0, stream>>>(ws));
   // ---- CA links: edges appended unordered, then CSR by inner cell, ordered ascending
   PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbrCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
-  PG_PROBED("kConnect", stream, kConnect<<<dim3(tunedGrid(ws, kTuneConnect, gx * 4), nEvents), 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
+  PG_PROBED("kConnect", stream, kConnect<<<dim3(tunedGrid(ws, kTuneConnect, gx * 4), nEvents), kConnectWarps * 32, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
   segScan(ws, kScanNeighbours, ws.nbrCount, ws.nbrOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, nEvents, stream,
           true);
   PG_PROBED("kEdgeScatter", stream, kEdgeScatter<<<dim3(tunedGrid(ws, kTuneEdgeScatter, gx), nEvents), 256, 0, stream>>>(ws, ws.scratchA, ws.scratchB));

@@ -668,11 +668,13 @@ __global__ void kNbrPool(Workspace ws) {
 // ------------------------------------------------------------------ fishbone
 
 // gpuFishbone.h:21-90 (early fishbone), one warp per hit with >= 2 cells
-// ending on it.  The hit's cells (first 128, put in ascending order here)
-// are staged in shared memory from the isOuterHitOfCell records; lane ic compares cell ic
-// with every later cell, as the serial double loop does.  Kills only write
-// doubletId = -1 and never change the `used` flags the loop reads, so the
-// lanes are independent.
+// ending on it.  The serial double loop compares only the hit's used cells
+// (with checkTrack, used and on a tuple): about one cell in ten.  So the
+// hit's cells (first 128) are filtered first, the used ones put in ascending
+// order and staged in shared memory from the isOuterHitOfCell records, and
+// lane ic compares used cell ic with every later one, as the serial loop
+// does.  Kills only write doubletId = -1 and never change the `used` flags
+// the loop reads, so the lanes are independent.
 constexpr int kFishWarps = 8;
 // checkTrack: the late fishbone (gpuFishbone.h:21-90 with checkTrack), which
 // also skips cells that no tuple goes through
@@ -680,8 +682,9 @@ __global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws, bool 
   __shared__ float sxA[kFishWarps][PF_MAX_CELLS_PER_HIT], syA[kFishWarps][PF_MAX_CELLS_PER_HIT],
       szA[kFishWarps][PF_MAX_CELLS_PER_HIT];
   __shared__ uint16_t sdA[kFishWarps][PF_MAX_CELLS_PER_HIT];
-  __shared__ uint8_t suA[kFishWarps][PF_MAX_CELLS_PER_HIT];
+  __shared__ uint8_t skA[kFishWarps][PF_MAX_CELLS_PER_HIT];
   __shared__ uint32_t rawA[kFishWarps][PF_MAX_CELLS_PER_HIT], scA[kFishWarps][PF_MAX_CELLS_PER_HIT];
+  static_assert(PF_MAX_CELLS_PER_HIT <= 256, "list positions are staged as bytes");
   const uint32_t e = blockIdx.y;
   const EventCounters* c = ws.ev + e;
   const uint32_t nHits = c->nHits;
@@ -698,38 +701,54 @@ __global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws, bool 
   float* sy = syA[w];
   float* sz = szA[w];
   uint16_t* sd = sdA[w];
-  uint8_t* su = suA[w];
+  uint8_t* sk = skA[w];
   uint32_t* raw = rawA[w];
   uint32_t* sc = scA[w];
   // One hit, done by the `width` lanes starting at lane g0 (the whole warp
-  // for up to 128 cells, a half warp for up to 16): stages the hit's cells in
-  // ascending cell order at sx..sc[o..] (the list is filled unordered) and
-  // compares them.
+  // for up to 128 cells, a half warp for up to 16): the used cells, with
+  // their list positions, compacted at raw/sk[o..] in list order, then
+  // staged in ascending cell order at sx..sc[o..] and compared.
   auto fishHit = [&](uint32_t h, uint32_t b, uint32_t s, uint32_t o, uint32_t g0, uint32_t width) {
     const uint32_t gl = lane - g0;
-    const float xo = s ? hh.xg[h] : 0.f, yo = s ? hh.yg[h] : 0.f, zo = s ? hh.zg[h] : 0.f;
-    for (uint32_t k = gl; k < s; k += width) raw[o + k] = ohCells[b + k];
+    const uint32_t gmask = width == 32 ? 0xffffffffu : ((1u << width) - 1u) << g0;
+    uint32_t nu = 0;  // used cells (uniform over the group)
+    for (uint32_t k0 = 0; k0 < s; k0 += width) {
+      const uint32_t k = k0 + gl;
+      uint32_t cell = 0;
+      bool used = false;
+      if (k < s) {
+        cell = ohCells[b + k];
+        used = ws.cellUsed[cb + cell] && !(checkTrack && trkOff[cell + 1] == trkOff[cell]);
+      }
+      const uint32_t bal = __ballot_sync(gmask, used) >> g0;
+      if (used) {
+        const uint32_t pos = nu + __popc(bal & ((1u << gl) - 1u));
+        raw[o + pos] = cell;
+        sk[o + pos] = uint8_t(k);
+      }
+      nu += __popc(bal);
+    }
+    if (nu < 2) nu = 0;  // nothing to compare
     __syncwarp();
-    for (uint32_t k = gl; k < s; k += width) {
-      const uint32_t cell = raw[o + k];
+    const float xo = nu ? hh.xg[h] : 0.f, yo = nu ? hh.yg[h] : 0.f, zo = nu ? hh.zg[h] : 0.f;
+    for (uint32_t u = gl; u < nu; u += width) {
+      const uint32_t cell = raw[o + u];
       uint32_t r = 0;
-      for (uint32_t m = 0; m < s; ++m) r += raw[o + m] < cell ? 1u : 0u;
+      for (uint32_t m = 0; m < nu; ++m) r += raw[o + m] < cell ? 1u : 0u;
+      const uint32_t k = sk[o + u];
       const float4 rec = ohRec[b + k];
       sx[o + r] = rec.x - xo;
       sy[o + r] = rec.y - yo;
       sz[o + r] = rec.z - zo;
       sd[o + r] = ohDet[b + k];
-      su[o + r] = ws.cellUsed[cb + cell] && !(checkTrack && trkOff[cell + 1] == trkOff[cell]) ? 1 : 0;
       sc[o + r] = cell;
     }
     __syncwarp();
-    for (uint32_t ic = gl; ic < s; ic += width) {
-      if (0 == su[o + ic]) continue;
+    for (uint32_t ic = gl; ic < nu; ic += width) {
       const float xi = sx[o + ic], yi = sy[o + ic], zi = sz[o + ic];
       const uint16_t di = sd[o + ic];
       const float ni = xi * xi + yi * yi + zi * zi;
-      for (uint32_t jc = ic + 1; jc < s; ++jc) {
-        if (0 == su[o + jc]) continue;
+      for (uint32_t jc = ic + 1; jc < nu; ++jc) {
         const float xj = sx[o + jc], yj = sy[o + jc], zj = sz[o + jc];
         const float nj = xj * xj + yj * yj + zj * zj;
         const float cos12 = xi * xj + yi * yj + zi * zj;

@@ -73,6 +73,8 @@ void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W, const Caps& cap) {
   c.take(ws.cellInnerR, C);
   c.take(ws.ohCount, size_t(E) * (cap.hits + 1));
   c.take(ws.ohOff, size_t(E) * (cap.hits + 1));
+  c.take(ws.hitTouch, size_t(E) * cap.hits);
+  c.take(ws.fishHits, size_t(E) * cap.hits);
   c.take(ws.ohCells, C);
   c.take(ws.ohRec, C);
   c.take(ws.ohDet, C);

@@ -643,24 +643,52 @@ __global__ void kEdgeScatter(Workspace ws, const uint32_t* edgeOc, const uint32_
   uint32_t n = min(c->nEdges, edgeCap);
   const uint32_t* off = ws.nbrOff + size_t(e) * (ws.cap.cells + 1);
   uint32_t* cur = ws.nbrCount + size_t(e) * (ws.cap.cells + 1);
+  uint32_t* touch = ws.hitTouch + size_t(e) * ws.cap.hits;
+  uint32_t* fishList = ws.ca.earlyFishbone ? ws.fishHits + size_t(e) * ws.cap.hits : nullptr;
+  const size_t cb = size_t(e) * ws.cap.cells;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     uint32_t oc = edgeOc[size_t(e) * ws.cap.scratch + k];
+    const uint32_t idx = edgeIdx[size_t(e) * ws.cap.scratch + k];
     uint32_t p = atomicAdd(&cur[oc], 1u);
-    if (off[oc] + p < edgeCap)
-      ws.nbr[size_t(e) * ws.cap.edges + off[oc] + p] = edgeIdx[size_t(e) * ws.cap.scratch + k];
+    if (off[oc] + p < edgeCap) ws.nbr[size_t(e) * ws.cap.edges + off[oc] + p] = idx;
     if (p == 1) noteSegment(ws, e, 1, oc);
+    if (fishList) {
+      // the link's cells end on these two hits; a hit on which two link ends
+      // land may have two used cells and goes to the early fishbone's list
+      const uint32_t h0 = ws.cellOuter[cb + oc], h1 = ws.cellOuter[cb + idx];
+      if (atomicAdd(&touch[h0], 1u) == 1u) fishList[atomicAdd(&c->nFishHits, 1u)] = h0;
+      if (atomicAdd(&touch[h1], 1u) == 1u) fishList[atomicAdd(&c->nFishHits, 1u)] = h1;
+    }
   }
 }
 
-// cells with at least one CA link must fit the 65535-list pool of the reference
+// cells with at least one CA link must fit the 65535-list pool of the reference.
+// The same pass clears the n-tuplet search's per-cell counts and lists the
+// cells with links: a tuple has at least two cells, so only they can start
+// one.  The list goes to startHitOff, which is free until the scan of the
+// start-hit counts writes it.
 __global__ void kNbrPool(Workspace ws) {
   uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
   uint32_t n = c->nCells;
   const uint32_t* off = ws.nbrOff + size_t(e) * (ws.cap.cells + 1);
+  uint32_t* tc = ws.startTupleCount + size_t(e) * (ws.cap.cells + 1);
+  uint32_t* hc = ws.startHitCount + size_t(e) * (ws.cap.cells + 1);
+  uint32_t* linked = ws.startHitOff + size_t(e) * (ws.cap.cells + 1);
   uint32_t local = 0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    local += (off[i + 1] > off[i]) ? 1u : 0u;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const bool has = off[i + 1] > off[i];
+    local += has ? 1u : 0u;
+    tc[i] = 0;
+    hc[i] = 0;
+    const uint32_t active = __activemask();
+    const uint32_t bal = __ballot_sync(active, has);
+    const uint32_t leader = __ffs(active) - 1;
+    uint32_t at = 0;
+    if (laneId() == leader && bal) at = atomicAdd(&c->nLinked, uint32_t(__popc(bal)));
+    at = __shfl_sync(active, at, leader);
+    if (has) linked[at + __popc(bal & lanemaskLt())] = i;
+  }
   local = __reduce_add_sync(0xffffffffu, local);
   if ((threadIdx.x & 31) == 0 && local) atomicAdd(&c->nNbrLists, local);
 }
@@ -764,15 +792,22 @@ __global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws, bool 
     }
     __syncwarp();
   };
+  // The hits: the list kEdgeScatter made (early fishbone, all links kept),
+  // else all of them.
   // Hits are taken two at a time: each half of the warp does one when both
   // have at most 16 cells (most hits have about ten), else the warp does them
   // one after the other.  A half with fewer than two cells compares nothing.
+  const uint32_t* list =
+      checkTrack || c->nEdges > min(ws.cap.edges, ws.cap.scratch) ? nullptr : ws.fishHits + size_t(e) * ws.cap.hits;
+  const uint32_t n = list ? c->nFishHits : nHits;
   const uint32_t stride = gridDim.x * kFishWarps;
-  for (uint32_t h = blockIdx.x * kFishWarps + w; h < nHits; h += 2 * stride) {
-    const uint32_t h2 = h + stride;
+  for (uint32_t i = blockIdx.x * kFishWarps + w; i < n; i += 2 * stride) {
+    const uint32_t h = list ? list[i] : i;
+    const uint32_t i2 = i + stride;
     const uint32_t b1 = ohOff[h], s1 = min(ohOff[h + 1] - b1, uint32_t(PF_MAX_CELLS_PER_HIT));
-    uint32_t b2 = 0, s2 = 0;
-    if (h2 < nHits) {
+    uint32_t h2 = 0, b2 = 0, s2 = 0;
+    if (i2 < n) {
+      h2 = list ? list[i2] : i2;
       b2 = ohOff[h2];
       s2 = min(ohOff[h2 + 1] - b2, uint32_t(PF_MAX_CELLS_PER_HIT));
     }
@@ -863,14 +898,17 @@ __global__ void kNtupletCount(Workspace ws) {
   namespace cg = cooperative_groups;
   uint32_t e = blockIdx.y;
   EventCounters* c = ws.ev + e;
-  uint32_t n = c->nCells;
   size_t cb = size_t(e) * ws.cap.cells;
   const uint32_t* nbrOff = ws.nbrOff + size_t(e) * (ws.cap.cells + 1);
   const uint32_t* nbr = ws.nbr + size_t(e) * ws.cap.edges;
   uint32_t* tc = ws.startTupleCount + size_t(e) * (ws.cap.cells + 1);
   uint32_t* hc = ws.startHitCount + size_t(e) * (ws.cap.cells + 1);
   const TupleStage st = tupleStage(ws, e);
-  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+  // the cells with links (kNbrPool; the counts of all others are zero)
+  const uint32_t* linked = ws.startHitOff + size_t(e) * (ws.cap.cells + 1);
+  const uint32_t nl = c->nLinked;
+  for (uint32_t li = blockIdx.x * blockDim.x + threadIdx.x; li < nl; li += gridDim.x * blockDim.x) {
+    const uint32_t idx = linked[li];
     uint32_t nt = 0, nh = 0;
     if (isStartCell(ws, cb, idx)) {
       bool ok = dfsNtuplets(idx, ws.cellDoubletId + cb, nbrOff, nbr, ws.ca.minHits, [&](int ncells, const uint32_t* cells) {
@@ -1516,6 +1554,8 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
   PG_PROBED("kOhRec", stream, kOhRec<<<dim3(tunedGrid(ws, kTuneOhRec, gx), nEvents), 256, 0, stream>>>(ws));
   // ---- CA links: edges appended unordered, then CSR by inner cell, ordered ascending
   PG_PROBED("kZero", stream, kZero<<<dim3(gx * 2, nEvents), 256, 0, stream>>>(ws.nbrCount, kCellCap + 1, kCellCap + 1, EVF(nCells)));
+  if (ws.ca.earlyFishbone)
+    PG_PROBED("kZero", stream, kZero<<<dim3(gx, nEvents), 256, 0, stream>>>(ws.hitTouch, kHitCap, kHitCap, EVF(nHits)));
   PG_PROBED("kConnect", stream, kConnect<<<dim3(tunedGrid(ws, kTuneConnect, gx * 4), nEvents), kConnectWarps * 32, 0, stream>>>(ws, ws.scratchA, ws.scratchB));
   segScan(ws, kScanNeighbours, ws.nbrCount, ws.nbrOff, kCellCap + 1, EVF(nCells), kCellCap, nullptr, 0, nEvents, stream,
           true);
@@ -1528,10 +1568,9 @@ cudaError_t runCA(const DeviceES& es, Workspace& ws, uint32_t nEvents, cudaStrea
     PG_PROBED("kFishbone", stream, kFishbone<<<dim3(tunedGrid(ws, kTuneFishbone, gx * 2), nEvents), 256, 0, stream>>>(ws, false));
   // ---- n-tuplets: DFS count, scans, DFS write, finalize
   PG_PROBED("kNtupletCount", stream, kNtupletCount<<<dim3(tunedGrid(ws, kTuneNtupletCount, gx * 8), nEvents), 128, 0, stream>>>(ws));
-  segScan(ws, kScanStartTuples, ws.startTupleCount, ws.startTupleOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcM),
-          nEvents, stream);
-  segScan(ws, kScanStartHits, ws.startHitCount, ws.startHitOff, kCellCap + 1, EVF(nCells), kCellCap, EVF(apcN), nEvents,
-          stream);
+  segScan2(ws, kScanStartTuples, ws.startTupleCount, ws.startTupleOff, &ws.ev[0].apcM, kScanStartHits, ws.startHitCount,
+           ws.startHitOff, &ws.ev[0].apcN, kCellCap + 1, EVF(nCells), kCellCap, sizeof(EventCounters) / 4, nEvents,
+           stream);
   PG_PROBED("kNtupletWrite", stream, kNtupletWrite<<<dim3(tunedGrid(ws, kTuneNtupletWrite, gx * 8), nEvents), 128, 0, stream>>>(ws));
   PG_PROBED("kTupleFinalize", stream, kTupleFinalize<<<dim3(32, nEvents), 1024, 0, stream>>>(ws));
   // ---- cell -> track lists

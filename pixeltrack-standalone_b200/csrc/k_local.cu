@@ -185,7 +185,7 @@ __global__ void kInitEvents(Workspace ws, uint32_t nEvents) {
     c->nSegList[0] = c->nSegList[1] = c->nSegList[2] = c->nSegList[3] = 0;
     c->nBigHitMod = 0;
     c->nearDoublet = c->nearCA = c->nearQuality = 0;
-    c->nStaged = 0;
+    c->nStaged = c->nFishHits = c->nLinked = 0;
     c->flags = c->nWords > ws.cap.fedWords ? kFlagTooManyWords : 0u;
     ws.scanEpoch[e] += 1;  // tags this batch's scan state words
   }

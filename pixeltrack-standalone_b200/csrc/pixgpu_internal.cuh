@@ -127,6 +127,8 @@ struct EventCounters {
   // cut decisions on their float boundary (cutNear): doublet, CA and quality cuts
   uint32_t nearDoublet, nearCA, nearQuality;
   uint32_t nStaged;             // tuples staged by the n-tuplet count pass
+  uint32_t nFishHits;           // entries of the early fishbone's hit list
+  uint32_t nLinked;             // cells with CA links (the n-tuplet search's start candidates)
 };
 
 // A cut decision counts as on its boundary when its two sides lie within
@@ -280,6 +282,8 @@ struct Workspace {
   // cells by outer hit (isOuterHitOfCell), CSR sorted ascending
   uint32_t* ohCount;         // [maxEvents][cap.hits + 1]
   uint32_t* ohOff;           // [maxEvents][cap.hits + 1]
+  uint32_t* hitTouch;        // [maxEvents][cap.hits]  CA link ends on cells ending at each hit
+  uint32_t* fishHits;        // [maxEvents][cap.hits]  hits with >= 2 such ends (early fishbone work list)
   uint32_t* ohCells;         // [maxEvents][cap.cells]
   float4* ohRec;             // [maxEvents][cap.cells] inner hit of each ohCells entry: x, y, z, +-r (- : dca region inner)
   uint16_t* ohDet;           // [maxEvents][cap.cells] module index of that inner hit
@@ -430,5 +434,10 @@ void launchPack(Workspace& ws, uint32_t nEvents, uint8_t* out, cudaStream_t s);
 void segScan(const Workspace& ws, ScanCall call, uint32_t* in, uint32_t* out, uint32_t stride,
              const uint32_t* lenPtr, uint32_t lenStride, uint32_t maxLen, uint32_t* totalPtr, uint32_t totalStride,
              uint32_t nEvents, cudaStream_t stream, bool zeroIn = false);
+// Two such scans of arrays with the same lengths and stride in one launch.
+void segScan2(const Workspace& ws, ScanCall call0, uint32_t* in0, uint32_t* out0, uint32_t* total0, ScanCall call1,
+              uint32_t* in1, uint32_t* out1, uint32_t* total1, uint32_t stride, const uint32_t* lenPtr,
+              uint32_t lenStride, uint32_t maxLen, uint32_t totalStride, uint32_t nEvents, cudaStream_t stream,
+              bool zeroIn = false);
 
 }  // namespace pixgpu

@@ -42,20 +42,27 @@ __device__ __forceinline__ uint64_t peek(const uint64_t* p) {
 
 constexpr uint32_t kLookBackPolls = 1u << 22;  // bound on the polls of one look-back (~0.3 s)
 
+// one of the arrays a launch scans (two arrays of the same lengths may share
+// a launch, each with its own tile states; the first one's ticket orders
+// the tiles)
+struct ScanArray {
+  uint32_t* in;
+  uint32_t* out;
+  uint32_t* total;  // per-event total (may be null)
+  uint32_t call;    // ScanCall: state region
+};
+
+template <uint32_t kArrays>
 __global__ void __launch_bounds__(kScanThreads, 3)
-    kScanOnePass(uint32_t* in, uint32_t* out, uint32_t stride, const uint32_t* lenPtr, uint32_t lenStride,
-                 uint32_t fixedLen, uint32_t* totalPtr, uint32_t totalStride, bool zeroIn, Workspace ws,
-                 uint32_t call) {
-  __shared__ uint32_t sh[33];
-  __shared__ uint32_t sTile, sPrefix;
+    kScanOnePass(ScanArray a0, ScanArray a1, uint32_t stride, const uint32_t* lenPtr, uint32_t lenStride,
+                 uint32_t fixedLen, uint32_t totalStride, bool zeroIn, Workspace ws) {
+  __shared__ uint32_t sh[kArrays][33];
+  __shared__ uint32_t sTile, sPrefix[kArrays];
   const uint32_t e = blockIdx.y;
   const uint32_t n = lenPtr ? min(lenPtr[size_t(e) * lenStride], fixedLen) : fixedLen;  // fixedLen: the capacity
   const uint32_t tiles = max(1u, (n + kScanTile - 1) / kScanTile);
-  uint32_t* src = in + size_t(e) * stride;
-  uint32_t* dst = out + size_t(e) * stride;
-  uint64_t* state = ws.scanState + (size_t(e) * kScanCalls + call) * ws.scanTiles;
-  uint32_t* ticket = ws.scanTicket + size_t(e) * kScanCalls + call;
-  const uint32_t tag = (ws.scanEpoch[e] * kScanCalls + call) & 0x3fffffffu;
+  auto arr = [&](uint32_t q) -> const ScanArray& { return q == 0 ? a0 : a1; };
+  uint32_t* ticket = ws.scanTicket + size_t(e) * kScanCalls + a0.call;
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (;;) {
     if (threadIdx.x == 0) sTile = atomicAdd(ticket, 1u);
@@ -64,30 +71,41 @@ __global__ void __launch_bounds__(kScanThreads, 3)
     if (t >= tiles) return;
     const uint32_t lo = t * kScanTile, hi = min(n, lo + kScanTile);
     const uint32_t w0 = lo + warp * 32 * kScanPer + lane;
-    uint32_t v[kScanPer];
-    uint32_t run = 0;  // exclusive prefix of the warp's run so far
+    uint32_t v[kArrays][kScanPer];
+    uint32_t base[kArrays], tileTot[kArrays];
 #pragma unroll
-    for (uint32_t j = 0; j < kScanPer; ++j) {
-      const uint32_t i = w0 + j * 32;
-      v[j] = i < hi ? src[i] : 0u;
+    for (uint32_t q = 0; q < kArrays; ++q) {
+      const uint32_t* src = arr(q).in + size_t(e) * stride;
+#pragma unroll
+      for (uint32_t j = 0; j < kScanPer; ++j) {
+        const uint32_t i = w0 + j * 32;
+        v[q][j] = i < hi ? src[i] : 0u;
+      }
     }
 #pragma unroll
-    for (uint32_t j = 0; j < kScanPer; ++j) {
-      const uint32_t x = v[j];
-      const uint32_t inc = warpInclusiveScan(x);
-      v[j] = run + inc - x;
-      run += __shfl_sync(0xffffffffu, inc, 31);
+    for (uint32_t q = 0; q < kArrays; ++q) {
+      uint32_t run = 0;  // exclusive prefix of the warp's run so far
+#pragma unroll
+      for (uint32_t j = 0; j < kScanPer; ++j) {
+        const uint32_t x = v[q][j];
+        const uint32_t inc = warpInclusiveScan(x);
+        v[q][j] = run + inc - x;
+        run += __shfl_sync(0xffffffffu, inc, 31);
+      }
+      const uint32_t wpre = blockExclusiveScan(lane == 31 ? run : 0u, sh[q], &tileTot[q]);
+      base[q] = __shfl_sync(0xffffffffu, wpre, 31);
     }
-    uint32_t tileTot;
-    const uint32_t wpre = blockExclusiveScan(lane == 31 ? run : 0u, sh, &tileTot);
-    const uint32_t base = __shfl_sync(0xffffffffu, wpre, 31);
-    // publish this tile's sum, then look back (warp 0)
-    if (warp == 0) {
+    // publish each array's tile sum, then look back (warp q for array q)
+    if (warp < kArrays) {
+      const uint32_t q = warp;
+      const uint32_t tot = q == 0 ? tileTot[0] : tileTot[kArrays - 1];
+      uint64_t* state = ws.scanState + (size_t(e) * kScanCalls + arr(q).call) * ws.scanTiles;
+      const uint32_t tag = (ws.scanEpoch[e] * kScanCalls + arr(q).call) & 0x3fffffffu;
       uint32_t prefix = 0;
       if (t == 0) {
-        if (lane == 0) publish(state, stateWord(tag, kStatusPrefix, tileTot));
+        if (lane == 0) publish(state, stateWord(tag, kStatusPrefix, tot));
       } else {
-        if (lane == 0) publish(state + t, stateWord(tag, kStatusSum, tileTot));
+        if (lane == 0) publish(state + t, stateWord(tag, kStatusSum, tot));
         int32_t k = int32_t(t) - 1;  // the window covers tiles k - 31 .. k
         uint32_t polls = 0;
         bool stalled = false;
@@ -112,27 +130,40 @@ __global__ void __launch_bounds__(kScanThreads, 3)
         }
         if (lane == 0) {
           if (stalled) atomicOr(&ws.ev[e].flags, kFlagScanStall);
-          publish(state + t, stateWord(tag, kStatusPrefix, prefix + tileTot));
+          publish(state + t, stateWord(tag, kStatusPrefix, prefix + tot));
         }
       }
-      if (lane == 0) sPrefix = prefix;
+      if (lane == 0) sPrefix[q] = prefix;
     }
     __syncthreads();
-    const uint32_t carry = sPrefix + base;
 #pragma unroll
-    for (uint32_t j = 0; j < kScanPer; ++j) {
-      const uint32_t i = w0 + j * 32;
-      if (i < hi) {
-        if (zeroIn) src[i] = 0u;
-        dst[i] = carry + v[j];
+    for (uint32_t q = 0; q < kArrays; ++q) {
+      uint32_t* src = arr(q).in + size_t(e) * stride;
+      uint32_t* dst = arr(q).out + size_t(e) * stride;
+      const uint32_t carry = sPrefix[q] + base[q];
+#pragma unroll
+      for (uint32_t j = 0; j < kScanPer; ++j) {
+        const uint32_t i = w0 + j * 32;
+        if (i < hi) {
+          if (zeroIn) src[i] = 0u;
+          dst[i] = carry + v[q][j];
+        }
       }
-    }
-    if (t == tiles - 1 && threadIdx.x == 0) {
-      dst[n] = sPrefix + tileTot;
-      if (totalPtr) totalPtr[size_t(e) * totalStride] = sPrefix + tileTot;
+      if (t == tiles - 1 && threadIdx.x == 0) {
+        dst[n] = sPrefix[q] + tileTot[q];
+        if (arr(q).total) arr(q).total[size_t(e) * totalStride] = sPrefix[q] + tileTot[q];
+      }
     }
     __syncthreads();  // sTile and sPrefix are rewritten by the next tile
   }
+}
+
+// CTAs per event: every tile of the longest array at once for small
+// batches; a CTA takes further tiles while there are any
+dim3 scanGrid(uint32_t maxLen, uint32_t nEvents) {
+  const uint32_t tiles = max(1u, (maxLen + kScanTile - 1) / kScanTile);
+  const uint32_t S = max(1u, min(tiles, max(8u, 1024u / max(nEvents, 1u))));
+  return dim3(S, nEvents);
 }
 
 }  // namespace
@@ -140,14 +171,20 @@ __global__ void __launch_bounds__(kScanThreads, 3)
 void segScan(const Workspace& ws, ScanCall call, uint32_t* in, uint32_t* out, uint32_t stride,
              const uint32_t* lenPtr, uint32_t lenStride, uint32_t maxLen, uint32_t* totalPtr, uint32_t totalStride,
              uint32_t nEvents, cudaStream_t stream, bool zeroIn) {
-  // CTAs per event: every tile of the longest array at once for small
-  // batches; a CTA takes further tiles while there are any
-  const uint32_t tiles = max(1u, (maxLen + kScanTile - 1) / kScanTile);
-  const uint32_t S = max(1u, min(tiles, max(8u, 1024u / max(nEvents, 1u))));
-  const dim3 g(S, nEvents);
+  const ScanArray a{in, out, totalPtr, uint32_t(call)};
   PG_PROBED("kScanOnePass", stream,
-            kScanOnePass<<<g, kScanThreads, 0, stream>>>(in, out, stride, lenPtr, lenStride, maxLen, totalPtr,
-                                                         totalStride, zeroIn, ws, uint32_t(call)));
+            kScanOnePass<1><<<scanGrid(maxLen, nEvents), kScanThreads, 0, stream>>>(
+                a, a, stride, lenPtr, lenStride, maxLen, totalStride, zeroIn, ws));
+}
+
+void segScan2(const Workspace& ws, ScanCall call0, uint32_t* in0, uint32_t* out0, uint32_t* total0, ScanCall call1,
+              uint32_t* in1, uint32_t* out1, uint32_t* total1, uint32_t stride, const uint32_t* lenPtr,
+              uint32_t lenStride, uint32_t maxLen, uint32_t totalStride, uint32_t nEvents, cudaStream_t stream,
+              bool zeroIn) {
+  const ScanArray a0{in0, out0, total0, uint32_t(call0)}, a1{in1, out1, total1, uint32_t(call1)};
+  PG_PROBED("kScanOnePass", stream,
+            kScanOnePass<2><<<scanGrid(maxLen, nEvents), kScanThreads, 0, stream>>>(
+                a0, a1, stride, lenPtr, lenStride, maxLen, totalStride, zeroIn, ws));
 }
 
 }  // namespace pixgpu

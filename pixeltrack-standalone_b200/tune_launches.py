@@ -4,7 +4,7 @@ kernel (pg_autotune) for each batch size on seeded synthetic events, and
 writes the per-device cache that Chain.tune_load, run_events.py and bench.py
 read.
 
-  python pixeltrack-standalone_b200/tune_launches.py --sizes 1,2,4,8,16,32,64 --pu 50
+  python pixeltrack-standalone_b200/tune_launches.py --sizes 1,2,4,8,16,32,64 --pu 50 --model calibrated
 
 Entries of other devices already in the cache file are kept.
 """
@@ -24,6 +24,7 @@ def main():
     p = argparse.ArgumentParser()
     p.add_argument("--sizes", default="1,2,4,8,16,32,64", help="batch sizes to tune")
     p.add_argument("--pu", type=float, default=50)
+    p.add_argument("--model", default=pixgpu.BENCH_MODEL, help="event model of the tuning events (dense, calibrated)")
     p.add_argument("--repeats", type=int, default=3, help="timed batches per trial (median)")
     p.add_argument("--seed", type=int, default=pixgpu.BASE_SEED + 9000)
     p.add_argument("--out", default=DEFAULT_CACHE)
@@ -31,7 +32,7 @@ def main():
     sizes = sorted({int(x) for x in a.sizes.split(",") if x.strip()})
     det = pixgpu.Detector()
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
-        raws = list(ex.map(lambda k: det.event(a.seed + k, a.pu), range(max(sizes))))
+        raws = list(ex.map(lambda k: det.event(a.seed + k, a.pu, model=a.model), range(max(sizes))))
     words = max(len(r) // 4 for r in raws)
     chain = pixgpu.Chain(det.es, max_events=max(sizes), max_words_per_batch=words * max(sizes) + 1024, slots=1)
     try:

@@ -87,8 +87,9 @@ KERNEL_BYTES = {
 
 # DRAM bytes per event of a kernel (dram__bytes_read.sum + dram__bytes_write.sum
 # of one ncu capture on 16 PU50 events, divided by 16; traffic scales with the
-# events of a launch), from the full-set capture of these three kernels
-NCU_DRAM_BYTES_PER_EVENT = {"kConnect": 9.25e6, "kDoubletWrite": 4.21e6, "kFishbone": 8.42e6}
+# events of a launch), from the full-set captures of these kernels
+NCU_DRAM_BYTES_PER_EVENT = {"kConnect": 5.17e6, "kDoubletCount": 0.46e6, "kFishbone": 2.51e6, "kNtupletCount": 1.86e6,
+                            "kDoubletWrite": 4.21e6}
 
 
 def chain_bytes(u):

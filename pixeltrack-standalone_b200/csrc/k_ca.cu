@@ -435,22 +435,33 @@ __global__ void kOuterHitFill(Workspace ws) {
 
 // ------------------------------------------------------------------ connect
 
-// GPUCACell::areAlignedRZ: fabs(float) binds to the double overload in the
-// serial build, so the left-hand product is formed in double precision
-__device__ __forceinline__ bool alignedRZ(float r1, float z1, float ri, float zi, float ro, float zo, float thetaCut,
-                                          uint32_t& near) {
+// GPUCACell::areAlignedRZ, single-precision part: false only for pairs that
+// fail the cut by a margin far above rounding (the squared inequality in
+// float with a relative margin of 1e-4; NaN operands, and right-hand sides
+// small enough for the squares to lose precision as subnormals, pass on to
+// the exact test)
+__device__ __forceinline__ bool alignedRZMaybe(float r1, float z1, float ri, float zi, float ro, float zo,
+                                               float thetaCut) {
   float radius_diff = fabsf(r1 - ro);
   float distance_13_squared = radius_diff * radius_diff + (z1 - zo) * (z1 - zo);
   const float area = z1 * (ri - ro) + zi * (ro - r1) + zo * (r1 - ri);
   const float rhs = thetaCut * distance_13_squared * radius_diff;
-  // cheap rejection: the squared inequality in float, with a relative margin
-  // far above its rounding error, rejects only pairs the exact test rejects
-  // (NaN operands, and right-hand sides small enough for the squares to lose
-  // precision as subnormals, fall through to the exact test)
-  if (rhs > 1e-15f && area * area * (kPtMin * kPtMin) * distance_13_squared > 1.0001f * rhs * rhs) return false;
+  return !(rhs > 1e-15f && area * area * (kPtMin * kPtMin) * distance_13_squared > 1.0001f * rhs * rhs);
+}
+
+// GPUCACell::areAlignedRZ: fabs(float) binds to the double overload in the
+// serial build, so the left-hand product is formed in double precision.
+// Pairs the single-precision part drops lie far from the boundary and are
+// not counted as near it.
+__device__ __forceinline__ bool alignedRZ(float r1, float z1, float ri, float zi, float ro, float zo, float thetaCut,
+                                          uint32_t& near) {
+  if (!alignedRZMaybe(r1, z1, ri, zi, ro, zo, thetaCut)) return false;
+  float radius_diff = fabsf(r1 - ro);
+  float distance_13_squared = radius_diff * radius_diff + (z1 - zo) * (z1 - zo);
+  const float area = z1 * (ri - ro) + zi * (ro - r1) + zo * (r1 - ri);
+  const float rhs = thetaCut * distance_13_squared * radius_diff;
   float pMin = kPtMin * sqrtf(distance_13_squared);
   double lhs = fabs(double(area));
-  // pairs the rejection above dropped lie far from the boundary
   near += cutNear(lhs * double(pMin), double(rhs));
   return lhs * double(pMin) <= double(rhs);
 }
@@ -510,14 +521,15 @@ __global__ void kOhRec(Workspace ws) {
 // and the lanes form groups of G candidates (G the power of two covering the
 // list, at most 32), each group testing another cell of the slot, so short
 // candidate lists still keep the lanes busy.
-// Only about 2 % of the pairs pass the r-z alignment test, so the pairs that
-// do are queued (per warp, in shared memory) and the dca test runs on 32
-// queued pairs at a time, every lane busy, instead of on every round that
-// has one passing lane.  Accepted links (oc <- idx) are appended unordered
+// Only about 2 % of the pairs pass the r-z alignment test, so only its
+// single-precision part runs on every pair; the pairs it keeps are queued
+// (per warp, in shared memory), and the exact r-z test (double precision,
+// with its margin count) and the dca test run on 32 queued pairs at a time,
+// every lane busy, instead of on every round that has one surviving lane.  Accepted links (oc <- idx) are appended unordered
 // with one atomic per warp and round.
 constexpr uint32_t kConnectWarps = 8;   // 256 threads
 constexpr uint32_t kConnectQueue = 64;  // ring of queued pairs per warp (a round adds at most 32)
-__global__ void __launch_bounds__(kConnectWarps * 32, 6) kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
+__global__ void __launch_bounds__(kConnectWarps * 32, 5) kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {
   // queued pair: ohRec/ohCells position of the candidate, the cell, the
   // slot's inner hit and the cell's outer hit
   __shared__ uint4 queueA[kConnectWarps][kConnectQueue];
@@ -550,8 +562,12 @@ __global__ void __launch_bounds__(kConnectWarps * 32, 6) kConnect(Workspace ws, 
       p = qe.x;
       idx = qe.y;
       const float4 r1 = ohRec[p];
+      // the slot's inner hit: its cells carry its r and z (kDoubletWrite)
+      const float ri = ws.cellInnerR[cb + idx], zi = ws.cellInnerZ[cb + idx];
+      const float thetaCut = hh.detInd[qe.z] < 1184 ? kThetaCutBarrel : kThetaCutForward;
       const float region = r1.w < 0.f ? kDcaCutInner : kDcaCutOuter;
-      ok = dcaCut(r1.x, r1.y, hh.xg[qe.z], hh.yg[qe.z], hh.xg[qe.w], hh.yg[qe.w], region, near);
+      ok = alignedRZ(fabsf(r1.w), r1.z, ri, zi, hh.rg[qe.w], hh.zg[qe.w], thetaCut, near) &&
+           dcaCut(r1.x, r1.y, hh.xg[qe.z], hh.yg[qe.z], hh.xg[qe.w], hh.yg[qe.w], region, near);
     }
     qHead += nq;
     const uint32_t mask = __ballot_sync(0xffffffffu, ok);
@@ -619,7 +635,7 @@ __global__ void __launch_bounds__(kConnectWarps * 32, 6) kConnect(Workspace ws, 
             const uint32_t t = t0 + grp;
             const uint32_t src = t < nc ? t : 0u;
             const float ro = __shfl_sync(0xffffffffu, sro, src), zo = __shfl_sync(0xffffffffu, szo, src);
-            const bool pass = t < nc && k < m && alignedRZ(rr1, r1.z, ri, zi, ro, zo, thetaCut, near);
+            const bool pass = t < nc && k < m && alignedRZMaybe(rr1, r1.z, ri, zi, ro, zo, thetaCut);
             const uint32_t mask = __ballot_sync(0xffffffffu, pass);
             if (mask == 0) continue;
             const uint32_t oh = __shfl_sync(0xffffffffu, soh, src);

@@ -809,31 +809,121 @@ __global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws, bool 
     __syncwarp();
   };
   // The hits: the list kEdgeScatter made (early fishbone, all links kept),
-  // else all of them.
-  // Hits are taken two at a time: each half of the warp does one when both
-  // have at most 16 cells (most hits have about ten), else the warp does them
-  // one after the other.  A half with fewer than two cells compares nothing.
+  // else all of them.  A lane per hit scans the hit's cells for the used
+  // ones (eight loads in flight); a hit with two to four of them (nearly
+  // all) is compared by its lane alone, the cells in registers put in
+  // ascending order by a sorting network; a hit with more is done by the
+  // whole warp (fishHit).  The lanes' memory accesses overlap instead of
+  // following one another hit after hit.
   const uint32_t* list =
       checkTrack || c->nEdges > min(ws.cap.edges, ws.cap.scratch) ? nullptr : ws.fishHits + size_t(e) * ws.cap.hits;
   const uint32_t n = list ? c->nFishHits : nHits;
-  const uint32_t stride = gridDim.x * kFishWarps;
-  for (uint32_t i = blockIdx.x * kFishWarps + w; i < n; i += 2 * stride) {
-    const uint32_t h = list ? list[i] : i;
-    const uint32_t i2 = i + stride;
-    const uint32_t b1 = ohOff[h], s1 = min(ohOff[h + 1] - b1, uint32_t(PF_MAX_CELLS_PER_HIT));
-    uint32_t h2 = 0, b2 = 0, s2 = 0;
-    if (i2 < n) {
-      h2 = list ? list[i2] : i2;
-      b2 = ohOff[h2];
-      s2 = min(ohOff[h2 + 1] - b2, uint32_t(PF_MAX_CELLS_PER_HIT));
+  const uint32_t stride = gridDim.x * kFishWarps * 32;
+  for (uint32_t i0 = (blockIdx.x * kFishWarps + w) * 32; i0 < n; i0 += stride) {
+    const uint32_t i = i0 + lane;
+    uint32_t h = 0, b = 0, s = 0;
+    if (i < n) {
+      h = list ? list[i] : i;
+      b = ohOff[h];
+      s = min(ohOff[h + 1] - b, uint32_t(PF_MAX_CELLS_PER_HIT));
     }
-    if (s1 <= 16 && s2 <= 16) {
-      const bool second = lane >= 16;
-      const uint32_t s = second ? s2 : s1;
-      fishHit(second ? h2 : h, second ? b2 : b1, s < 2 ? 0u : s, second ? 16u : 0u, second ? 16u : 0u, 16u);
-    } else {
-      if (s1 >= 2) fishHit(h, b1, s1, 0u, 0u, 32u);
-      if (s2 >= 2) fishHit(h2, b2, s2, 0u, 0u, 32u);
+    // the used cells: their number and the list positions of the first four
+    uint32_t nu = 0, k0 = 0, k1 = 0, k2 = 0, k3 = 0;
+    for (uint32_t kb = 0; kb < s; kb += 8) {
+      uint32_t cl[8];
+#pragma unroll
+      for (uint32_t j = 0; j < 8; ++j) cl[j] = kb + j < s ? ohCells[b + kb + j] : 0u;
+#pragma unroll
+      for (uint32_t j = 0; j < 8; ++j) {
+        const uint32_t k = kb + j;
+        const bool used =
+            k < s && ws.cellUsed[cb + cl[j]] && !(checkTrack && trkOff[cl[j] + 1] == trkOff[cl[j]]);
+        if (used) {
+          k0 = nu == 0 ? k : k0;
+          k1 = nu == 1 ? k : k1;
+          k2 = nu == 2 ? k : k2;
+          k3 = nu == 3 ? k : k3;
+          ++nu;
+        }
+      }
+    }
+    if (nu >= 2 && nu <= 4) {
+      const float xo = hh.xg[h], yo = hh.yg[h], zo = hh.zg[h];
+      uint32_t cc[4], dd[4];
+      float xx[4], yy[4], zz[4];
+#pragma unroll
+      for (uint32_t j = 0; j < 4; ++j) {
+        const uint32_t k = j == 0 ? k0 : j == 1 ? k1 : j == 2 ? k2 : k3;
+        cc[j] = 0xffffffffu;  // unused entries sort last
+        dd[j] = 0;
+        xx[j] = yy[j] = zz[j] = 0.f;
+        if (j < nu) {
+          const float4 rec = ohRec[b + k];
+          cc[j] = ohCells[b + k];
+          xx[j] = rec.x - xo;
+          yy[j] = rec.y - yo;
+          zz[j] = rec.z - zo;
+          dd[j] = ohDet[b + k];
+        }
+      }
+      // ascending cell order (the serial loop's order): a sorting network of
+      // five compare-exchanges
+      auto cx = [&](int a, int bb) {
+        if (cc[a] > cc[bb]) {
+          uint32_t t = cc[a];
+          cc[a] = cc[bb];
+          cc[bb] = t;
+          t = dd[a];
+          dd[a] = dd[bb];
+          dd[bb] = t;
+          float f = xx[a];
+          xx[a] = xx[bb];
+          xx[bb] = f;
+          f = yy[a];
+          yy[a] = yy[bb];
+          yy[bb] = f;
+          f = zz[a];
+          zz[a] = zz[bb];
+          zz[bb] = f;
+        }
+      };
+      cx(0, 1);
+      cx(2, 3);
+      cx(0, 2);
+      cx(1, 3);
+      cx(1, 2);
+#pragma unroll
+      for (uint32_t ic = 0; ic < 3; ++ic) {
+        if (ic + 1 < nu) {
+          const float xi = xx[ic], yi = yy[ic], zi = zz[ic];
+          const float ni = xi * xi + yi * yi + zi * zi;
+          bool stop = false;
+#pragma unroll
+          for (uint32_t jc = ic + 1; jc < 4; ++jc) {
+            if (!stop && jc < nu) {
+              const float xj = xx[jc], yj = yy[jc], zj = zz[jc];
+              const float nj = xj * xj + yj * yj + zj * zj;
+              const float cos12 = xi * xj + yi * yj + zi * zj;
+              if (dd[ic] != dd[jc] && cos12 * cos12 >= 0.99999f * ni * nj) {
+                if (ni > nj) {
+                  ws.cellDoubletId[cb + cc[ic]] = -1;
+                  stop = true;
+                } else {
+                  ws.cellDoubletId[cb + cc[jc]] = -1;
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+    // hits with more than four used cells: the whole warp, one at a time
+    uint32_t rest = __ballot_sync(0xffffffffu, nu > 4);
+    while (rest) {
+      const int l = __ffs(rest) - 1;
+      rest &= rest - 1;
+      fishHit(__shfl_sync(0xffffffffu, h, l), __shfl_sync(0xffffffffu, b, l), __shfl_sync(0xffffffffu, s, l), 0u,
+              0u, 32u);
     }
   }
 }

@@ -69,8 +69,6 @@ void layout(Workspace& ws, Carver& c, uint32_t E, uint32_t W, const Caps& cap) {
   c.take(ws.cellPair, C);
   c.take(ws.cellDoubletId, C);
   c.take(ws.cellUsed, C);
-  c.take(ws.cellInnerZ, C);
-  c.take(ws.cellInnerR, C);
   c.take(ws.ohCount, size_t(E) * (cap.hits + 1));
   c.take(ws.ohOff, size_t(E) * (cap.hits + 1));
   c.take(ws.hitTouch, size_t(E) * cap.hits);

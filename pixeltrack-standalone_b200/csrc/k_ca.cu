@@ -332,7 +332,6 @@ __global__ void __launch_bounds__(256, 5) kDoubletWrite(Workspace ws) {
   for (uint32_t r0 = 0; w + r0 * S < ntot; r0 += 32) {
     const uint32_t jl = w + (r0 + lane) * S;
     uint32_t myBase = 0, myN = 0, myAt = kNoTemp, myI = 0, myPair = 0;
-    float myZ = 0.f, myR = 0.f;
     if (jl < ntot) {
       myBase = off[jl];
       myN = myBase < ws.cap.cells ? min(off[jl + 1], ws.cap.cells) - myBase : 0u;
@@ -341,17 +340,13 @@ __global__ void __launch_bounds__(256, 5) kDoubletWrite(Workspace ws) {
       myAt = slotStage[jl];
       while (jl >= pt.pairCum[myPair]) ++myPair;
       myI = (0 == myPair ? jl : jl - pt.pairCum[myPair - 1]) + pt.layerStart[cLayerPairs[2 * myPair]];
-      myZ = hh.zg[myI];
-      myR = hh.rg[myI];
     }
-    auto put = [&](uint32_t idx, uint32_t i, uint32_t pair, float zi, float ri, uint32_t oi) {
+    auto put = [&](uint32_t idx, uint32_t i, uint32_t pair, uint32_t oi) {
       ws.cellInner[cb + idx] = i;
       ws.cellOuter[cb + idx] = oi;
       ws.cellPair[cb + idx] = uint8_t(pair);
       ws.cellDoubletId[cb + idx] = int32_t(idx);
       ws.cellUsed[cb + idx] = 0;
-      ws.cellInnerZ[cb + idx] = zi;
-      ws.cellInnerR[cb + idx] = ri;
       atomicAdd(&ohc[oi], 1u);
     };
     // The staged slots' doublets as one flat range over the warp's 32 slots,
@@ -372,10 +367,9 @@ __global__ void __launch_bounds__(256, 5) kDoubletWrite(Workspace ws) {
       const uint32_t b = __shfl_sync(0xffffffffu, myBase, l), at = __shfl_sync(0xffffffffu, myAt, l);
       const uint32_t x = __shfl_sync(0xffffffffu, excl, l), i = __shfl_sync(0xffffffffu, myI, l);
       const uint32_t pair = __shfl_sync(0xffffffffu, myPair, l);
-      const float zi = __shfl_sync(0xffffffffu, myZ, l), ri = __shfl_sync(0xffffffffu, myR, l);
       if (f < total) {
         const uint32_t k = f - x;
-        put(b + k, i, pair, zi, ri, stage[at + k]);
+        put(b + k, i, pair, stage[at + k]);
       }
     }
     // slots whose doublets did not fit the count pass's staging: found again
@@ -386,11 +380,10 @@ __global__ void __launch_bounds__(256, 5) kDoubletWrite(Workspace ws) {
       const uint32_t j = w + (r0 + uint32_t(l)) * S;
       const uint32_t base = __shfl_sync(0xffffffffu, myBase, l), n = __shfl_sync(0xffffffffu, myN, l);
       const uint32_t i = __shfl_sync(0xffffffffu, myI, l), pair = __shfl_sync(0xffffffffu, myPair, l);
-      const float zi = __shfl_sync(0xffffffffu, myZ, l), ri = __shfl_sync(0xffffffffu, myR, l);
       DoubletSeed d;
       doubletSeed(pt, hh, j, d);
       warpDoublets(d, rec, [&](uint32_t k, uint32_t oi) {
-        if (k < n) put(base + k, i, pair, zi, ri, oi);
+        if (k < n) put(base + k, i, pair, oi);
       });
     }
   }
@@ -506,9 +499,9 @@ __global__ void kOhRec(Workspace ws) {
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     const uint32_t oc = ws.ohCells[cb + p];
     const uint32_t ih = ws.cellInner[cb + oc];
-    const float r = ws.cellInnerR[cb + oc];
+    const float r = ws.rg[hb + ih];
     const uint16_t det = ws.detInd[hb + ih];
-    ws.ohRec[cb + p] = make_float4(ws.xg[hb + ih], ws.yg[hb + ih], ws.cellInnerZ[cb + oc], det < 96 ? -r : r);
+    ws.ohRec[cb + p] = make_float4(ws.xg[hb + ih], ws.yg[hb + ih], ws.zg[hb + ih], det < 96 ? -r : r);
     ws.ohDet[cb + p] = det;
   }
 }
@@ -562,8 +555,7 @@ __global__ void __launch_bounds__(kConnectWarps * 32, 5) kConnect(Workspace ws, 
       p = qe.x;
       idx = qe.y;
       const float4 r1 = ohRec[p];
-      // the slot's inner hit: its cells carry its r and z (kDoubletWrite)
-      const float ri = ws.cellInnerR[cb + idx], zi = ws.cellInnerZ[cb + idx];
+      const float ri = hh.rg[qe.z], zi = hh.zg[qe.z];  // the slot's inner hit
       const float thetaCut = hh.detInd[qe.z] < 1184 ? kThetaCutBarrel : kThetaCutForward;
       const float region = r1.w < 0.f ? kDcaCutInner : kDcaCutOuter;
       ok = alignedRZ(fabsf(r1.w), r1.z, ri, zi, hh.rg[qe.w], hh.zg[qe.w], thetaCut, near) &&
@@ -612,7 +604,7 @@ __global__ void __launch_bounds__(kConnectWarps * 32, 5) kConnect(Workspace ws, 
       const uint32_t ob = __shfl_sync(0xffffffffu, myOb, l);
       const uint32_t m = __shfl_sync(0xffffffffu, myM, l);
       const uint32_t h = ws.cellInner[cb + base];
-      const float ri = ws.cellInnerR[cb + base], zi = ws.cellInnerZ[cb + base];
+      const float ri = hh.rg[h], zi = hh.zg[h];
       const float thetaCut = hh.detInd[h] < 1184 ? kThetaCutBarrel : kThetaCutForward;
       // lanes form 32/G groups of G >= m candidates; each group tests one cell
       const uint32_t G = m > 16 ? 32u : (m > 8 ? 16u : (m > 4 ? 8u : (m > 2 ? 4u : (m > 1 ? 2u : 1u))));

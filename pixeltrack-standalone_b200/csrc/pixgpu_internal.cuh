@@ -278,7 +278,6 @@ struct Workspace {
   uint8_t* cellPair;
   int32_t* cellDoubletId;
   uint8_t* cellUsed;
-  float *cellInnerZ, *cellInnerR;
   // cells by outer hit (isOuterHitOfCell), CSR sorted ascending
   uint32_t* ohCount;         // [maxEvents][cap.hits + 1]
   uint32_t* ohOff;           // [maxEvents][cap.hits + 1]

@@ -88,8 +88,7 @@ KERNEL_BYTES = {
 # DRAM bytes per event of a kernel (dram__bytes_read.sum + dram__bytes_write.sum
 # of one ncu capture on 16 PU50 events, divided by 16; traffic scales with the
 # events of a launch), from the full-set captures of these kernels
-NCU_DRAM_BYTES_PER_EVENT = {"kConnect": 5.17e6, "kDoubletCount": 0.46e6, "kFishbone": 2.51e6, "kNtupletCount": 1.86e6,
-                            "kDoubletWrite": 4.21e6}
+NCU_DRAM_BYTES_PER_EVENT = {"kConnect": 4.41e6, "kDoubletCount": 0.46e6, "kFishbone": 2.51e6, "kNtupletCount": 1.83e6}
 
 
 def chain_bytes(u):
@@ -105,7 +104,7 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--batch", type=int, default=64, help="events per launch sequence")
     p.add_argument("--events", type=int, default=1000, help="distinct PU50 events (inputs > L2)")
-    p.add_argument("--slots", type=int, default=3, help="batches in flight")
+    p.add_argument("--slots", type=int, default=4, help="batches in flight")
     p.add_argument("--per-event", type=int, default=256, help="events for the one-event-per-launch leg")
     p.add_argument("--serve", type=int, default=4000, help="requests for the serving leg (0: skip)")
     p.add_argument("--serve-batch", type=int, default=32, help="max events per serving batch")

@@ -73,6 +73,9 @@ KERNEL_BYTES = {
     "kModuleBoundaries": lambda u: 6.0 * u["W"],
     "kFindClusters": lambda u: 24.0 * u["W"],         # findClus 10*W + charge cut 14*W (fused)
     "kGetHits": lambda u: 12.0 * u["W"] + 44.0 * u["H"] + 112.0 * u["M"],
+    # doublets: the count pass reads each hit's packed record and writes each
+    # doublet's outer hit once (staged); the write pass the doublet columns
+    "kDoubletCount": lambda u: 16.0 * u["H"] + 4.0 * u["C"],
     "kDoubletWrite": lambda u: 14.0 * u["H"] + 44.0 * u["C"],
     "kConnect": lambda u: 40.0 * u["C"] + 8.0 * u["E"],
     "kFishbone": lambda u: 16.0 * u["C"],
@@ -442,21 +445,34 @@ def run_ours(a):
     events = a.steps * B
     value, ms = replicas.job_rate(events, ms, device="cuda")
     kernel_ms = float(np.mean(probe_ms)) if probe_ms else None
-    launches_of_top = launches[top]
     hbm, peak_kind = peaks()
     u_evt = {k: v / events for k, v in units.items()}
-    roof = None
-    if kernel_ms and top in KERNEL_BYTES:
+
+    def roofline_of(name, k_ms, n_timed):
+        if not k_ms or name not in KERNEL_BYTES:
+            return None
         # bytes of one launch: the kernel processes the whole batch (B events) per launch,
         # split evenly over its launches per batch
-        bytes_per_launch = KERNEL_BYTES[top](u_evt) * B / launches_of_top
-        ach = bytes_per_launch / (kernel_ms / 1e3) / 1e9
-        roof = {"bound": "hbm", "kernel": top, "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                "traffic": (NCU_DRAM_BYTES_PER_EVENT[top] * B / launches_of_top
-                            if top in NCU_DRAM_BYTES_PER_EVENT else None),
+        bytes_per_launch = KERNEL_BYTES[name](u_evt) * B / launches[name]
+        ach = bytes_per_launch / (k_ms / 1e3) / 1e9
+        return {"bound": "hbm", "kernel": name, "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "traffic": (NCU_DRAM_BYTES_PER_EVENT[name] * B / launches[name]
+                            if name in NCU_DRAM_BYTES_PER_EVENT else None),
                 "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback 6650 GB/s",
-                "bytes_per_launch": bytes_per_launch, "launch_ms": kernel_ms, "launches_timed": len(probe_ms)}
+                "bytes_per_launch": bytes_per_launch, "launch_ms": k_ms, "launches_timed": n_timed}
+
+    roof = roofline_of(top, kernel_ms, len(probe_ms))
+    # the second kernel of the census, timed the same way over a shorter run
+    second = sorted(census, key=census.get)[-2] if len(census) > 1 else None
+    roof_next = None
+    if second:
+        chain.set_probe(second)
+        chain.prepare(B)
+        probe_ms.clear()
+        pipeline(chain, torch, max(a.steps // 4, 10), sub, lambda slot: probe_ms.extend(
+            m for _, m in chain.probe_read(slot)))
+        roof_next = roofline_of(second, float(np.mean(probe_ms)) if probe_ms else None, len(probe_ms))
     chain_ach = chain_bytes(u_evt) * value / world / 1e9
     chain.set_probe(None)
     chain.close()
@@ -474,7 +490,7 @@ def run_ours(a):
            "gpu_launches": launches_per_batch * a.steps,
            "launch_tuning": tuning,
            "clocks": clocks,
-           "roofline": roof,
+           "roofline": roof, "roofline_next": roof_next,
            "chain_roofline": {"achieved": chain_ach, "peak": hbm, "unit": "GB/s", "frac": chain_ach / hbm,
                               "bytes_per_event": chain_bytes(u_evt)},
            "units_per_event": u_evt,
@@ -566,7 +582,10 @@ def run_ours(a):
                         " + chain + results into mapped host memory"}
 
     legs = {scan: e2e_leg(scan) for scan in ("host", "device")}
-    out["e2e"] = legs[pixgpu.default_config().get("fed_scan") and "device" or "host"]
+    # the headline is the faster of the two public configurations (pg_config.fed_scan);
+    # both give the same products (tests/test_gpu_errors.py)
+    best_scan = max(legs, key=lambda k: legs[k]["value"])
+    out["e2e"] = dict(legs[best_scan], fed_scan=best_scan)
     out["e2e_by_fed_scan"] = {k: v["value"] for k, v in legs.items()}
 
     if rank == 0 and world == 1:

@@ -606,9 +606,11 @@ __global__ void __launch_bounds__(kConnectWarps * 32, 5) kConnect(Workspace ws, 
       const uint32_t h = ws.cellInner[cb + base];
       const float ri = hh.rg[h], zi = hh.zg[h];
       const float thetaCut = hh.detInd[h] < 1184 ? kThetaCutBarrel : kThetaCutForward;
-      // lanes form 32/G groups of G >= m candidates; each group tests one cell
-      const uint32_t G = m > 16 ? 32u : (m > 8 ? 16u : (m > 4 ? 8u : (m > 2 ? 4u : (m > 1 ? 2u : 1u))));
+      // lanes form R = 32/G groups of G = m candidates (up to 16; 32 above):
+      // each group tests one cell, lanes past the R groups idle
+      const uint32_t G = m > 16 ? 32u : m;
       const uint32_t R = 32u / G, grp = lane / G, kk = lane % G;
+      const bool inGroup = grp < R;
       for (uint32_t c0 = base; c0 < end; c0 += 32) {
         const uint32_t nc = min(32u, end - c0);
         float sro = 0.f, szo = 0.f;
@@ -627,7 +629,7 @@ __global__ void __launch_bounds__(kConnectWarps * 32, 5) kConnect(Workspace ws, 
             const uint32_t t = t0 + grp;
             const uint32_t src = t < nc ? t : 0u;
             const float ro = __shfl_sync(0xffffffffu, sro, src), zo = __shfl_sync(0xffffffffu, szo, src);
-            const bool pass = t < nc && k < m && alignedRZMaybe(rr1, r1.z, ri, zi, ro, zo, thetaCut);
+            const bool pass = inGroup && t < nc && k < m && alignedRZMaybe(rr1, r1.z, ri, zi, ro, zo, thetaCut);
             const uint32_t mask = __ballot_sync(0xffffffffu, pass);
             if (mask == 0) continue;
             const uint32_t oh = __shfl_sync(0xffffffffu, soh, src);

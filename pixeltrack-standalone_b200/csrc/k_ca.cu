@@ -511,9 +511,8 @@ __global__ void kOhRec(Workspace ws) {
 // candidate list (cells ending on h, first 128 in ascending order).  A warp
 // looks at 32 slots at once (warp w: slots w, w + S, ...) and takes the
 // non-empty ones in turn; for a slot, lane t stages the outer hit of cell t
-// and the lanes form groups of G candidates (G the power of two covering the
-// list, at most 32), each group testing another cell of the slot, so short
-// candidate lists still keep the lanes busy.
+// and the warp takes the slot's (cell, candidate) pairs flat, 32 at a time,
+// so short candidate lists still keep the lanes busy.
 // Only about 2 % of the pairs pass the r-z alignment test, so only its
 // single-precision part runs on every pair; the pairs it keeps are queued
 // (per warp, in shared memory), and the exact r-z test (double precision,
@@ -606,11 +605,13 @@ __global__ void __launch_bounds__(kConnectWarps * 32, 5) kConnect(Workspace ws, 
       const uint32_t h = ws.cellInner[cb + base];
       const float ri = hh.rg[h], zi = hh.zg[h];
       const float thetaCut = hh.detInd[h] < 1184 ? kThetaCutBarrel : kThetaCutForward;
-      // lanes form R = 32/G groups of G = m candidates (up to 16; 32 above):
-      // each group tests one cell, lanes past the R groups idle
-      const uint32_t G = m > 16 ? 32u : m;
-      const uint32_t R = 32u / G, grp = lane / G, kk = lane % G;
-      const bool inGroup = grp < R;
+      // the slot's (cell, candidate) pairs enumerated flat, 32 at a time:
+      // pair f is cell f / m of the chunk and candidate f % m, so only the
+      // last step of a chunk leaves lanes idle.  f < 32 * 128, so the
+      // quotient from the single-precision reciprocal is exact (the error,
+      // below 2^-11, is far under the 0.5 / m that (f + 0.5) / m keeps from
+      // an integer).
+      const float invM = 1.f / float(m);
       for (uint32_t c0 = base; c0 < end; c0 += 32) {
         const uint32_t nc = min(32u, end - c0);
         float sro = 0.f, szo = 0.f;
@@ -620,23 +621,22 @@ __global__ void __launch_bounds__(kConnectWarps * 32, 5) kConnect(Workspace ws, 
           sro = hh.rg[soh];
           szo = hh.zg[soh];
         }
-        for (uint32_t k0 = 0; k0 < m; k0 += G) {
-          const uint32_t k = k0 + kk;
+        const uint32_t P = nc * m;
+        for (uint32_t f0 = 0; f0 < P; f0 += 32) {
+          const uint32_t f = f0 + lane;
+          const bool valid = f < P;
+          const uint32_t t = valid ? uint32_t((float(f) + 0.5f) * invM) : 0u;
+          const uint32_t k = f - t * m;
+          const float ro = __shfl_sync(0xffffffffu, sro, t), zo = __shfl_sync(0xffffffffu, szo, t);
           float4 r1 = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (k < m) r1 = ohRec[ob + k];
-          const float rr1 = fabsf(r1.w);
-          for (uint32_t t0 = 0; t0 < nc; t0 += R) {
-            const uint32_t t = t0 + grp;
-            const uint32_t src = t < nc ? t : 0u;
-            const float ro = __shfl_sync(0xffffffffu, sro, src), zo = __shfl_sync(0xffffffffu, szo, src);
-            const bool pass = inGroup && t < nc && k < m && alignedRZMaybe(rr1, r1.z, ri, zi, ro, zo, thetaCut);
-            const uint32_t mask = __ballot_sync(0xffffffffu, pass);
-            if (mask == 0) continue;
-            const uint32_t oh = __shfl_sync(0xffffffffu, soh, src);
-            if (pass) queue[(qTail + __popc(mask & lanemaskLt())) & (kConnectQueue - 1)] = make_uint4(ob + k, c0 + t, h, oh);
-            qTail += __popc(mask);
-            if (qTail - qHead >= 32) drain(32);
-          }
+          if (valid) r1 = ohRec[ob + k];
+          const bool pass = valid && alignedRZMaybe(fabsf(r1.w), r1.z, ri, zi, ro, zo, thetaCut);
+          const uint32_t mask = __ballot_sync(0xffffffffu, pass);
+          if (mask == 0) continue;
+          const uint32_t oh = __shfl_sync(0xffffffffu, soh, t);
+          if (pass) queue[(qTail + __popc(mask & lanemaskLt())) & (kConnectQueue - 1)] = make_uint4(ob + k, c0 + t, h, oh);
+          qTail += __popc(mask);
+          if (qTail - qHead >= 32) drain(32);
         }
       }
     }

@@ -91,7 +91,7 @@ KERNEL_BYTES = {
 # DRAM bytes per event of a kernel (dram__bytes_read.sum + dram__bytes_write.sum
 # of one ncu capture on 16 PU50 events, divided by 16; traffic scales with the
 # events of a launch), from the full-set captures of these kernels
-NCU_DRAM_BYTES_PER_EVENT = {"kConnect": 4.41e6, "kDoubletCount": 0.46e6, "kFishbone": 2.51e6, "kNtupletCount": 1.83e6}
+NCU_DRAM_BYTES_PER_EVENT = {"kConnect": 4.39e6, "kDoubletCount": 0.46e6, "kFishbone": 2.51e6, "kNtupletCount": 1.83e6}
 
 
 def chain_bytes(u):

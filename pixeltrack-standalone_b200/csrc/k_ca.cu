@@ -583,15 +583,28 @@ __global__ void __launch_bounds__(kConnectWarps * 32, 5) kConnect(Workspace ws, 
     __syncwarp();  // the entries are read before the next round overwrites them
   };
   for (uint32_t r0 = 0; w + r0 * S < ntot; r0 += 32) {
+    // each lane sets up one slot (its inner hit and that hit's r, z and
+    // cut), so that the warp's loads for 32 slots overlap
     const uint32_t jl = w + (r0 + lane) * S;
-    uint32_t myBase = 0, myEnd = 0, myOb = 0, myM = 0;
+    uint32_t myBase = 0, myEnd = 0, myOb = 0, myM = 0, myH = 0;
+    float myRi = 0.f, myZi = 0.f, myTheta = 0.f, myInvM = 0.f;
     if (jl < ntot) {
       myBase = joff[jl];
       myEnd = min(joff[jl + 1], nCells);
       if (myBase < myEnd) {
-        const uint32_t h = ws.cellInner[cb + myBase];
-        myOb = ohOff[h];
-        myM = min(ohOff[h + 1] - myOb, uint32_t(PF_MAX_CELLS_PER_HIT));
+        myH = ws.cellInner[cb + myBase];
+        myOb = ohOff[myH];
+        myM = min(ohOff[myH + 1] - myOb, uint32_t(PF_MAX_CELLS_PER_HIT));
+        myRi = hh.rg[myH];
+        myZi = hh.zg[myH];
+        myTheta = hh.detInd[myH] < 1184 ? kThetaCutBarrel : kThetaCutForward;
+        // the slot's (cell, candidate) pairs are enumerated flat, 32 at a
+        // time: pair f is cell f / m of a chunk and candidate f % m, so only
+        // the last step of a chunk leaves lanes idle.  f < 32 * 128, so the
+        // quotient from the single-precision reciprocal is exact (the error,
+        // below 2^-11, is far under the 0.5 / m that (f + 0.5) / m keeps
+        // from an integer).
+        if (myM > 0) myInvM = 1.f / float(myM);
       }
     }
     uint32_t live = __ballot_sync(0xffffffffu, myBase < myEnd && myM > 0);
@@ -602,16 +615,10 @@ __global__ void __launch_bounds__(kConnectWarps * 32, 5) kConnect(Workspace ws, 
       const uint32_t end = __shfl_sync(0xffffffffu, myEnd, l);
       const uint32_t ob = __shfl_sync(0xffffffffu, myOb, l);
       const uint32_t m = __shfl_sync(0xffffffffu, myM, l);
-      const uint32_t h = ws.cellInner[cb + base];
-      const float ri = hh.rg[h], zi = hh.zg[h];
-      const float thetaCut = hh.detInd[h] < 1184 ? kThetaCutBarrel : kThetaCutForward;
-      // the slot's (cell, candidate) pairs enumerated flat, 32 at a time:
-      // pair f is cell f / m of the chunk and candidate f % m, so only the
-      // last step of a chunk leaves lanes idle.  f < 32 * 128, so the
-      // quotient from the single-precision reciprocal is exact (the error,
-      // below 2^-11, is far under the 0.5 / m that (f + 0.5) / m keeps from
-      // an integer).
-      const float invM = 1.f / float(m);
+      const uint32_t h = __shfl_sync(0xffffffffu, myH, l);
+      const float ri = __shfl_sync(0xffffffffu, myRi, l), zi = __shfl_sync(0xffffffffu, myZi, l);
+      const float thetaCut = __shfl_sync(0xffffffffu, myTheta, l);
+      const float invM = __shfl_sync(0xffffffffu, myInvM, l);
       for (uint32_t c0 = base; c0 < end; c0 += 32) {
         const uint32_t nc = min(32u, end - c0);
         float sro = 0.f, szo = 0.f;

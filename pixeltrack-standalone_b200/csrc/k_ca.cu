@@ -517,8 +517,9 @@ __global__ void kOhRec(Workspace ws) {
 // single-precision part runs on every pair; the pairs it keeps are queued
 // (per warp, in shared memory), and the exact r-z test (double precision,
 // with its margin count) and the dca test run on 32 queued pairs at a time,
-// every lane busy, instead of on every round that has one surviving lane.  Accepted links (oc <- idx) are appended unordered
-// with one atomic per warp and round.
+// every lane busy, instead of on every round that has one surviving lane.
+// Accepted links (oc <- idx) are appended unordered with one atomic per warp
+// and round.
 constexpr uint32_t kConnectWarps = 8;   // 256 threads
 constexpr uint32_t kConnectQueue = 64;  // ring of queued pairs per warp (a round adds at most 32)
 __global__ void __launch_bounds__(kConnectWarps * 32, 5) kConnect(Workspace ws, uint32_t* edgeOc, uint32_t* edgeIdx) {

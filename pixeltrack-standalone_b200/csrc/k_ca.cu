@@ -750,10 +750,10 @@ __global__ void __launch_bounds__(kFishWarps * 32) kFishbone(Workspace ws, bool 
   uint8_t* sk = skA[w];
   uint32_t* raw = rawA[w];
   uint32_t* sc = scA[w];
-  // One hit, done by the `width` lanes starting at lane g0 (the whole warp
-  // for up to 128 cells, a half warp for up to 16): the used cells, with
-  // their list positions, compacted at raw/sk[o..] in list order, then
-  // staged in ascending cell order at sx..sc[o..] and compared.
+  // One hit, done by the `width` lanes starting at lane g0 (the loop below
+  // gives it the whole warp, for hits with more than four used cells): the
+  // used cells, with their list positions, compacted at raw/sk[o..] in list
+  // order, then staged in ascending cell order at sx..sc[o..] and compared.
   auto fishHit = [&](uint32_t h, uint32_t b, uint32_t s, uint32_t o, uint32_t g0, uint32_t width) {
     const uint32_t gl = lane - g0;
     const uint32_t gmask = width == 32 ? 0xffffffffu : ((1u << width) - 1u) << g0;
